@@ -1,0 +1,14 @@
+// errors.hpp — status codes and the per-thread last-error message of the C ABI.
+#pragma once
+#include <string>
+
+#include "crush.h"
+
+namespace crush {
+
+// Records `msg` as the calling thread's last error and returns `code`.
+int fail(int code, const std::string& msg);
+const std::string& last_error();
+void clear_error();
+
+}  // namespace crush

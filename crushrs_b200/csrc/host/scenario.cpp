@@ -1,0 +1,576 @@
+// scenario.cpp — host-side model construction (C++17).
+//
+// Restates the reference's mesh generator and vehicle scenario builders so
+// that a model built here is node-for-node, face-for-face the model crushrs
+// builds (see include/crush_scenario.h for the reference functions covered).
+// Model construction is host work at set-up; the per-step path is on the GPU.
+#include "crush_scenario.h"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "errors.hpp"
+
+namespace {
+
+enum BlockFace { XMin = 1, XMax = 2, YMin = 4, YMax = 8, ZMin = 16, ZMax = 32 };
+
+struct ContactDef {
+    std::vector<uint32_t> nodes;
+    std::vector<double> scale;
+    std::vector<uint32_t> faces;  // 4 per face
+    double stiffness = 0.0, max_distance = 0.0;
+};
+struct VehicleDef {
+    std::vector<uint32_t> nodes;
+    uint32_t accel = 0;
+    std::vector<uint32_t> front;
+};
+
+}  // namespace
+
+struct crush_model {
+    std::vector<double> positions;
+    std::vector<uint32_t> hexes;
+    std::vector<int32_t> hex_part;
+    std::vector<std::string> part_names;
+    std::vector<crush_material> materials;
+    std::vector<double> velocity;
+    std::vector<uint32_t> fixed;
+    std::vector<std::array<uint32_t, 4>> faces;
+    std::vector<std::vector<size_t>> face_set_list;  // in creation order
+    std::map<std::string, size_t> face_set_index;
+    std::map<std::string, std::vector<uint32_t>> node_sets;
+    std::vector<ContactDef> contacts;
+    std::vector<VehicleDef> vehicles;
+    crush_settings settings;
+    // descriptor views
+    std::vector<crush_contact> contact_desc;
+    std::vector<crush_vehicle> vehicle_desc;
+};
+
+namespace {
+
+crush_material elastic_material(double e, double nu, double rho) {
+    crush_material m;
+    std::memset(&m, 0, sizeof(m));
+    m.model = CRUSH_MAT_ELASTIC;
+    m.youngs_modulus = e;
+    m.poisson_ratio = nu;
+    m.density = rho;
+    m.transverse_factor = 1.0;
+    return m;
+}
+
+size_t add_part(crush_model* m, const std::string& name) {
+    m->part_names.push_back(name);
+    m->materials.push_back(elastic_material(1.0, 0.0, 1.0));  // Model::new default, src/model.rs:170
+    return m->part_names.size() - 1;
+}
+
+int part_index(const crush_model* m, const std::string& name) {
+    for (size_t p = 0; p < m->part_names.size(); ++p)
+        if (m->part_names[p] == name) return (int)p;
+    return -1;
+}
+
+// Mesh::add_hex_block_n, src/mesh.rs:117-171. surfaces: (face bit, set name) in order.
+size_t add_hex_block_n(crush_model* m, const std::string& part_name, const double origin[3], const double size[3],
+                       const int32_t n_in[3], const std::vector<std::pair<int, std::string>>& surfaces) {
+    size_t n[3];
+    for (int a = 0; a < 3; ++a) n[a] = (size_t)std::max<int32_t>(n_in[a], 1);
+    double d[3];
+    for (int a = 0; a < 3; ++a) d[a] = size[a] / (double)n[a];
+    size_t node0 = m->positions.size() / 3;
+    auto id = [&](size_t i, size_t j, size_t k) { return (uint32_t)(node0 + i + (n[0] + 1) * (j + (n[1] + 1) * k)); };
+    for (size_t k = 0; k <= n[2]; ++k)
+        for (size_t j = 0; j <= n[1]; ++j)
+            for (size_t i = 0; i <= n[0]; ++i) {
+                m->positions.push_back(origin[0] + (double)i * d[0]);
+                m->positions.push_back(origin[1] + (double)j * d[1]);
+                m->positions.push_back(origin[2] + (double)k * d[2]);
+                m->velocity.insert(m->velocity.end(), {0.0, 0.0, 0.0});
+            }
+    size_t part = add_part(m, part_name);
+    for (size_t k = 0; k < n[2]; ++k)
+        for (size_t j = 0; j < n[1]; ++j)
+            for (size_t i = 0; i < n[0]; ++i) {
+                uint32_t h[8] = {id(i, j, k), id(i + 1, j, k), id(i + 1, j + 1, k), id(i, j + 1, k),
+                                 id(i, j, k + 1), id(i + 1, j, k + 1), id(i + 1, j + 1, k + 1), id(i, j + 1, k + 1)};
+                m->hexes.insert(m->hexes.end(), h, h + 8);
+                m->hex_part.push_back((int32_t)part);
+            }
+    for (const auto& sf : surfaces) {
+        int a;
+        bool max_side;
+        switch (sf.first) {
+            case XMin: a = 0; max_side = false; break;
+            case XMax: a = 0; max_side = true; break;
+            case YMin: a = 1; max_side = false; break;
+            case YMax: a = 1; max_side = true; break;
+            case ZMin: a = 2; max_side = false; break;
+            default: a = 2; max_side = true; break;
+        }
+        int b = (a + 1) % 3, c = (a + 2) % 3;
+        size_t fixed = max_side ? n[a] : 0;
+        auto at = [&](size_t ib, size_t ic) {
+            size_t ijk[3];
+            ijk[a] = fixed;
+            ijk[b] = ib;
+            ijk[c] = ic;
+            return id(ijk[0], ijk[1], ijk[2]);
+        };
+        std::vector<size_t> set;
+        for (size_t ic = 0; ic < n[c]; ++ic)
+            for (size_t ib = 0; ib < n[b]; ++ib) {
+                uint32_t p0 = at(ib, ic), p1 = at(ib + 1, ic), p2 = at(ib + 1, ic + 1), p3 = at(ib, ic + 1);
+                if (max_side) m->faces.push_back({p0, p1, p2, p3});
+                else m->faces.push_back({p0, p3, p2, p1});
+                set.push_back(m->faces.size() - 1);
+            }
+        m->face_set_index[sf.second] = m->face_set_list.size();
+        m->face_set_list.push_back(set);
+    }
+    std::vector<uint32_t> all;
+    for (size_t i = node0; i < m->positions.size() / 3; ++i) all.push_back((uint32_t)i);
+    m->node_sets[part_name] = all;
+    return part;
+}
+
+// Mesh::add_hex_block, src/mesh.rs:111 (n = round(size / h), at least 1; f64::round rounds half away from zero).
+size_t add_hex_block(crush_model* m, const std::string& part_name, const double origin[3], const double size[3], double h,
+                     const std::vector<std::pair<int, std::string>>& surfaces) {
+    int32_t n[3];
+    for (int a = 0; a < 3; ++a) n[a] = (int32_t)std::max(std::round(size[a] / h), 1.0);
+    return add_hex_block_n(m, part_name, origin, size, n, surfaces);
+}
+
+const std::vector<size_t>* face_set(const crush_model* m, const std::string& name) {
+    auto it = m->face_set_index.find(name);
+    return it == m->face_set_index.end() ? nullptr : &m->face_set_list[it->second];
+}
+
+// Mesh::face_set_nodes, src/mesh.rs:97 (sorted, unique).
+bool face_set_nodes(const crush_model* m, const std::string& name, std::vector<uint32_t>* out) {
+    const std::vector<size_t>* set = face_set(m, name);
+    if (!set) return false;
+    std::set<uint32_t> s;
+    for (size_t f : *set) s.insert(m->faces[f].begin(), m->faces[f].end());
+    out->assign(s.begin(), s.end());
+    return true;
+}
+
+// Mesh::part_nodes, src/mesh.rs:74.
+std::vector<uint32_t> part_nodes(const crush_model* m, int part) {
+    std::set<uint32_t> s;
+    for (size_t e = 0; e < m->hex_part.size(); ++e)
+        if (m->hex_part[e] == part) s.insert(&m->hexes[8 * e], &m->hexes[8 * e] + 8);
+    return std::vector<uint32_t>(s.begin(), s.end());
+}
+
+// Material::scaled, src/material.rs:200.
+crush_material scaled(const crush_material& in, double f) {
+    crush_material m = in;
+    m.youngs_modulus *= f;
+    m.density *= f;
+    m.yield_stress *= f;
+    m.hardening *= f;
+    for (int i = 0; i < m.n_curve; ++i) m.curve[i][1] *= f;
+    if (m.has_densification) m.densification[1] *= f;
+    return m;
+}
+
+struct VehicleCtx {
+    const crush_vehicle_spec* spec;
+    std::string name;
+    double y_center, z_bottom;
+};
+
+double frontal_area(const crush_vehicle_spec& v) { return v.size[1] * v.size[2]; }
+double contact_modulus(const crush_vehicle_spec& v) {
+    return v.contact_modulus > 0.0 ? v.contact_modulus : v.material.youngs_modulus;
+}
+// Vehicle::contact_stiffness_per_node, src/vehicle.rs:384 (no crush zone: h_front = h).
+double contact_stiffness_per_node(const crush_vehicle_spec& v, size_t n_face, double h) {
+    return contact_modulus(v) * frontal_area(v) / ((double)n_face * h);
+}
+bool in_rail_box(const crush_vehicle_spec& v, double y, double z) {
+    return v.has_rail_box && std::fabs(y) < 0.5 * v.rail_box_width && z > v.rail_box_z[0] && z < v.rail_box_z[1];
+}
+// Vehicle::rail_box_factors, src/vehicle.rs:367.
+void rail_box_factors(const crush_vehicle_spec& v, double area_fraction, double* f_rails, double* f_skin) {
+    double f = std::min(std::max(v.has_rail_box ? v.rail_box_force_fraction : 0.0, 0.0), 1.0);
+    double a = std::min(std::max(area_fraction, 1e-6), 1.0 - 1e-6);
+    *f_rails = f / a;
+    *f_skin = (1.0 - f) / (1.0 - a);
+}
+
+crush_material crush_material_of(const crush_vehicle_spec& v) {
+    crush_material m = v.material;
+    if (!(m.density > 0.0)) m.density = v.mass / (v.size[0] * v.size[1] * v.size[2]);
+    return m;
+}
+
+// add_vehicle, src/vehicle.rs:663 (uniform block); the rail box, when asked,
+// is carved out of the whole block (src/vehicle.rs:710-733 does it on the crush zone).
+void add_vehicle(crush_model* m, VehicleCtx& vc, double front_x, bool plus_x, double h) {
+    const crush_vehicle_spec& v = *vc.spec;
+    double x0 = plus_x ? front_x - v.size[0] : front_x;
+    int face = plus_x ? XMax : XMin;
+    double origin[3] = {x0, vc.y_center - v.size[1] / 2.0, vc.z_bottom};
+    add_hex_block(m, vc.name, origin, v.size, h, {{face, vc.name + "_front"}, {ZMin, vc.name + "_bottom"}});
+    if (v.has_rail_box) {
+        int from = part_index(m, vc.name);
+        size_t to = add_part(m, vc.name + "_rails");
+        for (size_t e = 0; e < m->hex_part.size(); ++e) {
+            if (m->hex_part[e] != from) continue;
+            double ys = 0.0, zs = 0.0;
+            for (int i = 0; i < 8; ++i) {
+                ys += m->positions[3 * m->hexes[8 * e + i] + 1];
+                zs += m->positions[3 * m->hexes[8 * e + i] + 2];
+            }
+            double yc = ys / 8.0 - vc.y_center, zc = zs / 8.0 - vc.z_bottom;
+            if (in_rail_box(v, yc, zc)) m->hex_part[e] = (int32_t)to;
+        }
+    }
+}
+
+void set_velocity(crush_model* m, const std::string& set, const double v[3]) {
+    for (uint32_t n : m->node_sets[set])
+        for (int d = 0; d < 3; ++d) m->velocity[3 * n + d] = v[d];
+}
+
+// assign_vehicle, src/vehicle.rs:750 (+ the rail-box split of :755-770).
+void assign_vehicle(crush_model* m, const VehicleCtx& vc, const double vel[3]) {
+    const crush_vehicle_spec& v = *vc.spec;
+    crush_material crush = crush_material_of(v);
+    int skin = part_index(m, vc.name);
+    int rails = v.has_rail_box ? part_index(m, vc.name + "_rails") : -1;
+    if (rails >= 0) {
+        size_t n_rails = 0, n_skin = 0;
+        for (int32_t p : m->hex_part) {
+            n_rails += p == rails;
+            n_skin += p == skin;
+        }
+        double fr = 1.0, fs = 1.0;
+        if (n_rails > 0 && n_skin > 0) rail_box_factors(v, (double)n_rails / (double)(n_rails + n_skin), &fr, &fs);
+        m->materials[rails] = scaled(crush, fr);
+        m->materials[skin] = scaled(crush, fs);
+    } else {
+        m->materials[skin] = crush;
+    }
+    set_velocity(m, vc.name, vel);
+}
+
+// Vehicle::front_contact_scales, src/vehicle.rs:397.
+std::vector<double> front_contact_scales(const crush_model* m, const VehicleCtx& vc, double h) {
+    const crush_vehicle_spec& v = *vc.spec;
+    std::vector<double> out;
+    if (!v.has_rail_box) return out;
+    std::vector<uint32_t> nodes;
+    if (!face_set_nodes(m, vc.name + "_front", &nodes)) return out;
+    size_t ny = (size_t)std::max(std::round(v.size[1] / h), 1.0);
+    size_t nz = (size_t)std::max(std::round(v.size[2] / h), 1.0);
+    double dy = v.size[1] / (double)ny, dz = v.size[2] / (double)nz;
+    double lo[3] = {1e308, 1e308, 1e308}, hi[3] = {-1e308, -1e308, -1e308};
+    for (uint32_t n : nodes)
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = std::min(lo[d], m->positions[3 * n + d]);
+            hi[d] = std::max(hi[d], m->positions[3 * n + d]);
+        }
+    double y_center = 0.5 * (lo[1] + hi[1]), z_bottom = lo[2];
+    size_t cells = ny * nz, n_rails = 0;
+    for (size_t c = 0; c < cells; ++c)
+        if (in_rail_box(v, (double)(c % ny) * dy + 0.5 * dy - 0.5 * v.size[1], (double)(c / ny) * dz + 0.5 * dz)) ++n_rails;
+    if (n_rails == 0 || n_rails == cells) return out;
+    double fr, fs;
+    rail_box_factors(v, (double)n_rails / (double)cells, &fr, &fs);
+    static const double S[4][2] = {{-0.5, -0.5}, {0.5, -0.5}, {-0.5, 0.5}, {0.5, 0.5}};
+    for (uint32_t n : nodes) {
+        const double* p = &m->positions[3 * n];
+        double sum = 0.0;
+        int count = 0;
+        for (const auto& s : S) {
+            double yc = p[1] - y_center + s[0] * dy, zc = p[2] - z_bottom + s[1] * dz;
+            if (std::fabs(yc) < 0.5 * v.size[1] && zc > 0.0 && zc < v.size[2]) {
+                sum += in_rail_box(v, yc, zc) ? fr : fs;
+                ++count;
+            }
+        }
+        out.push_back(count > 0 ? sum / (double)count : 1.0);
+    }
+    return out;
+}
+
+// add_ground, src/vehicle.rs:829 (a fixed elastic slab, face set `<name>_face`).
+void add_ground(crush_model* m, double z, const double x[2], const double y[2], double thickness) {
+    double h = std::max(std::min(x[1] - x[0], y[1] - y[0]) / 8.0, thickness);
+    double origin[3] = {x[0], y[0], z - thickness};
+    double size[3] = {x[1] - x[0], y[1] - y[0], thickness};
+    add_hex_block(m, "ground", origin, size, h, {{ZMax, "ground_face"}});
+}
+
+void add_contact_one_way(crush_model* m, const std::string& nodes_set, const std::string& faces_set, double k, double md,
+                         const std::vector<double>& scale) {
+    ContactDef c;
+    face_set_nodes(m, nodes_set, &c.nodes);
+    for (size_t f : *face_set(m, faces_set)) c.faces.insert(c.faces.end(), m->faces[f].begin(), m->faces[f].end());
+    c.stiffness = k;
+    c.max_distance = md;
+    c.scale = scale;
+    m->contacts.push_back(c);
+}
+
+// add_ground_contact, src/vehicle.rs:838. `n_face_override` (> 0) reproduces
+// the T-bone side profile, whose `<name>_front` set does not exist so the
+// reference falls back to the number of underbody nodes.
+void add_ground_contact(crush_model* m, const VehicleCtx& vc, double clearance, double h, bool side_profile) {
+    std::vector<uint32_t> bottom, front;
+    face_set_nodes(m, vc.name + "_bottom", &bottom);
+    size_t n_bottom = bottom.empty() ? 1 : bottom.size();
+    size_t n_face = (!side_profile && face_set_nodes(m, vc.name + "_front", &front)) ? front.size() : n_bottom;
+    int g = part_index(m, "ground");
+    m->materials[g] = elastic_material(1e9, 0.3, 1000.0);
+    for (uint32_t n : m->node_sets["ground"]) m->fixed.push_back(n);
+    add_contact_one_way(m, vc.name + "_bottom", "ground_face", contact_stiffness_per_node(*vc.spec, n_face, h), clearance + 0.3, {});
+}
+
+// Model::add_contact_pair_scaled, src/model.rs:257.
+void add_contact_pair_scaled(crush_model* m, const std::string& a, const std::string& b, double k, double md,
+                             const std::vector<double>& sa, const std::vector<double>& sb) {
+    add_contact_one_way(m, a, b, 0.5 * k, md, sa);
+    add_contact_one_way(m, b, a, 0.5 * k, md, sb);
+}
+
+// add_vehicle_accelerometer, src/vehicle.rs:792-822 -> Mesh::nearest_node (first minimum).
+uint32_t accelerometer_node(const crush_model* m, const std::string& part, const std::string& front_face) {
+    int p = part_index(m, part);
+    std::vector<uint32_t> nodes = part_nodes(m, p);
+    double lo[3] = {1.7976931348623157e308, 1.7976931348623157e308, 1.7976931348623157e308};
+    double hi[3] = {-1.7976931348623157e308, -1.7976931348623157e308, -1.7976931348623157e308};
+    for (uint32_t n : nodes)
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = std::min(lo[d], m->positions[3 * n + d]);
+            hi[d] = std::max(hi[d], m->positions[3 * n + d]);
+        }
+    std::vector<uint32_t> front;
+    face_set_nodes(m, front_face, &front);
+    double c[3] = {0, 0, 0};
+    for (uint32_t n : front)
+        for (int d = 0; d < 3; ++d) c[d] += m->positions[3 * n + d] / (double)front.size();
+    double at[3] = {0.5 * (lo[0] + hi[0]), 0.5 * (lo[1] + hi[1]), lo[2] + 0.35 * (hi[2] - lo[2])};
+    for (int d = 0; d < 2; ++d) {
+        double len = hi[d] - lo[d];
+        if (c[d] <= lo[d] + 1e-6 * len) at[d] = hi[d] - 0.25 * len;
+        else if (c[d] >= hi[d] - 1e-6 * len) at[d] = lo[d] + 0.25 * len;
+    }
+    uint32_t best = nodes.empty() ? 0 : nodes[0];
+    double best_d = 1e308;
+    bool first = true;
+    for (uint32_t n : nodes) {
+        double d2 = 0.0;
+        for (int d = 0; d < 3; ++d) d2 += (m->positions[3 * n + d] - at[d]) * (m->positions[3 * n + d] - at[d]);
+        if (first || d2 < best_d) { best = n; best_d = d2; first = false; }
+    }
+    return best;
+}
+
+void add_vehicle_output(crush_model* m, const std::string& name, const std::string& front_face) {
+    VehicleDef v;
+    v.nodes = m->node_sets[name];
+    v.accel = accelerometer_node(m, name, front_face);
+    face_set_nodes(m, front_face, &v.front);
+    m->vehicles.push_back(v);
+}
+
+int check_spec(const crush_vehicle_spec& v) {
+    if (!(v.mass > 0.0) || !(v.size[0] > 0.0) || !(v.size[1] > 0.0) || !(v.size[2] > 0.0))
+        return crush::fail(CRUSH_ERR_INVALID, "a vehicle needs a positive mass and size");
+    if (v.material.model != CRUSH_MAT_HONEYCOMB) return crush::fail(CRUSH_ERR_UNSUPPORTED, "vehicle crush material must be honeycomb");
+    if (!(v.material.youngs_modulus > 0.0)) return crush::fail(CRUSH_ERR_INVALID, "vehicle modulus must be positive");
+    return CRUSH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+crush_settings crush_settings_default(double end_time) {
+    crush_settings s;
+    std::memset(&s, 0, sizeof(s));
+    s.end_time = end_time;
+    s.dt_scale = 0.85;
+    s.time_step = 0.0;
+    s.adaptive_check_steps = 5;
+    s.hourglass = 0.1;
+    s.velocity_damping = 1.0;
+    s.mass_scaling = 0.25;
+    s.stop_rule = CRUSH_STOP_END_TIME;
+    s.max_steps = 0;
+    return s;
+}
+
+int crush_scenario_build(const crush_scenario* s, crush_model** out) {
+    if (!s || !out) return crush::fail(CRUSH_ERR_INVALID, "null scenario");
+    *out = nullptr;
+    int st = check_spec(s->a);
+    if (st == CRUSH_OK) st = check_spec(s->b);
+    if (st != CRUSH_OK) return st;
+    if (!(s->element_size > 0.0)) return crush::fail(CRUSH_ERR_INVALID, "element size must be positive");
+    crush_model* m = new crush_model();
+    const double h = s->element_size, gap = 0.005;
+    VehicleCtx a{&s->a, "a", 0.0, 0.0};
+    VehicleCtx b{&s->b, "b", s->layout == CRUSH_LAYOUT_TBONE ? -s->offset : s->offset, 0.0};
+    bool road = s->clearance >= 0.0;
+    if (s->layout == CRUSH_LAYOUT_HEADON) {
+        // HeadOn::build, src/headon.rs:40-66
+        add_vehicle(m, a, -gap, true, h);
+        add_vehicle(m, b, gap, false, h);
+        if (road) {
+            double w = std::max(s->a.size[1], s->b.size[1]) + 2.0 * std::fabs(s->offset);
+            double xr[2] = {-s->a.size[0] - 3.0, s->b.size[0] + 3.0}, yr[2] = {-w, w};
+            add_ground(m, -s->clearance, xr, yr, 0.3);
+        }
+        double va[3] = {s->speed_a, 0.0, 0.0}, vb[3] = {-s->speed_b, 0.0, 0.0};
+        assign_vehicle(m, a, va);
+        assign_vehicle(m, b, vb);
+        if (road) {
+            add_ground_contact(m, a, s->clearance, h, false);
+            add_ground_contact(m, b, s->clearance, h, false);
+        }
+        std::vector<uint32_t> fa, fb;
+        face_set_nodes(m, "a_front", &fa);
+        face_set_nodes(m, "b_front", &fb);
+        size_t n_face = std::min(fa.size(), fb.size());
+        double k = std::min(contact_stiffness_per_node(s->a, n_face, h), contact_stiffness_per_node(s->b, n_face, h));
+        add_contact_pair_scaled(m, "a_front", "b_front", k, 0.3, front_contact_scales(m, a, h), front_contact_scales(m, b, h));
+    } else if (s->layout == CRUSH_LAYOUT_TBONE) {
+        // src/bin/crushrs.rs:550-576: A's front into the x-min side of B.
+        add_vehicle(m, a, -gap, true, h);
+        double origin[3] = {gap, -s->offset - s->b.size[1] / 2.0, 0.0};
+        add_hex_block(m, "b", origin, s->b.size, h, {{XMin, "b_front"}, {ZMin, "b_bottom"}});
+        if (road) {
+            double w = s->b.size[1] + s->a.size[1];
+            double xr[2] = {-s->a.size[0] - 3.0, s->b.size[0] + 3.0}, yr[2] = {-w, w};
+            add_ground(m, -s->clearance, xr, yr, 0.3);
+        }
+        double va[3] = {s->speed_a, 0.0, 0.0}, vb[3] = {0.0, s->speed_b, 0.0};
+        assign_vehicle(m, a, va);
+        m->materials[part_index(m, "b")] = crush_material_of(s->b);
+        set_velocity(m, "b", vb);
+        if (road) {
+            add_ground_contact(m, a, s->clearance, h, false);
+            add_ground_contact(m, b, s->clearance, h, true);
+        }
+        std::vector<uint32_t> fb;
+        face_set_nodes(m, "b_front", &fb);
+        double k = std::min(contact_stiffness_per_node(s->b, fb.size(), h), contact_stiffness_per_node(s->a, fb.size(), h));
+        add_contact_pair_scaled(m, "a_front", "b_front", k, 0.3, {}, {});
+    } else {
+        delete m;
+        return crush::fail(CRUSH_ERR_INVALID, "unknown layout");
+    }
+    m->settings = s->settings;
+    add_vehicle_output(m, "a", "a_front");
+    add_vehicle_output(m, "b", "b_front");
+    *out = m;
+    return CRUSH_OK;
+}
+
+void crush_model_free(crush_model* m) { delete m; }
+
+crush_settings* crush_model_settings(crush_model* m) { return m ? &m->settings : nullptr; }
+
+int crush_model_desc_get(const crush_model* mc, crush_model_desc* d) {
+    if (!mc || !d) return crush::fail(CRUSH_ERR_INVALID, "null model");
+    crush_model* m = const_cast<crush_model*>(mc);
+    m->contact_desc.clear();
+    for (const ContactDef& c : m->contacts) {
+        crush_contact k;
+        k.n_nodes = (int64_t)c.nodes.size();
+        k.nodes = c.nodes.data();
+        k.node_scale = c.scale.empty() ? nullptr : c.scale.data();
+        k.n_faces = (int64_t)c.faces.size() / 4;
+        k.faces = c.faces.data();
+        k.stiffness = c.stiffness;
+        k.max_distance = c.max_distance;
+        m->contact_desc.push_back(k);
+    }
+    m->vehicle_desc.clear();
+    for (const VehicleDef& v : m->vehicles) {
+        crush_vehicle w;
+        w.n_nodes = (int64_t)v.nodes.size();
+        w.nodes = v.nodes.data();
+        w.accel_node = v.accel;
+        w.n_front = (int64_t)v.front.size();
+        w.front_nodes = v.front.data();
+        m->vehicle_desc.push_back(w);
+    }
+    std::memset(d, 0, sizeof(*d));
+    d->n_nodes = (int64_t)m->positions.size() / 3;
+    d->positions = m->positions.data();
+    d->n_hexes = (int64_t)m->hex_part.size();
+    d->hexes = m->hexes.data();
+    d->hex_part = m->hex_part.data();
+    d->n_parts = (int32_t)m->materials.size();
+    d->materials = m->materials.data();
+    d->initial_velocity = m->velocity.data();
+    d->n_fixed = (int64_t)m->fixed.size();
+    d->fixed_nodes = m->fixed.data();
+    d->n_contacts = (int32_t)m->contact_desc.size();
+    d->contacts = m->contact_desc.data();
+    d->n_vehicles = (int32_t)m->vehicle_desc.size();
+    d->vehicles = m->vehicle_desc.data();
+    d->settings = m->settings;
+    return CRUSH_OK;
+}
+
+int crush_model_new(crush_model** out) {
+    if (!out) return crush::fail(CRUSH_ERR_INVALID, "null output");
+    *out = new crush_model();
+    (*out)->settings = crush_settings_default(0.15);
+    return CRUSH_OK;
+}
+
+int crush_model_add_block(crush_model* m, const double origin[3], const double size[3], const int32_t n[3], int32_t surfaces,
+                          int32_t* part_out) {
+    if (!m) return crush::fail(CRUSH_ERR_INVALID, "null model");
+    std::vector<std::pair<int, std::string>> sf;
+    static const int ORDER[6] = {XMin, XMax, YMin, YMax, ZMin, ZMax};
+    std::string name = "part" + std::to_string(m->part_names.size());
+    for (int f : ORDER)
+        if (surfaces & f) sf.push_back({f, name + "_face" + std::to_string(f)});
+    size_t p = add_hex_block_n(m, name, origin, size, n, sf);
+    if (part_out) *part_out = (int32_t)p;
+    return CRUSH_OK;
+}
+
+int crush_model_face_set(const crush_model* m, int32_t k, int64_t* n_faces, uint32_t* faces) {
+    if (!m || k < 0 || k >= (int32_t)m->face_set_list.size()) return crush::fail(CRUSH_ERR_INVALID, "face set out of range");
+    const std::vector<size_t>& set = m->face_set_list[k];
+    *n_faces = (int64_t)set.size();
+    if (faces)
+        for (size_t i = 0; i < set.size(); ++i)
+            for (int j = 0; j < 4; ++j) faces[4 * i + j] = m->faces[set[i]][j];
+    return CRUSH_OK;
+}
+
+int crush_model_set_materials(crush_model* m, int32_t n, const crush_material* mats) {
+    if (!m || n != (int32_t)m->materials.size()) return crush::fail(CRUSH_ERR_INVALID, "material count must match parts");
+    std::copy(mats, mats + n, m->materials.begin());
+    return CRUSH_OK;
+}
+
+int crush_model_set_velocity(crush_model* m, const double* v) {
+    if (!m || !v) return crush::fail(CRUSH_ERR_INVALID, "null velocity");
+    std::copy(v, v + m->velocity.size(), m->velocity.begin());
+    return CRUSH_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,240 @@
+/*
+ * crush.h — C ABI of the B200 explicit time-step engine for crushrs-style
+ * crash models (one-point honeycomb hexahedra, node-to-face penalty contact,
+ * central-difference integration with selective mass scaling).
+ *
+ * The entry points replace the Rust-internal calls the reference solver makes
+ * on its hot path (paths are relative to the crushrs source tree):
+ *
+ *   crush_compute_forces   <- Elements::compute_forces      src/kernel.rs:160
+ *                             (Blocks::compute_forces + scatter,
+ *                              src/kernel_simd.rs:558, :573)
+ *   crush_contact_apply    <- ContactRuntime::apply         src/contact.rs:92
+ *   crush_stable_dt        <- Elements::stable_time_step    src/kernel.rs:207
+ *   crush_mass_scaling     <- Elements::mass_scaling        src/kernel.rs:243
+ *   crush_create           <- Elements::build               src/kernel.rs:53
+ *                             + Model::lumped_masses        src/model.rs:268
+ *                             + ContactRuntime::new         src/contact.rs:48
+ *   crush_run              <- crushrs::run                  src/solver.rs:190
+ *   crush_vehicle_result   <- part_delta_v / crush_rear     src/bin/crushrs.rs:237, :265
+ *
+ * Conventions
+ *   - Every function returns an int status: CRUSH_OK (0) or a negative
+ *     CRUSH_ERR_* code; crush_stable_dt may also return CRUSH_NONE (1) for the
+ *     reference's `None`. Nothing aborts the process; crush_last_error()
+ *     gives a message for the calling thread's last failure.
+ *   - Buffers passed in are caller-owned host memory unless the name says
+ *     `_device`, in which case they are device pointers on the context's GPU.
+ *     "accum" outputs are ADDED into, like the reference's `global: &mut [f64]`
+ *     (callers zero them first, as solver.rs:307,327 does).
+ *   - Vectors of nodal quantities are flat f64 arrays of length 3*n_nodes
+ *     (x,y,z interleaved), exactly the reference's `u`, `v`, `f_int`, `f_ext`.
+ *   - One context per thread, or an external mutex. Work is ordered on the
+ *     context's CUDA stream; host-buffer entry points synchronise before
+ *     returning.
+ */
+#ifndef CRUSH_H
+#define CRUSH_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CRUSH_OK 0
+#define CRUSH_NONE 1
+#define CRUSH_ERR_INVALID (-1)
+#define CRUSH_ERR_NONFINITE (-2)
+#define CRUSH_ERR_OOM (-3)
+#define CRUSH_ERR_TIMEOUT (-4)
+#define CRUSH_ERR_CUDA (-5)
+#define CRUSH_ERR_UNSUPPORTED (-6)
+#define CRUSH_ERR_BUSY (-7)
+
+/* Material models (src/material.rs:20). Honeycomb runs on the device kernels.
+ * Elastic parts are accepted only when every node of every element of the
+ * part is fixed (a rigid road or wall slab): their deformation gradient stays
+ * the identity, so they carry no force and contribute only a constant
+ * element stability limit. */
+#define CRUSH_MAT_HONEYCOMB 0
+#define CRUSH_MAT_ELASTIC 1
+
+#define CRUSH_MAX_KNOTS 8
+
+/* One part's material, mirroring Material + Plasticity (src/material.rs:42,155). */
+typedef struct crush_material {
+    int32_t model;             /* CRUSH_MAT_* */
+    double youngs_modulus;     /* Pa */
+    double poisson_ratio;      /* honeycomb: 0 */
+    double density;            /* kg/m^3 */
+    double yield_stress;       /* Pa, bilinear curve when n_curve == 0 */
+    double hardening;          /* Pa per unit compaction */
+    int32_t n_curve;           /* 0, or 2..8 tabulated knots (one fewer with densification) */
+    double curve[CRUSH_MAX_KNOTS][2]; /* [compaction, yield stress] ascending from c = 0 */
+    int32_t has_densification; /* 1: lock-up knot [c_lock, k_lock] appended */
+    double densification[2];
+    double transverse_factor;  /* cap factor of local y, z normal stresses (1 = isotropic) */
+} crush_material;
+
+/* One-way node-to-face penalty contact (src/model.rs:13). A two-way pair is
+ * two of these at half stiffness each (src/model.rs:257). */
+typedef struct crush_contact {
+    int64_t n_nodes;
+    const uint32_t* nodes;     /* primary (slave) nodes, sorted unique */
+    const double* node_scale;  /* per-node stiffness factor aligned with nodes, or NULL (= 1) */
+    int64_t n_faces;
+    const uint32_t* faces;     /* 4 node ids per quad, counter-clockwise about the outward normal */
+    double stiffness;          /* N/m per node */
+    double max_distance;       /* m */
+} crush_contact;
+
+/* Stop rules for crush_run. */
+#define CRUSH_STOP_END_TIME 0
+/* Run until the two vehicles separate: every 10 steps after the first contact
+ * hit, stop when vehicle[1]'s mass-weighted mean x-velocity minus vehicle[0]'s
+ * is >= 0 and no contact node has penetrated for the last 100 steps. The
+ * settings' max_steps caps the run. Not in the reference (which only runs to
+ * end_time); defined identically in the oracle. */
+#define CRUSH_STOP_SEPARATION 1
+
+/* Solver settings (src/model.rs:76-150). */
+typedef struct crush_settings {
+    double end_time;           /* s */
+    double dt_scale;           /* safety factor on the stable step (0.85) */
+    double time_step;          /* fixed step if > 0, else adaptive */
+    int32_t adaptive_check_steps; /* re-evaluate the stable step every N steps (5) */
+    double hourglass;          /* stabilisation stiffness as a fraction of E (0.1) */
+    double velocity_damping;   /* per-step velocity factor (1.0) */
+    double mass_scaling;       /* dt floor as a fraction of the initial stable step (0.25) */
+    int32_t stop_rule;         /* CRUSH_STOP_* */
+    int32_t max_steps;         /* 0 = unlimited */
+} crush_settings;
+
+/* Outputs wanted per vehicle: delta-v over `nodes` (src/bin/crushrs.rs:237)
+ * and crush = |u_x(accel_node) - mean u_x(front_nodes)| (src/bin/crushrs.rs:265). */
+typedef struct crush_vehicle {
+    int64_t n_nodes;
+    const uint32_t* nodes;
+    uint32_t accel_node;
+    int64_t n_front;
+    const uint32_t* front_nodes;
+} crush_vehicle;
+
+/* Whole model (src/model.rs:153), as flat arrays. */
+typedef struct crush_model_desc {
+    int64_t n_nodes;
+    const double* positions;        /* 3*n_nodes reference coordinates */
+    int64_t n_hexes;
+    const uint32_t* hexes;          /* 8 node ids per hexahedron, C3D8 order */
+    const int32_t* hex_part;        /* part index per hexahedron */
+    int32_t n_parts;
+    const crush_material* materials;/* one per part */
+    const double* initial_velocity; /* 3*n_nodes */
+    int64_t n_fixed;
+    const uint32_t* fixed_nodes;
+    int32_t n_contacts;
+    const crush_contact* contacts;
+    int32_t n_vehicles;
+    const crush_vehicle* vehicles;
+    crush_settings settings;
+} crush_model_desc;
+
+/* Per-vehicle result of a run. */
+typedef struct crush_vehicle_result {
+    double mass;          /* kg, lumped masses without added mass */
+    double delta_v[3];    /* m/s, FP64 mass-weighted mean velocity change */
+    double velocity[3];   /* m/s, final mass-weighted mean velocity */
+    double crush;         /* m */
+} crush_vehicle_result;
+
+typedef struct crush_results {
+    double time;          /* simulated time reached (s) */
+    int64_t steps;
+    int64_t eroded_elements;
+    double dt_min;        /* smallest step taken */
+    double added_mass_max;/* kg, largest total added by mass scaling */
+    int32_t status;       /* CRUSH_OK or CRUSH_ERR_NONFINITE */
+    int32_t n_vehicles;
+    crush_vehicle_result vehicle[4];
+} crush_results;
+
+typedef struct crush_ctx crush_ctx;
+
+/* Last error message of the calling thread ("" if none). */
+const char* crush_last_error(void);
+
+/* Library and device information: fills name (>= 64 bytes), returns SM count
+ * or a negative status. */
+int crush_device_info(int device, char* name, int name_len);
+
+/* ---- single-model context: drop-in for the reference's hot-path calls ---- */
+
+/* Upload a model to `device`, run the device geometry precompute
+ * (HexGeometry::new, src/element.rs:141), build the node incidence used by the
+ * deterministic force gather, lumped masses, contact runtimes and the initial
+ * stable step. The desc's arrays may be freed after return. */
+int crush_create(const crush_model_desc* desc, int device, crush_ctx** out);
+void crush_destroy(crush_ctx* ctx);
+
+/* Sizes of the uploaded model. */
+int crush_sizes(const crush_ctx* ctx, int64_t* n_nodes, int64_t* n_hexes, int64_t* n_active_hexes);
+
+/* Element forces at displacement u (host, 3N), committing material states;
+ * the nodal sum is ADDED into f_int_accum (host, 3N). `newly_eroded` gets the
+ * number of elements that inverted in this call (may be NULL).
+ * Replaces Elements::compute_forces (src/kernel.rs:160). */
+int crush_compute_forces(crush_ctx* ctx, const double* u, double* f_int_accum, int64_t* newly_eroded);
+/* The same with device buffers (3N f64 each); f_int_device is overwritten. */
+int crush_compute_forces_device(crush_ctx* ctx, const double* u_device, double* f_int_device, int64_t* newly_eroded);
+
+/* Penalty forces of contact `contact_id` for the configuration X + u, ADDED
+ * into f_ext_accum (host, 3N). `masses` are the lumped nodal masses (N) the
+ * soft-constraint limit uses; NULL = the context's own. `v` feeds the
+ * reference's damping term, whose ratio is the constant 0, so it may be NULL.
+ * Replaces ContactRuntime::apply (src/contact.rs:92). */
+int crush_contact_apply(crush_ctx* ctx, int contact_id, const double* u, const double* v,
+                        const double* masses, double dt, double* f_ext_accum,
+                        int64_t* penetration_count, double* max_penetration);
+
+/* Smallest element stability limit f(nu) L / c_d at X + u (host, 3N).
+ * Returns CRUSH_NONE (and *dt = +inf) when no element gives a finite limit.
+ * Replaces Elements::stable_time_step (src/kernel.rs:207). */
+int crush_stable_dt(crush_ctx* ctx, const double* u, double* dt);
+
+/* Selective mass scaling: nodal mass `added` (host, N; overwritten) so that no
+ * element's limit falls below dt_min; returns the total in *total.
+ * element_mass (host, n_hexes) may be NULL for the context's rho*V.
+ * Replaces Elements::mass_scaling (src/kernel.rs:243). */
+int crush_mass_scaling(crush_ctx* ctx, const double* u, double dt_min, const double* element_mass,
+                       double* added, double* total);
+
+/* Lumped nodal masses (N) and element masses rho*V (n_hexes), host outputs. */
+int crush_masses(crush_ctx* ctx, double* lumped, double* element_mass);
+
+/* Per-element f32 data the device derived in set-up, for parity checks:
+ * grad (24/hex), volume (1), gamma (32), h (144, column-major as in
+ * src/kernel_simd.rs:189), all f32; any pointer may be NULL. */
+int crush_element_data(crush_ctx* ctx, float* grad, float* volume, float* gamma, float* h);
+/* Material state per element: 25 f32 (F_prev^-1 9, R 9, stress 6, compaction)
+ * and eroded flags; set_ writes them back (both host arrays, n_hexes long). */
+int crush_get_state(crush_ctx* ctx, float* state, uint8_t* eroded);
+int crush_set_state(crush_ctx* ctx, const float* state, const uint8_t* eroded);
+
+/* ---- device-resident run (solver::run, src/solver.rs:190) ---- */
+int crush_run(crush_ctx* ctx, crush_results* results);
+/* Begin a run (set-up of solver.rs:197-286) without stepping. */
+int crush_run_begin(crush_ctx* ctx);
+/* Advance an open run by n_steps (fewer if it stops); *done = 1 when finished. */
+int crush_run_steps(crush_ctx* ctx, int64_t n_steps, int* done);
+/* Results of the open run so far (final after *done). */
+int crush_run_results(crush_ctx* ctx, crush_results* results);
+/* Nodal displacement and velocity (host, 3N each; either may be NULL). */
+int crush_run_state(crush_ctx* ctx, double* u, double* v);
+/* Kernel launches issued by this context since creation. */
+int64_t crush_launch_count(const crush_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,187 @@
+"""ctypes bindings of the oracle (oracle/liboracle.so): the CPU restatement of
+the reference used as the checker. Only tests, smoke() and bench.py's CPU
+baseline load it."""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from crushrs_b200 import abi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_SO = os.path.join(ORACLE_DIR, "liboracle.so")
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(ORACLE_SO):
+        subprocess.run(["make", "-s", "-C", ORACLE_DIR, "CXX=g++"], check=True)
+    lib = C.CDLL(ORACLE_SO)
+    P = C.POINTER
+    dp = P(C.c_double)
+    fp = P(C.c_float)
+    vp = C.c_void_p
+    lib.oracle_last_error.restype = C.c_char_p
+    lib.oracle_hardware_threads.restype = C.c_int
+    lib.oracle_geometry.argtypes = [dp, C.c_double, C.c_double, C.c_double, C.c_double, dp, dp, dp, dp, dp]
+    lib.oracle_char_length.argtypes = [dp, dp, dp]
+    lib.oracle_honeycomb_update.argtypes = [P(abi.Material), dp, dp, dp, dp]
+    lib.oracle_honeycomb_params.argtypes = [P(abi.Material), dp]
+    lib.oracle_yield_at.argtypes = [P(abi.Material), C.c_double, dp, dp, dp, dp]
+    lib.oracle_session_new.restype = vp
+    lib.oracle_session_new.argtypes = [P(abi.ModelDesc), C.c_int, C.c_int]
+    lib.oracle_session_free.argtypes = [vp]
+    lib.oracle_session_forces.argtypes = [vp, dp, dp, P(C.c_int64)]
+    lib.oracle_session_stable_dt.argtypes = [vp, dp, dp]
+    lib.oracle_session_element_dts.argtypes = [vp, dp, dp]
+    lib.oracle_session_mass_scaling.argtypes = [vp, dp, C.c_double, dp, dp, dp]
+    lib.oracle_session_masses.argtypes = [vp, dp, dp]
+    lib.oracle_session_geometry.argtypes = [vp, dp, dp, dp, dp]
+    lib.oracle_session_set_lane_geometry.argtypes = [vp, fp, fp, fp, fp]
+    lib.oracle_session_get_state.argtypes = [vp, fp, P(C.c_uint8)]
+    lib.oracle_session_set_state.argtypes = [vp, fp, P(C.c_uint8)]
+    lib.oracle_session_contact_apply.argtypes = [vp, C.c_int, dp, dp, dp, C.c_double, dp, P(C.c_int64), dp]
+    lib.oracle_session_contact_nodes.argtypes = [vp, C.c_int, P(C.c_uint32), P(C.c_int64)]
+    lib.oracle_run.argtypes = [P(abi.ModelDesc), C.c_int, C.c_int, P(abi.Results), dp, dp, dp, C.c_int64, dp]
+    _lib = lib
+    return lib
+
+
+def ptr(a, ctype=C.c_double):
+    return None if a is None else a.ctypes.data_as(C.POINTER(ctype))
+
+
+def error():
+    return load().oracle_last_error().decode()
+
+
+def geometry(x, youngs, poisson, density, hourglass=0.1):
+    lib = load()
+    x = np.ascontiguousarray(x, np.float64).reshape(24)
+    grad, vol, lumped, gamma, h = np.zeros(24), np.zeros(1), np.zeros(8), np.zeros(32), np.zeros(144)
+    st = lib.oracle_geometry(ptr(x), youngs, poisson, density, hourglass, ptr(grad), ptr(vol), ptr(lumped), ptr(gamma), ptr(h))
+    assert st == 0, error()
+    return dict(grad=grad.reshape(8, 3), volume=vol[0], lumped=lumped, gamma=gamma.reshape(8, 4), h=h.reshape(12, 12))
+
+
+def char_length(p):
+    lib = load()
+    p = np.ascontiguousarray(p, np.float64).reshape(24)
+    l, v = C.c_double(), C.c_double()
+    lib.oracle_char_length(ptr(p), C.byref(l), C.byref(v))
+    return l.value, v.value
+
+
+def default_state():
+    s = np.zeros(25)
+    s[[0, 4, 8]] = 1.0
+    s[[9, 13, 17]] = 1.0
+    return s
+
+
+def honeycomb_update(mat, f, state):
+    lib = load()
+    f = np.ascontiguousarray(f, np.float64).reshape(9)
+    state = np.ascontiguousarray(state, np.float64)
+    tau, out = np.zeros(9), np.zeros(25)
+    st = lib.oracle_honeycomb_update(C.byref(mat), ptr(f), ptr(state), ptr(tau), ptr(out))
+    assert st == 0, error()
+    return tau.reshape(3, 3), out
+
+
+def yield_at(mat, c):
+    lib = load()
+    a, b, c2, d = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+    st = lib.oracle_yield_at(C.byref(mat), c, C.byref(a), C.byref(b), C.byref(c2), C.byref(d))
+    assert st == 0, error()
+    return (a.value, b.value), (c2.value, d.value)
+
+
+class Session:
+    """Elements + contact runtimes of one model (the drop-in calls)."""
+
+    def __init__(self, desc, simd=True, threads=1):
+        self.lib = load()
+        self.desc = desc
+        self.h = self.lib.oracle_session_new(C.byref(desc), int(simd), threads)
+        assert self.h, error()
+        self.n_nodes = desc.n_nodes
+        self.n_hexes = desc.n_hexes
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.oracle_session_free(self.h)
+            self.h = None
+
+    def forces(self, u, out=None):
+        u = np.ascontiguousarray(u, np.float64).reshape(-1)
+        f = np.zeros(3 * self.n_nodes) if out is None else out
+        n = C.c_int64()
+        self.lib.oracle_session_forces(self.h, ptr(u), ptr(f), C.byref(n))
+        return f, n.value
+
+    def stable_dt(self, u):
+        dt = C.c_double()
+        st = self.lib.oracle_session_stable_dt(self.h, ptr(np.ascontiguousarray(u, np.float64)), C.byref(dt))
+        return (dt.value if st == 0 else None)
+
+    def element_dts(self, u):
+        out = np.zeros(self.n_hexes)
+        self.lib.oracle_session_element_dts(self.h, ptr(np.ascontiguousarray(u, np.float64)), ptr(out))
+        return out
+
+    def mass_scaling(self, u, dt_min, element_mass=None):
+        added = np.zeros(self.n_nodes)
+        total = C.c_double()
+        self.lib.oracle_session_mass_scaling(self.h, ptr(np.ascontiguousarray(u, np.float64)), dt_min, ptr(element_mass), ptr(added), C.byref(total))
+        return added, total.value
+
+    def masses(self):
+        lumped, em = np.zeros(self.n_nodes), np.zeros(self.n_hexes)
+        self.lib.oracle_session_masses(self.h, ptr(lumped), ptr(em))
+        return lumped, em
+
+    def geometry(self):
+        g, v, gm, hh = np.zeros((self.n_hexes, 24)), np.zeros(self.n_hexes), np.zeros((self.n_hexes, 32)), np.zeros((self.n_hexes, 144))
+        self.lib.oracle_session_geometry(self.h, ptr(g), ptr(v), ptr(gm), ptr(hh))
+        return g, v, gm, hh
+
+    def set_lane_geometry(self, grad, volume, gamma, h):
+        arrs = [np.ascontiguousarray(a, np.float32) for a in (grad, volume, gamma, h)]
+        self.lib.oracle_session_set_lane_geometry(self.h, *[ptr(a, C.c_float) for a in arrs])
+
+    def get_state(self):
+        s, e = np.zeros((self.n_hexes, 25), np.float32), np.zeros(self.n_hexes, np.uint8)
+        self.lib.oracle_session_get_state(self.h, ptr(s, C.c_float), ptr(e, C.c_uint8))
+        return s, e
+
+    def set_state(self, s, e):
+        s = np.ascontiguousarray(s, np.float32)
+        e = np.ascontiguousarray(e, np.uint8)
+        self.lib.oracle_session_set_state(self.h, ptr(s, C.c_float), ptr(e, C.c_uint8))
+
+    def contact_apply(self, c, u, v, masses, dt, force=None):
+        f = np.zeros(3 * self.n_nodes) if force is None else force
+        cnt, mp = C.c_int64(), C.c_double()
+        st = self.lib.oracle_session_contact_apply(self.h, c, ptr(np.ascontiguousarray(u, np.float64)), ptr(v), ptr(masses), dt, ptr(f), C.byref(cnt), C.byref(mp))
+        assert st == 0, error()
+        return f, cnt.value, mp.value
+
+
+def run(desc, simd=True, threads=1, want_state=False, want_dt=0):
+    lib = load()
+    r = abi.Results()
+    n = desc.n_nodes
+    u = np.zeros(3 * n) if want_state else None
+    v = np.zeros(3 * n) if want_state else None
+    dt = np.zeros(want_dt) if want_dt else None
+    sec = np.zeros(3)
+    st = lib.oracle_run(C.byref(desc), int(simd), threads, C.byref(r), ptr(u), ptr(v), ptr(dt), want_dt, ptr(sec))
+    assert st in (0, abi.CRUSH_ERR_NONFINITE), error()
+    return r, u, v, dt, sec
