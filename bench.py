@@ -1,0 +1,314 @@
+#!/usr/bin/env python
+"""Headline benchmark: explicit time steps of the refined head-on crash
+(278,640 one-point honeycomb hexahedra, 299,108 nodes) on the B200 engine.
+
+One step = the whole explicit time step of the model: stable-dt check and
+mass scaling (every 5 steps), node-to-face contact over the device grid, the
+half step, the element forces, the ordered force gather with the full step.
+
+Printed JSON line (rank 0):
+  value      element-updates/s of the whole job, device-timed (CUDA events on
+             the engine's stream), inputs resident in HBM; per-step working
+             set (~0.33 GB) is larger than L2, so no flush is needed.
+  e2e        the same metric through the reference-facing C-ABI drop-in calls
+             with host buffers (crush_contact_apply + crush_compute_forces
+             per step, the central-difference update on the host): every
+             step copies u host->device and the forces device->host.
+  e2e_run    elem-upd/s of a whole crash through crush_create + crush_run
+             (host model in, delta-v out), host-clock timed.
+  roofline   HBM roofline of the element-force kernel: algorithmic bytes per
+             launch (870 B per element + 24 B per node) over its average
+             device time inside the timed region.
+  cpu_baseline  the oracle's f32 8-lane restatement of the reference step on
+             all host threads, a bounded number of steps of the same mesh.
+--impl reference runs that CPU restatement as the reference arm.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_ELEM_KERNEL = 870  # per element: conn 32, grad 96, volume 4, gamma 128, H 312, state r+w 200, eroded r+w 2, corner forces 96
+BYTES_NODE_KERNEL = 24   # per node: positions + displacements read by the element kernel
+BYTES_STEP_ELEM = 998    # whole step, per element
+BYTES_STEP_NODE = 92     # whole step, per node
+METRIC = "crashes/sec + p50/p99 latency vs plain GPU path at <=0.5% delta-v err; elem-upd/s"
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def read_traffic(n_elem):
+    """dram bytes per element-kernel launch from the committed ncu summary,
+    scaled from the captured case by elements."""
+    path = os.path.join(ROOT, "profiles", "k_forces_refined_headon.txt")
+    try:
+        vals = {}
+        with open(path) as f:
+            for line in f:
+                if ":" in line:
+                    k, v = line.split(":", 1)
+                    vals[k.strip()] = v.strip()
+        per_elem = float(vals["dram_bytes_per_element"])
+        return per_elem * n_elem
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def all_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def cpu_reference(desc, steps, threads):
+    """The oracle's restatement of the reference step loop, bounded to `steps`."""
+    from tests import oracle_lib as O
+
+    s = desc.settings
+    saved = (s.max_steps, s.stop_rule)
+    desc.settings.max_steps = steps
+    desc.settings.stop_rule = 0
+    try:
+        r, _, _, _, sec = O.run(desc, simd=True, threads=threads)
+    finally:
+        desc.settings.max_steps, desc.settings.stop_rule = saved
+    loop = sec[3]
+    return r.steps, loop, sec
+
+
+def e2e_dropin(ctx, desc, steps, n_hc):
+    """Reference-facing drop-in loop (src/solver.rs:287-342 as the caller):
+    host f64 state, GPU contact + element forces through the C ABI each step."""
+    import torch
+
+    n = desc.n_nodes
+    pin = lambda: torch.zeros(3 * n, dtype=torch.float64).pin_memory().numpy()
+    u, v, vh, f_int, f_ext = pin(), pin(), pin(), pin(), pin()
+    v[:] = np.ctypeslib.as_array(desc.initial_velocity, (3 * n,))
+    lumped, _ = ctx.masses()
+    inv_m = np.repeat(np.where(lumped > 0, 1.0 / np.where(lumped > 0, lumped, 1.0), 0.0), 3)
+    fixed = np.zeros(n, bool)
+    if desc.n_fixed:
+        fixed[np.ctypeslib.as_array(desc.fixed_nodes, (desc.n_fixed,))] = True
+    fixed3 = np.repeat(fixed, 3)
+    dt = 1e-5
+    ctx.compute_forces(u, f_int)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        f_ext[:] = 0.0
+        for c in range(desc.n_contacts):
+            ctx.contact_apply(c, u, None, None, dt, f_ext)
+        a = (f_ext - f_int) * inv_m
+        vh[:] = v + 0.5 * dt * a
+        u += dt * vh
+        u[fixed3] = 0.0
+        f_int[:] = 0.0
+        ctx.compute_forces(u, f_int)
+        a = (f_ext - f_int) * inv_m
+        v[:] = vh + 0.5 * dt * a
+        v[fixed3] = 0.0
+    wall = time.perf_counter() - t0
+    h2d = 8 * 3 * n * (desc.n_contacts + 1)
+    d2h = 8 * 3 * n * (desc.n_contacts + 1)
+    return n_hc * steps / wall, h2d, d2h
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=40)
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+
+    world, rank, local = dist_setup()
+    from crushrs_b200 import scenarios as S
+
+    model = S.Model.build(S.refined_headon())
+    desc = model.desc
+    n_nodes = desc.n_nodes
+    config = {"workload": "refined head-on, 0.05 m hexahedra (36x30x138 + 36x24x150)", "elements": None, "nodes": n_nodes,
+              "steps_per_run": "to separation, <= 5000", "l2": "per-step working set > L2 (126 MB), no flush",
+              "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        threads = os.cpu_count() or 1
+        n_hc = sum(1 for p in model.hex_part() if model.material(p).model == 0)
+        config["elements"] = n_hc
+        steps, loop, sec = cpu_reference(desc, args.steps, threads)
+        value = n_hc * steps / loop
+        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "elem-upd/s", "n_gpus": args.gpus, "steps": int(steps),
+                "warmup": args.warmup, "ms_per_step": 1e3 * loop / steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32 element / f64 nodal", "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": value, "unit": "elem-upd/s", "cores": threads, "kind": "port",
+                                 "sample": f"{steps} steps of the refined head-on (whole step: contact, forces, update, dt), oracle f32 8-lane AVX2 restatement"},
+                "e2e": {"value": value, "unit": "elem-upd/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    from crushrs_b200.engine import Context
+
+    ctx = Context(desc, device=local)
+    n_hc = ctx.n_active
+    config["elements"] = n_hc
+    ctx.run_begin()
+    ctx.run_steps_timed(args.warmup, phases=True)
+    barrier(world)
+    launches0 = ctx.launches()
+    with ClockSampler(local) as clocks:
+        done, ms, phases, psteps = ctx.run_steps_timed(args.steps, phases=True)
+    launches = ctx.launches() - launches0
+    ms_max = all_max(ms, world)
+    barrier(world)
+    value = world * n_hc * args.steps / (ms_max / 1e3)
+    peak, peak_kind = measured_peak()
+    forces_ms = phases[3] / psteps
+    bytes_launch = BYTES_ELEM_KERNEL * n_hc + BYTES_NODE_KERNEL * n_nodes
+    achieved = bytes_launch / (forces_ms / 1e3) / 1e9
+    step_bytes = BYTES_STEP_ELEM * n_hc + BYTES_STEP_NODE * n_nodes
+    step_gbs = step_bytes / (ms / args.steps / 1e3) / 1e9
+    traffic = read_traffic(n_hc)
+    line = {"metric": METRIC, "value": value, "unit": "elem-upd/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 element / f64 nodal", "data": "synthetic", "config": config, "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": "k_forces", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "traffic": traffic, "bytes_per_launch": bytes_launch, "avg_launch_ms": forces_ms},
+            "step_roofline": {"bytes_per_step": step_bytes, "achieved": step_gbs, "frac": step_gbs / peak},
+            "phase_ms_per_step": {k: v / psteps for k, v in zip(["dt", "contact", "half", "forces", "gather_full", "checks"], phases)},
+            "clocks": clocks.summary(), "run_done_early": done}
+    if rank == 0 and world == 1 and not args.no_e2e:
+        e, h2d, d2h = e2e_dropin(ctx, desc, args.e2e_steps, n_hc)
+        line["e2e"] = {"value": e, "unit": "elem-upd/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                       "path": "crush_contact_apply x contacts + crush_compute_forces, host f64 state, pinned buffers"}
+        ctx.close()
+        t0 = time.perf_counter()
+        c2 = Context(desc, device=local)
+        r = c2.run()
+        wall = time.perf_counter() - t0
+        line["e2e_run"] = {"value": n_hc * r.steps / wall, "unit": "elem-upd/s", "steps": int(r.steps), "wall_s": wall,
+                           "h2d_bytes_per_step": int((8 * 6 * n_nodes + 36 * desc.n_hexes) / max(r.steps, 1)),
+                           "d2h_bytes_per_step": int(8 * 3 * n_nodes / max(r.steps, 1)),
+                           "delta_v": [r.vehicle[k].delta_v[0] for k in range(r.n_vehicles)]}
+        c2.close()
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        steps, loop, sec = cpu_reference(desc, args.cpu_steps, threads)
+        line["cpu_baseline"] = {"value": n_hc * steps / loop, "unit": "elem-upd/s", "cores": threads, "kind": "port",
+                                "sample": f"{steps} steps of the same mesh (contact, forces, update, dt), oracle f32 8-lane AVX2 restatement"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -200,3 +200,4 @@ def declare_engine_api(lib):
     lib.crush_run_state.argtypes = [vp, dp, dp]
     lib.crush_launch_count.argtypes = [vp]
     lib.crush_launch_count.restype = C.c_int64
+    lib.crush_run_steps_timed.argtypes = [vp, C.c_int64, P(C.c_int), dp, dp, P(C.c_int)]

@@ -140,6 +140,9 @@ struct crush_ctx {
     int period = 20;
     cudaGraphExec_t graph = nullptr;
     int64_t graph_launches = 0;
+    bool profiling = false;
+    bool last_was_graph = false;
+    std::vector<cudaEvent_t> prof_ev;
 
     ElementArrays el() const {
         ElementArrays e;
@@ -200,6 +203,7 @@ struct crush_ctx {
     }
     ~crush_ctx() {
         if (graph) cudaGraphExecDestroy(graph);
+        for (cudaEvent_t e : prof_ev) cudaEventDestroy(e);
         if (stream) cudaStreamSynchronize(stream);
         for (void* p : allocs) cudaFree(p);
         if (stream) cudaStreamDestroy(stream);
@@ -547,11 +551,19 @@ int sync(crush_ctx* c) {
 }
 
 // One explicit step on the stream (src/solver.rs:287-345).
-int enqueue_step(crush_ctx* c, long long step) {
+// Phase boundaries of one step recorded when profiling: start, after dt,
+// after contact, after half step, after element forces, after full step, end.
+constexpr int N_PHASE_EVENTS = 7;
+
+int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr) {
     const crush_settings& s = c->settings;
     ElementArrays el = c->el();
     NodeArrays nd = c->nd();
     int n = 0;
+    auto mark = [&](int i) {
+        if (ev) cudaEventRecord(ev[i], c->stream);
+    };
+    mark(0);
     const bool adaptive = !(s.time_step > 0.0) && s.adaptive_check_steps > 0;
     if (adaptive && step % s.adaptive_check_steps == 0) {
         launch_elem_dt(c->stream, el, nd, c->ctl, c->u, c->dt_partials, 1);
@@ -559,13 +571,18 @@ int enqueue_step(crush_ctx* c, long long step) {
         launch_mass_scaling(c->stream, el, nd, c->ctl, 0);
         n += 3;
     }
+    mark(1);
     if (c->n_contacts > 0) {
         launch_contact(c->stream, c->ca, nd, c->ctl, 0, c->n_contacts, c->n_faces, c->n_slaves, c->entries_cap, 0.0, c->mass, c->f_ext, 1);
         n += (c->n_faces > 0 ? 3 : 0) + (c->n_slaves > 0 ? 1 : 0) + 1;
     }
+    mark(2);
     launch_half(c->stream, nd, c->ctl);
+    mark(3);
     launch_forces(c->stream, el, nd, c->ctl, 1);
+    mark(4);
     launch_full(c->stream, el, nd, c->ctl);
+    mark(5);
     n += 2 + (c->n_hc > 0 ? 1 : 0);
     if ((step + 1) % 20 == 0) {
         launch_nonfinite(c->stream, nd, c->ctl);
@@ -578,6 +595,7 @@ int enqueue_step(crush_ctx* c, long long step) {
     }
     launch_step_end(c->stream, c->ctl, c->ca, sep ? 1 : 0);
     ++n;
+    mark(6);
     return check_launch(c, n);
 }
 
@@ -626,11 +644,26 @@ int run_begin(crush_ctx* c) {
     return sync(c);
 }
 
+int ensure_prof_events(crush_ctx* c) {
+    size_t want = (size_t)std::max(c->period, 1) * N_PHASE_EVENTS;
+    while (c->prof_ev.size() < want) {
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        c->prof_ev.push_back(e);
+    }
+    return CRUSH_OK;
+}
+
 int build_graph(crush_ctx* c) {
+    if (c->profiling) {
+        int st0 = ensure_prof_events(c);
+        if (st0 != CRUSH_OK) return st0;
+    }
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     int st = CRUSH_OK;
-    for (int k = 0; k < c->period && st == CRUSH_OK; ++k) st = enqueue_step(c, k);
+    for (int k = 0; k < c->period && st == CRUSH_OK; ++k)
+        st = enqueue_step(c, k, c->profiling ? &c->prof_ev[(size_t)k * N_PHASE_EVENTS] : nullptr);
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
     if (st != CRUSH_OK) return st;
     if (e != cudaSuccess) return crush::fail(CRUSH_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
@@ -658,11 +691,18 @@ int run_steps(crush_ctx* c, long long n_steps, int* done) {
             c->host_step += c->period;
             issued += c->period;
         } else {
-            st = enqueue_step(c, c->host_step);
+            if (c->profiling) {
+                st = ensure_prof_events(c);
+                if (st != CRUSH_OK) return st;
+            }
+            st = enqueue_step(c, c->host_step, c->profiling ? &c->prof_ev[0] : nullptr);
             if (st != CRUSH_OK) return st;
             c->host_step += 1;
             issued += 1;
+            c->last_was_graph = false;
+            continue;
         }
+        c->last_was_graph = true;
     }
     int d = 0;
     CK(cudaMemcpyAsync(&d, &c->ctl->done, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -970,6 +1010,79 @@ int crush_run_state(crush_ctx* c, double* u, double* v) {
     return sync(c);
 }
 
+int crush_run_steps_timed(crush_ctx* c, int64_t n_steps, int* done, double* ms, double* phase_ms, int* phase_steps) {
+    if (!c) return crush::fail(CRUSH_ERR_INVALID, "null context");
+    CK(cudaSetDevice(c->device));
+    const bool want_phases = phase_ms != nullptr;
+    if (want_phases != c->profiling) {
+        c->profiling = want_phases;
+        if (c->graph) {
+            cudaGraphExecDestroy(c->graph);
+            c->graph = nullptr;
+        }
+    }
+    cudaEvent_t t0, t1;
+    CK(cudaEventCreate(&t0));
+    CK(cudaEventCreate(&t1));
+    CK(cudaEventRecord(t0, c->stream));
+    // run_steps ends with a sync after reading the done flag; record t1 first.
+    int st = CRUSH_OK;
+    {
+        long long issued = 0;
+        while (issued < n_steps && st == CRUSH_OK) {
+            const bool use_graph = c->period > 0 && c->host_step % c->period == 0 && n_steps - issued >= c->period;
+            const long long chunk = use_graph ? c->period : 1;
+            // enqueue without the trailing sync of run_steps
+            if (use_graph) {
+                if (!c->graph) {
+                    int64_t before = c->launches;
+                    st = build_graph(c);
+                    if (st != CRUSH_OK) break;
+                    c->graph_launches = c->launches - before;
+                    c->launches = before;
+                }
+                cudaError_t e = cudaGraphLaunch(c->graph, c->stream);
+                if (e != cudaSuccess) { st = crush::fail(CRUSH_ERR_CUDA, cudaGetErrorString(e)); break; }
+                c->launches += c->graph_launches;
+                c->host_step += c->period;
+                c->last_was_graph = true;
+            } else {
+                if (c->profiling) {
+                    st = ensure_prof_events(c);
+                    if (st != CRUSH_OK) break;
+                }
+                st = enqueue_step(c, c->host_step, c->profiling ? &c->prof_ev[0] : nullptr);
+                c->host_step += 1;
+                c->last_was_graph = false;
+            }
+            issued += chunk;
+        }
+    }
+    CK(cudaEventRecord(t1, c->stream));
+    int d = 0;
+    CK(cudaMemcpyAsync(&d, &c->ctl->done, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    float elapsed = 0.f;
+    CK(cudaEventElapsedTime(&elapsed, t0, t1));
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (st != CRUSH_OK) return st;
+    if (done) *done = d;
+    if (ms) *ms = elapsed;
+    if (want_phases) {
+        int steps = c->last_was_graph ? c->period : 1;
+        for (int i = 0; i < N_PHASE_EVENTS - 1; ++i) phase_ms[i] = 0.0;
+        for (int k = 0; k < steps; ++k)
+            for (int i = 0; i < N_PHASE_EVENTS - 1; ++i) {
+                float x = 0.f;
+                CK(cudaEventElapsedTime(&x, c->prof_ev[(size_t)k * N_PHASE_EVENTS + i], c->prof_ev[(size_t)k * N_PHASE_EVENTS + i + 1]));
+                phase_ms[i] += x;
+            }
+        if (phase_steps) *phase_steps = steps;
+    }
+    return CRUSH_OK;
+}
+
 int crush_run(crush_ctx* c, crush_results* r) {
     if (!c || !r) return crush::fail(CRUSH_ERR_INVALID, "null argument");
     int st = crush_run_begin(c);
@@ -977,7 +1090,8 @@ int crush_run(crush_ctx* c, crush_results* r) {
     int done = 0;
     const long long chunk = c->period > 0 ? 10 * (long long)c->period : 200;
     long long total = 0;
-    const long long cap = 100000000ll;
+    // A run that has not finished after this many steps is returned as a timeout.
+    const long long cap = c->settings.max_steps > 0 ? (long long)c->settings.max_steps + chunk : 2000000ll;
     while (!done && total < cap) {
         st = run_steps(c, chunk, &done);
         if (st != CRUSH_OK) return st;
@@ -985,6 +1099,10 @@ int crush_run(crush_ctx* c, crush_results* r) {
     }
     st = results(c, r);
     if (st != CRUSH_OK) return st;
+    if (!done && r->status == CRUSH_OK) {
+        r->status = CRUSH_ERR_TIMEOUT;
+        return crush::fail(CRUSH_ERR_TIMEOUT, "run did not finish within " + std::to_string(cap) + " steps");
+    }
     return r->status;
 }
 

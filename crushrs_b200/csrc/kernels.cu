@@ -650,6 +650,38 @@ __device__ __forceinline__ unsigned cell_hash(long long i, long long j, long lon
     return (unsigned)(h ^ (h >> 29));
 }
 
+// Grid cells covered by a face's expanded box. False (the face goes to the
+// contact's overflow list) when the box is not finite or spans more than
+// MAX_CELLS_PER_FACE cells; each axis range is checked before any product,
+// so a loop over the returned range is always short.
+__device__ __forceinline__ bool face_cells(const FaceGeo& g, double cs, long long* i0, long long* i1, long long* j0,
+                                           long long* j1, long long* k0, long long* k1) {
+    for (int d = 0; d < 3; ++d)
+        if (!isfinite(g.lo[d]) || !isfinite(g.hi[d]) || !(g.lo[d] <= g.hi[d])) return false;
+    const double lim = 4.0e15;  // cell coordinates stay exact in f64 and far from long long overflow
+    double a0 = floor(g.lo[0] / cs), a1 = floor(g.hi[0] / cs);
+    double b0 = floor(g.lo[1] / cs), b1 = floor(g.hi[1] / cs);
+    double c0 = floor(g.lo[2] / cs), c1 = floor(g.hi[2] / cs);
+    if (fabs(a0) > lim || fabs(a1) > lim || fabs(b0) > lim || fabs(b1) > lim || fabs(c0) > lim || fabs(c1) > lim) return false;
+    const double da = a1 - a0, db = b1 - b0, dc = c1 - c0;
+    if (da < 0.0 || db < 0.0 || dc < 0.0 || da >= MAX_CELLS_PER_FACE || db >= MAX_CELLS_PER_FACE || dc >= MAX_CELLS_PER_FACE) return false;
+    if ((da + 1.0) * (db + 1.0) * (dc + 1.0) > MAX_CELLS_PER_FACE) return false;
+    *i0 = (long long)a0; *i1 = (long long)a1;
+    *j0 = (long long)b0; *j1 = (long long)b1;
+    *k0 = (long long)c0; *k1 = (long long)c1;
+    return true;
+}
+
+// Cell of a point (any finite coordinates; non-finite points map to cell 0).
+__device__ __forceinline__ unsigned point_cell_hash(const double* p, double cs) {
+    long long q[3];
+    for (int d = 0; d < 3; ++d) {
+        double a = floor(p[d] / cs);
+        q[d] = (isfinite(a) && fabs(a) <= 4.0e15) ? (long long)a : 0;
+    }
+    return cell_hash(q[0], q[1], q[2]);
+}
+
 __global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctl, int c0, int c1, int run_mode) {
     long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (run_mode && ctl->done) return;
@@ -685,12 +717,9 @@ __global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctl, i
     }
     ca.geo[f] = g;
     const double cs = ca.cell[c];
-    long long i0 = (long long)floor(g.lo[0] / cs), i1 = (long long)floor(g.hi[0] / cs);
-    long long j0 = (long long)floor(g.lo[1] / cs), j1 = (long long)floor(g.hi[1] / cs);
-    long long k0 = (long long)floor(g.lo[2] / cs), k1 = (long long)floor(g.hi[2] / cs);
-    long long ncell = (i1 - i0 + 1) * (j1 - j0 + 1) * (k1 - k0 + 1);
+    long long i0, i1, j0, j1, k0, k1;
     const int local = (int)(f - ca.face_off[c]);
-    if (!(ncell >= 1 && ncell <= MAX_CELLS_PER_FACE)) {
+    if (!face_cells(g, cs, &i0, &i1, &j0, &j1, &k0, &k1)) {
         int slot = atomicAdd(&ca.n_overflow[c], 1);
         if (slot < ca.overflow_cap) ca.overflow[(long long)c * ca.overflow_cap + slot] = local;
         return;
@@ -739,11 +768,8 @@ __global__ void k_contact_fill(ContactArrays ca, Control* ctl, int c0, int c1, i
     const int c = contact_of(ca.face_off, ca.n_contacts, f);
     const FaceGeo& g = ca.geo[f];
     const double cs = ca.cell[c];
-    long long i0 = (long long)floor(g.lo[0] / cs), i1 = (long long)floor(g.hi[0] / cs);
-    long long j0 = (long long)floor(g.lo[1] / cs), j1 = (long long)floor(g.hi[1] / cs);
-    long long k0 = (long long)floor(g.lo[2] / cs), k1 = (long long)floor(g.hi[2] / cs);
-    long long ncell = (i1 - i0 + 1) * (j1 - j0 + 1) * (k1 - k0 + 1);
-    if (!(ncell >= 1 && ncell <= MAX_CELLS_PER_FACE)) return;
+    long long i0, i1, j0, j1, k0, k1;
+    if (!face_cells(g, cs, &i0, &i1, &j0, &j1, &k0, &k1)) return;
     const int local = (int)(f - ca.face_off[c]);
     const int tab = ca.tab_off[c];
     const unsigned mask = (unsigned)(ca.tab_off[c + 1] - tab - 1);
@@ -814,7 +840,7 @@ __global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctl, 
         const double cs = ca.cell[c];
         const int tab = ca.tab_off[c];
         const unsigned mask = (unsigned)(ca.tab_off[c + 1] - tab - 1);
-        const int b = tab + (int)(cell_hash((long long)floor(p[0] / cs), (long long)floor(p[1] / cs), (long long)floor(p[2] / cs)) & mask);
+        const int b = tab + (int)(point_cell_hash(p, cs) & mask);
         const int e0 = ca.starts[b], e1 = e0 + ca.counts[b];
         for (int k = e0; k < e1 && k < entries_cap; ++k) {
             const int f = ca.entries[k];

@@ -1,0 +1,153 @@
+"""Python face of the engine's C ABI, named after the reference's hot-path
+calls (crushrs src/kernel.rs, src/contact.rs, src/solver.rs).
+
+    ctx = Context(model_desc)               # Elements::build + lumped masses + ContactRuntime::new
+    n = ctx.compute_forces(u, f_int)        # Elements::compute_forces (adds into f_int)
+    ctx.contact_apply(c, u, v, m, dt, f)    # ContactRuntime::apply (adds into f)
+    dt = ctx.stable_time_step(u)            # Elements::stable_time_step (None if no limit)
+    total = ctx.mass_scaling(u, dt_min, element_mass, added)
+    results = ctx.run()                     # crushrs::run
+
+Every call goes to the CUDA library; there is no CPU path.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from .native import CrushError, check, lib
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Context:
+    """One model resident on one GPU (crush_ctx)."""
+
+    def __init__(self, desc, device=0):
+        self._lib = lib()
+        h = C.c_void_p()
+        check(self._lib.crush_create(C.byref(desc), device, C.byref(h)))
+        self.h = h
+        nn, ne, na = C.c_int64(), C.c_int64(), C.c_int64()
+        check(self._lib.crush_sizes(self.h, C.byref(nn), C.byref(ne), C.byref(na)))
+        self.n_nodes, self.n_hexes, self.n_active = nn.value, ne.value, na.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._lib.crush_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- drop-in calls ----
+    def compute_forces(self, u, global_forces):
+        """Element forces at u, added into global_forces (3N f64); returns the newly eroded count."""
+        assert global_forces.dtype == np.float64 and global_forces.flags.c_contiguous
+        u = _f64(u)
+        n = C.c_int64()
+        check(self._lib.crush_compute_forces(self.h, _dp(u), _dp(global_forces), C.byref(n)))
+        return n.value
+
+    def compute_forces_device(self, u_ptr, f_ptr, want_count=False):
+        """Device-pointer variant (ints are raw CUDA addresses)."""
+        n = C.c_int64()
+        check(self._lib.crush_compute_forces_device(self.h, C.c_void_p(u_ptr), C.c_void_p(f_ptr), C.byref(n) if want_count else None))
+        return n.value
+
+    def contact_apply(self, contact_id, u, v, masses, dt, force):
+        assert force.dtype == np.float64 and force.flags.c_contiguous
+        cnt, mp = C.c_int64(), C.c_double()
+        check(self._lib.crush_contact_apply(self.h, contact_id, _dp(_f64(u)), None if v is None else _dp(_f64(v)),
+                                            None if masses is None else _dp(_f64(masses)), dt, _dp(force), C.byref(cnt), C.byref(mp)))
+        return cnt.value, mp.value
+
+    def stable_time_step(self, u):
+        dt = C.c_double()
+        st = check(self._lib.crush_stable_dt(self.h, _dp(_f64(u)), C.byref(dt)), allow=(abi.CRUSH_OK, abi.CRUSH_NONE))
+        return dt.value if st == abi.CRUSH_OK else None
+
+    def mass_scaling(self, u, dt_min, element_mass=None, added=None):
+        added = np.zeros(self.n_nodes) if added is None else added
+        total = C.c_double()
+        em = None if element_mass is None else _f64(element_mass)
+        check(self._lib.crush_mass_scaling(self.h, _dp(_f64(u)), dt_min, _dp(em), _dp(added), C.byref(total)))
+        return total.value, added
+
+    def masses(self):
+        lumped, em = np.zeros(self.n_nodes), np.zeros(self.n_hexes)
+        check(self._lib.crush_masses(self.h, _dp(lumped), _dp(em)))
+        return lumped, em
+
+    def element_data(self):
+        n = self.n_active
+        g, v, gm, hh = (np.zeros((n, 24), np.float32), np.zeros(n, np.float32), np.zeros((n, 32), np.float32),
+                        np.zeros((n, 144), np.float32))
+        fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+        check(self._lib.crush_element_data(self.h, fp(g), fp(v), fp(gm), fp(hh)))
+        return g, v, gm, hh
+
+    def get_state(self):
+        s, e = np.zeros((self.n_active, 25), np.float32), np.zeros(self.n_active, np.uint8)
+        check(self._lib.crush_get_state(self.h, s.ctypes.data_as(C.POINTER(C.c_float)), e.ctypes.data_as(C.POINTER(C.c_uint8))))
+        return s, e
+
+    def set_state(self, s, e):
+        s = np.ascontiguousarray(s, np.float32)
+        e = np.ascontiguousarray(e, np.uint8)
+        check(self._lib.crush_set_state(self.h, s.ctypes.data_as(C.POINTER(C.c_float)), e.ctypes.data_as(C.POINTER(C.c_uint8))))
+
+    # ---- whole runs ----
+    def run(self):
+        r = abi.Results()
+        st = self._lib.crush_run(self.h, C.byref(r))
+        if st not in (abi.CRUSH_OK, abi.CRUSH_ERR_NONFINITE):
+            raise CrushError(st, self._lib.crush_last_error().decode())
+        return r
+
+    def run_begin(self):
+        check(self._lib.crush_run_begin(self.h))
+
+    def run_steps(self, n):
+        done = C.c_int()
+        check(self._lib.crush_run_steps(self.h, n, C.byref(done)))
+        return bool(done.value)
+
+    def run_steps_timed(self, n, phases=False):
+        """Advance n steps; returns (done, device ms, phase ms array or None, phase steps)."""
+        done, ms = C.c_int(), C.c_double()
+        ph = np.zeros(6) if phases else None
+        ps = C.c_int()
+        check(self._lib.crush_run_steps_timed(self.h, n, C.byref(done), C.byref(ms), _dp(ph), C.byref(ps)))
+        return bool(done.value), ms.value, ph, ps.value
+
+    def results(self):
+        r = abi.Results()
+        check(self._lib.crush_run_results(self.h, C.byref(r)))
+        return r
+
+    def state(self):
+        u, v = np.zeros(3 * self.n_nodes), np.zeros(3 * self.n_nodes)
+        check(self._lib.crush_run_state(self.h, _dp(u), _dp(v)))
+        return u, v
+
+    def launches(self):
+        return self._lib.crush_launch_count(self.h)
+
+
+def run(desc, device=0):
+    """crushrs::run on the GPU: results of a whole run of `desc`."""
+    ctx = Context(desc, device)
+    try:
+        return ctx.run()
+    finally:
+        ctx.close()

@@ -227,6 +227,13 @@ int crush_run(crush_ctx* ctx, crush_results* results);
 int crush_run_begin(crush_ctx* ctx);
 /* Advance an open run by n_steps (fewer if it stops); *done = 1 when finished. */
 int crush_run_steps(crush_ctx* ctx, int64_t n_steps, int* done);
+/* crush_run_steps with the device time of the steps measured by CUDA events
+ * on the context's stream (*ms). With phase_ms (6 doubles) non-NULL the step
+ * graph also records events between phases and phase_ms gets the summed
+ * device time of each phase (stable dt + mass scaling, contact, half step,
+ * element forces, force gather + full step, checks) over the last
+ * *phase_steps steps of the call. */
+int crush_run_steps_timed(crush_ctx* ctx, int64_t n_steps, int* done, double* ms, double* phase_ms, int* phase_steps);
 /* Results of the open run so far (final after *done). */
 int crush_run_results(crush_ctx* ctx, crush_results* results);
 /* Nodal displacement and velocity (host, 3N each; either may be NULL). */

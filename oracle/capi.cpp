@@ -245,7 +245,12 @@ int oracle_run(const crush_model_desc* d, int simd, int threads, crush_results* 
     if (v_out) std::memcpy(v_out, r.v.data(), r.v.size() * sizeof(double));
     if (dt_log)
         for (int64_t k = 0; k < dt_log_cap && k < (int64_t)r.dt_log.size(); ++k) dt_log[k] = r.dt_log[k];
-    if (seconds3) { seconds3[0] = r.wall_seconds; seconds3[1] = r.force_seconds; seconds3[2] = r.contact_seconds; }
+    if (seconds3) {  // wall, forces, contact, step loop
+        seconds3[0] = r.wall_seconds;
+        seconds3[1] = r.force_seconds;
+        seconds3[2] = r.contact_seconds;
+        seconds3[3] = r.loop_seconds;
+    }
     return r.status;
 }
 

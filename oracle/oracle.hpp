@@ -189,7 +189,7 @@ struct RunResults {
     int status = 0;
     std::vector<double> u, v, masses;
     std::vector<double> dt_log;
-    double force_seconds = 0.0, contact_seconds = 0.0, wall_seconds = 0.0;
+    double force_seconds = 0.0, contact_seconds = 0.0, wall_seconds = 0.0, loop_seconds = 0.0;
 };
 std::string run(const Model& m, const RunOptions& opt, RunResults* r);
 // Delta-v / crush outputs (bin/crushrs.rs:237, :265).

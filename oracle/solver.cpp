@@ -94,6 +94,7 @@ std::string run(const Model& model, const RunOptions& opt, RunResults* res) {
             for (uint32_t nd : f) if (!fixed_set.count(nd)) counts[c] = 1;
     int64_t last_hit = -1;
 
+    double loop0 = now_s();
     double t = 0.0;
     int64_t step = 0;
     int64_t eroded_total = 0;
@@ -165,6 +166,7 @@ std::string run(const Model& model, const RunOptions& opt, RunResults* res) {
     res->u = u;
     res->v = v;
     res->masses = masses;
+    res->loop_seconds = now_s() - loop0;
     res->wall_seconds = now_s() - wall0;
     return "";
 }

@@ -181,7 +181,7 @@ def run(desc, simd=True, threads=1, want_state=False, want_dt=0):
     u = np.zeros(3 * n) if want_state else None
     v = np.zeros(3 * n) if want_state else None
     dt = np.zeros(want_dt) if want_dt else None
-    sec = np.zeros(3)
+    sec = np.zeros(4)  # wall, forces, contact, step loop (s)
     st = lib.oracle_run(C.byref(desc), int(simd), threads, C.byref(r), ptr(u), ptr(v), ptr(dt), want_dt, ptr(sec))
     assert st in (0, abi.CRUSH_ERR_NONFINITE), error()
     return r, u, v, dt, sec
