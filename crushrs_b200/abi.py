@@ -201,3 +201,4 @@ def declare_engine_api(lib):
     lib.crush_launch_count.argtypes = [vp]
     lib.crush_launch_count.restype = C.c_int64
     lib.crush_run_steps_timed.argtypes = [vp, C.c_int64, P(C.c_int), dp, dp, P(C.c_int)]
+    lib.crush_set_profiling.argtypes = [vp, C.c_int]

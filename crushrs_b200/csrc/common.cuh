@@ -63,6 +63,7 @@ struct Control {
     int done;
     int status;
     int nonfinite;
+    int copy_timeout;     // an element tile's bulk copy did not complete within the wait bound
     int mass_scale_now;
     int hit_this_step;
     int adaptive;
@@ -70,7 +71,10 @@ struct Control {
     int pad0;
     long long eroded_step;
     double vx[4];         // mean x-velocities for the separation rule
+    double vx_part[4][64][2];  // per-block (mass, x-momentum) partial sums of the vehicles
 };
+
+constexpr int VX_BLOCKS = 64;
 
 // The step's dt from the control block: dt_cfl clipped to the end time,
 // never below 1e-15 (src/solver.rs:300).

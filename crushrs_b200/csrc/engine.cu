@@ -141,6 +141,7 @@ struct crush_ctx {
     cudaGraphExec_t graph = nullptr;
     int64_t graph_launches = 0;
     bool profiling = false;
+    int prof_level = 2;  // 1: events around the element-force kernel only; 2: every phase
     bool last_was_graph = false;
     std::vector<cudaEvent_t> prof_ev;
 
@@ -361,8 +362,14 @@ int create_impl(const crush_model_desc* d, int device, crush_ctx* c) {
     std::vector<int> face_off(1, 0), slave_off(1, 0), tab_off(1, 0), counts_for_stop;
     std::vector<uint32_t> faces, slaves;
     std::vector<double> scales, stiff, md, cell;
-    // roles per node: (contact, slave position, face member)
-    std::map<uint32_t, std::vector<std::array<int, 3>>> roles;
+    // roles per node: contact, position among the contact's primary nodes
+    // (-1: none), and the contact's faces that contain the node
+    struct Role {
+        int c;
+        int slave;
+        std::vector<int> faces;
+    };
+    std::map<uint32_t, std::vector<Role>> roles;
     for (int k = 0; k < d->n_contacts; ++k) {
         const crush_contact& cd = d->contacts[k];
         if (cd.n_nodes < 0 || cd.n_faces < 0 || (cd.n_nodes > 0 && !cd.nodes) || (cd.n_faces > 0 && !cd.faces))
@@ -371,8 +378,10 @@ int create_impl(const crush_model_desc* d, int device, crush_ctx* c) {
         double lo[3] = {INF, INF, INF}, hi[3] = {-INF, -INF, -INF};
         bool stop = false;
         double ext = 0.0;
+        std::vector<std::array<double, 6>> keys;  // grid key box of each face at the reference positions
         for (int64_t f = 0; f < cd.n_faces; ++f) {
             double flo[3] = {INF, INF, INF}, fhi[3] = {-INF, -INF, -INF};
+            double xs[4][3];
             for (int j = 0; j < 4; ++j) {
                 uint32_t n = cd.faces[4 * f + j];
                 if (n >= (uint64_t)N) return crush::fail(CRUSH_ERR_INVALID, "contact face node out of range");
@@ -380,13 +389,28 @@ int create_impl(const crush_model_desc* d, int device, crush_ctx* c) {
                 if (!fixed[n]) stop = true;
                 for (int dd = 0; dd < 3; ++dd) {
                     double p = d->positions[3 * n + dd];
+                    xs[j][dd] = p;
                     lo[dd] = std::fmin(lo[dd], p);
                     hi[dd] = std::fmax(hi[dd], p);
                     flo[dd] = std::fmin(flo[dd], p);
                     fhi[dd] = std::fmax(fhi[dd], p);
                 }
             }
-            for (int dd = 0; dd < 3; ++dd) ext = std::max(ext, fhi[dd] - flo[dd] + 2.0 * cd.max_distance);
+            double fext = std::max({fhi[0] - flo[0], fhi[1] - flo[1], fhi[2] - flo[2]});
+            ext = std::max(ext, fext);
+            double e1[3], e2[3], nrm[3];
+            for (int dd = 0; dd < 3; ++dd) { e1[dd] = xs[1][dd] - xs[0][dd]; e2[dd] = xs[2][dd] - xs[0][dd]; }
+            nrm[0] = e1[1] * e2[2] - e1[2] * e2[1];
+            nrm[1] = e1[2] * e2[0] - e1[0] * e2[2];
+            nrm[2] = e1[0] * e2[1] - e1[1] * e2[0];
+            double len = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+            std::array<double, 6> kb;
+            for (int dd = 0; dd < 3; ++dd) {
+                double nd = len > 0.0 ? nrm[dd] / len : 0.0;
+                kb[dd] = flo[dd] - 0.25 * fext - cd.max_distance * std::max(nd, 0.0);
+                kb[3 + dd] = fhi[dd] + 0.25 * fext + cd.max_distance * std::max(-nd, 0.0);
+            }
+            keys.push_back(kb);
         }
         for (int dd = 0; dd < 3; ++dd) { lo[dd] += -cd.max_distance; hi[dd] += cd.max_distance; }
         std::vector<uint32_t> all_nodes;
@@ -403,39 +427,51 @@ int create_impl(const crush_model_desc* d, int device, crush_ctx* c) {
             if (!inside) continue;
             slaves.push_back(n);
             scales.push_back(cd.node_scale ? cd.node_scale[i] : 1.0);
-            roles[n].push_back({k, kept, 0});
+            roles[n].push_back(Role{k, kept, {}});
             ++kept;
         }
         for (int64_t f = 0; f < cd.n_faces; ++f)
             for (int j = 0; j < 4; ++j) {
                 uint32_t n = cd.faces[4 * f + j];
                 auto& r = roles[n];
-                if (!r.empty() && r.back()[0] == k) r.back()[2] = 1;
-                else r.push_back({k, -1, 1});
+                if (r.empty() || r.back().c != k) r.push_back(Role{k, -1, {}});
+                if (r.back().faces.empty() || r.back().faces.back() != (int)f) r.back().faces.push_back((int)f);
             }
         c->contact_nodes_all.push_back(all_nodes);
         c->contact_stiffness.push_back(cd.stiffness);
         face_off.push_back(face_off.back() + (int)cd.n_faces);
         slave_off.push_back(slave_off.back() + kept);
-        size_t t = next_pow2(std::max<size_t>(256, 4 * (size_t)cd.n_faces));
+        // Grid cell: twice the largest face; table: twice the initial key-box
+        // cell count, a power of two.
+        const double cs = ext > 0.0 ? 2.0 * ext : 1.0;
+        size_t inserts = 0;
+        for (const auto& kb : keys) {
+            size_t cells = 1;
+            for (int dd = 0; dd < 3; ++dd) cells *= (size_t)(std::floor(kb[3 + dd] / cs) - std::floor(kb[dd] / cs) + 1.0);
+            inserts += std::min<size_t>(cells, 128);
+        }
+        size_t t = next_pow2(std::max<size_t>(1024, 2 * inserts));
         tab_off.push_back(tab_off.back() + (int)t);
         stiff.push_back(cd.stiffness);
         md.push_back(cd.max_distance);
-        cell.push_back(ext > 0.0 ? ext : 1.0);
+        cell.push_back(cs);
         counts_for_stop.push_back(stop ? 1 : 0);
     }
     c->n_faces = face_off.back();
     c->n_slaves = slave_off.back();
-    c->entries_cap = (int)std::max<long long>(64, c->n_faces * 64);
+    c->entries_cap = 0;
     std::vector<uint32_t> cnode, cnode_off(1, 0);
-    std::vector<int> crole_contact, crole_slave;
+    std::vector<int> crole_contact, crole_slave, crole_faces;
     std::vector<uint8_t> crole_face;
+    std::vector<uint32_t> crole_faces_off(1, 0);
     for (auto& kv : roles) {
         cnode.push_back(kv.first);
         for (auto& r : kv.second) {
-            crole_contact.push_back(r[0]);
-            crole_slave.push_back(r[1]);
-            crole_face.push_back((uint8_t)r[2]);
+            crole_contact.push_back(r.c);
+            crole_slave.push_back(r.slave);
+            crole_face.push_back(r.faces.empty() ? 0 : 1);
+            crole_faces.insert(crole_faces.end(), r.faces.begin(), r.faces.end());
+            crole_faces_off.push_back((uint32_t)crole_faces.size());
         }
         cnode_off.push_back((uint32_t)crole_contact.size());
     }
@@ -455,9 +491,7 @@ int create_impl(const crush_model_desc* d, int device, crush_ctx* c) {
     TRY(c->upload(const_cast<double**>(&ca.cell), cell.data(), cell.size()));
     TRY(c->upload(const_cast<int**>(&ca.tab_off), tab_off.data(), nc1));
     TRY(c->alloc(&ca.counts, std::max(tab_off.back(), 1)));
-    TRY(c->alloc(&ca.starts, std::max(tab_off.back(), 1)));
-    TRY(c->alloc(&ca.entries, c->entries_cap));
-    ca.entry_off = nullptr;
+    TRY(c->alloc(&ca.entries, (size_t)std::max(tab_off.back(), 1) * BUCKET_CAP));
     ca.overflow_cap = (int)std::max<long long>(1, face_off.empty() ? 1 : *std::max_element(face_off.begin(), face_off.end()));
     {
         int cap = 1;
@@ -476,6 +510,11 @@ int create_impl(const crush_model_desc* d, int device, crush_ctx* c) {
     TRY(c->upload(const_cast<int**>(&ca.crole_contact), crole_contact.data(), crole_contact.size()));
     TRY(c->upload(const_cast<int**>(&ca.crole_slave), crole_slave.data(), crole_slave.size()));
     TRY(c->upload(const_cast<uint8_t**>(&ca.crole_face), crole_face.data(), crole_face.size()));
+    TRY(c->upload(const_cast<uint32_t**>(&ca.crole_faces_off), crole_faces_off.data(), crole_faces_off.size()));
+    TRY(c->upload(const_cast<int**>(&ca.crole_faces), crole_faces.data(), crole_faces.size()));
+    TRY(c->alloc(&ca.face_hits, std::max<long long>(c->n_faces, 1)));
+    TRY(c->alloc(&ca.face_list, (size_t)std::max<long long>(c->n_faces, 1) * FACE_HIT_CAP));
+    CK(cudaMemsetAsync(ca.face_hits, 0, sizeof(int) * std::max<long long>(c->n_faces, 1), c->stream));
     CK(cudaMemsetAsync(ca.counts, 0, sizeof(int) * std::max(tab_off.back(), 1), c->stream));
     CK(cudaMemsetAsync(ca.n_overflow, 0, sizeof(int) * std::max(c->n_contacts, 1), c->stream));
     CK(cudaMemsetAsync(ca.entry_overrun, 0, sizeof(int) * std::max(c->n_contacts, 1), c->stream));
@@ -555,13 +594,18 @@ int sync(crush_ctx* c) {
 // after contact, after half step, after element forces, after full step, end.
 constexpr int N_PHASE_EVENTS = 7;
 
-int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr) {
+int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool capturing = false) {
     const crush_settings& s = c->settings;
     ElementArrays el = c->el();
     NodeArrays nd = c->nd();
     int n = 0;
+    // Inside a stream capture an event record must be an external event node
+    // for its timestamp to be readable after the graph runs.
     auto mark = [&](int i) {
-        if (ev) cudaEventRecord(ev[i], c->stream);
+        if (!ev) return;
+        if (c->prof_level == 1 && i != 3 && i != 4) return;  // element-force kernel only
+        if (capturing) cudaEventRecordWithFlags(ev[i], c->stream, cudaEventRecordExternal);
+        else cudaEventRecord(ev[i], c->stream);
     };
     mark(0);
     const bool adaptive = !(s.time_step > 0.0) && s.adaptive_check_steps > 0;
@@ -574,7 +618,7 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr) {
     mark(1);
     if (c->n_contacts > 0) {
         launch_contact(c->stream, c->ca, nd, c->ctl, 0, c->n_contacts, c->n_faces, c->n_slaves, c->entries_cap, 0.0, c->mass, c->f_ext, 1);
-        n += (c->n_faces > 0 ? 3 : 0) + (c->n_slaves > 0 ? 1 : 0) + 1;
+        n += (c->n_faces > 0 ? 1 : 0) + (c->n_slaves > 0 ? 1 : 0) + 1;
     }
     mark(2);
     launch_half(c->stream, nd, c->ctl);
@@ -663,7 +707,7 @@ int build_graph(crush_ctx* c) {
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     int st = CRUSH_OK;
     for (int k = 0; k < c->period && st == CRUSH_OK; ++k)
-        st = enqueue_step(c, k, c->profiling ? &c->prof_ev[(size_t)k * N_PHASE_EVENTS] : nullptr);
+        st = enqueue_step(c, k, c->profiling ? &c->prof_ev[(size_t)k * N_PHASE_EVENTS] : nullptr, true);
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
     if (st != CRUSH_OK) return st;
     if (e != cudaSuccess) return crush::fail(CRUSH_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
@@ -797,15 +841,21 @@ int crush_compute_forces_device(crush_ctx* c, const double* u_device, double* f_
     CK(cudaSetDevice(c->device));
     NodeArrays nd = c->nd();
     nd.u = const_cast<double*>(u_device);
-    if (newly) CK(cudaMemsetAsync(&c->ctl_aux->eroded_step, 0, sizeof(long long), c->stream));
+    if (newly) {
+        CK(cudaMemsetAsync(&c->ctl_aux->eroded_step, 0, sizeof(long long), c->stream));
+        CK(cudaMemsetAsync(&c->ctl_aux->copy_timeout, 0, sizeof(int), c->stream));
+    }
     launch_forces(c->stream, c->el(), nd, c->ctl_aux, 0);
     launch_gather(c->stream, c->el(), nd, f_device);
     int st = check_launch(c, (c->n_hc > 0 ? 1 : 0) + 1);
     if (st != CRUSH_OK) return st;
     if (newly) {
         long long k = 0;
+        int timeout = 0;
         CK(cudaMemcpyAsync(&k, &c->ctl_aux->eroded_step, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(&timeout, &c->ctl_aux->copy_timeout, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
+        if (timeout) return crush::fail(CRUSH_ERR_TIMEOUT, "element tile copy did not complete");
         *newly = k;
     }
     return CRUSH_OK;
@@ -852,7 +902,7 @@ int crush_contact_apply(crush_ctx* c, int id, const double* u, const double* v, 
     CK(cudaMemcpyAsync(so, c->ca.slave_off + id, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     launch_contact(c->stream, c->ca, nd, nullptr, id, id + 1, fo[1] - fo[0], so[1] - so[0], c->entries_cap, dt, m, c->f_tmp, 0);
-    int st = check_launch(c, 5);
+    int st = check_launch(c, (fo[1] > fo[0] ? 1 : 0) + (so[1] > so[0] ? 1 : 0) + 1);
     if (st != CRUSH_OK) return st;
     std::vector<double> f(3 * c->n_nodes);
     unsigned long long cnt = 0, mp = 0;
@@ -1010,6 +1060,18 @@ int crush_run_state(crush_ctx* c, double* u, double* v) {
     return sync(c);
 }
 
+int crush_set_profiling(crush_ctx* c, int level) {
+    if (!c || level < 1 || level > 2) return crush::fail(CRUSH_ERR_INVALID, "profiling level must be 1 or 2");
+    if (level != c->prof_level) {
+        c->prof_level = level;
+        if (c->graph) {
+            cudaGraphExecDestroy(c->graph);
+            c->graph = nullptr;
+        }
+    }
+    return CRUSH_OK;
+}
+
 int crush_run_steps_timed(crush_ctx* c, int64_t n_steps, int* done, double* ms, double* phase_ms, int* phase_steps) {
     if (!c) return crush::fail(CRUSH_ERR_INVALID, "null context");
     CK(cudaSetDevice(c->device));
@@ -1074,6 +1136,7 @@ int crush_run_steps_timed(crush_ctx* c, int64_t n_steps, int* done, double* ms, 
         for (int i = 0; i < N_PHASE_EVENTS - 1; ++i) phase_ms[i] = 0.0;
         for (int k = 0; k < steps; ++k)
             for (int i = 0; i < N_PHASE_EVENTS - 1; ++i) {
+                if (c->prof_level == 1 && i != 3) continue;
                 float x = 0.f;
                 CK(cudaEventElapsedTime(&x, c->prof_ev[(size_t)k * N_PHASE_EVENTS + i], c->prof_ev[(size_t)k * N_PHASE_EVENTS + i + 1]));
                 phase_ms[i] += x;

@@ -299,7 +299,13 @@ __global__ void k_init_state(long long n_hc, long long stride, float4* __restric
 // ---------------------------------------------------------------------------
 // Element forces (src/kernel_simd.rs:300-491, one element per thread).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(TPB) k_forces(ElementArrays el, NodeArrays nd, Control* ctl, int respect_done) {
+#ifndef FORCES_TPB
+#define FORCES_TPB 256
+#endif
+#ifndef FORCES_MINB
+#define FORCES_MINB 2
+#endif
+__global__ void __launch_bounds__(FORCES_TPB, FORCES_MINB) k_forces(ElementArrays el, NodeArrays nd, Control* ctl, int respect_done) {
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (respect_done && ctl->done) return;
     if (e >= el.n_hc) return;
@@ -625,11 +631,26 @@ __global__ void k_step_end(Control* ctl, ContactArrays ca, int check_separation)
         ctl->status = -2;  // CRUSH_ERR_NONFINITE
         return;
     }
+    if (ctl->copy_timeout) {
+        ctl->done = 1;
+        ctl->status = -4;  // CRUSH_ERR_TIMEOUT
+        return;
+    }
     if (ctl->max_steps > 0 && ctl->step >= ctl->max_steps) ctl->done = 1;
     if (!(ctl->t < ctl->end_time)) ctl->done = 1;
-    if (check_separation && ctl->stop_rule == 1 && ctl->step % 10 == 0 && ctl->last_hit >= 0 &&
-        ctl->step - 1 - ctl->last_hit >= 100 && ctl->vx[1] - ctl->vx[0] >= 0.0)
-        ctl->done = 1;
+    if (check_separation) {
+        for (int veh = 0; veh < 2; ++veh) {
+            double m = 0.0, p = 0.0;
+            for (int b = 0; b < VX_BLOCKS; ++b) {
+                m += ctl->vx_part[veh][b][0];
+                p += ctl->vx_part[veh][b][1];
+            }
+            ctl->vx[veh] = m > 0.0 ? p / m : 0.0;
+        }
+        if (ctl->stop_rule == 1 && ctl->step % 10 == 0 && ctl->last_hit >= 0 && ctl->step - 1 - ctl->last_hit >= 100 &&
+            ctl->vx[1] - ctl->vx[0] >= 0.0)
+            ctl->done = 1;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -637,7 +658,7 @@ __global__ void k_step_end(Control* ctl, ContactArrays ca, int check_separation)
 // hashed uniform grid rebuilt every step, first-hit (minimum face index)
 // search per primary node, and an ordered gather of the reactions.
 // ---------------------------------------------------------------------------
-constexpr int MAX_CELLS_PER_FACE = 64;
+constexpr int MAX_CELLS_PER_FACE = 1024;
 
 __device__ __forceinline__ int contact_of(const int* off, int n_contacts, long long i) {
     int c = 0;
@@ -650,25 +671,28 @@ __device__ __forceinline__ unsigned cell_hash(long long i, long long j, long lon
     return (unsigned)(h ^ (h >> 29));
 }
 
-// Grid cells covered by a face's expanded box. False (the face goes to the
-// contact's overflow list) when the box is not finite or spans more than
+// Grid cells covered by a box. False (the face goes to the contact's
+// overflow list) when the box is not finite or spans more than
 // MAX_CELLS_PER_FACE cells; each axis range is checked before any product,
 // so a loop over the returned range is always short.
-__device__ __forceinline__ bool face_cells(const FaceGeo& g, double cs, long long* i0, long long* i1, long long* j0,
-                                           long long* j1, long long* k0, long long* k1) {
+__device__ __forceinline__ bool box_cells(const double* lo, const double* hi, double cs, long long* r) {
     for (int d = 0; d < 3; ++d)
-        if (!isfinite(g.lo[d]) || !isfinite(g.hi[d]) || !(g.lo[d] <= g.hi[d])) return false;
+        if (!isfinite(lo[d]) || !isfinite(hi[d]) || !(lo[d] <= hi[d])) return false;
     const double lim = 4.0e15;  // cell coordinates stay exact in f64 and far from long long overflow
-    double a0 = floor(g.lo[0] / cs), a1 = floor(g.hi[0] / cs);
-    double b0 = floor(g.lo[1] / cs), b1 = floor(g.hi[1] / cs);
-    double c0 = floor(g.lo[2] / cs), c1 = floor(g.hi[2] / cs);
-    if (fabs(a0) > lim || fabs(a1) > lim || fabs(b0) > lim || fabs(b1) > lim || fabs(c0) > lim || fabs(c1) > lim) return false;
-    const double da = a1 - a0, db = b1 - b0, dc = c1 - c0;
-    if (da < 0.0 || db < 0.0 || dc < 0.0 || da >= MAX_CELLS_PER_FACE || db >= MAX_CELLS_PER_FACE || dc >= MAX_CELLS_PER_FACE) return false;
-    if ((da + 1.0) * (db + 1.0) * (dc + 1.0) > MAX_CELLS_PER_FACE) return false;
-    *i0 = (long long)a0; *i1 = (long long)a1;
-    *j0 = (long long)b0; *j1 = (long long)b1;
-    *k0 = (long long)c0; *k1 = (long long)c1;
+    double a[6];
+    for (int d = 0; d < 3; ++d) {
+        a[2 * d] = floor(lo[d] / cs);
+        a[2 * d + 1] = floor(hi[d] / cs);
+        if (fabs(a[2 * d]) > lim || fabs(a[2 * d + 1]) > lim) return false;
+    }
+    double prod = 1.0;
+    for (int d = 0; d < 3; ++d) {
+        const double span = a[2 * d + 1] - a[2 * d];
+        if (span < 0.0 || span >= MAX_CELLS_PER_FACE) return false;
+        prod *= span + 1.0;
+    }
+    if (prod > MAX_CELLS_PER_FACE) return false;
+    for (int k = 0; k < 6; ++k) r[k] = (long long)a[k];
     return true;
 }
 
@@ -682,12 +706,21 @@ __device__ __forceinline__ unsigned point_cell_hash(const double* p, double cs) 
     return cell_hash(q[0], q[1], q[2]);
 }
 
+// Face geometry (src/contact.rs:95-110) and its insertion into the grid, one
+// warp per face (every lane derives the same geometry; the lanes split the
+// cells). The grid key box is a superset of every point the narrow test can
+// accept: a hit needs -max_distance <= signed <= 0, i.e. the point lies at
+// most max_distance behind its projection along -n, and the projection inside
+// one of the face's triangles with barycentric tolerance 0.1, i.e. within the
+// triangle scaled 1.3x about its centroid, which lies inside the face's box
+// grown by 0.2 of its largest extent. So the key box is the face box grown by
+// 0.25 x extent + 4 x warp on every side and by max_distance x n_d on the
+// inner side of axis d.
 __global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctl, int c0, int c1, int run_mode) {
-    long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (run_mode && ctl->done) return;
-    const long long f_begin = ca.face_off[c0], f_end = ca.face_off[c1];
-    f += f_begin;
-    if (f >= f_end) return;
+    const long long f = ca.face_off[c0] + (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (f >= ca.face_off[c1]) return;
     const int c = contact_of(ca.face_off, ca.n_contacts, f);
     FaceGeo g;
     for (int k = 0; k < 4; ++k) {
@@ -705,6 +738,7 @@ __global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctl, i
     double len = sqrt(nx * nx + ny * ny + nz * nz);
     g.n[0] = nx / len; g.n[1] = ny / len; g.n[2] = nz / len;
     const double md = ca.max_distance[c];
+    double flo[3], fhi[3];
     for (int d = 0; d < 3; ++d) {
         g.c[d] = (((g.x[0][d] + g.x[1][d]) + g.x[2][d]) + g.x[3][d]) / 4.0;
         double lo = g.x[0][d], hi = g.x[0][d];
@@ -712,75 +746,44 @@ __global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctl, i
             lo = fmin(lo, g.x[k][d]);
             hi = fmax(hi, g.x[k][d]);
         }
+        flo[d] = lo;
+        fhi[d] = hi;
         g.lo[d] = lo + -md;
         g.hi[d] = hi + md;
     }
-    ca.geo[f] = g;
-    const double cs = ca.cell[c];
-    long long i0, i1, j0, j1, k0, k1;
+    if (lane == 0) {
+        ca.geo[f] = g;
+        ca.face_hits[f] = 0;
+    }
+    const double ext = fmax(fmax(fhi[0] - flo[0], fhi[1] - flo[1]), fhi[2] - flo[2]);
+    double warp = 0.0;
+    for (int k = 0; k < 4; ++k)
+        warp = fmax(warp, fabs(g.n[0] * (g.x[k][0] - g.c[0]) + g.n[1] * (g.x[k][1] - g.c[1]) + g.n[2] * (g.x[k][2] - g.c[2])));
+    const double slack = 0.25 * ext + 4.0 * warp + 1e-9 * (1.0 + ext + md);
+    double klo[3], khi[3];
+    for (int d = 0; d < 3; ++d) {
+        klo[d] = fmax(flo[d] - slack - md * fmax(g.n[d], 0.0), g.lo[d]);
+        khi[d] = fmin(fhi[d] + slack + md * fmax(-g.n[d], 0.0), g.hi[d]);
+    }
     const int local = (int)(f - ca.face_off[c]);
-    if (!face_cells(g, cs, &i0, &i1, &j0, &j1, &k0, &k1)) {
-        int slot = atomicAdd(&ca.n_overflow[c], 1);
-        if (slot < ca.overflow_cap) ca.overflow[(long long)c * ca.overflow_cap + slot] = local;
+    long long r[6];
+    if (!box_cells(klo, khi, ca.cell[c], r)) {
+        if (lane == 0) {
+            int slot = atomicAdd(&ca.n_overflow[c], 1);
+            if (slot < ca.overflow_cap) ca.overflow[(long long)c * ca.overflow_cap + slot] = local;
+            else ca.entry_overrun[c] = 1;
+        }
         return;
     }
     const int tab = ca.tab_off[c];
     const unsigned mask = (unsigned)(ca.tab_off[c + 1] - tab - 1);
-    for (long long i = i0; i <= i1; ++i)
-        for (long long j = j0; j <= j1; ++j)
-            for (long long k = k0; k <= k1; ++k) atomicAdd(&ca.counts[tab + (cell_hash(i, j, k) & mask)], 1);
-}
-
-// Exclusive scan of the grid counts of contacts [c0, c1) (one block).
-__global__ void __launch_bounds__(1024) k_contact_scan(ContactArrays ca, Control* ctl, int c0, int c1, int run_mode) {
-    __shared__ int s_part[1024];
-    if (run_mode && ctl->done) return;
-    const int begin = ca.tab_off[c0], end = ca.tab_off[c1];
-    const int n = end - begin;
-    const int per = (n + blockDim.x - 1) / blockDim.x;
-    const int lo = begin + threadIdx.x * per;
-    const int hi = min(lo + per, end);
-    int sum = 0;
-    for (int i = lo; i < hi; ++i) sum += ca.counts[i];
-    s_part[threadIdx.x] = sum;
-    __syncthreads();
-    for (int w = 1; w < (int)blockDim.x; w <<= 1) {
-        int v = threadIdx.x >= (unsigned)w ? s_part[threadIdx.x - w] : 0;
-        __syncthreads();
-        s_part[threadIdx.x] += v;
-        __syncthreads();
+    const int ni = (int)(r[1] - r[0] + 1), nj = (int)(r[3] - r[2] + 1), nk = (int)(r[5] - r[4] + 1);
+    for (int q = lane; q < ni * nj * nk; q += 32) {
+        const long long i = r[0] + q % ni, j = r[2] + (q / ni) % nj, k = r[4] + q / (ni * nj);
+        const int b = tab + (int)(cell_hash(i, j, k) & mask);
+        const int slot = atomicAdd(&ca.counts[b], 1);
+        if (slot < BUCKET_CAP) ca.entries[(long long)b * BUCKET_CAP + slot] = local;
     }
-    int run = s_part[threadIdx.x] - sum;
-    for (int i = lo; i < hi; ++i) {
-        int cnt = ca.counts[i];
-        ca.starts[i] = run;
-        ca.counts[i] = 0;
-        run += cnt;
-    }
-}
-
-__global__ void k_contact_fill(ContactArrays ca, Control* ctl, int c0, int c1, int run_mode, int entries_cap) {
-    long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (run_mode && ctl->done) return;
-    const long long f_begin = ca.face_off[c0], f_end = ca.face_off[c1];
-    f += f_begin;
-    if (f >= f_end) return;
-    const int c = contact_of(ca.face_off, ca.n_contacts, f);
-    const FaceGeo& g = ca.geo[f];
-    const double cs = ca.cell[c];
-    long long i0, i1, j0, j1, k0, k1;
-    if (!face_cells(g, cs, &i0, &i1, &j0, &j1, &k0, &k1)) return;
-    const int local = (int)(f - ca.face_off[c]);
-    const int tab = ca.tab_off[c];
-    const unsigned mask = (unsigned)(ca.tab_off[c + 1] - tab - 1);
-    for (long long i = i0; i <= i1; ++i)
-        for (long long j = j0; j <= j1; ++j)
-            for (long long k = k0; k <= k1; ++k) {
-                const int b = tab + (int)(cell_hash(i, j, k) & mask);
-                const int pos = ca.starts[b] + atomicAdd(&ca.counts[b], 1);
-                if (pos < entries_cap) ca.entries[pos] = local;
-                else ca.entry_overrun[c] = 1;
-            }
 }
 
 // src/contact.rs:29-43
@@ -817,41 +820,63 @@ __device__ __forceinline__ bool face_hit(const FaceGeo& g, const double* p, doub
     return inside;
 }
 
+constexpr int SLAVE_LANES = 32;
+
+// First-hit search: SLAVE_LANES lanes per primary node test its grid bucket
+// (all of the contact's faces when the bucket overflowed) and the contact's
+// overflow faces, and keep the smallest face index that hits — the face the
+// reference's in-order scan with `break` finds (src/contact.rs:115-157).
 __global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctl, int c0, int c1, int run_mode, double dt_override,
-                                 const double* __restrict__ masses, int entries_cap) {
-    long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+                                 const double* __restrict__ masses) {
     if (run_mode && ctl->done) return;
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x % SLAVE_LANES;
     const long long s_begin = ca.slave_off[c0], s_end = ca.slave_off[c1];
-    s += s_begin;
-    if (s >= s_end) return;
-    const int c = contact_of(ca.slave_off, ca.n_contacts, s);
-    const long long n = ca.slaves[s];
-    const double p[3] = {nd.pos[3 * n] + nd.u[3 * n], nd.pos[3 * n + 1] + nd.u[3 * n + 1], nd.pos[3 * n + 2] + nd.u[3 * n + 2]};
-    const double md = ca.max_distance[c];
-    const long long fb = ca.face_off[c];
-    const FaceGeo* geo = ca.geo + fb;
+    const long long s = s_begin + gid / SLAVE_LANES;
+    const bool live = s < s_end;
     int best = INT_MAX;
     double best_sd = 0.0, sd;
-    if (ca.entry_overrun[c]) {
-        const int nf = (int)(ca.face_off[c + 1] - fb);
-        for (int f = 0; f < nf; ++f)
-            if (face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; break; }
-    } else {
-        const double cs = ca.cell[c];
+    int c = 0;
+    long long n = 0;
+    double p[3] = {0.0, 0.0, 0.0}, md = 0.0;
+    const FaceGeo* geo = nullptr;
+    if (live) {
+        c = contact_of(ca.slave_off, ca.n_contacts, s);
+        n = ca.slaves[s];
+        p[0] = nd.pos[3 * n] + nd.u[3 * n];
+        p[1] = nd.pos[3 * n + 1] + nd.u[3 * n + 1];
+        p[2] = nd.pos[3 * n + 2] + nd.u[3 * n + 2];
+        md = ca.max_distance[c];
+        const long long fb = ca.face_off[c];
+        geo = ca.geo + fb;
         const int tab = ca.tab_off[c];
         const unsigned mask = (unsigned)(ca.tab_off[c + 1] - tab - 1);
-        const int b = tab + (int)(point_cell_hash(p, cs) & mask);
-        const int e0 = ca.starts[b], e1 = e0 + ca.counts[b];
-        for (int k = e0; k < e1 && k < entries_cap; ++k) {
-            const int f = ca.entries[k];
-            if (f < best && face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; }
-        }
-        const int no = min(ca.n_overflow[c], ca.overflow_cap);
-        for (int k = 0; k < no; ++k) {
-            const int f = ca.overflow[(long long)c * ca.overflow_cap + k];
-            if (f < best && face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; }
+        const int b = tab + (int)(point_cell_hash(p, ca.cell[c]) & mask);
+        const int cnt = ca.counts[b];
+        if (cnt > BUCKET_CAP || ca.entry_overrun[c]) {
+            const int nf = (int)(ca.face_off[c + 1] - fb);
+            for (int f = lane; f < nf; f += SLAVE_LANES)
+                if (f < best && face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; }
+        } else {
+            const int* ent = ca.entries + (long long)b * BUCKET_CAP;
+            for (int k = lane; k < cnt; k += SLAVE_LANES) {
+                const int f = ent[k];
+                if (f < best && face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; }
+            }
+            const int no = min(ca.n_overflow[c], ca.overflow_cap);
+            for (int k = lane; k < no; k += SLAVE_LANES) {
+                const int f = ca.overflow[(long long)c * ca.overflow_cap + k];
+                if (f < best && face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; }
+            }
         }
     }
+#pragma unroll
+    for (int off = SLAVE_LANES / 2; off > 0; off >>= 1) {
+        const int ob = __shfl_down_sync(0xffffffffu, best, off, SLAVE_LANES);
+        const double osd = __shfl_down_sync(0xffffffffu, best_sd, off, SLAVE_LANES);
+        if (ob < best) { best = ob; best_sd = osd; }
+    }
+    if (!live || lane != 0) return;
     if (best == INT_MAX) {
         ca.hit[s] = -1;
         return;
@@ -866,65 +891,77 @@ __global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctl, 
     ca.hit_force[3 * s] = mag * g.n[0];
     ca.hit_force[3 * s + 1] = mag * g.n[1];
     ca.hit_force[3 * s + 2] = mag * g.n[2];
+    const long long F = ca.face_off[c] + best;
+    const int slot = atomicAdd(&ca.face_hits[F], 1);
+    if (slot < FACE_HIT_CAP) ca.face_list[F * FACE_HIT_CAP + slot] = (int)s;
     atomicAdd(&ca.pen_count[c], 1ull);
     atomicMax(&ca.pen_max_bits[c], (unsigned long long)__double_as_longlong(-best_sd));
 }
 
-// Ordered reaction gather: one warp per contact node walks its contacts in
-// order and, within each, the primary nodes in order, adding +F for its own
-// hit and -F/4 for every hit on a face it belongs to — the sequence in which
-// src/contact.rs:146-153 adds them. Also clears the grid counts.
+constexpr int MAX_NODE_EVENTS = 48;
+
+// Ordered reaction gather, one thread per contact node: for each of its
+// contacts (in order) it collects its own hit (+F) and the hits on the faces
+// it belongs to (-F/4), sorts them by primary-node order (own before face for
+// the same primary node) and sums them in that order — the sequence in which
+// src/contact.rs:146-153 adds them to f_ext. Then clears the grid.
 __global__ void k_contact_gather(ContactArrays ca, NodeArrays nd, Control* ctl, int c0, int c1, int run_mode,
                                  double* __restrict__ f_out, int skip_fixed) {
     if (run_mode && ctl->done) return;
-    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (warp < ca.n_cnodes) {
-        const long long n = ca.cnode[warp];
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < ca.n_cnodes) {
+        const long long n = ca.cnode[i];
         if (!(skip_fixed && nd.fixed[n])) {
             double sx = 0.0, sy = 0.0, sz = 0.0;
             bool touched = false;
-            for (uint32_t r = ca.cnode_off[warp]; r < ca.cnode_off[warp + 1]; ++r) {
+            for (uint32_t r = ca.cnode_off[i]; r < ca.cnode_off[i + 1]; ++r) {
                 const int c = ca.crole_contact[r];
                 if (c < c0 || c >= c1) continue;
                 touched = true;
-                const long long sb = ca.slave_off[c], se = ca.slave_off[c + 1];
+                const long long sb = ca.slave_off[c];
                 const int own = ca.crole_slave[r];
-                if (!ca.crole_face[r]) {
-                    if (own >= 0 && ca.hit[sb + own] >= 0) {
-                        sx += ca.hit_force[3 * (sb + own)];
-                        sy += ca.hit_force[3 * (sb + own) + 1];
-                        sz += ca.hit_force[3 * (sb + own) + 2];
+                unsigned long long ev[MAX_NODE_EVENTS];
+                int ne = 0;
+                bool overflow = false;
+                if (own >= 0 && ca.hit[sb + own] >= 0) ev[ne++] = 2ull * (unsigned long long)(sb + own);
+                for (uint32_t q = ca.crole_faces_off[r]; q < ca.crole_faces_off[r + 1]; ++q) {
+                    const long long f = ca.face_off[c] + ca.crole_faces[q];
+                    const int cnt = ca.face_hits[f];
+                    if (cnt > FACE_HIT_CAP) { overflow = true; break; }
+                    for (int k = 0; k < cnt; ++k) {
+                        if (ne < MAX_NODE_EVENTS) ev[ne++] = 2ull * (unsigned long long)ca.face_list[f * FACE_HIT_CAP + k] + 1ull;
+                        else overflow = true;
                     }
-                    continue;
                 }
-                const uint32_t* faces = ca.faces + 4 * ca.face_off[c];
-                for (long long base = sb; base < se; base += 32) {
-                    const long long s = base + lane;
-                    int flags = 0;
-                    if (s < se) {
-                        const int h = ca.hit[s];
-                        if (h >= 0) {
-                            if (s - sb == own) flags |= 1;
-                            const uint32_t* q = faces + 4 * (long long)h;
-                            if (q[0] == n || q[1] == n || q[2] == n || q[3] == n) flags |= 2;
-                        }
+                if (!overflow) {
+                    for (int a = 1; a < ne; ++a) {  // insertion sort, tiny lists
+                        unsigned long long key = ev[a];
+                        int b = a - 1;
+                        while (b >= 0 && ev[b] > key) { ev[b + 1] = ev[b]; --b; }
+                        ev[b + 1] = key;
                     }
-                    unsigned mask = __ballot_sync(0xffffffffu, flags != 0);
-                    while (mask) {
-                        const int l = __ffs(mask) - 1;
-                        mask &= mask - 1;
-                        const int fl = __shfl_sync(0xffffffffu, flags, l);
-                        const long long ss = base + l;
-                        if (lane == 0) {
-                            const double fx = ca.hit_force[3 * ss], fy = ca.hit_force[3 * ss + 1], fz = ca.hit_force[3 * ss + 2];
-                            if (fl & 1) { sx += fx; sy += fy; sz += fz; }
-                            if (fl & 2) { sx -= 0.25 * fx; sy -= 0.25 * fy; sz -= 0.25 * fz; }
-                        }
+                    for (int a = 0; a < ne; ++a) {
+                        const long long s = (long long)(ev[a] >> 1);
+                        const double fx = ca.hit_force[3 * s], fy = ca.hit_force[3 * s + 1], fz = ca.hit_force[3 * s + 2];
+                        if (ev[a] & 1ull) { sx -= 0.25 * fx; sy -= 0.25 * fy; sz -= 0.25 * fz; }
+                        else { sx += fx; sy += fy; sz += fz; }
+                    }
+                } else {
+                    // More events than the lists hold: walk the contact's
+                    // primary nodes in order instead.
+                    const long long se = ca.slave_off[c + 1];
+                    const uint32_t* faces = ca.faces + 4 * ca.face_off[c];
+                    for (long long s = sb; s < se; ++s) {
+                        const int h = ca.hit[s];
+                        if (h < 0) continue;
+                        const double fx = ca.hit_force[3 * s], fy = ca.hit_force[3 * s + 1], fz = ca.hit_force[3 * s + 2];
+                        if (s - sb == own) { sx += fx; sy += fy; sz += fz; }
+                        const uint32_t* qn = faces + 4 * (long long)h;
+                        if (qn[0] == n || qn[1] == n || qn[2] == n || qn[3] == n) { sx -= 0.25 * fx; sy -= 0.25 * fy; sz -= 0.25 * fz; }
                     }
                 }
             }
-            if (lane == 0 && touched) {
+            if (touched) {
                 f_out[3 * n] = sx;
                 f_out[3 * n + 1] = sy;
                 f_out[3 * n + 2] = sz;
@@ -932,10 +969,12 @@ __global__ void k_contact_gather(ContactArrays ca, NodeArrays nd, Control* ctl, 
         }
     }
     // Clear the grid for the next build.
-    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long nthreads = (long long)gridDim.x * blockDim.x;
-    for (long long i = ca.tab_off[c0] + tid; i < ca.tab_off[c1]; i += nthreads) ca.counts[i] = 0;
-    for (long long c = c0 + tid; c < c1; c += nthreads) ca.n_overflow[c] = 0;
+    for (long long k = ca.tab_off[c0] + i; k < ca.tab_off[c1]; k += nthreads) ca.counts[k] = 0;
+    for (long long c = c0 + i; c < c1; c += nthreads) {
+        ca.n_overflow[c] = 0;
+        ca.entry_overrun[c] = 0;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -970,13 +1009,19 @@ __global__ void __launch_bounds__(VEH_TPB) k_vehicle_sums(const long long* __res
         for (int k = 0; k < 7; ++k) out[7 * veh + k] = s[k][0];
 }
 
+// Mean x-velocity partial sums for the separation rule: VX_BLOCKS blocks per
+// vehicle, each over a contiguous slice of the vehicle's nodes; k_step_end
+// adds the partials in block order.
 __global__ void __launch_bounds__(VEH_TPB) k_vehicle_vx(const long long* __restrict__ off, const uint32_t* __restrict__ nodes,
                                                         const double* __restrict__ mass, const double* __restrict__ v, Control* ctl) {
     __shared__ double sm[VEH_TPB], sp[VEH_TPB];
     if (ctl->done) return;
-    const int veh = blockIdx.x;
+    const int veh = blockIdx.x / VX_BLOCKS, b = blockIdx.x % VX_BLOCKS;
+    const long long n0 = off[veh], len = off[veh + 1] - off[veh];
+    const long long per = (len + VX_BLOCKS - 1) / VX_BLOCKS;
+    const long long lo = n0 + b * per, hi = min(lo + per, n0 + len);
     double m_acc = 0.0, p_acc = 0.0;
-    for (long long i = off[veh] + threadIdx.x; i < off[veh + 1]; i += VEH_TPB) {
+    for (long long i = lo + threadIdx.x; i < hi; i += VEH_TPB) {
         const long long n = nodes[i];
         m_acc += mass[n];
         p_acc += mass[n] * v[3 * n];
@@ -991,7 +1036,10 @@ __global__ void __launch_bounds__(VEH_TPB) k_vehicle_vx(const long long* __restr
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0 && veh < 4) ctl->vx[veh] = sm[0] > 0.0 ? sp[0] / sm[0] : 0.0;
+    if (threadIdx.x == 0 && veh < 4) {
+        ctl->vx_part[veh][b][0] = sm[0];
+        ctl->vx_part[veh][b][1] = sp[0];
+    }
 }
 
 }  // namespace
@@ -1016,7 +1064,7 @@ void launch_init_state(cudaStream_t s, long long n_hc, long long stride, float4*
 }
 void launch_forces(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctl, int respect_done) {
     if (el.n_hc <= 0) return;
-    k_forces<<<(unsigned)blocks_for(el.n_hc, TPB), TPB, 0, s>>>(el, nd, ctl, respect_done);
+    k_forces<<<(unsigned)blocks_for(el.n_hc, FORCES_TPB), FORCES_TPB, 0, s>>>(el, nd, ctl, respect_done);
 }
 void launch_gather(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, double* f_out) {
     k_gather<<<(unsigned)blocks_for(nd.n, TPB), TPB, 0, s>>>(el, nd, f_out);
@@ -1052,27 +1100,23 @@ void launch_vehicle_sums(cudaStream_t s, int n_veh, const long long* veh_off, co
 void launch_vehicle_vx(cudaStream_t s, int n_veh, const long long* veh_off, const uint32_t* veh_nodes, const double* mass,
                        const double* v, Control* ctl) {
     if (n_veh <= 0) return;
-    k_vehicle_vx<<<n_veh, VEH_TPB, 0, s>>>(veh_off, veh_nodes, mass, v, ctl);
+    k_vehicle_vx<<<std::min(n_veh, 4) * VX_BLOCKS, VEH_TPB, 0, s>>>(veh_off, veh_nodes, mass, v, ctl);
 }
 
 // Contact pass over contacts [c0, c1): faces + grid, first-hit search, ordered
 // reaction gather into f_out. n_faces / n_slaves are the host-known totals of
 // that range. dt_override > 0 is the drop-in call (no run control block).
 void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctl, int c0, int c1,
-                          long long n_faces, long long n_slaves, int entries_cap, double dt_override, const double* masses,
-                          double* f_out, int skip_fixed) {
+                    long long n_faces, long long n_slaves, int entries_cap, double dt_override, const double* masses,
+                    double* f_out, int skip_fixed) {
+    (void)entries_cap;
     if (c1 <= c0) return;
     const int run_mode = dt_override > 0.0 ? 0 : 1;
-    if (n_faces > 0) {
-        k_contact_faces<<<(unsigned)blocks_for(n_faces, TPB), TPB, 0, s>>>(ca, nd, ctl, c0, c1, run_mode);
-        k_contact_scan<<<1, 1024, 0, s>>>(ca, ctl, c0, c1, run_mode);
-        k_contact_fill<<<(unsigned)blocks_for(n_faces, TPB), TPB, 0, s>>>(ca, ctl, c0, c1, run_mode, entries_cap);
-    }
+    if (n_faces > 0) k_contact_faces<<<(unsigned)blocks_for(n_faces * 32, TPB), TPB, 0, s>>>(ca, nd, ctl, c0, c1, run_mode);
     if (n_slaves > 0)
-        k_contact_slaves<<<(unsigned)blocks_for(n_slaves, TPB), TPB, 0, s>>>(ca, nd, ctl, c0, c1, run_mode, dt_override, masses,
-                                                                           entries_cap);
-    long long warps = ca.n_cnodes > 0 ? ca.n_cnodes : 1;
-    k_contact_gather<<<(unsigned)blocks_for(warps * 32, TPB), TPB, 0, s>>>(ca, nd, ctl, c0, c1, run_mode, f_out, skip_fixed);
+        k_contact_slaves<<<(unsigned)blocks_for(n_slaves * SLAVE_LANES, TPB), TPB, 0, s>>>(ca, nd, ctl, c0, c1, run_mode, dt_override, masses);
+    long long nodes = ca.n_cnodes > 0 ? ca.n_cnodes : 1;
+    k_contact_gather<<<(unsigned)blocks_for(nodes, 128), 128, 0, s>>>(ca, nd, ctl, c0, c1, run_mode, f_out, skip_fixed);
 }
 
 }  // namespace crush

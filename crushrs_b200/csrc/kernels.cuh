@@ -50,27 +50,32 @@ struct FaceGeo {
     double hi[3];
 };
 
+// Grid buckets hold up to BUCKET_CAP faces (a fuller bucket makes its
+// primary nodes test every face of the contact); per-face hit lists hold
+// FACE_HIT_CAP primary nodes (fuller lists make the gather walk the contact's
+// primary nodes in order).
+constexpr int BUCKET_CAP = 64;
+constexpr int FACE_HIT_CAP = 8;
+
 struct ContactArrays {
     int n_contacts;
     const int* face_off;        // n_contacts+1
     const uint32_t* faces;      // 4 per face (global face index)
     FaceGeo* geo;               // per face
     const int* slave_off;       // n_contacts+1
-    const uint32_t* slaves;     // node id per slave
+    const uint32_t* slaves;     // node id per primary node
     const double* slave_scale;
-    int* hit;                   // per slave: local face index or -1
-    double* hit_force;          // 3 per slave
+    int* hit;                   // per primary node: local face index or -1
+    double* hit_force;          // 3 per primary node
     const double* stiffness;    // per contact
     const double* max_distance; // per contact
     const double* cell;         // per contact grid cell size
     const int* tab_off;         // n_contacts+1, hash tables concatenated (each a power of two)
-    int* counts;                // per table entry
-    int* starts;
-    int* entries;               // face local index per grid entry
-    const int* entry_off;       // n_contacts+1 capacity of entries per contact
-    int* overflow;              // per contact: face list of faces spanning too many cells
+    int* counts;                // per bucket: faces inserted this step
+    int* entries;               // BUCKET_CAP local face indices per bucket
+    int* overflow;              // per contact: faces whose key box spans too many cells
     int* n_overflow;            // per contact
-    int* entry_overrun;         // per contact flag: entries capacity exceeded
+    int* entry_overrun;         // per contact flag: overflow list full (search every face)
     int overflow_cap;           // per contact capacity of overflow
     unsigned long long* pen_count;  // per contact, per step
     unsigned long long* pen_max_bits;
@@ -80,8 +85,12 @@ struct ContactArrays {
     const uint32_t* cnode;      // node id
     const uint32_t* cnode_off;  // n_cnodes+1
     const int* crole_contact;   // per role: contact id
-    const int* crole_slave;     // per role: slave position within the contact (-1 none)
+    const int* crole_slave;     // per role: position among the contact's primary nodes (-1 none)
     const uint8_t* crole_face;  // per role: node belongs to a face of the contact
+    const uint32_t* crole_faces_off;  // per role + 1: range in crole_faces
+    const int* crole_faces;     // local indices of the contact's faces that contain the node
+    int* face_hits;             // per face: primary nodes hitting it this step
+    int* face_list;             // FACE_HIT_CAP primary nodes (global index) per face
 };
 
 void launch_setup_geometry(cudaStream_t s, long long n_all, const double* pos, const uint32_t* conn_all,

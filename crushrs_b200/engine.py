@@ -122,6 +122,10 @@ class Context:
         check(self._lib.crush_run_steps(self.h, n, C.byref(done)))
         return bool(done.value)
 
+    def set_profiling(self, level):
+        """1: time only the element-force kernel inside the step graph; 2: every phase."""
+        check(self._lib.crush_set_profiling(self.h, level))
+
     def run_steps_timed(self, n, phases=False):
         """Advance n steps; returns (done, device ms, phase ms array or None, phase steps)."""
         done, ms = C.c_int(), C.c_double()

@@ -234,6 +234,10 @@ int crush_run_steps(crush_ctx* ctx, int64_t n_steps, int* done);
  * element forces, force gather + full step, checks) over the last
  * *phase_steps steps of the call. */
 int crush_run_steps_timed(crush_ctx* ctx, int64_t n_steps, int* done, double* ms, double* phase_ms, int* phase_steps);
+/* What crush_run_steps_timed's phase events cover: 1 = only the element-force
+ * kernel (two events per step, little overhead; phase_ms[3] is filled),
+ * 2 = every phase (default). */
+int crush_set_profiling(crush_ctx* ctx, int level);
 /* Results of the open run so far (final after *done). */
 int crush_run_results(crush_ctx* ctx, crush_results* results);
 /* Nodal displacement and velocity (host, 3N each; either may be NULL). */
