@@ -20,7 +20,7 @@ constexpr int P_CONN = 0;    // 2 planes: node ids 0-3, 4-7 (uint32 bits)
 constexpr int P_GRAD = 2;    // 6 planes: dN/dX at the centre, grad[3 i + c]
 constexpr int P_GAMMA = 8;   // 8 planes: gamma[4 i + a]
 constexpr int P_H = 16;      // 20 planes: upper triangle of H, row-major (78 used)
-constexpr int P_META = 36;   // 1 plane: volume (f32), material index, model element index, pad
+constexpr int P_META = 36;   // 1 plane: volume (f32), material index, model element index, crash slot
 constexpr int N_STATIC_PLANES = 37;
 // State: F_prev^-1 (9), R (9), stress (6), compaction, eroded flag (as bits), 2 pad.
 constexpr int N_STATE_PLANES = 7;
@@ -55,6 +55,7 @@ struct Control {
     double damping;       // velocity damping factor
     double added_mass_max;
     double added_total;   // total of the last mass scaling
+    double added_total_acc;  // accumulating total of the current stable-dt pass
     unsigned long long dt_stable_bits;  // atomicMin target (bit pattern of a non-negative double)
     long long step;
     long long eroded_total;

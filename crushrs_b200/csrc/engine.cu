@@ -1,11 +1,15 @@
-// engine.cu — the single-model context and the C ABI of include/crush.h.
+// engine.cu — the engine context and the C ABI of include/crush.h.
 //
-// Host side (C++17): validates the model, builds the node incidence CSRs and
-// contact tables, owns every device buffer, and drives the explicit step loop
-// (src/solver.rs:190-381) as a fixed sequence of kernels on one stream,
-// captured into a CUDA graph one period of steps at a time. All per-step
-// decisions (dt, mass scaling, stop rules) are taken on the device from a
-// control block, so the loop never waits on the host.
+// A context holds one or many crash models ("slots") resident on one GPU.
+// Host side (C++17): validates the models, concatenates them (disjoint node,
+// element, face and contact ranges), builds the node incidence CSRs and the
+// contact tables, owns every device buffer, and drives the explicit step
+// loop (src/solver.rs:190-381) as one fixed sequence of kernels per step over
+// all slots, captured into a CUDA graph one period of steps at a time. Each
+// slot keeps its own control block on the device (time, step, dt, mass
+// scaling, stop rules), so slots of different sizes and step sizes advance
+// together and finish independently, and every slot's arithmetic is the
+// arithmetic it has alone.
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -13,7 +17,6 @@
 #include <limits>
 #include <map>
 #include <numeric>
-#include <set>
 #include <string>
 #include <vector>
 
@@ -35,6 +38,7 @@ namespace {
     } while (0)
 
 const double INF = std::numeric_limits<double>::infinity();
+const unsigned long long INF_BITS = 0x7ff0000000000000ull;
 
 // HoneycombParams::from_material with Plasticity::check (src/material.rs:116-151, :430-449).
 int honeycomb_params(const crush_material& m, double knots[MAX_KNOTS][3], std::string* err) {
@@ -86,6 +90,17 @@ size_t next_pow2(size_t x) {
     return p;
 }
 
+// Contacts with fewer faces than this are searched exhaustively by a warp per
+// primary node; larger ones get a hashed grid.
+constexpr int64_t GRID_MIN_FACES = 512;
+
+struct Slot {
+    crush_settings settings{};
+    long long node0 = 0, n_nodes = 0, elem0 = 0, n_elems = 0;
+    int contact0 = 0, n_contacts = 0, vehicle0 = 0, n_vehicles = 0;
+    double contact_dt = INF, stable = INF, dt_floor = 0.0, dt0 = 0.0;
+};
+
 }  // namespace
 
 struct crush_ctx {
@@ -95,41 +110,42 @@ struct crush_ctx {
     int64_t launches = 0;
 
     // sizes
+    int n_slots = 0;
+    std::vector<Slot> slots;
     long long n_nodes = 0, n_all = 0, n_hc = 0, stride = 0;
     std::vector<int64_t> hc_index;   // model element -> honeycomb index or -1
     std::vector<uint32_t> hc_model;  // honeycomb index -> model element
-    crush_settings settings{};
-    double contact_dt = INF, stable = INF, dt_floor = 0.0, dt0 = 0.0;
+    int check_steps = 5;             // common adaptive_check_steps of the slots
+    bool adaptive = true;
+    bool any_separation = false;
 
     // device arrays
     double *pos = nullptr, *u = nullptr, *v = nullptr, *v0 = nullptr, *v_half = nullptr, *f_int = nullptr, *f_ext = nullptr;
     double *inv_mass = nullptr, *mass = nullptr, *added = nullptr, *lumped = nullptr, *volume = nullptr, *dt_factor = nullptr;
-    double *elem_mass = nullptr, *elem_dt = nullptr, *elem_extra = nullptr, *dt_partials = nullptr;
+    double *elem_mass = nullptr, *elem_dt = nullptr, *elem_extra = nullptr;
     double *u_tmp = nullptr, *f_tmp = nullptr, *n_tmp = nullptr, *n_tmp2 = nullptr, *e_tmp = nullptr;
     uint8_t *fixed = nullptr, *eroded_all = nullptr;
     uint32_t *conn_all = nullptr, *hc_off = nullptr, *hc_slot = nullptr, *all_off = nullptr, *all_slot = nullptr;
+    uint32_t *node_slot = nullptr, *elem_slot = nullptr;
     int32_t* part = nullptr;
-    double* mat3 = nullptr;
+    double* mat4 = nullptr;
     int64_t* hc_index_d = nullptr;
     float4 *planes = nullptr, *state = nullptr;
     float* corner = nullptr;
     MaterialF32* mats = nullptr;
-    Control* ctl = nullptr;      // the run
-    Control* ctl_aux = nullptr;  // drop-in calls
-    int dt_blocks = 1;
+    Control* ctls = nullptr;      // the run, one per slot
+    Control* ctls_aux = nullptr;  // drop-in calls, one per slot
 
     // contact
     ContactArrays ca{};
     int n_contacts = 0;
     long long n_faces = 0, n_slaves = 0;
-    int entries_cap = 0;
+    std::vector<int> face_off_h, slave_off_h;
     std::vector<std::vector<uint32_t>> contact_nodes_all;  // unfiltered primary nodes (for contact_dt)
     std::vector<double> contact_stiffness;
 
     // vehicles
-    int n_veh = 0;
-    long long* veh_off = nullptr;
-    uint32_t* veh_nodes = nullptr;
+    VehicleArrays va{};
     double* veh_out = nullptr;
     std::vector<uint32_t> veh_accel;
     std::vector<std::vector<uint32_t>> veh_front;
@@ -160,6 +176,7 @@ struct crush_ctx {
         e.eroded_all = eroded_all;
         e.elem_dt = elem_dt;
         e.elem_extra = elem_extra;
+        e.elem_slot = elem_slot;
         return e;
     }
     NodeArrays nd() const {
@@ -179,6 +196,7 @@ struct crush_ctx {
         a.hc_slot = hc_slot;
         a.all_off = all_off;
         a.all_slot = all_slot;
+        a.node_slot = node_slot;
         return a;
     }
 
@@ -202,6 +220,13 @@ struct crush_ctx {
         if (count) CK(cudaMemcpyAsync(*p, host, count * sizeof(T), cudaMemcpyHostToDevice, stream));
         return CRUSH_OK;
     }
+    template <typename T>
+    int upload_const(const T** p, const std::vector<T>& host) {
+        T* q = nullptr;
+        int st = upload(&q, host.data(), host.size());
+        *p = q;
+        return st;
+    }
     ~crush_ctx() {
         if (graph) cudaGraphExecDestroy(graph);
         for (cudaEvent_t e : prof_ev) cudaEventDestroy(e);
@@ -220,79 +245,132 @@ int check_launch(crush_ctx* c, int n = 1) {
     return CRUSH_OK;
 }
 
-int create_impl(const crush_model_desc* d, int device, crush_ctx* c) {
+int sync(crush_ctx* c) {
+    CK(cudaStreamSynchronize(c->stream));
+    return CRUSH_OK;
+}
+
+// Combined host arrays of all slots.
+struct Combined {
+    std::vector<double> positions, v0, mat4;
+    std::vector<uint32_t> hexes, fixed_list;
+    std::vector<int32_t> hex_part;
+    std::vector<MaterialF32> mats;
+    std::vector<crush_material> materials;
+    std::vector<uint8_t> fixed;
+    std::vector<uint32_t> node_slot, elem_slot;
+};
+
+int validate_and_append(const crush_model_desc* d, int slot, Combined& cm, Slot& sl) {
     if (!d || d->n_nodes <= 0 || !d->positions || d->n_hexes < 0 || (d->n_hexes > 0 && (!d->hexes || !d->hex_part)))
         return crush::fail(CRUSH_ERR_INVALID, "invalid model description");
-    if (d->n_nodes >= (1ll << 31) || d->n_hexes >= (1ll << 28)) return crush::fail(CRUSH_ERR_INVALID, "model too large");
     if (d->n_parts <= 0 || !d->materials) return crush::fail(CRUSH_ERR_INVALID, "model needs at least one material");
     const crush_settings& s = d->settings;
     if (!(s.dt_scale > 0.0) || s.adaptive_check_steps < 0 || !(s.hourglass >= 0.0))
         return crush::fail(CRUSH_ERR_INVALID, "invalid settings");
-    c->settings = s;
-    c->device = device;
-    CK(cudaSetDevice(device));
-    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     const long long N = d->n_nodes, E = d->n_hexes;
-    c->n_nodes = N;
-    c->n_all = E;
-
-    // Fixed nodes.
-    std::vector<uint8_t> fixed(N, 0);
+    const long long n0 = (long long)cm.positions.size() / 3;
+    const int p0 = (int)cm.materials.size();
+    if (n0 + N >= (1ll << 31) || (long long)cm.hex_part.size() + E >= (1ll << 28)) return crush::fail(CRUSH_ERR_INVALID, "model too large");
+    sl.settings = s;
+    sl.node0 = n0;
+    sl.n_nodes = N;
+    sl.elem0 = (long long)cm.hex_part.size();
+    sl.n_elems = E;
+    cm.positions.insert(cm.positions.end(), d->positions, d->positions + 3 * N);
+    if (d->initial_velocity) cm.v0.insert(cm.v0.end(), d->initial_velocity, d->initial_velocity + 3 * N);
+    else cm.v0.insert(cm.v0.end(), 3 * N, 0.0);
+    cm.fixed.insert(cm.fixed.end(), N, 0);
+    cm.node_slot.insert(cm.node_slot.end(), N, (uint32_t)slot);
     for (int64_t i = 0; i < d->n_fixed; ++i) {
         if (d->fixed_nodes[i] >= (uint64_t)N) return crush::fail(CRUSH_ERR_INVALID, "fixed node out of range");
-        fixed[d->fixed_nodes[i]] = 1;
+        cm.fixed[n0 + d->fixed_nodes[i]] = 1;
     }
-    // Materials.
-    std::vector<MaterialF32> mats(d->n_parts);
-    std::vector<double> mat3(3 * d->n_parts);
     for (int p = 0; p < d->n_parts; ++p) {
         const crush_material& m = d->materials[p];
         if (!(m.density > 0.0) || !(m.youngs_modulus > 0.0) || !(m.poisson_ratio >= 0.0 && m.poisson_ratio < 0.5))
             return crush::fail(CRUSH_ERR_INVALID, "material " + std::to_string(p) + ": needs E > 0, density > 0, 0 <= nu < 0.5");
-        mat3[3 * p] = m.youngs_modulus;
-        mat3[3 * p + 1] = m.poisson_ratio;
-        mat3[3 * p + 2] = m.density;
-        std::memset(&mats[p], 0, sizeof(MaterialF32));
+        MaterialF32 mf;
+        std::memset(&mf, 0, sizeof(mf));
         if (m.model == CRUSH_MAT_HONEYCOMB) {
             double knots[MAX_KNOTS][3];
             std::string err;
             if (honeycomb_params(m, knots, &err) != 0) return crush::fail(CRUSH_ERR_INVALID, "material " + std::to_string(p) + ": " + err);
-            mats[p].youngs = (float)m.youngs_modulus;
-            mats[p].trans = (float)m.transverse_factor;
+            mf.youngs = (float)m.youngs_modulus;
+            mf.trans = (float)m.transverse_factor;
             for (int k = 0; k < MAX_KNOTS; ++k) {
-                mats[p].knot_c[k] = (float)knots[k][0];
-                mats[p].knot_s[k] = (float)knots[k][1];
-                mats[p].knot_h[k] = (float)knots[k][2];
+                mf.knot_c[k] = (float)knots[k][0];
+                mf.knot_s[k] = (float)knots[k][1];
+                mf.knot_h[k] = (float)knots[k][2];
             }
         } else if (m.model != CRUSH_MAT_ELASTIC) {
             return crush::fail(CRUSH_ERR_UNSUPPORTED, "unknown material model");
         }
+        cm.mats.push_back(mf);
+        cm.materials.push_back(m);
+        cm.mat4.insert(cm.mat4.end(), {m.youngs_modulus, m.poisson_ratio, m.density, s.hourglass});
     }
-    // Elements: honeycomb ones run the force kernel; elastic ones must be rigid.
-    c->hc_index.assign(E, -1);
-    c->hc_model.clear();
     for (long long e = 0; e < E; ++e) {
         int p = d->hex_part[e];
         if (p < 0 || p >= d->n_parts) return crush::fail(CRUSH_ERR_INVALID, "hexahedron part out of range");
-        for (int i = 0; i < 8; ++i)
+        for (int i = 0; i < 8; ++i) {
             if (d->hexes[8 * e + i] >= (uint64_t)N) return crush::fail(CRUSH_ERR_INVALID, "hexahedron node out of range");
-        if (d->materials[p].model == CRUSH_MAT_HONEYCOMB) {
-            c->hc_index[e] = (int64_t)c->hc_model.size();
-            c->hc_model.push_back((uint32_t)e);
-        } else {
+            cm.hexes.push_back((uint32_t)(n0 + d->hexes[8 * e + i]));
+        }
+        cm.hex_part.push_back(p0 + p);
+        cm.elem_slot.push_back((uint32_t)slot);
+        if (d->materials[p].model != CRUSH_MAT_HONEYCOMB)
             for (int i = 0; i < 8; ++i)
-                if (!fixed[d->hexes[8 * e + i]])
+                if (!cm.fixed[n0 + d->hexes[8 * e + i]])
                     return crush::fail(CRUSH_ERR_UNSUPPORTED, "elastic elements are supported only as rigid slabs (every node fixed)");
+    }
+    return CRUSH_OK;
+}
+
+int create_impl(const crush_model_desc* const* descs, int n_desc, int device, crush_ctx* c) {
+    if (n_desc <= 0 || !descs) return crush::fail(CRUSH_ERR_INVALID, "no models");
+    c->device = device;
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->n_slots = n_desc;
+    c->slots.resize(n_desc);
+    Combined cm;
+    for (int k = 0; k < n_desc; ++k) {
+        int st = validate_and_append(descs[k], k, cm, c->slots[k]);
+        if (st != CRUSH_OK) return st;
+    }
+    // The step schedule is shared: every slot must re-check its stable step
+    // on the same cadence.
+    {
+        const crush_settings& s0 = descs[0]->settings;
+        c->adaptive = !(s0.time_step > 0.0) && s0.adaptive_check_steps > 0;
+        c->check_steps = s0.adaptive_check_steps > 0 ? s0.adaptive_check_steps : 1;
+        for (int k = 0; k < n_desc; ++k) {
+            const crush_settings& s = descs[k]->settings;
+            bool ad = !(s.time_step > 0.0) && s.adaptive_check_steps > 0;
+            if (ad != c->adaptive || (ad && s.adaptive_check_steps != c->check_steps))
+                return crush::fail(CRUSH_ERR_UNSUPPORTED, "models of one context must share adaptive_check_steps and time-step mode");
+            if (s.stop_rule == CRUSH_STOP_SEPARATION) c->any_separation = true;
         }
     }
+    const long long N = (long long)cm.positions.size() / 3, E = (long long)cm.hex_part.size();
+    c->n_nodes = N;
+    c->n_all = E;
+    c->hc_index.assign(E, -1);
+    c->hc_model.clear();
+    for (long long e = 0; e < E; ++e)
+        if (cm.materials[cm.hex_part[e]].model == CRUSH_MAT_HONEYCOMB) {
+            c->hc_index[e] = (int64_t)c->hc_model.size();
+            c->hc_model.push_back((uint32_t)e);
+        }
     c->n_hc = (long long)c->hc_model.size();
     c->stride = std::max<long long>(32, (c->n_hc + 31) / 32 * 32);
     // Node incidence CSRs, slots in increasing element order.
     std::vector<uint32_t> all_off(N + 1, 0), hc_off(N + 1, 0);
     for (long long e = 0; e < E; ++e)
         for (int i = 0; i < 8; ++i) {
-            all_off[d->hexes[8 * e + i] + 1]++;
-            if (c->hc_index[e] >= 0) hc_off[d->hexes[8 * e + i] + 1]++;
+            all_off[cm.hexes[8 * e + i] + 1]++;
+            if (c->hc_index[e] >= 0) hc_off[cm.hexes[8 * e + i] + 1]++;
         }
     for (long long n = 0; n < N; ++n) {
         all_off[n + 1] += all_off[n];
@@ -303,7 +381,7 @@ int create_impl(const crush_model_desc* d, int device, crush_ctx* c) {
         std::vector<uint32_t> ca(all_off.begin(), all_off.end() - 1), ch(hc_off.begin(), hc_off.end() - 1);
         for (long long e = 0; e < E; ++e)
             for (int i = 0; i < 8; ++i) {
-                uint32_t n = d->hexes[8 * e + i];
+                uint32_t n = cm.hexes[8 * e + i];
                 all_slot[ca[n]++] = (uint32_t)(8 * e + i);
                 if (c->hc_index[e] >= 0) hc_slot[ch[n]++] = (uint32_t)(8 * c->hc_index[e] + i);
             }
@@ -311,40 +389,39 @@ int create_impl(const crush_model_desc* d, int device, crush_ctx* c) {
 
     int st;
 #define TRY(x) do { st = (x); if (st != CRUSH_OK) return st; } while (0)
-    TRY(c->upload(&c->pos, d->positions, 3 * N));
-    TRY(c->upload(&c->conn_all, d->hexes, 8 * E));
-    TRY(c->upload(&c->part, d->hex_part, E));
-    TRY(c->upload(&c->mat3, mat3.data(), mat3.size()));
-    TRY(c->upload(&c->mats, mats.data(), mats.size()));
+    TRY(c->upload(&c->pos, cm.positions.data(), 3 * N));
+    TRY(c->upload(&c->conn_all, cm.hexes.data(), 8 * E));
+    TRY(c->upload(&c->part, cm.hex_part.data(), E));
+    TRY(c->upload(&c->mat4, cm.mat4.data(), cm.mat4.size()));
+    TRY(c->upload(&c->mats, cm.mats.data(), cm.mats.size()));
     TRY(c->upload(&c->hc_index_d, c->hc_index.data(), E));
-    TRY(c->upload(&c->fixed, fixed.data(), N));
+    TRY(c->upload(&c->fixed, cm.fixed.data(), N));
+    TRY(c->upload(&c->node_slot, cm.node_slot.data(), N));
+    TRY(c->upload(&c->elem_slot, cm.elem_slot.data(), E));
     TRY(c->upload(&c->all_off, all_off.data(), N + 1));
     TRY(c->upload(&c->all_slot, all_slot.data(), all_slot.size()));
     TRY(c->upload(&c->hc_off, hc_off.data(), N + 1));
     TRY(c->upload(&c->hc_slot, hc_slot.data(), hc_slot.size()));
-    std::vector<double> v0(3 * N, 0.0);
-    if (d->initial_velocity) std::copy(d->initial_velocity, d->initial_velocity + 3 * N, v0.begin());
-    TRY(c->upload(&c->v0, v0.data(), 3 * N));
+    TRY(c->upload(&c->v0, cm.v0.data(), 3 * N));
     for (double** p : {&c->u, &c->v, &c->v_half, &c->f_int, &c->f_ext, &c->u_tmp, &c->f_tmp}) TRY(c->alloc(p, 3 * N));
     for (double** p : {&c->inv_mass, &c->mass, &c->added, &c->n_tmp, &c->n_tmp2}) TRY(c->alloc(p, N));
     for (double** p : {&c->volume, &c->dt_factor, &c->elem_mass, &c->elem_dt, &c->elem_extra, &c->e_tmp}) TRY(c->alloc(p, E));
     TRY(c->alloc(&c->lumped, 8 * E));
     TRY(c->alloc(&c->eroded_all, E));
-    c->dt_blocks = elem_dt_blocks(E);
-    TRY(c->alloc(&c->dt_partials, c->dt_blocks));
     TRY(c->alloc(&c->planes, (size_t)N_STATIC_PLANES * c->stride));
     TRY(c->alloc(&c->state, (size_t)N_STATE_PLANES * c->stride));
     TRY(c->alloc(&c->corner, (size_t)24 * std::max<long long>(c->n_hc, 1)));
-    TRY(c->alloc(&c->ctl, 1));
-    TRY(c->alloc(&c->ctl_aux, 1));
+    TRY(c->alloc(&c->ctls, c->n_slots));
+    TRY(c->alloc(&c->ctls_aux, c->n_slots));
     CK(cudaMemsetAsync(c->planes, 0, sizeof(float4) * N_STATIC_PLANES * c->stride, c->stream));
     CK(cudaMemsetAsync(c->eroded_all, 0, E, c->stream));
+    CK(cudaMemsetAsync(c->ctls, 0, sizeof(Control) * c->n_slots, c->stream));
 
     // Device set-up geometry (HexGeometry::new for every element).
     int* bad = nullptr;
     TRY(c->alloc(&bad, 1));
     CK(cudaMemsetAsync(bad, 0, sizeof(int), c->stream));
-    launch_setup_geometry(c->stream, E, c->pos, c->conn_all, c->part, c->mat3, s.hourglass, c->hc_index_d, c->stride, c->planes,
+    launch_setup_geometry(c->stream, E, c->pos, c->conn_all, c->part, c->mat4, c->hc_index_d, c->elem_slot, c->stride, c->planes,
                           c->volume, c->lumped, c->dt_factor, c->elem_mass, bad);
     TRY(check_launch(c));
     launch_node_masses(c->stream, N, c->all_off, c->all_slot, c->lumped, c->mass, c->inv_mass);
@@ -358,108 +435,124 @@ int create_impl(const crush_model_desc* d, int device, crush_ctx* c) {
     if (bad_h == 2) return crush::fail(CRUSH_ERR_INVALID, "hourglass modes not independent");
 
     // ---- contacts (ContactRuntime::new, src/contact.rs:48-70) ----
-    c->n_contacts = d->n_contacts;
-    std::vector<int> face_off(1, 0), slave_off(1, 0), tab_off(1, 0), counts_for_stop;
+    std::vector<int> face_off(1, 0), slave_off(1, 0), tab_off(1, 0), counts_for_stop, face_contact, slave_contact, contact_slot;
+    std::vector<int> slot_contact_off(1, 0);
     std::vector<uint32_t> faces, slaves;
     std::vector<double> scales, stiff, md, cell;
-    // roles per node: contact, position among the contact's primary nodes
-    // (-1: none), and the contact's faces that contain the node
     struct Role {
         int c;
         int slave;
         std::vector<int> faces;
     };
     std::map<uint32_t, std::vector<Role>> roles;
-    for (int k = 0; k < d->n_contacts; ++k) {
-        const crush_contact& cd = d->contacts[k];
-        if (cd.n_nodes < 0 || cd.n_faces < 0 || (cd.n_nodes > 0 && !cd.nodes) || (cd.n_faces > 0 && !cd.faces))
-            return crush::fail(CRUSH_ERR_INVALID, "invalid contact " + std::to_string(k));
-        if (!(cd.max_distance >= 0.0) || !(cd.stiffness >= 0.0)) return crush::fail(CRUSH_ERR_INVALID, "invalid contact parameters");
-        double lo[3] = {INF, INF, INF}, hi[3] = {-INF, -INF, -INF};
-        bool stop = false;
-        double ext = 0.0;
-        std::vector<std::array<double, 6>> keys;  // grid key box of each face at the reference positions
-        for (int64_t f = 0; f < cd.n_faces; ++f) {
-            double flo[3] = {INF, INF, INF}, fhi[3] = {-INF, -INF, -INF};
-            double xs[4][3];
-            for (int j = 0; j < 4; ++j) {
-                uint32_t n = cd.faces[4 * f + j];
-                if (n >= (uint64_t)N) return crush::fail(CRUSH_ERR_INVALID, "contact face node out of range");
-                faces.push_back(n);
-                if (!fixed[n]) stop = true;
-                for (int dd = 0; dd < 3; ++dd) {
-                    double p = d->positions[3 * n + dd];
-                    xs[j][dd] = p;
-                    lo[dd] = std::fmin(lo[dd], p);
-                    hi[dd] = std::fmax(hi[dd], p);
-                    flo[dd] = std::fmin(flo[dd], p);
-                    fhi[dd] = std::fmax(fhi[dd], p);
+    int kc = 0;
+    for (int sidx = 0; sidx < n_desc; ++sidx) {
+        const crush_model_desc* d = descs[sidx];
+        const long long n0 = c->slots[sidx].node0;
+        c->slots[sidx].contact0 = kc;
+        c->slots[sidx].n_contacts = d->n_contacts;
+        for (int k = 0; k < d->n_contacts; ++k, ++kc) {
+            const crush_contact& cd = d->contacts[k];
+            if (cd.n_nodes < 0 || cd.n_faces < 0 || (cd.n_nodes > 0 && !cd.nodes) || (cd.n_faces > 0 && !cd.faces))
+                return crush::fail(CRUSH_ERR_INVALID, "invalid contact " + std::to_string(k));
+            if (!(cd.max_distance >= 0.0) || !(cd.stiffness >= 0.0)) return crush::fail(CRUSH_ERR_INVALID, "invalid contact parameters");
+            double lo[3] = {INF, INF, INF}, hi[3] = {-INF, -INF, -INF};
+            bool stop = false;
+            double ext = 0.0;
+            std::vector<std::array<double, 6>> keys;  // grid key box of each face at the reference positions
+            for (int64_t f = 0; f < cd.n_faces; ++f) {
+                double flo[3] = {INF, INF, INF}, fhi[3] = {-INF, -INF, -INF};
+                double xs[4][3];
+                for (int j = 0; j < 4; ++j) {
+                    uint32_t nl = cd.faces[4 * f + j];
+                    if (nl >= (uint64_t)d->n_nodes) return crush::fail(CRUSH_ERR_INVALID, "contact face node out of range");
+                    uint32_t n = (uint32_t)(n0 + nl);
+                    faces.push_back(n);
+                    if (!cm.fixed[n]) stop = true;
+                    for (int dd = 0; dd < 3; ++dd) {
+                        double p = cm.positions[3 * (size_t)n + dd];
+                        xs[j][dd] = p;
+                        lo[dd] = std::fmin(lo[dd], p);
+                        hi[dd] = std::fmax(hi[dd], p);
+                        flo[dd] = std::fmin(flo[dd], p);
+                        fhi[dd] = std::fmax(fhi[dd], p);
+                    }
                 }
+                face_contact.push_back(kc);
+                double fext = std::max({fhi[0] - flo[0], fhi[1] - flo[1], fhi[2] - flo[2]});
+                ext = std::max(ext, fext);
+                double e1[3], e2[3], nrm[3];
+                for (int dd = 0; dd < 3; ++dd) { e1[dd] = xs[1][dd] - xs[0][dd]; e2[dd] = xs[2][dd] - xs[0][dd]; }
+                nrm[0] = e1[1] * e2[2] - e1[2] * e2[1];
+                nrm[1] = e1[2] * e2[0] - e1[0] * e2[2];
+                nrm[2] = e1[0] * e2[1] - e1[1] * e2[0];
+                double len = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+                std::array<double, 6> kb;
+                for (int dd = 0; dd < 3; ++dd) {
+                    double nd = len > 0.0 ? nrm[dd] / len : 0.0;
+                    kb[dd] = flo[dd] - 0.25 * fext - cd.max_distance * std::max(nd, 0.0);
+                    kb[3 + dd] = fhi[dd] + 0.25 * fext + cd.max_distance * std::max(-nd, 0.0);
+                }
+                keys.push_back(kb);
             }
-            double fext = std::max({fhi[0] - flo[0], fhi[1] - flo[1], fhi[2] - flo[2]});
-            ext = std::max(ext, fext);
-            double e1[3], e2[3], nrm[3];
-            for (int dd = 0; dd < 3; ++dd) { e1[dd] = xs[1][dd] - xs[0][dd]; e2[dd] = xs[2][dd] - xs[0][dd]; }
-            nrm[0] = e1[1] * e2[2] - e1[2] * e2[1];
-            nrm[1] = e1[2] * e2[0] - e1[0] * e2[2];
-            nrm[2] = e1[0] * e2[1] - e1[1] * e2[0];
-            double len = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
-            std::array<double, 6> kb;
-            for (int dd = 0; dd < 3; ++dd) {
-                double nd = len > 0.0 ? nrm[dd] / len : 0.0;
-                kb[dd] = flo[dd] - 0.25 * fext - cd.max_distance * std::max(nd, 0.0);
-                kb[3 + dd] = fhi[dd] + 0.25 * fext + cd.max_distance * std::max(-nd, 0.0);
+            for (int dd = 0; dd < 3; ++dd) { lo[dd] += -cd.max_distance; hi[dd] += cd.max_distance; }
+            std::vector<uint32_t> all_nodes;
+            int kept = 0;
+            for (int64_t i = 0; i < cd.n_nodes; ++i) {
+                uint32_t nl = cd.nodes[i];
+                if (nl >= (uint64_t)d->n_nodes) return crush::fail(CRUSH_ERR_INVALID, "contact node out of range");
+                uint32_t n = (uint32_t)(n0 + nl);
+                all_nodes.push_back(n);
+                bool inside = true;
+                for (int dd = 0; dd < 3; ++dd) {
+                    double p = cm.positions[3 * (size_t)n + dd];
+                    if (!(p >= lo[dd] && p <= hi[dd])) inside = false;
+                }
+                if (!inside) continue;
+                slaves.push_back(n);
+                slave_contact.push_back(kc);
+                scales.push_back(cd.node_scale ? cd.node_scale[i] : 1.0);
+                roles[n].push_back(Role{kc, kept, {}});
+                ++kept;
             }
-            keys.push_back(kb);
+            for (int64_t f = 0; f < cd.n_faces; ++f)
+                for (int j = 0; j < 4; ++j) {
+                    uint32_t n = (uint32_t)(n0 + cd.faces[4 * f + j]);
+                    auto& r = roles[n];
+                    if (r.empty() || r.back().c != kc) r.push_back(Role{kc, -1, {}});
+                    if (r.back().faces.empty() || r.back().faces.back() != (int)f) r.back().faces.push_back((int)f);
+                }
+            c->contact_nodes_all.push_back(all_nodes);
+            c->contact_stiffness.push_back(cd.stiffness);
+            face_off.push_back(face_off.back() + (int)cd.n_faces);
+            slave_off.push_back(slave_off.back() + kept);
+            // Grid cell: twice the largest face; table: twice the initial key-box
+            // cell count, a power of two. Small contacts get no grid.
+            const double cs = ext > 0.0 ? 2.0 * ext : 1.0;
+            size_t t = 0;
+            if (cd.n_faces >= GRID_MIN_FACES) {
+                size_t inserts = 0;
+                for (const auto& kb : keys) {
+                    size_t cells = 1;
+                    for (int dd = 0; dd < 3; ++dd) cells *= (size_t)(std::floor(kb[3 + dd] / cs) - std::floor(kb[dd] / cs) + 1.0);
+                    inserts += std::min<size_t>(cells, 1024);
+                }
+                t = next_pow2(std::max<size_t>(1024, 2 * inserts));
+            }
+            tab_off.push_back(tab_off.back() + (int)t);
+            stiff.push_back(cd.stiffness);
+            md.push_back(cd.max_distance);
+            cell.push_back(cs);
+            counts_for_stop.push_back(stop ? 1 : 0);
+            contact_slot.push_back(sidx);
         }
-        for (int dd = 0; dd < 3; ++dd) { lo[dd] += -cd.max_distance; hi[dd] += cd.max_distance; }
-        std::vector<uint32_t> all_nodes;
-        int kept = 0;
-        for (int64_t i = 0; i < cd.n_nodes; ++i) {
-            uint32_t n = cd.nodes[i];
-            if (n >= (uint64_t)N) return crush::fail(CRUSH_ERR_INVALID, "contact node out of range");
-            all_nodes.push_back(n);
-            bool inside = true;
-            for (int dd = 0; dd < 3; ++dd) {
-                double p = d->positions[3 * n + dd];
-                if (!(p >= lo[dd] && p <= hi[dd])) inside = false;
-            }
-            if (!inside) continue;
-            slaves.push_back(n);
-            scales.push_back(cd.node_scale ? cd.node_scale[i] : 1.0);
-            roles[n].push_back(Role{k, kept, {}});
-            ++kept;
-        }
-        for (int64_t f = 0; f < cd.n_faces; ++f)
-            for (int j = 0; j < 4; ++j) {
-                uint32_t n = cd.faces[4 * f + j];
-                auto& r = roles[n];
-                if (r.empty() || r.back().c != k) r.push_back(Role{k, -1, {}});
-                if (r.back().faces.empty() || r.back().faces.back() != (int)f) r.back().faces.push_back((int)f);
-            }
-        c->contact_nodes_all.push_back(all_nodes);
-        c->contact_stiffness.push_back(cd.stiffness);
-        face_off.push_back(face_off.back() + (int)cd.n_faces);
-        slave_off.push_back(slave_off.back() + kept);
-        // Grid cell: twice the largest face; table: twice the initial key-box
-        // cell count, a power of two.
-        const double cs = ext > 0.0 ? 2.0 * ext : 1.0;
-        size_t inserts = 0;
-        for (const auto& kb : keys) {
-            size_t cells = 1;
-            for (int dd = 0; dd < 3; ++dd) cells *= (size_t)(std::floor(kb[3 + dd] / cs) - std::floor(kb[dd] / cs) + 1.0);
-            inserts += std::min<size_t>(cells, 128);
-        }
-        size_t t = next_pow2(std::max<size_t>(1024, 2 * inserts));
-        tab_off.push_back(tab_off.back() + (int)t);
-        stiff.push_back(cd.stiffness);
-        md.push_back(cd.max_distance);
-        cell.push_back(cs);
-        counts_for_stop.push_back(stop ? 1 : 0);
+        slot_contact_off.push_back(kc);
     }
+    c->n_contacts = kc;
     c->n_faces = face_off.back();
     c->n_slaves = slave_off.back();
-    c->entries_cap = 0;
+    c->face_off_h = face_off;
+    c->slave_off_h = slave_off;
     std::vector<uint32_t> cnode, cnode_off(1, 0);
     std::vector<int> crole_contact, crole_slave, crole_faces;
     std::vector<uint8_t> crole_face;
@@ -477,125 +570,149 @@ int create_impl(const crush_model_desc* d, int device, crush_ctx* c) {
     }
     ContactArrays& ca = c->ca;
     ca.n_contacts = c->n_contacts;
-    int nc1 = c->n_contacts + 1;
-    TRY(c->upload(const_cast<int**>(&ca.face_off), face_off.data(), nc1));
-    TRY(c->upload(const_cast<uint32_t**>(&ca.faces), faces.data(), faces.size()));
+    ca.n_slots = c->n_slots;
+    TRY(c->upload_const(&ca.face_off, face_off));
+    TRY(c->upload_const(&ca.faces, faces));
     TRY(c->alloc(&ca.geo, std::max<long long>(c->n_faces, 1)));
-    TRY(c->upload(const_cast<int**>(&ca.slave_off), slave_off.data(), nc1));
-    TRY(c->upload(const_cast<uint32_t**>(&ca.slaves), slaves.data(), slaves.size()));
-    TRY(c->upload(const_cast<double**>(&ca.slave_scale), scales.data(), scales.size()));
+    TRY(c->upload_const(&ca.slave_off, slave_off));
+    TRY(c->upload_const(&ca.slaves, slaves));
+    TRY(c->upload_const(&ca.slave_scale, scales));
     TRY(c->alloc(&ca.hit, std::max<long long>(c->n_slaves, 1)));
     TRY(c->alloc(&ca.hit_force, 3 * std::max<long long>(c->n_slaves, 1)));
-    TRY(c->upload(const_cast<double**>(&ca.stiffness), stiff.data(), stiff.size()));
-    TRY(c->upload(const_cast<double**>(&ca.max_distance), md.data(), md.size()));
-    TRY(c->upload(const_cast<double**>(&ca.cell), cell.data(), cell.size()));
-    TRY(c->upload(const_cast<int**>(&ca.tab_off), tab_off.data(), nc1));
+    TRY(c->upload_const(&ca.stiffness, stiff));
+    TRY(c->upload_const(&ca.max_distance, md));
+    TRY(c->upload_const(&ca.cell, cell));
+    TRY(c->upload_const(&ca.tab_off, tab_off));
     TRY(c->alloc(&ca.counts, std::max(tab_off.back(), 1)));
     TRY(c->alloc(&ca.entries, (size_t)std::max(tab_off.back(), 1) * BUCKET_CAP));
-    ca.overflow_cap = (int)std::max<long long>(1, face_off.empty() ? 1 : *std::max_element(face_off.begin(), face_off.end()));
     {
         int cap = 1;
         for (int k = 0; k < c->n_contacts; ++k) cap = std::max(cap, face_off[k + 1] - face_off[k]);
         ca.overflow_cap = cap;
+        // Overflow lists exist only for contacts with a grid.
+        size_t grid_contacts = 0;
+        for (int k = 0; k < c->n_contacts; ++k) grid_contacts += tab_off[k + 1] > tab_off[k];
+        if (grid_contacts == 0) ca.overflow_cap = 1;
     }
     TRY(c->alloc(&ca.overflow, (size_t)std::max(c->n_contacts, 1) * ca.overflow_cap));
     TRY(c->alloc(&ca.n_overflow, std::max(c->n_contacts, 1)));
     TRY(c->alloc(&ca.entry_overrun, std::max(c->n_contacts, 1)));
     TRY(c->alloc(&ca.pen_count, std::max(c->n_contacts, 1)));
     TRY(c->alloc(&ca.pen_max_bits, std::max(c->n_contacts, 1)));
-    TRY(c->upload(const_cast<int**>(&ca.counts_for_stop), counts_for_stop.data(), counts_for_stop.size()));
+    TRY(c->upload_const(&ca.counts_for_stop, counts_for_stop));
     ca.n_cnodes = (long long)cnode.size();
-    TRY(c->upload(const_cast<uint32_t**>(&ca.cnode), cnode.data(), cnode.size()));
-    TRY(c->upload(const_cast<uint32_t**>(&ca.cnode_off), cnode_off.data(), cnode_off.size()));
-    TRY(c->upload(const_cast<int**>(&ca.crole_contact), crole_contact.data(), crole_contact.size()));
-    TRY(c->upload(const_cast<int**>(&ca.crole_slave), crole_slave.data(), crole_slave.size()));
-    TRY(c->upload(const_cast<uint8_t**>(&ca.crole_face), crole_face.data(), crole_face.size()));
-    TRY(c->upload(const_cast<uint32_t**>(&ca.crole_faces_off), crole_faces_off.data(), crole_faces_off.size()));
-    TRY(c->upload(const_cast<int**>(&ca.crole_faces), crole_faces.data(), crole_faces.size()));
+    TRY(c->upload_const(&ca.cnode, cnode));
+    TRY(c->upload_const(&ca.cnode_off, cnode_off));
+    TRY(c->upload_const(&ca.crole_contact, crole_contact));
+    TRY(c->upload_const(&ca.crole_slave, crole_slave));
+    TRY(c->upload_const(&ca.crole_face, crole_face));
+    TRY(c->upload_const(&ca.crole_faces_off, crole_faces_off));
+    TRY(c->upload_const(&ca.crole_faces, crole_faces));
     TRY(c->alloc(&ca.face_hits, std::max<long long>(c->n_faces, 1)));
     TRY(c->alloc(&ca.face_list, (size_t)std::max<long long>(c->n_faces, 1) * FACE_HIT_CAP));
-    CK(cudaMemsetAsync(ca.face_hits, 0, sizeof(int) * std::max<long long>(c->n_faces, 1), c->stream));
+    TRY(c->upload_const(&ca.face_contact, face_contact));
+    TRY(c->upload_const(&ca.slave_contact, slave_contact));
+    TRY(c->upload_const(&ca.contact_slot, contact_slot));
+    TRY(c->upload_const(&ca.slot_contact_off, slot_contact_off));
     CK(cudaMemsetAsync(ca.counts, 0, sizeof(int) * std::max(tab_off.back(), 1), c->stream));
     CK(cudaMemsetAsync(ca.n_overflow, 0, sizeof(int) * std::max(c->n_contacts, 1), c->stream));
     CK(cudaMemsetAsync(ca.entry_overrun, 0, sizeof(int) * std::max(c->n_contacts, 1), c->stream));
     CK(cudaMemsetAsync(ca.pen_count, 0, sizeof(unsigned long long) * std::max(c->n_contacts, 1), c->stream));
     CK(cudaMemsetAsync(ca.pen_max_bits, 0, sizeof(unsigned long long) * std::max(c->n_contacts, 1), c->stream));
+    CK(cudaMemsetAsync(ca.face_hits, 0, sizeof(int) * std::max<long long>(c->n_faces, 1), c->stream));
 
     // ---- vehicles ----
-    c->n_veh = std::min(d->n_vehicles, 4);
     std::vector<long long> voff(1, 0);
     std::vector<uint32_t> vnodes;
-    for (int k = 0; k < c->n_veh; ++k) {
-        const crush_vehicle& vd = d->vehicles[k];
-        for (int64_t i = 0; i < vd.n_nodes; ++i) {
-            if (vd.nodes[i] >= (uint64_t)N) return crush::fail(CRUSH_ERR_INVALID, "vehicle node out of range");
-            vnodes.push_back(vd.nodes[i]);
+    std::vector<int> vslot, vlocal;
+    long long max_vnodes = 0;
+    for (int sidx = 0; sidx < n_desc; ++sidx) {
+        const crush_model_desc* d = descs[sidx];
+        const long long n0 = c->slots[sidx].node0;
+        c->slots[sidx].vehicle0 = (int)vslot.size();
+        int nv = std::min(d->n_vehicles, 4);
+        c->slots[sidx].n_vehicles = nv;
+        for (int k = 0; k < nv; ++k) {
+            const crush_vehicle& vd = d->vehicles[k];
+            for (int64_t i = 0; i < vd.n_nodes; ++i) {
+                if (vd.nodes[i] >= (uint64_t)d->n_nodes) return crush::fail(CRUSH_ERR_INVALID, "vehicle node out of range");
+                vnodes.push_back((uint32_t)(n0 + vd.nodes[i]));
+            }
+            max_vnodes = std::max<long long>(max_vnodes, vd.n_nodes);
+            voff.push_back((long long)vnodes.size());
+            if (vd.accel_node >= (uint64_t)d->n_nodes) return crush::fail(CRUSH_ERR_INVALID, "accelerometer node out of range");
+            c->veh_accel.push_back((uint32_t)(n0 + vd.accel_node));
+            std::vector<uint32_t> fr;
+            for (int64_t i = 0; i < vd.n_front; ++i) {
+                if (vd.front_nodes[i] >= (uint64_t)d->n_nodes) return crush::fail(CRUSH_ERR_INVALID, "front node out of range");
+                fr.push_back((uint32_t)(n0 + vd.front_nodes[i]));
+            }
+            c->veh_front.push_back(fr);
+            vslot.push_back(sidx);
+            vlocal.push_back(k);
         }
-        voff.push_back((long long)vnodes.size());
-        if (vd.accel_node >= (uint64_t)N) return crush::fail(CRUSH_ERR_INVALID, "accelerometer node out of range");
-        c->veh_accel.push_back(vd.accel_node);
-        std::vector<uint32_t> fr(vd.front_nodes, vd.front_nodes + vd.n_front);
-        for (uint32_t n : fr)
-            if (n >= (uint64_t)N) return crush::fail(CRUSH_ERR_INVALID, "front node out of range");
-        c->veh_front.push_back(fr);
     }
-    TRY(c->upload(&c->veh_off, voff.data(), voff.size()));
-    TRY(c->upload(&c->veh_nodes, vnodes.data(), vnodes.size()));
-    TRY(c->alloc(&c->veh_out, 7 * 4));
+    VehicleArrays& va = c->va;
+    va.n_vehicles = (int)vslot.size();
+    va.vx_blocks = (int)std::min<long long>(VX_BLOCKS, std::max<long long>(1, (max_vnodes + 2047) / 2048));
+    TRY(c->upload_const(&va.off, voff));
+    TRY(c->upload_const(&va.nodes, vnodes));
+    TRY(c->upload_const(&va.slot, vslot));
+    TRY(c->upload_const(&va.local, vlocal));
+    TRY(c->alloc(&c->veh_out, 7 * std::max(va.n_vehicles, 1)));
 
-    // ---- time step (src/solver.rs:214-228) ----
-    for (size_t k = 0; k < c->contact_nodes_all.size(); ++k)
-        for (uint32_t n : c->contact_nodes_all[k])
-            if (mass_h[n] > 0.0 && c->contact_stiffness[k] > 0.0)
-                c->contact_dt = std::fmin(c->contact_dt, 2.0 * std::sqrt(mass_h[n] / c->contact_stiffness[k]));
+    // ---- time step per slot (src/solver.rs:214-228) ----
+    for (int sidx = 0; sidx < n_desc; ++sidx) {
+        Slot& sl = c->slots[sidx];
+        for (int k = sl.contact0; k < sl.contact0 + sl.n_contacts; ++k)
+            for (uint32_t n : c->contact_nodes_all[k])
+                if (mass_h[n] > 0.0 && c->contact_stiffness[k] > 0.0)
+                    sl.contact_dt = std::fmin(sl.contact_dt, 2.0 * std::sqrt(mass_h[n] / c->contact_stiffness[k]));
+    }
     launch_init_state(c->stream, c->n_hc, c->stride, c->state);
     TRY(check_launch(c));
     CK(cudaMemsetAsync(c->u_tmp, 0, sizeof(double) * 3 * N, c->stream));
-    Control aux{};
-    aux.dt_stable_bits = 0x7ff0000000000000ull;
-    aux.dt_floor = 0.0;
-    CK(cudaMemcpyAsync(c->ctl_aux, &aux, sizeof(Control), cudaMemcpyHostToDevice, c->stream));
-    launch_elem_dt(c->stream, c->el(), c->nd(), c->ctl_aux, c->u_tmp, c->dt_partials, 0);
+    std::vector<Control> aux(c->n_slots);
+    std::memset(aux.data(), 0, sizeof(Control) * aux.size());
+    for (Control& a : aux) a.dt_stable_bits = INF_BITS;
+    CK(cudaMemcpyAsync(c->ctls_aux, aux.data(), sizeof(Control) * aux.size(), cudaMemcpyHostToDevice, c->stream));
+    launch_elem_dt(c->stream, c->el(), c->nd(), c->ctls_aux, c->u_tmp, 0);
     TRY(check_launch(c));
-    CK(cudaMemcpyAsync(&aux, c->ctl_aux, sizeof(Control), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(aux.data(), c->ctls_aux, sizeof(Control) * aux.size(), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    double stable;
-    std::memcpy(&stable, &aux.dt_stable_bits, sizeof(double));
-    if (!std::isfinite(stable)) {
-        static const int EDGES[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6}, {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
-        double mn = INF, cmax = 0.0;
-        for (long long e = 0; e < E; ++e) {
-            cmax = std::fmax(cmax, wave_speed(d->materials[d->hex_part[e]]));
-            for (auto& ed : EDGES) {
-                const double* p = d->positions + 3 * d->hexes[8 * e + ed[0]];
-                const double* q = d->positions + 3 * d->hexes[8 * e + ed[1]];
-                mn = std::fmin(mn, std::sqrt((p[0] - q[0]) * (p[0] - q[0]) + (p[1] - q[1]) * (p[1] - q[1]) + (p[2] - q[2]) * (p[2] - q[2])));
+    for (int sidx = 0; sidx < n_desc; ++sidx) {
+        Slot& sl = c->slots[sidx];
+        double stable;
+        std::memcpy(&stable, &aux[sidx].dt_stable_bits, sizeof(double));
+        if (!std::isfinite(stable)) {
+            static const int EDGES[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6}, {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+            double mn = INF, cmax = 0.0;
+            for (long long e = sl.elem0; e < sl.elem0 + sl.n_elems; ++e) {
+                cmax = std::fmax(cmax, wave_speed(cm.materials[cm.hex_part[e]]));
+                for (auto& ed : EDGES) {
+                    const double* p = &cm.positions[3 * (size_t)cm.hexes[8 * e + ed[0]]];
+                    const double* q = &cm.positions[3 * (size_t)cm.hexes[8 * e + ed[1]]];
+                    mn = std::fmin(mn, std::sqrt((p[0] - q[0]) * (p[0] - q[0]) + (p[1] - q[1]) * (p[1] - q[1]) + (p[2] - q[2]) * (p[2] - q[2])));
+                }
             }
+            stable = mn / (std::sqrt(3.0) * cmax);
         }
-        stable = mn / (std::sqrt(3.0) * cmax);
+        sl.stable = std::fmin(stable, sl.contact_dt);
+        sl.dt_floor = sl.settings.mass_scaling > 0.0 ? sl.settings.mass_scaling * sl.stable : 0.0;
+        sl.dt0 = sl.settings.time_step > 0.0 ? sl.settings.time_step : sl.stable * sl.settings.dt_scale;
     }
-    c->stable = std::fmin(stable, c->contact_dt);
-    c->dt_floor = s.mass_scaling > 0.0 ? s.mass_scaling * c->stable : 0.0;
-    c->dt0 = s.time_step > 0.0 ? s.time_step : c->stable * s.dt_scale;
-    int chk = s.adaptive_check_steps > 0 ? s.adaptive_check_steps : 1;
-    c->period = std::lcm(chk, 20);
+    c->period = std::lcm(c->check_steps, 20);
     if (c->period > 200) c->period = 0;  // no graph for odd periods
     return CRUSH_OK;
 #undef TRY
 }
 
-int sync(crush_ctx* c) {
-    CK(cudaStreamSynchronize(c->stream));
-    return CRUSH_OK;
-}
-
-// One explicit step on the stream (src/solver.rs:287-345).
+// One explicit step of every slot on the stream (src/solver.rs:287-345).
 // Phase boundaries of one step recorded when profiling: start, after dt,
 // after contact, after half step, after element forces, after full step, end.
 constexpr int N_PHASE_EVENTS = 7;
 
 int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool capturing = false) {
-    const crush_settings& s = c->settings;
     ElementArrays el = c->el();
     NodeArrays nd = c->nd();
     int n = 0;
@@ -608,36 +725,35 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
         else cudaEventRecord(ev[i], c->stream);
     };
     mark(0);
-    const bool adaptive = !(s.time_step > 0.0) && s.adaptive_check_steps > 0;
-    if (adaptive && step % s.adaptive_check_steps == 0) {
-        launch_elem_dt(c->stream, el, nd, c->ctl, c->u, c->dt_partials, 1);
-        launch_dt_finalize(c->stream, c->ctl, c->dt_partials, c->dt_blocks);
-        launch_mass_scaling(c->stream, el, nd, c->ctl, 0);
+    if (c->adaptive && step % c->check_steps == 0) {
+        launch_elem_dt(c->stream, el, nd, c->ctls, c->u, 1);
+        launch_dt_finalize(c->stream, c->ctls, c->n_slots);
+        launch_mass_scaling(c->stream, el, nd, c->ctls, 0);
         n += 3;
     }
     mark(1);
     if (c->n_contacts > 0) {
-        launch_contact(c->stream, c->ca, nd, c->ctl, 0, c->n_contacts, c->n_faces, c->n_slaves, c->entries_cap, 0.0, c->mass, c->f_ext, 1);
+        launch_contact(c->stream, c->ca, nd, c->ctls, 0, c->n_contacts, c->n_faces, c->n_slaves, 0.0, c->mass, c->f_ext, 1);
         n += (c->n_faces > 0 ? 1 : 0) + (c->n_slaves > 0 ? 1 : 0) + 1;
     }
     mark(2);
-    launch_half(c->stream, nd, c->ctl);
+    launch_half(c->stream, nd, c->ctls);
     mark(3);
-    launch_forces(c->stream, el, nd, c->ctl, 1);
+    launch_forces(c->stream, el, nd, c->ctls, 1);
     mark(4);
-    launch_full(c->stream, el, nd, c->ctl);
+    launch_full(c->stream, el, nd, c->ctls);
     mark(5);
     n += 2 + (c->n_hc > 0 ? 1 : 0);
     if ((step + 1) % 20 == 0) {
-        launch_nonfinite(c->stream, nd, c->ctl);
+        launch_nonfinite(c->stream, nd, c->ctls);
         ++n;
     }
-    const bool sep = s.stop_rule == CRUSH_STOP_SEPARATION && (step + 1) % 10 == 0 && c->n_veh >= 2;
+    const bool sep = c->any_separation && (step + 1) % 10 == 0 && c->va.n_vehicles > 0;
     if (sep) {
-        launch_vehicle_vx(c->stream, c->n_veh, c->veh_off, c->veh_nodes, c->mass, c->v, c->ctl);
+        launch_vehicle_vx(c->stream, c->va, c->mass, c->v, c->ctls);
         ++n;
     }
-    launch_step_end(c->stream, c->ctl, c->ca, sep ? 1 : 0);
+    launch_step_end(c->stream, c->ctls, c->ca, c->va, sep ? 1 : 0);
     ++n;
     mark(6);
     return check_launch(c, n);
@@ -659,30 +775,34 @@ int run_begin(crush_ctx* c) {
     launch_node_masses(c->stream, N, c->all_off, c->all_slot, c->lumped, c->mass, c->inv_mass);
     int st = check_launch(c, 2);
     if (st != CRUSH_OK) return st;
-    Control h{};
-    h.t = 0.0;
-    h.end_time = c->settings.end_time;
-    h.dt_cfl = c->dt0;
-    h.dt_min = INF;
-    h.dt_floor = c->dt_floor;
-    h.dt_scale = c->settings.dt_scale;
-    h.contact_dt = c->contact_dt;
-    h.damping = c->settings.velocity_damping;
-    h.dt_stable_bits = 0x7ff0000000000000ull;
-    h.step = 0;
-    h.last_hit = -1;
-    h.max_steps = c->settings.max_steps;
-    h.done = (0.0 < c->settings.end_time) ? 0 : 1;
-    h.stop_rule = c->settings.stop_rule;
-    CK(cudaMemcpyAsync(c->ctl, &h, sizeof(Control), cudaMemcpyHostToDevice, c->stream));
+    std::vector<Control> h(c->n_slots);
+    std::memset(h.data(), 0, sizeof(Control) * h.size());
+    for (int k = 0; k < c->n_slots; ++k) {
+        const Slot& sl = c->slots[k];
+        Control& x = h[k];
+        x.t = 0.0;
+        x.end_time = sl.settings.end_time;
+        x.dt_cfl = sl.dt0;
+        x.dt_min = INF;
+        x.dt_floor = sl.dt_floor;
+        x.dt_scale = sl.settings.dt_scale;
+        x.contact_dt = sl.contact_dt;
+        x.damping = sl.settings.velocity_damping;
+        x.dt_stable_bits = INF_BITS;
+        x.step = 0;
+        x.last_hit = -1;
+        x.max_steps = sl.settings.max_steps;
+        x.done = (0.0 < sl.settings.end_time) ? 0 : 1;
+        x.stop_rule = sl.settings.stop_rule;
+    }
+    CK(cudaMemcpyAsync(c->ctls, h.data(), sizeof(Control) * h.size(), cudaMemcpyHostToDevice, c->stream));
     // Initial internal forces at u = 0 (src/solver.rs:254); the count of
     // elements it erodes is not added to the run's total (as there).
-    launch_forces(c->stream, c->el(), c->nd(), c->ctl, 0);
+    launch_forces(c->stream, c->el(), c->nd(), c->ctls, 0);
     launch_gather(c->stream, c->el(), c->nd(), c->f_int);
-    st = check_launch(c, 2);
+    st = check_launch(c, (c->n_hc > 0 ? 1 : 0) + 1);
     if (st != CRUSH_OK) return st;
-    long long zero = 0;
-    CK(cudaMemcpyAsync(&c->ctl->eroded_step, &zero, sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->ctls, h.data(), sizeof(Control) * h.size(), cudaMemcpyHostToDevice, c->stream));
     c->host_step = 0;
     c->run_open = true;
     return sync(c);
@@ -717,12 +837,14 @@ int build_graph(crush_ctx* c) {
     return CRUSH_OK;
 }
 
-int run_steps(crush_ctx* c, long long n_steps, int* done) {
+// Issue n_steps steps (graphs where the step index is on a period boundary).
+int issue_steps(crush_ctx* c, long long n_steps) {
     if (!c->run_open) return crush::fail(CRUSH_ERR_INVALID, "no open run (call crush_run_begin)");
     long long issued = 0;
     int st;
     while (issued < n_steps) {
-        if (c->period > 0 && c->host_step % c->period == 0 && n_steps - issued >= c->period) {
+        const bool use_graph = c->period > 0 && c->host_step % c->period == 0 && n_steps - issued >= c->period;
+        if (use_graph) {
             if (!c->graph) {
                 int64_t before = c->launches;
                 st = build_graph(c);
@@ -734,6 +856,7 @@ int run_steps(crush_ctx* c, long long n_steps, int* done) {
             c->launches += c->graph_launches;
             c->host_step += c->period;
             issued += c->period;
+            c->last_was_graph = true;
         } else {
             if (c->profiling) {
                 st = ensure_prof_events(c);
@@ -744,28 +867,47 @@ int run_steps(crush_ctx* c, long long n_steps, int* done) {
             c->host_step += 1;
             issued += 1;
             c->last_was_graph = false;
-            continue;
         }
-        c->last_was_graph = true;
     }
-    int d = 0;
-    CK(cudaMemcpyAsync(&d, &c->ctl->done, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    return CRUSH_OK;
+}
+
+// Whether every slot has finished (device flags read back; synchronises).
+int all_done(crush_ctx* c, int* done) {
+    std::vector<Control> h(c->n_slots);
+    CK(cudaMemcpyAsync(h.data(), c->ctls, sizeof(Control) * h.size(), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    int d = 1;
+    for (const Control& x : h) d &= x.done ? 1 : 0;
+    *done = d;
+    return CRUSH_OK;
+}
+
+int run_steps(crush_ctx* c, long long n_steps, int* done) {
+    int st = issue_steps(c, n_steps);
+    if (st != CRUSH_OK) return st;
+    int d = 0;
+    st = all_done(c, &d);
+    if (st != CRUSH_OK) return st;
     if (done) *done = d;
     return CRUSH_OK;
 }
 
-int results(crush_ctx* c, crush_results* r) {
+int results(crush_ctx* c, int slot, crush_results* r) {
+    if (slot < 0 || slot >= c->n_slots) return crush::fail(CRUSH_ERR_INVALID, "slot out of range");
     Control h;
-    CK(cudaMemcpyAsync(&h, c->ctl, sizeof(Control), cudaMemcpyDeviceToHost, c->stream));
-    launch_vehicle_sums(c->stream, c->n_veh, c->veh_off, c->veh_nodes, c->mass, c->v, c->v0, c->veh_out);
-    int st = check_launch(c, c->n_veh > 0 ? 1 : 0);
-    if (st != CRUSH_OK) return st;
-    double sums[28];
-    if (c->n_veh > 0) CK(cudaMemcpyAsync(sums, c->veh_out, sizeof(double) * 7 * c->n_veh, cudaMemcpyDeviceToHost, c->stream));
-    // Crush needs u_x of the accelerometer and front nodes only.
-    std::vector<double> u(3 * c->n_nodes);
-    CK(cudaMemcpyAsync(u.data(), c->u, sizeof(double) * 3 * c->n_nodes, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(&h, c->ctls + slot, sizeof(Control), cudaMemcpyDeviceToHost, c->stream));
+    const Slot& sl = c->slots[slot];
+    std::vector<double> sums(7 * std::max(c->va.n_vehicles, 1));
+    if (c->va.n_vehicles > 0) {
+        launch_vehicle_sums(c->stream, c->va, c->mass, c->v, c->v0, c->veh_out);
+        int st = check_launch(c, 1);
+        if (st != CRUSH_OK) return st;
+        CK(cudaMemcpyAsync(sums.data(), c->veh_out, sizeof(double) * 7 * c->va.n_vehicles, cudaMemcpyDeviceToHost, c->stream));
+    }
+    // Crush needs u_x of the slot's accelerometer and front nodes only.
+    std::vector<double> u(3 * sl.n_nodes);
+    CK(cudaMemcpyAsync(u.data(), c->u + 3 * sl.node0, sizeof(double) * 3 * sl.n_nodes, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     std::memset(r, 0, sizeof(*r));
     r->time = h.t;
@@ -774,9 +916,10 @@ int results(crush_ctx* c, crush_results* r) {
     r->dt_min = h.dt_min;
     r->added_mass_max = h.added_mass_max;
     r->status = h.status;
-    r->n_vehicles = c->n_veh;
-    for (int k = 0; k < c->n_veh; ++k) {
-        const double* s = sums + 7 * k;
+    r->n_vehicles = sl.n_vehicles;
+    for (int k = 0; k < sl.n_vehicles; ++k) {
+        const int gv = sl.vehicle0 + k;
+        const double* s = sums.data() + 7 * gv;
         crush_vehicle_result& vr = r->vehicle[k];
         vr.mass = s[0];
         for (int dd = 0; dd < 3; ++dd) {
@@ -786,10 +929,47 @@ int results(crush_ctx* c, crush_results* r) {
             vr.delta_v[dd] = v1 - v0;
         }
         double fu = 0.0;
-        for (uint32_t n : c->veh_front[k]) fu += u[3 * (size_t)n];
-        fu = c->veh_front[k].empty() ? 0.0 : fu / (double)c->veh_front[k].size();
-        vr.crush = std::fabs(u[3 * (size_t)c->veh_accel[k]] - fu);
+        for (uint32_t n : c->veh_front[gv]) fu += u[3 * (size_t)(n - sl.node0)];
+        fu = c->veh_front[gv].empty() ? 0.0 : fu / (double)c->veh_front[gv].size();
+        vr.crush = std::fabs(u[3 * (size_t)(c->veh_accel[gv] - sl.node0)] - fu);
     }
+    return CRUSH_OK;
+}
+
+int reset_aux(crush_ctx* c, double dt_floor) {
+    std::vector<Control> aux(c->n_slots);
+    std::memset(aux.data(), 0, sizeof(Control) * aux.size());
+    for (Control& a : aux) {
+        a.dt_stable_bits = INF_BITS;
+        a.dt_floor = dt_floor;
+    }
+    CK(cudaMemcpyAsync(c->ctls_aux, aux.data(), sizeof(Control) * aux.size(), cudaMemcpyHostToDevice, c->stream));
+    return CRUSH_OK;
+}
+
+int read_aux(crush_ctx* c, std::vector<Control>* aux) {
+    aux->resize(c->n_slots);
+    CK(cudaMemcpyAsync(aux->data(), c->ctls_aux, sizeof(Control) * aux->size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return CRUSH_OK;
+}
+
+int run_to_end(crush_ctx* c) {
+    int st = run_begin(c);
+    if (st != CRUSH_OK) return st;
+    int done = 0;
+    const long long chunk = c->period > 0 ? 10 * (long long)c->period : 200;
+    long long total = 0;
+    long long cap = 0;
+    for (const Slot& sl : c->slots) cap = std::max<long long>(cap, sl.settings.max_steps > 0 ? sl.settings.max_steps : 2000000ll);
+    cap += chunk;
+    // A run that has not finished after this many steps is returned as a timeout.
+    while (!done && total < cap) {
+        st = run_steps(c, chunk, &done);
+        if (st != CRUSH_OK) return st;
+        total += chunk;
+    }
+    if (!done) return crush::fail(CRUSH_ERR_TIMEOUT, "run did not finish within " + std::to_string(cap) + " steps");
     return CRUSH_OK;
 }
 
@@ -811,17 +991,22 @@ int crush_device_info(int device, char* name, int name_len) {
     return p.multiProcessorCount;
 }
 
-int crush_create(const crush_model_desc* desc, int device, crush_ctx** out) {
+int crush_batch_create(const crush_model_desc* const* descs, int n, int device, crush_ctx** out) {
     if (!out) return crush::fail(CRUSH_ERR_INVALID, "null output");
     *out = nullptr;
     crush_ctx* c = new crush_ctx();
-    int st = create_impl(desc, device, c);
+    int st = create_impl(descs, n, device, c);
     if (st != CRUSH_OK) {
         delete c;
         return st;
     }
     *out = c;
     return CRUSH_OK;
+}
+
+int crush_create(const crush_model_desc* desc, int device, crush_ctx** out) {
+    const crush_model_desc* one[1] = {desc};
+    return crush_batch_create(one, 1, device, out);
 }
 
 void crush_destroy(crush_ctx* ctx) { delete ctx; }
@@ -834,6 +1019,8 @@ int crush_sizes(const crush_ctx* c, int64_t* n_nodes, int64_t* n_hexes, int64_t*
     return CRUSH_OK;
 }
 
+int crush_batch_size(const crush_ctx* c) { return c ? c->n_slots : 0; }
+
 int64_t crush_launch_count(const crush_ctx* c) { return c ? c->launches : 0; }
 
 int crush_compute_forces_device(crush_ctx* c, const double* u_device, double* f_device, int64_t* newly) {
@@ -842,20 +1029,19 @@ int crush_compute_forces_device(crush_ctx* c, const double* u_device, double* f_
     NodeArrays nd = c->nd();
     nd.u = const_cast<double*>(u_device);
     if (newly) {
-        CK(cudaMemsetAsync(&c->ctl_aux->eroded_step, 0, sizeof(long long), c->stream));
-        CK(cudaMemsetAsync(&c->ctl_aux->copy_timeout, 0, sizeof(int), c->stream));
+        int st = reset_aux(c, 0.0);
+        if (st != CRUSH_OK) return st;
     }
-    launch_forces(c->stream, c->el(), nd, c->ctl_aux, 0);
+    launch_forces(c->stream, c->el(), nd, c->ctls_aux, 0);
     launch_gather(c->stream, c->el(), nd, f_device);
     int st = check_launch(c, (c->n_hc > 0 ? 1 : 0) + 1);
     if (st != CRUSH_OK) return st;
     if (newly) {
+        std::vector<Control> aux;
+        st = read_aux(c, &aux);
+        if (st != CRUSH_OK) return st;
         long long k = 0;
-        int timeout = 0;
-        CK(cudaMemcpyAsync(&k, &c->ctl_aux->eroded_step, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaMemcpyAsync(&timeout, &c->ctl_aux->copy_timeout, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        if (timeout) return crush::fail(CRUSH_ERR_TIMEOUT, "element tile copy did not complete");
+        for (const Control& a : aux) k += a.eroded_step;
         *newly = k;
     }
     return CRUSH_OK;
@@ -896,13 +1082,9 @@ int crush_contact_apply(crush_ctx* c, int id, const double* u, const double* v, 
     CK(cudaMemsetAsync(c->ca.pen_max_bits + id, 0, sizeof(unsigned long long), c->stream));
     NodeArrays nd = c->nd();
     nd.u = c->u_tmp;
-    // host mirror of this contact's face / slave ranges
-    int fo[2], so[2];
-    CK(cudaMemcpyAsync(fo, c->ca.face_off + id, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaMemcpyAsync(so, c->ca.slave_off + id, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    launch_contact(c->stream, c->ca, nd, nullptr, id, id + 1, fo[1] - fo[0], so[1] - so[0], c->entries_cap, dt, m, c->f_tmp, 0);
-    int st = check_launch(c, (fo[1] > fo[0] ? 1 : 0) + (so[1] > so[0] ? 1 : 0) + 1);
+    const long long nf = c->face_off_h[id + 1] - c->face_off_h[id], ns = c->slave_off_h[id + 1] - c->slave_off_h[id];
+    launch_contact(c->stream, c->ca, nd, c->ctls_aux, id, id + 1, nf, ns, dt, m, c->f_tmp, 0);
+    int st = check_launch(c, (nf > 0 ? 1 : 0) + (ns > 0 ? 1 : 0) + 1);
     if (st != CRUSH_OK) return st;
     std::vector<double> f(3 * c->n_nodes);
     unsigned long long cnt = 0, mp = 0;
@@ -922,17 +1104,22 @@ int crush_stable_dt(crush_ctx* c, const double* u, double* dt) {
     if (!c || !u || !dt) return crush::fail(CRUSH_ERR_INVALID, "null argument");
     CK(cudaSetDevice(c->device));
     CK(cudaMemcpyAsync(c->u_tmp, u, sizeof(double) * 3 * c->n_nodes, cudaMemcpyHostToDevice, c->stream));
-    Control aux{};
-    aux.dt_stable_bits = 0x7ff0000000000000ull;
-    CK(cudaMemcpyAsync(c->ctl_aux, &aux, sizeof(Control), cudaMemcpyHostToDevice, c->stream));
-    launch_elem_dt(c->stream, c->el(), c->nd(), c->ctl_aux, c->u_tmp, c->dt_partials, 0);
-    int st = check_launch(c);
+    int st = reset_aux(c, 0.0);
     if (st != CRUSH_OK) return st;
-    unsigned long long bits = 0;
-    CK(cudaMemcpyAsync(&bits, &c->ctl_aux->dt_stable_bits, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    std::memcpy(dt, &bits, sizeof(double));
-    return std::isfinite(*dt) ? CRUSH_OK : CRUSH_NONE;
+    launch_elem_dt(c->stream, c->el(), c->nd(), c->ctls_aux, c->u_tmp, 0);
+    st = check_launch(c);
+    if (st != CRUSH_OK) return st;
+    std::vector<Control> aux;
+    st = read_aux(c, &aux);
+    if (st != CRUSH_OK) return st;
+    double m = INF;
+    for (const Control& a : aux) {
+        double x;
+        std::memcpy(&x, &a.dt_stable_bits, sizeof(double));
+        m = std::fmin(m, x);
+    }
+    *dt = m;
+    return std::isfinite(m) ? CRUSH_OK : CRUSH_NONE;
 }
 
 int crush_mass_scaling(crush_ctx* c, const double* u, double dt_min, const double* element_mass, double* added, double* total) {
@@ -944,23 +1131,21 @@ int crush_mass_scaling(crush_ctx* c, const double* u, double dt_min, const doubl
         CK(cudaMemcpyAsync(c->e_tmp, element_mass, sizeof(double) * c->n_all, cudaMemcpyHostToDevice, c->stream));
         el.elem_mass = c->e_tmp;
     }
-    Control aux{};
-    aux.dt_stable_bits = 0x7ff0000000000000ull;
-    aux.dt_floor = dt_min;
-    CK(cudaMemcpyAsync(c->ctl_aux, &aux, sizeof(Control), cudaMemcpyHostToDevice, c->stream));
+    int st = reset_aux(c, dt_min);
+    if (st != CRUSH_OK) return st;
     NodeArrays nd = c->nd();
     nd.added = c->n_tmp;
     nd.inv_mass = c->n_tmp2;
-    launch_elem_dt(c->stream, el, nd, c->ctl_aux, c->u_tmp, c->dt_partials, 0);
-    launch_mass_scaling(c->stream, el, nd, c->ctl_aux, 1);
-    int st = check_launch(c, 2);
+    launch_elem_dt(c->stream, el, nd, c->ctls_aux, c->u_tmp, 0);
+    launch_mass_scaling(c->stream, el, nd, c->ctls_aux, 1);
+    st = check_launch(c, 2);
     if (st != CRUSH_OK) return st;
-    std::vector<double> parts(c->dt_blocks);
     CK(cudaMemcpyAsync(added, c->n_tmp, sizeof(double) * c->n_nodes, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaMemcpyAsync(parts.data(), c->dt_partials, sizeof(double) * c->dt_blocks, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
+    std::vector<Control> aux;
+    st = read_aux(c, &aux);
+    if (st != CRUSH_OK) return st;
     double t = 0.0;
-    for (double p : parts) t += p;
+    for (const Control& a : aux) t += a.added_total_acc;
     if (total) *total = t;
     return CRUSH_OK;
 }
@@ -1050,7 +1235,13 @@ int crush_run_steps(crush_ctx* c, int64_t n_steps, int* done) {
 int crush_run_results(crush_ctx* c, crush_results* r) {
     if (!c || !r) return crush::fail(CRUSH_ERR_INVALID, "null argument");
     CK(cudaSetDevice(c->device));
-    return results(c, r);
+    return results(c, 0, r);
+}
+
+int crush_batch_results(crush_ctx* c, int slot, crush_results* r) {
+    if (!c || !r) return crush::fail(CRUSH_ERR_INVALID, "null argument");
+    CK(cudaSetDevice(c->device));
+    return results(c, slot, r);
 }
 
 int crush_run_state(crush_ctx* c, double* u, double* v) {
@@ -1087,45 +1278,17 @@ int crush_run_steps_timed(crush_ctx* c, int64_t n_steps, int* done, double* ms, 
     CK(cudaEventCreate(&t0));
     CK(cudaEventCreate(&t1));
     CK(cudaEventRecord(t0, c->stream));
-    // run_steps ends with a sync after reading the done flag; record t1 first.
-    int st = CRUSH_OK;
-    {
-        long long issued = 0;
-        while (issued < n_steps && st == CRUSH_OK) {
-            const bool use_graph = c->period > 0 && c->host_step % c->period == 0 && n_steps - issued >= c->period;
-            const long long chunk = use_graph ? c->period : 1;
-            // enqueue without the trailing sync of run_steps
-            if (use_graph) {
-                if (!c->graph) {
-                    int64_t before = c->launches;
-                    st = build_graph(c);
-                    if (st != CRUSH_OK) break;
-                    c->graph_launches = c->launches - before;
-                    c->launches = before;
-                }
-                cudaError_t e = cudaGraphLaunch(c->graph, c->stream);
-                if (e != cudaSuccess) { st = crush::fail(CRUSH_ERR_CUDA, cudaGetErrorString(e)); break; }
-                c->launches += c->graph_launches;
-                c->host_step += c->period;
-                c->last_was_graph = true;
-            } else {
-                if (c->profiling) {
-                    st = ensure_prof_events(c);
-                    if (st != CRUSH_OK) break;
-                }
-                st = enqueue_step(c, c->host_step, c->profiling ? &c->prof_ev[0] : nullptr);
-                c->host_step += 1;
-                c->last_was_graph = false;
-            }
-            issued += chunk;
-        }
+    int st = issue_steps(c, n_steps);
+    if (st != CRUSH_OK) {
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        return st;
     }
     CK(cudaEventRecord(t1, c->stream));
     int d = 0;
-    CK(cudaMemcpyAsync(&d, &c->ctl->done, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
+    st = all_done(c, &d);
     float elapsed = 0.f;
-    CK(cudaEventElapsedTime(&elapsed, t0, t1));
+    cudaEventElapsedTime(&elapsed, t0, t1);
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     if (st != CRUSH_OK) return st;
@@ -1148,25 +1311,24 @@ int crush_run_steps_timed(crush_ctx* c, int64_t n_steps, int* done, double* ms, 
 
 int crush_run(crush_ctx* c, crush_results* r) {
     if (!c || !r) return crush::fail(CRUSH_ERR_INVALID, "null argument");
-    int st = crush_run_begin(c);
+    CK(cudaSetDevice(c->device));
+    int st = run_to_end(c);
     if (st != CRUSH_OK) return st;
-    int done = 0;
-    const long long chunk = c->period > 0 ? 10 * (long long)c->period : 200;
-    long long total = 0;
-    // A run that has not finished after this many steps is returned as a timeout.
-    const long long cap = c->settings.max_steps > 0 ? (long long)c->settings.max_steps + chunk : 2000000ll;
-    while (!done && total < cap) {
-        st = run_steps(c, chunk, &done);
-        if (st != CRUSH_OK) return st;
-        total += chunk;
-    }
-    st = results(c, r);
+    st = results(c, 0, r);
     if (st != CRUSH_OK) return st;
-    if (!done && r->status == CRUSH_OK) {
-        r->status = CRUSH_ERR_TIMEOUT;
-        return crush::fail(CRUSH_ERR_TIMEOUT, "run did not finish within " + std::to_string(cap) + " steps");
-    }
     return r->status;
+}
+
+int crush_batch_run(crush_ctx* c, crush_results* r) {
+    if (!c || !r) return crush::fail(CRUSH_ERR_INVALID, "null argument");
+    CK(cudaSetDevice(c->device));
+    int st = run_to_end(c);
+    if (st != CRUSH_OK) return st;
+    for (int k = 0; k < c->n_slots; ++k) {
+        st = results(c, k, r + k);
+        if (st != CRUSH_OK) return st;
+    }
+    return CRUSH_OK;
 }
 
 }  // extern "C"

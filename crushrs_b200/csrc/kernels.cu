@@ -100,8 +100,9 @@ __device__ bool reference_gradients(const double x[8][3], const double dn[8][3],
 
 __global__ void __launch_bounds__(128) k_setup_geometry(long long n_all, const double* __restrict__ pos,
                                                         const uint32_t* __restrict__ conn, const int32_t* __restrict__ part,
-                                                        const double* __restrict__ mat, double hourglass,
-                                                        const int64_t* __restrict__ hc_index, long long stride,
+                                                        const double* __restrict__ mat,
+                                                        const int64_t* __restrict__ hc_index, const uint32_t* __restrict__ elem_slot,
+                                                        long long stride,
                                                         float4* __restrict__ planes, double* __restrict__ volume_out,
                                                         double* __restrict__ lumped_out, double* __restrict__ dt_factor,
                                                         double* __restrict__ elem_mass, int* __restrict__ bad) {
@@ -114,7 +115,7 @@ __global__ void __launch_bounds__(128) k_setup_geometry(long long n_all, const d
         for (int d = 0; d < 3; ++d) x[i][d] = pos[3 * (long long)nid[i] + d];
     }
     const int p = part[e];
-    const double youngs = mat[3 * p], nu = mat[3 * p + 1], rho = mat[3 * p + 2];
+    const double youngs = mat[4 * p], nu = mat[4 * p + 1], rho = mat[4 * p + 2], hourglass = mat[4 * p + 3];
     double dnc[8][3], gc[8][3], detc;
     shape_derivatives(0.0, 0.0, 0.0, dnc);
     if (!reference_gradients(x, dnc, gc, &detc)) {
@@ -273,7 +274,7 @@ __global__ void __launch_bounds__(128) k_setup_geometry(long long n_all, const d
         for (int aa = 0; aa < 4; ++aa) gm[4 * i + aa] = (float)gam[i][aa];
     for (int k = 0; k < 8; ++k) pl[(P_GAMMA + k) * stride + h] = make_float4(gm[4 * k], gm[4 * k + 1], gm[4 * k + 2], gm[4 * k + 3]);
     for (int k = 0; k < 20; ++k) pl[(P_H + k) * stride + h] = make_float4(hs[4 * k], hs[4 * k + 1], hs[4 * k + 2], hs[4 * k + 3]);
-    pl[P_META * stride + h] = make_float4((float)volume, __uint_as_float((uint32_t)p), __uint_as_float((uint32_t)e), 0.0f);
+    pl[P_META * stride + h] = make_float4((float)volume, __uint_as_float((uint32_t)p), __uint_as_float((uint32_t)e), __uint_as_float(elem_slot[e]));
 }
 
 // Lumped nodal masses: Σ over incident (element, corner) in element order
@@ -305,11 +306,13 @@ __global__ void k_init_state(long long n_hc, long long stride, float4* __restric
 #ifndef FORCES_MINB
 #define FORCES_MINB 2
 #endif
-__global__ void __launch_bounds__(FORCES_TPB, FORCES_MINB) k_forces(ElementArrays el, NodeArrays nd, Control* ctl, int respect_done) {
+__global__ void __launch_bounds__(FORCES_TPB, FORCES_MINB) k_forces(ElementArrays el, NodeArrays nd, Control* ctls, int respect_done) {
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (respect_done && ctl->done) return;
     if (e >= el.n_hc) return;
     const long long S = el.stride;
+    const float4 meta = ld_plane(el.planes, S, P_META, e);
+    Control* ctl = ctls + __float_as_uint(meta.w);
+    if (respect_done && ctl->done) return;
     float4* out = reinterpret_cast<float4*>(el.corner + 24 * e);
     const float4 st6 = el.state[6 * S + e];
     if (__float_as_uint(st6.y) != 0u) {  // already eroded: no force
@@ -358,8 +361,7 @@ __global__ void __launch_bounds__(FORCES_TPB, FORCES_MINB) k_forces(ElementArray
     const float det = det3(f);
     if (det <= 0.0f) {  // inverted: erode (src/kernel_simd.rs:324-331)
         el.state[6 * S + e] = make_float4(st6.x, __uint_as_float(1u), st6.z, st6.w);
-        const uint32_t model_e = __float_as_uint(ld_plane(el.planes, S, P_META, e).z);
-        el.eroded_all[model_e] = 1;
+        el.eroded_all[__float_as_uint(meta.z)] = 1;
         atomicAdd(reinterpret_cast<unsigned long long*>(&ctl->eroded_step), 1ull);
         for (int k = 0; k < 6; ++k) out[k] = make_float4(0.f, 0.f, 0.f, 0.f);
         return;
@@ -371,7 +373,6 @@ __global__ void __launch_bounds__(FORCES_TPB, FORCES_MINB) k_forces(ElementArray
         st[4 * k] = s4.x; st[4 * k + 1] = s4.y; st[4 * k + 2] = s4.z; st[4 * k + 3] = s4.w;
     }
     st[24] = st6.x; st[25] = st6.y; st[26] = st6.z; st[27] = st6.w;
-    const float4 meta = ld_plane(el.planes, S, P_META, e);
     const MaterialF32& mat = el.mats[__float_as_uint(meta.y)];
     M3f tau, f_inv;
     honeycomb_update(f, det, st, mat, tau, f_inv);
@@ -445,9 +446,11 @@ __global__ void k_gather(ElementArrays el, NodeArrays nd, double* __restrict__ f
 }
 
 // Half step: v½ = v + ½dt (f_ext - f_int)/m ; u += dt v½ ; fixed -> 0 (src/solver.rs:314-323).
-__global__ void k_half(NodeArrays nd, Control* ctl) {
+__global__ void k_half(NodeArrays nd, Control* ctls) {
     long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= nd.n || ctl->done) return;
+    if (n >= nd.n) return;
+    const Control* ctl = ctls + nd.node_slot[n];
+    if (ctl->done) return;
     const double dt = step_dt(ctl);
     const double im = nd.inv_mass[n];
     const bool fixed = nd.fixed[n] != 0;
@@ -467,9 +470,11 @@ __global__ void k_half(NodeArrays nd, Control* ctl) {
 }
 
 // Full step with the fused force gather: v = (v½ + ½dt a) damping (src/solver.rs:334-342).
-__global__ void k_full(ElementArrays el, NodeArrays nd, Control* ctl) {
+__global__ void k_full(ElementArrays el, NodeArrays nd, Control* ctls) {
     long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= nd.n || ctl->done) return;
+    if (n >= nd.n) return;
+    const Control* ctl = ctls + nd.node_slot[n];
+    if (ctl->done) return;
     const double dt = step_dt(ctl);
     double f[3];
     gather_node(nd, el.corner, n, f[0], f[1], f[2]);
@@ -527,58 +532,71 @@ __device__ void char_length_and_volume(const double p[8][3], double* l, double* 
 
 constexpr int DT_TPB = 256;
 
-__global__ void __launch_bounds__(DT_TPB) k_elem_dt(ElementArrays el, NodeArrays nd, Control* ctl, const double* __restrict__ u,
-                                                    double* __restrict__ partials, int respect_done) {
-    __shared__ double s_min[DT_TPB];
-    __shared__ double s_sum[DT_TPB];
-    if (respect_done && ctl->done) return;
-    long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+// Per-element stability limit and mass-scaling surplus. The minimum per crash
+// slot is an atomicMin on the bit pattern of a non-negative double (order
+// independent); lanes of a warp that share a slot reduce first.
+__global__ void __launch_bounds__(DT_TPB) k_elem_dt(ElementArrays el, NodeArrays nd, Control* ctls, const double* __restrict__ u,
+                                                    int respect_done) {
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    uint32_t slot = 0xffffffffu;
     double dt = CUDART_INF, extra = 0.0;
     if (e < el.n_all) {
-        if (!el.eroded_all[e]) {
-            double p[8][3];
-            for (int i = 0; i < 8; ++i) {
-                long long n = el.conn_all[8 * e + i];
-                for (int d = 0; d < 3; ++d) p[i][d] = nd.pos[3 * n + d] + u[3 * n + d];
+        slot = el.elem_slot[e];
+        Control* ctl = ctls + slot;
+        if (respect_done && ctl->done) {
+            slot = 0xffffffffu;
+        } else {
+            if (!el.eroded_all[e]) {
+                double p[8][3];
+                for (int i = 0; i < 8; ++i) {
+                    long long n = el.conn_all[8 * e + i];
+                    for (int d = 0; d < 3; ++d) p[i][d] = nd.pos[3 * n + d] + u[3 * n + d];
+                }
+                double l, vol;
+                char_length_and_volume(p, &l, &vol);
+                if (isfinite(l) && vol > 0.0) dt = l * el.dt_factor[e];
             }
-            double l, vol;
-            char_length_and_volume(p, &l, &vol);
-            if (isfinite(l) && vol > 0.0) dt = l * el.dt_factor[e];
+            const double floor = ctl->dt_floor;
+            if (dt < floor) {
+                double r = floor / dt;
+                extra = (fmin(r * r, 100.0) - 1.0) * el.elem_mass[e];
+            }
+            el.elem_dt[e] = dt;
+            el.elem_extra[e] = extra;
         }
-        const double floor = ctl->dt_floor;
-        if (dt < floor) {
-            double r = floor / dt;
-            extra = (fmin(r * r, 100.0) - 1.0) * el.elem_mass[e];
-        }
-        el.elem_dt[e] = dt;
-        el.elem_extra[e] = extra;
     }
-    s_min[threadIdx.x] = dt;
-    s_sum[threadIdx.x] = extra;
-    __syncthreads();
-    for (int w = DT_TPB / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) {
-            s_min[threadIdx.x] = fmin(s_min[threadIdx.x], s_min[threadIdx.x + w]);
-            s_sum[threadIdx.x] = s_sum[threadIdx.x] + s_sum[threadIdx.x + w];
+    const uint32_t s0 = __shfl_sync(0xffffffffu, slot, 0);
+    const bool uniform = __all_sync(0xffffffffu, slot == s0);
+    if (uniform) {
+        if (s0 == 0xffffffffu) return;
+        for (int off = 16; off > 0; off >>= 1) {
+            dt = fmin(dt, __shfl_down_sync(0xffffffffu, dt, off));
+            extra += __shfl_down_sync(0xffffffffu, extra, off);
         }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        atomicMin(&ctl->dt_stable_bits, (unsigned long long)__double_as_longlong(s_min[0]));
-        partials[blockIdx.x] = s_sum[0];
+        if (lane == 0) {
+            atomicMin(&ctls[s0].dt_stable_bits, (unsigned long long)__double_as_longlong(dt));
+            if (extra > 0.0) atomicAdd(&ctls[s0].added_total_acc, extra);
+        }
+    } else if (slot != 0xffffffffu) {
+        atomicMin(&ctls[slot].dt_stable_bits, (unsigned long long)__double_as_longlong(dt));
+        if (extra > 0.0) atomicAdd(&ctls[slot].added_total_acc, extra);
     }
 }
 
-// The adaptive step decision of src/solver.rs:288-299 (one thread).
-__global__ void k_dt_finalize(Control* ctl, const double* __restrict__ partials, int n_blocks) {
+// The adaptive step decision of src/solver.rs:288-299, one thread per slot.
+__global__ void k_dt_finalize(Control* ctls, int n_slots) {
+    const int sl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sl >= n_slots) return;
+    Control* ctl = ctls + sl;
     if (ctl->done) return;
     const double dt_stable = __longlong_as_double((long long)ctl->dt_stable_bits);
+    const double total = ctl->added_total_acc;
     ctl->dt_stable_bits = (unsigned long long)__double_as_longlong(CUDART_INF);
+    ctl->added_total_acc = 0.0;
     if (!isfinite(dt_stable)) return;
     double dt_use = dt_stable;
     if (ctl->dt_floor > 0.0 && dt_stable < ctl->dt_floor) {
-        double total = 0.0;
-        for (int b = 0; b < n_blocks; ++b) total += partials[b];
         ctl->mass_scale_now = 1;
         ctl->added_total = total;
         ctl->added_mass_max = fmax(ctl->added_mass_max, total);
@@ -588,9 +606,10 @@ __global__ void k_dt_finalize(Control* ctl, const double* __restrict__ partials,
 }
 
 // Added nodal mass (element order, src/kernel.rs:246-255) and 1/(m + added).
-__global__ void k_mass_scaling(ElementArrays el, NodeArrays nd, Control* ctl, int force_apply) {
+__global__ void k_mass_scaling(ElementArrays el, NodeArrays nd, Control* ctls, int force_apply) {
     long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= nd.n) return;
+    const Control* ctl = ctls + nd.node_slot[n];
     if (!force_apply && (ctl->done || !ctl->mass_scale_now)) return;
     const double floor = ctl->dt_floor;
     double add = 0.0;
@@ -603,14 +622,19 @@ __global__ void k_mass_scaling(ElementArrays el, NodeArrays nd, Control* ctl, in
     nd.inv_mass[n] = m > 0.0 ? 1.0 / m : 0.0;
 }
 
-__global__ void k_nonfinite(NodeArrays nd, Control* ctl) {
+__global__ void k_nonfinite(NodeArrays nd, Control* ctls) {
     long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= 3 * nd.n || ctl->done) return;
+    if (k >= 3 * nd.n) return;
+    Control* ctl = ctls + nd.node_slot[k / 3];
+    if (ctl->done) return;
     if (!isfinite(nd.u[k])) ctl->nonfinite = 1;
 }
 
-// End of a step (src/solver.rs:344-345 plus the stop rules).
-__global__ void k_step_end(Control* ctl, ContactArrays ca, int check_separation) {
+// End of a step (src/solver.rs:344-345 plus the stop rules), one thread per slot.
+__global__ void k_step_end(Control* ctls, ContactArrays ca, VehicleArrays va, int check_separation) {
+    const int sl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sl >= ca.n_slots) return;
+    Control* ctl = ctls + sl;
     if (ctl->done) return;
     const double dt = step_dt(ctl);
     ctl->step += 1;
@@ -620,7 +644,7 @@ __global__ void k_step_end(Control* ctl, ContactArrays ca, int check_separation)
     ctl->eroded_step = 0;
     ctl->mass_scale_now = 0;
     int hit = 0;
-    for (int c = 0; c < ca.n_contacts; ++c) {
+    for (int c = ca.slot_contact_off[sl]; c < ca.slot_contact_off[sl + 1]; ++c) {
         if (ca.counts_for_stop[c] && ca.pen_count[c] > 0) hit = 1;
         ca.pen_count[c] = 0;
         ca.pen_max_bits[c] = 0;
@@ -641,7 +665,7 @@ __global__ void k_step_end(Control* ctl, ContactArrays ca, int check_separation)
     if (check_separation) {
         for (int veh = 0; veh < 2; ++veh) {
             double m = 0.0, p = 0.0;
-            for (int b = 0; b < VX_BLOCKS; ++b) {
+            for (int b = 0; b < va.vx_blocks; ++b) {
                 m += ctl->vx_part[veh][b][0];
                 p += ctl->vx_part[veh][b][1];
             }
@@ -660,11 +684,6 @@ __global__ void k_step_end(Control* ctl, ContactArrays ca, int check_separation)
 // ---------------------------------------------------------------------------
 constexpr int MAX_CELLS_PER_FACE = 1024;
 
-__device__ __forceinline__ int contact_of(const int* off, int n_contacts, long long i) {
-    int c = 0;
-    while (c + 1 < n_contacts && i >= off[c + 1]) ++c;
-    return c;
-}
 __device__ __forceinline__ unsigned cell_hash(long long i, long long j, long long k) {
     unsigned long long h = (unsigned long long)i * 73856093ull ^ (unsigned long long)j * 19349663ull ^
                            (unsigned long long)k * 83492791ull;
@@ -716,12 +735,12 @@ __device__ __forceinline__ unsigned point_cell_hash(const double* p, double cs) 
 // grown by 0.2 of its largest extent. So the key box is the face box grown by
 // 0.25 x extent + 4 x warp on every side and by max_distance x n_d on the
 // inner side of axis d.
-__global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctl, int c0, int c1, int run_mode) {
-    if (run_mode && ctl->done) return;
+__global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, int c1, int run_mode) {
     const long long f = ca.face_off[c0] + (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (f >= ca.face_off[c1]) return;
-    const int c = contact_of(ca.face_off, ca.n_contacts, f);
+    const int c = ca.face_contact[f];
+    if (run_mode && ctls[ca.contact_slot[c]].done) return;
     FaceGeo g;
     for (int k = 0; k < 4; ++k) {
         long long n = ca.faces[4 * f + k];
@@ -766,6 +785,8 @@ __global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctl, i
         khi[d] = fmin(fhi[d] + slack + md * fmax(-g.n[d], 0.0), g.hi[d]);
     }
     const int local = (int)(f - ca.face_off[c]);
+    const int tab = ca.tab_off[c];
+    if (ca.tab_off[c + 1] == tab) return;  // no grid: the contact is searched exhaustively
     long long r[6];
     if (!box_cells(klo, khi, ca.cell[c], r)) {
         if (lane == 0) {
@@ -775,7 +796,6 @@ __global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctl, i
         }
         return;
     }
-    const int tab = ca.tab_off[c];
     const unsigned mask = (unsigned)(ca.tab_off[c + 1] - tab - 1);
     const int ni = (int)(r[1] - r[0] + 1), nj = (int)(r[3] - r[2] + 1), nk = (int)(r[5] - r[4] + 1);
     for (int q = lane; q < ni * nj * nk; q += 32) {
@@ -823,17 +843,22 @@ __device__ __forceinline__ bool face_hit(const FaceGeo& g, const double* p, doub
 constexpr int SLAVE_LANES = 32;
 
 // First-hit search: SLAVE_LANES lanes per primary node test its grid bucket
-// (all of the contact's faces when the bucket overflowed) and the contact's
-// overflow faces, and keep the smallest face index that hits — the face the
-// reference's in-order scan with `break` finds (src/contact.rs:115-157).
-__global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctl, int c0, int c1, int run_mode, double dt_override,
+// and the contact's overflow faces — or every face of the contact when it has
+// no grid (small contacts) or the bucket overflowed — and keep the smallest
+// face index that hits: the face the reference's in-order scan with `break`
+// finds (src/contact.rs:115-157).
+__global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, int c1, int run_mode, double dt_override,
                                  const double* __restrict__ masses) {
-    if (run_mode && ctl->done) return;
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x % SLAVE_LANES;
     const long long s_begin = ca.slave_off[c0], s_end = ca.slave_off[c1];
     const long long s = s_begin + gid / SLAVE_LANES;
-    const bool live = s < s_end;
+    bool live = s < s_end;
+    const Control* ctl = nullptr;
+    if (live) {
+        ctl = ctls + ca.contact_slot[ca.slave_contact[s]];
+        if (run_mode && ctl->done) live = false;
+    }
     int best = INT_MAX;
     double best_sd = 0.0, sd;
     int c = 0;
@@ -841,7 +866,7 @@ __global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctl, 
     double p[3] = {0.0, 0.0, 0.0}, md = 0.0;
     const FaceGeo* geo = nullptr;
     if (live) {
-        c = contact_of(ca.slave_off, ca.n_contacts, s);
+        c = ca.slave_contact[s];
         n = ca.slaves[s];
         p[0] = nd.pos[3 * n] + nd.u[3 * n];
         p[1] = nd.pos[3 * n + 1] + nd.u[3 * n + 1];
@@ -850,10 +875,11 @@ __global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctl, 
         const long long fb = ca.face_off[c];
         geo = ca.geo + fb;
         const int tab = ca.tab_off[c];
-        const unsigned mask = (unsigned)(ca.tab_off[c + 1] - tab - 1);
+        const bool grid = ca.tab_off[c + 1] > tab;
+        const unsigned mask = grid ? (unsigned)(ca.tab_off[c + 1] - tab - 1) : 0u;
         const int b = tab + (int)(point_cell_hash(p, ca.cell[c]) & mask);
-        const int cnt = ca.counts[b];
-        if (cnt > BUCKET_CAP || ca.entry_overrun[c]) {
+        const int cnt = grid ? ca.counts[b] : 0;
+        if (!grid || cnt > BUCKET_CAP || ca.entry_overrun[c]) {
             const int nf = (int)(ca.face_off[c + 1] - fb);
             for (int f = lane; f < nf; f += SLAVE_LANES)
                 if (f < best && face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; }
@@ -905,13 +931,12 @@ constexpr int MAX_NODE_EVENTS = 48;
 // it belongs to (-F/4), sorts them by primary-node order (own before face for
 // the same primary node) and sums them in that order — the sequence in which
 // src/contact.rs:146-153 adds them to f_ext. Then clears the grid.
-__global__ void k_contact_gather(ContactArrays ca, NodeArrays nd, Control* ctl, int c0, int c1, int run_mode,
+__global__ void k_contact_gather(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, int c1, int run_mode,
                                  double* __restrict__ f_out, int skip_fixed) {
-    if (run_mode && ctl->done) return;
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < ca.n_cnodes) {
         const long long n = ca.cnode[i];
-        if (!(skip_fixed && nd.fixed[n])) {
+        if (!(skip_fixed && nd.fixed[n]) && !(run_mode && ctls[nd.node_slot[n]].done)) {
             double sx = 0.0, sy = 0.0, sz = 0.0;
             bool touched = false;
             for (uint32_t r = ca.cnode_off[i]; r < ca.cnode_off[i + 1]; ++r) {
@@ -979,18 +1004,17 @@ __global__ void k_contact_gather(ContactArrays ca, NodeArrays nd, Control* ctl, 
 
 // ---------------------------------------------------------------------------
 // FP64 vehicle reductions (delta-v, crush, separation rule), one block per
-// vehicle, fixed summation order.
+// vehicle (or per vehicle slice), fixed summation order.
 // ---------------------------------------------------------------------------
 constexpr int VEH_TPB = 256;
 
-__global__ void __launch_bounds__(VEH_TPB) k_vehicle_sums(const long long* __restrict__ off, const uint32_t* __restrict__ nodes,
-                                                          const double* __restrict__ mass, const double* __restrict__ v,
+__global__ void __launch_bounds__(VEH_TPB) k_vehicle_sums(VehicleArrays va, const double* __restrict__ mass, const double* __restrict__ v,
                                                           const double* __restrict__ v0, double* __restrict__ out) {
     __shared__ double s[7][VEH_TPB];
     const int veh = blockIdx.x;
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-    for (long long i = off[veh] + threadIdx.x; i < off[veh + 1]; i += VEH_TPB) {
-        const long long n = nodes[i];
+    for (long long i = va.off[veh] + threadIdx.x; i < va.off[veh + 1]; i += VEH_TPB) {
+        const long long n = va.nodes[i];
         const double m = mass[n];
         acc[0] += m;
         for (int d = 0; d < 3; ++d) {
@@ -1009,20 +1033,32 @@ __global__ void __launch_bounds__(VEH_TPB) k_vehicle_sums(const long long* __res
         for (int k = 0; k < 7; ++k) out[7 * veh + k] = s[k][0];
 }
 
-// Mean x-velocity partial sums for the separation rule: VX_BLOCKS blocks per
-// vehicle, each over a contiguous slice of the vehicle's nodes; k_step_end
-// adds the partials in block order.
-__global__ void __launch_bounds__(VEH_TPB) k_vehicle_vx(const long long* __restrict__ off, const uint32_t* __restrict__ nodes,
-                                                        const double* __restrict__ mass, const double* __restrict__ v, Control* ctl) {
+// Blocks a vehicle's separation-rule reduction uses: one per 2048 nodes, at
+// most VX_BLOCKS. It depends only on the vehicle itself, so a crash reduces
+// in the same order alone and inside a batch.
+__device__ __forceinline__ long long vx_blocks_of(long long len) {
+    const long long b = (len + 2047) / 2048;
+    return b < 1 ? 1 : (b > VX_BLOCKS ? VX_BLOCKS : b);
+}
+
+// Mean x-velocity partial sums for the separation rule: vx_blocks_of(len)
+// blocks per vehicle, each over a contiguous slice of the vehicle's nodes
+// (the launch has va.vx_blocks, the largest count; surplus blocks write zero
+// partials); k_step_end adds the partials in block order.
+__global__ void __launch_bounds__(VEH_TPB) k_vehicle_vx(VehicleArrays va, const double* __restrict__ mass, const double* __restrict__ v,
+                                                        Control* ctls) {
     __shared__ double sm[VEH_TPB], sp[VEH_TPB];
-    if (ctl->done) return;
-    const int veh = blockIdx.x / VX_BLOCKS, b = blockIdx.x % VX_BLOCKS;
-    const long long n0 = off[veh], len = off[veh + 1] - off[veh];
-    const long long per = (len + VX_BLOCKS - 1) / VX_BLOCKS;
-    const long long lo = n0 + b * per, hi = min(lo + per, n0 + len);
+    const int veh = blockIdx.x / va.vx_blocks, b = blockIdx.x % va.vx_blocks;
+    Control* ctl = ctls + va.slot[veh];
+    const int lv = va.local[veh];
+    if (ctl->done || lv >= 4) return;
+    const long long n0 = va.off[veh], len = va.off[veh + 1] - va.off[veh];
+    const long long nb = vx_blocks_of(len);
+    const long long per = (len + nb - 1) / nb;
+    const long long lo = b < nb ? n0 + b * per : n0 + len, hi = min(lo + per, n0 + len);
     double m_acc = 0.0, p_acc = 0.0;
     for (long long i = lo + threadIdx.x; i < hi; i += VEH_TPB) {
-        const long long n = nodes[i];
+        const long long n = va.nodes[i];
         m_acc += mass[n];
         p_acc += mass[n] * v[3 * n];
     }
@@ -1036,9 +1072,9 @@ __global__ void __launch_bounds__(VEH_TPB) k_vehicle_vx(const long long* __restr
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0 && veh < 4) {
-        ctl->vx_part[veh][b][0] = sm[0];
-        ctl->vx_part[veh][b][1] = sp[0];
+    if (threadIdx.x == 0) {
+        ctl->vx_part[lv][b][0] = sm[0];
+        ctl->vx_part[lv][b][1] = sp[0];
     }
 }
 
@@ -1048,11 +1084,11 @@ __global__ void __launch_bounds__(VEH_TPB) k_vehicle_vx(const long long* __restr
 // Launchers
 // ---------------------------------------------------------------------------
 void launch_setup_geometry(cudaStream_t s, long long n_all, const double* pos, const uint32_t* conn_all, const int32_t* part,
-                           const double* mat, double hourglass, const int64_t* hc_index, long long stride, float4* planes,
-                           double* volume, double* lumped, double* dt_factor, double* elem_mass, int* bad) {
+                           const double* mat, const int64_t* hc_index, const uint32_t* elem_slot, long long stride,
+                           float4* planes, double* volume, double* lumped, double* dt_factor, double* elem_mass, int* bad) {
     if (n_all <= 0) return;
-    k_setup_geometry<<<(unsigned)blocks_for(n_all, 128), 128, 0, s>>>(n_all, pos, conn_all, part, mat, hourglass, hc_index, stride,
-                                                                       planes, volume, lumped, dt_factor, elem_mass, bad);
+    k_setup_geometry<<<(unsigned)blocks_for(n_all, 128), 128, 0, s>>>(n_all, pos, conn_all, part, mat, hc_index, elem_slot,
+                                                                       stride, planes, volume, lumped, dt_factor, elem_mass, bad);
 }
 void launch_node_masses(cudaStream_t s, long long n, const uint32_t* off, const uint32_t* slot, const double* lumped,
                         double* mass, double* inv_mass) {
@@ -1062,61 +1098,57 @@ void launch_init_state(cudaStream_t s, long long n_hc, long long stride, float4*
     if (n_hc <= 0) return;
     k_init_state<<<(unsigned)blocks_for(n_hc, TPB), TPB, 0, s>>>(n_hc, stride, state);
 }
-void launch_forces(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctl, int respect_done) {
+void launch_forces(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, int respect_done) {
     if (el.n_hc <= 0) return;
-    k_forces<<<(unsigned)blocks_for(el.n_hc, FORCES_TPB), FORCES_TPB, 0, s>>>(el, nd, ctl, respect_done);
+    k_forces<<<(unsigned)blocks_for(el.n_hc, FORCES_TPB), FORCES_TPB, 0, s>>>(el, nd, ctls, respect_done);
 }
 void launch_gather(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, double* f_out) {
     k_gather<<<(unsigned)blocks_for(nd.n, TPB), TPB, 0, s>>>(el, nd, f_out);
 }
-void launch_half(cudaStream_t s, const NodeArrays& nd, Control* ctl) {
-    k_half<<<(unsigned)blocks_for(nd.n, TPB), TPB, 0, s>>>(nd, ctl);
+void launch_half(cudaStream_t s, const NodeArrays& nd, Control* ctls) {
+    k_half<<<(unsigned)blocks_for(nd.n, TPB), TPB, 0, s>>>(nd, ctls);
 }
-void launch_full(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctl) {
-    k_full<<<(unsigned)blocks_for(nd.n, TPB), TPB, 0, s>>>(el, nd, ctl);
+void launch_full(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls) {
+    k_full<<<(unsigned)blocks_for(nd.n, TPB), TPB, 0, s>>>(el, nd, ctls);
 }
-int elem_dt_blocks(long long n_all) { return (int)blocks_for(n_all > 0 ? n_all : 1, DT_TPB); }
-void launch_elem_dt(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctl, const double* u, double* partials,
-                    int respect_done) {
-    k_elem_dt<<<elem_dt_blocks(el.n_all), DT_TPB, 0, s>>>(el, nd, ctl, u, partials, respect_done);
+void launch_elem_dt(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, const double* u, int respect_done) {
+    if (el.n_all <= 0) return;
+    k_elem_dt<<<(unsigned)blocks_for(el.n_all, DT_TPB), DT_TPB, 0, s>>>(el, nd, ctls, u, respect_done);
 }
-void launch_dt_finalize(cudaStream_t s, Control* ctl, const double* partials, int n_blocks) {
-    k_dt_finalize<<<1, 1, 0, s>>>(ctl, partials, n_blocks);
+void launch_dt_finalize(cudaStream_t s, Control* ctls, int n_slots) {
+    k_dt_finalize<<<(unsigned)blocks_for(n_slots, 128), 128, 0, s>>>(ctls, n_slots);
 }
-void launch_mass_scaling(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctl, int force_apply) {
-    k_mass_scaling<<<(unsigned)blocks_for(nd.n, TPB), TPB, 0, s>>>(el, nd, ctl, force_apply);
+void launch_mass_scaling(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, int force_apply) {
+    k_mass_scaling<<<(unsigned)blocks_for(nd.n, TPB), TPB, 0, s>>>(el, nd, ctls, force_apply);
 }
-void launch_nonfinite(cudaStream_t s, const NodeArrays& nd, Control* ctl) {
-    k_nonfinite<<<(unsigned)blocks_for(3 * nd.n, TPB), TPB, 0, s>>>(nd, ctl);
+void launch_nonfinite(cudaStream_t s, const NodeArrays& nd, Control* ctls) {
+    k_nonfinite<<<(unsigned)blocks_for(3 * nd.n, TPB), TPB, 0, s>>>(nd, ctls);
 }
-void launch_step_end(cudaStream_t s, Control* ctl, const ContactArrays& ca, int check_separation) {
-    k_step_end<<<1, 1, 0, s>>>(ctl, ca, check_separation);
+void launch_step_end(cudaStream_t s, Control* ctls, const ContactArrays& ca, const VehicleArrays& va, int check_separation) {
+    k_step_end<<<(unsigned)blocks_for(ca.n_slots, 128), 128, 0, s>>>(ctls, ca, va, check_separation);
 }
-void launch_vehicle_sums(cudaStream_t s, int n_veh, const long long* veh_off, const uint32_t* veh_nodes, const double* mass,
-                         const double* v, const double* v0, double* out) {
-    if (n_veh <= 0) return;
-    k_vehicle_sums<<<n_veh, VEH_TPB, 0, s>>>(veh_off, veh_nodes, mass, v, v0, out);
+void launch_vehicle_sums(cudaStream_t s, const VehicleArrays& va, const double* mass, const double* v, const double* v0, double* out) {
+    if (va.n_vehicles <= 0) return;
+    k_vehicle_sums<<<va.n_vehicles, VEH_TPB, 0, s>>>(va, mass, v, v0, out);
 }
-void launch_vehicle_vx(cudaStream_t s, int n_veh, const long long* veh_off, const uint32_t* veh_nodes, const double* mass,
-                       const double* v, Control* ctl) {
-    if (n_veh <= 0) return;
-    k_vehicle_vx<<<std::min(n_veh, 4) * VX_BLOCKS, VEH_TPB, 0, s>>>(veh_off, veh_nodes, mass, v, ctl);
+void launch_vehicle_vx(cudaStream_t s, const VehicleArrays& va, const double* mass, const double* v, Control* ctls) {
+    if (va.n_vehicles <= 0) return;
+    k_vehicle_vx<<<(unsigned)(va.n_vehicles * va.vx_blocks), VEH_TPB, 0, s>>>(va, mass, v, ctls);
 }
 
 // Contact pass over contacts [c0, c1): faces + grid, first-hit search, ordered
 // reaction gather into f_out. n_faces / n_slaves are the host-known totals of
-// that range. dt_override > 0 is the drop-in call (no run control block).
-void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctl, int c0, int c1,
-                    long long n_faces, long long n_slaves, int entries_cap, double dt_override, const double* masses,
-                    double* f_out, int skip_fixed) {
-    (void)entries_cap;
+// that range. dt_override > 0 is the drop-in call (no run control).
+void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1,
+                    long long n_faces, long long n_slaves, double dt_override, const double* masses, double* f_out,
+                    int skip_fixed) {
     if (c1 <= c0) return;
     const int run_mode = dt_override > 0.0 ? 0 : 1;
-    if (n_faces > 0) k_contact_faces<<<(unsigned)blocks_for(n_faces * 32, TPB), TPB, 0, s>>>(ca, nd, ctl, c0, c1, run_mode);
+    if (n_faces > 0) k_contact_faces<<<(unsigned)blocks_for(n_faces * 32, TPB), TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode);
     if (n_slaves > 0)
-        k_contact_slaves<<<(unsigned)blocks_for(n_slaves * SLAVE_LANES, TPB), TPB, 0, s>>>(ca, nd, ctl, c0, c1, run_mode, dt_override, masses);
+        k_contact_slaves<<<(unsigned)blocks_for(n_slaves * SLAVE_LANES, TPB), TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses);
     long long nodes = ca.n_cnodes > 0 ? ca.n_cnodes : 1;
-    k_contact_gather<<<(unsigned)blocks_for(nodes, 128), 128, 0, s>>>(ca, nd, ctl, c0, c1, run_mode, f_out, skip_fixed);
+    k_contact_gather<<<(unsigned)blocks_for(nodes, 128), 128, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, f_out, skip_fixed);
 }
 
 }  // namespace crush

@@ -21,6 +21,7 @@ struct ElementArrays {
     uint8_t* eroded_all;     // per model element
     double* elem_dt;         // per model element (written by the dt kernel)
     double* elem_extra;      // per model element added mass (mass scaling)
+    const uint32_t* elem_slot;  // crash slot per model element
 };
 
 struct NodeArrays {
@@ -39,6 +40,7 @@ struct NodeArrays {
     const uint32_t* hc_slot;
     const uint32_t* all_off; // N+1 CSR over all model (element, corner) slots
     const uint32_t* all_slot;
+    const uint32_t* node_slot;  // crash slot per node
 };
 
 // Contact runtime arrays (all contacts concatenated).
@@ -91,32 +93,46 @@ struct ContactArrays {
     const int* crole_faces;     // local indices of the contact's faces that contain the node
     int* face_hits;             // per face: primary nodes hitting it this step
     int* face_list;             // FACE_HIT_CAP primary nodes (global index) per face
+    const int* face_contact;    // contact of each face
+    const int* slave_contact;   // contact of each primary node entry
+    const int* contact_slot;    // crash slot of each contact
+    const int* slot_contact_off;// n_slots+1: contacts of each crash slot
+    int n_slots;
 };
 
+// Vehicles of all crash slots: node lists and the reduction layout.
+struct VehicleArrays {
+    int n_vehicles;
+    const long long* off;       // n_vehicles+1 into nodes
+    const uint32_t* nodes;
+    const int* slot;            // crash slot of each vehicle
+    const int* local;           // index of the vehicle within its slot (0..3)
+    int vx_blocks;              // blocks per vehicle for the separation-rule reduction (<= 64)
+};
+
+// Every launcher takes the array of per-crash control blocks (`ctls`, one
+// per crash slot); entities find their slot through the *_slot arrays.
 void launch_setup_geometry(cudaStream_t s, long long n_all, const double* pos, const uint32_t* conn_all,
-                           const int32_t* part, const double* mat_e_nu_rho, double hourglass, const int64_t* hc_index,
-                           long long stride, float4* planes, double* volume, double* lumped, double* dt_factor,
-                           double* elem_mass, int* bad);
+                           const int32_t* part, const double* mat_e_nu_rho_hg, const int64_t* hc_index,
+                           const uint32_t* elem_slot, long long stride, float4* planes, double* volume, double* lumped,
+                           double* dt_factor, double* elem_mass, int* bad);
 void launch_node_masses(cudaStream_t s, long long n, const uint32_t* off, const uint32_t* slot, const double* lumped,
                         double* mass, double* inv_mass);
 void launch_init_state(cudaStream_t s, long long n_hc, long long stride, float4* state);
-void launch_forces(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctl, int respect_done);
+void launch_forces(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, int respect_done);
 void launch_gather(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, double* f_out);
-void launch_half(cudaStream_t s, const NodeArrays& nd, Control* ctl);
-void launch_full(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctl);
-void launch_elem_dt(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctl, const double* u,
-                    double* block_partials, int respect_done);
-int elem_dt_blocks(long long n_all);
-void launch_dt_finalize(cudaStream_t s, Control* ctl, const double* block_partials, int n_blocks);
-void launch_mass_scaling(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctl, int force_apply);
-void launch_nonfinite(cudaStream_t s, const NodeArrays& nd, Control* ctl);
-void launch_step_end(cudaStream_t s, Control* ctl, const ContactArrays& ca, int check_separation);
-void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctl, int c0, int c1,
-                    long long n_faces, long long n_slaves, int entries_cap, double dt_override, const double* masses,
-                    double* f_out, int skip_fixed);
-void launch_vehicle_sums(cudaStream_t s, int n_veh, const long long* veh_off, const uint32_t* veh_nodes,
-                         const double* mass, const double* v, const double* v0, double* out5);
-void launch_vehicle_vx(cudaStream_t s, int n_veh, const long long* veh_off, const uint32_t* veh_nodes,
-                       const double* mass, const double* v, Control* ctl);
+void launch_half(cudaStream_t s, const NodeArrays& nd, Control* ctls);
+void launch_full(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls);
+void launch_elem_dt(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, const double* u, int respect_done);
+void launch_dt_finalize(cudaStream_t s, Control* ctls, int n_slots);
+void launch_mass_scaling(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, int force_apply);
+void launch_nonfinite(cudaStream_t s, const NodeArrays& nd, Control* ctls);
+void launch_step_end(cudaStream_t s, Control* ctls, const ContactArrays& ca, const VehicleArrays& va, int check_separation);
+void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1,
+                    long long n_faces, long long n_slaves, double dt_override, const double* masses, double* f_out,
+                    int skip_fixed);
+void launch_vehicle_sums(cudaStream_t s, const VehicleArrays& va, const double* mass, const double* v, const double* v0,
+                         double* out7);
+void launch_vehicle_vx(cudaStream_t s, const VehicleArrays& va, const double* mass, const double* v, Control* ctls);
 
 }  // namespace crush

@@ -27,13 +27,19 @@ def _f64(a):
 
 
 class Context:
-    """One model resident on one GPU (crush_ctx)."""
+    """One model, or a batch of models (a list of descriptors), resident on
+    one GPU (crush_ctx)."""
 
     def __init__(self, desc, device=0):
         self._lib = lib()
         h = C.c_void_p()
-        check(self._lib.crush_create(C.byref(desc), device, C.byref(h)))
+        if isinstance(desc, (list, tuple)):
+            arr = (C.POINTER(abi.ModelDesc) * len(desc))(*[C.pointer(d) for d in desc])
+            check(self._lib.crush_batch_create(arr, len(desc), device, C.byref(h)))
+        else:
+            check(self._lib.crush_create(C.byref(desc), device, C.byref(h)))
         self.h = h
+        self.n_slots = self._lib.crush_batch_size(self.h)
         nn, ne, na = C.c_int64(), C.c_int64(), C.c_int64()
         check(self._lib.crush_sizes(self.h, C.byref(nn), C.byref(ne), C.byref(na)))
         self.n_nodes, self.n_hexes, self.n_active = nn.value, ne.value, na.value
@@ -134,10 +140,16 @@ class Context:
         check(self._lib.crush_run_steps_timed(self.h, n, C.byref(done), C.byref(ms), _dp(ph), C.byref(ps)))
         return bool(done.value), ms.value, ph, ps.value
 
-    def results(self):
+    def results(self, slot=0):
         r = abi.Results()
-        check(self._lib.crush_run_results(self.h, C.byref(r)))
+        check(self._lib.crush_batch_results(self.h, slot, C.byref(r)))
         return r
+
+    def batch_run(self):
+        """Run every slot to its stop; list of per-slot Results."""
+        rs = (abi.Results * self.n_slots)()
+        check(self._lib.crush_batch_run(self.h, rs))
+        return list(rs)
 
     def state(self):
         u, v = np.zeros(3 * self.n_nodes), np.zeros(3 * self.n_nodes)

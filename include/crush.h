@@ -245,6 +245,30 @@ int crush_run_state(crush_ctx* ctx, double* u, double* v);
 /* Kernel launches issued by this context since creation. */
 int64_t crush_launch_count(const crush_ctx* ctx);
 
+/* ---- batched contexts: many crash models in one context ----
+ *
+ * No counterpart in the reference, whose unit of work is one model per
+ * process (src/bin/crushrs.rs:30). A batch context holds n models ("slots")
+ * resident on one GPU; every step is one launch sequence over the nodes and
+ * elements of all slots, and each slot carries its own device control block
+ * (time, step, stable dt, mass scaling, stop rule), so slots of different
+ * sizes and step sizes advance together and each stops on its own rule. The
+ * arithmetic of every slot is the arithmetic of the same model run alone:
+ * its results are bit-identical to crush_create + crush_run of that model.
+ * All models of a batch must share adaptive_check_steps and the time-step
+ * mode (fixed time_step or adaptive). The drop-in calls above act on all
+ * slots at once (nodes and elements in slot order; contact ids run over the
+ * slots' contacts in order); crush_stable_dt then returns the minimum over
+ * the slots. crush_create is crush_batch_create with n = 1. */
+int crush_batch_create(const crush_model_desc* const* descs, int n, int device, crush_ctx** out);
+/* Number of slots of a context (1 for crush_create). */
+int crush_batch_size(const crush_ctx* ctx);
+/* Run every slot to its stop; results[n] receives each slot's results. */
+int crush_batch_run(crush_ctx* ctx, crush_results* results);
+/* Results of one slot of the open run (crush_run_begin / crush_run_steps
+ * drive all slots; *done = 1 once every slot has stopped). */
+int crush_batch_results(crush_ctx* ctx, int slot, crush_results* results);
+
 #ifdef __cplusplus
 }
 #endif
