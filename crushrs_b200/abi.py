@@ -206,3 +206,19 @@ def declare_engine_api(lib):
     lib.crush_batch_size.argtypes = [vp]
     lib.crush_batch_run.argtypes = [vp, P(Results)]
     lib.crush_batch_results.argtypes = [vp, C.c_int, P(Results)]
+    lib.crush_contact_apply_static.argtypes = [C.c_int64, vp, vp, vp, C.c_int64, vp, vp, C.c_int64, vp,
+                                               C.c_double, C.c_double, C.c_double, vp, vp, vp]
+
+
+class ContactStats(C.Structure):
+    """crush_contact_stats (device-side output of crush_contact_apply_static)."""
+    _fields_ = [
+        ("penetration_count", C.c_int64),
+        ("max_penetration", C.c_double),
+        ("status", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+STATIC_MAX_NODES = 16384
+STATIC_MAX_FACES = 16384

@@ -8,6 +8,9 @@ namespace crush {
 
 // Records `msg` as the calling thread's last error and returns `code`.
 int fail(int code, const std::string& msg);
+// The same for a message with static storage: records the pointer only, so
+// the error path itself allocates nothing.
+int fail_literal(int code, const char* msg);
 const std::string& last_error();
 void clear_error();
 

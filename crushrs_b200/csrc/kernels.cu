@@ -1152,3 +1152,287 @@ void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& n
 }
 
 }  // namespace crush
+
+// ---------------------------------------------------------------------------
+// Allocation-free contact call (crush_contact_apply_static): the primary-node
+// filter of ContactRuntime::new (src/contact.rs:48-70) and one
+// ContactRuntime::apply (src/contact.rs:92-160) for a single contact, with
+// every intermediate in a fixed-size StaticContactScratch record. The search
+// is exhaustive (no grid, whose table size would depend on the mesh), with
+// the same narrow test, first-hit rule and force formula as the run's contact
+// kernels; reactions are applied by node occurrence in the reference's order.
+// ---------------------------------------------------------------------------
+namespace crush {
+namespace {
+
+constexpr int STATIC_TPB = 256;
+constexpr int STATIC_ONE_BLOCK = 1024;
+constexpr int STATIC_TILE = 256;
+
+// Single block: validates node ids, resets the record's counters and forms
+// the filter box: the faces' bounding box at the reference positions grown by
+// max_distance.
+__global__ void __launch_bounds__(STATIC_ONE_BLOCK) k_static_prepare(StaticContactScratch* sc, long long n_model,
+                                                                      const double* __restrict__ pos, long long n_nodes,
+                                                                      const uint32_t* __restrict__ nodes, long long n_faces,
+                                                                      const uint32_t* __restrict__ faces, double md) {
+    __shared__ double s_lo[3][STATIC_ONE_BLOCK / 32], s_hi[3][STATIC_ONE_BLOCK / 32];
+    __shared__ int s_bad;
+    if (threadIdx.x == 0) s_bad = 0;
+    __syncthreads();
+    double lo[3] = {CUDART_INF, CUDART_INF, CUDART_INF}, hi[3] = {-CUDART_INF, -CUDART_INF, -CUDART_INF};
+    int bad = 0;
+    for (long long k = threadIdx.x; k < 4 * n_faces; k += blockDim.x) {
+        const uint32_t n = faces[k];
+        if (n >= n_model) {
+            bad = 1;
+            continue;
+        }
+        for (int d = 0; d < 3; ++d) {
+            const double p = pos[3 * (long long)n + d];
+            lo[d] = fmin(lo[d], p);
+            hi[d] = fmax(hi[d], p);
+        }
+    }
+    for (long long k = threadIdx.x; k < n_nodes; k += blockDim.x)
+        if (nodes[k] >= n_model) bad = 1;
+    if (bad) atomicOr(&s_bad, 1);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int d = 0; d < 3; ++d)
+        for (int off = 16; off > 0; off >>= 1) {
+            lo[d] = fmin(lo[d], __shfl_down_sync(0xffffffffu, lo[d], off));
+            hi[d] = fmax(hi[d], __shfl_down_sync(0xffffffffu, hi[d], off));
+        }
+    if (lane == 0)
+        for (int d = 0; d < 3; ++d) {
+            s_lo[d][w] = lo[d];
+            s_hi[d][w] = hi[d];
+        }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int d = 0; d < 3; ++d) {
+            double a = s_lo[d][0], b = s_hi[d][0];
+            for (int k = 1; k < (int)(blockDim.x / 32); ++k) {
+                a = fmin(a, s_lo[d][k]);
+                b = fmax(b, s_hi[d][k]);
+            }
+            sc->box_lo[d] = a + -md;
+            sc->box_hi[d] = b + md;
+        }
+        sc->pen_count = 0;
+        sc->pen_max_bits = 0;
+        sc->n_hits = 0;
+        sc->error = s_bad;
+    }
+}
+
+// Face geometry at X + u, thread per face (the arithmetic of k_contact_faces).
+__global__ void k_static_faces(StaticContactScratch* sc, const double* __restrict__ pos, const double* __restrict__ u,
+                               long long n_faces, const uint32_t* __restrict__ faces, double md) {
+    const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n_faces || sc->error) return;
+    FaceGeo g;
+    for (int k = 0; k < 4; ++k) {
+        const long long n = faces[4 * f + k];
+        for (int d = 0; d < 3; ++d) g.x[k][d] = pos[3 * n + d] + u[3 * n + d];
+    }
+    double e1[3], e2[3];
+    for (int d = 0; d < 3; ++d) {
+        e1[d] = g.x[1][d] - g.x[0][d];
+        e2[d] = g.x[2][d] - g.x[0][d];
+    }
+    const double nx = e1[1] * e2[2] - e1[2] * e2[1];
+    const double ny = e1[2] * e2[0] - e1[0] * e2[2];
+    const double nz = e1[0] * e2[1] - e1[1] * e2[0];
+    const double len = sqrt(nx * nx + ny * ny + nz * nz);
+    g.n[0] = nx / len;
+    g.n[1] = ny / len;
+    g.n[2] = nz / len;
+    for (int d = 0; d < 3; ++d) {
+        g.c[d] = (((g.x[0][d] + g.x[1][d]) + g.x[2][d]) + g.x[3][d]) / 4.0;
+        double lo = g.x[0][d], hi = g.x[0][d];
+        for (int k = 1; k < 4; ++k) {
+            lo = fmin(lo, g.x[k][d]);
+            hi = fmax(hi, g.x[k][d]);
+        }
+        g.lo[d] = lo + -md;
+        g.hi[d] = hi + md;
+    }
+    sc->geo[f] = g;
+}
+
+// Warp per primary-node entry: the filter, then the smallest face index that
+// passes the narrow test (the face the reference's in-order scan finds) and
+// the penalty force on it.
+__global__ void k_static_search(StaticContactScratch* sc, const double* __restrict__ pos, const double* __restrict__ u,
+                                const double* __restrict__ masses, long long n_nodes, const uint32_t* __restrict__ nodes,
+                                const double* __restrict__ node_scale, long long n_faces, double stiffness, double md,
+                                double dt) {
+    const long long s = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // warp-uniform
+    const int lane = threadIdx.x & 31;
+    if (s >= n_nodes || sc->error) return;
+    const long long n = nodes[s];
+    bool keep = true;
+    for (int d = 0; d < 3; ++d) {
+        const double x = pos[3 * n + d];
+        if (!(x >= sc->box_lo[d] && x <= sc->box_hi[d])) keep = false;
+    }
+    if (!keep) {
+        if (lane == 0) sc->hit[s] = -1;
+        return;
+    }
+    const double p[3] = {pos[3 * n] + u[3 * n], pos[3 * n + 1] + u[3 * n + 1], pos[3 * n + 2] + u[3 * n + 2]};
+    int best = INT_MAX;
+    double best_sd = 0.0, sd;
+    for (long long f = lane; f < n_faces; f += 32)
+        if (f < best && face_hit(sc->geo[f], p, md, &sd)) {
+            best = (int)f;
+            best_sd = sd;
+        }
+    for (int off = 16; off > 0; off >>= 1) {
+        const int ob = __shfl_down_sync(0xffffffffu, best, off);
+        const double osd = __shfl_down_sync(0xffffffffu, best_sd, off);
+        if (ob < best) {
+            best = ob;
+            best_sd = osd;
+        }
+    }
+    if (lane != 0) return;
+    if (best == INT_MAX) {
+        sc->hit[s] = -1;
+        return;
+    }
+    const double scale = node_scale ? node_scale[s] : 1.0;
+    const double m = masses[n];
+    const double depth = fmin(-best_sd, 0.1 * md);
+    const double k_pen = fmin(stiffness * scale, 0.1 * m / (dt * dt));
+    const double mag = fmin(k_pen * depth, m * 1.0e5);
+    const FaceGeo& g = sc->geo[best];
+    sc->hit[s] = best;
+    sc->hit_force[3 * s] = mag * g.n[0];
+    sc->hit_force[3 * s + 1] = mag * g.n[1];
+    sc->hit_force[3 * s + 2] = mag * g.n[2];
+    atomicAdd(&sc->pen_count, 1ull);
+    atomicMax(&sc->pen_max_bits, (unsigned long long)__double_as_longlong(-best_sd));
+}
+
+// Single block: the entries that hit, compacted in entry order.
+__global__ void __launch_bounds__(STATIC_ONE_BLOCK) k_static_compact(StaticContactScratch* sc, long long n_nodes) {
+    __shared__ int s_warp[STATIC_ONE_BLOCK / 32];
+    __shared__ int s_base;
+    if (sc->error) return;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) s_base = 0;
+    __syncthreads();
+    for (long long c0 = 0; c0 < n_nodes; c0 += blockDim.x) {
+        const long long i = c0 + threadIdx.x;
+        const bool flag = i < n_nodes && sc->hit[i] >= 0;
+        const unsigned ballot = __ballot_sync(0xffffffffu, flag);
+        if (lane == 0) s_warp[w] = __popc(ballot);
+        __syncthreads();
+        int before = 0, total = 0;
+        for (int k = 0; k < nw; ++k) {
+            if (k < w) before += s_warp[k];
+            total += s_warp[k];
+        }
+        if (flag) sc->hit_list[s_base + before + __popc(ballot & ((1u << lane) - 1u))] = (int)i;
+        __syncthreads();
+        if (threadIdx.x == 0) s_base += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) sc->n_hits = s_base;
+}
+
+// Thread per node occurrence (the primary-node entries, then the face
+// corners): the node's force value after this contact, adding the hits in
+// entry order — +F for its own hit, -F/4 per corner it fills on a hit face —
+// starting from the value in f_accum (src/contact.rs:146-153).
+__global__ void __launch_bounds__(STATIC_TPB) k_static_occ(StaticContactScratch* sc, long long n_nodes, const uint32_t* __restrict__ nodes,
+                                                           long long n_faces, const uint32_t* __restrict__ faces,
+                                                           const double* __restrict__ f_accum) {
+    __shared__ uint32_t t_node[STATIC_TILE];
+    __shared__ uint32_t t_face[STATIC_TILE][4];
+    __shared__ double t_f[STATIC_TILE][3];
+    if (sc->error) return;  // grid-uniform
+    const long long n_occ = n_nodes + 4 * n_faces;
+    const long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = o < n_occ;
+    const long long n = live ? (long long)(o < n_nodes ? nodes[o] : faces[o - n_nodes]) : 0;
+    double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+    if (live) {
+        v0 = f_accum[3 * n];
+        v1 = f_accum[3 * n + 1];
+        v2 = f_accum[3 * n + 2];
+    }
+    const int H = sc->n_hits;
+    for (int t0 = 0; t0 < H; t0 += STATIC_TILE) {
+        const int nt = min(STATIC_TILE, H - t0);
+        __syncthreads();
+        for (int k = threadIdx.x; k < nt; k += blockDim.x) {
+            const int s = sc->hit_list[t0 + k];
+            const long long fc = sc->hit[s];
+            t_node[k] = nodes[s];
+            for (int j = 0; j < 4; ++j) t_face[k][j] = faces[4 * fc + j];
+            for (int d = 0; d < 3; ++d) t_f[k][d] = sc->hit_force[3 * s + d];
+        }
+        __syncthreads();
+        if (live)
+            for (int k = 0; k < nt; ++k) {
+                if (t_node[k] == (uint32_t)n) {
+                    v0 += t_f[k][0];
+                    v1 += t_f[k][1];
+                    v2 += t_f[k][2];
+                }
+                for (int j = 0; j < 4; ++j)
+                    if (t_face[k][j] == (uint32_t)n) {
+                        v0 -= 0.25 * t_f[k][0];
+                        v1 -= 0.25 * t_f[k][1];
+                        v2 -= 0.25 * t_f[k][2];
+                    }
+            }
+    }
+    if (live) {
+        sc->occ[3 * o] = v0;
+        sc->occ[3 * o + 1] = v1;
+        sc->occ[3 * o + 2] = v2;
+    }
+}
+
+// Thread per occurrence: store the node's new value (every occurrence of a
+// node holds the same value, so repeated stores agree); thread 0 reports.
+__global__ void k_static_write(StaticContactScratch* sc, long long n_nodes, const uint32_t* __restrict__ nodes, long long n_faces,
+                               const uint32_t* __restrict__ faces, double* __restrict__ f_accum, int64_t* stats_count,
+                               double* stats_max, int* stats_status) {
+    const long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int err = sc->error;
+    if (o == 0) {
+        if (stats_count) *stats_count = err ? 0 : (int64_t)sc->pen_count;
+        if (stats_max) *stats_max = err ? 0.0 : __longlong_as_double((long long)sc->pen_max_bits);
+        if (stats_status) *stats_status = err ? -1 : 0;  // CRUSH_ERR_INVALID / CRUSH_OK
+    }
+    if (err || o >= n_nodes + 4 * n_faces) return;
+    const long long n = o < n_nodes ? nodes[o] : faces[o - n_nodes];
+    f_accum[3 * n] = sc->occ[3 * o];
+    f_accum[3 * n + 1] = sc->occ[3 * o + 1];
+    f_accum[3 * n + 2] = sc->occ[3 * o + 2];
+}
+
+}  // namespace
+
+void launch_contact_static(cudaStream_t s, StaticContactScratch* sc, long long n_model_nodes, const double* pos, const double* u,
+                           const double* masses, long long n_nodes, const uint32_t* nodes, const double* node_scale,
+                           long long n_faces, const uint32_t* faces, double stiffness, double max_distance, double dt,
+                           double* f_accum, int64_t* stats_count, double* stats_max, int* stats_status) {
+    k_static_prepare<<<1, STATIC_ONE_BLOCK, 0, s>>>(sc, n_model_nodes, pos, n_nodes, nodes, n_faces, faces, max_distance);
+    if (n_faces > 0) k_static_faces<<<(unsigned)blocks_for(n_faces, STATIC_TPB), STATIC_TPB, 0, s>>>(sc, pos, u, n_faces, faces, max_distance);
+    if (n_nodes > 0)
+        k_static_search<<<(unsigned)blocks_for(n_nodes * 32, STATIC_TPB), STATIC_TPB, 0, s>>>(
+            sc, pos, u, masses, n_nodes, nodes, node_scale, n_faces, stiffness, max_distance, dt);
+    k_static_compact<<<1, STATIC_ONE_BLOCK, 0, s>>>(sc, n_nodes);
+    const long long n_occ = n_nodes + 4 * n_faces;
+    if (n_occ > 0) k_static_occ<<<(unsigned)blocks_for(n_occ, STATIC_TPB), STATIC_TPB, 0, s>>>(sc, n_nodes, nodes, n_faces, faces, f_accum);
+    k_static_write<<<(unsigned)blocks_for(n_occ > 0 ? n_occ : 1, STATIC_TPB), STATIC_TPB, 0, s>>>(
+        sc, n_nodes, nodes, n_faces, faces, f_accum, stats_count, stats_max, stats_status);
+}
+
+}  // namespace crush

@@ -135,4 +135,29 @@ void launch_vehicle_sums(cudaStream_t s, const VehicleArrays& va, const double* 
                          double* out7);
 void launch_vehicle_vx(cudaStream_t s, const VehicleArrays& va, const double* mass, const double* v, Control* ctls);
 
+// Fixed-size scratch of the allocation-free contact call
+// (crush_contact_apply_static): one record in a static device array, so the
+// call needs no allocation. Limits: STATIC_MAX_NODES primary nodes (before
+// the bounding-box filter) and STATIC_MAX_FACES faces per call.
+constexpr int STATIC_MAX_NODES = 16384;
+constexpr int STATIC_MAX_FACES = 16384;
+constexpr int STATIC_MAX_OCC = STATIC_MAX_NODES + 4 * STATIC_MAX_FACES;  // node occurrences
+struct StaticContactScratch {
+    FaceGeo geo[STATIC_MAX_FACES];
+    double hit_force[3 * STATIC_MAX_NODES];
+    double occ[3 * STATIC_MAX_OCC];    // new force value of the node of each occurrence
+    int hit[STATIC_MAX_NODES];         // face hit by each primary node entry, or -1
+    int hit_list[STATIC_MAX_NODES];    // entries that hit, in entry order
+    double box_lo[3], box_hi[3];       // primary-node filter box (reference positions)
+    unsigned long long pen_count, pen_max_bits;
+    int n_hits;
+    int error;                         // 1: a node id was out of range (nothing is written)
+};
+
+// The call's kernels on `s`; every count is within the limits above.
+void launch_contact_static(cudaStream_t s, StaticContactScratch* sc, long long n_model_nodes, const double* pos, const double* u,
+                           const double* masses, long long n_nodes, const uint32_t* nodes, const double* node_scale,
+                           long long n_faces, const uint32_t* faces, double stiffness, double max_distance, double dt,
+                           double* f_accum, int64_t* stats_count, double* stats_max, int* stats_status);
+
 }  // namespace crush

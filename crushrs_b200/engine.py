@@ -160,6 +160,20 @@ class Context:
         return self._lib.crush_launch_count(self.h)
 
 
+def contact_apply_static(n_model_nodes, positions, u, masses, nodes, node_scale, faces, stiffness, max_distance, dt,
+                         f_accum, stats=None, stream=0):
+    """crush_contact_apply_static: one contact's penalty forces added into
+    f_accum, with no allocation and no context. Every array argument is a raw
+    device address (int) on the current device — nodes / faces as
+    (address, count) pairs, node_scale and stats may be None; `stream` is a
+    cudaStream_t address (0 = legacy default stream). Asynchronous."""
+    (nodes_ptr, n_nodes), (faces_ptr, n_faces) = nodes, faces
+    vp = C.c_void_p
+    check(lib().crush_contact_apply_static(n_model_nodes, vp(positions), vp(u), vp(masses), n_nodes, vp(nodes_ptr),
+                                           vp(node_scale), n_faces, vp(faces_ptr), stiffness, max_distance, dt,
+                                           vp(f_accum), vp(stats), vp(stream)))
+
+
 def run(desc, device=0):
     """crushrs::run on the GPU: results of a whole run of `desc`."""
     ctx = Context(desc, device)

@@ -269,6 +269,63 @@ int crush_batch_run(crush_ctx* ctx, crush_results* results);
  * drive all slots; *done = 1 once every slot has stopped). */
 int crush_batch_results(crush_ctx* ctx, int slot, crush_results* results);
 
+/* ---- allocation-free contact call ----
+ *
+ * No counterpart in the reference (its ContactRuntime::new + ::apply,
+ * src/contact.rs:48, :92, allocate their face list on every call). For
+ * callers that cannot allocate device memory at the point of the call: a
+ * solver step loop running inside another framework's memory pool (a
+ * cudaMalloc there fails or fragments the pool), or a serving loop
+ * overlapping many crashes on streams, where cudaMalloc / cudaFree would
+ * synchronise the device. It needs no context either.
+ *
+ * One ContactRuntime::new filter + ContactRuntime::apply for one contact on
+ * device buffers: primary nodes nodes_device[n_nodes] (model node ids) with
+ * optional penalty scales node_scale_device[n_nodes] (NULL = 1), quads
+ * faces_device[4 * n_faces], reference positions positions_device and
+ * displacements u_device (3 * n_model_nodes f64 each), lumped masses
+ * masses_device (n_model_nodes). The penalty forces are ADDED into
+ * f_accum_device (3 * n_model_nodes f64), each node's contributions in the
+ * reference's order starting from the value already there (zero it first for
+ * the contact's forces alone). With f_accum zero the result is bit-identical
+ * to crush_contact_apply of the same contact.
+ *
+ * Limits: n_nodes <= CRUSH_STATIC_MAX_NODES and n_faces <=
+ * CRUSH_STATIC_MAX_FACES; larger contacts are rejected with
+ * CRUSH_ERR_INVALID and a message (use crush_contact_apply). The primary-node
+ * search is exhaustive (cost n_nodes x n_faces).
+ *
+ * Memory: the call allocates nothing, host or device. Its scratch is one
+ * fixed-size record (about 5.4 MB) in this library's static device memory,
+ * one copy per device. The call clears what it uses at its start, so nothing
+ * needs zeroing by the caller. The FIRST call on each device resolves the
+ * record's address (cudaGetSymbolAddress, which may load the library's
+ * kernels onto the device): make that first call with the device current and
+ * before any stream capture. Every call on a device shares the one record, so
+ * calls that can overlap in time (other streams or threads without ordering
+ * between them) race and corrupt each other's results: serialise them.
+ *
+ * Asynchronous: six kernel launches on `stream` (a cudaStream_t; NULL = the
+ * legacy default stream) of the current device, no copy, no synchronisation.
+ * The host checks only sizes and arguments; node ids are checked on the
+ * device: an id >= n_model_nodes writes nothing and sets stats->status to
+ * CRUSH_ERR_INVALID. stats_device (device memory, may be NULL) receives the
+ * penetration count, the largest penetration and that status when the
+ * stream reaches the end of the call. */
+#define CRUSH_STATIC_MAX_NODES 16384
+#define CRUSH_STATIC_MAX_FACES 16384
+typedef struct crush_contact_stats {
+    int64_t penetration_count;
+    double max_penetration;
+    int32_t status;
+    int32_t reserved;
+} crush_contact_stats;
+int crush_contact_apply_static(int64_t n_model_nodes, const double* positions_device, const double* u_device,
+                               const double* masses_device, int64_t n_nodes, const uint32_t* nodes_device,
+                               const double* node_scale_device, int64_t n_faces, const uint32_t* faces_device,
+                               double stiffness, double max_distance, double dt, double* f_accum_device,
+                               crush_contact_stats* stats_device, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
