@@ -597,6 +597,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->alloc(&ca.overflow, (size_t)std::max(c->n_contacts, 1) * ca.overflow_cap));
     TRY(c->alloc(&ca.n_overflow, std::max(c->n_contacts, 1)));
     TRY(c->alloc(&ca.entry_overrun, std::max(c->n_contacts, 1)));
+    TRY(c->alloc(&ca.search_stats, 3 * (size_t)std::max(c->n_contacts, 1)));
     TRY(c->alloc(&ca.pen_count, std::max(c->n_contacts, 1)));
     TRY(c->alloc(&ca.pen_max_bits, std::max(c->n_contacts, 1)));
     TRY(c->upload_const(&ca.counts_for_stop, counts_for_stop));
@@ -617,6 +618,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     CK(cudaMemsetAsync(ca.counts, 0, sizeof(int) * std::max(tab_off.back(), 1), c->stream));
     CK(cudaMemsetAsync(ca.n_overflow, 0, sizeof(int) * std::max(c->n_contacts, 1), c->stream));
     CK(cudaMemsetAsync(ca.entry_overrun, 0, sizeof(int) * std::max(c->n_contacts, 1), c->stream));
+    CK(cudaMemsetAsync(ca.search_stats, 0, sizeof(unsigned long long) * 3 * std::max(c->n_contacts, 1), c->stream));
     CK(cudaMemsetAsync(ca.pen_count, 0, sizeof(unsigned long long) * std::max(c->n_contacts, 1), c->stream));
     CK(cudaMemsetAsync(ca.pen_max_bits, 0, sizeof(unsigned long long) * std::max(c->n_contacts, 1), c->stream));
     CK(cudaMemsetAsync(ca.face_hits, 0, sizeof(int) * std::max<long long>(c->n_faces, 1), c->stream));
@@ -1242,6 +1244,14 @@ int crush_batch_results(crush_ctx* c, int slot, crush_results* r) {
     if (!c || !r) return crush::fail(CRUSH_ERR_INVALID, "null argument");
     CK(cudaSetDevice(c->device));
     return results(c, slot, r);
+}
+
+int crush_contact_search_stats(crush_ctx* c, int id, uint64_t* out, int reset) {
+    if (!c || !out) return crush::fail(CRUSH_ERR_INVALID, "null argument");
+    if (id < 0 || id >= c->n_contacts) return crush::fail(CRUSH_ERR_INVALID, "contact id out of range");
+    CK(cudaMemcpyAsync(out, c->ca.search_stats + 3 * id, 3 * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
+    if (reset) CK(cudaMemsetAsync(c->ca.search_stats + 3 * id, 0, 3 * sizeof(uint64_t), c->stream));
+    return sync(c);
 }
 
 int crush_run_state(crush_ctx* c, double* u, double* v) {

@@ -793,6 +793,7 @@ __global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctls, 
             int slot = atomicAdd(&ca.n_overflow[c], 1);
             if (slot < ca.overflow_cap) ca.overflow[(long long)c * ca.overflow_cap + slot] = local;
             else ca.entry_overrun[c] = 1;
+            atomicAdd(&ca.search_stats[3 * c + 1], 1ull);
         }
         return;
     }
@@ -803,6 +804,7 @@ __global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctls, 
         const int b = tab + (int)(cell_hash(i, j, k) & mask);
         const int slot = atomicAdd(&ca.counts[b], 1);
         if (slot < BUCKET_CAP) ca.entries[(long long)b * BUCKET_CAP + slot] = local;
+        else atomicAdd(&ca.search_stats[3 * c + 2], 1ull);
     }
 }
 
@@ -880,6 +882,7 @@ __global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctls,
         const int b = tab + (int)(point_cell_hash(p, ca.cell[c]) & mask);
         const int cnt = grid ? ca.counts[b] : 0;
         if (!grid || cnt > BUCKET_CAP || ca.entry_overrun[c]) {
+            if (grid && lane == 0) atomicAdd(&ca.search_stats[3 * c], 1ull);
             const int nf = (int)(ca.face_off[c + 1] - fb);
             for (int f = lane; f < nf; f += SLAVE_LANES)
                 if (f < best && face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; }
@@ -925,19 +928,24 @@ __global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctls,
 }
 
 constexpr int MAX_NODE_EVENTS = 48;
+constexpr int GATHER_TPB = 128;
 
-// Ordered reaction gather, one thread per contact node: for each of its
-// contacts (in order) it collects its own hit (+F) and the hits on the faces
-// it belongs to (-F/4), sorts them by primary-node order (own before face for
-// the same primary node) and sums them in that order — the sequence in which
-// src/contact.rs:146-153 adds them to f_ext. Then clears the grid.
-__global__ void k_contact_gather(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, int c1, int run_mode,
-                                 double* __restrict__ f_out, int skip_fixed) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+// Ordered reaction gather, one warp per contact node: for each of its
+// contacts (in order) lane 0 collects the node's own hit (+F) and the hits on
+// the faces it belongs to (-F/4), sorts them by primary-node order (own
+// before face for the same primary node) and sums them in that order — the
+// sequence in which src/contact.rs:146-153 adds them to f_ext. When the
+// per-face hit lists overflowed, the whole warp walks the contact's primary
+// nodes in order instead, 32 at a time, and applies the matching hits in
+// order. Then the grid is cleared for the next build.
+__global__ void __launch_bounds__(GATHER_TPB) k_contact_gather(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, int c1,
+                                                               int run_mode, double* __restrict__ f_out, int skip_fixed) {
+    const long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // warp-uniform
+    const int lane = threadIdx.x & 31;
     if (i < ca.n_cnodes) {
         const long long n = ca.cnode[i];
         if (!(skip_fixed && nd.fixed[n]) && !(run_mode && ctls[nd.node_slot[n]].done)) {
-            double sx = 0.0, sy = 0.0, sz = 0.0;
+            double sx = 0.0, sy = 0.0, sz = 0.0;  // lane 0's sum
             bool touched = false;
             for (uint32_t r = ca.cnode_off[i]; r < ca.cnode_off[i + 1]; ++r) {
                 const int c = ca.crole_contact[r];
@@ -945,48 +953,81 @@ __global__ void k_contact_gather(ContactArrays ca, NodeArrays nd, Control* ctls,
                 touched = true;
                 const long long sb = ca.slave_off[c];
                 const int own = ca.crole_slave[r];
-                unsigned long long ev[MAX_NODE_EVENTS];
-                int ne = 0;
-                bool overflow = false;
-                if (own >= 0 && ca.hit[sb + own] >= 0) ev[ne++] = 2ull * (unsigned long long)(sb + own);
-                for (uint32_t q = ca.crole_faces_off[r]; q < ca.crole_faces_off[r + 1]; ++q) {
-                    const long long f = ca.face_off[c] + ca.crole_faces[q];
-                    const int cnt = ca.face_hits[f];
-                    if (cnt > FACE_HIT_CAP) { overflow = true; break; }
-                    for (int k = 0; k < cnt; ++k) {
-                        if (ne < MAX_NODE_EVENTS) ev[ne++] = 2ull * (unsigned long long)ca.face_list[f * FACE_HIT_CAP + k] + 1ull;
-                        else overflow = true;
+                int overflow = 0;
+                if (lane == 0) {
+                    unsigned long long ev[MAX_NODE_EVENTS];
+                    int ne = 0;
+                    if (own >= 0 && ca.hit[sb + own] >= 0) ev[ne++] = 2ull * (unsigned long long)(sb + own);
+                    for (uint32_t q = ca.crole_faces_off[r]; q < ca.crole_faces_off[r + 1] && !overflow; ++q) {
+                        const long long f = ca.face_off[c] + ca.crole_faces[q];
+                        const int cnt = ca.face_hits[f];
+                        if (cnt > FACE_HIT_CAP) {
+                            overflow = 1;
+                            break;
+                        }
+                        for (int k = 0; k < cnt; ++k) {
+                            if (ne < MAX_NODE_EVENTS) ev[ne++] = 2ull * (unsigned long long)ca.face_list[f * FACE_HIT_CAP + k] + 1ull;
+                            else overflow = 1;
+                        }
+                    }
+                    if (!overflow) {
+                        for (int a = 1; a < ne; ++a) {  // insertion sort, tiny lists
+                            unsigned long long key = ev[a];
+                            int b = a - 1;
+                            while (b >= 0 && ev[b] > key) { ev[b + 1] = ev[b]; --b; }
+                            ev[b + 1] = key;
+                        }
+                        for (int a = 0; a < ne; ++a) {
+                            const long long s = (long long)(ev[a] >> 1);
+                            const double fx = ca.hit_force[3 * s], fy = ca.hit_force[3 * s + 1], fz = ca.hit_force[3 * s + 2];
+                            if (ev[a] & 1ull) { sx -= 0.25 * fx; sy -= 0.25 * fy; sz -= 0.25 * fz; }
+                            else { sx += fx; sy += fy; sz += fz; }
+                        }
                     }
                 }
-                if (!overflow) {
-                    for (int a = 1; a < ne; ++a) {  // insertion sort, tiny lists
-                        unsigned long long key = ev[a];
-                        int b = a - 1;
-                        while (b >= 0 && ev[b] > key) { ev[b + 1] = ev[b]; --b; }
-                        ev[b + 1] = key;
-                    }
-                    for (int a = 0; a < ne; ++a) {
-                        const long long s = (long long)(ev[a] >> 1);
-                        const double fx = ca.hit_force[3 * s], fy = ca.hit_force[3 * s + 1], fz = ca.hit_force[3 * s + 2];
-                        if (ev[a] & 1ull) { sx -= 0.25 * fx; sy -= 0.25 * fy; sz -= 0.25 * fz; }
-                        else { sx += fx; sy += fy; sz += fz; }
-                    }
-                } else {
-                    // More events than the lists hold: walk the contact's
-                    // primary nodes in order instead.
+                overflow = __shfl_sync(0xffffffffu, overflow, 0);
+                if (overflow) {
+                    // More events than the lists hold: the warp walks the
+                    // contact's primary nodes in order, 32 per round; every
+                    // lane applies the round's matches in lane order, so all
+                    // lanes hold lane 0's running sum.
+                    double wx = __shfl_sync(0xffffffffu, sx, 0), wy = __shfl_sync(0xffffffffu, sy, 0),
+                           wz = __shfl_sync(0xffffffffu, sz, 0);
                     const long long se = ca.slave_off[c + 1];
                     const uint32_t* faces = ca.faces + 4 * ca.face_off[c];
-                    for (long long s = sb; s < se; ++s) {
-                        const int h = ca.hit[s];
-                        if (h < 0) continue;
-                        const double fx = ca.hit_force[3 * s], fy = ca.hit_force[3 * s + 1], fz = ca.hit_force[3 * s + 2];
-                        if (s - sb == own) { sx += fx; sy += fy; sz += fz; }
-                        const uint32_t* qn = faces + 4 * (long long)h;
-                        if (qn[0] == n || qn[1] == n || qn[2] == n || qn[3] == n) { sx -= 0.25 * fx; sy -= 0.25 * fy; sz -= 0.25 * fz; }
+                    for (long long s0 = sb; s0 < se; s0 += 32) {
+                        const long long s = s0 + lane;
+                        int kind = 0;  // bit 0: own hit, bit 1: hit on a face containing n
+                        double fx = 0.0, fy = 0.0, fz = 0.0;
+                        if (s < se) {
+                            const int h = ca.hit[s];
+                            if (h >= 0) {
+                                const uint32_t* qn = faces + 4 * (long long)h;
+                                kind = (s - sb == own ? 1 : 0) | ((qn[0] == n || qn[1] == n || qn[2] == n || qn[3] == n) ? 2 : 0);
+                                if (kind) {
+                                    fx = ca.hit_force[3 * s];
+                                    fy = ca.hit_force[3 * s + 1];
+                                    fz = ca.hit_force[3 * s + 2];
+                                }
+                            }
+                        }
+                        unsigned m = __ballot_sync(0xffffffffu, kind != 0);
+                        while (m) {
+                            const int l = __ffs(m) - 1;
+                            m &= m - 1;
+                            const int k = __shfl_sync(0xffffffffu, kind, l);
+                            const double gx = __shfl_sync(0xffffffffu, fx, l), gy = __shfl_sync(0xffffffffu, fy, l),
+                                         gz = __shfl_sync(0xffffffffu, fz, l);
+                            if (k & 1) { wx += gx; wy += gy; wz += gz; }
+                            if (k & 2) { wx -= 0.25 * gx; wy -= 0.25 * gy; wz -= 0.25 * gz; }
+                        }
                     }
+                    sx = wx;
+                    sy = wy;
+                    sz = wz;
                 }
             }
-            if (touched) {
+            if (touched && lane == 0) {
                 f_out[3 * n] = sx;
                 f_out[3 * n + 1] = sy;
                 f_out[3 * n + 2] = sz;
@@ -994,9 +1035,10 @@ __global__ void k_contact_gather(ContactArrays ca, NodeArrays nd, Control* ctls,
         }
     }
     // Clear the grid for the next build.
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long nthreads = (long long)gridDim.x * blockDim.x;
-    for (long long k = ca.tab_off[c0] + i; k < ca.tab_off[c1]; k += nthreads) ca.counts[k] = 0;
-    for (long long c = c0 + i; c < c1; c += nthreads) {
+    for (long long k = ca.tab_off[c0] + t; k < ca.tab_off[c1]; k += nthreads) ca.counts[k] = 0;
+    for (long long c = c0 + t; c < c1; c += nthreads) {
         ca.n_overflow[c] = 0;
         ca.entry_overrun[c] = 0;
     }
@@ -1148,7 +1190,8 @@ void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& n
     if (n_slaves > 0)
         k_contact_slaves<<<(unsigned)blocks_for(n_slaves * SLAVE_LANES, TPB), TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses);
     long long nodes = ca.n_cnodes > 0 ? ca.n_cnodes : 1;
-    k_contact_gather<<<(unsigned)blocks_for(nodes, 128), 128, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, f_out, skip_fixed);
+    k_contact_gather<<<(unsigned)blocks_for(nodes * 32, GATHER_TPB), GATHER_TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, f_out,
+                                                                                        skip_fixed);
 }
 
 }  // namespace crush

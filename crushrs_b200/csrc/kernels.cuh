@@ -78,6 +78,9 @@ struct ContactArrays {
     int* overflow;              // per contact: faces whose key box spans too many cells
     int* n_overflow;            // per contact
     int* entry_overrun;         // per contact flag: overflow list full (search every face)
+    unsigned long long* search_stats;  // 3 per contact, accumulated: primary nodes that searched every
+                                       // face (full bucket / overrun), faces put on the overflow list,
+                                       // bucket inserts dropped at BUCKET_CAP
     int overflow_cap;           // per contact capacity of overflow
     unsigned long long* pen_count;  // per contact, per step
     unsigned long long* pen_max_bits;

@@ -159,6 +159,12 @@ class Context:
     def launches(self):
         return self._lib.crush_launch_count(self.h)
 
+    def contact_search_stats(self, contact_id, reset=False):
+        """(fallback searches, overflow faces, dropped grid inserts) of a contact."""
+        out = (C.c_uint64 * 3)()
+        check(self._lib.crush_contact_search_stats(self.h, contact_id, out, int(reset)))
+        return tuple(out)
+
 
 def contact_apply_static(n_model_nodes, positions, u, masses, nodes, node_scale, faces, stiffness, max_distance, dt,
                          f_accum, stats=None, stream=0):

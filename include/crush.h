@@ -244,6 +244,13 @@ int crush_run_results(crush_ctx* ctx, crush_results* results);
 int crush_run_state(crush_ctx* ctx, double* u, double* v);
 /* Kernel launches issued by this context since creation. */
 int64_t crush_launch_count(const crush_ctx* ctx);
+/* Broad-phase statistics of contact `contact_id` accumulated since creation
+ * (or the last reset): out[0] primary-node searches that fell back to every
+ * face of the contact (full grid bucket or overflow list), out[1] faces put
+ * on the overflow list (key box over too many cells), out[2] grid inserts
+ * dropped at a full bucket. No counterpart in the reference (whose search
+ * is exhaustive). reset != 0 zeroes them after reading. */
+int crush_contact_search_stats(crush_ctx* ctx, int contact_id, uint64_t* out, int reset);
 
 /* ---- batched contexts: many crash models in one context ----
  *
