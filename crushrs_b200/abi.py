@@ -203,6 +203,7 @@ def declare_engine_api(lib):
     lib.crush_run_steps_timed.argtypes = [vp, C.c_int64, P(C.c_int), dp, dp, P(C.c_int)]
     lib.crush_set_profiling.argtypes = [vp, C.c_int]
     lib.crush_contact_search_stats.argtypes = [vp, C.c_int, P(C.c_uint64), C.c_int]
+    lib.crush_set_contact_search.argtypes = [vp, C.c_int]
     lib.crush_batch_create.argtypes = [P(P(ModelDesc)), C.c_int, C.c_int, P(vp)]
     lib.crush_batch_size.argtypes = [vp]
     lib.crush_batch_run.argtypes = [vp, P(Results)]

@@ -89,4 +89,86 @@ __device__ __forceinline__ float4 ld_plane(const float4* __restrict__ planes, lo
     return __ldg(planes + p * stride + e);
 }
 
+// ---------------- contact broad phase, shared by the kernels and the host ----------------
+// Hash of grid cell (i, j, k) of grid level `level` (cell size cell * 4^level).
+__host__ __device__ __forceinline__ unsigned cell_hash(long long i, long long j, long long k, int level) {
+    unsigned long long h = (unsigned long long)i * 73856093ull ^ (unsigned long long)j * 19349663ull ^
+                           (unsigned long long)k * 83492791ull ^ (unsigned long long)level * 2654435761ull;
+    return (unsigned)(h ^ (h >> 29));
+}
+
+// Grid key box of a face at corners x (unit normal n, centre c): a box that
+// contains every point the narrow test (src/contact.rs:113-128) can accept.
+// A hit needs the point p inside the face box +- md, signed = n.(p - c) in
+// [-md, 0], and proj = p - n signed (on the face plane) passing
+// point_in_triangle for one of the triangles 012, 023, 123, 130. That test
+// takes the barycentric coordinates of proj's orthogonal projection onto the
+// triangle's plane, with tolerance 0.1: the projection lies in the triangle
+// scaled 1.3x about its centroid. The face-plane points that project into
+// that scaled triangle form the triangle whose corners are the scaled
+// corners moved along the triangle normal onto the face plane (unbounded
+// when the two planes are perpendicular). So the key box is the box of those
+// corners over the four triangles, extended by md along -n, grown by a
+// rounding margin and clipped to the face box +- md (which alone bounds it).
+// Degenerate triangles accept nothing and are skipped.
+__host__ __device__ inline void face_key_box(const double x[4][3], const double n[3], const double c[3], double md, double* klo,
+                                             double* khi) {
+    double flo[3], fhi[3];
+    for (int d = 0; d < 3; ++d) {
+        double lo = x[0][d], hi = x[0][d];
+        for (int k = 1; k < 4; ++k) {
+            lo = fmin(lo, x[k][d]);
+            hi = fmax(hi, x[k][d]);
+        }
+        flo[d] = lo;
+        fhi[d] = hi;
+        klo[d] = lo + -md;  // the narrow test's face box
+        khi[d] = hi + md;
+    }
+    const int tri[4][3] = {{0, 1, 2}, {0, 2, 3}, {1, 2, 3}, {1, 3, 0}};
+    double rlo[3] = {1e300, 1e300, 1e300}, rhi[3] = {-1e300, -1e300, -1e300};
+    for (int t = 0; t < 4; ++t) {
+        const double* a = x[tri[t][0]];
+        const double* b = x[tri[t][1]];
+        const double* e = x[tri[t][2]];
+        double u[3], v[3];
+        for (int d = 0; d < 3; ++d) {
+            u[d] = b[d] - a[d];
+            v[d] = e[d] - a[d];
+        }
+        double m[3] = {u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]};
+        const double len = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+        if (!(len > 0.0)) continue;  // degenerate (or non-finite): accepts nothing
+        for (int d = 0; d < 3; ++d) m[d] /= len;
+        const double dn = n[0] * m[0] + n[1] * m[1] + n[2] * m[2];
+        if (!(fabs(dn) > 1e-6)) return;  // nearly perpendicular planes: keep the face box +- md
+        double cen[3];
+        for (int d = 0; d < 3; ++d) cen[d] = (a[d] + b[d] + e[d]) / 3.0;
+        const double* corner[3] = {a, b, e};
+        for (int k = 0; k < 3; ++k) {
+            double w[3];
+            for (int d = 0; d < 3; ++d) w[d] = cen[d] + 1.3001 * (corner[k][d] - cen[d]);
+            const double tt = (n[0] * (c[0] - w[0]) + n[1] * (c[1] - w[1]) + n[2] * (c[2] - w[2])) / dn;
+            for (int d = 0; d < 3; ++d) {
+                const double q = w[d] + tt * m[d];
+                rlo[d] = fmin(rlo[d], q);
+                rhi[d] = fmax(rhi[d], q);
+            }
+        }
+    }
+    if (!(rlo[0] <= rhi[0])) {  // every triangle degenerate: no point can hit
+        for (int d = 0; d < 3; ++d) {
+            klo[d] = 1.0;
+            khi[d] = -1.0;
+        }
+        return;
+    }
+    const double ext = fmax(fmax(fhi[0] - flo[0], fhi[1] - flo[1]), fhi[2] - flo[2]);
+    for (int d = 0; d < 3; ++d) {
+        const double margin = 1e-7 * (1.0 + ext + md + fabs(rlo[d]) + fabs(rhi[d]));
+        klo[d] = fmax(klo[d], rlo[d] - md * fmax(n[d], 0.0) - margin);
+        khi[d] = fmin(khi[d], rhi[d] + md * fmax(-n[d], 0.0) + margin);
+    }
+}
+
 }  // namespace crush

@@ -92,7 +92,7 @@ size_t next_pow2(size_t x) {
 
 // Contacts with fewer faces than this are searched exhaustively by a warp per
 // primary node; larger ones get a hashed grid.
-constexpr int64_t GRID_MIN_FACES = 512;
+constexpr int64_t GRID_MIN_FACES = 256;
 
 struct Slot {
     crush_settings settings{};
@@ -141,8 +141,8 @@ struct crush_ctx {
     int n_contacts = 0;
     long long n_faces = 0, n_slaves = 0;
     std::vector<int> face_off_h, slave_off_h;
-    std::vector<std::vector<uint32_t>> contact_nodes_all;  // unfiltered primary nodes (for contact_dt)
-    std::vector<double> contact_stiffness;
+    std::vector<uint8_t> is_static_h;
+    std::vector<int> tab_off_h;
 
     // vehicles
     VehicleArrays va{};
@@ -437,20 +437,36 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     // ---- contacts (ContactRuntime::new, src/contact.rs:48-70) ----
     std::vector<int> face_off(1, 0), slave_off(1, 0), tab_off(1, 0), counts_for_stop, face_contact, slave_contact, contact_slot;
     std::vector<int> slot_contact_off(1, 0);
-    std::vector<uint32_t> faces, slaves;
+    std::vector<uint32_t> faces, slaves, dyn_faces;
     std::vector<double> scales, stiff, md, cell;
-    struct Role {
-        int c;
-        int slave;
-        std::vector<int> faces;
+    std::vector<uint8_t> is_static;
+    std::vector<long long> st_tab_off(1, 0);
+    std::vector<uint32_t> st_off;
+    std::vector<int> st_entries;
+    // Contact-node roles, built per slot: (node, contact, sequence) sorted
+    // gives, for every node, its contacts in order with its primary-node
+    // entries and the faces it belongs to (src/contact.rs:146-153 order).
+    struct RoleItem {
+        uint32_t node;
+        int contact;
+        int seq;
+        int slave;  // >= 0: primary-node entry index within the contact
+        int face;   // >= 0: local face index
     };
-    std::map<uint32_t, std::vector<Role>> roles;
+    std::vector<uint32_t> cnode, cnode_off(1, 0);
+    std::vector<int> crole_contact, crole_slave, crole_faces;
+    std::vector<uint8_t> crole_face;
+    std::vector<uint32_t> crole_faces_off(1, 0);
+    std::vector<RoleItem> items;
     int kc = 0;
     for (int sidx = 0; sidx < n_desc; ++sidx) {
         const crush_model_desc* d = descs[sidx];
-        const long long n0 = c->slots[sidx].node0;
-        c->slots[sidx].contact0 = kc;
-        c->slots[sidx].n_contacts = d->n_contacts;
+        Slot& sl = c->slots[sidx];
+        const long long n0 = sl.node0;
+        sl.contact0 = kc;
+        sl.n_contacts = d->n_contacts;
+        items.clear();
+        int seq = 0;
         for (int k = 0; k < d->n_contacts; ++k, ++kc) {
             const crush_contact& cd = d->contacts[k];
             if (cd.n_nodes < 0 || cd.n_faces < 0 || (cd.n_nodes > 0 && !cd.nodes) || (cd.n_faces > 0 && !cd.faces))
@@ -459,10 +475,9 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
             double lo[3] = {INF, INF, INF}, hi[3] = {-INF, -INF, -INF};
             bool stop = false;
             double ext = 0.0;
-            std::vector<std::array<double, 6>> keys;  // grid key box of each face at the reference positions
+            const size_t face0 = faces.size() / 4;
             for (int64_t f = 0; f < cd.n_faces; ++f) {
                 double flo[3] = {INF, INF, INF}, fhi[3] = {-INF, -INF, -INF};
-                double xs[4][3];
                 for (int j = 0; j < 4; ++j) {
                     uint32_t nl = cd.faces[4 * f + j];
                     if (nl >= (uint64_t)d->n_nodes) return crush::fail(CRUSH_ERR_INVALID, "contact face node out of range");
@@ -471,7 +486,6 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
                     if (!cm.fixed[n]) stop = true;
                     for (int dd = 0; dd < 3; ++dd) {
                         double p = cm.positions[3 * (size_t)n + dd];
-                        xs[j][dd] = p;
                         lo[dd] = std::fmin(lo[dd], p);
                         hi[dd] = std::fmax(hi[dd], p);
                         flo[dd] = std::fmin(flo[dd], p);
@@ -479,30 +493,16 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
                     }
                 }
                 face_contact.push_back(kc);
-                double fext = std::max({fhi[0] - flo[0], fhi[1] - flo[1], fhi[2] - flo[2]});
-                ext = std::max(ext, fext);
-                double e1[3], e2[3], nrm[3];
-                for (int dd = 0; dd < 3; ++dd) { e1[dd] = xs[1][dd] - xs[0][dd]; e2[dd] = xs[2][dd] - xs[0][dd]; }
-                nrm[0] = e1[1] * e2[2] - e1[2] * e2[1];
-                nrm[1] = e1[2] * e2[0] - e1[0] * e2[2];
-                nrm[2] = e1[0] * e2[1] - e1[1] * e2[0];
-                double len = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
-                std::array<double, 6> kb;
-                for (int dd = 0; dd < 3; ++dd) {
-                    double nd = len > 0.0 ? nrm[dd] / len : 0.0;
-                    kb[dd] = flo[dd] - 0.25 * fext - cd.max_distance * std::max(nd, 0.0);
-                    kb[3 + dd] = fhi[dd] + 0.25 * fext + cd.max_distance * std::max(-nd, 0.0);
-                }
-                keys.push_back(kb);
+                ext = std::max(ext, std::max({fhi[0] - flo[0], fhi[1] - flo[1], fhi[2] - flo[2]}));
             }
             for (int dd = 0; dd < 3; ++dd) { lo[dd] += -cd.max_distance; hi[dd] += cd.max_distance; }
-            std::vector<uint32_t> all_nodes;
             int kept = 0;
             for (int64_t i = 0; i < cd.n_nodes; ++i) {
                 uint32_t nl = cd.nodes[i];
                 if (nl >= (uint64_t)d->n_nodes) return crush::fail(CRUSH_ERR_INVALID, "contact node out of range");
                 uint32_t n = (uint32_t)(n0 + nl);
-                all_nodes.push_back(n);
+                // contact_dt over every listed node (src/solver.rs:217-223)
+                if (mass_h[n] > 0.0 && cd.stiffness > 0.0) sl.contact_dt = std::fmin(sl.contact_dt, 2.0 * std::sqrt(mass_h[n] / cd.stiffness));
                 bool inside = true;
                 for (int dd = 0; dd < 3; ++dd) {
                     double p = cm.positions[3 * (size_t)n + dd];
@@ -512,34 +512,97 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
                 slaves.push_back(n);
                 slave_contact.push_back(kc);
                 scales.push_back(cd.node_scale ? cd.node_scale[i] : 1.0);
-                roles[n].push_back(Role{kc, kept, {}});
+                items.push_back(RoleItem{n, kc, seq++, kept, -1});
                 ++kept;
             }
             for (int64_t f = 0; f < cd.n_faces; ++f)
-                for (int j = 0; j < 4; ++j) {
-                    uint32_t n = (uint32_t)(n0 + cd.faces[4 * f + j]);
-                    auto& r = roles[n];
-                    if (r.empty() || r.back().c != kc) r.push_back(Role{kc, -1, {}});
-                    if (r.back().faces.empty() || r.back().faces.back() != (int)f) r.back().faces.push_back((int)f);
-                }
-            c->contact_nodes_all.push_back(all_nodes);
-            c->contact_stiffness.push_back(cd.stiffness);
+                for (int j = 0; j < 4; ++j) items.push_back(RoleItem{(uint32_t)(n0 + cd.faces[4 * f + j]), kc, seq++, -1, (int)f});
             face_off.push_back(face_off.back() + (int)cd.n_faces);
             slave_off.push_back(slave_off.back() + kept);
-            // Grid cell: twice the largest face; table: twice the initial key-box
-            // cell count, a power of two. Small contacts get no grid.
-            const double cs = ext > 0.0 ? 2.0 * ext : 1.0;
-            size_t t = 0;
-            if (cd.n_faces >= GRID_MIN_FACES) {
-                size_t inserts = 0;
-                for (const auto& kb : keys) {
-                    size_t cells = 1;
-                    for (int dd = 0; dd < 3; ++dd) cells *= (size_t)(std::floor(kb[3 + dd] / cs) - std::floor(kb[dd] / cs) + 1.0);
-                    inserts += std::min<size_t>(cells, 1024);
+            const double cs = ext > 0.0 ? 2.0 * ext : 1.0;  // grid cell: twice the largest face
+            const bool stat = !stop && cd.n_faces > 0;
+            size_t t = 0, st = 0;
+            if (stat) {
+                // Exact hashed grid of the fixed faces, in CSR form.
+                std::vector<std::pair<uint32_t, int>> ins;  // (bucket before masking, face)
+                bool ok = true;
+                for (int64_t f = 0; f < cd.n_faces && ok; ++f) {
+                    double x[4][3], e1[3], e2[3], nr[3], ctr[3], klo[3], khi[3];
+                    for (int j = 0; j < 4; ++j)
+                        for (int dd = 0; dd < 3; ++dd) x[j][dd] = cm.positions[3 * (size_t)faces[4 * (face0 + f) + j] + dd];
+                    for (int dd = 0; dd < 3; ++dd) { e1[dd] = x[1][dd] - x[0][dd]; e2[dd] = x[2][dd] - x[0][dd]; }
+                    nr[0] = e1[1] * e2[2] - e1[2] * e2[1];
+                    nr[1] = e1[2] * e2[0] - e1[0] * e2[2];
+                    nr[2] = e1[0] * e2[1] - e1[1] * e2[0];
+                    const double len = std::sqrt(nr[0] * nr[0] + nr[1] * nr[1] + nr[2] * nr[2]);
+                    for (int dd = 0; dd < 3; ++dd) {
+                        nr[dd] = nr[dd] / len;
+                        ctr[dd] = (((x[0][dd] + x[1][dd]) + x[2][dd]) + x[3][dd]) / 4.0;
+                    }
+                    face_key_box(x, nr, ctr, cd.max_distance, klo, khi);
+                    long long r[6];
+                    double cells = 1.0;
+                    for (int dd = 0; dd < 3; ++dd) {
+                        if (!std::isfinite(klo[dd]) || !std::isfinite(khi[dd]) || std::fabs(klo[dd] / cs) > 4.0e15 ||
+                            std::fabs(khi[dd] / cs) > 4.0e15) {
+                            ok = false;
+                            break;
+                        }
+                        r[2 * dd] = (long long)std::floor(klo[dd] / cs);
+                        r[2 * dd + 1] = (long long)std::floor(khi[dd] / cs);
+                        cells *= (double)(r[2 * dd + 1] - r[2 * dd] + 1);
+                    }
+                    if (!ok || cells > 4096.0) { ok = false; break; }
+                    for (long long kz = r[4]; kz <= r[5]; ++kz)
+                        for (long long jy = r[2]; jy <= r[3]; ++jy)
+                            for (long long ix = r[0]; ix <= r[1]; ++ix) ins.push_back({cell_hash(ix, jy, kz, 0), (int)f});
                 }
-                t = next_pow2(std::max<size_t>(1024, 2 * inserts));
+                if (ok) {
+                    st = next_pow2(std::max<size_t>(16, 2 * ins.size()));
+                    std::vector<uint32_t> cnt(st + 1, 0);
+                    for (auto& e : ins) cnt[(e.first & (st - 1)) + 1]++;
+                    const uint32_t base = (uint32_t)st_entries.size();
+                    for (size_t b2 = 0; b2 < st; ++b2) cnt[b2 + 1] += cnt[b2];
+                    std::vector<int> ent(ins.size());
+                    std::vector<uint32_t> cur(cnt.begin(), cnt.end() - 1);
+                    for (auto& e : ins) ent[cur[e.first & (st - 1)]++] = e.second;  // faces ascending within a bucket
+                    for (size_t b2 = 0; b2 <= st; ++b2) st_off.push_back(base + cnt[b2]);
+                    st_entries.insert(st_entries.end(), ent.begin(), ent.end());
+                } else {
+                    st = 0;
+                    st_off.push_back((uint32_t)st_entries.size());
+                }
+            } else {
+                st_off.push_back((uint32_t)st_entries.size());
+                for (int64_t f = 0; f < cd.n_faces; ++f) dyn_faces.push_back((uint32_t)(face0 + f));
+                if (cd.n_faces >= GRID_MIN_FACES) {
+                    // Hierarchical table: four times the level-0 key-box cells
+                    // of the faces at the reference positions, a power of two.
+                    size_t inserts = 0;
+                    for (int64_t f = 0; f < cd.n_faces; ++f) {
+                        double x[4][3], e1[3], e2[3], nr[3], ctr[3], klo[3], khi[3];
+                        for (int j = 0; j < 4; ++j)
+                            for (int dd = 0; dd < 3; ++dd) x[j][dd] = cm.positions[3 * (size_t)faces[4 * (face0 + f) + j] + dd];
+                        for (int dd = 0; dd < 3; ++dd) { e1[dd] = x[1][dd] - x[0][dd]; e2[dd] = x[2][dd] - x[0][dd]; }
+                        nr[0] = e1[1] * e2[2] - e1[2] * e2[1];
+                        nr[1] = e1[2] * e2[0] - e1[0] * e2[2];
+                        nr[2] = e1[0] * e2[1] - e1[1] * e2[0];
+                        const double len = std::sqrt(nr[0] * nr[0] + nr[1] * nr[1] + nr[2] * nr[2]);
+                        for (int dd = 0; dd < 3; ++dd) {
+                            nr[dd] = len > 0.0 ? nr[dd] / len : 0.0;
+                            ctr[dd] = (((x[0][dd] + x[1][dd]) + x[2][dd]) + x[3][dd]) / 4.0;
+                        }
+                        face_key_box(x, nr, ctr, cd.max_distance, klo, khi);
+                        double cells = 1.0;
+                        for (int dd = 0; dd < 3; ++dd) cells *= std::floor(khi[dd] / cs) - std::floor(klo[dd] / cs) + 1.0;
+                        inserts += (size_t)std::min(std::isfinite(cells) && cells > 0.0 ? cells : 0.0, (double)LEVEL_CELL_BUDGET);
+                    }
+                    t = next_pow2(std::max<size_t>(1024, 4 * inserts));
+                }
             }
             tab_off.push_back(tab_off.back() + (int)t);
+            st_tab_off.push_back(st_tab_off.back() + (long long)st);
+            is_static.push_back(stat && st > 0 ? 1 : 0);
             stiff.push_back(cd.stiffness);
             md.push_back(cd.max_distance);
             cell.push_back(cs);
@@ -547,27 +610,58 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
             contact_slot.push_back(sidx);
         }
         slot_contact_off.push_back(kc);
+        // Roles of this slot's nodes.
+        std::sort(items.begin(), items.end(), [](const RoleItem& x, const RoleItem& y) {
+            return x.node != y.node ? x.node < y.node : (x.contact != y.contact ? x.contact < y.contact : x.seq < y.seq);
+        });
+        for (size_t i0 = 0; i0 < items.size();) {
+            size_t i1 = i0;
+            while (i1 < items.size() && items[i1].node == items[i0].node) ++i1;
+            cnode.push_back(items[i0].node);
+            for (size_t a0 = i0; a0 < i1;) {
+                size_t a1 = a0;
+                while (a1 < i1 && items[a1].contact == items[a0].contact) ++a1;
+                // One role per primary-node entry (or one without), the faces on the last.
+                int n_slave_roles = 0;
+                for (size_t q = a0; q < a1; ++q) n_slave_roles += items[q].slave >= 0;
+                const int n_roles = std::max(n_slave_roles, 1);
+                int made = 0;
+                for (size_t q = a0; q < a1 && made < n_slave_roles; ++q)
+                    if (items[q].slave >= 0) {
+                        ++made;
+                        crole_contact.push_back(items[a0].contact);
+                        crole_slave.push_back(items[q].slave);
+                        if (made < n_roles) {
+                            crole_face.push_back(0);
+                            crole_faces_off.push_back((uint32_t)crole_faces.size());
+                        }
+                    }
+                if (n_slave_roles == 0) {
+                    crole_contact.push_back(items[a0].contact);
+                    crole_slave.push_back(-1);
+                }
+                int last = -1;
+                bool any_face = false;
+                for (size_t q = a0; q < a1; ++q)
+                    if (items[q].face >= 0 && items[q].face != last) {
+                        crole_faces.push_back(items[q].face);
+                        last = items[q].face;
+                        any_face = true;
+                    }
+                crole_face.push_back(any_face ? 1 : 0);
+                crole_faces_off.push_back((uint32_t)crole_faces.size());
+                a0 = a1;
+            }
+            cnode_off.push_back((uint32_t)crole_contact.size());
+            i0 = i1;
+        }
     }
     c->n_contacts = kc;
     c->n_faces = face_off.back();
     c->n_slaves = slave_off.back();
     c->face_off_h = face_off;
     c->slave_off_h = slave_off;
-    std::vector<uint32_t> cnode, cnode_off(1, 0);
-    std::vector<int> crole_contact, crole_slave, crole_faces;
-    std::vector<uint8_t> crole_face;
-    std::vector<uint32_t> crole_faces_off(1, 0);
-    for (auto& kv : roles) {
-        cnode.push_back(kv.first);
-        for (auto& r : kv.second) {
-            crole_contact.push_back(r.c);
-            crole_slave.push_back(r.slave);
-            crole_face.push_back(r.faces.empty() ? 0 : 1);
-            crole_faces.insert(crole_faces.end(), r.faces.begin(), r.faces.end());
-            crole_faces_off.push_back((uint32_t)crole_faces.size());
-        }
-        cnode_off.push_back((uint32_t)crole_contact.size());
-    }
+    c->is_static_h = is_static;
     ContactArrays& ca = c->ca;
     ca.n_contacts = c->n_contacts;
     ca.n_slots = c->n_slots;
@@ -584,19 +678,36 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->upload_const(&ca.cell, cell));
     TRY(c->upload_const(&ca.tab_off, tab_off));
     TRY(c->alloc(&ca.counts, std::max(tab_off.back(), 1)));
-    TRY(c->alloc(&ca.entries, (size_t)std::max(tab_off.back(), 1) * BUCKET_CAP));
+    TRY(c->alloc(&ca.boff, std::max(tab_off.back(), 1)));
+    TRY(c->alloc(&ca.blen, std::max(tab_off.back(), 1)));
+    {
+        std::vector<long long> ent_off(1, 0);
+        std::vector<uint32_t> grid_faces;
+        for (int k = 0; k < kc; ++k) {
+            const bool g = tab_off[k + 1] > tab_off[k];
+            ent_off.push_back(ent_off.back() + (g ? (long long)(face_off[k + 1] - face_off[k]) * LEVEL_CELL_BUDGET : 0));
+            if (g)
+                for (int f = face_off[k]; f < face_off[k + 1]; ++f) grid_faces.push_back((uint32_t)f);
+        }
+        TRY(c->upload_const(&ca.ent_off, ent_off));
+        TRY(c->alloc(&ca.entries, (size_t)std::max<long long>(ent_off.back(), 1)));
+        ca.n_grid_faces = (long long)grid_faces.size();
+        TRY(c->upload_const(&ca.grid_faces, grid_faces));
+    }
+    TRY(c->alloc(&ca.ent_cursor, std::max(kc, 1)));
+    ca.n_buckets = tab_off.back();
+    ca.exhaustive = 0;
+    c->tab_off_h = tab_off;
     {
         int cap = 1;
-        for (int k = 0; k < c->n_contacts; ++k) cap = std::max(cap, face_off[k + 1] - face_off[k]);
-        ca.overflow_cap = cap;
-        // Overflow lists exist only for contacts with a grid.
-        size_t grid_contacts = 0;
-        for (int k = 0; k < c->n_contacts; ++k) grid_contacts += tab_off[k + 1] > tab_off[k];
-        if (grid_contacts == 0) ca.overflow_cap = 1;
+        for (int k = 0; k < c->n_contacts; ++k)
+            if (tab_off[k + 1] > tab_off[k]) cap = std::max(cap, face_off[k + 1] - face_off[k]);
+        ca.overflow_cap = cap;  // overflow lists exist only for contacts with a dynamic grid
     }
     TRY(c->alloc(&ca.overflow, (size_t)std::max(c->n_contacts, 1) * ca.overflow_cap));
     TRY(c->alloc(&ca.n_overflow, std::max(c->n_contacts, 1)));
     TRY(c->alloc(&ca.entry_overrun, std::max(c->n_contacts, 1)));
+    TRY(c->alloc(&ca.levels_used, std::max(c->n_contacts, 1)));
     TRY(c->alloc(&ca.search_stats, 3 * (size_t)std::max(c->n_contacts, 1)));
     TRY(c->alloc(&ca.pen_count, std::max(c->n_contacts, 1)));
     TRY(c->alloc(&ca.pen_max_bits, std::max(c->n_contacts, 1)));
@@ -615,9 +726,18 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->upload_const(&ca.slave_contact, slave_contact));
     TRY(c->upload_const(&ca.contact_slot, contact_slot));
     TRY(c->upload_const(&ca.slot_contact_off, slot_contact_off));
+    TRY(c->upload_const(&ca.is_static, is_static));
+    TRY(c->upload_const(&ca.st_tab_off, st_tab_off));
+    TRY(c->upload_const(&ca.st_off, st_off));
+    TRY(c->upload_const(&ca.st_entries, st_entries));
+    ca.n_dyn_faces = (long long)dyn_faces.size();
+    TRY(c->upload_const(&ca.dyn_faces, dyn_faces));
     CK(cudaMemsetAsync(ca.counts, 0, sizeof(int) * std::max(tab_off.back(), 1), c->stream));
     CK(cudaMemsetAsync(ca.n_overflow, 0, sizeof(int) * std::max(c->n_contacts, 1), c->stream));
     CK(cudaMemsetAsync(ca.entry_overrun, 0, sizeof(int) * std::max(c->n_contacts, 1), c->stream));
+    CK(cudaMemsetAsync(ca.levels_used, 0, sizeof(int) * std::max(c->n_contacts, 1), c->stream));
+    CK(cudaMemsetAsync(ca.ent_cursor, 0, sizeof(int) * std::max(c->n_contacts, 1), c->stream));
+    CK(cudaMemsetAsync(ca.blen, 0, sizeof(int) * std::max(tab_off.back(), 1), c->stream));
     CK(cudaMemsetAsync(ca.search_stats, 0, sizeof(unsigned long long) * 3 * std::max(c->n_contacts, 1), c->stream));
     CK(cudaMemsetAsync(ca.pen_count, 0, sizeof(unsigned long long) * std::max(c->n_contacts, 1), c->stream));
     CK(cudaMemsetAsync(ca.pen_max_bits, 0, sizeof(unsigned long long) * std::max(c->n_contacts, 1), c->stream));
@@ -663,14 +783,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->upload_const(&va.local, vlocal));
     TRY(c->alloc(&c->veh_out, 7 * std::max(va.n_vehicles, 1)));
 
-    // ---- time step per slot (src/solver.rs:214-228) ----
-    for (int sidx = 0; sidx < n_desc; ++sidx) {
-        Slot& sl = c->slots[sidx];
-        for (int k = sl.contact0; k < sl.contact0 + sl.n_contacts; ++k)
-            for (uint32_t n : c->contact_nodes_all[k])
-                if (mass_h[n] > 0.0 && c->contact_stiffness[k] > 0.0)
-                    sl.contact_dt = std::fmin(sl.contact_dt, 2.0 * std::sqrt(mass_h[n] / c->contact_stiffness[k]));
-    }
+    // ---- time step per slot (src/solver.rs:214-228; contact_dt above) ----
     launch_init_state(c->stream, c->n_hc, c->stride, c->state);
     TRY(check_launch(c));
     CK(cudaMemsetAsync(c->u_tmp, 0, sizeof(double) * 3 * N, c->stream));
@@ -735,8 +848,10 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
     }
     mark(1);
     if (c->n_contacts > 0) {
-        launch_contact(c->stream, c->ca, nd, c->ctls, 0, c->n_contacts, c->n_faces, c->n_slaves, 0.0, c->mass, c->f_ext, 1);
-        n += (c->n_faces > 0 ? 1 : 0) + (c->n_slaves > 0 ? 1 : 0) + 1;
+        launch_contact(c->stream, c->ca, nd, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 0.0, c->mass,
+                       c->f_ext, 1);
+        n += (c->ca.n_dyn_faces > 0 ? 1 : 0) + (c->ca.n_buckets > 0 && !c->ca.exhaustive ? (c->ca.n_grid_faces > 0 ? 2 : 1) : 0) +
+             (c->n_slaves > 0 ? 1 : 0) + 1;
     }
     mark(2);
     launch_half(c->stream, nd, c->ctls);
@@ -803,6 +918,10 @@ int run_begin(crush_ctx* c) {
     launch_forces(c->stream, c->el(), c->nd(), c->ctls, 0);
     launch_gather(c->stream, c->el(), c->nd(), c->f_int);
     st = check_launch(c, (c->n_hc > 0 ? 1 : 0) + 1);
+    if (st != CRUSH_OK) return st;
+    // Geometry of every contact face at u = 0; static faces keep it.
+    launch_contact_geometry(c->stream, c->ca, c->nd(), 0, c->n_contacts, 0, c->n_faces);
+    st = check_launch(c, c->n_faces > 0 ? 1 : 0);
     if (st != CRUSH_OK) return st;
     CK(cudaMemcpyAsync(c->ctls, h.data(), sizeof(Control) * h.size(), cudaMemcpyHostToDevice, c->stream));
     c->host_step = 0;
@@ -1085,9 +1204,17 @@ int crush_contact_apply(crush_ctx* c, int id, const double* u, const double* v, 
     NodeArrays nd = c->nd();
     nd.u = c->u_tmp;
     const long long nf = c->face_off_h[id + 1] - c->face_off_h[id], ns = c->slave_off_h[id + 1] - c->slave_off_h[id];
-    launch_contact(c->stream, c->ca, nd, c->ctls_aux, id, id + 1, nf, ns, dt, m, c->f_tmp, 0);
-    int st = check_launch(c, (nf > 0 ? 1 : 0) + (ns > 0 ? 1 : 0) + 1);
+    const long long bk0 = c->tab_off_h[id], bk1 = c->tab_off_h[id + 1];
+    launch_contact(c->stream, c->ca, nd, c->ctls_aux, id, id + 1, c->face_off_h[id], nf, ns, bk0, bk1, dt, m, c->f_tmp, 0);
+    int st = check_launch(c, (nf > 0 ? 1 : 0) + (bk1 > bk0 && !c->ca.exhaustive ? (nf > 0 ? 2 : 1) : 0) + (ns > 0 ? 1 : 0) + 1);
     if (st != CRUSH_OK) return st;
+    if (c->run_open && c->is_static_h[id]) {
+        // The call rebuilt the static faces' geometry at its own u: restore
+        // the open run's (static faces keep it for the whole run).
+        launch_contact_geometry(c->stream, c->ca, c->nd(), id, id + 1, c->face_off_h[id], nf);
+        st = check_launch(c);
+        if (st != CRUSH_OK) return st;
+    }
     std::vector<double> f(3 * c->n_nodes);
     unsigned long long cnt = 0, mp = 0;
     CK(cudaMemcpyAsync(f.data(), c->f_tmp, bytes, cudaMemcpyDeviceToHost, c->stream));
@@ -1244,6 +1371,18 @@ int crush_batch_results(crush_ctx* c, int slot, crush_results* r) {
     if (!c || !r) return crush::fail(CRUSH_ERR_INVALID, "null argument");
     CK(cudaSetDevice(c->device));
     return results(c, slot, r);
+}
+
+int crush_set_contact_search(crush_ctx* c, int exhaustive) {
+    if (!c || (exhaustive != 0 && exhaustive != 1)) return crush::fail(CRUSH_ERR_INVALID, "exhaustive must be 0 or 1");
+    if (c->ca.exhaustive != exhaustive) {
+        c->ca.exhaustive = exhaustive;
+        if (c->graph) {
+            cudaGraphExecDestroy(c->graph);
+            c->graph = nullptr;
+        }
+    }
+    return CRUSH_OK;
 }
 
 int crush_contact_search_stats(crush_ctx* c, int id, uint64_t* out, int reset) {

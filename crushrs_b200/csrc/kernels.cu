@@ -678,23 +678,16 @@ __global__ void k_step_end(Control* ctls, ContactArrays ca, VehicleArrays va, in
 }
 
 // ---------------------------------------------------------------------------
-// Node-to-face penalty contact (src/contact.rs:92-160): face geometry and a
-// hashed uniform grid rebuilt every step, first-hit (minimum face index)
-// search per primary node, and an ordered gather of the reactions.
+// Node-to-face penalty contact (src/contact.rs:92-160): face geometry, a
+// broad phase (a hierarchical hashed grid rebuilt every step for moving
+// faces, an exact grid built once for static ones), first-hit (minimum face
+// index) search per primary node, and an ordered gather of the reactions.
 // ---------------------------------------------------------------------------
-constexpr int MAX_CELLS_PER_FACE = 1024;
 
-__device__ __forceinline__ unsigned cell_hash(long long i, long long j, long long k) {
-    unsigned long long h = (unsigned long long)i * 73856093ull ^ (unsigned long long)j * 19349663ull ^
-                           (unsigned long long)k * 83492791ull;
-    return (unsigned)(h ^ (h >> 29));
-}
-
-// Grid cells covered by a box. False (the face goes to the contact's
-// overflow list) when the box is not finite or spans more than
-// MAX_CELLS_PER_FACE cells; each axis range is checked before any product,
-// so a loop over the returned range is always short.
-__device__ __forceinline__ bool box_cells(const double* lo, const double* hi, double cs, long long* r) {
+// Grid cells a box covers at cell size cs. False when the box is not finite
+// or covers more than `budget` cells; each axis range is checked before any
+// product, so a loop over the returned range is always short.
+__device__ __forceinline__ bool box_cells(const double* lo, const double* hi, double cs, long long* r, int budget) {
     for (int d = 0; d < 3; ++d)
         if (!isfinite(lo[d]) || !isfinite(hi[d]) || !(lo[d] <= hi[d])) return false;
     const double lim = 4.0e15;  // cell coordinates stay exact in f64 and far from long long overflow
@@ -707,41 +700,27 @@ __device__ __forceinline__ bool box_cells(const double* lo, const double* hi, do
     double prod = 1.0;
     for (int d = 0; d < 3; ++d) {
         const double span = a[2 * d + 1] - a[2 * d];
-        if (span < 0.0 || span >= MAX_CELLS_PER_FACE) return false;
+        if (span < 0.0 || span >= budget) return false;
         prod *= span + 1.0;
     }
-    if (prod > MAX_CELLS_PER_FACE) return false;
+    if (prod > budget) return false;
     for (int k = 0; k < 6; ++k) r[k] = (long long)a[k];
     return true;
 }
 
-// Cell of a point (any finite coordinates; non-finite points map to cell 0).
-__device__ __forceinline__ unsigned point_cell_hash(const double* p, double cs) {
+// Hash of the cell of a point (any finite coordinates; non-finite points map
+// to cell 0) at cell size cs and grid level `level`.
+__device__ __forceinline__ unsigned point_cell_hash(const double* p, double cs, int level) {
     long long q[3];
     for (int d = 0; d < 3; ++d) {
         double a = floor(p[d] / cs);
         q[d] = (isfinite(a) && fabs(a) <= 4.0e15) ? (long long)a : 0;
     }
-    return cell_hash(q[0], q[1], q[2]);
+    return cell_hash(q[0], q[1], q[2], level);
 }
 
-// Face geometry (src/contact.rs:95-110) and its insertion into the grid, one
-// warp per face (every lane derives the same geometry; the lanes split the
-// cells). The grid key box is a superset of every point the narrow test can
-// accept: a hit needs -max_distance <= signed <= 0, i.e. the point lies at
-// most max_distance behind its projection along -n, and the projection inside
-// one of the face's triangles with barycentric tolerance 0.1, i.e. within the
-// triangle scaled 1.3x about its centroid, which lies inside the face's box
-// grown by 0.2 of its largest extent. So the key box is the face box grown by
-// 0.25 x extent + 4 x warp on every side and by max_distance x n_d on the
-// inner side of axis d.
-__global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, int c1, int run_mode) {
-    const long long f = ca.face_off[c0] + (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31;
-    if (f >= ca.face_off[c1]) return;
-    const int c = ca.face_contact[f];
-    if (run_mode && ctls[ca.contact_slot[c]].done) return;
-    FaceGeo g;
+// Face geometry (src/contact.rs:95-110) at X + u.
+__device__ __forceinline__ void face_geometry(const ContactArrays& ca, const NodeArrays& nd, long long f, double md, FaceGeo& g) {
     for (int k = 0; k < 4; ++k) {
         long long n = ca.faces[4 * f + k];
         for (int d = 0; d < 3; ++d) g.x[k][d] = nd.pos[3 * n + d] + nd.u[3 * n + d];
@@ -756,8 +735,6 @@ __global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctls, 
     double nz = e1[0] * e2[1] - e1[1] * e2[0];
     double len = sqrt(nx * nx + ny * ny + nz * nz);
     g.n[0] = nx / len; g.n[1] = ny / len; g.n[2] = nz / len;
-    const double md = ca.max_distance[c];
-    double flo[3], fhi[3];
     for (int d = 0; d < 3; ++d) {
         g.c[d] = (((g.x[0][d] + g.x[1][d]) + g.x[2][d]) + g.x[3][d]) / 4.0;
         double lo = g.x[0][d], hi = g.x[0][d];
@@ -765,31 +742,53 @@ __global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctls, 
             lo = fmin(lo, g.x[k][d]);
             hi = fmax(hi, g.x[k][d]);
         }
-        flo[d] = lo;
-        fhi[d] = hi;
         g.lo[d] = lo + -md;
         g.hi[d] = hi + md;
     }
-    if (lane == 0) {
-        ca.geo[f] = g;
-        ca.face_hits[f] = 0;
-    }
-    const double ext = fmax(fmax(fhi[0] - flo[0], fhi[1] - flo[1]), fhi[2] - flo[2]);
-    double warp = 0.0;
-    for (int k = 0; k < 4; ++k)
-        warp = fmax(warp, fabs(g.n[0] * (g.x[k][0] - g.c[0]) + g.n[1] * (g.x[k][1] - g.c[1]) + g.n[2] * (g.x[k][2] - g.c[2])));
-    const double slack = 0.25 * ext + 4.0 * warp + 1e-9 * (1.0 + ext + md);
+}
+
+// The grid level and cell range of face f's key box (from its geometry):
+// returns the level, GRID_LEVELS for the overflow list, -1 for no insertion.
+__device__ __forceinline__ int face_cells(const ContactArrays& ca, const FaceGeo& g, int c, long long* r) {
     double klo[3], khi[3];
-    for (int d = 0; d < 3; ++d) {
-        klo[d] = fmax(flo[d] - slack - md * fmax(g.n[d], 0.0), g.lo[d]);
-        khi[d] = fmin(fhi[d] + slack + md * fmax(-g.n[d], 0.0), g.hi[d]);
-    }
-    const int local = (int)(f - ca.face_off[c]);
+    face_key_box(g.x, g.n, g.c, ca.max_distance[c], klo, khi);
+    if (klo[0] > khi[0] || klo[1] > khi[1] || klo[2] > khi[2]) return -1;  // no point can hit the face
+    double cs = ca.cell[c];
+    for (int level = 0; level < GRID_LEVELS; ++level, cs *= 4.0)
+        if (box_cells(klo, khi, cs, r, LEVEL_CELL_BUDGET)) return level;
+    return GRID_LEVELS;
+}
+
+// Thread per face. Pass 0: geometry; for faces of contacts with a dynamic
+// grid also the count of their key box's cells per bucket, or their place on
+// the overflow list. Pass 1 (grid faces only, after k_grid_alloc): the fill of
+// the buckets, which returns every count to zero. Pass 2: geometry only. The
+// faces are
+// face_list[0, n) when face_list is given, else face_off[c0] + [0, n).
+__global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, const uint32_t* __restrict__ face_list,
+                                long long n, int run_mode, int pass) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const long long f = face_list ? (long long)face_list[t] : ca.face_off[c0] + t;
+    const int c = ca.face_contact[f];
+    if (run_mode && ctls[ca.contact_slot[c]].done) return;
     const int tab = ca.tab_off[c];
-    if (ca.tab_off[c + 1] == tab) return;  // no grid: the contact is searched exhaustively
+    const bool grid = ca.tab_off[c + 1] > tab && !ca.exhaustive;
+    FaceGeo g;
+    if (pass != 1) {
+        face_geometry(ca, nd, f, ca.max_distance[c], g);
+        ca.geo[f] = g;
+        if (!grid || pass == 2) return;
+    } else {
+        if (!grid) return;
+        g = ca.geo[f];
+    }
     long long r[6];
-    if (!box_cells(klo, khi, ca.cell[c], r)) {
-        if (lane == 0) {
+    const int level = face_cells(ca, g, c, r);
+    if (level < 0) return;
+    const int local = (int)(f - ca.face_off[c]);
+    if (level == GRID_LEVELS) {
+        if (pass == 0) {
             int slot = atomicAdd(&ca.n_overflow[c], 1);
             if (slot < ca.overflow_cap) ca.overflow[(long long)c * ca.overflow_cap + slot] = local;
             else ca.entry_overrun[c] = 1;
@@ -797,15 +796,49 @@ __global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctls, 
         }
         return;
     }
+    if (pass == 0 && !(ca.levels_used[c] & (1 << level))) atomicOr(&ca.levels_used[c], 1 << level);
     const unsigned mask = (unsigned)(ca.tab_off[c + 1] - tab - 1);
-    const int ni = (int)(r[1] - r[0] + 1), nj = (int)(r[3] - r[2] + 1), nk = (int)(r[5] - r[4] + 1);
-    for (int q = lane; q < ni * nj * nk; q += 32) {
-        const long long i = r[0] + q % ni, j = r[2] + (q / ni) % nj, k = r[4] + q / (ni * nj);
-        const int b = tab + (int)(cell_hash(i, j, k) & mask);
-        const int slot = atomicAdd(&ca.counts[b], 1);
-        if (slot < BUCKET_CAP) ca.entries[(long long)b * BUCKET_CAP + slot] = local;
-        else atomicAdd(&ca.search_stats[3 * c + 2], 1ull);
+    for (long long k = r[4]; k <= r[5]; ++k)
+        for (long long j = r[2]; j <= r[3]; ++j)
+            for (long long i = r[0]; i <= r[1]; ++i) {
+                const int b = tab + (int)(cell_hash(i, j, k, level) & mask);
+                if (pass == 0) {
+                    atomicAdd(&ca.counts[b], 1);
+                } else {
+                    const int pos = atomicSub(&ca.counts[b], 1) - 1;
+                    ca.entries[ca.boff[b] + pos] = local;
+                }
+            }
+}
+
+// Thread per dynamic bucket: its range in the contact's entries, allocated
+// with one atomic per warp (a warp's buckets belong to one table, since tables
+// are multiples of 1024 buckets).
+__global__ void k_grid_alloc(ContactArrays ca, int c0, int c1) {
+    const long long b = (long long)ca.tab_off[c0] + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    if (b - lane >= ca.tab_off[c1]) return;  // warp-uniform
+    // the warp's contact: the last c with tab_off[c] <= b (binary search)
+    int lo = c0, hi = c1 - 1;
+    const long long b0 = b - lane;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (ca.tab_off[mid] <= b0) lo = mid;
+        else hi = mid - 1;
     }
+    const int c = lo;
+    const int cnt = ca.counts[b];
+    int incl = cnt;
+    for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += y;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    int base = 0;
+    if (lane == 0 && total > 0) base = atomicAdd(&ca.ent_cursor[c], total);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    ca.boff[b] = (unsigned)(ca.ent_off[c] + base + incl - cnt);
+    ca.blen[b] = cnt;
 }
 
 // src/contact.rs:29-43
@@ -844,11 +877,13 @@ __device__ __forceinline__ bool face_hit(const FaceGeo& g, const double* p, doub
 
 constexpr int SLAVE_LANES = 32;
 
-// First-hit search: SLAVE_LANES lanes per primary node test its grid bucket
-// and the contact's overflow faces — or every face of the contact when it has
-// no grid (small contacts) or the bucket overflowed — and keep the smallest
-// face index that hits: the face the reference's in-order scan with `break`
-// finds (src/contact.rs:115-157).
+// First-hit search: SLAVE_LANES lanes per primary node test the faces its
+// broad phase offers — the static grid's bucket, or the dynamic grid's bucket
+// at every level in use plus the contact's overflow faces — or every face of
+// the contact when it has no grid (small contacts), a dynamic bucket
+// overflowed, or this is a drop-in call on a static contact; and keep the
+// smallest face index that hits: the face the reference's in-order scan with
+// `break` finds (src/contact.rs:115-157).
 __global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, int c1, int run_mode, double dt_override,
                                  const double* __restrict__ masses) {
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -875,29 +910,47 @@ __global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctls,
         p[2] = nd.pos[3 * n + 2] + nd.u[3 * n + 2];
         md = ca.max_distance[c];
         const long long fb = ca.face_off[c];
+        const int nf = (int)(ca.face_off[c + 1] - fb);
         geo = ca.geo + fb;
+        const long long st0 = ca.st_tab_off[c], st1 = ca.st_tab_off[c + 1];
         const int tab = ca.tab_off[c];
-        const bool grid = ca.tab_off[c + 1] > tab;
-        const unsigned mask = grid ? (unsigned)(ca.tab_off[c + 1] - tab - 1) : 0u;
-        const int b = tab + (int)(point_cell_hash(p, ca.cell[c]) & mask);
-        const int cnt = grid ? ca.counts[b] : 0;
-        if (!grid || cnt > BUCKET_CAP || ca.entry_overrun[c]) {
-            if (grid && lane == 0) atomicAdd(&ca.search_stats[3 * c], 1ull);
-            const int nf = (int)(ca.face_off[c + 1] - fb);
-            for (int f = lane; f < nf; f += SLAVE_LANES)
+        const bool dyn_grid = ca.tab_off[c + 1] > tab;
+        bool all = false;
+        if (run_mode && st1 > st0 && !ca.exhaustive) {
+            // Static grid: the bucket of the point's cell, exact.
+            const unsigned mask = (unsigned)(st1 - st0 - 1);
+            const long long bk = st0 + (point_cell_hash(p, ca.cell[c], 0) & mask);
+            const uint32_t e0 = ca.st_off[bk + c], e1 = ca.st_off[bk + c + 1];
+            for (uint32_t k = e0 + lane; k < e1; k += SLAVE_LANES) {
+                const int f = ca.st_entries[k];
                 if (f < best && face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; }
-        } else {
-            const int* ent = ca.entries + (long long)b * BUCKET_CAP;
-            for (int k = lane; k < cnt; k += SLAVE_LANES) {
-                const int f = ent[k];
-                if (f < best && face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; }
+            }
+        } else if (dyn_grid && !ca.exhaustive && !ca.entry_overrun[c]) {
+            const unsigned mask = (unsigned)(ca.tab_off[c + 1] - tab - 1);
+            const int used = ca.levels_used[c];
+            double cs = ca.cell[c];
+            for (int level = 0; level < GRID_LEVELS; ++level, cs *= 4.0) {
+                if (!(used & (1 << level))) continue;
+                const int b = tab + (int)(point_cell_hash(p, cs, level) & mask);
+                const unsigned e0 = ca.boff[b];
+                const int cnt = ca.blen[b];
+                for (int k = lane; k < cnt; k += SLAVE_LANES) {
+                    const int f = ca.entries[e0 + k];
+                    if (f < best && face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; }
+                }
             }
             const int no = min(ca.n_overflow[c], ca.overflow_cap);
             for (int k = lane; k < no; k += SLAVE_LANES) {
                 const int f = ca.overflow[(long long)c * ca.overflow_cap + k];
                 if (f < best && face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; }
             }
+        } else {
+            all = true;
+            if (dyn_grid && !ca.exhaustive && lane == 0) atomicAdd(&ca.search_stats[3 * c], 1ull);
         }
+        if (all)
+            for (int f = lane; f < nf; f += SLAVE_LANES)
+                if (f < best && face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; }
     }
 #pragma unroll
     for (int off = SLAVE_LANES / 2; off > 0; off >>= 1) {
@@ -1037,10 +1090,11 @@ __global__ void __launch_bounds__(GATHER_TPB) k_contact_gather(ContactArrays ca,
     // Clear the grid for the next build.
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long nthreads = (long long)gridDim.x * blockDim.x;
-    for (long long k = ca.tab_off[c0] + t; k < ca.tab_off[c1]; k += nthreads) ca.counts[k] = 0;
     for (long long c = c0 + t; c < c1; c += nthreads) {
         ca.n_overflow[c] = 0;
         ca.entry_overrun[c] = 0;
+        ca.levels_used[c] = 0;
+        ca.ent_cursor[c] = 0;
     }
 }
 
@@ -1178,20 +1232,35 @@ void launch_vehicle_vx(cudaStream_t s, const VehicleArrays& va, const double* ma
     k_vehicle_vx<<<(unsigned)(va.n_vehicles * va.vx_blocks), VEH_TPB, 0, s>>>(va, mass, v, ctls);
 }
 
-// Contact pass over contacts [c0, c1): faces + grid, first-hit search, ordered
-// reaction gather into f_out. n_faces / n_slaves are the host-known totals of
-// that range. dt_override > 0 is the drop-in call (no run control).
-void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1,
-                    long long n_faces, long long n_slaves, double dt_override, const double* masses, double* f_out,
-                    int skip_fixed) {
+void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
+                    long long n_faces, long long n_slaves, long long bk0, long long bk1, double dt_override, const double* masses,
+                    double* f_out, int skip_fixed) {
     if (c1 <= c0) return;
     const int run_mode = dt_override > 0.0 ? 0 : 1;
-    if (n_faces > 0) k_contact_faces<<<(unsigned)blocks_for(n_faces * 32, TPB), TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode);
+    if (n_faces > 0) cudaMemsetAsync(ca.face_hits + f0, 0, sizeof(int) * n_faces, s);
+    // run: only moving faces (static ones keep their geometry); drop-in: every face of the range
+    const uint32_t* list = run_mode ? ca.dyn_faces : nullptr;
+    const long long n_list = run_mode ? ca.n_dyn_faces : n_faces;
+    if (n_list > 0) k_contact_faces<<<(unsigned)blocks_for(n_list, TPB), TPB, 0, s>>>(ca, nd, ctls, c0, list, n_list, run_mode, 0);
+    if (bk1 > bk0 && !ca.exhaustive) {
+        k_grid_alloc<<<(unsigned)blocks_for(bk1 - bk0, TPB), TPB, 0, s>>>(ca, c0, c1);
+        const uint32_t* glist = run_mode ? ca.grid_faces : nullptr;
+        const long long n_glist = run_mode ? ca.n_grid_faces : n_faces;
+        if (n_glist > 0)
+            k_contact_faces<<<(unsigned)blocks_for(n_glist, TPB), TPB, 0, s>>>(ca, nd, ctls, c0, glist, n_glist, run_mode, 1);
+    }
     if (n_slaves > 0)
         k_contact_slaves<<<(unsigned)blocks_for(n_slaves * SLAVE_LANES, TPB), TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses);
     long long nodes = ca.n_cnodes > 0 ? ca.n_cnodes : 1;
     k_contact_gather<<<(unsigned)blocks_for(nodes * 32, GATHER_TPB), GATHER_TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, f_out,
                                                                                         skip_fixed);
+}
+
+void launch_contact_geometry(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, int c0, int c1, long long f0,
+                             long long n_faces) {
+    (void)f0;
+    if (c1 <= c0 || n_faces <= 0) return;
+    k_contact_faces<<<(unsigned)blocks_for(n_faces, TPB), TPB, 0, s>>>(ca, nd, nullptr, c0, nullptr, n_faces, 0, 2);
 }
 
 }  // namespace crush

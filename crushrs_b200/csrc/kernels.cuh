@@ -52,12 +52,17 @@ struct FaceGeo {
     double hi[3];
 };
 
-// Grid buckets hold up to BUCKET_CAP faces (a fuller bucket makes its
-// primary nodes test every face of the contact); per-face hit lists hold
-// FACE_HIT_CAP primary nodes (fuller lists make the gather walk the contact's
-// primary nodes in order).
-constexpr int BUCKET_CAP = 64;
+// Per-face hit lists hold FACE_HIT_CAP primary nodes (fuller lists make the
+// gather walk the contact's primary nodes in order).
 constexpr int FACE_HIT_CAP = 8;
+// Dynamic grids are hashed and hierarchical: level l has cells of size
+// cell * 4^l, and a face goes into the finest level where its key box covers
+// at most LEVEL_CELL_BUDGET cells (beyond the last level, or not finite: the
+// overflow list). Buckets are exact CSR ranges rebuilt every step (count,
+// allocate, fill), so a contact needs at most faces x LEVEL_CELL_BUDGET
+// entries and no bucket ever overflows.
+constexpr int GRID_LEVELS = 6;
+constexpr int LEVEL_CELL_BUDGET = 64;
 
 struct ContactArrays {
     int n_contacts;
@@ -72,15 +77,19 @@ struct ContactArrays {
     const double* stiffness;    // per contact
     const double* max_distance; // per contact
     const double* cell;         // per contact grid cell size
-    const int* tab_off;         // n_contacts+1, hash tables concatenated (each a power of two)
-    int* counts;                // per bucket: faces inserted this step
-    int* entries;               // BUCKET_CAP local face indices per bucket
+    const int* tab_off;         // n_contacts+1, hash tables concatenated (each a power of two, >= 1024)
+    int* counts;                // per bucket: faces to insert this step (zero again after the fill)
+    unsigned* boff;             // per bucket: start of its range in entries
+    int* blen;                  // per bucket: length of its range
+    const long long* ent_off;   // n_contacts+1: entry capacity ranges (faces x LEVEL_CELL_BUDGET)
+    int* ent_cursor;            // per contact: entries allocated this step
+    int* entries;               // local face indices
     int* overflow;              // per contact: faces whose key box spans too many cells
     int* n_overflow;            // per contact
     int* entry_overrun;         // per contact flag: overflow list full (search every face)
-    unsigned long long* search_stats;  // 3 per contact, accumulated: primary nodes that searched every
-                                       // face (full bucket / overrun), faces put on the overflow list,
-                                       // bucket inserts dropped at BUCKET_CAP
+    unsigned long long* search_stats;  // 3 per contact, accumulated: primary-node searches that tested
+                                       // every face of a contact with a grid (overflow list overrun),
+                                       // faces put on the overflow list, (unused: 0)
     int overflow_cap;           // per contact capacity of overflow
     unsigned long long* pen_count;  // per contact, per step
     unsigned long long* pen_max_bits;
@@ -101,6 +110,19 @@ struct ContactArrays {
     const int* contact_slot;    // crash slot of each contact
     const int* slot_contact_off;// n_slots+1: contacts of each crash slot
     int n_slots;
+    int* levels_used;           // per contact: bit l set when a face went to grid level l this step
+    // Static contacts (every face node fixed): geometry computed once per run
+    // and an exact hashed grid built at set-up, in CSR form.
+    const uint8_t* is_static;   // per contact
+    const long long* st_tab_off;// n_contacts+1: bucket ranges of the static tables (power of two each, or 0)
+    const uint32_t* st_off;     // per bucket + 1 per table: CSR offsets into st_entries
+    const int* st_entries;      // local face indices, ascending within a bucket
+    const uint32_t* dyn_faces;  // global indices of the faces of non-static contacts
+    long long n_dyn_faces;
+    const uint32_t* grid_faces; // global indices of the faces of contacts with a dynamic grid
+    long long n_grid_faces;
+    long long n_buckets;        // total dynamic buckets (tab_off[n_contacts])
+    int exhaustive;             // 1: every search tests every face of its contact (no broad phase)
 };
 
 // Vehicles of all crash slots: node lists and the reduction layout.
@@ -131,9 +153,17 @@ void launch_dt_finalize(cudaStream_t s, Control* ctls, int n_slots);
 void launch_mass_scaling(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, int force_apply);
 void launch_nonfinite(cudaStream_t s, const NodeArrays& nd, Control* ctls);
 void launch_step_end(cudaStream_t s, Control* ctls, const ContactArrays& ca, const VehicleArrays& va, int check_separation);
-void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1,
-                    long long n_faces, long long n_slaves, double dt_override, const double* masses, double* f_out,
-                    int skip_fixed);
+// Contact pass over contacts [c0, c1) (faces [f0, f0 + n_faces), n_slaves
+// primary-node entries, dynamic grid buckets [bk0, bk1)). dt_override > 0 is a drop-in call: every face's
+// geometry is rebuilt and static contacts are searched exhaustively; the run
+// (dt_override = 0) rebuilds only the dynamic faces and uses the static grids.
+void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
+                    long long n_faces, long long n_slaves, long long bk0, long long bk1, double dt_override, const double* masses,
+                    double* f_out, int skip_fixed);
+// Geometry of every face of contacts [c0, c1) at X + u (no grid insertion):
+// the static contacts' geometry for a run.
+void launch_contact_geometry(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, int c0, int c1, long long f0,
+                             long long n_faces);
 void launch_vehicle_sums(cudaStream_t s, const VehicleArrays& va, const double* mass, const double* v, const double* v0,
                          double* out7);
 void launch_vehicle_vx(cudaStream_t s, const VehicleArrays& va, const double* mass, const double* v, Control* ctls);

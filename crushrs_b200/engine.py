@@ -159,8 +159,12 @@ class Context:
     def launches(self):
         return self._lib.crush_launch_count(self.h)
 
+    def set_contact_search(self, exhaustive):
+        """True: every contact search tests every face (no broad phase)."""
+        check(self._lib.crush_set_contact_search(self.h, int(bool(exhaustive))))
+
     def contact_search_stats(self, contact_id, reset=False):
-        """(fallback searches, overflow faces, dropped grid inserts) of a contact."""
+        """(exhaustive fallback searches, overflow faces, reserved) of a contact."""
         out = (C.c_uint64 * 3)()
         check(self._lib.crush_contact_search_stats(self.h, contact_id, out, int(reset)))
         return tuple(out)

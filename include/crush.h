@@ -245,12 +245,17 @@ int crush_run_state(crush_ctx* ctx, double* u, double* v);
 /* Kernel launches issued by this context since creation. */
 int64_t crush_launch_count(const crush_ctx* ctx);
 /* Broad-phase statistics of contact `contact_id` accumulated since creation
- * (or the last reset): out[0] primary-node searches that fell back to every
- * face of the contact (full grid bucket or overflow list), out[1] faces put
- * on the overflow list (key box over too many cells), out[2] grid inserts
- * dropped at a full bucket. No counterpart in the reference (whose search
- * is exhaustive). reset != 0 zeroes them after reading. */
+ * (or the last reset): out[0] primary-node searches of a contact with a grid
+ * that tested every face (its overflow list overran), out[1] faces put on the
+ * overflow list (key box not finite or beyond the coarsest grid level),
+ * out[2] reserved (0). No counterpart in the reference (whose search is
+ * exhaustive). reset != 0 zeroes them after reading. */
 int crush_contact_search_stats(crush_ctx* ctx, int contact_id, uint64_t* out, int reset);
+/* exhaustive = 1 makes every contact search test every face of its contact,
+ * as the reference does (src/contact.rs:115); 0 (default) uses the grids.
+ * Both give the same hits: the grids only skip faces that cannot pass the
+ * narrow test. For checking that equality; takes effect at the next step. */
+int crush_set_contact_search(crush_ctx* ctx, int exhaustive);
 
 /* ---- batched contexts: many crash models in one context ----
  *
