@@ -204,12 +204,23 @@ def declare_engine_api(lib):
     lib.crush_set_profiling.argtypes = [vp, C.c_int]
     lib.crush_contact_search_stats.argtypes = [vp, C.c_int, P(C.c_uint64), C.c_int]
     lib.crush_set_contact_search.argtypes = [vp, C.c_int]
+    lib.crush_autotune.argtypes = [vp, P(Tuning)]
+    lib.crush_get_tuning.argtypes = [vp, P(Tuning)]
     lib.crush_batch_create.argtypes = [P(P(ModelDesc)), C.c_int, C.c_int, P(vp)]
     lib.crush_batch_size.argtypes = [vp]
     lib.crush_batch_run.argtypes = [vp, P(Results)]
     lib.crush_batch_results.argtypes = [vp, C.c_int, P(Results)]
     lib.crush_contact_apply_static.argtypes = [C.c_int64, vp, vp, vp, C.c_int64, vp, vp, C.c_int64, vp,
                                                C.c_double, C.c_double, C.c_double, vp, vp, vp]
+
+
+class Tuning(C.Structure):
+    """crush_tuning: the launch schedule the autotuner chose."""
+    _fields_ = [
+        ("slave_lanes", C.c_int32),
+        ("reserved", C.c_int32),
+        ("contact_ms", C.c_double * 4),
+    ]
 
 
 class ContactStats(C.Structure):

@@ -11,6 +11,12 @@
 // together and finish independently, and every slot's arithmetic is the
 // arithmetic it has alone.
 #include <algorithm>
+#include <memory>
+#include <thread>
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <array>
 #include <cmath>
 #include <cstring>
@@ -101,6 +107,85 @@ struct Slot {
     double contact_dt = INF, stable = INF, dt_floor = 0.0, dt0 = 0.0;
 };
 
+// Runs fn(i) for i in [0, n) on up to `hardware_concurrency` host threads
+// (dynamic scheduling); serial for n == 1.
+template <class F>
+void parallel_for(long long n, F&& fn) {
+    unsigned hw = std::thread::hardware_concurrency();
+    const long long T = std::min<long long>(n, std::min<unsigned>(hw ? hw : 1, 64));
+    if (T <= 1) {
+        for (long long i = 0; i < n; ++i) fn(i);
+        return;
+    }
+    std::atomic<long long> next{0};
+    std::vector<std::thread> th;
+    th.reserve(T);
+    for (long long t = 0; t < T; ++t)
+        th.emplace_back([&] {
+            for (long long i = next++; i < n; i = next++) fn(i);
+        });
+    for (auto& x : th) x.join();
+}
+
+// Host-to-device copies through two pinned staging buffers (set-up only):
+// chunks are copied into pinned memory by several threads and sent by DMA
+// while the next chunk is filled. Small copies go directly.
+struct Stager {
+    cudaStream_t s = nullptr;
+    char* buf[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    size_t cap = 0;
+    int cur = 0;
+    static constexpr size_t DIRECT = 1 << 20;
+    int init(cudaStream_t stream, size_t total) {
+        s = stream;
+        if (total < 8 * DIRECT) return CRUSH_OK;  // small contexts: direct copies
+        cap = std::min<size_t>(total, 64u << 20);
+        for (int k = 0; k < 2; ++k) {
+            if (cudaMallocHost(&buf[k], cap) != cudaSuccess || cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                release();
+                return CRUSH_OK;  // fall back to direct copies
+            }
+        }
+        return CRUSH_OK;
+    }
+    int copy(void* dst, const void* src, size_t bytes) {
+        if (!bytes) return CRUSH_OK;
+        if (!buf[0] || bytes < DIRECT) {
+            CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+            return CRUSH_OK;
+        }
+        for (size_t off = 0; off < bytes; off += cap) {
+            const size_t n = std::min(cap, bytes - off);
+            CK(cudaEventSynchronize(ev[cur]));  // the buffer's previous DMA is done
+            const size_t piece = (n + 15) / 16;
+            char* b = buf[cur];
+            const char* sp = static_cast<const char*>(src) + off;
+            parallel_for(16, [&](long long k) {
+                const size_t a = std::min(n, (size_t)k * piece), e = std::min(n, a + piece);
+                if (e > a) std::memcpy(b + a, sp + a, e - a);
+            });
+            CK(cudaMemcpyAsync(static_cast<char*>(dst) + off, b, n, cudaMemcpyHostToDevice, s));
+            CK(cudaEventRecord(ev[cur], s));
+            cur ^= 1;
+        }
+        return CRUSH_OK;
+    }
+    void release() {
+        if (s) cudaStreamSynchronize(s);
+        for (int k = 0; k < 2; ++k) {
+            if (buf[k]) cudaFreeHost(buf[k]);
+            if (ev[k]) cudaEventDestroy(ev[k]);
+            buf[k] = nullptr;
+            ev[k] = nullptr;
+        }
+    }
+    ~Stager() { release(); }
+};
+
+int stager_copy(Stager* st, void* dst, const void* src, size_t bytes) { return st->copy(dst, src, bytes); }
+
 }  // namespace
 
 struct crush_ctx {
@@ -143,12 +228,19 @@ struct crush_ctx {
     std::vector<int> face_off_h, slave_off_h;
     std::vector<uint8_t> is_static_h;
     std::vector<int> tab_off_h;
+    int slave_lanes = 32;  // lanes per primary-node contact search (autotuned)
+    bool tuned = false;
+    long long last_tune_step = 0;  // the open run's step of the last tuning
+    double tune_ms[4] = {0, 0, 0, 0};
 
     // vehicles
     VehicleArrays va{};
     double* veh_out = nullptr;
-    std::vector<uint32_t> veh_accel;
-    std::vector<std::vector<uint32_t>> veh_front;
+    // crush measure: per vehicle its front nodes then its accelerometer node
+    std::vector<uint32_t> crush_nodes_h;
+    std::vector<size_t> crush_off_h{0};
+    uint32_t* crush_nodes = nullptr;
+    double* crush_ux = nullptr;
 
     // run
     bool run_open = false;
@@ -160,6 +252,7 @@ struct crush_ctx {
     int prof_level = 2;  // 1: events around the element-force kernel only; 2: every phase
     bool last_was_graph = false;
     std::vector<cudaEvent_t> prof_ev;
+    Stager* stager = nullptr;  // set-up only: pinned staging of uploads
 
     ElementArrays el() const {
         ElementArrays e;
@@ -217,7 +310,9 @@ struct crush_ctx {
     int upload(T** p, const T* host, size_t count) {
         int st = alloc(p, count);
         if (st != CRUSH_OK) return st;
-        if (count) CK(cudaMemcpyAsync(*p, host, count * sizeof(T), cudaMemcpyHostToDevice, stream));
+        if (!count) return CRUSH_OK;
+        if (stager) return stager_copy(stager, *p, host, count * sizeof(T));
+        CK(cudaMemcpyAsync(*p, host, count * sizeof(T), cudaMemcpyHostToDevice, stream));
         return CRUSH_OK;
     }
     template <typename T>
@@ -250,52 +345,95 @@ int sync(crush_ctx* c) {
     return CRUSH_OK;
 }
 
-// Combined host arrays of all slots.
-struct Combined {
-    std::vector<double> positions, v0, mat4;
-    std::vector<uint32_t> hexes, fixed_list;
-    std::vector<int32_t> hex_part;
-    std::vector<MaterialF32> mats;
-    std::vector<crush_material> materials;
-    std::vector<uint8_t> fixed;
-    std::vector<uint32_t> node_slot, elem_slot;
+// Set-up phase timing to stderr when the environment sets CRUSH_TRACE=1.
+struct Trace {
+    bool on = std::getenv("CRUSH_TRACE") && std::getenv("CRUSH_TRACE")[0] == '1';
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now(), t = t0;
+    void mark(const char* what) {
+        if (!on) return;
+        auto now = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "[crush] %-28s %8.2f ms (total %8.2f ms)\n", what, std::chrono::duration<double, std::milli>(now - t).count(),
+                     std::chrono::duration<double, std::milli>(now - t0).count());
+        t = now;
+    }
 };
 
-int validate_and_append(const crush_model_desc* d, int slot, Combined& cm, Slot& sl) {
+// A host array left uninitialised on allocation (large set-up arrays are
+// written in full by the per-slot passes, so zeroing them first is waste).
+template <typename T>
+struct Buf {
+    std::unique_ptr<T[]> p;
+    size_t n = 0;
+    void alloc(size_t m) {
+        p.reset(new T[m ? m : 1]);
+        n = m;
+    }
+    T* data() { return p.get(); }
+    const T* data() const { return p.get(); }
+    T& operator[](size_t i) { return p[i]; }
+    const T& operator[](size_t i) const { return p[i]; }
+    size_t size() const { return n; }
+};
+
+// Combined host arrays of all slots.
+struct Combined {
+    Buf<double> positions, v0;
+    std::vector<double> mat4;
+    Buf<uint32_t> hexes;
+    Buf<int32_t> hex_part;
+    std::vector<MaterialF32> mats;
+    std::vector<crush_material> materials;
+    Buf<uint8_t> fixed;
+    Buf<uint32_t> node_slot, elem_slot;
+};
+
+struct SlotError {
+    int code = CRUSH_OK;
+    std::string msg;
+    void set(int c, const std::string& m) {
+        if (code == CRUSH_OK) {
+            code = c;
+            msg = m;
+        }
+    }
+};
+
+// Cheap checks of a model description (sizes and pointers).
+int check_desc(const crush_model_desc* d) {
     if (!d || d->n_nodes <= 0 || !d->positions || d->n_hexes < 0 || (d->n_hexes > 0 && (!d->hexes || !d->hex_part)))
         return crush::fail(CRUSH_ERR_INVALID, "invalid model description");
     if (d->n_parts <= 0 || !d->materials) return crush::fail(CRUSH_ERR_INVALID, "model needs at least one material");
+    if (d->n_fixed < 0 || (d->n_fixed > 0 && !d->fixed_nodes)) return crush::fail(CRUSH_ERR_INVALID, "invalid fixed node list");
+    if (d->n_contacts < 0 || (d->n_contacts > 0 && !d->contacts)) return crush::fail(CRUSH_ERR_INVALID, "invalid contact list");
+    if (d->n_vehicles < 0 || (d->n_vehicles > 0 && !d->vehicles)) return crush::fail(CRUSH_ERR_INVALID, "invalid vehicle list");
     const crush_settings& s = d->settings;
     if (!(s.dt_scale > 0.0) || s.adaptive_check_steps < 0 || !(s.hourglass >= 0.0))
         return crush::fail(CRUSH_ERR_INVALID, "invalid settings");
-    const long long N = d->n_nodes, E = d->n_hexes;
-    const long long n0 = (long long)cm.positions.size() / 3;
-    const int p0 = (int)cm.materials.size();
-    if (n0 + N >= (1ll << 31) || (long long)cm.hex_part.size() + E >= (1ll << 28)) return crush::fail(CRUSH_ERR_INVALID, "model too large");
-    sl.settings = s;
-    sl.node0 = n0;
-    sl.n_nodes = N;
-    sl.elem0 = (long long)cm.hex_part.size();
-    sl.n_elems = E;
-    cm.positions.insert(cm.positions.end(), d->positions, d->positions + 3 * N);
-    if (d->initial_velocity) cm.v0.insert(cm.v0.end(), d->initial_velocity, d->initial_velocity + 3 * N);
-    else cm.v0.insert(cm.v0.end(), 3 * N, 0.0);
-    cm.fixed.insert(cm.fixed.end(), N, 0);
-    cm.node_slot.insert(cm.node_slot.end(), N, (uint32_t)slot);
+    return CRUSH_OK;
+}
+
+// Slot k's nodes, parts and elements into the combined arrays at its offsets.
+void fill_slot(const crush_model_desc* d, int slot, const Slot& sl, int p0, Combined& cm, long long* n_hc, SlotError& err) {
+    const long long N = d->n_nodes, E = d->n_hexes, n0 = sl.node0, e0 = sl.elem0;
+    std::memcpy(&cm.positions[3 * n0], d->positions, sizeof(double) * 3 * N);
+    if (d->initial_velocity) std::memcpy(&cm.v0[3 * n0], d->initial_velocity, sizeof(double) * 3 * N);
+    else std::memset(&cm.v0[3 * n0], 0, sizeof(double) * 3 * N);
+    std::memset(&cm.fixed[n0], 0, N);
+    for (long long i = 0; i < N; ++i) cm.node_slot[n0 + i] = (uint32_t)slot;
     for (int64_t i = 0; i < d->n_fixed; ++i) {
-        if (d->fixed_nodes[i] >= (uint64_t)N) return crush::fail(CRUSH_ERR_INVALID, "fixed node out of range");
+        if (d->fixed_nodes[i] >= (uint64_t)N) return err.set(CRUSH_ERR_INVALID, "fixed node out of range");
         cm.fixed[n0 + d->fixed_nodes[i]] = 1;
     }
     for (int p = 0; p < d->n_parts; ++p) {
         const crush_material& m = d->materials[p];
         if (!(m.density > 0.0) || !(m.youngs_modulus > 0.0) || !(m.poisson_ratio >= 0.0 && m.poisson_ratio < 0.5))
-            return crush::fail(CRUSH_ERR_INVALID, "material " + std::to_string(p) + ": needs E > 0, density > 0, 0 <= nu < 0.5");
+            return err.set(CRUSH_ERR_INVALID, "material " + std::to_string(p) + ": needs E > 0, density > 0, 0 <= nu < 0.5");
         MaterialF32 mf;
         std::memset(&mf, 0, sizeof(mf));
         if (m.model == CRUSH_MAT_HONEYCOMB) {
             double knots[MAX_KNOTS][3];
-            std::string err;
-            if (honeycomb_params(m, knots, &err) != 0) return crush::fail(CRUSH_ERR_INVALID, "material " + std::to_string(p) + ": " + err);
+            std::string e;
+            if (honeycomb_params(m, knots, &e) != 0) return err.set(CRUSH_ERR_INVALID, "material " + std::to_string(p) + ": " + e);
             mf.youngs = (float)m.youngs_modulus;
             mf.trans = (float)m.transverse_factor;
             for (int k = 0; k < MAX_KNOTS; ++k) {
@@ -304,40 +442,290 @@ int validate_and_append(const crush_model_desc* d, int slot, Combined& cm, Slot&
                 mf.knot_h[k] = (float)knots[k][2];
             }
         } else if (m.model != CRUSH_MAT_ELASTIC) {
-            return crush::fail(CRUSH_ERR_UNSUPPORTED, "unknown material model");
+            return err.set(CRUSH_ERR_UNSUPPORTED, "unknown material model");
         }
-        cm.mats.push_back(mf);
-        cm.materials.push_back(m);
-        cm.mat4.insert(cm.mat4.end(), {m.youngs_modulus, m.poisson_ratio, m.density, s.hourglass});
+        cm.mats[p0 + p] = mf;
+        cm.materials[p0 + p] = m;
+        const double m4[4] = {m.youngs_modulus, m.poisson_ratio, m.density, d->settings.hourglass};
+        std::memcpy(&cm.mat4[4 * (size_t)(p0 + p)], m4, sizeof(m4));
     }
+    long long hc = 0;
     for (long long e = 0; e < E; ++e) {
-        int p = d->hex_part[e];
-        if (p < 0 || p >= d->n_parts) return crush::fail(CRUSH_ERR_INVALID, "hexahedron part out of range");
+        const int p = d->hex_part[e];
+        if (p < 0 || p >= d->n_parts) return err.set(CRUSH_ERR_INVALID, "hexahedron part out of range");
+        const bool honey = d->materials[p].model == CRUSH_MAT_HONEYCOMB;
         for (int i = 0; i < 8; ++i) {
-            if (d->hexes[8 * e + i] >= (uint64_t)N) return crush::fail(CRUSH_ERR_INVALID, "hexahedron node out of range");
-            cm.hexes.push_back((uint32_t)(n0 + d->hexes[8 * e + i]));
+            const uint64_t n = d->hexes[8 * e + i];
+            if (n >= (uint64_t)N) return err.set(CRUSH_ERR_INVALID, "hexahedron node out of range");
+            if (!honey && !cm.fixed[n0 + n])
+                return err.set(CRUSH_ERR_UNSUPPORTED, "elastic elements are supported only as rigid slabs (every node fixed)");
+            cm.hexes[8 * (e0 + e) + i] = (uint32_t)(n0 + n);
         }
-        cm.hex_part.push_back(p0 + p);
-        cm.elem_slot.push_back((uint32_t)slot);
-        if (d->materials[p].model != CRUSH_MAT_HONEYCOMB)
-            for (int i = 0; i < 8; ++i)
-                if (!cm.fixed[n0 + d->hexes[8 * e + i]])
-                    return crush::fail(CRUSH_ERR_UNSUPPORTED, "elastic elements are supported only as rigid slabs (every node fixed)");
+        cm.hex_part[e0 + e] = p0 + p;
+        cm.elem_slot[e0 + e] = (uint32_t)slot;
+        hc += honey ? 1 : 0;
     }
-    return CRUSH_OK;
+    *n_hc = hc;
+}
+
+// One slot's contacts (ContactRuntime::new, src/contact.rs:48-70), with
+// slot-local offsets; concatenated afterwards.
+struct ContactPart {
+    std::vector<int> nf, ns, tab, st;
+    std::vector<uint8_t> stat, stop;
+    std::vector<double> stiff, md, cell;
+    std::vector<uint32_t> faces, slaves, dyn_faces, grid_faces;  // faces/slaves: global node ids; *_faces: slot-local
+    std::vector<double> scales;
+    std::vector<uint32_t> st_off;  // per contact T+1 entries, slot-local into st_entries
+    std::vector<int> st_entries;
+    std::vector<uint32_t> cnode, cnode_off{0}, crole_faces_off{0};
+    std::vector<int> crole_contact, crole_slave, crole_faces;
+    std::vector<uint8_t> crole_face;
+    double contact_dt = INF;
+};
+
+// The geometry the broad phase needs of one face at the reference positions.
+void face_frame(const double* pos, const uint32_t* q, double x[4][3], double nr[3], double ctr[3]) {
+    double e1[3], e2[3];
+    for (int j = 0; j < 4; ++j)
+        for (int dd = 0; dd < 3; ++dd) x[j][dd] = pos[3 * (size_t)q[j] + dd];
+    for (int dd = 0; dd < 3; ++dd) {
+        e1[dd] = x[1][dd] - x[0][dd];
+        e2[dd] = x[2][dd] - x[0][dd];
+    }
+    nr[0] = e1[1] * e2[2] - e1[2] * e2[1];
+    nr[1] = e1[2] * e2[0] - e1[0] * e2[2];
+    nr[2] = e1[0] * e2[1] - e1[1] * e2[0];
+    const double len = std::sqrt(nr[0] * nr[0] + nr[1] * nr[1] + nr[2] * nr[2]);
+    for (int dd = 0; dd < 3; ++dd) {
+        nr[dd] = len > 0.0 ? nr[dd] / len : 0.0;
+        ctr[dd] = (((x[0][dd] + x[1][dd]) + x[2][dd]) + x[3][dd]) / 4.0;
+    }
+}
+
+void build_contacts(const crush_model_desc* d, const Slot& sl, const Combined& cm, const std::vector<double>& mass_h, ContactPart& cp,
+                    SlotError& err) {
+    const long long n0 = sl.node0;
+    // Contact-node roles: (node, contact, sequence) sorted gives, for every
+    // node, its contacts in order with its primary-node entries and the faces
+    // it belongs to (the src/contact.rs:146-153 order).
+    struct RoleItem {
+        uint32_t node;
+        int contact;
+        int seq;
+        int slave;  // >= 0: primary-node entry index within the contact
+        int face;   // >= 0: local face index
+    };
+    std::vector<RoleItem> items;
+    int seq = 0;
+    for (int k = 0; k < d->n_contacts; ++k) {
+        const crush_contact& cd = d->contacts[k];
+        const int kc = sl.contact0 + k;
+        if (cd.n_nodes < 0 || cd.n_faces < 0 || (cd.n_nodes > 0 && !cd.nodes) || (cd.n_faces > 0 && !cd.faces))
+            return err.set(CRUSH_ERR_INVALID, "invalid contact " + std::to_string(k));
+        if (!(cd.max_distance >= 0.0) || !(cd.stiffness >= 0.0)) return err.set(CRUSH_ERR_INVALID, "invalid contact parameters");
+        double lo[3] = {INF, INF, INF}, hi[3] = {-INF, -INF, -INF};
+        bool stop = false;
+        double ext = 0.0;
+        const size_t face0 = cp.faces.size() / 4;
+        for (int64_t f = 0; f < cd.n_faces; ++f) {
+            double flo[3] = {INF, INF, INF}, fhi[3] = {-INF, -INF, -INF};
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t nl = cd.faces[4 * f + j];
+                if (nl >= (uint64_t)d->n_nodes) return err.set(CRUSH_ERR_INVALID, "contact face node out of range");
+                const uint32_t n = (uint32_t)(n0 + nl);
+                cp.faces.push_back(n);
+                if (!cm.fixed[n]) stop = true;
+                for (int dd = 0; dd < 3; ++dd) {
+                    const double p = cm.positions[3 * (size_t)n + dd];
+                    lo[dd] = std::fmin(lo[dd], p);
+                    hi[dd] = std::fmax(hi[dd], p);
+                    flo[dd] = std::fmin(flo[dd], p);
+                    fhi[dd] = std::fmax(fhi[dd], p);
+                }
+            }
+            ext = std::max(ext, std::max({fhi[0] - flo[0], fhi[1] - flo[1], fhi[2] - flo[2]}));
+        }
+        for (int dd = 0; dd < 3; ++dd) {
+            lo[dd] += -cd.max_distance;
+            hi[dd] += cd.max_distance;
+        }
+        int kept = 0;
+        for (int64_t i = 0; i < cd.n_nodes; ++i) {
+            const uint32_t nl = cd.nodes[i];
+            if (nl >= (uint64_t)d->n_nodes) return err.set(CRUSH_ERR_INVALID, "contact node out of range");
+            const uint32_t n = (uint32_t)(n0 + nl);
+            // contact_dt over every listed node (src/solver.rs:217-223)
+            if (mass_h[n] > 0.0 && cd.stiffness > 0.0) cp.contact_dt = std::fmin(cp.contact_dt, 2.0 * std::sqrt(mass_h[n] / cd.stiffness));
+            bool inside = true;
+            for (int dd = 0; dd < 3; ++dd) {
+                const double p = cm.positions[3 * (size_t)n + dd];
+                if (!(p >= lo[dd] && p <= hi[dd])) inside = false;
+            }
+            if (!inside) continue;
+            cp.slaves.push_back(n);
+            cp.scales.push_back(cd.node_scale ? cd.node_scale[i] : 1.0);
+            items.push_back(RoleItem{n, kc, seq++, kept, -1});
+            ++kept;
+        }
+        for (int64_t f = 0; f < cd.n_faces; ++f)
+            for (int j = 0; j < 4; ++j) items.push_back(RoleItem{(uint32_t)(n0 + cd.faces[4 * f + j]), kc, seq++, -1, (int)f});
+        const double cs = ext > 0.0 ? 2.0 * ext : 1.0;  // grid cell: twice the largest face
+        const bool stat = !stop && cd.n_faces > 0;
+        size_t t = 0, st = 0;
+        const uint32_t* fq = cp.faces.data() + 4 * face0;
+        if (stat) {
+            // Exact hashed grid of the fixed faces, in CSR form.
+            std::vector<std::pair<uint32_t, int>> ins;  // (hash, face)
+            bool ok = true;
+            for (int64_t f = 0; f < cd.n_faces && ok; ++f) {
+                double x[4][3], nr[3], ctr[3], klo[3], khi[3];
+                face_frame(cm.positions.data(), fq + 4 * f, x, nr, ctr);
+                face_key_box(x, nr, ctr, cd.max_distance, klo, khi);
+                long long r[6];
+                double cells = 1.0;
+                for (int dd = 0; dd < 3; ++dd) {
+                    if (!std::isfinite(klo[dd]) || !std::isfinite(khi[dd]) || std::fabs(klo[dd] / cs) > 4.0e15 ||
+                        std::fabs(khi[dd] / cs) > 4.0e15) {
+                        ok = false;
+                        break;
+                    }
+                    r[2 * dd] = (long long)std::floor(klo[dd] / cs);
+                    r[2 * dd + 1] = (long long)std::floor(khi[dd] / cs);
+                    cells *= (double)(r[2 * dd + 1] - r[2 * dd] + 1);
+                }
+                if (!ok || cells > 4096.0) {
+                    ok = false;
+                    break;
+                }
+                for (long long kz = r[4]; kz <= r[5]; ++kz)
+                    for (long long jy = r[2]; jy <= r[3]; ++jy)
+                        for (long long ix = r[0]; ix <= r[1]; ++ix) ins.push_back({cell_hash(ix, jy, kz, 0), (int)f});
+            }
+            const uint32_t base = (uint32_t)cp.st_entries.size();
+            if (ok) {
+                st = next_pow2(std::max<size_t>(16, 2 * ins.size()));
+                std::vector<uint32_t> cnt(st + 1, 0);
+                for (auto& e : ins) cnt[(e.first & (st - 1)) + 1]++;
+                for (size_t b2 = 0; b2 < st; ++b2) cnt[b2 + 1] += cnt[b2];
+                cp.st_entries.resize(base + ins.size());
+                std::vector<uint32_t> cur(cnt.begin(), cnt.end() - 1);
+                for (auto& e : ins) cp.st_entries[base + cur[e.first & (st - 1)]++] = e.second;  // faces ascending in a bucket
+                for (size_t b2 = 0; b2 <= st; ++b2) cp.st_off.push_back(base + cnt[b2]);
+            } else {
+                st = 0;
+                cp.st_off.push_back(base);
+            }
+        } else {
+            cp.st_off.push_back((uint32_t)cp.st_entries.size());
+            for (int64_t f = 0; f < cd.n_faces; ++f) cp.dyn_faces.push_back((uint32_t)(face0 + f));
+            if (cd.n_faces >= GRID_MIN_FACES) {
+                // Hierarchical table: four times the level-0 key-box cells of
+                // the faces at the reference positions, a power of two.
+                size_t inserts = 0;
+                for (int64_t f = 0; f < cd.n_faces; ++f) {
+                    double x[4][3], nr[3], ctr[3], klo[3], khi[3];
+                    face_frame(cm.positions.data(), fq + 4 * f, x, nr, ctr);
+                    face_key_box(x, nr, ctr, cd.max_distance, klo, khi);
+                    double cells = 1.0;
+                    for (int dd = 0; dd < 3; ++dd) cells *= std::floor(khi[dd] / cs) - std::floor(klo[dd] / cs) + 1.0;
+                    inserts += (size_t)std::min(std::isfinite(cells) && cells > 0.0 ? cells : 0.0, (double)LEVEL_CELL_BUDGET);
+                }
+                t = next_pow2(std::max<size_t>(1024, 4 * inserts));
+                for (int64_t f = 0; f < cd.n_faces; ++f) cp.grid_faces.push_back((uint32_t)(face0 + f));
+            }
+        }
+        cp.nf.push_back((int)cd.n_faces);
+        cp.ns.push_back(kept);
+        cp.tab.push_back((int)t);
+        cp.st.push_back((int)st);
+        cp.stat.push_back(stat && st > 0 ? 1 : 0);
+        cp.stop.push_back(stop ? 1 : 0);
+        cp.stiff.push_back(cd.stiffness);
+        cp.md.push_back(cd.max_distance);
+        cp.cell.push_back(cs);
+    }
+    std::sort(items.begin(), items.end(), [](const RoleItem& x, const RoleItem& y) {
+        return x.node != y.node ? x.node < y.node : (x.contact != y.contact ? x.contact < y.contact : x.seq < y.seq);
+    });
+    for (size_t i0 = 0; i0 < items.size();) {
+        size_t i1 = i0;
+        while (i1 < items.size() && items[i1].node == items[i0].node) ++i1;
+        cp.cnode.push_back(items[i0].node);
+        for (size_t a0 = i0; a0 < i1;) {
+            size_t a1 = a0;
+            while (a1 < i1 && items[a1].contact == items[a0].contact) ++a1;
+            // One role per primary-node entry (or one without), the faces on the last.
+            int n_slave_roles = 0;
+            for (size_t q = a0; q < a1; ++q) n_slave_roles += items[q].slave >= 0;
+            const int n_roles = std::max(n_slave_roles, 1);
+            int made = 0;
+            for (size_t q = a0; q < a1 && made < n_slave_roles; ++q)
+                if (items[q].slave >= 0) {
+                    ++made;
+                    cp.crole_contact.push_back(items[a0].contact);
+                    cp.crole_slave.push_back(items[q].slave);
+                    if (made < n_roles) {
+                        cp.crole_face.push_back(0);
+                        cp.crole_faces_off.push_back((uint32_t)cp.crole_faces.size());
+                    }
+                }
+            if (n_slave_roles == 0) {
+                cp.crole_contact.push_back(items[a0].contact);
+                cp.crole_slave.push_back(-1);
+            }
+            int last = -1;
+            bool any_face = false;
+            for (size_t q = a0; q < a1; ++q)
+                if (items[q].face >= 0 && items[q].face != last) {
+                    cp.crole_faces.push_back(items[q].face);
+                    last = items[q].face;
+                    any_face = true;
+                }
+            cp.crole_face.push_back(any_face ? 1 : 0);
+            cp.crole_faces_off.push_back((uint32_t)cp.crole_faces.size());
+            a0 = a1;
+        }
+        cp.cnode_off.push_back((uint32_t)cp.crole_contact.size());
+        i0 = i1;
+    }
+}
+
+template <typename T>
+void append(std::vector<T>& dst, const std::vector<T>& src) {
+    dst.insert(dst.end(), src.begin(), src.end());
 }
 
 int create_impl(const crush_model_desc* const* descs, int n_desc, int device, crush_ctx* c) {
     if (n_desc <= 0 || !descs) return crush::fail(CRUSH_ERR_INVALID, "no models");
+    Trace trace;
     c->device = device;
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     c->n_slots = n_desc;
     c->slots.resize(n_desc);
-    Combined cm;
+    // ---- sizes and offsets of every slot ----
+    long long N = 0, E = 0;
+    int P = 0, K = 0;
+    std::vector<int> part0(n_desc);
     for (int k = 0; k < n_desc; ++k) {
-        int st = validate_and_append(descs[k], k, cm, c->slots[k]);
-        if (st != CRUSH_OK) return st;
+        const crush_model_desc* d = descs[k];
+        int st0 = check_desc(d);
+        if (st0 != CRUSH_OK) return st0;
+        Slot& sl = c->slots[k];
+        sl.settings = d->settings;
+        sl.node0 = N;
+        sl.n_nodes = d->n_nodes;
+        sl.elem0 = E;
+        sl.n_elems = d->n_hexes;
+        sl.contact0 = K;
+        sl.n_contacts = d->n_contacts;
+        part0[k] = P;
+        N += d->n_nodes;
+        E += d->n_hexes;
+        P += d->n_parts;
+        K += d->n_contacts;
+        if (N >= (1ll << 31) || E >= (1ll << 28)) return crush::fail(CRUSH_ERR_INVALID, "models too large for one context");
     }
     // The step schedule is shared: every slot must re-check its stable step
     // on the same cadence.
@@ -353,42 +741,86 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
             if (s.stop_rule == CRUSH_STOP_SEPARATION) c->any_separation = true;
         }
     }
-    const long long N = (long long)cm.positions.size() / 3, E = (long long)cm.hex_part.size();
+    Combined cm;
+    cm.positions.alloc(3 * N);
+    cm.v0.alloc(3 * N);
+    cm.fixed.alloc(N);
+    cm.node_slot.alloc(N);
+    cm.hexes.alloc(8 * E);
+    cm.hex_part.alloc(E);
+    cm.elem_slot.alloc(E);
+    cm.mats.resize(P);
+    cm.materials.resize(P);
+    cm.mat4.resize(4 * (size_t)P);
+    std::vector<SlotError> errs(n_desc);
+    std::vector<long long> slot_hc(n_desc, 0);
+    parallel_for(n_desc, [&](long long k) { fill_slot(descs[k], (int)k, c->slots[k], part0[k], cm, &slot_hc[k], errs[k]); });
+    for (auto& e : errs)
+        if (e.code != CRUSH_OK) return crush::fail(e.code, e.msg);
+    trace.mark("validate + concatenate");
     c->n_nodes = N;
     c->n_all = E;
-    c->hc_index.assign(E, -1);
-    c->hc_model.clear();
-    for (long long e = 0; e < E; ++e)
-        if (cm.materials[cm.hex_part[e]].model == CRUSH_MAT_HONEYCOMB) {
-            c->hc_index[e] = (int64_t)c->hc_model.size();
-            c->hc_model.push_back((uint32_t)e);
-        }
-    c->n_hc = (long long)c->hc_model.size();
+    // Honeycomb numbering (element order) and the node incidence CSRs, per
+    // slot in parallel: a slot's nodes are touched only by its own elements.
+    std::vector<long long> hc0(n_desc + 1, 0);
+    for (int k = 0; k < n_desc; ++k) hc0[k + 1] = hc0[k] + slot_hc[k];
+    c->n_hc = hc0[n_desc];
     c->stride = std::max<long long>(32, (c->n_hc + 31) / 32 * 32);
-    // Node incidence CSRs, slots in increasing element order.
-    std::vector<uint32_t> all_off(N + 1, 0), hc_off(N + 1, 0);
-    for (long long e = 0; e < E; ++e)
-        for (int i = 0; i < 8; ++i) {
-            all_off[cm.hexes[8 * e + i] + 1]++;
-            if (c->hc_index[e] >= 0) hc_off[cm.hexes[8 * e + i] + 1]++;
-        }
-    for (long long n = 0; n < N; ++n) {
-        all_off[n + 1] += all_off[n];
-        hc_off[n + 1] += hc_off[n];
-    }
-    std::vector<uint32_t> all_slot(all_off[N]), hc_slot(hc_off[N]);
-    {
-        std::vector<uint32_t> ca(all_off.begin(), all_off.end() - 1), ch(hc_off.begin(), hc_off.end() - 1);
-        for (long long e = 0; e < E; ++e)
-            for (int i = 0; i < 8; ++i) {
-                uint32_t n = cm.hexes[8 * e + i];
-                all_slot[ca[n]++] = (uint32_t)(8 * e + i);
-                if (c->hc_index[e] >= 0) hc_slot[ch[n]++] = (uint32_t)(8 * c->hc_index[e] + i);
+    c->hc_index.resize(E);
+    c->hc_model.resize(c->n_hc);
+    Buf<uint32_t> all_off, hc_off, all_slot, hc_slot;
+    all_off.alloc(N + 1);
+    hc_off.alloc(N + 1);
+    all_slot.alloc(8 * E);
+    hc_slot.alloc(8 * c->n_hc);
+    parallel_for(n_desc, [&](long long k) {
+        const Slot& sl = c->slots[k];
+        const long long n0 = sl.node0, e0 = sl.elem0, nn = sl.n_nodes;
+        long long h = hc0[k];
+        for (long long e = e0; e < e0 + sl.n_elems; ++e)
+            if (cm.materials[cm.hex_part[e]].model == CRUSH_MAT_HONEYCOMB) {
+                c->hc_index[e] = h;
+                c->hc_model[h++] = (uint32_t)e;
+            } else {
+                c->hc_index[e] = -1;
             }
-    }
+        // per-node counts, then offsets from the slot's first entry (a slot
+        // writes only off[n0, n0 + nn))
+        std::vector<uint32_t> cnt_a(nn, 0), cnt_b(nn, 0);
+        for (long long e = e0; e < e0 + sl.n_elems; ++e) {
+            const bool honey = c->hc_index[e] >= 0;
+            for (int i = 0; i < 8; ++i) {
+                const uint32_t n = cm.hexes[8 * e + i];
+                cnt_a[n - n0]++;
+                if (honey) cnt_b[n - n0]++;
+            }
+        }
+        uint32_t a = (uint32_t)(8 * e0), b = (uint32_t)(8 * hc0[k]);
+        for (long long n = n0; n < n0 + nn; ++n) {
+            all_off[n] = a;
+            hc_off[n] = b;
+            a += cnt_a[n - n0];
+            b += cnt_b[n - n0];
+        }
+        std::vector<uint32_t> cura(all_off.data() + n0, all_off.data() + n0 + nn), curb(hc_off.data() + n0, hc_off.data() + n0 + nn);
+        for (long long e = e0; e < e0 + sl.n_elems; ++e) {
+            const long long he = c->hc_index[e];
+            for (int i = 0; i < 8; ++i) {
+                const uint32_t n = cm.hexes[8 * e + i];
+                all_slot[cura[n - n0]++] = (uint32_t)(8 * e + i);
+                if (he >= 0) hc_slot[curb[n - n0]++] = (uint32_t)(8 * he + i);
+            }
+        }
+    });
+    all_off[N] = (uint32_t)(8 * E);
+    hc_off[N] = (uint32_t)(8 * c->n_hc);
+    trace.mark("node incidence CSR");
 
     int st;
 #define TRY(x) do { st = (x); if (st != CRUSH_OK) return st; } while (0)
+    Stager stager;
+    stager.init(c->stream, sizeof(double) * 6 * N + sizeof(uint32_t) * 27 * E);
+    c->stager = &stager;
     TRY(c->upload(&c->pos, cm.positions.data(), 3 * N));
     TRY(c->upload(&c->conn_all, cm.hexes.data(), 8 * E));
     TRY(c->upload(&c->part, cm.hex_part.data(), E));
@@ -416,6 +848,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     CK(cudaMemsetAsync(c->planes, 0, sizeof(float4) * N_STATIC_PLANES * c->stride, c->stream));
     CK(cudaMemsetAsync(c->eroded_all, 0, E, c->stream));
     CK(cudaMemsetAsync(c->ctls, 0, sizeof(Control) * c->n_slots, c->stream));
+    trace.mark("uploads + allocations");
 
     // Device set-up geometry (HexGeometry::new for every element).
     int* bad = nullptr;
@@ -433,229 +866,91 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     CK(cudaStreamSynchronize(c->stream));
     if (bad_h == 1) return crush::fail(CRUSH_ERR_INVALID, "degenerate hexahedron (singular Jacobian)");
     if (bad_h == 2) return crush::fail(CRUSH_ERR_INVALID, "hourglass modes not independent");
+    trace.mark("device geometry + masses");
 
-    // ---- contacts (ContactRuntime::new, src/contact.rs:48-70) ----
-    std::vector<int> face_off(1, 0), slave_off(1, 0), tab_off(1, 0), counts_for_stop, face_contact, slave_contact, contact_slot;
-    std::vector<int> slot_contact_off(1, 0);
-    std::vector<uint32_t> faces, slaves, dyn_faces;
-    std::vector<double> scales, stiff, md, cell;
-    std::vector<uint8_t> is_static;
-    std::vector<long long> st_tab_off(1, 0);
-    std::vector<uint32_t> st_off;
-    std::vector<int> st_entries;
-    // Contact-node roles, built per slot: (node, contact, sequence) sorted
-    // gives, for every node, its contacts in order with its primary-node
-    // entries and the faces it belongs to (src/contact.rs:146-153 order).
-    struct RoleItem {
-        uint32_t node;
-        int contact;
-        int seq;
-        int slave;  // >= 0: primary-node entry index within the contact
-        int face;   // >= 0: local face index
+    // ---- contacts: per slot in parallel, then concatenated ----
+    std::vector<ContactPart> parts(n_desc);
+    parallel_for(n_desc, [&](long long k) { build_contacts(descs[k], c->slots[k], cm, mass_h, parts[k], errs[k]); });
+    for (auto& e : errs)
+        if (e.code != CRUSH_OK) return crush::fail(e.code, e.msg);
+    // Concatenation: per-slot bases, then every slot copies its part in parallel.
+    struct Base {
+        long long face, slave, ste, stoff, dyn, grid, cnode, role, rface;
     };
-    std::vector<uint32_t> cnode, cnode_off(1, 0);
-    std::vector<int> crole_contact, crole_slave, crole_faces;
-    std::vector<uint8_t> crole_face;
-    std::vector<uint32_t> crole_faces_off(1, 0);
-    std::vector<RoleItem> items;
-    int kc = 0;
-    for (int sidx = 0; sidx < n_desc; ++sidx) {
-        const crush_model_desc* d = descs[sidx];
-        Slot& sl = c->slots[sidx];
-        const long long n0 = sl.node0;
-        sl.contact0 = kc;
-        sl.n_contacts = d->n_contacts;
-        items.clear();
-        int seq = 0;
-        for (int k = 0; k < d->n_contacts; ++k, ++kc) {
-            const crush_contact& cd = d->contacts[k];
-            if (cd.n_nodes < 0 || cd.n_faces < 0 || (cd.n_nodes > 0 && !cd.nodes) || (cd.n_faces > 0 && !cd.faces))
-                return crush::fail(CRUSH_ERR_INVALID, "invalid contact " + std::to_string(k));
-            if (!(cd.max_distance >= 0.0) || !(cd.stiffness >= 0.0)) return crush::fail(CRUSH_ERR_INVALID, "invalid contact parameters");
-            double lo[3] = {INF, INF, INF}, hi[3] = {-INF, -INF, -INF};
-            bool stop = false;
-            double ext = 0.0;
-            const size_t face0 = faces.size() / 4;
-            for (int64_t f = 0; f < cd.n_faces; ++f) {
-                double flo[3] = {INF, INF, INF}, fhi[3] = {-INF, -INF, -INF};
-                for (int j = 0; j < 4; ++j) {
-                    uint32_t nl = cd.faces[4 * f + j];
-                    if (nl >= (uint64_t)d->n_nodes) return crush::fail(CRUSH_ERR_INVALID, "contact face node out of range");
-                    uint32_t n = (uint32_t)(n0 + nl);
-                    faces.push_back(n);
-                    if (!cm.fixed[n]) stop = true;
-                    for (int dd = 0; dd < 3; ++dd) {
-                        double p = cm.positions[3 * (size_t)n + dd];
-                        lo[dd] = std::fmin(lo[dd], p);
-                        hi[dd] = std::fmax(hi[dd], p);
-                        flo[dd] = std::fmin(flo[dd], p);
-                        fhi[dd] = std::fmax(fhi[dd], p);
-                    }
-                }
-                face_contact.push_back(kc);
-                ext = std::max(ext, std::max({fhi[0] - flo[0], fhi[1] - flo[1], fhi[2] - flo[2]}));
-            }
-            for (int dd = 0; dd < 3; ++dd) { lo[dd] += -cd.max_distance; hi[dd] += cd.max_distance; }
-            int kept = 0;
-            for (int64_t i = 0; i < cd.n_nodes; ++i) {
-                uint32_t nl = cd.nodes[i];
-                if (nl >= (uint64_t)d->n_nodes) return crush::fail(CRUSH_ERR_INVALID, "contact node out of range");
-                uint32_t n = (uint32_t)(n0 + nl);
-                // contact_dt over every listed node (src/solver.rs:217-223)
-                if (mass_h[n] > 0.0 && cd.stiffness > 0.0) sl.contact_dt = std::fmin(sl.contact_dt, 2.0 * std::sqrt(mass_h[n] / cd.stiffness));
-                bool inside = true;
-                for (int dd = 0; dd < 3; ++dd) {
-                    double p = cm.positions[3 * (size_t)n + dd];
-                    if (!(p >= lo[dd] && p <= hi[dd])) inside = false;
-                }
-                if (!inside) continue;
-                slaves.push_back(n);
-                slave_contact.push_back(kc);
-                scales.push_back(cd.node_scale ? cd.node_scale[i] : 1.0);
-                items.push_back(RoleItem{n, kc, seq++, kept, -1});
-                ++kept;
-            }
-            for (int64_t f = 0; f < cd.n_faces; ++f)
-                for (int j = 0; j < 4; ++j) items.push_back(RoleItem{(uint32_t)(n0 + cd.faces[4 * f + j]), kc, seq++, -1, (int)f});
-            face_off.push_back(face_off.back() + (int)cd.n_faces);
-            slave_off.push_back(slave_off.back() + kept);
-            const double cs = ext > 0.0 ? 2.0 * ext : 1.0;  // grid cell: twice the largest face
-            const bool stat = !stop && cd.n_faces > 0;
-            size_t t = 0, st = 0;
-            if (stat) {
-                // Exact hashed grid of the fixed faces, in CSR form.
-                std::vector<std::pair<uint32_t, int>> ins;  // (bucket before masking, face)
-                bool ok = true;
-                for (int64_t f = 0; f < cd.n_faces && ok; ++f) {
-                    double x[4][3], e1[3], e2[3], nr[3], ctr[3], klo[3], khi[3];
-                    for (int j = 0; j < 4; ++j)
-                        for (int dd = 0; dd < 3; ++dd) x[j][dd] = cm.positions[3 * (size_t)faces[4 * (face0 + f) + j] + dd];
-                    for (int dd = 0; dd < 3; ++dd) { e1[dd] = x[1][dd] - x[0][dd]; e2[dd] = x[2][dd] - x[0][dd]; }
-                    nr[0] = e1[1] * e2[2] - e1[2] * e2[1];
-                    nr[1] = e1[2] * e2[0] - e1[0] * e2[2];
-                    nr[2] = e1[0] * e2[1] - e1[1] * e2[0];
-                    const double len = std::sqrt(nr[0] * nr[0] + nr[1] * nr[1] + nr[2] * nr[2]);
-                    for (int dd = 0; dd < 3; ++dd) {
-                        nr[dd] = nr[dd] / len;
-                        ctr[dd] = (((x[0][dd] + x[1][dd]) + x[2][dd]) + x[3][dd]) / 4.0;
-                    }
-                    face_key_box(x, nr, ctr, cd.max_distance, klo, khi);
-                    long long r[6];
-                    double cells = 1.0;
-                    for (int dd = 0; dd < 3; ++dd) {
-                        if (!std::isfinite(klo[dd]) || !std::isfinite(khi[dd]) || std::fabs(klo[dd] / cs) > 4.0e15 ||
-                            std::fabs(khi[dd] / cs) > 4.0e15) {
-                            ok = false;
-                            break;
-                        }
-                        r[2 * dd] = (long long)std::floor(klo[dd] / cs);
-                        r[2 * dd + 1] = (long long)std::floor(khi[dd] / cs);
-                        cells *= (double)(r[2 * dd + 1] - r[2 * dd] + 1);
-                    }
-                    if (!ok || cells > 4096.0) { ok = false; break; }
-                    for (long long kz = r[4]; kz <= r[5]; ++kz)
-                        for (long long jy = r[2]; jy <= r[3]; ++jy)
-                            for (long long ix = r[0]; ix <= r[1]; ++ix) ins.push_back({cell_hash(ix, jy, kz, 0), (int)f});
-                }
-                if (ok) {
-                    st = next_pow2(std::max<size_t>(16, 2 * ins.size()));
-                    std::vector<uint32_t> cnt(st + 1, 0);
-                    for (auto& e : ins) cnt[(e.first & (st - 1)) + 1]++;
-                    const uint32_t base = (uint32_t)st_entries.size();
-                    for (size_t b2 = 0; b2 < st; ++b2) cnt[b2 + 1] += cnt[b2];
-                    std::vector<int> ent(ins.size());
-                    std::vector<uint32_t> cur(cnt.begin(), cnt.end() - 1);
-                    for (auto& e : ins) ent[cur[e.first & (st - 1)]++] = e.second;  // faces ascending within a bucket
-                    for (size_t b2 = 0; b2 <= st; ++b2) st_off.push_back(base + cnt[b2]);
-                    st_entries.insert(st_entries.end(), ent.begin(), ent.end());
-                } else {
-                    st = 0;
-                    st_off.push_back((uint32_t)st_entries.size());
-                }
-            } else {
-                st_off.push_back((uint32_t)st_entries.size());
-                for (int64_t f = 0; f < cd.n_faces; ++f) dyn_faces.push_back((uint32_t)(face0 + f));
-                if (cd.n_faces >= GRID_MIN_FACES) {
-                    // Hierarchical table: four times the level-0 key-box cells
-                    // of the faces at the reference positions, a power of two.
-                    size_t inserts = 0;
-                    for (int64_t f = 0; f < cd.n_faces; ++f) {
-                        double x[4][3], e1[3], e2[3], nr[3], ctr[3], klo[3], khi[3];
-                        for (int j = 0; j < 4; ++j)
-                            for (int dd = 0; dd < 3; ++dd) x[j][dd] = cm.positions[3 * (size_t)faces[4 * (face0 + f) + j] + dd];
-                        for (int dd = 0; dd < 3; ++dd) { e1[dd] = x[1][dd] - x[0][dd]; e2[dd] = x[2][dd] - x[0][dd]; }
-                        nr[0] = e1[1] * e2[2] - e1[2] * e2[1];
-                        nr[1] = e1[2] * e2[0] - e1[0] * e2[2];
-                        nr[2] = e1[0] * e2[1] - e1[1] * e2[0];
-                        const double len = std::sqrt(nr[0] * nr[0] + nr[1] * nr[1] + nr[2] * nr[2]);
-                        for (int dd = 0; dd < 3; ++dd) {
-                            nr[dd] = len > 0.0 ? nr[dd] / len : 0.0;
-                            ctr[dd] = (((x[0][dd] + x[1][dd]) + x[2][dd]) + x[3][dd]) / 4.0;
-                        }
-                        face_key_box(x, nr, ctr, cd.max_distance, klo, khi);
-                        double cells = 1.0;
-                        for (int dd = 0; dd < 3; ++dd) cells *= std::floor(khi[dd] / cs) - std::floor(klo[dd] / cs) + 1.0;
-                        inserts += (size_t)std::min(std::isfinite(cells) && cells > 0.0 ? cells : 0.0, (double)LEVEL_CELL_BUDGET);
-                    }
-                    t = next_pow2(std::max<size_t>(1024, 4 * inserts));
-                }
-            }
-            tab_off.push_back(tab_off.back() + (int)t);
-            st_tab_off.push_back(st_tab_off.back() + (long long)st);
-            is_static.push_back(stat && st > 0 ? 1 : 0);
-            stiff.push_back(cd.stiffness);
-            md.push_back(cd.max_distance);
-            cell.push_back(cs);
-            counts_for_stop.push_back(stop ? 1 : 0);
-            contact_slot.push_back(sidx);
-        }
-        slot_contact_off.push_back(kc);
-        // Roles of this slot's nodes.
-        std::sort(items.begin(), items.end(), [](const RoleItem& x, const RoleItem& y) {
-            return x.node != y.node ? x.node < y.node : (x.contact != y.contact ? x.contact < y.contact : x.seq < y.seq);
-        });
-        for (size_t i0 = 0; i0 < items.size();) {
-            size_t i1 = i0;
-            while (i1 < items.size() && items[i1].node == items[i0].node) ++i1;
-            cnode.push_back(items[i0].node);
-            for (size_t a0 = i0; a0 < i1;) {
-                size_t a1 = a0;
-                while (a1 < i1 && items[a1].contact == items[a0].contact) ++a1;
-                // One role per primary-node entry (or one without), the faces on the last.
-                int n_slave_roles = 0;
-                for (size_t q = a0; q < a1; ++q) n_slave_roles += items[q].slave >= 0;
-                const int n_roles = std::max(n_slave_roles, 1);
-                int made = 0;
-                for (size_t q = a0; q < a1 && made < n_slave_roles; ++q)
-                    if (items[q].slave >= 0) {
-                        ++made;
-                        crole_contact.push_back(items[a0].contact);
-                        crole_slave.push_back(items[q].slave);
-                        if (made < n_roles) {
-                            crole_face.push_back(0);
-                            crole_faces_off.push_back((uint32_t)crole_faces.size());
-                        }
-                    }
-                if (n_slave_roles == 0) {
-                    crole_contact.push_back(items[a0].contact);
-                    crole_slave.push_back(-1);
-                }
-                int last = -1;
-                bool any_face = false;
-                for (size_t q = a0; q < a1; ++q)
-                    if (items[q].face >= 0 && items[q].face != last) {
-                        crole_faces.push_back(items[q].face);
-                        last = items[q].face;
-                        any_face = true;
-                    }
-                crole_face.push_back(any_face ? 1 : 0);
-                crole_faces_off.push_back((uint32_t)crole_faces.size());
-                a0 = a1;
-            }
-            cnode_off.push_back((uint32_t)crole_contact.size());
-            i0 = i1;
+    std::vector<Base> base(n_desc + 1);
+    base[0] = Base{0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int k = 0; k < n_desc; ++k) {
+        const ContactPart& cp = parts[k];
+        const Base& b0 = base[k];
+        base[k + 1] = Base{b0.face + (long long)cp.faces.size() / 4, b0.slave + (long long)cp.slaves.size(),
+                           b0.ste + (long long)cp.st_entries.size(), b0.stoff + (long long)cp.st_off.size(),
+                           b0.dyn + (long long)cp.dyn_faces.size(), b0.grid + (long long)cp.grid_faces.size(),
+                           b0.cnode + (long long)cp.cnode.size(), b0.role + (long long)cp.crole_contact.size(),
+                           b0.rface + (long long)cp.crole_faces.size()};
+        c->slots[k].contact_dt = cp.contact_dt;
+    }
+    const Base& tot = base[n_desc];
+    const int kc = K;
+    if (tot.face >= (1ll << 31) || tot.slave >= (1ll << 31) || tot.ste >= (1ll << 32) || tot.role >= (1ll << 32) || tot.rface >= (1ll << 31))
+        return crush::fail(CRUSH_ERR_INVALID, "contacts too large for one context");
+    std::vector<int> face_off(kc + 1), slave_off(kc + 1), tab_off(kc + 1), counts_for_stop(kc), face_contact(tot.face),
+        slave_contact(tot.slave), contact_slot(kc), slot_contact_off(n_desc + 1);
+    std::vector<uint32_t> faces(4 * tot.face), slaves(tot.slave), dyn_faces(tot.dyn), grid_faces(tot.grid);
+    std::vector<double> scales(tot.slave), stiff(kc), md(kc), cell(kc);
+    std::vector<uint8_t> is_static(kc);
+    std::vector<long long> st_tab_off(kc + 1);
+    std::vector<uint32_t> st_off(tot.stoff);
+    std::vector<int> st_entries(tot.ste);
+    std::vector<uint32_t> cnode(tot.cnode), cnode_off(tot.cnode + 1), crole_faces_off(tot.role + 1);
+    std::vector<int> crole_contact(tot.role), crole_slave(tot.role), crole_faces(tot.rface);
+    std::vector<uint8_t> crole_face(tot.role);
+    // per-contact prefix sums (serial, one entry per contact)
+    face_off[0] = slave_off[0] = tab_off[0] = 0;
+    st_tab_off[0] = 0;
+    for (int k = 0, q = 0; k < n_desc; ++k) {
+        const ContactPart& cp = parts[k];
+        slot_contact_off[k] = q;
+        for (size_t j = 0; j < cp.nf.size(); ++j, ++q) {
+            face_off[q + 1] = face_off[q] + cp.nf[j];
+            slave_off[q + 1] = slave_off[q] + cp.ns[j];
+            tab_off[q + 1] = tab_off[q] + cp.tab[j];
+            st_tab_off[q + 1] = st_tab_off[q] + cp.st[j];
+            is_static[q] = cp.stat[j];
+            counts_for_stop[q] = cp.stop[j];
+            contact_slot[q] = k;
+            stiff[q] = cp.stiff[j];
+            md[q] = cp.md[j];
+            cell[q] = cp.cell[j];
         }
     }
+    slot_contact_off[n_desc] = kc;
+    cnode_off[0] = 0;
+    crole_faces_off[0] = 0;
+    parallel_for(n_desc, [&](long long k) {
+        const ContactPart& cp = parts[k];
+        const Base& b = base[k];
+        const int q0 = c->slots[k].contact0;
+        for (size_t j = 0; j < cp.nf.size(); ++j) {
+            std::fill(face_contact.begin() + face_off[q0 + j], face_contact.begin() + face_off[q0 + j + 1], (int)(q0 + j));
+            std::fill(slave_contact.begin() + slave_off[q0 + j], slave_contact.begin() + slave_off[q0 + j + 1], (int)(q0 + j));
+        }
+        std::copy(cp.faces.begin(), cp.faces.end(), faces.begin() + 4 * b.face);
+        std::copy(cp.slaves.begin(), cp.slaves.end(), slaves.begin() + b.slave);
+        std::copy(cp.scales.begin(), cp.scales.end(), scales.begin() + b.slave);
+        for (size_t j = 0; j < cp.st_off.size(); ++j) st_off[b.stoff + j] = cp.st_off[j] + (uint32_t)b.ste;
+        std::copy(cp.st_entries.begin(), cp.st_entries.end(), st_entries.begin() + b.ste);
+        for (size_t j = 0; j < cp.dyn_faces.size(); ++j) dyn_faces[b.dyn + j] = cp.dyn_faces[j] + (uint32_t)b.face;
+        for (size_t j = 0; j < cp.grid_faces.size(); ++j) grid_faces[b.grid + j] = cp.grid_faces[j] + (uint32_t)b.face;
+        std::copy(cp.cnode.begin(), cp.cnode.end(), cnode.begin() + b.cnode);
+        for (size_t j = 1; j < cp.cnode_off.size(); ++j) cnode_off[b.cnode + j] = cp.cnode_off[j] + (uint32_t)b.role;
+        std::copy(cp.crole_contact.begin(), cp.crole_contact.end(), crole_contact.begin() + b.role);
+        std::copy(cp.crole_slave.begin(), cp.crole_slave.end(), crole_slave.begin() + b.role);
+        std::copy(cp.crole_face.begin(), cp.crole_face.end(), crole_face.begin() + b.role);
+        std::copy(cp.crole_faces.begin(), cp.crole_faces.end(), crole_faces.begin() + b.rface);
+        for (size_t j = 1; j < cp.crole_faces_off.size(); ++j) crole_faces_off[b.role + j] = cp.crole_faces_off[j] + (uint32_t)b.rface;
+    });
+    parts.clear();
+    parts.shrink_to_fit();
     c->n_contacts = kc;
     c->n_faces = face_off.back();
     c->n_slaves = slave_off.back();
@@ -682,12 +977,9 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->alloc(&ca.blen, std::max(tab_off.back(), 1)));
     {
         std::vector<long long> ent_off(1, 0);
-        std::vector<uint32_t> grid_faces;
         for (int k = 0; k < kc; ++k) {
             const bool g = tab_off[k + 1] > tab_off[k];
             ent_off.push_back(ent_off.back() + (g ? (long long)(face_off[k + 1] - face_off[k]) * LEVEL_CELL_BUDGET : 0));
-            if (g)
-                for (int f = face_off[k]; f < face_off[k + 1]; ++f) grid_faces.push_back((uint32_t)f);
         }
         TRY(c->upload_const(&ca.ent_off, ent_off));
         TRY(c->alloc(&ca.entries, (size_t)std::max<long long>(ent_off.back(), 1)));
@@ -695,6 +987,8 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
         TRY(c->upload_const(&ca.grid_faces, grid_faces));
     }
     TRY(c->alloc(&ca.ent_cursor, std::max(kc, 1)));
+    TRY(c->alloc(&ca.gather_work, std::max<size_t>(cnode.size(), 1)));
+    TRY(c->alloc(&ca.gather_count, 1));
     ca.n_buckets = tab_off.back();
     ca.exhaustive = 0;
     c->tab_off_h = tab_off;
@@ -742,6 +1036,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     CK(cudaMemsetAsync(ca.pen_count, 0, sizeof(unsigned long long) * std::max(c->n_contacts, 1), c->stream));
     CK(cudaMemsetAsync(ca.pen_max_bits, 0, sizeof(unsigned long long) * std::max(c->n_contacts, 1), c->stream));
     CK(cudaMemsetAsync(ca.face_hits, 0, sizeof(int) * std::max<long long>(c->n_faces, 1), c->stream));
+    trace.mark("contacts");
 
     // ---- vehicles ----
     std::vector<long long> voff(1, 0);
@@ -756,20 +1051,23 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
         c->slots[sidx].n_vehicles = nv;
         for (int k = 0; k < nv; ++k) {
             const crush_vehicle& vd = d->vehicles[k];
+            if (vd.n_nodes < 0 || (vd.n_nodes > 0 && !vd.nodes) || vd.n_front < 0 || (vd.n_front > 0 && !vd.front_nodes))
+                return crush::fail(CRUSH_ERR_INVALID, "invalid vehicle");
+            const size_t b = vnodes.size();
+            vnodes.resize(b + vd.n_nodes);
             for (int64_t i = 0; i < vd.n_nodes; ++i) {
                 if (vd.nodes[i] >= (uint64_t)d->n_nodes) return crush::fail(CRUSH_ERR_INVALID, "vehicle node out of range");
-                vnodes.push_back((uint32_t)(n0 + vd.nodes[i]));
+                vnodes[b + i] = (uint32_t)(n0 + vd.nodes[i]);
             }
             max_vnodes = std::max<long long>(max_vnodes, vd.n_nodes);
             voff.push_back((long long)vnodes.size());
             if (vd.accel_node >= (uint64_t)d->n_nodes) return crush::fail(CRUSH_ERR_INVALID, "accelerometer node out of range");
-            c->veh_accel.push_back((uint32_t)(n0 + vd.accel_node));
-            std::vector<uint32_t> fr;
             for (int64_t i = 0; i < vd.n_front; ++i) {
                 if (vd.front_nodes[i] >= (uint64_t)d->n_nodes) return crush::fail(CRUSH_ERR_INVALID, "front node out of range");
-                fr.push_back((uint32_t)(n0 + vd.front_nodes[i]));
+                c->crush_nodes_h.push_back((uint32_t)(n0 + vd.front_nodes[i]));
             }
-            c->veh_front.push_back(fr);
+            c->crush_nodes_h.push_back((uint32_t)(n0 + vd.accel_node));
+            c->crush_off_h.push_back(c->crush_nodes_h.size());
             vslot.push_back(sidx);
             vlocal.push_back(k);
         }
@@ -782,6 +1080,11 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->upload_const(&va.slot, vslot));
     TRY(c->upload_const(&va.local, vlocal));
     TRY(c->alloc(&c->veh_out, 7 * std::max(va.n_vehicles, 1)));
+    TRY(c->upload(&c->crush_nodes, c->crush_nodes_h.data(), c->crush_nodes_h.size()));
+    TRY(c->alloc(&c->crush_ux, std::max<size_t>(c->crush_nodes_h.size(), 1)));
+    stager.release();
+    c->stager = nullptr;
+    trace.mark("vehicles");
 
     // ---- time step per slot (src/solver.rs:214-228; contact_dt above) ----
     launch_init_state(c->stream, c->n_hc, c->stride, c->state);
@@ -816,6 +1119,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
         sl.dt_floor = sl.settings.mass_scaling > 0.0 ? sl.settings.mass_scaling * sl.stable : 0.0;
         sl.dt0 = sl.settings.time_step > 0.0 ? sl.settings.time_step : sl.stable * sl.settings.dt_scale;
     }
+    trace.mark("initial stable step");
     c->period = std::lcm(c->check_steps, 20);
     if (c->period > 200) c->period = 0;  // no graph for odd periods
     return CRUSH_OK;
@@ -849,9 +1153,8 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
     mark(1);
     if (c->n_contacts > 0) {
         launch_contact(c->stream, c->ca, nd, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 0.0, c->mass,
-                       c->f_ext, 1);
-        n += (c->ca.n_dyn_faces > 0 ? 1 : 0) + (c->ca.n_buckets > 0 && !c->ca.exhaustive ? (c->ca.n_grid_faces > 0 ? 2 : 1) : 0) +
-             (c->n_slaves > 0 ? 1 : 0) + 1;
+                       c->f_ext, 1, c->slave_lanes);
+        n += contact_launches(c->ca, true, c->n_faces, c->n_slaves, 0, c->ca.n_buckets);
     }
     mark(2);
     launch_half(c->stream, nd, c->ctls);
@@ -874,6 +1177,59 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
     ++n;
     mark(6);
     return check_launch(c, n);
+}
+
+constexpr long long RETUNE_STEPS = 1000;
+
+// Launch autotuner: times the run's contact pass (at the open run's state,
+// output into scratch, no state change) with 4, 8, 16 and 32 lanes per
+// primary-node search, three passes each after a warm-up, and keeps the
+// fastest. Every choice finds the same hits; only the speed differs.
+int autotune(crush_ctx* c) {
+    c->tuned = true;
+    for (double& x : c->tune_ms) x = 0.0;
+    if (c->n_slaves == 0 || c->n_contacts == 0) return CRUSH_OK;
+    cudaEvent_t t0, t1;
+    CK(cudaEventCreate(&t0));
+    CK(cudaEventCreate(&t1));
+    const int options[4] = {4, 8, 16, 32};
+    double best = INF;
+    int best_lanes = c->slave_lanes;
+    NodeArrays nd = c->nd();
+    int st = CRUSH_OK;
+    for (int k = 0; k < 4 && st == CRUSH_OK; ++k) {
+        const int lanes = options[k];
+        for (int rep = 0; rep < 4; ++rep) {
+            if (rep == 1) cudaEventRecord(t0, c->stream);
+            launch_contact(c->stream, c->ca, nd, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 0.0, c->mass,
+                           c->f_tmp, 1, lanes);
+            st = check_launch(c, contact_launches(c->ca, true, c->n_faces, c->n_slaves, 0, c->ca.n_buckets));
+            if (st != CRUSH_OK) break;
+        }
+        cudaEventRecord(t1, c->stream);
+        cudaEventSynchronize(t1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, t0, t1);
+        c->tune_ms[k] = ms / 3.0;
+        if (c->tune_ms[k] < best) {
+            best = c->tune_ms[k];
+            best_lanes = lanes;
+        }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (st != CRUSH_OK) return st;
+    // The passes counted penetrations; the run starts from none.
+    CK(cudaMemsetAsync(c->ca.pen_count, 0, sizeof(unsigned long long) * c->n_contacts, c->stream));
+    CK(cudaMemsetAsync(c->ca.pen_max_bits, 0, sizeof(unsigned long long) * c->n_contacts, c->stream));
+    if (best_lanes != c->slave_lanes) {
+        c->slave_lanes = best_lanes;
+        if (c->graph) {
+            cudaGraphExecDestroy(c->graph);
+            c->graph = nullptr;
+        }
+    }
+    return CRUSH_OK;
 }
 
 int run_begin(crush_ctx* c) {
@@ -925,7 +1281,12 @@ int run_begin(crush_ctx* c) {
     if (st != CRUSH_OK) return st;
     CK(cudaMemcpyAsync(c->ctls, h.data(), sizeof(Control) * h.size(), cudaMemcpyHostToDevice, c->stream));
     c->host_step = 0;
+    c->last_tune_step = 0;
     c->run_open = true;
+    if (!c->tuned) {
+        st = autotune(c);
+        if (st != CRUSH_OK) return st;
+    }
     return sync(c);
 }
 
@@ -964,6 +1325,13 @@ int issue_steps(crush_ctx* c, long long n_steps) {
     long long issued = 0;
     int st;
     while (issued < n_steps) {
+        // Crushed faces change the contact search as a run goes on: re-tune
+        // every RETUNE_STEPS steps, on a graph boundary.
+        if (c->host_step - c->last_tune_step >= RETUNE_STEPS && (c->period == 0 || c->host_step % c->period == 0)) {
+            st = autotune(c);
+            if (st != CRUSH_OK) return st;
+            c->last_tune_step = c->host_step;
+        }
         const bool use_graph = c->period > 0 && c->host_step % c->period == 0 && n_steps - issued >= c->period;
         if (use_graph) {
             if (!c->graph) {
@@ -1014,48 +1382,58 @@ int run_steps(crush_ctx* c, long long n_steps, int* done) {
     return CRUSH_OK;
 }
 
-int results(crush_ctx* c, int slot, crush_results* r) {
-    if (slot < 0 || slot >= c->n_slots) return crush::fail(CRUSH_ERR_INVALID, "slot out of range");
-    Control h;
-    CK(cudaMemcpyAsync(&h, c->ctls + slot, sizeof(Control), cudaMemcpyDeviceToHost, c->stream));
-    const Slot& sl = c->slots[slot];
-    std::vector<double> sums(7 * std::max(c->va.n_vehicles, 1));
+// Results of slots [s0, s1) into r[0, s1 - s0): one FP64 vehicle-sum launch
+// and one gather of the u_x values the crush measure needs, then the
+// per-vehicle arithmetic on the host (src/bin/crushrs.rs:237-271).
+int results_range(crush_ctx* c, int s0, int s1, crush_results* r) {
+    if (s0 < 0 || s1 > c->n_slots || s0 >= s1) return crush::fail(CRUSH_ERR_INVALID, "slot out of range");
+    std::vector<Control> h(s1 - s0);
+    CK(cudaMemcpyAsync(h.data(), c->ctls + s0, sizeof(Control) * h.size(), cudaMemcpyDeviceToHost, c->stream));
+    std::vector<double> sums(7 * std::max(c->va.n_vehicles, 1)), ux(std::max<size_t>(c->crush_nodes_h.size(), 1));
     if (c->va.n_vehicles > 0) {
         launch_vehicle_sums(c->stream, c->va, c->mass, c->v, c->v0, c->veh_out);
-        int st = check_launch(c, 1);
+        launch_gather_ux(c->stream, (long long)c->crush_nodes_h.size(), c->crush_nodes, c->u, c->crush_ux);
+        int st = check_launch(c, 2);
         if (st != CRUSH_OK) return st;
         CK(cudaMemcpyAsync(sums.data(), c->veh_out, sizeof(double) * 7 * c->va.n_vehicles, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(ux.data(), c->crush_ux, sizeof(double) * c->crush_nodes_h.size(), cudaMemcpyDeviceToHost, c->stream));
     }
-    // Crush needs u_x of the slot's accelerometer and front nodes only.
-    std::vector<double> u(3 * sl.n_nodes);
-    CK(cudaMemcpyAsync(u.data(), c->u + 3 * sl.node0, sizeof(double) * 3 * sl.n_nodes, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    std::memset(r, 0, sizeof(*r));
-    r->time = h.t;
-    r->steps = h.step;
-    r->eroded_elements = h.eroded_total;
-    r->dt_min = h.dt_min;
-    r->added_mass_max = h.added_mass_max;
-    r->status = h.status;
-    r->n_vehicles = sl.n_vehicles;
-    for (int k = 0; k < sl.n_vehicles; ++k) {
-        const int gv = sl.vehicle0 + k;
-        const double* s = sums.data() + 7 * gv;
-        crush_vehicle_result& vr = r->vehicle[k];
-        vr.mass = s[0];
-        for (int dd = 0; dd < 3; ++dd) {
-            double v1 = s[0] > 0.0 ? s[1 + dd] / s[0] : 0.0;
-            double v0 = s[0] > 0.0 ? s[4 + dd] / s[0] : 0.0;
-            vr.velocity[dd] = v1;
-            vr.delta_v[dd] = v1 - v0;
+    for (int slot = s0; slot < s1; ++slot) {
+        const Control& x = h[slot - s0];
+        const Slot& sl = c->slots[slot];
+        crush_results* out = r + (slot - s0);
+        std::memset(out, 0, sizeof(*out));
+        out->time = x.t;
+        out->steps = x.step;
+        out->eroded_elements = x.eroded_total;
+        out->dt_min = x.dt_min;
+        out->added_mass_max = x.added_mass_max;
+        out->status = x.status;
+        out->n_vehicles = sl.n_vehicles;
+        for (int k = 0; k < sl.n_vehicles; ++k) {
+            const int gv = sl.vehicle0 + k;
+            const double* sv = sums.data() + 7 * gv;
+            crush_vehicle_result& vr = out->vehicle[k];
+            vr.mass = sv[0];
+            for (int dd = 0; dd < 3; ++dd) {
+                double v1 = sv[0] > 0.0 ? sv[1 + dd] / sv[0] : 0.0;
+                double v0 = sv[0] > 0.0 ? sv[4 + dd] / sv[0] : 0.0;
+                vr.velocity[dd] = v1;
+                vr.delta_v[dd] = v1 - v0;
+            }
+            // u_x of the front nodes in order, then of the accelerometer
+            const size_t f0 = c->crush_off_h[gv], f1 = c->crush_off_h[gv + 1] - 1;
+            double fu = 0.0;
+            for (size_t q = f0; q < f1; ++q) fu += ux[q];
+            fu = f1 > f0 ? fu / (double)(f1 - f0) : 0.0;
+            vr.crush = std::fabs(ux[f1] - fu);
         }
-        double fu = 0.0;
-        for (uint32_t n : c->veh_front[gv]) fu += u[3 * (size_t)(n - sl.node0)];
-        fu = c->veh_front[gv].empty() ? 0.0 : fu / (double)c->veh_front[gv].size();
-        vr.crush = std::fabs(u[3 * (size_t)(c->veh_accel[gv] - sl.node0)] - fu);
     }
     return CRUSH_OK;
 }
+
+int results(crush_ctx* c, int slot, crush_results* r) { return results_range(c, slot, slot + 1, r); }
 
 int reset_aux(crush_ctx* c, double dt_floor) {
     std::vector<Control> aux(c->n_slots);
@@ -1205,8 +1583,9 @@ int crush_contact_apply(crush_ctx* c, int id, const double* u, const double* v, 
     nd.u = c->u_tmp;
     const long long nf = c->face_off_h[id + 1] - c->face_off_h[id], ns = c->slave_off_h[id + 1] - c->slave_off_h[id];
     const long long bk0 = c->tab_off_h[id], bk1 = c->tab_off_h[id + 1];
-    launch_contact(c->stream, c->ca, nd, c->ctls_aux, id, id + 1, c->face_off_h[id], nf, ns, bk0, bk1, dt, m, c->f_tmp, 0);
-    int st = check_launch(c, (nf > 0 ? 1 : 0) + (bk1 > bk0 && !c->ca.exhaustive ? (nf > 0 ? 2 : 1) : 0) + (ns > 0 ? 1 : 0) + 1);
+    launch_contact(c->stream, c->ca, nd, c->ctls_aux, id, id + 1, c->face_off_h[id], nf, ns, bk0, bk1, dt, m, c->f_tmp, 0,
+                   c->slave_lanes);
+    int st = check_launch(c, contact_launches(c->ca, false, nf, ns, bk0, bk1));
     if (st != CRUSH_OK) return st;
     if (c->run_open && c->is_static_h[id]) {
         // The call rebuilt the static faces' geometry at its own u: restore
@@ -1373,6 +1752,23 @@ int crush_batch_results(crush_ctx* c, int slot, crush_results* r) {
     return results(c, slot, r);
 }
 
+int crush_autotune(crush_ctx* c, crush_tuning* out) {
+    if (!c) return crush::fail(CRUSH_ERR_INVALID, "null context");
+    if (!c->run_open) return crush::fail(CRUSH_ERR_INVALID, "no open run (call crush_run_begin)");
+    CK(cudaSetDevice(c->device));
+    int st = autotune(c);
+    if (st != CRUSH_OK) return st;
+    return crush_get_tuning(c, out);
+}
+
+int crush_get_tuning(const crush_ctx* c, crush_tuning* out) {
+    if (!c || !out) return crush::fail(CRUSH_ERR_INVALID, "null argument");
+    std::memset(out, 0, sizeof(*out));
+    out->slave_lanes = c->slave_lanes;
+    for (int k = 0; k < 4; ++k) out->contact_ms[k] = c->tune_ms[k];
+    return CRUSH_OK;
+}
+
 int crush_set_contact_search(crush_ctx* c, int exhaustive) {
     if (!c || (exhaustive != 0 && exhaustive != 1)) return crush::fail(CRUSH_ERR_INVALID, "exhaustive must be 0 or 1");
     if (c->ca.exhaustive != exhaustive) {
@@ -1473,11 +1869,7 @@ int crush_batch_run(crush_ctx* c, crush_results* r) {
     CK(cudaSetDevice(c->device));
     int st = run_to_end(c);
     if (st != CRUSH_OK) return st;
-    for (int k = 0; k < c->n_slots; ++k) {
-        st = results(c, k, r + k);
-        if (st != CRUSH_OK) return st;
-    }
-    return CRUSH_OK;
+    return results_range(c, 0, c->n_slots, r);
 }
 
 }  // extern "C"

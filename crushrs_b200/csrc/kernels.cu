@@ -875,21 +875,21 @@ __device__ __forceinline__ bool face_hit(const FaceGeo& g, const double* p, doub
     return inside;
 }
 
-constexpr int SLAVE_LANES = 32;
-
-// First-hit search: SLAVE_LANES lanes per primary node test the faces its
-// broad phase offers — the static grid's bucket, or the dynamic grid's bucket
-// at every level in use plus the contact's overflow faces — or every face of
-// the contact when it has no grid (small contacts), a dynamic bucket
-// overflowed, or this is a drop-in call on a static contact; and keep the
-// smallest face index that hits: the face the reference's in-order scan with
-// `break` finds (src/contact.rs:115-157).
+// First-hit search: LANES lanes per primary node (a power of two <= 32,
+// chosen per context by the launch autotuner) test the faces its broad phase
+// offers — the static grid's bucket, or the dynamic grid's bucket at every
+// level in use plus the contact's overflow faces — or every face of the
+// contact when it has no grid (small contacts), its overflow list overran, or
+// this is a drop-in call on a static contact; and keep the smallest face
+// index that hits: the face the reference's in-order scan with `break` finds
+// (src/contact.rs:115-157).
+template <int LANES>
 __global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, int c1, int run_mode, double dt_override,
                                  const double* __restrict__ masses) {
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x % SLAVE_LANES;
+    const int lane = threadIdx.x % LANES;
     const long long s_begin = ca.slave_off[c0], s_end = ca.slave_off[c1];
-    const long long s = s_begin + gid / SLAVE_LANES;
+    const long long s = s_begin + gid / LANES;
     bool live = s < s_end;
     const Control* ctl = nullptr;
     if (live) {
@@ -921,7 +921,7 @@ __global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctls,
             const unsigned mask = (unsigned)(st1 - st0 - 1);
             const long long bk = st0 + (point_cell_hash(p, ca.cell[c], 0) & mask);
             const uint32_t e0 = ca.st_off[bk + c], e1 = ca.st_off[bk + c + 1];
-            for (uint32_t k = e0 + lane; k < e1; k += SLAVE_LANES) {
+            for (uint32_t k = e0 + lane; k < e1; k += LANES) {
                 const int f = ca.st_entries[k];
                 if (f < best && face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; }
             }
@@ -934,13 +934,13 @@ __global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctls,
                 const int b = tab + (int)(point_cell_hash(p, cs, level) & mask);
                 const unsigned e0 = ca.boff[b];
                 const int cnt = ca.blen[b];
-                for (int k = lane; k < cnt; k += SLAVE_LANES) {
+                for (int k = lane; k < cnt; k += LANES) {
                     const int f = ca.entries[e0 + k];
                     if (f < best && face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; }
                 }
             }
             const int no = min(ca.n_overflow[c], ca.overflow_cap);
-            for (int k = lane; k < no; k += SLAVE_LANES) {
+            for (int k = lane; k < no; k += LANES) {
                 const int f = ca.overflow[(long long)c * ca.overflow_cap + k];
                 if (f < best && face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; }
             }
@@ -949,13 +949,13 @@ __global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctls,
             if (dyn_grid && !ca.exhaustive && lane == 0) atomicAdd(&ca.search_stats[3 * c], 1ull);
         }
         if (all)
-            for (int f = lane; f < nf; f += SLAVE_LANES)
+            for (int f = lane; f < nf; f += LANES)
                 if (f < best && face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; }
     }
 #pragma unroll
-    for (int off = SLAVE_LANES / 2; off > 0; off >>= 1) {
-        const int ob = __shfl_down_sync(0xffffffffu, best, off, SLAVE_LANES);
-        const double osd = __shfl_down_sync(0xffffffffu, best_sd, off, SLAVE_LANES);
+    for (int off = LANES / 2; off > 0; off >>= 1) {
+        const int ob = __shfl_down_sync(0xffffffffu, best, off, LANES);
+        const double osd = __shfl_down_sync(0xffffffffu, best_sd, off, LANES);
         if (ob < best) { best = ob; best_sd = osd; }
     }
     if (!live || lane != 0) return;
@@ -982,119 +982,137 @@ __global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctls,
 
 constexpr int MAX_NODE_EVENTS = 48;
 constexpr int GATHER_TPB = 128;
+constexpr int WALK_BLOCKS = 296;  // 2 x 148 SMs of 4 warps
 
-// Ordered reaction gather, one warp per contact node: for each of its
-// contacts (in order) lane 0 collects the node's own hit (+F) and the hits on
-// the faces it belongs to (-F/4), sorts them by primary-node order (own
-// before face for the same primary node) and sums them in that order — the
-// sequence in which src/contact.rs:146-153 adds them to f_ext. When the
-// per-face hit lists overflowed, the whole warp walks the contact's primary
-// nodes in order instead, 32 at a time, and applies the matching hits in
-// order. Then the grid is cleared for the next build.
+// Lane 0's part of one role of contact node n (contact c, own primary-node
+// entry `own` or -1): collect its own hit (+F) and the hits on the faces it
+// belongs to (-F/4), sort them by primary-node order (own before face for the
+// same primary node) and add them in that order to (sx, sy, sz) — the
+// sequence in which src/contact.rs:146-153 adds them to f_ext. Returns false,
+// adding nothing, when the per-face hit lists overflowed.
+__device__ __forceinline__ bool role_sum(const ContactArrays& ca, uint32_t r, int c, int own, double& sx, double& sy, double& sz) {
+    const long long sb = ca.slave_off[c];
+    unsigned long long ev[MAX_NODE_EVENTS];
+    int ne = 0;
+    if (own >= 0 && ca.hit[sb + own] >= 0) ev[ne++] = 2ull * (unsigned long long)(sb + own);
+    for (uint32_t q = ca.crole_faces_off[r]; q < ca.crole_faces_off[r + 1]; ++q) {
+        const long long f = ca.face_off[c] + ca.crole_faces[q];
+        const int cnt = ca.face_hits[f];
+        if (cnt > FACE_HIT_CAP || ne + cnt > MAX_NODE_EVENTS) return false;
+        for (int k = 0; k < cnt; ++k) ev[ne++] = 2ull * (unsigned long long)ca.face_list[f * FACE_HIT_CAP + k] + 1ull;
+    }
+    for (int a = 1; a < ne; ++a) {  // insertion sort, tiny lists
+        unsigned long long key = ev[a];
+        int b = a - 1;
+        while (b >= 0 && ev[b] > key) { ev[b + 1] = ev[b]; --b; }
+        ev[b + 1] = key;
+    }
+    for (int a = 0; a < ne; ++a) {
+        const long long s = (long long)(ev[a] >> 1);
+        const double fx = ca.hit_force[3 * s], fy = ca.hit_force[3 * s + 1], fz = ca.hit_force[3 * s + 2];
+        if (ev[a] & 1ull) { sx -= 0.25 * fx; sy -= 0.25 * fy; sz -= 0.25 * fz; }
+        else { sx += fx; sy += fy; sz += fz; }
+    }
+    return true;
+}
+
+// Ordered reaction gather, one thread per contact node, over its contacts in
+// order. A node whose per-face hit lists overflowed is handed to
+// k_contact_gather_walk instead (its output is written there). Then the grid
+// bookkeeping is cleared for the next build.
 __global__ void __launch_bounds__(GATHER_TPB) k_contact_gather(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, int c1,
                                                                int run_mode, double* __restrict__ f_out, int skip_fixed) {
-    const long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // warp-uniform
-    const int lane = threadIdx.x & 31;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < ca.n_cnodes) {
         const long long n = ca.cnode[i];
         if (!(skip_fixed && nd.fixed[n]) && !(run_mode && ctls[nd.node_slot[n]].done)) {
-            double sx = 0.0, sy = 0.0, sz = 0.0;  // lane 0's sum
-            bool touched = false;
-            for (uint32_t r = ca.cnode_off[i]; r < ca.cnode_off[i + 1]; ++r) {
+            double sx = 0.0, sy = 0.0, sz = 0.0;
+            bool touched = false, ok = true;
+            for (uint32_t r = ca.cnode_off[i]; r < ca.cnode_off[i + 1] && ok; ++r) {
                 const int c = ca.crole_contact[r];
                 if (c < c0 || c >= c1) continue;
                 touched = true;
-                const long long sb = ca.slave_off[c];
-                const int own = ca.crole_slave[r];
-                int overflow = 0;
-                if (lane == 0) {
-                    unsigned long long ev[MAX_NODE_EVENTS];
-                    int ne = 0;
-                    if (own >= 0 && ca.hit[sb + own] >= 0) ev[ne++] = 2ull * (unsigned long long)(sb + own);
-                    for (uint32_t q = ca.crole_faces_off[r]; q < ca.crole_faces_off[r + 1] && !overflow; ++q) {
-                        const long long f = ca.face_off[c] + ca.crole_faces[q];
-                        const int cnt = ca.face_hits[f];
-                        if (cnt > FACE_HIT_CAP) {
-                            overflow = 1;
-                            break;
-                        }
-                        for (int k = 0; k < cnt; ++k) {
-                            if (ne < MAX_NODE_EVENTS) ev[ne++] = 2ull * (unsigned long long)ca.face_list[f * FACE_HIT_CAP + k] + 1ull;
-                            else overflow = 1;
-                        }
-                    }
-                    if (!overflow) {
-                        for (int a = 1; a < ne; ++a) {  // insertion sort, tiny lists
-                            unsigned long long key = ev[a];
-                            int b = a - 1;
-                            while (b >= 0 && ev[b] > key) { ev[b + 1] = ev[b]; --b; }
-                            ev[b + 1] = key;
-                        }
-                        for (int a = 0; a < ne; ++a) {
-                            const long long s = (long long)(ev[a] >> 1);
-                            const double fx = ca.hit_force[3 * s], fy = ca.hit_force[3 * s + 1], fz = ca.hit_force[3 * s + 2];
-                            if (ev[a] & 1ull) { sx -= 0.25 * fx; sy -= 0.25 * fy; sz -= 0.25 * fz; }
-                            else { sx += fx; sy += fy; sz += fz; }
-                        }
-                    }
-                }
-                overflow = __shfl_sync(0xffffffffu, overflow, 0);
-                if (overflow) {
-                    // More events than the lists hold: the warp walks the
-                    // contact's primary nodes in order, 32 per round; every
-                    // lane applies the round's matches in lane order, so all
-                    // lanes hold lane 0's running sum.
-                    double wx = __shfl_sync(0xffffffffu, sx, 0), wy = __shfl_sync(0xffffffffu, sy, 0),
-                           wz = __shfl_sync(0xffffffffu, sz, 0);
-                    const long long se = ca.slave_off[c + 1];
-                    const uint32_t* faces = ca.faces + 4 * ca.face_off[c];
-                    for (long long s0 = sb; s0 < se; s0 += 32) {
-                        const long long s = s0 + lane;
-                        int kind = 0;  // bit 0: own hit, bit 1: hit on a face containing n
-                        double fx = 0.0, fy = 0.0, fz = 0.0;
-                        if (s < se) {
-                            const int h = ca.hit[s];
-                            if (h >= 0) {
-                                const uint32_t* qn = faces + 4 * (long long)h;
-                                kind = (s - sb == own ? 1 : 0) | ((qn[0] == n || qn[1] == n || qn[2] == n || qn[3] == n) ? 2 : 0);
-                                if (kind) {
-                                    fx = ca.hit_force[3 * s];
-                                    fy = ca.hit_force[3 * s + 1];
-                                    fz = ca.hit_force[3 * s + 2];
-                                }
-                            }
-                        }
-                        unsigned m = __ballot_sync(0xffffffffu, kind != 0);
-                        while (m) {
-                            const int l = __ffs(m) - 1;
-                            m &= m - 1;
-                            const int k = __shfl_sync(0xffffffffu, kind, l);
-                            const double gx = __shfl_sync(0xffffffffu, fx, l), gy = __shfl_sync(0xffffffffu, fy, l),
-                                         gz = __shfl_sync(0xffffffffu, fz, l);
-                            if (k & 1) { wx += gx; wy += gy; wz += gz; }
-                            if (k & 2) { wx -= 0.25 * gx; wy -= 0.25 * gy; wz -= 0.25 * gz; }
-                        }
-                    }
-                    sx = wx;
-                    sy = wy;
-                    sz = wz;
-                }
+                ok = role_sum(ca, r, c, ca.crole_slave[r], sx, sy, sz);
             }
-            if (touched && lane == 0) {
+            if (!ok) {
+                ca.gather_work[atomicAdd(ca.gather_count, 1)] = (int)i;
+            } else if (touched) {
                 f_out[3 * n] = sx;
                 f_out[3 * n + 1] = sy;
                 f_out[3 * n + 2] = sz;
             }
         }
     }
-    // Clear the grid for the next build.
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long nthreads = (long long)gridDim.x * blockDim.x;
-    for (long long c = c0 + t; c < c1; c += nthreads) {
+    for (long long c = c0 + i; c < c1; c += nthreads) {
         ca.n_overflow[c] = 0;
         ca.entry_overrun[c] = 0;
         ca.levels_used[c] = 0;
         ca.ent_cursor[c] = 0;
+    }
+}
+
+// The contact nodes whose hit lists overflowed, one warp per node (warps
+// stride over the list): lane 0 sums the roles whose lists fit; for a role
+// whose lists overflowed the warp walks the contact's primary nodes in order,
+// 32 per round, and every lane applies the round's matches in lane order, so
+// all lanes hold lane 0's running sum.
+__global__ void __launch_bounds__(GATHER_TPB) k_contact_gather_walk(ContactArrays ca, int c0, int c1, double* __restrict__ f_out) {
+    const int lane = threadIdx.x & 31;
+    const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const int count = *ca.gather_count;
+    for (long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < count; w += warps) {
+        const long long i = ca.gather_work[w];
+        const long long n = ca.cnode[i];
+        double sx = 0.0, sy = 0.0, sz = 0.0;  // lane 0's sum
+        for (uint32_t r = ca.cnode_off[i]; r < ca.cnode_off[i + 1]; ++r) {
+            const int c = ca.crole_contact[r];
+            if (c < c0 || c >= c1) continue;
+            const long long sb = ca.slave_off[c];
+            const int own = ca.crole_slave[r];
+            int ok = 1;
+            if (lane == 0) ok = role_sum(ca, r, c, own, sx, sy, sz) ? 1 : 0;
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (ok) continue;
+            double wx = __shfl_sync(0xffffffffu, sx, 0), wy = __shfl_sync(0xffffffffu, sy, 0), wz = __shfl_sync(0xffffffffu, sz, 0);
+            const long long se = ca.slave_off[c + 1];
+            const uint32_t* faces = ca.faces + 4 * ca.face_off[c];
+            for (long long s0 = sb; s0 < se; s0 += 32) {
+                const long long s = s0 + lane;
+                int kind = 0;  // bit 0: own hit, bit 1: hit on a face containing n
+                double fx = 0.0, fy = 0.0, fz = 0.0;
+                if (s < se) {
+                    const int h = ca.hit[s];
+                    if (h >= 0) {
+                        const uint32_t* qn = faces + 4 * (long long)h;
+                        kind = (s - sb == own ? 1 : 0) | ((qn[0] == n || qn[1] == n || qn[2] == n || qn[3] == n) ? 2 : 0);
+                        if (kind) {
+                            fx = ca.hit_force[3 * s];
+                            fy = ca.hit_force[3 * s + 1];
+                            fz = ca.hit_force[3 * s + 2];
+                        }
+                    }
+                }
+                unsigned m = __ballot_sync(0xffffffffu, kind != 0);
+                while (m) {
+                    const int l = __ffs(m) - 1;
+                    m &= m - 1;
+                    const int k = __shfl_sync(0xffffffffu, kind, l);
+                    const double gx = __shfl_sync(0xffffffffu, fx, l), gy = __shfl_sync(0xffffffffu, fy, l),
+                                 gz = __shfl_sync(0xffffffffu, fz, l);
+                    if (k & 1) { wx += gx; wy += gy; wz += gz; }
+                    if (k & 2) { wx -= 0.25 * gx; wy -= 0.25 * gy; wz -= 0.25 * gz; }
+                }
+            }
+            sx = wx;
+            sy = wy;
+            sz = wz;
+        }
+        if (lane == 0) {
+            f_out[3 * n] = sx;
+            f_out[3 * n + 1] = sy;
+            f_out[3 * n + 2] = sz;
+        }
     }
 }
 
@@ -1127,6 +1145,12 @@ __global__ void __launch_bounds__(VEH_TPB) k_vehicle_sums(VehicleArrays va, cons
     }
     if (threadIdx.x == 0)
         for (int k = 0; k < 7; ++k) out[7 * veh + k] = s[k][0];
+}
+
+// u_x of listed nodes (the crush measure's inputs).
+__global__ void k_gather_ux(long long n, const uint32_t* __restrict__ nodes, const double* __restrict__ u, double* __restrict__ out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = u[3 * (long long)nodes[i]];
 }
 
 // Blocks a vehicle's separation-rule reduction uses: one per 2048 nodes, at
@@ -1227,6 +1251,10 @@ void launch_vehicle_sums(cudaStream_t s, const VehicleArrays& va, const double* 
     if (va.n_vehicles <= 0) return;
     k_vehicle_sums<<<va.n_vehicles, VEH_TPB, 0, s>>>(va, mass, v, v0, out);
 }
+void launch_gather_ux(cudaStream_t s, long long n, const uint32_t* nodes, const double* u, double* out) {
+    if (n <= 0) return;
+    k_gather_ux<<<(unsigned)blocks_for(n, TPB), TPB, 0, s>>>(n, nodes, u, out);
+}
 void launch_vehicle_vx(cudaStream_t s, const VehicleArrays& va, const double* mass, const double* v, Control* ctls) {
     if (va.n_vehicles <= 0) return;
     k_vehicle_vx<<<(unsigned)(va.n_vehicles * va.vx_blocks), VEH_TPB, 0, s>>>(va, mass, v, ctls);
@@ -1234,7 +1262,7 @@ void launch_vehicle_vx(cudaStream_t s, const VehicleArrays& va, const double* ma
 
 void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
                     long long n_faces, long long n_slaves, long long bk0, long long bk1, double dt_override, const double* masses,
-                    double* f_out, int skip_fixed) {
+                    double* f_out, int skip_fixed, int lanes) {
     if (c1 <= c0) return;
     const int run_mode = dt_override > 0.0 ? 0 : 1;
     if (n_faces > 0) cudaMemsetAsync(ca.face_hits + f0, 0, sizeof(int) * n_faces, s);
@@ -1249,11 +1277,28 @@ void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& n
         if (n_glist > 0)
             k_contact_faces<<<(unsigned)blocks_for(n_glist, TPB), TPB, 0, s>>>(ca, nd, ctls, c0, glist, n_glist, run_mode, 1);
     }
-    if (n_slaves > 0)
-        k_contact_slaves<<<(unsigned)blocks_for(n_slaves * SLAVE_LANES, TPB), TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses);
+    if (n_slaves > 0) {
+        const unsigned g = (unsigned)blocks_for(n_slaves * lanes, TPB);
+        switch (lanes) {
+            case 4: k_contact_slaves<4><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses); break;
+            case 8: k_contact_slaves<8><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses); break;
+            case 16: k_contact_slaves<16><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses); break;
+            default: k_contact_slaves<32><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses); break;
+        }
+    }
+    cudaMemsetAsync(ca.gather_count, 0, sizeof(int), s);
     long long nodes = ca.n_cnodes > 0 ? ca.n_cnodes : 1;
-    k_contact_gather<<<(unsigned)blocks_for(nodes * 32, GATHER_TPB), GATHER_TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, f_out,
-                                                                                        skip_fixed);
+    k_contact_gather<<<(unsigned)blocks_for(nodes, GATHER_TPB), GATHER_TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, f_out, skip_fixed);
+    const long long walk_blocks = blocks_for(nodes * 32, GATHER_TPB);
+    k_contact_gather_walk<<<(unsigned)(walk_blocks < WALK_BLOCKS ? walk_blocks : WALK_BLOCKS), GATHER_TPB, 0, s>>>(ca, c0, c1, f_out);
+}
+
+int contact_launches(const ContactArrays& ca, bool run_mode, long long n_faces, long long n_slaves, long long bk0, long long bk1) {
+    int k = 2;  // gather + overflow walk
+    if ((run_mode ? ca.n_dyn_faces : n_faces) > 0) ++k;
+    if (bk1 > bk0 && !ca.exhaustive) k += (run_mode ? ca.n_grid_faces : n_faces) > 0 ? 2 : 1;
+    if (n_slaves > 0) ++k;
+    return k;
 }
 
 void launch_contact_geometry(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, int c0, int c1, long long f0,

@@ -123,6 +123,8 @@ struct ContactArrays {
     long long n_grid_faces;
     long long n_buckets;        // total dynamic buckets (tab_off[n_contacts])
     int exhaustive;             // 1: every search tests every face of its contact (no broad phase)
+    int* gather_work;           // contact nodes whose hit lists overflowed this pass (n_cnodes capacity)
+    int* gather_count;          // their number
 };
 
 // Vehicles of all crash slots: node lists and the reduction layout.
@@ -154,12 +156,15 @@ void launch_mass_scaling(cudaStream_t s, const ElementArrays& el, const NodeArra
 void launch_nonfinite(cudaStream_t s, const NodeArrays& nd, Control* ctls);
 void launch_step_end(cudaStream_t s, Control* ctls, const ContactArrays& ca, const VehicleArrays& va, int check_separation);
 // Contact pass over contacts [c0, c1) (faces [f0, f0 + n_faces), n_slaves
-// primary-node entries, dynamic grid buckets [bk0, bk1)). dt_override > 0 is a drop-in call: every face's
+// primary-node entries, dynamic grid buckets [bk0, bk1)); `lanes` lanes per
+// primary-node search (4, 8, 16 or 32). dt_override > 0 is a drop-in call: every face's
 // geometry is rebuilt and static contacts are searched exhaustively; the run
 // (dt_override = 0) rebuilds only the dynamic faces and uses the static grids.
 void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
                     long long n_faces, long long n_slaves, long long bk0, long long bk1, double dt_override, const double* masses,
-                    double* f_out, int skip_fixed);
+                    double* f_out, int skip_fixed, int lanes);
+// Kernel launches one launch_contact call issues.
+int contact_launches(const ContactArrays& ca, bool run_mode, long long n_faces, long long n_slaves, long long bk0, long long bk1);
 // Geometry of every face of contacts [c0, c1) at X + u (no grid insertion):
 // the static contacts' geometry for a run.
 void launch_contact_geometry(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, int c0, int c1, long long f0,
@@ -167,6 +172,7 @@ void launch_contact_geometry(cudaStream_t s, const ContactArrays& ca, const Node
 void launch_vehicle_sums(cudaStream_t s, const VehicleArrays& va, const double* mass, const double* v, const double* v0,
                          double* out7);
 void launch_vehicle_vx(cudaStream_t s, const VehicleArrays& va, const double* mass, const double* v, Control* ctls);
+void launch_gather_ux(cudaStream_t s, long long n, const uint32_t* nodes, const double* u, double* out);
 
 // Fixed-size scratch of the allocation-free contact call
 // (crush_contact_apply_static): one record in a static device array, so the

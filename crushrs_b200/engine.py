@@ -159,6 +159,18 @@ class Context:
     def launches(self):
         return self._lib.crush_launch_count(self.h)
 
+    def tuning(self):
+        """The autotuned launch schedule: (slave lanes, contact ms per lane option 4/8/16/32)."""
+        t = abi.Tuning()
+        check(self._lib.crush_get_tuning(self.h, C.byref(t)))
+        return t.slave_lanes, list(t.contact_ms)
+
+    def autotune(self):
+        """Re-tune at the open run's current state; returns tuning()."""
+        t = abi.Tuning()
+        check(self._lib.crush_autotune(self.h, C.byref(t)))
+        return t.slave_lanes, list(t.contact_ms)
+
     def set_contact_search(self, exhaustive):
         """True: every contact search tests every face (no broad phase)."""
         check(self._lib.crush_set_contact_search(self.h, int(bool(exhaustive))))
