@@ -210,8 +210,56 @@ def declare_engine_api(lib):
     lib.crush_batch_size.argtypes = [vp]
     lib.crush_batch_run.argtypes = [vp, P(Results)]
     lib.crush_batch_results.argtypes = [vp, C.c_int, P(Results)]
+    lib.crush_batch_results_range.argtypes = [vp, C.c_int, C.c_int, P(Results)]
+    lib.crush_batch_done.argtypes = [vp, P(C.c_int), P(C.c_int)]
+    lib.crush_server_create.argtypes = [P(ServerConfig), P(vp)]
+    lib.crush_server_submit.argtypes = [vp, P(ModelDesc), P(C.c_uint64)]
+    lib.crush_server_poll.argtypes = [vp, P(ServerResult), C.c_int, P(C.c_int), C.c_int]
+    lib.crush_server_stats_get.argtypes = [vp, P(ServerStats)]
+    lib.crush_server_destroy.argtypes = [vp]
+    lib.crush_server_destroy.restype = None
+    lib.crush_model_footprint.argtypes = [P(ModelDesc)]
+    lib.crush_model_footprint.restype = C.c_double
     lib.crush_contact_apply_static.argtypes = [C.c_int64, vp, vp, vp, C.c_int64, vp, vp, C.c_int64, vp,
                                                C.c_double, C.c_double, C.c_double, vp, vp, vp]
+
+
+class ServerConfig(C.Structure):
+    """crush_server_config (include/crush_server.h)."""
+    _fields_ = [
+        ("device", C.c_int32),
+        ("max_waves", C.c_int32),
+        ("max_wave_slots", C.c_int32),
+        ("chunk_steps", C.c_int32),
+        ("max_wave_elements", C.c_int64),
+        ("hbm_budget_bytes", C.c_double),
+        ("gather_ms", C.c_double),
+    ]
+
+
+class ServerResult(C.Structure):
+    _fields_ = [
+        ("ticket", C.c_uint64),
+        ("status", C.c_int32),
+        ("wave", C.c_int32),
+        ("submit_s", C.c_double),
+        ("start_s", C.c_double),
+        ("finish_s", C.c_double),
+        ("results", Results),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_int64),
+        ("completed", C.c_int64),
+        ("waves", C.c_int64),
+        ("queued", C.c_int64),
+        ("running", C.c_int64),
+        ("bytes_in_use", C.c_double),
+        ("peak_bytes_in_use", C.c_double),
+        ("budget_bytes", C.c_double),
+    ]
 
 
 class Tuning(C.Structure):

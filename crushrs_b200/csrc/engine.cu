@@ -220,6 +220,10 @@ struct crush_ctx {
     MaterialF32* mats = nullptr;
     Control* ctls = nullptr;      // the run, one per slot
     Control* ctls_aux = nullptr;  // drop-in calls, one per slot
+    int* slot_done = nullptr;     // per slot: done flag mirrored by the step-end kernel
+    ActiveBuild ab{};             // active chunk lists of the run
+    std::vector<long long> space_off_h;
+    std::vector<int> done_h;
 
     // contact
     ContactArrays ca{};
@@ -270,7 +274,31 @@ struct crush_ctx {
         e.elem_dt = elem_dt;
         e.elem_extra = elem_extra;
         e.elem_slot = elem_slot;
+        e.act_hc = e.act_all = Active{nullptr, nullptr};
         return e;
+    }
+    // The run's bundles: kernels visit only the active chunks.
+    ElementArrays el_run() const {
+        ElementArrays e = el();
+        e.act_hc = active(0);
+        e.act_all = active(1);
+        return e;
+    }
+    NodeArrays nd_run() const {
+        NodeArrays a = nd();
+        a.act_node = active(2);
+        return a;
+    }
+    ContactArrays ca_run() const {
+        ContactArrays x = ca;
+        x.act_slave = active(3);
+        x.act_cnode = active(4);
+        x.act_dynf = active(5);
+        return x;
+    }
+    Active active(int space) const {
+        if (!ab.lists) return Active{nullptr, nullptr};
+        return Active{ab.lists + space_off_h[space], ab.counts + space};
     }
     NodeArrays nd() const {
         NodeArrays a;
@@ -290,6 +318,7 @@ struct crush_ctx {
         a.all_off = all_off;
         a.all_slot = all_slot;
         a.node_slot = node_slot;
+        a.act_node = Active{nullptr, nullptr};
         return a;
     }
 
@@ -845,6 +874,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->alloc(&c->corner, (size_t)24 * std::max<long long>(c->n_hc, 1)));
     TRY(c->alloc(&c->ctls, c->n_slots));
     TRY(c->alloc(&c->ctls_aux, c->n_slots));
+    TRY(c->alloc(&c->slot_done, c->n_slots));
     CK(cudaMemsetAsync(c->planes, 0, sizeof(float4) * N_STATIC_PLANES * c->stride, c->stream));
     CK(cudaMemsetAsync(c->eroded_all, 0, E, c->stream));
     CK(cudaMemsetAsync(c->ctls, 0, sizeof(Control) * c->n_slots, c->stream));
@@ -1082,6 +1112,49 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->alloc(&c->veh_out, 7 * std::max(va.n_vehicles, 1)));
     TRY(c->upload(&c->crush_nodes, c->crush_nodes_h.data(), c->crush_nodes_h.size()));
     TRY(c->alloc(&c->crush_ux, std::max<size_t>(c->crush_nodes_h.size(), 1)));
+    // ---- active chunk tables: slot range of every 256-entity chunk ----
+    {
+        const long long sizes[ACTIVE_SPACES] = {c->n_hc, E, N, (long long)slaves.size(), (long long)cnode.size(), (long long)dyn_faces.size()};
+        c->space_off_h.assign(ACTIVE_SPACES + 1, 0);
+        for (int sp = 0; sp < ACTIVE_SPACES; ++sp) c->space_off_h[sp + 1] = c->space_off_h[sp] + (sizes[sp] + CHUNK - 1) / CHUNK;
+        const long long nch = c->space_off_h[ACTIVE_SPACES];
+        std::vector<int> lo(nch), hi(nch);
+        auto slot_of = [&](int sp, long long i) -> int {
+            switch (sp) {
+                case 0: return (int)cm.elem_slot[c->hc_model[i]];
+                case 1: return (int)cm.elem_slot[i];
+                case 2: return (int)cm.node_slot[i];
+                case 3: return contact_slot[slave_contact[i]];
+                case 4: return (int)cm.node_slot[cnode[i]];
+                default: return contact_slot[face_contact[dyn_faces[i]]];
+            }
+        };
+        parallel_for(nch, [&](long long q) {
+            int sp = 0;
+            while (sp + 1 < ACTIVE_SPACES && q >= c->space_off_h[sp + 1]) ++sp;
+            const long long i0 = (q - c->space_off_h[sp]) * CHUNK, i1 = std::min(i0 + CHUNK, sizes[sp]);
+            int a = INT32_MAX, b = -1;
+            for (long long i = i0; i < i1; ++i) {
+                const int sl = slot_of(sp, i);
+                a = std::min(a, sl);
+                b = std::max(b, sl);
+            }
+            lo[q] = a;
+            hi[q] = b;
+        });
+        c->ab.n_chunks = nch;
+        const int* lo_d = nullptr;
+        const int* hi_d = nullptr;
+        const long long* off_d = nullptr;
+        TRY(c->upload_const(&lo_d, lo));
+        TRY(c->upload_const(&hi_d, hi));
+        TRY(c->upload_const(&off_d, c->space_off_h));
+        c->ab.chunk_lo = lo_d;
+        c->ab.chunk_hi = hi_d;
+        c->ab.space_off = off_d;
+        TRY(c->alloc(&c->ab.lists, std::max<long long>(nch, 1)));
+        TRY(c->alloc(&c->ab.counts, ACTIVE_SPACES));
+    }
     stager.release();
     c->stager = nullptr;
     trace.mark("vehicles");
@@ -1132,8 +1205,9 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
 constexpr int N_PHASE_EVENTS = 7;
 
 int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool capturing = false) {
-    ElementArrays el = c->el();
-    NodeArrays nd = c->nd();
+    ElementArrays el = c->el_run();
+    NodeArrays nd = c->nd_run();
+    ContactArrays cr = c->ca_run();
     int n = 0;
     // Inside a stream capture an event record must be an external event node
     // for its timestamp to be readable after the graph runs.
@@ -1144,6 +1218,11 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
         else cudaEventRecord(ev[i], c->stream);
     };
     mark(0);
+    // Every 20 steps: the chunks that still hold a running crash.
+    if (step % 20 == 0) {
+        launch_build_active(c->stream, c->ab, c->ctls);
+        ++n;
+    }
     if (c->adaptive && step % c->check_steps == 0) {
         launch_elem_dt(c->stream, el, nd, c->ctls, c->u, 1);
         launch_dt_finalize(c->stream, c->ctls, c->n_slots);
@@ -1152,7 +1231,7 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
     }
     mark(1);
     if (c->n_contacts > 0) {
-        launch_contact(c->stream, c->ca, nd, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 0.0, c->mass,
+        launch_contact(c->stream, cr, nd, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 0.0, c->mass,
                        c->f_ext, 1, c->slave_lanes);
         n += contact_launches(c->ca, true, c->n_faces, c->n_slaves, 0, c->ca.n_buckets);
     }
@@ -1173,7 +1252,7 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
         launch_vehicle_vx(c->stream, c->va, c->mass, c->v, c->ctls);
         ++n;
     }
-    launch_step_end(c->stream, c->ctls, c->ca, c->va, sep ? 1 : 0);
+    launch_step_end(c->stream, c->ctls, cr, c->va, sep ? 1 : 0, c->slot_done);
     ++n;
     mark(6);
     return check_launch(c, n);
@@ -1280,6 +1359,9 @@ int run_begin(crush_ctx* c) {
     st = check_launch(c, c->n_faces > 0 ? 1 : 0);
     if (st != CRUSH_OK) return st;
     CK(cudaMemcpyAsync(c->ctls, h.data(), sizeof(Control) * h.size(), cudaMemcpyHostToDevice, c->stream));
+    c->done_h.resize(c->n_slots);
+    for (int k = 0; k < c->n_slots; ++k) c->done_h[k] = h[k].done;
+    CK(cudaMemcpyAsync(c->slot_done, c->done_h.data(), sizeof(int) * c->n_slots, cudaMemcpyHostToDevice, c->stream));
     c->host_step = 0;
     c->last_tune_step = 0;
     c->run_open = true;
@@ -1363,11 +1445,11 @@ int issue_steps(crush_ctx* c, long long n_steps) {
 
 // Whether every slot has finished (device flags read back; synchronises).
 int all_done(crush_ctx* c, int* done) {
-    std::vector<Control> h(c->n_slots);
-    CK(cudaMemcpyAsync(h.data(), c->ctls, sizeof(Control) * h.size(), cudaMemcpyDeviceToHost, c->stream));
+    c->done_h.resize(c->n_slots);
+    CK(cudaMemcpyAsync(c->done_h.data(), c->slot_done, sizeof(int) * c->n_slots, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     int d = 1;
-    for (const Control& x : h) d &= x.done ? 1 : 0;
+    for (int x : c->done_h) d &= x ? 1 : 0;
     *done = d;
     return CRUSH_OK;
 }
@@ -1744,6 +1826,23 @@ int crush_run_results(crush_ctx* c, crush_results* r) {
     if (!c || !r) return crush::fail(CRUSH_ERR_INVALID, "null argument");
     CK(cudaSetDevice(c->device));
     return results(c, 0, r);
+}
+
+int crush_batch_done(crush_ctx* c, int* done_flags, int* all) {
+    if (!c) return crush::fail(CRUSH_ERR_INVALID, "null context");
+    CK(cudaSetDevice(c->device));
+    int d = 0;
+    int st = all_done(c, &d);
+    if (st != CRUSH_OK) return st;
+    if (done_flags) std::memcpy(done_flags, c->done_h.data(), sizeof(int) * c->n_slots);
+    if (all) *all = d;
+    return CRUSH_OK;
+}
+
+int crush_batch_results_range(crush_ctx* c, int first, int count, crush_results* r) {
+    if (!c || !r) return crush::fail(CRUSH_ERR_INVALID, "null argument");
+    CK(cudaSetDevice(c->device));
+    return results_range(c, first, first + count, r);
 }
 
 int crush_batch_results(crush_ctx* c, int slot, crush_results* r) {

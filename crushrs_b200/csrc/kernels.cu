@@ -31,6 +31,32 @@ constexpr int TPB = 256;
 
 __host__ __device__ inline long long blocks_for(long long n, int tpb) { return (n + tpb - 1) / tpb; }
 
+// Active-chunk iteration: thread g of the grid-stride loop handles entity
+// active_entity(g) (mult threads per entity, lane = the thread's rank among
+// them). Chunks are multiples of a warp, so the 32 lanes of a warp always
+// take the same number of iterations and stay converged.
+__device__ __forceinline__ long long active_total(const Active& a, long long n, int mult) {
+    const long long chunks = a.list ? (long long)*a.count : (n + CHUNK - 1) / CHUNK;
+    return chunks * CHUNK * mult;
+}
+__device__ __forceinline__ long long active_entity(const Active& a, long long g, int mult, int* lane) {
+    const long long per = (long long)CHUNK * mult;
+    const long long item = g / per, within = g - item * per;
+    const long long chunk = a.list ? (long long)a.list[item] : item;
+    *lane = (int)(within % mult);
+    return chunk * CHUNK + within / mult;
+}
+#define FOR_ACTIVE(a, n, mult, g) \
+    for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x, g##_end = active_total(a, n, mult); g < g##_end; \
+         g += (long long)gridDim.x * blockDim.x)
+
+// Grid of a FOR_ACTIVE launch: every chunk once, at most `cap` blocks.
+inline unsigned active_grid(long long n, int mult, int tpb, long long cap) {
+    const long long need = blocks_for(((n + CHUNK - 1) / CHUNK) * CHUNK * mult, tpb);
+    return (unsigned)(need < 1 ? 1 : (need < cap ? need : cap));
+}
+constexpr long long GRID_CAP = 148 * 64;
+
 // ---------------------------------------------------------------------------
 // Set-up geometry (f64), restating src/element.rs:141-162 (HexGeometry::new)
 // with the hourglass stiffness reduced directly to its rank-12 form.
@@ -306,8 +332,7 @@ __global__ void k_init_state(long long n_hc, long long stride, float4* __restric
 #ifndef FORCES_MINB
 #define FORCES_MINB 2
 #endif
-__global__ void __launch_bounds__(FORCES_TPB, FORCES_MINB) k_forces(ElementArrays el, NodeArrays nd, Control* ctls, int respect_done) {
-    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void forces_body(const ElementArrays& el, const NodeArrays& nd, Control* ctls, int respect_done, long long e) {
     if (e >= el.n_hc) return;
     const long long S = el.stride;
     const float4 meta = ld_plane(el.planes, S, P_META, e);
@@ -435,6 +460,13 @@ __device__ __forceinline__ void gather_node(const NodeArrays& nd, const float* _
     }
 }
 
+__global__ void __launch_bounds__(FORCES_TPB, FORCES_MINB) k_forces(ElementArrays el, NodeArrays nd, Control* ctls, int respect_done) {
+    FOR_ACTIVE(el.act_hc, el.n_hc, 1, g) {
+        int lane;
+        forces_body(el, nd, ctls, respect_done, active_entity(el.act_hc, g, 1, &lane));
+    }
+}
+
 __global__ void k_gather(ElementArrays el, NodeArrays nd, double* __restrict__ f_out) {
     long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= nd.n) return;
@@ -446,8 +478,7 @@ __global__ void k_gather(ElementArrays el, NodeArrays nd, double* __restrict__ f
 }
 
 // Half step: v½ = v + ½dt (f_ext - f_int)/m ; u += dt v½ ; fixed -> 0 (src/solver.rs:314-323).
-__global__ void k_half(NodeArrays nd, Control* ctls) {
-    long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void half_body(const NodeArrays& nd, const Control* ctls, long long n) {
     if (n >= nd.n) return;
     const Control* ctl = ctls + nd.node_slot[n];
     if (ctl->done) return;
@@ -469,9 +500,15 @@ __global__ void k_half(NodeArrays nd, Control* ctls) {
     }
 }
 
+__global__ void k_half(NodeArrays nd, Control* ctls) {
+    FOR_ACTIVE(nd.act_node, nd.n, 1, g) {
+        int lane;
+        half_body(nd, ctls, active_entity(nd.act_node, g, 1, &lane));
+    }
+}
+
 // Full step with the fused force gather: v = (v½ + ½dt a) damping (src/solver.rs:334-342).
-__global__ void k_full(ElementArrays el, NodeArrays nd, Control* ctls) {
-    long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void full_body(const ElementArrays& el, const NodeArrays& nd, const Control* ctls, long long n) {
     if (n >= nd.n) return;
     const Control* ctl = ctls + nd.node_slot[n];
     if (ctl->done) return;
@@ -487,6 +524,13 @@ __global__ void k_full(ElementArrays el, NodeArrays nd, Control* ctls) {
         double v = (nd.v_half[k] + 0.5 * dt * a) * damping;
         nd.v[k] = fixed ? 0.0 : v;
         nd.f_int[k] = f[d];
+    }
+}
+
+__global__ void k_full(ElementArrays el, NodeArrays nd, Control* ctls) {
+    FOR_ACTIVE(nd.act_node, nd.n, 1, g) {
+        int lane;
+        full_body(el, nd, ctls, active_entity(nd.act_node, g, 1, &lane));
     }
 }
 
@@ -535,9 +579,8 @@ constexpr int DT_TPB = 256;
 // Per-element stability limit and mass-scaling surplus. The minimum per crash
 // slot is an atomicMin on the bit pattern of a non-negative double (order
 // independent); lanes of a warp that share a slot reduce first.
-__global__ void __launch_bounds__(DT_TPB) k_elem_dt(ElementArrays el, NodeArrays nd, Control* ctls, const double* __restrict__ u,
-                                                    int respect_done) {
-    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void elem_dt_body(const ElementArrays& el, const NodeArrays& nd, Control* ctls, const double* __restrict__ u,
+                                             int respect_done, long long e) {
     const int lane = threadIdx.x & 31;
     uint32_t slot = 0xffffffffu;
     double dt = CUDART_INF, extra = 0.0;
@@ -584,6 +627,14 @@ __global__ void __launch_bounds__(DT_TPB) k_elem_dt(ElementArrays el, NodeArrays
     }
 }
 
+__global__ void __launch_bounds__(DT_TPB) k_elem_dt(ElementArrays el, NodeArrays nd, Control* ctls, const double* __restrict__ u,
+                                                    int respect_done) {
+    FOR_ACTIVE(el.act_all, el.n_all, 1, g) {
+        int lane;
+        elem_dt_body(el, nd, ctls, u, respect_done, active_entity(el.act_all, g, 1, &lane));
+    }
+}
+
 // The adaptive step decision of src/solver.rs:288-299, one thread per slot.
 __global__ void k_dt_finalize(Control* ctls, int n_slots) {
     const int sl = blockIdx.x * blockDim.x + threadIdx.x;
@@ -606,8 +657,8 @@ __global__ void k_dt_finalize(Control* ctls, int n_slots) {
 }
 
 // Added nodal mass (element order, src/kernel.rs:246-255) and 1/(m + added).
-__global__ void k_mass_scaling(ElementArrays el, NodeArrays nd, Control* ctls, int force_apply) {
-    long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void mass_scaling_body(const ElementArrays& el, const NodeArrays& nd, const Control* ctls, int force_apply,
+                                                  long long n) {
     if (n >= nd.n) return;
     const Control* ctl = ctls + nd.node_slot[n];
     if (!force_apply && (ctl->done || !ctl->mass_scale_now)) return;
@@ -622,20 +673,63 @@ __global__ void k_mass_scaling(ElementArrays el, NodeArrays nd, Control* ctls, i
     nd.inv_mass[n] = m > 0.0 ? 1.0 / m : 0.0;
 }
 
+__global__ void k_mass_scaling(ElementArrays el, NodeArrays nd, Control* ctls, int force_apply) {
+    FOR_ACTIVE(nd.act_node, nd.n, 1, g) {
+        int lane;
+        mass_scaling_body(el, nd, ctls, force_apply, active_entity(nd.act_node, g, 1, &lane));
+    }
+}
+
 __global__ void k_nonfinite(NodeArrays nd, Control* ctls) {
-    long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= 3 * nd.n) return;
-    Control* ctl = ctls + nd.node_slot[k / 3];
-    if (ctl->done) return;
-    if (!isfinite(nd.u[k])) ctl->nonfinite = 1;
+    FOR_ACTIVE(nd.act_node, nd.n, 1, g) {
+        int lane;
+        const long long n = active_entity(nd.act_node, g, 1, &lane);
+        if (n >= nd.n) continue;
+        Control* ctl = ctls + nd.node_slot[n];
+        if (ctl->done) continue;
+        if (!isfinite(nd.u[3 * n]) || !isfinite(nd.u[3 * n + 1]) || !isfinite(nd.u[3 * n + 2])) ctl->nonfinite = 1;
+    }
+}
+
+// The active chunk lists: thread per chunk (all entity spaces), a chunk is
+// active while any crash slot it holds is still running. One atomic per warp
+// and space.
+__global__ void k_build_active(ActiveBuild b, const Control* __restrict__ ctls) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    int space = -1;
+    bool alive = false;
+    if (t < b.n_chunks) {
+        space = 0;
+        while (space + 1 < ACTIVE_SPACES && t >= b.space_off[space + 1]) ++space;
+        for (int k = b.chunk_lo[t]; k <= b.chunk_hi[t] && !alive; ++k) alive = !ctls[k].done;
+    }
+    const unsigned want = __ballot_sync(0xffffffffu, alive);
+    const unsigned same = __match_any_sync(0xffffffffu, space);
+    const unsigned grp = want & same;
+    if (alive) {
+        const int leader = __ffs(grp) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(&b.counts[space], __popc(grp));
+        base = __shfl_sync(grp, base, leader);
+        b.lists[b.space_off[space] + base + __popc(grp & ((1u << lane) - 1u))] = (int)(t - b.space_off[space]);
+    }
 }
 
 // End of a step (src/solver.rs:344-345 plus the stop rules), one thread per slot.
-__global__ void k_step_end(Control* ctls, ContactArrays ca, VehicleArrays va, int check_separation) {
+__device__ void step_end_slot(Control* ctl, int sl, const ContactArrays& ca, const VehicleArrays& va, int check_separation);
+
+// One thread per slot; also mirrors each slot's done flag into done_out (a
+// compact array the host polls).
+__global__ void k_step_end(Control* ctls, ContactArrays ca, VehicleArrays va, int check_separation, int* __restrict__ done_out) {
     const int sl = blockIdx.x * blockDim.x + threadIdx.x;
     if (sl >= ca.n_slots) return;
     Control* ctl = ctls + sl;
-    if (ctl->done) return;
+    if (!ctl->done) step_end_slot(ctl, sl, ca, va, check_separation);
+    done_out[sl] = ctl->done;
+}
+
+__device__ void step_end_slot(Control* ctl, int sl, const ContactArrays& ca, const VehicleArrays& va, int check_separation) {
     const double dt = step_dt(ctl);
     ctl->step += 1;
     ctl->t = ctl->t + dt;
@@ -765,9 +859,8 @@ __device__ __forceinline__ int face_cells(const ContactArrays& ca, const FaceGeo
 // the buckets, which returns every count to zero. Pass 2: geometry only. The
 // faces are
 // face_list[0, n) when face_list is given, else face_off[c0] + [0, n).
-__global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, const uint32_t* __restrict__ face_list,
-                                long long n, int run_mode, int pass) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void contact_face_body(const ContactArrays& ca, const NodeArrays& nd, const Control* ctls, int c0,
+                                                  const uint32_t* __restrict__ face_list, long long n, int run_mode, int pass, long long t) {
     if (t >= n) return;
     const long long f = face_list ? (long long)face_list[t] : ca.face_off[c0] + t;
     const int c = ca.face_contact[f];
@@ -809,6 +902,14 @@ __global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctls, 
                     ca.entries[ca.boff[b] + pos] = local;
                 }
             }
+}
+
+__global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, const uint32_t* __restrict__ face_list,
+                                long long n, int run_mode, int pass, Active act) {
+    FOR_ACTIVE(act, n, 1, g) {
+        int lane;
+        contact_face_body(ca, nd, ctls, c0, face_list, n, run_mode, pass, active_entity(act, g, 1, &lane));
+    }
 }
 
 // Thread per dynamic bucket: its range in the contact's entries, allocated
@@ -884,12 +985,11 @@ __device__ __forceinline__ bool face_hit(const FaceGeo& g, const double* p, doub
 // index that hits: the face the reference's in-order scan with `break` finds
 // (src/contact.rs:115-157).
 template <int LANES>
-__global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, int c1, int run_mode, double dt_override,
-                                 const double* __restrict__ masses) {
-    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x % LANES;
+__device__ __forceinline__ void contact_slave_body(const ContactArrays& ca, const NodeArrays& nd, const Control* ctls, int c0, int c1,
+                                                   int run_mode, double dt_override, const double* __restrict__ masses, long long e,
+                                                   int lane) {
     const long long s_begin = ca.slave_off[c0], s_end = ca.slave_off[c1];
-    const long long s = s_begin + gid / LANES;
+    const long long s = s_begin + e;
     bool live = s < s_end;
     const Control* ctl = nullptr;
     if (live) {
@@ -980,6 +1080,17 @@ __global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctls,
     atomicMax(&ca.pen_max_bits[c], (unsigned long long)__double_as_longlong(-best_sd));
 }
 
+template <int LANES>
+__global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, int c1, int run_mode, double dt_override,
+                                 const double* __restrict__ masses, long long n_slaves) {
+    const Active act = run_mode ? ca.act_slave : Active{nullptr, nullptr};
+    FOR_ACTIVE(act, n_slaves, LANES, g) {
+        int lane;
+        const long long e = active_entity(act, g, LANES, &lane);
+        contact_slave_body<LANES>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses, e, lane);
+    }
+}
+
 constexpr int MAX_NODE_EVENTS = 48;
 constexpr int GATHER_TPB = 128;
 constexpr int WALK_BLOCKS = 296;  // 2 x 148 SMs of 4 warps
@@ -1020,9 +1131,8 @@ __device__ __forceinline__ bool role_sum(const ContactArrays& ca, uint32_t r, in
 // order. A node whose per-face hit lists overflowed is handed to
 // k_contact_gather_walk instead (its output is written there). Then the grid
 // bookkeeping is cleared for the next build.
-__global__ void __launch_bounds__(GATHER_TPB) k_contact_gather(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, int c1,
-                                                               int run_mode, double* __restrict__ f_out, int skip_fixed) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void gather_body(const ContactArrays& ca, const NodeArrays& nd, const Control* ctls, int c0, int c1,
+                                            int run_mode, double* __restrict__ f_out, int skip_fixed, long long i) {
     if (i < ca.n_cnodes) {
         const long long n = ca.cnode[i];
         if (!(skip_fixed && nd.fixed[n]) && !(run_mode && ctls[nd.node_slot[n]].done)) {
@@ -1043,8 +1153,19 @@ __global__ void __launch_bounds__(GATHER_TPB) k_contact_gather(ContactArrays ca,
             }
         }
     }
+}
+
+__global__ void __launch_bounds__(GATHER_TPB) k_contact_gather(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, int c1,
+                                                               int run_mode, double* __restrict__ f_out, int skip_fixed) {
+    const Active act = run_mode ? ca.act_cnode : Active{nullptr, nullptr};
+    FOR_ACTIVE(act, ca.n_cnodes, 1, g) {
+        int lane;
+        gather_body(ca, nd, ctls, c0, c1, run_mode, f_out, skip_fixed, active_entity(act, g, 1, &lane));
+    }
+    // Clear the grid bookkeeping for the next build.
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long nthreads = (long long)gridDim.x * blockDim.x;
-    for (long long c = c0 + i; c < c1; c += nthreads) {
+    for (long long c = c0 + t; c < c1; c += nthreads) {
         ca.n_overflow[c] = 0;
         ca.entry_overrun[c] = 0;
         ca.levels_used[c] = 0;
@@ -1220,32 +1341,38 @@ void launch_init_state(cudaStream_t s, long long n_hc, long long stride, float4*
 }
 void launch_forces(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, int respect_done) {
     if (el.n_hc <= 0) return;
-    k_forces<<<(unsigned)blocks_for(el.n_hc, FORCES_TPB), FORCES_TPB, 0, s>>>(el, nd, ctls, respect_done);
+    k_forces<<<active_grid(el.n_hc, 1, FORCES_TPB, 148 * FORCES_MINB * 4), FORCES_TPB, 0, s>>>(el, nd, ctls, respect_done);
 }
 void launch_gather(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, double* f_out) {
     k_gather<<<(unsigned)blocks_for(nd.n, TPB), TPB, 0, s>>>(el, nd, f_out);
 }
 void launch_half(cudaStream_t s, const NodeArrays& nd, Control* ctls) {
-    k_half<<<(unsigned)blocks_for(nd.n, TPB), TPB, 0, s>>>(nd, ctls);
+    k_half<<<active_grid(nd.n, 1, TPB, GRID_CAP), TPB, 0, s>>>(nd, ctls);
 }
 void launch_full(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls) {
-    k_full<<<(unsigned)blocks_for(nd.n, TPB), TPB, 0, s>>>(el, nd, ctls);
+    k_full<<<active_grid(nd.n, 1, TPB, GRID_CAP), TPB, 0, s>>>(el, nd, ctls);
 }
 void launch_elem_dt(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, const double* u, int respect_done) {
     if (el.n_all <= 0) return;
-    k_elem_dt<<<(unsigned)blocks_for(el.n_all, DT_TPB), DT_TPB, 0, s>>>(el, nd, ctls, u, respect_done);
+    k_elem_dt<<<active_grid(el.n_all, 1, DT_TPB, GRID_CAP), DT_TPB, 0, s>>>(el, nd, ctls, u, respect_done);
 }
 void launch_dt_finalize(cudaStream_t s, Control* ctls, int n_slots) {
     k_dt_finalize<<<(unsigned)blocks_for(n_slots, 128), 128, 0, s>>>(ctls, n_slots);
 }
 void launch_mass_scaling(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, int force_apply) {
-    k_mass_scaling<<<(unsigned)blocks_for(nd.n, TPB), TPB, 0, s>>>(el, nd, ctls, force_apply);
+    k_mass_scaling<<<active_grid(nd.n, 1, TPB, GRID_CAP), TPB, 0, s>>>(el, nd, ctls, force_apply);
 }
 void launch_nonfinite(cudaStream_t s, const NodeArrays& nd, Control* ctls) {
-    k_nonfinite<<<(unsigned)blocks_for(3 * nd.n, TPB), TPB, 0, s>>>(nd, ctls);
+    k_nonfinite<<<active_grid(nd.n, 1, TPB, GRID_CAP), TPB, 0, s>>>(nd, ctls);
 }
-void launch_step_end(cudaStream_t s, Control* ctls, const ContactArrays& ca, const VehicleArrays& va, int check_separation) {
-    k_step_end<<<(unsigned)blocks_for(ca.n_slots, 128), 128, 0, s>>>(ctls, ca, va, check_separation);
+void launch_build_active(cudaStream_t s, const ActiveBuild& b, const Control* ctls) {
+    if (b.n_chunks <= 0) return;
+    cudaMemsetAsync(b.counts, 0, sizeof(int) * ACTIVE_SPACES, s);
+    k_build_active<<<(unsigned)blocks_for(b.n_chunks, TPB), TPB, 0, s>>>(b, ctls);
+}
+void launch_step_end(cudaStream_t s, Control* ctls, const ContactArrays& ca, const VehicleArrays& va, int check_separation,
+                     int* done_out) {
+    k_step_end<<<(unsigned)blocks_for(ca.n_slots, 128), 128, 0, s>>>(ctls, ca, va, check_separation, done_out);
 }
 void launch_vehicle_sums(cudaStream_t s, const VehicleArrays& va, const double* mass, const double* v, const double* v0, double* out) {
     if (va.n_vehicles <= 0) return;
@@ -1269,26 +1396,30 @@ void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& n
     // run: only moving faces (static ones keep their geometry); drop-in: every face of the range
     const uint32_t* list = run_mode ? ca.dyn_faces : nullptr;
     const long long n_list = run_mode ? ca.n_dyn_faces : n_faces;
-    if (n_list > 0) k_contact_faces<<<(unsigned)blocks_for(n_list, TPB), TPB, 0, s>>>(ca, nd, ctls, c0, list, n_list, run_mode, 0);
+    if (n_list > 0)
+        k_contact_faces<<<active_grid(n_list, 1, TPB, GRID_CAP), TPB, 0, s>>>(ca, nd, ctls, c0, list, n_list, run_mode, 0,
+                                                                            run_mode ? ca.act_dynf : Active{nullptr, nullptr});
     if (bk1 > bk0 && !ca.exhaustive) {
         k_grid_alloc<<<(unsigned)blocks_for(bk1 - bk0, TPB), TPB, 0, s>>>(ca, c0, c1);
         const uint32_t* glist = run_mode ? ca.grid_faces : nullptr;
         const long long n_glist = run_mode ? ca.n_grid_faces : n_faces;
         if (n_glist > 0)
-            k_contact_faces<<<(unsigned)blocks_for(n_glist, TPB), TPB, 0, s>>>(ca, nd, ctls, c0, glist, n_glist, run_mode, 1);
+            k_contact_faces<<<active_grid(n_glist, 1, TPB, GRID_CAP), TPB, 0, s>>>(ca, nd, ctls, c0, glist, n_glist, run_mode, 1,
+                                                                                 Active{nullptr, nullptr});
     }
     if (n_slaves > 0) {
-        const unsigned g = (unsigned)blocks_for(n_slaves * lanes, TPB);
+        const unsigned g = active_grid(n_slaves, lanes, TPB, GRID_CAP);
         switch (lanes) {
-            case 4: k_contact_slaves<4><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses); break;
-            case 8: k_contact_slaves<8><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses); break;
-            case 16: k_contact_slaves<16><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses); break;
-            default: k_contact_slaves<32><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses); break;
+            case 4: k_contact_slaves<4><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses, n_slaves); break;
+            case 8: k_contact_slaves<8><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses, n_slaves); break;
+            case 16: k_contact_slaves<16><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses, n_slaves); break;
+            default: k_contact_slaves<32><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses, n_slaves); break;
         }
     }
     cudaMemsetAsync(ca.gather_count, 0, sizeof(int), s);
     long long nodes = ca.n_cnodes > 0 ? ca.n_cnodes : 1;
-    k_contact_gather<<<(unsigned)blocks_for(nodes, GATHER_TPB), GATHER_TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, f_out, skip_fixed);
+    k_contact_gather<<<active_grid(nodes, 1, GATHER_TPB, GRID_CAP * 2), GATHER_TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, f_out,
+                                                                                          skip_fixed);
     const long long walk_blocks = blocks_for(nodes * 32, GATHER_TPB);
     k_contact_gather_walk<<<(unsigned)(walk_blocks < WALK_BLOCKS ? walk_blocks : WALK_BLOCKS), GATHER_TPB, 0, s>>>(ca, c0, c1, f_out);
 }
@@ -1305,7 +1436,8 @@ void launch_contact_geometry(cudaStream_t s, const ContactArrays& ca, const Node
                              long long n_faces) {
     (void)f0;
     if (c1 <= c0 || n_faces <= 0) return;
-    k_contact_faces<<<(unsigned)blocks_for(n_faces, TPB), TPB, 0, s>>>(ca, nd, nullptr, c0, nullptr, n_faces, 0, 2);
+    k_contact_faces<<<active_grid(n_faces, 1, TPB, GRID_CAP), TPB, 0, s>>>(ca, nd, nullptr, c0, nullptr, n_faces, 0, 2,
+                                                                         Active{nullptr, nullptr});
 }
 
 }  // namespace crush

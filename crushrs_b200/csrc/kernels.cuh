@@ -5,6 +5,15 @@
 
 namespace crush {
 
+// Work lists of active 256-entity chunks: a kernel given a list visits only
+// the chunks on it (the chunks that hold an entity of a crash slot still
+// running, rebuilt every 20 steps); a null list means every chunk.
+constexpr int CHUNK = 256;
+struct Active {
+    const int* list;   // chunk indices
+    const int* count;  // their number (device)
+};
+
 // Element-side device arrays of one model (honeycomb elements only in the
 // planes; all model elements in the f64 arrays used by dt / mass scaling).
 struct ElementArrays {
@@ -22,6 +31,7 @@ struct ElementArrays {
     double* elem_dt;         // per model element (written by the dt kernel)
     double* elem_extra;      // per model element added mass (mass scaling)
     const uint32_t* elem_slot;  // crash slot per model element
+    Active act_hc, act_all;     // active chunks of honeycomb / all elements
 };
 
 struct NodeArrays {
@@ -41,6 +51,7 @@ struct NodeArrays {
     const uint32_t* all_off; // N+1 CSR over all model (element, corner) slots
     const uint32_t* all_slot;
     const uint32_t* node_slot;  // crash slot per node
+    Active act_node;            // active chunks of nodes
 };
 
 // Contact runtime arrays (all contacts concatenated).
@@ -125,7 +136,20 @@ struct ContactArrays {
     int exhaustive;             // 1: every search tests every face of its contact (no broad phase)
     int* gather_work;           // contact nodes whose hit lists overflowed this pass (n_cnodes capacity)
     int* gather_count;          // their number
+    Active act_slave, act_cnode, act_dynf;  // active chunks of primary-node entries, contact nodes, moving faces
 };
+
+// Chunks of every entity space with the crash-slot range each covers, and
+// the active lists built from them.
+struct ActiveBuild {
+    long long n_chunks;          // all spaces together
+    const int* chunk_lo;         // first and last slot of each chunk
+    const int* chunk_hi;
+    const long long* space_off;  // ACTIVE_SPACES + 1 chunk offsets
+    int* lists;                  // same layout as the chunks
+    int* counts;                 // ACTIVE_SPACES
+};
+constexpr int ACTIVE_SPACES = 6;  // honeycomb elements, all elements, nodes, primary-node entries, contact nodes, moving faces
 
 // Vehicles of all crash slots: node lists and the reduction layout.
 struct VehicleArrays {
@@ -154,7 +178,9 @@ void launch_elem_dt(cudaStream_t s, const ElementArrays& el, const NodeArrays& n
 void launch_dt_finalize(cudaStream_t s, Control* ctls, int n_slots);
 void launch_mass_scaling(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, int force_apply);
 void launch_nonfinite(cudaStream_t s, const NodeArrays& nd, Control* ctls);
-void launch_step_end(cudaStream_t s, Control* ctls, const ContactArrays& ca, const VehicleArrays& va, int check_separation);
+void launch_build_active(cudaStream_t s, const ActiveBuild& b, const Control* ctls);
+void launch_step_end(cudaStream_t s, Control* ctls, const ContactArrays& ca, const VehicleArrays& va, int check_separation,
+                     int* done_out);
 // Contact pass over contacts [c0, c1) (faces [f0, f0 + n_faces), n_slaves
 // primary-node entries, dynamic grid buckets [bk0, bk1)); `lanes` lanes per
 // primary-node search (4, 8, 16 or 32). dt_override > 0 is a drop-in call: every face's

@@ -279,3 +279,37 @@ def batch_headon(i, seed=BATCH_SEED):
     a = vehicle(ma, sa, _block_material(E, ma / np.prod(sa), sya))
     b = vehicle(mb, sb, _block_material(E, mb / np.prod(sb), syb))
     return scenario(a, b, va, vb, offset=off, clearance=0.15, element_size=h, end_time=0.12)
+
+
+SERVE_SEED = 0xD1B54A32D192ED03
+SERVE_KINDS = ("head-on", "t-bone", "rear-end")
+
+
+def serve_query(i, seed=SERVE_SEED, e_range=(300, 20000)):
+    """Delta-v query i of the serving workload: a head-on, T-bone or rear-end
+    (one third each), 300-20000 hexahedra (log-uniform), element size from
+    {0.1, 0.15, 0.2, 0.25, 0.3} m, speeds 5-30 m/s, masses 1000-3000 kg,
+    bilinear sigma_y 0.2-0.6 MPa. Deterministic in (seed, i). Returns
+    (kind, scenario)."""
+    rng = XorShift64Star(seed ^ ((i + 1) * 0xBF58476D1CE4E5B9 & 0xFFFFFFFFFFFFFFFF))
+    for _ in range(4):
+        rng.next_u64()
+    kind = SERVE_KINDS[int(rng.uniform(0, 3)) % 3]
+    h, sa, sb = _seeded_pair(rng, e_range[0], e_range[1], h_choices=(0.1, 0.15, 0.2, 0.25, 0.3))
+    ma, mb = rng.uniform(1000, 3000), rng.uniform(1000, 3000)
+    sya, syb = rng.uniform(0.2e6, 0.6e6), rng.uniform(0.2e6, 0.6e6)
+    E = 5e6
+    a = vehicle(ma, sa, _block_material(E, ma / np.prod(sa), sya))
+    b = vehicle(mb, sb, _block_material(E, mb / np.prod(sb), syb))
+    if kind == "head-on":
+        va, vb = rng.uniform(5, 30), rng.uniform(5, 30)
+        return kind, scenario(a, b, va, vb, offset=rng.uniform(0.0, 0.9), clearance=0.15, element_size=h, end_time=0.12)
+    if kind == "t-bone":
+        # B turned 90 degrees: its length along y, its side facing A's front
+        va = rng.uniform(5, 30)
+        bt = vehicle(mb, (sb[1], sb[0], sb[2]), _block_material(E, mb / np.prod(sb), syb))
+        return kind, scenario(a, bt, va, 0.0, offset=rng.uniform(0.0, 0.3) * sb[0], clearance=0.15, element_size=h,
+                              layout=abi.LAYOUT_TBONE, end_time=0.12)
+    va = rng.uniform(10, 30)  # rear-end: B moves the same way, slower
+    vb = va * rng.uniform(0.1, 0.6)
+    return kind, scenario(a, b, va, -vb, offset=rng.uniform(0.0, 0.5), clearance=0.15, element_size=h, end_time=0.12)

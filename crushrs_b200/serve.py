@@ -1,0 +1,104 @@
+"""Python face of the continuous-batching crash server (include/crush_server.h).
+
+    with Server(max_waves=4) as srv:
+        t = srv.submit(model.desc)          # copies the model, returns a ticket
+        for r in srv.poll(wait_ms=100):     # finished crashes, as they finish
+            print(r.ticket, r.results.vehicle[0].delta_v[0], r.finish_s - r.submit_s)
+
+Also an open-loop Poisson load driver for latency and throughput figures.
+"""
+import ctypes as C
+import math
+import time
+
+from . import abi
+from .native import check, lib
+
+
+class Server:
+    """crush_server: waves of batched contexts on one GPU."""
+
+    def __init__(self, device=0, max_waves=4, max_wave_slots=2048, chunk_steps=100, max_wave_elements=8_000_000,
+                 hbm_budget_bytes=0.0, gather_ms=2.0):
+        self._lib = lib()
+        cfg = abi.ServerConfig(device, max_waves, max_wave_slots, chunk_steps, max_wave_elements, hbm_budget_bytes, gather_ms)
+        h = C.c_void_p()
+        check(self._lib.crush_server_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+
+    def submit(self, desc):
+        t = C.c_uint64()
+        check(self._lib.crush_server_submit(self.h, C.byref(desc), C.byref(t)))
+        return t.value
+
+    def poll(self, max_results=256, wait_ms=0):
+        out = (abi.ServerResult * max_results)()
+        n = C.c_int()
+        check(self._lib.crush_server_poll(self.h, out, max_results, C.byref(n), wait_ms))
+        return [out[k] for k in range(n.value)]
+
+    def stats(self):
+        s = abi.ServerStats()
+        check(self._lib.crush_server_stats_get(self.h, C.byref(s)))
+        return s
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._lib.crush_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def footprint(desc):
+    """The server's admission estimate of a model's device bytes."""
+    return lib().crush_model_footprint(C.byref(desc))
+
+
+def open_loop(server, models, rate, seed=1):
+    """Submit `models` (objects with .desc) at Poisson arrival times of the
+    given rate (req/s), open loop; returns (results by ticket, wall seconds,
+    ticket -> model index)."""
+    rng = _Rng(seed)
+    t0 = time.perf_counter()
+    t_next = 0.0
+    tickets = {}
+    results = {}
+    i = 0
+    while i < len(models) or len(results) < len(models):
+        now = time.perf_counter() - t0
+        while i < len(models) and t_next <= now:
+            tickets[server.submit(models[i].desc)] = i
+            i += 1
+            t_next += -math.log(1.0 - rng.uniform()) / rate
+        wait = 0 if i < len(models) else 20
+        for r in server.poll(wait_ms=wait):
+            results[r.ticket] = r
+        if i < len(models):
+            sleep = t_next - (time.perf_counter() - t0)
+            if sleep > 0:
+                time.sleep(min(sleep, 0.002))
+    return results, time.perf_counter() - t0, tickets
+
+
+class _Rng:
+    def __init__(self, seed):
+        self.s = seed & 0xFFFFFFFFFFFFFFFF or 1
+
+    def uniform(self):
+        x = self.s
+        x ^= x >> 12
+        x ^= (x << 25) & 0xFFFFFFFFFFFFFFFF
+        x ^= x >> 27
+        self.s = x
+        return (((x * 0x2545F4914F6CDD1D) & 0xFFFFFFFFFFFFFFFF) >> 11) / float(1 << 53)

@@ -295,6 +295,12 @@ int crush_batch_run(crush_ctx* ctx, crush_results* results);
 /* Results of one slot of the open run (crush_run_begin / crush_run_steps
  * drive all slots; *done = 1 once every slot has stopped). */
 int crush_batch_results(crush_ctx* ctx, int slot, crush_results* results);
+/* Results of slots [first, first + count) in one pass (one device read). */
+int crush_batch_results_range(crush_ctx* ctx, int first, int count, crush_results* results);
+/* Which slots of the open run have stopped: done_flags[n] (may be NULL) and
+ * *all = 1 when every slot has (may be NULL). Reads a compact flag array the
+ * step kernels keep; synchronises the context's stream. */
+int crush_batch_done(crush_ctx* ctx, int* done_flags, int* all);
 
 /* ---- allocation-free contact call ----
  *

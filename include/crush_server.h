@@ -1,0 +1,67 @@
+/*
+ * crush_server.h — continuous-batching crash server on one GPU.
+ *
+ * No counterpart in the reference, which runs one crash per process
+ * (src/bin/crushrs.rs:30). Requests (whole crash models) are submitted from
+ * any thread and answered asynchronously. A scheduler thread groups waiting
+ * requests into waves and starts each wave as a batched context
+ * (crush_batch_create) on its own CUDA stream and host thread as soon as the
+ * wave fits the HBM budget and a wave slot is free, so waves that start while
+ * others run overlap on the device. Every crash is reported the moment its
+ * own stop rule ends it (the wave's other crashes run on), and its results
+ * are bit-identical to crush_create + crush_run of the same model alone.
+ */
+#ifndef CRUSH_SERVER_H
+#define CRUSH_SERVER_H
+
+#include <stdint.h>
+
+#include "crush.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct crush_server crush_server;
+
+typedef struct crush_server_config {
+    int32_t device;
+    int32_t max_waves;          /* waves running at once (default 4) */
+    int32_t max_wave_slots;     /* crashes per wave (default 2048) */
+    int32_t chunk_steps;        /* steps between completion checks of a wave (default 100) */
+    int64_t max_wave_elements;  /* elements per wave (default 8,000,000) */
+    double hbm_budget_bytes;    /* device memory the waves may hold together (0 = 80% of free memory) */
+    double gather_ms;           /* while a wave runs, wait this long for more arrivals before starting the next (default 2) */
+} crush_server_config;
+
+typedef struct crush_server_result {
+    uint64_t ticket;
+    int32_t status;             /* CRUSH_OK, CRUSH_ERR_NONFINITE, or the error that stopped the wave */
+    int32_t wave;               /* index of the wave that ran it */
+    double submit_s;            /* server clock (s since creation) at submit */
+    double start_s;             /* wave start (its context creation began) */
+    double finish_s;            /* result available */
+    crush_results results;
+} crush_server_result;
+
+typedef struct crush_server_stats {
+    int64_t submitted, completed, waves, queued, running;
+    double bytes_in_use, peak_bytes_in_use, budget_bytes;
+} crush_server_stats;
+
+/* config may be NULL (defaults). */
+int crush_server_create(const crush_server_config* config, crush_server** out);
+/* Copies the model (the caller may free it on return) and queues it. */
+int crush_server_submit(crush_server* srv, const crush_model_desc* desc, uint64_t* ticket);
+/* Up to max finished results into out, waiting up to wait_ms for the first. */
+int crush_server_poll(crush_server* srv, crush_server_result* out, int max, int* n, int wait_ms);
+int crush_server_stats_get(crush_server* srv, crush_server_stats* out);
+/* Estimated device bytes of a model inside a wave (the admission measure). */
+double crush_model_footprint(const crush_model_desc* desc);
+/* Finishes every submitted request, then stops the server's threads. */
+void crush_server_destroy(crush_server* srv);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
