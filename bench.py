@@ -1,27 +1,37 @@
 #!/usr/bin/env python
-"""Headline benchmark: explicit time steps of the refined head-on crash
-(278,640 one-point honeycomb hexahedra, 299,108 nodes) on the B200 engine.
+"""Headline benchmark of the B200 crash engine.
 
-One step = the whole explicit time step of the model: stable-dt check and
-mass scaling (every 5 steps), node-to-face contact over the device grid, the
-half step, the element forces, the ordered force gather with the full step.
+Main line (the workload the metric is quoted on when it fits one GPU): the
+refined head-on, 278,640 one-point honeycomb hexahedra, 299,666 nodes, run to
+separation (<= 5000 steps). One step = the whole explicit time step: stable-dt
+check and mass scaling (every 5 steps), node-to-face contact, the half step,
+the element forces, the ordered force gather with the full step.
 
-Printed JSON line (rank 0):
-  value      element-updates/s of the whole job, device-timed (CUDA events on
-             the engine's stream), inputs resident in HBM; per-step working
-             set (~0.33 GB) is larger than L2, so no flush is needed.
-  e2e        the same metric through the reference-facing C-ABI drop-in calls
-             with host buffers (crush_contact_apply + crush_compute_forces
-             per step, the central-difference update on the host): every
-             step copies u host->device and the forces device->host.
-  e2e_run    elem-upd/s of a whole crash through crush_create + crush_run
-             (host model in, delta-v out), host-clock timed.
+  value      element-updates/s of the whole job over exactly K steps after W
+             warm-up steps, device-timed (CUDA events on the engine's stream),
+             inputs resident in HBM; the per-step working set (~0.33 GB) is
+             larger than L2, so no flush is needed.
+  e2e        the same metric end to end through the reference-facing C ABI
+             with host buffers: crush_create from the host model (the upload
+             inside the timed region) + crush_run to separation + the FP64
+             delta-v results read back, host-clock timed.
+  e2e_dropin the drop-in loop a reference caller would write (src/solver.rs:
+             287-342 on the host, crush_contact_apply + crush_compute_forces
+             per step, u in and forces out through host buffers).
   roofline   HBM roofline of the element-force kernel: algorithmic bytes per
              launch (870 B per element + 24 B per node) over its average
              device time inside the timed region.
   cpu_baseline  the oracle's f32 8-lane restatement of the reference step on
              all host threads, a bounded number of steps of the same mesh.
---impl reference runs that CPU restatement as the reference arm.
+  batched    4096 seeded uneven head-on crashes (300-6000 elements) in one
+             batched context, crashes/s (host clock, set-up included) against
+             the plain one-crash-per-launch path (crush_create + crush_run per
+             crash) on a sample, and the FP64 delta-v error of a sample against
+             the reference's f64 scalar restatement.
+  serving    the crash server under an open-loop Poisson stream of seeded
+             head-on / T-bone / rear-end queries (300-20000 elements):
+             crashes/s and p50/p99 submit-to-result latency.
+--impl reference runs the CPU restatement of the reference as the reference arm.
 """
 import argparse
 import json
@@ -85,7 +95,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                                          "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except Exception:
@@ -125,7 +135,11 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup():
+def dist_setup(backend=None):
+    """One process per GPU (torchrun's env): the process group for the
+    barrier and the max-over-ranks timing. The single-mesh workload does not
+    shard, so ranks run replicas and exchange nothing else. backend: "nccl"
+    (default) or "gloo" (the CPU tests of this path)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -135,19 +149,25 @@ def dist_setup():
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
+        backend = backend or "nccl"
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
     return world, rank, local
 
 
 def all_max(x, world):
+    """Max of x over the ranks (the job's time is its slowest rank's)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -212,14 +232,106 @@ def e2e_dropin(ctx, desc, steps, n_hc):
     return n_hc * steps / wall, h2d, d2h
 
 
+def e2e_run(desc, device, n_hc, n_nodes):
+    """crush_create from the host model + crush_run + results: host-clock elem-upd/s."""
+    from crushrs_b200.engine import Context
+
+    t0 = time.perf_counter()
+    ctx = Context(desc, device=device)
+    r = ctx.run()
+    wall = time.perf_counter() - t0
+    ctx.close()
+    steps = max(int(r.steps), 1)
+    h2d = 8 * 6 * n_nodes + 36 * desc.n_hexes  # positions, velocities, hexes, parts, incidence
+    return {"value": n_hc * r.steps / wall, "unit": "elem-upd/s", "steps": int(r.steps), "wall_s": wall,
+            "h2d_bytes_per_step": int(h2d / steps), "d2h_bytes_per_step": int((8 * 7 * 2 + 4 * 4096) / steps),
+            "path": "crush_create (host model) + crush_run to separation + FP64 delta-v read back",
+            "delta_v": [r.vehicle[k].delta_v[0] for k in range(r.n_vehicles)]}
+
+
+def batched_section(n, plain_sample, oracle_sample, device):
+    """4096 seeded uneven head-on crashes in one batched context vs the plain
+    one-crash-per-launch path."""
+    from crushrs_b200 import scenarios as S
+    from crushrs_b200.engine import Context
+
+    models = [S.Model.build(S.batch_headon(i)) for i in range(n)]
+    elems = sum(m.n_hexes for m in models)
+    w = Context(models[0].desc, device=device)  # CUDA and module warm-up
+    w.run()
+    w.close()
+    t0 = time.perf_counter()
+    ctx = Context([m.desc for m in models], device=device)
+    t1 = time.perf_counter()
+    rs = ctx.batch_run()
+    t2 = time.perf_counter()
+    lanes, _ = ctx.tuning()
+    launches = ctx.launches()
+    ctx.close()
+    steps = [int(r.steps) for r in rs]
+    eu = sum(m.n_hexes * st for m, st in zip(models, steps))
+    # plain path: one context and one run per crash, a sample, after its own warm-up
+    times = []
+    same = True
+    for i in range(plain_sample):
+        t = time.perf_counter()
+        c = Context(models[i].desc, device=device)
+        r = c.run()
+        c.close()
+        times.append(time.perf_counter() - t)
+        same &= r.steps == rs[i].steps and list(r.vehicle[0].delta_v) == list(rs[i].vehicle[0].delta_v)
+    plain_s = statistics.median(times)
+    batched_cps = n / (t2 - t0)
+    out = {"crashes": n, "elements": elems, "create_s": t1 - t0, "run_s": t2 - t1, "crashes_per_s": batched_cps,
+           "elem_upd_per_s": eu / (t2 - t0), "steps_mean": statistics.mean(steps), "steps_max": max(steps),
+           "gpu_launches": int(launches), "slave_lanes": lanes,
+           "plain": {"crashes_per_s": 1.0 / plain_s, "median_s_per_crash": plain_s, "sample": plain_sample,
+                     "path": "crush_create + crush_run per crash (CUDA graphs of 20 steps)"},
+           "speedup_vs_plain": batched_cps * plain_s, "batched_equals_plain": bool(same)}
+    if oracle_sample:
+        from tests import oracle_lib as O
+
+        errs = []
+        for i in range(oracle_sample):
+            ro, _, _, _, _ = O.run(models[i].desc, simd=False, threads=os.cpu_count() or 1)
+            for k in range(rs[i].n_vehicles):
+                ref = ro.vehicle[k].delta_v[0]
+                errs.append(abs(rs[i].vehicle[k].delta_v[0] - ref) / max(abs(ref), 1e-9))
+        out["delta_v_max_rel_err_vs_f64_oracle"] = max(errs)
+        out["delta_v_oracle_sample"] = oracle_sample
+    return out
+
+
+def serving_section(rate, seconds, device):
+    """The crash server under an open-loop Poisson stream at `rate` req/s."""
+    from crushrs_b200 import scenarios as S
+    from crushrs_b200.serve import Server, open_loop
+
+    n = max(1, int(rate * seconds))
+    models = [S.Model.build(S.serve_query(i)[1]) for i in range(n)]
+    with Server(device=device, max_waves=4) as srv:
+        res, wall, _ = open_loop(srv, models, rate=rate)
+        st = srv.stats()
+    lat = sorted(r.finish_s - r.submit_s for r in res.values())
+    pick = lambda q: lat[min(len(lat) - 1, int(q * len(lat)))]
+    return {"rate_req_per_s": rate, "seconds": seconds, "crashes": len(res), "crashes_per_s": len(res) / wall,
+            "p50_ms": 1e3 * pick(0.5), "p99_ms": 1e3 * pick(0.99), "waves": int(st.waves), "peak_gb": st.peak_bytes_in_use / 1e9,
+            "elements_mean": sum(m.n_hexes for m in models) / n, "ok": all(r.status == 0 for r in res.values())}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--batch", type=int, default=4096, help="crashes of the batched section (0: skip)")
+    ap.add_argument("--plain-sample", type=int, default=64)
+    ap.add_argument("--oracle-sample", type=int, default=4)
+    ap.add_argument("--serve-rates", default="100,200", help="req/s of the serving section ('' : skip)")
+    ap.add_argument("--serve-seconds", type=float, default=30.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -232,8 +344,9 @@ def main():
     model = S.Model.build(S.refined_headon())
     desc = model.desc
     n_nodes = desc.n_nodes
-    config = {"workload": "refined head-on, 0.05 m hexahedra (36x30x138 + 36x24x150)", "elements": None, "nodes": n_nodes,
-              "steps_per_run": "to separation, <= 5000", "l2": "per-step working set > L2 (126 MB), no flush",
+    config = {"workload": "refined head-on, 0.05 m hexahedra (36x30x138 + 36x24x150), run to separation (<= 5000 steps)",
+              "elements": None, "nodes": n_nodes, "timed_steps": f"steps {args.warmup}..{args.warmup + args.steps}",
+              "l2": "per-step working set > L2 (126 MB), no flush",
               "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
 
     if args.impl == "reference":
@@ -242,7 +355,7 @@ def main():
         threads = os.cpu_count() or 1
         n_hc = sum(1 for p in model.hex_part() if model.material(p).model == 0)
         config["elements"] = n_hc
-        steps, loop, sec = cpu_reference(desc, args.steps, threads)
+        steps, loop, sec = cpu_reference(desc, args.cpu_steps, threads)
         value = n_hc * steps / loop
         line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "elem-upd/s", "n_gpus": args.gpus, "steps": int(steps),
                 "warmup": args.warmup, "ms_per_step": 1e3 * loop / steps, "higher_is_better": True, "scaling": "weak",
@@ -271,6 +384,8 @@ def main():
         ctx.run_steps_timed(align, phases=True)
     barrier(world)
     launches0 = ctx.launches()
+    # phase events of the last graph only; the force kernel's average comes
+    # from a separate profiled window of the same length inside the run
     with ClockSampler(local) as clocks:
         done, ms, phases, psteps = ctx.run_steps_timed(args.steps, phases=True)
     launches = ctx.launches() - launches0
@@ -278,6 +393,7 @@ def main():
     barrier(world)
     ctx.set_profiling(2)
     _, _, all_phases, all_psteps = ctx.run_steps_timed(20, phases=True)
+    lanes, tune_ms = ctx.tuning()
     value = world * n_hc * args.steps / (ms_max / 1e3)
     peak, peak_kind = measured_peak()
     forces_ms = phases[3] / psteps
@@ -293,21 +409,19 @@ def main():
                          "peak_kind": peak_kind, "traffic": traffic, "bytes_per_launch": bytes_launch, "avg_launch_ms": forces_ms},
             "step_roofline": {"bytes_per_step": step_bytes, "achieved": step_gbs, "frac": step_gbs / peak},
             "phase_ms_per_step": {k: v / all_psteps for k, v in zip(["dt", "contact", "half", "forces", "gather_full", "checks"], all_phases)},
-            "clocks": clocks.summary(), "run_done_early": done}
+            "clocks": clocks.summary(), "run_done_early": done, "slave_lanes": lanes}
+    ctx.close()
     if rank == 0 and world == 1 and not args.no_e2e:
-        e, h2d, d2h = e2e_dropin(ctx, desc, args.e2e_steps, n_hc)
-        line["e2e"] = {"value": e, "unit": "elem-upd/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                       "path": "crush_contact_apply x contacts + crush_compute_forces, host f64 state, pinned buffers"}
-        ctx.close()
-        t0 = time.perf_counter()
-        c2 = Context(desc, device=local)
-        r = c2.run()
-        wall = time.perf_counter() - t0
-        line["e2e_run"] = {"value": n_hc * r.steps / wall, "unit": "elem-upd/s", "steps": int(r.steps), "wall_s": wall,
-                           "h2d_bytes_per_step": int((8 * 6 * n_nodes + 36 * desc.n_hexes) / max(r.steps, 1)),
-                           "d2h_bytes_per_step": int(8 * 3 * n_nodes / max(r.steps, 1)),
-                           "delta_v": [r.vehicle[k].delta_v[0] for k in range(r.n_vehicles)]}
-        c2.close()
+        line["e2e"] = e2e_run(desc, local, n_hc, n_nodes)
+        c3 = Context(desc, device=local)
+        e, h2d, d2h = e2e_dropin(c3, desc, args.e2e_steps, n_hc)
+        c3.close()
+        line["e2e_dropin"] = {"value": e, "unit": "elem-upd/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                              "path": "crush_contact_apply x contacts + crush_compute_forces per step, host f64 state, pinned buffers"}
+    if rank == 0 and world == 1 and args.batch > 0:
+        line["batched"] = batched_section(args.batch, args.plain_sample, args.oracle_sample, local)
+    if rank == 0 and world == 1 and args.serve_rates:
+        line["serving"] = [serving_section(float(r), args.serve_seconds, local) for r in args.serve_rates.split(",") if r]
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         steps, loop, sec = cpu_reference(desc, args.cpu_steps, threads)

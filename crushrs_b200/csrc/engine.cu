@@ -532,8 +532,7 @@ void face_frame(const double* pos, const uint32_t* q, double x[4][3], double nr[
     }
 }
 
-void build_contacts(const crush_model_desc* d, const Slot& sl, const Combined& cm, const std::vector<double>& mass_h, ContactPart& cp,
-                    SlotError& err) {
+void build_contacts(const crush_model_desc* d, const Slot& sl, const Combined& cm, ContactPart& cp, SlotError& err) {
     const long long n0 = sl.node0;
     // Contact-node roles: (node, contact, sequence) sorted gives, for every
     // node, its contacts in order with its primary-node entries and the faces
@@ -584,8 +583,6 @@ void build_contacts(const crush_model_desc* d, const Slot& sl, const Combined& c
             const uint32_t nl = cd.nodes[i];
             if (nl >= (uint64_t)d->n_nodes) return err.set(CRUSH_ERR_INVALID, "contact node out of range");
             const uint32_t n = (uint32_t)(n0 + nl);
-            // contact_dt over every listed node (src/solver.rs:217-223)
-            if (mass_h[n] > 0.0 && cd.stiffness > 0.0) cp.contact_dt = std::fmin(cp.contact_dt, 2.0 * std::sqrt(mass_h[n] / cd.stiffness));
             bool inside = true;
             for (int dd = 0; dd < 3; ++dd) {
                 const double p = cm.positions[3 * (size_t)n + dd];
@@ -889,6 +886,13 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(check_launch(c));
     launch_node_masses(c->stream, N, c->all_off, c->all_slot, c->lumped, c->mass, c->inv_mass);
     TRY(check_launch(c));
+    trace.mark("device geometry launched");
+
+    // ---- contacts: per slot in parallel (overlapping the device set-up), then concatenated ----
+    std::vector<ContactPart> parts(n_desc);
+    parallel_for(n_desc, [&](long long k) { build_contacts(descs[k], c->slots[k], cm, parts[k], errs[k]); });
+    for (auto& e : errs)
+        if (e.code != CRUSH_OK) return crush::fail(e.code, e.msg);
     int bad_h = 0;
     CK(cudaMemcpyAsync(&bad_h, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     std::vector<double> mass_h(N);
@@ -896,13 +900,21 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     CK(cudaStreamSynchronize(c->stream));
     if (bad_h == 1) return crush::fail(CRUSH_ERR_INVALID, "degenerate hexahedron (singular Jacobian)");
     if (bad_h == 2) return crush::fail(CRUSH_ERR_INVALID, "hourglass modes not independent");
-    trace.mark("device geometry + masses");
-
-    // ---- contacts: per slot in parallel, then concatenated ----
-    std::vector<ContactPart> parts(n_desc);
-    parallel_for(n_desc, [&](long long k) { build_contacts(descs[k], c->slots[k], cm, mass_h, parts[k], errs[k]); });
-    for (auto& e : errs)
-        if (e.code != CRUSH_OK) return crush::fail(e.code, e.msg);
+    // contact_dt over every listed node of the slot's contacts (src/solver.rs:217-223)
+    parallel_for(n_desc, [&](long long k) {
+        const crush_model_desc* d = descs[k];
+        double cdt = INF;
+        for (int q = 0; q < d->n_contacts; ++q) {
+            const crush_contact& cd = d->contacts[q];
+            if (!(cd.stiffness > 0.0)) continue;
+            for (int64_t i = 0; i < cd.n_nodes; ++i) {
+                const double m = mass_h[c->slots[k].node0 + cd.nodes[i]];
+                if (m > 0.0) cdt = std::fmin(cdt, 2.0 * std::sqrt(m / cd.stiffness));
+            }
+        }
+        parts[k].contact_dt = cdt;
+    });
+    trace.mark("contacts built, masses");
     // Concatenation: per-slot bases, then every slot copies its part in parallel.
     struct Base {
         long long face, slave, ste, stoff, dyn, grid, cnode, role, rface;

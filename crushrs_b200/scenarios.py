@@ -313,3 +313,34 @@ def serve_query(i, seed=SERVE_SEED, e_range=(300, 20000)):
     va = rng.uniform(10, 30)  # rear-end: B moves the same way, slower
     vb = va * rng.uniform(0.1, 0.6)
     return kind, scenario(a, b, va, -vb, offset=rng.uniform(0.0, 0.5), clearance=0.15, element_size=h, end_time=0.12)
+
+
+def tbone_coverage():
+    """T-bone coverage case (about 2000 hexahedra): A's front into the side of
+    B turned 90 degrees (B's length along y), B's side sigma_y 0.15 MPa,
+    A at 13.41 m/s (30 mph), B at rest, element size 0.2 m."""
+    h = 0.2
+    sa, sb = (3.4, 1.6, 1.2), (1.6, 4.6, 1.2)
+    ma, mb = 1600.0, 1400.0
+    E = 5e6
+    a = vehicle(ma, sa, _block_material(E, ma / np.prod(sa), 0.4e6))
+    b = vehicle(mb, sb, _block_material(E, mb / np.prod(sb), 0.15e6))
+    return scenario(a, b, 30 * MPH, 0.0, offset=0.3, clearance=0.15, element_size=h, layout=abi.LAYOUT_TBONE, end_time=0.1)
+
+
+def railbox_coverage(densify=False, speed=9.0):
+    """Rail-box coverage case (about 2000 hexahedra): head-on where A's front
+    has a central rail box 0.9 m wide over z 0.3-0.9 m carrying 0.7 of the
+    crush force (modulus, yield and density scaled alike), element size 0.2 m,
+    both at `speed` m/s. densify=True adds the lock-up knot [0.75, 50 MPa] to
+    both materials. With densification at 15 m/s elements invert and erode."""
+    h = 0.2
+    sa, sb = (3.6, 1.8, 1.2), (3.6, 1.8, 1.2)
+    ma, mb = 1800.0, 1500.0
+    E = 5e6
+    dens = (0.75, 50e6) if densify else None
+    ha = honeycomb(E, ma / np.prod(sa), 0.45e6, 0.2e6, densification=dens)
+    hb = honeycomb(E, mb / np.prod(sb), 0.35e6, 0.2e6, densification=dens)
+    a = vehicle(ma, sa, ha, rail_box=(0.9, (0.3, 0.9), 0.7))
+    b = vehicle(mb, sb, hb)
+    return scenario(a, b, speed, speed, offset=0.0, clearance=0.15, element_size=h, end_time=0.1)
