@@ -232,6 +232,8 @@ struct crush_ctx {
     std::vector<int> face_off_h, slave_off_h;
     std::vector<uint8_t> is_static_h;
     std::vector<int> tab_off_h;
+    std::vector<uint8_t> is_brute_h;      // per contact: searched by one block, exhaustively
+    std::vector<uint32_t> grid_slaves_h;  // entries of the other contacts
     int slave_lanes = 32;  // lanes per primary-node contact search (autotuned)
     bool tuned = false;
     long long last_tune_step = 0;  // the open run's step of the last tuning
@@ -504,7 +506,7 @@ struct ContactPart {
     std::vector<uint8_t> stat, stop;
     std::vector<double> stiff, md, cell;
     std::vector<uint32_t> faces, slaves, dyn_faces, grid_faces;  // faces/slaves: global node ids; *_faces: slot-local
-    std::vector<double> scales;
+    std::vector<double> scales, box;  // box: 6 per contact (static key-box union, else everything)
     std::vector<uint32_t> st_off;  // per contact T+1 entries, slot-local into st_entries
     std::vector<int> st_entries;
     std::vector<uint32_t> cnode, cnode_off{0}, crole_faces_off{0};
@@ -604,6 +606,7 @@ void build_contacts(const crush_model_desc* d, const Slot& sl, const Combined& c
             // Exact hashed grid of the fixed faces, in CSR form.
             std::vector<std::pair<uint32_t, int>> ins;  // (hash, face)
             bool ok = true;
+            double box[6] = {INF, INF, INF, -INF, -INF, -INF};  // union of the key boxes
             for (int64_t f = 0; f < cd.n_faces && ok; ++f) {
                 double x[4][3], nr[3], ctr[3], klo[3], khi[3];
                 face_frame(cm.positions.data(), fq + 4 * f, x, nr, ctr);
@@ -624,11 +627,16 @@ void build_contacts(const crush_model_desc* d, const Slot& sl, const Combined& c
                     ok = false;
                     break;
                 }
+                for (int dd = 0; dd < 3; ++dd) {
+                    box[dd] = std::fmin(box[dd], klo[dd]);
+                    box[3 + dd] = std::fmax(box[3 + dd], khi[dd]);
+                }
                 for (long long kz = r[4]; kz <= r[5]; ++kz)
                     for (long long jy = r[2]; jy <= r[3]; ++jy)
                         for (long long ix = r[0]; ix <= r[1]; ++ix) ins.push_back({cell_hash(ix, jy, kz, 0), (int)f});
             }
             const uint32_t base = (uint32_t)cp.st_entries.size();
+            if (ok) cp.box.insert(cp.box.end(), box, box + 6);
             if (ok) {
                 st = next_pow2(std::max<size_t>(16, 2 * ins.size()));
                 std::vector<uint32_t> cnt(st + 1, 0);
@@ -660,6 +668,10 @@ void build_contacts(const crush_model_desc* d, const Slot& sl, const Combined& c
                 t = next_pow2(std::max<size_t>(1024, 4 * inserts));
                 for (int64_t f = 0; f < cd.n_faces; ++f) cp.grid_faces.push_back((uint32_t)(face0 + f));
             }
+        }
+        if (cp.box.size() < 6 * (cp.nf.size() + 1)) {
+            const double all[6] = {-INF, -INF, -INF, INF, INF, INF};
+            cp.box.insert(cp.box.end(), all, all + 6);
         }
         cp.nf.push_back((int)cd.n_faces);
         cp.ns.push_back(kept);
@@ -938,7 +950,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     std::vector<int> face_off(kc + 1), slave_off(kc + 1), tab_off(kc + 1), counts_for_stop(kc), face_contact(tot.face),
         slave_contact(tot.slave), contact_slot(kc), slot_contact_off(n_desc + 1);
     std::vector<uint32_t> faces(4 * tot.face), slaves(tot.slave), dyn_faces(tot.dyn), grid_faces(tot.grid);
-    std::vector<double> scales(tot.slave), stiff(kc), md(kc), cell(kc);
+    std::vector<double> scales(tot.slave), stiff(kc), md(kc), cell(kc), st_box(6 * (size_t)std::max(kc, 1));
     std::vector<uint8_t> is_static(kc);
     std::vector<long long> st_tab_off(kc + 1);
     std::vector<uint32_t> st_off(tot.stoff);
@@ -979,6 +991,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
         std::copy(cp.faces.begin(), cp.faces.end(), faces.begin() + 4 * b.face);
         std::copy(cp.slaves.begin(), cp.slaves.end(), slaves.begin() + b.slave);
         std::copy(cp.scales.begin(), cp.scales.end(), scales.begin() + b.slave);
+        std::copy(cp.box.begin(), cp.box.end(), st_box.begin() + 6 * (size_t)q0);
         for (size_t j = 0; j < cp.st_off.size(); ++j) st_off[b.stoff + j] = cp.st_off[j] + (uint32_t)b.ste;
         std::copy(cp.st_entries.begin(), cp.st_entries.end(), st_entries.begin() + b.ste);
         for (size_t j = 0; j < cp.dyn_faces.size(); ++j) dyn_faces[b.dyn + j] = cp.dyn_faces[j] + (uint32_t)b.face;
@@ -1028,6 +1041,29 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
         ca.n_grid_faces = (long long)grid_faces.size();
         TRY(c->upload_const(&ca.grid_faces, grid_faces));
     }
+    {
+        // exhaustive contacts (no grid) get a block each; the rest are listed by entry
+        std::vector<int> brute;
+        std::vector<uint32_t> gslaves;
+        c->is_brute_h.assign(std::max(kc, 1), 0);
+        for (int k = 0; k < kc; ++k) {
+            const bool grid = tab_off[k + 1] > tab_off[k] || st_tab_off[k + 1] > st_tab_off[k];
+            if (!grid && face_off[k + 1] - face_off[k] <= 255 && slave_off[k + 1] > slave_off[k]) {
+                brute.push_back(k);
+                c->is_brute_h[k] = 1;
+            } else {
+                for (int q = slave_off[k]; q < slave_off[k + 1]; ++q) gslaves.push_back((uint32_t)q);
+            }
+        }
+        ca.n_brute = (int)brute.size();
+        ca.brute_max_faces = 1;
+        for (int k : brute) ca.brute_max_faces = std::max(ca.brute_max_faces, face_off[k + 1] - face_off[k]);
+        ca.n_grid_slaves = (long long)gslaves.size();
+        TRY(c->upload_const(&ca.brute_contacts, brute));
+        TRY(c->upload_const(&ca.grid_slaves, gslaves));
+        ca.is_brute_h = c->is_brute_h.data();
+        c->grid_slaves_h = std::move(gslaves);
+    }
     TRY(c->alloc(&ca.ent_cursor, std::max(kc, 1)));
     TRY(c->alloc(&ca.gather_work, std::max<size_t>(cnode.size(), 1)));
     TRY(c->alloc(&ca.gather_count, 1));
@@ -1066,6 +1102,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->upload_const(&ca.st_tab_off, st_tab_off));
     TRY(c->upload_const(&ca.st_off, st_off));
     TRY(c->upload_const(&ca.st_entries, st_entries));
+    TRY(c->upload_const(&ca.st_box, st_box));
     ca.n_dyn_faces = (long long)dyn_faces.size();
     TRY(c->upload_const(&ca.dyn_faces, dyn_faces));
     CK(cudaMemsetAsync(ca.counts, 0, sizeof(int) * std::max(tab_off.back(), 1), c->stream));
@@ -1126,7 +1163,8 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->alloc(&c->crush_ux, std::max<size_t>(c->crush_nodes_h.size(), 1)));
     // ---- active chunk tables: slot range of every 256-entity chunk ----
     {
-        const long long sizes[ACTIVE_SPACES] = {c->n_hc, E, N, (long long)slaves.size(), (long long)cnode.size(), (long long)dyn_faces.size()};
+        const long long sizes[ACTIVE_SPACES] = {c->n_hc, E, N, (long long)c->grid_slaves_h.size(), (long long)cnode.size(),
+                                                (long long)dyn_faces.size()};
         c->space_off_h.assign(ACTIVE_SPACES + 1, 0);
         for (int sp = 0; sp < ACTIVE_SPACES; ++sp) c->space_off_h[sp + 1] = c->space_off_h[sp] + (sizes[sp] + CHUNK - 1) / CHUNK;
         const long long nch = c->space_off_h[ACTIVE_SPACES];
@@ -1136,7 +1174,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
                 case 0: return (int)cm.elem_slot[c->hc_model[i]];
                 case 1: return (int)cm.elem_slot[i];
                 case 2: return (int)cm.node_slot[i];
-                case 3: return contact_slot[slave_contact[i]];
+                case 3: return contact_slot[slave_contact[c->grid_slaves_h[i]]];
                 case 4: return (int)cm.node_slot[cnode[i]];
                 default: return contact_slot[face_contact[dyn_faces[i]]];
             }
@@ -1245,7 +1283,7 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
     if (c->n_contacts > 0) {
         launch_contact(c->stream, cr, nd, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 0.0, c->mass,
                        c->f_ext, 1, c->slave_lanes);
-        n += contact_launches(c->ca, true, c->n_faces, c->n_slaves, 0, c->ca.n_buckets);
+        n += contact_launches(c->ca, true, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 0);
     }
     mark(2);
     launch_half(c->stream, nd, c->ctls);
@@ -1294,7 +1332,7 @@ int autotune(crush_ctx* c) {
             if (rep == 1) cudaEventRecord(t0, c->stream);
             launch_contact(c->stream, c->ca, nd, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 0.0, c->mass,
                            c->f_tmp, 1, lanes);
-            st = check_launch(c, contact_launches(c->ca, true, c->n_faces, c->n_slaves, 0, c->ca.n_buckets));
+            st = check_launch(c, contact_launches(c->ca, true, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 0));
             if (st != CRUSH_OK) break;
         }
         cudaEventRecord(t1, c->stream);
@@ -1679,7 +1717,7 @@ int crush_contact_apply(crush_ctx* c, int id, const double* u, const double* v, 
     const long long bk0 = c->tab_off_h[id], bk1 = c->tab_off_h[id + 1];
     launch_contact(c->stream, c->ca, nd, c->ctls_aux, id, id + 1, c->face_off_h[id], nf, ns, bk0, bk1, dt, m, c->f_tmp, 0,
                    c->slave_lanes);
-    int st = check_launch(c, contact_launches(c->ca, false, nf, ns, bk0, bk1));
+    int st = check_launch(c, contact_launches(c->ca, false, nf, ns, bk0, bk1, id));
     if (st != CRUSH_OK) return st;
     if (c->run_open && c->is_static_h[id]) {
         // The call rebuilt the static faces' geometry at its own u: restore

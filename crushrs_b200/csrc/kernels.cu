@@ -984,13 +984,31 @@ __device__ __forceinline__ bool face_hit(const FaceGeo& g, const double* p, doub
 // this is a drop-in call on a static contact; and keep the smallest face
 // index that hits: the face the reference's in-order scan with `break` finds
 // (src/contact.rs:115-157).
+// The penalty force of primary-node entry s (node n of contact c) on its
+// first-hit face `best` (src/contact.rs:130-153: depth capped at 0.1 md,
+// stiffness limited to 0.1 m / dt^2, force capped at m * 1e5).
+__device__ __forceinline__ void record_hit(const ContactArrays& ca, long long s, int c, long long n, int best, double best_sd, double dt,
+                                           const double* __restrict__ masses, const FaceGeo& g) {
+    const double md = ca.max_distance[c];
+    const double m = masses[n];
+    const double depth = fmin(-best_sd, 0.1 * md);
+    const double k_pen = fmin(ca.stiffness[c] * ca.slave_scale[s], 0.1 * m / (dt * dt));
+    const double mag = fmin(k_pen * depth, m * 1.0e5);
+    ca.hit[s] = best;
+    ca.hit_force[3 * s] = mag * g.n[0];
+    ca.hit_force[3 * s + 1] = mag * g.n[1];
+    ca.hit_force[3 * s + 2] = mag * g.n[2];
+    const long long F = ca.face_off[c] + best;
+    const int slot = atomicAdd(&ca.face_hits[F], 1);
+    if (slot < FACE_HIT_CAP) ca.face_list[F * FACE_HIT_CAP + slot] = (int)s;
+    atomicAdd(&ca.pen_count[c], 1ull);
+    atomicMax(&ca.pen_max_bits[c], (unsigned long long)__double_as_longlong(-best_sd));
+}
+
 template <int LANES>
 __device__ __forceinline__ void contact_slave_body(const ContactArrays& ca, const NodeArrays& nd, const Control* ctls, int c0, int c1,
-                                                   int run_mode, double dt_override, const double* __restrict__ masses, long long e,
-                                                   int lane) {
-    const long long s_begin = ca.slave_off[c0], s_end = ca.slave_off[c1];
-    const long long s = s_begin + e;
-    bool live = s < s_end;
+                                                   int run_mode, double dt_override, const double* __restrict__ masses, long long s,
+                                                   bool live, int lane) {
     const Control* ctl = nullptr;
     if (live) {
         ctl = ctls + ca.contact_slot[ca.slave_contact[s]];
@@ -1016,7 +1034,11 @@ __device__ __forceinline__ void contact_slave_body(const ContactArrays& ca, cons
         const int tab = ca.tab_off[c];
         const bool dyn_grid = ca.tab_off[c + 1] > tab;
         bool all = false;
-        if (run_mode && st1 > st0 && !ca.exhaustive) {
+        const double* box = ca.st_box + 6 * c;
+        if (run_mode && st1 > st0 && !ca.exhaustive &&
+            !(p[0] >= box[0] && p[0] <= box[3] && p[1] >= box[1] && p[1] <= box[4] && p[2] >= box[2] && p[2] <= box[5])) {
+            // Outside every key box of the fixed faces: nothing to test.
+        } else if (run_mode && st1 > st0 && !ca.exhaustive) {
             // Static grid: the bucket of the point's cell, exact.
             const unsigned mask = (unsigned)(st1 - st0 - 1);
             const long long bk = st0 + (point_cell_hash(p, ca.cell[c], 0) & mask);
@@ -1063,31 +1085,60 @@ __device__ __forceinline__ void contact_slave_body(const ContactArrays& ca, cons
         ca.hit[s] = -1;
         return;
     }
-    const double dt = dt_override > 0.0 ? dt_override : step_dt(ctl);
-    const double m = masses[n];
-    const double depth = fmin(-best_sd, 0.1 * md);
-    const double k_pen = fmin(ca.stiffness[c] * ca.slave_scale[s], 0.1 * m / (dt * dt));
-    const double mag = fmin(k_pen * depth, m * 1.0e5);
-    const FaceGeo& g = geo[best];
-    ca.hit[s] = best;
-    ca.hit_force[3 * s] = mag * g.n[0];
-    ca.hit_force[3 * s + 1] = mag * g.n[1];
-    ca.hit_force[3 * s + 2] = mag * g.n[2];
-    const long long F = ca.face_off[c] + best;
-    const int slot = atomicAdd(&ca.face_hits[F], 1);
-    if (slot < FACE_HIT_CAP) ca.face_list[F * FACE_HIT_CAP + slot] = (int)s;
-    atomicAdd(&ca.pen_count[c], 1ull);
-    atomicMax(&ca.pen_max_bits[c], (unsigned long long)__double_as_longlong(-best_sd));
+    record_hit(ca, s, c, n, best, best_sd, dt_override > 0.0 ? dt_override : step_dt(ctl), masses, geo[best]);
 }
 
 template <int LANES>
 __global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, int c1, int run_mode, double dt_override,
                                  const double* __restrict__ masses, long long n_slaves) {
-    const Active act = run_mode ? ca.act_slave : Active{nullptr, nullptr};
+    // run: the primary-node entries of contacts with a grid (a list), else
+    // the entries of contacts [c0, c1)
+    const bool listed = run_mode && !ca.exhaustive;
+    const Active act = listed ? ca.act_slave : Active{nullptr, nullptr};
+    const long long s_begin = ca.slave_off[c0];
     FOR_ACTIVE(act, n_slaves, LANES, g) {
         int lane;
         const long long e = active_entity(act, g, LANES, &lane);
-        contact_slave_body<LANES>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses, e, lane);
+        const bool live = e < n_slaves;
+        const long long s = !live ? 0 : (listed ? (long long)ca.grid_slaves[e] : s_begin + e);
+        contact_slave_body<LANES>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses, s, live, lane);
+    }
+}
+
+// Contacts searched exhaustively (fewer faces than the grid threshold), one
+// block per contact: the contact's face geometry is staged in shared memory
+// and each thread scans the faces in order for one primary node and stops at
+// the first hit, as src/contact.rs:115-157 does.
+constexpr int BRUTE_TPB = 128;
+constexpr int BRUTE_MAX_FACES = 255;  // 255 x 192 B fits the default 48 KB of shared memory
+__global__ void __launch_bounds__(BRUTE_TPB) k_contact_brute(ContactArrays ca, NodeArrays nd, Control* ctls, const int* __restrict__ list,
+                                                            int single, int run_mode, double dt_override, const double* __restrict__ masses) {
+    extern __shared__ double sbuf[];
+    FaceGeo* sgeo = reinterpret_cast<FaceGeo*>(sbuf);
+    const int c = list ? list[blockIdx.x] : single;
+    const Control* ctl = ctls + ca.contact_slot[c];
+    if (run_mode && ctl->done) return;  // block-uniform
+    const long long fb = ca.face_off[c];
+    const int nf = (int)(ca.face_off[c + 1] - fb);
+    const double* src = reinterpret_cast<const double*>(ca.geo + fb);
+    for (int k = threadIdx.x; k < nf * (int)(sizeof(FaceGeo) / sizeof(double)); k += blockDim.x) sbuf[k] = src[k];
+    __syncthreads();
+    const double md = ca.max_distance[c];
+    for (long long s = ca.slave_off[c] + threadIdx.x; s < ca.slave_off[c + 1]; s += blockDim.x) {
+        const long long n = ca.slaves[s];
+        const double p[3] = {nd.pos[3 * n] + nd.u[3 * n], nd.pos[3 * n + 1] + nd.u[3 * n + 1], nd.pos[3 * n + 2] + nd.u[3 * n + 2]};
+        int best = -1;
+        double sd = 0.0;
+        for (int f = 0; f < nf; ++f)
+            if (face_hit(sgeo[f], p, md, &sd)) {
+                best = f;
+                break;
+            }
+        if (best < 0) {
+            ca.hit[s] = -1;
+            continue;
+        }
+        record_hit(ca, s, c, n, best, sd, dt_override > 0.0 ? dt_override : step_dt(ctl), masses, sgeo[best]);
     }
 }
 
@@ -1407,6 +1458,17 @@ void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& n
             k_contact_faces<<<active_grid(n_glist, 1, TPB, GRID_CAP), TPB, 0, s>>>(ca, nd, ctls, c0, glist, n_glist, run_mode, 1,
                                                                                  Active{nullptr, nullptr});
     }
+    // Exhaustive contacts: a block each (run: the listed ones; drop-in: the one contact if it is one).
+    if (!ca.exhaustive) {
+        if (run_mode && ca.n_brute > 0)
+            k_contact_brute<<<(unsigned)ca.n_brute, BRUTE_TPB, sizeof(FaceGeo) * ca.brute_max_faces, s>>>(ca, nd, ctls, ca.brute_contacts,
+                                                                                                          0, 1, dt_override, masses);
+        if (!run_mode && c1 == c0 + 1 && ca.is_brute_h && ca.is_brute_h[c0]) {
+            k_contact_brute<<<1, BRUTE_TPB, sizeof(FaceGeo) * BRUTE_MAX_FACES, s>>>(ca, nd, ctls, nullptr, c0, 0, dt_override, masses);
+            n_slaves = 0;
+        }
+        if (run_mode) n_slaves = ca.n_grid_slaves;
+    }
     if (n_slaves > 0) {
         const unsigned g = active_grid(n_slaves, lanes, TPB, GRID_CAP);
         switch (lanes) {
@@ -1424,10 +1486,20 @@ void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& n
     k_contact_gather_walk<<<(unsigned)(walk_blocks < WALK_BLOCKS ? walk_blocks : WALK_BLOCKS), GATHER_TPB, 0, s>>>(ca, c0, c1, f_out);
 }
 
-int contact_launches(const ContactArrays& ca, bool run_mode, long long n_faces, long long n_slaves, long long bk0, long long bk1) {
+int contact_launches(const ContactArrays& ca, bool run_mode, long long n_faces, long long n_slaves, long long bk0, long long bk1,
+                     int c0) {
     int k = 2;  // gather + overflow walk
     if ((run_mode ? ca.n_dyn_faces : n_faces) > 0) ++k;
     if (bk1 > bk0 && !ca.exhaustive) k += (run_mode ? ca.n_grid_faces : n_faces) > 0 ? 2 : 1;
+    if (!ca.exhaustive) {
+        if (run_mode) {
+            k += ca.n_brute > 0 ? 1 : 0;
+            n_slaves = ca.n_grid_slaves;
+        } else if (ca.is_brute_h && ca.is_brute_h[c0]) {
+            ++k;
+            n_slaves = 0;
+        }
+    }
     if (n_slaves > 0) ++k;
     return k;
 }

@@ -136,7 +136,16 @@ struct ContactArrays {
     int exhaustive;             // 1: every search tests every face of its contact (no broad phase)
     int* gather_work;           // contact nodes whose hit lists overflowed this pass (n_cnodes capacity)
     int* gather_count;          // their number
-    Active act_slave, act_cnode, act_dynf;  // active chunks of primary-node entries, contact nodes, moving faces
+    Active act_slave, act_cnode, act_dynf;  // active chunks of grid-searched entries, contact nodes, moving faces
+    // Contacts without a grid are searched by one block each; the entries of
+    // the others are listed for the lane-parallel search.
+    const int* brute_contacts;
+    int n_brute;
+    int brute_max_faces;        // most faces of a listed contact (its shared-memory stage)
+    const double* st_box;       // 6 per contact: union of a static contact's key boxes (lo xyz, hi xyz)
+    const uint32_t* grid_slaves;
+    long long n_grid_slaves;
+    const uint8_t* is_brute_h;  // host copy, per contact (launchers only)
 };
 
 // Chunks of every entity space with the crash-slot range each covers, and
@@ -149,7 +158,7 @@ struct ActiveBuild {
     int* lists;                  // same layout as the chunks
     int* counts;                 // ACTIVE_SPACES
 };
-constexpr int ACTIVE_SPACES = 6;  // honeycomb elements, all elements, nodes, primary-node entries, contact nodes, moving faces
+constexpr int ACTIVE_SPACES = 6;  // honeycomb elements, all elements, nodes, grid-searched entries, contact nodes, moving faces
 
 // Vehicles of all crash slots: node lists and the reduction layout.
 struct VehicleArrays {
@@ -190,7 +199,8 @@ void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& n
                     long long n_faces, long long n_slaves, long long bk0, long long bk1, double dt_override, const double* masses,
                     double* f_out, int skip_fixed, int lanes);
 // Kernel launches one launch_contact call issues.
-int contact_launches(const ContactArrays& ca, bool run_mode, long long n_faces, long long n_slaves, long long bk0, long long bk1);
+int contact_launches(const ContactArrays& ca, bool run_mode, long long n_faces, long long n_slaves, long long bk0, long long bk1,
+                     int c0);
 // Geometry of every face of contacts [c0, c1) at X + u (no grid insertion):
 // the static contacts' geometry for a run.
 void launch_contact_geometry(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, int c0, int c1, long long f0,
