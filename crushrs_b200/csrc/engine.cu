@@ -1093,7 +1093,8 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->upload_const(&ca.crole_faces_off, crole_faces_off));
     TRY(c->upload_const(&ca.crole_faces, crole_faces));
     TRY(c->alloc(&ca.face_hits, std::max<long long>(c->n_faces, 1)));
-    TRY(c->alloc(&ca.face_list, (size_t)std::max<long long>(c->n_faces, 1) * FACE_HIT_CAP));
+    ca.hit_cap = c->n_faces <= (1ll << 20) ? 32 : 8;
+    TRY(c->alloc(&ca.face_list, (size_t)std::max<long long>(c->n_faces, 1) * ca.hit_cap));
     TRY(c->upload_const(&ca.face_contact, face_contact));
     TRY(c->upload_const(&ca.slave_contact, slave_contact));
     TRY(c->upload_const(&ca.contact_slot, contact_slot));

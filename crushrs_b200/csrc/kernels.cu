@@ -853,35 +853,41 @@ __device__ __forceinline__ int face_cells(const ContactArrays& ca, const FaceGeo
     return GRID_LEVELS;
 }
 
-// Thread per face. Pass 0: geometry; for faces of contacts with a dynamic
-// grid also the count of their key box's cells per bucket, or their place on
-// the overflow list. Pass 1 (grid faces only, after k_grid_alloc): the fill of
-// the buckets, which returns every count to zero. Pass 2: geometry only. The
-// faces are
-// face_list[0, n) when face_list is given, else face_off[c0] + [0, n).
+// Thread per face: the face's geometry at X + u. The faces are
+// face_list[0, n) when face_list is given (the run: moving faces only), else
+// face_off[c0] + [0, n).
 __device__ __forceinline__ void contact_face_body(const ContactArrays& ca, const NodeArrays& nd, const Control* ctls, int c0,
                                                   const uint32_t* __restrict__ face_list, long long n, int run_mode, int pass, long long t) {
     if (t >= n) return;
     const long long f = face_list ? (long long)face_list[t] : ca.face_off[c0] + t;
     const int c = ca.face_contact[f];
     if (run_mode && ctls[ca.contact_slot[c]].done) return;
-    const int tab = ca.tab_off[c];
-    const bool grid = ca.tab_off[c + 1] > tab && !ca.exhaustive;
     FaceGeo g;
-    if (pass != 1) {
-        face_geometry(ca, nd, f, ca.max_distance[c], g);
-        ca.geo[f] = g;
-        if (!grid || pass == 2) return;
-    } else {
-        if (!grid) return;
-        g = ca.geo[f];
-    }
+    face_geometry(ca, nd, f, ca.max_distance[c], g);
+    ca.geo[f] = g;
+}
+
+// Warp per face of a contact with a dynamic grid: every lane derives the
+// face's grid level and key-box cells from its geometry, and the lanes split
+// the cells. Pass 0 counts the cells' inserts per bucket (or puts the face on
+// the overflow list); pass 1, after k_grid_alloc, fills the buckets, which
+// returns every count to zero.
+__global__ void k_contact_insert(ContactArrays ca, Control* ctls, int c0, const uint32_t* __restrict__ face_list, long long n,
+                                 int run_mode, int pass) {
+    const long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // warp-uniform
+    const int lane = threadIdx.x & 31;
+    if (t >= n) return;
+    const long long f = face_list ? (long long)face_list[t] : ca.face_off[c0] + t;
+    const int c = ca.face_contact[f];
+    const int tab = ca.tab_off[c];
+    if (ca.tab_off[c + 1] == tab || (run_mode && ctls[ca.contact_slot[c]].done)) return;
+    const FaceGeo g = ca.geo[f];
     long long r[6];
     const int level = face_cells(ca, g, c, r);
     if (level < 0) return;
     const int local = (int)(f - ca.face_off[c]);
     if (level == GRID_LEVELS) {
-        if (pass == 0) {
+        if (pass == 0 && lane == 0) {
             int slot = atomicAdd(&ca.n_overflow[c], 1);
             if (slot < ca.overflow_cap) ca.overflow[(long long)c * ca.overflow_cap + slot] = local;
             else ca.entry_overrun[c] = 1;
@@ -889,19 +895,19 @@ __device__ __forceinline__ void contact_face_body(const ContactArrays& ca, const
         }
         return;
     }
-    if (pass == 0 && !(ca.levels_used[c] & (1 << level))) atomicOr(&ca.levels_used[c], 1 << level);
+    if (pass == 0 && lane == 0 && !(ca.levels_used[c] & (1 << level))) atomicOr(&ca.levels_used[c], 1 << level);
     const unsigned mask = (unsigned)(ca.tab_off[c + 1] - tab - 1);
-    for (long long k = r[4]; k <= r[5]; ++k)
-        for (long long j = r[2]; j <= r[3]; ++j)
-            for (long long i = r[0]; i <= r[1]; ++i) {
-                const int b = tab + (int)(cell_hash(i, j, k, level) & mask);
-                if (pass == 0) {
-                    atomicAdd(&ca.counts[b], 1);
-                } else {
-                    const int pos = atomicSub(&ca.counts[b], 1) - 1;
-                    ca.entries[ca.boff[b] + pos] = local;
-                }
-            }
+    const int ni = (int)(r[1] - r[0] + 1), nj = (int)(r[3] - r[2] + 1), nk = (int)(r[5] - r[4] + 1);
+    for (int q = lane; q < ni * nj * nk; q += 32) {
+        const long long i = r[0] + q % ni, j = r[2] + (q / ni) % nj, k = r[4] + q / (ni * nj);
+        const int b = tab + (int)(cell_hash(i, j, k, level) & mask);
+        if (pass == 0) {
+            atomicAdd(&ca.counts[b], 1);
+        } else {
+            const int pos = atomicSub(&ca.counts[b], 1) - 1;
+            ca.entries[ca.boff[b] + pos] = local;
+        }
+    }
 }
 
 __global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, const uint32_t* __restrict__ face_list,
@@ -1000,7 +1006,7 @@ __device__ __forceinline__ void record_hit(const ContactArrays& ca, long long s,
     ca.hit_force[3 * s + 2] = mag * g.n[2];
     const long long F = ca.face_off[c] + best;
     const int slot = atomicAdd(&ca.face_hits[F], 1);
-    if (slot < FACE_HIT_CAP) ca.face_list[F * FACE_HIT_CAP + slot] = (int)s;
+    if (slot < ca.hit_cap) ca.face_list[F * ca.hit_cap + slot] = (int)s;
     atomicAdd(&ca.pen_count[c], 1ull);
     atomicMax(&ca.pen_max_bits[c], (unsigned long long)__double_as_longlong(-best_sd));
 }
@@ -1142,7 +1148,7 @@ __global__ void __launch_bounds__(BRUTE_TPB) k_contact_brute(ContactArrays ca, N
     }
 }
 
-constexpr int MAX_NODE_EVENTS = 48;
+constexpr int MAX_NODE_EVENTS = 64;
 constexpr int GATHER_TPB = 128;
 constexpr int WALK_BLOCKS = 296;  // 2 x 148 SMs of 4 warps
 
@@ -1160,8 +1166,8 @@ __device__ __forceinline__ bool role_sum(const ContactArrays& ca, uint32_t r, in
     for (uint32_t q = ca.crole_faces_off[r]; q < ca.crole_faces_off[r + 1]; ++q) {
         const long long f = ca.face_off[c] + ca.crole_faces[q];
         const int cnt = ca.face_hits[f];
-        if (cnt > FACE_HIT_CAP || ne + cnt > MAX_NODE_EVENTS) return false;
-        for (int k = 0; k < cnt; ++k) ev[ne++] = 2ull * (unsigned long long)ca.face_list[f * FACE_HIT_CAP + k] + 1ull;
+        if (cnt > ca.hit_cap || ne + cnt > MAX_NODE_EVENTS) return false;
+        for (int k = 0; k < cnt; ++k) ev[ne++] = 2ull * (unsigned long long)ca.face_list[f * ca.hit_cap + k] + 1ull;
     }
     for (int a = 1; a < ne; ++a) {  // insertion sort, tiny lists
         unsigned long long key = ev[a];
@@ -1451,12 +1457,13 @@ void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& n
         k_contact_faces<<<active_grid(n_list, 1, TPB, GRID_CAP), TPB, 0, s>>>(ca, nd, ctls, c0, list, n_list, run_mode, 0,
                                                                             run_mode ? ca.act_dynf : Active{nullptr, nullptr});
     if (bk1 > bk0 && !ca.exhaustive) {
-        k_grid_alloc<<<(unsigned)blocks_for(bk1 - bk0, TPB), TPB, 0, s>>>(ca, c0, c1);
         const uint32_t* glist = run_mode ? ca.grid_faces : nullptr;
         const long long n_glist = run_mode ? ca.n_grid_faces : n_faces;
         if (n_glist > 0)
-            k_contact_faces<<<active_grid(n_glist, 1, TPB, GRID_CAP), TPB, 0, s>>>(ca, nd, ctls, c0, glist, n_glist, run_mode, 1,
-                                                                                 Active{nullptr, nullptr});
+            k_contact_insert<<<(unsigned)blocks_for(n_glist * 32, TPB), TPB, 0, s>>>(ca, ctls, c0, glist, n_glist, run_mode, 0);
+        k_grid_alloc<<<(unsigned)blocks_for(bk1 - bk0, TPB), TPB, 0, s>>>(ca, c0, c1);
+        if (n_glist > 0)
+            k_contact_insert<<<(unsigned)blocks_for(n_glist * 32, TPB), TPB, 0, s>>>(ca, ctls, c0, glist, n_glist, run_mode, 1);
     }
     // Exhaustive contacts: a block each (run: the listed ones; drop-in: the one contact if it is one).
     if (!ca.exhaustive) {
@@ -1490,7 +1497,7 @@ int contact_launches(const ContactArrays& ca, bool run_mode, long long n_faces, 
                      int c0) {
     int k = 2;  // gather + overflow walk
     if ((run_mode ? ca.n_dyn_faces : n_faces) > 0) ++k;
-    if (bk1 > bk0 && !ca.exhaustive) k += (run_mode ? ca.n_grid_faces : n_faces) > 0 ? 2 : 1;
+    if (bk1 > bk0 && !ca.exhaustive) k += (run_mode ? ca.n_grid_faces : n_faces) > 0 ? 3 : 1;
     if (!ca.exhaustive) {
         if (run_mode) {
             k += ca.n_brute > 0 ? 1 : 0;

@@ -63,9 +63,9 @@ struct FaceGeo {
     double hi[3];
 };
 
-// Per-face hit lists hold FACE_HIT_CAP primary nodes (fuller lists make the
-// gather walk the contact's primary nodes in order).
-constexpr int FACE_HIT_CAP = 8;
+// Per-face hit lists hold hit_cap primary nodes (32, or 8 for contexts with
+// over a million faces; fuller lists make the gather walk the contact's
+// primary nodes in order).
 // Dynamic grids are hashed and hierarchical: level l has cells of size
 // cell * 4^l, and a face goes into the finest level where its key box covers
 // at most LEVEL_CELL_BUDGET cells (beyond the last level, or not finite: the
@@ -115,7 +115,8 @@ struct ContactArrays {
     const uint32_t* crole_faces_off;  // per role + 1: range in crole_faces
     const int* crole_faces;     // local indices of the contact's faces that contain the node
     int* face_hits;             // per face: primary nodes hitting it this step
-    int* face_list;             // FACE_HIT_CAP primary nodes (global index) per face
+    int* face_list;             // hit_cap primary nodes (global index) per face
+    int hit_cap;
     const int* face_contact;    // contact of each face
     const int* slave_contact;   // contact of each primary node entry
     const int* contact_slot;    // crash slot of each contact
