@@ -280,14 +280,16 @@ def batched_section(n, plain_sample, oracle_sample, device):
         c.close()
         times.append(time.perf_counter() - t)
         same &= r.steps == rs[i].steps and list(r.vehicle[0].delta_v) == list(rs[i].vehicle[0].delta_v)
-    plain_s = statistics.median(times)
     batched_cps = n / (t2 - t0)
     out = {"crashes": n, "elements": elems, "create_s": t1 - t0, "run_s": t2 - t1, "crashes_per_s": batched_cps,
            "elem_upd_per_s": eu / (t2 - t0), "steps_mean": statistics.mean(steps), "steps_max": max(steps),
-           "gpu_launches": int(launches), "slave_lanes": lanes,
-           "plain": {"crashes_per_s": 1.0 / plain_s, "median_s_per_crash": plain_s, "sample": plain_sample,
-                     "path": "crush_create + crush_run per crash (CUDA graphs of 20 steps)"},
-           "speedup_vs_plain": batched_cps * plain_s, "batched_equals_plain": bool(same)}
+           "gpu_launches": int(launches), "slave_lanes": lanes}
+    if times:
+        plain_s = statistics.median(times)
+        out["plain"] = {"crashes_per_s": 1.0 / plain_s, "median_s_per_crash": plain_s, "sample": plain_sample,
+                        "path": "crush_create + crush_run per crash (CUDA graphs of 20 steps)"}
+        out["speedup_vs_plain"] = batched_cps * plain_s
+        out["batched_equals_plain"] = bool(same)
     if oracle_sample:
         from tests import oracle_lib as O
 
@@ -334,7 +336,18 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=30.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--sections", default="refined,e2e,batched,serving,cpu",
+                    help="which parts to run (profiling runs pick one; the refined part gives the main line's value)")
     args = ap.parse_args()
+    sections = set(args.sections.split(","))
+    if "e2e" not in sections:
+        args.no_e2e = True
+    if "cpu" not in sections:
+        args.no_cpu = True
+    if "batched" not in sections:
+        args.batch = 0
+    if "serving" not in sections:
+        args.serve_rates = ""
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
 
@@ -367,6 +380,16 @@ def main():
         return
 
     from crushrs_b200.engine import Context
+
+    if "refined" not in sections:
+        line = {"metric": METRIC, "sections": sorted(sections)}
+        if rank == 0 and world == 1 and args.batch > 0:
+            line["batched"] = batched_section(args.batch, args.plain_sample, args.oracle_sample, local)
+        if rank == 0 and world == 1 and args.serve_rates:
+            line["serving"] = [serving_section(float(r), args.serve_seconds, local) for r in args.serve_rates.split(",") if r]
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
 
     ctx = Context(desc, device=local)
     n_hc = ctx.n_active
