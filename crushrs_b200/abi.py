@@ -267,7 +267,7 @@ class Tuning(C.Structure):
     _fields_ = [
         ("slave_lanes", C.c_int32),
         ("reserved", C.c_int32),
-        ("contact_ms", C.c_double * 4),
+        ("contact_ms", C.c_double * 6),
     ]
 
 

@@ -237,7 +237,7 @@ struct crush_ctx {
     int slave_lanes = 32;  // lanes per primary-node contact search (autotuned)
     bool tuned = false;
     long long last_tune_step = 0;  // the open run's step of the last tuning
-    double tune_ms[4] = {0, 0, 0, 0};
+    double tune_ms[6] = {0, 0, 0, 0, 0, 0};
 
     // vehicles
     VehicleArrays va{};
@@ -1312,7 +1312,7 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
 constexpr long long RETUNE_STEPS = 1000;
 
 // Launch autotuner: times the run's contact pass (at the open run's state,
-// output into scratch, no state change) with 4, 8, 16 and 32 lanes per
+// output into scratch, no state change) with 1, 2, 4, 8, 16 and 32 lanes per
 // primary-node search, three passes each after a warm-up, and keeps the
 // fastest. Every choice finds the same hits; only the speed differs.
 int autotune(crush_ctx* c) {
@@ -1322,12 +1322,12 @@ int autotune(crush_ctx* c) {
     cudaEvent_t t0, t1;
     CK(cudaEventCreate(&t0));
     CK(cudaEventCreate(&t1));
-    const int options[4] = {4, 8, 16, 32};
+    const int options[6] = {1, 2, 4, 8, 16, 32};
     double best = INF;
     int best_lanes = c->slave_lanes;
     NodeArrays nd = c->nd();
     int st = CRUSH_OK;
-    for (int k = 0; k < 4 && st == CRUSH_OK; ++k) {
+    for (int k = 0; k < 6 && st == CRUSH_OK; ++k) {
         const int lanes = options[k];
         for (int rep = 0; rep < 4; ++rep) {
             if (rep == 1) cudaEventRecord(t0, c->stream);
@@ -1915,7 +1915,7 @@ int crush_get_tuning(const crush_ctx* c, crush_tuning* out) {
     if (!c || !out) return crush::fail(CRUSH_ERR_INVALID, "null argument");
     std::memset(out, 0, sizeof(*out));
     out->slave_lanes = c->slave_lanes;
-    for (int k = 0; k < 4; ++k) out->contact_ms[k] = c->tune_ms[k];
+    for (int k = 0; k < 6; ++k) out->contact_ms[k] = c->tune_ms[k];
     return CRUSH_OK;
 }
 

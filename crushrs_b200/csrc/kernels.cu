@@ -1116,6 +1116,7 @@ __global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctls,
 // and each thread scans the faces in order for one primary node and stops at
 // the first hit, as src/contact.rs:115-157 does.
 constexpr int BRUTE_TPB = 128;
+constexpr int BRUTE_LANES = 4;
 constexpr int BRUTE_MAX_FACES = 255;  // 255 x 192 B fits the default 48 KB of shared memory
 __global__ void __launch_bounds__(BRUTE_TPB) k_contact_brute(ContactArrays ca, NodeArrays nd, Control* ctls, const int* __restrict__ list,
                                                             int single, int run_mode, double dt_override, const double* __restrict__ masses) {
@@ -1130,21 +1131,41 @@ __global__ void __launch_bounds__(BRUTE_TPB) k_contact_brute(ContactArrays ca, N
     for (int k = threadIdx.x; k < nf * (int)(sizeof(FaceGeo) / sizeof(double)); k += blockDim.x) sbuf[k] = src[k];
     __syncthreads();
     const double md = ca.max_distance[c];
-    for (long long s = ca.slave_off[c] + threadIdx.x; s < ca.slave_off[c + 1]; s += blockDim.x) {
-        const long long n = ca.slaves[s];
-        const double p[3] = {nd.pos[3 * n] + nd.u[3 * n], nd.pos[3 * n + 1] + nd.u[3 * n + 1], nd.pos[3 * n + 2] + nd.u[3 * n + 2]};
-        int best = -1;
-        double sd = 0.0;
-        for (int f = 0; f < nf; ++f)
-            if (face_hit(sgeo[f], p, md, &sd)) {
-                best = f;
-                break;
+    // BRUTE_LANES lanes per primary node, each scanning every BRUTE_LANES-th
+    // face in order up to its first hit; the smallest hit index wins.
+    const int lane = threadIdx.x % BRUTE_LANES;
+    const long long s_end = ca.slave_off[c + 1];
+    for (long long base = ca.slave_off[c]; base < s_end; base += blockDim.x / BRUTE_LANES) {  // block-uniform
+        const long long s = base + threadIdx.x / BRUTE_LANES;
+        const bool live = s < s_end;
+        long long n = 0;
+        int best = INT_MAX;
+        double best_sd = 0.0, sd;
+        if (live) {
+            n = ca.slaves[s];
+            const double p[3] = {nd.pos[3 * n] + nd.u[3 * n], nd.pos[3 * n + 1] + nd.u[3 * n + 1], nd.pos[3 * n + 2] + nd.u[3 * n + 2]};
+            for (int f = lane; f < nf; f += BRUTE_LANES)
+                if (face_hit(sgeo[f], p, md, &sd)) {
+                    best = f;
+                    best_sd = sd;
+                    break;
+                }
+        }
+#pragma unroll
+        for (int off = BRUTE_LANES / 2; off > 0; off >>= 1) {
+            const int ob = __shfl_down_sync(0xffffffffu, best, off, BRUTE_LANES);
+            const double osd = __shfl_down_sync(0xffffffffu, best_sd, off, BRUTE_LANES);
+            if (ob < best) {
+                best = ob;
+                best_sd = osd;
             }
-        if (best < 0) {
+        }
+        if (!live || lane != 0) continue;
+        if (best == INT_MAX) {
             ca.hit[s] = -1;
             continue;
         }
-        record_hit(ca, s, c, n, best, sd, dt_override > 0.0 ? dt_override : step_dt(ctl), masses, sgeo[best]);
+        record_hit(ca, s, c, n, best, best_sd, dt_override > 0.0 ? dt_override : step_dt(ctl), masses, sgeo[best]);
     }
 }
 
@@ -1479,6 +1500,8 @@ void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& n
     if (n_slaves > 0) {
         const unsigned g = active_grid(n_slaves, lanes, TPB, GRID_CAP);
         switch (lanes) {
+            case 1: k_contact_slaves<1><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses, n_slaves); break;
+            case 2: k_contact_slaves<2><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses, n_slaves); break;
             case 4: k_contact_slaves<4><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses, n_slaves); break;
             case 8: k_contact_slaves<8><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses, n_slaves); break;
             case 16: k_contact_slaves<16><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses, n_slaves); break;

@@ -160,7 +160,7 @@ class Context:
         return self._lib.crush_launch_count(self.h)
 
     def tuning(self):
-        """The autotuned launch schedule: (slave lanes, contact ms per lane option 4/8/16/32)."""
+        """The autotuned launch schedule: (slave lanes, contact ms per lane option 1/2/4/8/16/32)."""
         t = abi.Tuning()
         check(self._lib.crush_get_tuning(self.h, C.byref(t)))
         return t.slave_lanes, list(t.contact_ms)

@@ -259,13 +259,13 @@ int crush_set_contact_search(crush_ctx* ctx, int exhaustive);
 
 /* Launch schedule of a context, chosen by the engine's autotuner (no
  * counterpart in the reference). The first crush_run_begin of a context times
- * the run's contact pass with 4, 8, 16 and 32 lanes per primary-node search
+ * the run's contact pass with 1, 2, 4, 8, 16 and 32 lanes per primary-node search
  * on the context's own models and keeps the fastest; all choices find the
  * same hits. */
 typedef struct crush_tuning {
     int32_t slave_lanes;   /* lanes per primary-node search */
     int32_t reserved;
-    double contact_ms[4];  /* measured contact pass with 4, 8, 16, 32 lanes (0 = not measured) */
+    double contact_ms[6];  /* measured contact pass with 1, 2, 4, 8, 16, 32 lanes (0 = not measured) */
 } crush_tuning;
 /* Re-tune now, at the open run's current state (e.g. late in a crash, when
  * crushed faces change the search); the next step uses the new schedule. */
