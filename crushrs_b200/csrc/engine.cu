@@ -191,6 +191,8 @@ int stager_copy(Stager* st, void* dst, const void* src, size_t bytes) { return s
 struct crush_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;               // the contact search of the next step runs here, beside the forces
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::vector<void*> allocs;
     int64_t launches = 0;
 
@@ -296,6 +298,7 @@ struct crush_ctx {
         x.act_slave = active(3);
         x.act_cnode = active(4);
         x.act_dynf = active(5);
+        x.act_allslave = active(6);
         return x;
     }
     Active active(int space) const {
@@ -357,7 +360,11 @@ struct crush_ctx {
         if (graph) cudaGraphExecDestroy(graph);
         for (cudaEvent_t e : prof_ev) cudaEventDestroy(e);
         if (stream) cudaStreamSynchronize(stream);
+        if (side) cudaStreamSynchronize(side);
         for (void* p : allocs) cudaFree(p);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (side) cudaStreamDestroy(side);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -740,6 +747,13 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     c->device = device;
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    {
+        int lo = 0, hi = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        CK(cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, hi));  // search blocks first when SMs free up
+        CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+    }
     c->n_slots = n_desc;
     c->slots.resize(n_desc);
     // ---- sizes and offsets of every slot ----
@@ -1023,6 +1037,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->upload_const(&ca.slave_scale, scales));
     TRY(c->alloc(&ca.hit, std::max<long long>(c->n_slaves, 1)));
     TRY(c->alloc(&ca.hit_force, 3 * std::max<long long>(c->n_slaves, 1)));
+    TRY(c->alloc(&ca.hit_sd, std::max<long long>(c->n_slaves, 1)));
     TRY(c->upload_const(&ca.stiffness, stiff));
     TRY(c->upload_const(&ca.max_distance, md));
     TRY(c->upload_const(&ca.cell, cell));
@@ -1165,7 +1180,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     // ---- active chunk tables: slot range of every 256-entity chunk ----
     {
         const long long sizes[ACTIVE_SPACES] = {c->n_hc, E, N, (long long)c->grid_slaves_h.size(), (long long)cnode.size(),
-                                                (long long)dyn_faces.size()};
+                                                (long long)dyn_faces.size(), (long long)slaves.size()};
         c->space_off_h.assign(ACTIVE_SPACES + 1, 0);
         for (int sp = 0; sp < ACTIVE_SPACES; ++sp) c->space_off_h[sp + 1] = c->space_off_h[sp] + (sizes[sp] + CHUNK - 1) / CHUNK;
         const long long nch = c->space_off_h[ACTIVE_SPACES];
@@ -1177,7 +1192,8 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
                 case 2: return (int)cm.node_slot[i];
                 case 3: return contact_slot[slave_contact[c->grid_slaves_h[i]]];
                 case 4: return (int)cm.node_slot[cnode[i]];
-                default: return contact_slot[face_contact[dyn_faces[i]]];
+                case 5: return contact_slot[face_contact[dyn_faces[i]]];
+                default: return contact_slot[slave_contact[i]];
             }
         };
         parallel_for(nch, [&](long long q) {
@@ -1281,13 +1297,24 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
         n += 3;
     }
     mark(1);
+    // Contact forces of this step from the search run beside the previous
+    // step's forces (or at crush_run_begin for the first step).
     if (c->n_contacts > 0) {
-        launch_contact(c->stream, cr, nd, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 0.0, c->mass,
-                       c->f_ext, 1, c->slave_lanes);
-        n += contact_launches(c->ca, true, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 0);
+        launch_contact_finish(c->stream, cr, nd, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0.0, c->mass, c->f_ext, 1);
+        n += contact_finish_launches(c->n_slaves);
     }
     mark(2);
     launch_half(c->stream, nd, c->ctls);
+    // The next step's contact search needs only the new X + u: it runs on
+    // the side stream while this step's forces and update run.
+    if (c->n_contacts > 0) {
+        cudaEventRecord(c->ev_fork, c->stream);
+        cudaStreamWaitEvent(c->side, c->ev_fork, 0);
+        launch_contact_search(c->side, cr, nd, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 1,
+                              c->slave_lanes);
+        n += contact_search_launches(c->ca, true, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 0);
+        cudaEventRecord(c->ev_join, c->side);
+    }
     mark(3);
     launch_forces(c->stream, el, nd, c->ctls, 1);
     mark(4);
@@ -1305,11 +1332,22 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
     }
     launch_step_end(c->stream, c->ctls, cr, c->va, sep ? 1 : 0, c->slot_done);
     ++n;
+    if (c->n_contacts > 0) cudaStreamWaitEvent(c->stream, c->ev_join, 0);
     mark(6);
     return check_launch(c, n);
 }
 
 constexpr long long RETUNE_STEPS = 1000;
+
+// The contact search at the open run's current X + u, on the main stream:
+// what the next step's contact forces read (run begin, and after anything
+// that reused the search buffers).
+int search_now(crush_ctx* c) {
+    if (c->n_contacts == 0) return CRUSH_OK;
+    launch_contact_search(c->stream, c->ca, c->nd(), c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 1,
+                          c->slave_lanes);
+    return check_launch(c, contact_search_launches(c->ca, true, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 0));
+}
 
 // Launch autotuner: times the run's contact pass (at the open run's state,
 // output into scratch, no state change) with 1, 2, 4, 8, 16 and 32 lanes per
@@ -1420,6 +1458,8 @@ int run_begin(crush_ctx* c) {
         st = autotune(c);
         if (st != CRUSH_OK) return st;
     }
+    st = search_now(c);
+    if (st != CRUSH_OK) return st;
     return sync(c);
 }
 
@@ -1720,11 +1760,15 @@ int crush_contact_apply(crush_ctx* c, int id, const double* u, const double* v, 
                    c->slave_lanes);
     int st = check_launch(c, contact_launches(c->ca, false, nf, ns, bk0, bk1, id));
     if (st != CRUSH_OK) return st;
-    if (c->run_open && c->is_static_h[id]) {
-        // The call rebuilt the static faces' geometry at its own u: restore
-        // the open run's (static faces keep it for the whole run).
-        launch_contact_geometry(c->stream, c->ca, c->nd(), id, id + 1, c->face_off_h[id], nf);
-        st = check_launch(c);
+    if (c->run_open) {
+        // The call reused the run's contact buffers at its own u: restore the
+        // open run's static geometry and pending search.
+        if (c->is_static_h[id]) {
+            launch_contact_geometry(c->stream, c->ca, c->nd(), id, id + 1, c->face_off_h[id], nf);
+            st = check_launch(c);
+            if (st != CRUSH_OK) return st;
+        }
+        st = search_now(c);
         if (st != CRUSH_OK) return st;
     }
     std::vector<double> f(3 * c->n_nodes);

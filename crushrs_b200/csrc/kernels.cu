@@ -1091,7 +1091,8 @@ __device__ __forceinline__ void contact_slave_body(const ContactArrays& ca, cons
         ca.hit[s] = -1;
         return;
     }
-    record_hit(ca, s, c, n, best, best_sd, dt_override > 0.0 ? dt_override : step_dt(ctl), masses, geo[best]);
+    ca.hit[s] = best;
+    ca.hit_sd[s] = best_sd;
 }
 
 template <int LANES>
@@ -1165,7 +1166,31 @@ __global__ void __launch_bounds__(BRUTE_TPB) k_contact_brute(ContactArrays ca, N
             ca.hit[s] = -1;
             continue;
         }
-        record_hit(ca, s, c, n, best, best_sd, dt_override > 0.0 ? dt_override : step_dt(ctl), masses, sgeo[best]);
+        ca.hit[s] = best;
+        ca.hit_sd[s] = best_sd;
+    }
+}
+
+// The penalty forces of the hits the search found (src/contact.rs:130-153),
+// thread per primary-node entry: run the search finished before (possibly
+// overlapping other work); this pass needs the step's dt and records the
+// per-face hit lists and the penetration counters.
+__global__ void k_contact_force(ContactArrays ca, Control* ctls, int c0, int run_mode, double dt_override,
+                                const double* __restrict__ masses, long long n_slaves) {
+    const Active act = run_mode ? ca.act_allslave : Active{nullptr, nullptr};
+    const long long s0 = ca.slave_off[c0];
+    FOR_ACTIVE(act, n_slaves, 1, g) {
+        int lane;
+        const long long e = active_entity(act, g, 1, &lane);
+        if (e >= n_slaves) continue;
+        const long long s = s0 + e;
+        const int best = ca.hit[s];
+        if (best < 0) continue;
+        const int c = ca.slave_contact[s];
+        const Control* ctl = ctls + ca.contact_slot[c];
+        if (run_mode && ctl->done) continue;
+        record_hit(ca, s, c, ca.slaves[s], best, ca.hit_sd[s], dt_override > 0.0 ? dt_override : step_dt(ctl), masses,
+                   ca.geo[ca.face_off[c] + best]);
     }
 }
 
@@ -1465,12 +1490,10 @@ void launch_vehicle_vx(cudaStream_t s, const VehicleArrays& va, const double* ma
     k_vehicle_vx<<<(unsigned)(va.n_vehicles * va.vx_blocks), VEH_TPB, 0, s>>>(va, mass, v, ctls);
 }
 
-void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
-                    long long n_faces, long long n_slaves, long long bk0, long long bk1, double dt_override, const double* masses,
-                    double* f_out, int skip_fixed, int lanes) {
+void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
+                           long long n_faces, long long n_slaves, long long bk0, long long bk1, int run_mode, int lanes) {
+    (void)f0;
     if (c1 <= c0) return;
-    const int run_mode = dt_override > 0.0 ? 0 : 1;
-    if (n_faces > 0) cudaMemsetAsync(ca.face_hits + f0, 0, sizeof(int) * n_faces, s);
     // run: only moving faces (static ones keep their geometry); drop-in: every face of the range
     const uint32_t* list = run_mode ? ca.dyn_faces : nullptr;
     const long long n_list = run_mode ? ca.n_dyn_faces : n_faces;
@@ -1490,9 +1513,9 @@ void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& n
     if (!ca.exhaustive) {
         if (run_mode && ca.n_brute > 0)
             k_contact_brute<<<(unsigned)ca.n_brute, BRUTE_TPB, sizeof(FaceGeo) * ca.brute_max_faces, s>>>(ca, nd, ctls, ca.brute_contacts,
-                                                                                                          0, 1, dt_override, masses);
+                                                                                                          0, 1, 0.0, nullptr);
         if (!run_mode && c1 == c0 + 1 && ca.is_brute_h && ca.is_brute_h[c0]) {
-            k_contact_brute<<<1, BRUTE_TPB, sizeof(FaceGeo) * BRUTE_MAX_FACES, s>>>(ca, nd, ctls, nullptr, c0, 0, dt_override, masses);
+            k_contact_brute<<<1, BRUTE_TPB, sizeof(FaceGeo) * BRUTE_MAX_FACES, s>>>(ca, nd, ctls, nullptr, c0, 0, 0.0, nullptr);
             n_slaves = 0;
         }
         if (run_mode) n_slaves = ca.n_grid_slaves;
@@ -1500,14 +1523,24 @@ void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& n
     if (n_slaves > 0) {
         const unsigned g = active_grid(n_slaves, lanes, TPB, GRID_CAP);
         switch (lanes) {
-            case 1: k_contact_slaves<1><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses, n_slaves); break;
-            case 2: k_contact_slaves<2><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses, n_slaves); break;
-            case 4: k_contact_slaves<4><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses, n_slaves); break;
-            case 8: k_contact_slaves<8><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses, n_slaves); break;
-            case 16: k_contact_slaves<16><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses, n_slaves); break;
-            default: k_contact_slaves<32><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses, n_slaves); break;
+            case 1: k_contact_slaves<1><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, 0.0, nullptr, n_slaves); break;
+            case 2: k_contact_slaves<2><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, 0.0, nullptr, n_slaves); break;
+            case 4: k_contact_slaves<4><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, 0.0, nullptr, n_slaves); break;
+            case 8: k_contact_slaves<8><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, 0.0, nullptr, n_slaves); break;
+            case 16: k_contact_slaves<16><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, 0.0, nullptr, n_slaves); break;
+            default: k_contact_slaves<32><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, 0.0, nullptr, n_slaves); break;
         }
     }
+}
+
+void launch_contact_finish(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
+                           long long n_faces, long long n_slaves, double dt_override, const double* masses, double* f_out,
+                           int skip_fixed) {
+    if (c1 <= c0) return;
+    const int run_mode = dt_override > 0.0 ? 0 : 1;
+    if (n_faces > 0) cudaMemsetAsync(ca.face_hits + f0, 0, sizeof(int) * n_faces, s);
+    if (n_slaves > 0)
+        k_contact_force<<<active_grid(n_slaves, 1, TPB, GRID_CAP), TPB, 0, s>>>(ca, ctls, c0, run_mode, dt_override, masses, n_slaves);
     cudaMemsetAsync(ca.gather_count, 0, sizeof(int), s);
     long long nodes = ca.n_cnodes > 0 ? ca.n_cnodes : 1;
     k_contact_gather<<<active_grid(nodes, 1, GATHER_TPB, GRID_CAP * 2), GATHER_TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, f_out,
@@ -1516,9 +1549,16 @@ void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& n
     k_contact_gather_walk<<<(unsigned)(walk_blocks < WALK_BLOCKS ? walk_blocks : WALK_BLOCKS), GATHER_TPB, 0, s>>>(ca, c0, c1, f_out);
 }
 
-int contact_launches(const ContactArrays& ca, bool run_mode, long long n_faces, long long n_slaves, long long bk0, long long bk1,
-                     int c0) {
-    int k = 2;  // gather + overflow walk
+void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
+                    long long n_faces, long long n_slaves, long long bk0, long long bk1, double dt_override, const double* masses,
+                    double* f_out, int skip_fixed, int lanes) {
+    launch_contact_search(s, ca, nd, ctls, c0, c1, f0, n_faces, n_slaves, bk0, bk1, dt_override > 0.0 ? 0 : 1, lanes);
+    launch_contact_finish(s, ca, nd, ctls, c0, c1, f0, n_faces, n_slaves, dt_override, masses, f_out, skip_fixed);
+}
+
+int contact_search_launches(const ContactArrays& ca, bool run_mode, long long n_faces, long long n_slaves, long long bk0, long long bk1,
+                            int c0) {
+    int k = 0;
     if ((run_mode ? ca.n_dyn_faces : n_faces) > 0) ++k;
     if (bk1 > bk0 && !ca.exhaustive) k += (run_mode ? ca.n_grid_faces : n_faces) > 0 ? 3 : 1;
     if (!ca.exhaustive) {
@@ -1532,6 +1572,13 @@ int contact_launches(const ContactArrays& ca, bool run_mode, long long n_faces, 
     }
     if (n_slaves > 0) ++k;
     return k;
+}
+
+int contact_finish_launches(long long n_slaves) { return 2 + (n_slaves > 0 ? 1 : 0); }
+
+int contact_launches(const ContactArrays& ca, bool run_mode, long long n_faces, long long n_slaves, long long bk0, long long bk1,
+                     int c0) {
+    return contact_search_launches(ca, run_mode, n_faces, n_slaves, bk0, bk1, c0) + contact_finish_launches(n_slaves);
 }
 
 void launch_contact_geometry(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, int c0, int c1, long long f0,

@@ -83,7 +83,8 @@ struct ContactArrays {
     const int* slave_off;       // n_contacts+1
     const uint32_t* slaves;     // node id per primary node
     const double* slave_scale;
-    int* hit;                   // per primary node: local face index or -1
+    int* hit;                   // per primary node: local face index or -1 (written by the search)
+    double* hit_sd;             // per primary node: signed distance to that face
     double* hit_force;          // 3 per primary node
     const double* stiffness;    // per contact
     const double* max_distance; // per contact
@@ -138,6 +139,7 @@ struct ContactArrays {
     int* gather_work;           // contact nodes whose hit lists overflowed this pass (n_cnodes capacity)
     int* gather_count;          // their number
     Active act_slave, act_cnode, act_dynf;  // active chunks of grid-searched entries, contact nodes, moving faces
+    Active act_allslave;        // active chunks of all primary-node entries (the force pass)
     // Contacts without a grid are searched by one block each; the entries of
     // the others are listed for the lane-parallel search.
     const int* brute_contacts;
@@ -159,7 +161,8 @@ struct ActiveBuild {
     int* lists;                  // same layout as the chunks
     int* counts;                 // ACTIVE_SPACES
 };
-constexpr int ACTIVE_SPACES = 6;  // honeycomb elements, all elements, nodes, grid-searched entries, contact nodes, moving faces
+constexpr int ACTIVE_SPACES = 7;  // honeycomb elements, all elements, nodes, grid-searched entries, contact nodes, moving faces,
+                                  // all primary-node entries
 
 // Vehicles of all crash slots: node lists and the reduction layout.
 struct VehicleArrays {
@@ -202,6 +205,18 @@ void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& n
 // Kernel launches one launch_contact call issues.
 int contact_launches(const ContactArrays& ca, bool run_mode, long long n_faces, long long n_slaves, long long bk0, long long bk1,
                      int c0);
+// The two halves of a contact pass. The search (face geometry, grids, first
+// hits) needs only X + u and may run while other work of the step runs; the
+// finish (forces of the hits with the step's dt, hit lists, counters, the
+// ordered gather into f_out) follows it.
+void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
+                           long long n_faces, long long n_slaves, long long bk0, long long bk1, int run_mode, int lanes);
+void launch_contact_finish(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
+                           long long n_faces, long long n_slaves, double dt_override, const double* masses, double* f_out,
+                           int skip_fixed);
+int contact_search_launches(const ContactArrays& ca, bool run_mode, long long n_faces, long long n_slaves, long long bk0, long long bk1,
+                            int c0);
+int contact_finish_launches(long long n_slaves);
 // Geometry of every face of contacts [c0, c1) at X + u (no grid insertion):
 // the static contacts' geometry for a run.
 void launch_contact_geometry(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, int c0, int c1, long long f0,
