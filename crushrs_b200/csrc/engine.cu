@@ -516,9 +516,8 @@ struct ContactPart {
     std::vector<double> scales, box;  // box: 6 per contact (static key-box union, else everything)
     std::vector<uint32_t> st_off;  // per contact T+1 entries, slot-local into st_entries
     std::vector<int> st_entries;
-    std::vector<uint32_t> cnode, cnode_off{0}, crole_faces_off{0};
-    std::vector<int> crole_contact, crole_slave, crole_faces;
-    std::vector<uint8_t> crole_face;
+    std::vector<uint32_t> cnode, cnode_off{0};  // contact nodes (ascending node id) and their role ranges
+    std::vector<int> crole_contact, crole_slave;
     double contact_dt = INF;
 };
 
@@ -700,35 +699,20 @@ void build_contacts(const crush_model_desc* d, const Slot& sl, const Combined& c
         for (size_t a0 = i0; a0 < i1;) {
             size_t a1 = a0;
             while (a1 < i1 && items[a1].contact == items[a0].contact) ++a1;
-            // One role per primary-node entry (or one without), the faces on the last.
+            // One role per primary-node entry (or one without).
             int n_slave_roles = 0;
             for (size_t q = a0; q < a1; ++q) n_slave_roles += items[q].slave >= 0;
-            const int n_roles = std::max(n_slave_roles, 1);
             int made = 0;
             for (size_t q = a0; q < a1 && made < n_slave_roles; ++q)
                 if (items[q].slave >= 0) {
                     ++made;
                     cp.crole_contact.push_back(items[a0].contact);
                     cp.crole_slave.push_back(items[q].slave);
-                    if (made < n_roles) {
-                        cp.crole_face.push_back(0);
-                        cp.crole_faces_off.push_back((uint32_t)cp.crole_faces.size());
-                    }
                 }
             if (n_slave_roles == 0) {
                 cp.crole_contact.push_back(items[a0].contact);
                 cp.crole_slave.push_back(-1);
             }
-            int last = -1;
-            bool any_face = false;
-            for (size_t q = a0; q < a1; ++q)
-                if (items[q].face >= 0 && items[q].face != last) {
-                    cp.crole_faces.push_back(items[q].face);
-                    last = items[q].face;
-                    any_face = true;
-                }
-            cp.crole_face.push_back(any_face ? 1 : 0);
-            cp.crole_faces_off.push_back((uint32_t)cp.crole_faces.size());
             a0 = a1;
         }
         cp.cnode_off.push_back((uint32_t)cp.crole_contact.size());
@@ -943,23 +927,22 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     trace.mark("contacts built, masses");
     // Concatenation: per-slot bases, then every slot copies its part in parallel.
     struct Base {
-        long long face, slave, ste, stoff, dyn, grid, cnode, role, rface;
+        long long face, slave, ste, stoff, dyn, grid, cnode, role;
     };
     std::vector<Base> base(n_desc + 1);
-    base[0] = Base{0, 0, 0, 0, 0, 0, 0, 0, 0};
+    base[0] = Base{0, 0, 0, 0, 0, 0, 0, 0};
     for (int k = 0; k < n_desc; ++k) {
         const ContactPart& cp = parts[k];
         const Base& b0 = base[k];
         base[k + 1] = Base{b0.face + (long long)cp.faces.size() / 4, b0.slave + (long long)cp.slaves.size(),
                            b0.ste + (long long)cp.st_entries.size(), b0.stoff + (long long)cp.st_off.size(),
                            b0.dyn + (long long)cp.dyn_faces.size(), b0.grid + (long long)cp.grid_faces.size(),
-                           b0.cnode + (long long)cp.cnode.size(), b0.role + (long long)cp.crole_contact.size(),
-                           b0.rface + (long long)cp.crole_faces.size()};
+                           b0.cnode + (long long)cp.cnode.size(), b0.role + (long long)cp.crole_contact.size()};
         c->slots[k].contact_dt = cp.contact_dt;
     }
     const Base& tot = base[n_desc];
     const int kc = K;
-    if (tot.face >= (1ll << 31) || tot.slave >= (1ll << 31) || tot.ste >= (1ll << 32) || tot.role >= (1ll << 32) || tot.rface >= (1ll << 31))
+    if (tot.face >= (1ll << 31) || tot.slave >= (1ll << 31) || tot.ste >= (1ll << 32) || tot.role >= (1ll << 32))
         return crush::fail(CRUSH_ERR_INVALID, "contacts too large for one context");
     std::vector<int> face_off(kc + 1), slave_off(kc + 1), tab_off(kc + 1), counts_for_stop(kc), face_contact(tot.face),
         slave_contact(tot.slave), contact_slot(kc), slot_contact_off(n_desc + 1);
@@ -969,9 +952,10 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     std::vector<long long> st_tab_off(kc + 1);
     std::vector<uint32_t> st_off(tot.stoff);
     std::vector<int> st_entries(tot.ste);
-    std::vector<uint32_t> cnode(tot.cnode), cnode_off(tot.cnode + 1), crole_faces_off(tot.role + 1);
-    std::vector<int> crole_contact(tot.role), crole_slave(tot.role), crole_faces(tot.rface);
-    std::vector<uint8_t> crole_face(tot.role);
+    std::vector<uint32_t> cnode(tot.cnode), cnode_off(tot.cnode + 1);
+    std::vector<int> crole_contact(tot.role), crole_slave(tot.role);
+    // contact node of every primary-node entry and face corner (| CN_FIXED)
+    std::vector<uint32_t> slave_cn(tot.slave), face_cn(4 * tot.face);
     // per-contact prefix sums (serial, one entry per contact)
     face_off[0] = slave_off[0] = tab_off[0] = 0;
     st_tab_off[0] = 0;
@@ -993,7 +977,6 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     }
     slot_contact_off[n_desc] = kc;
     cnode_off[0] = 0;
-    crole_faces_off[0] = 0;
     parallel_for(n_desc, [&](long long k) {
         const ContactPart& cp = parts[k];
         const Base& b = base[k];
@@ -1014,9 +997,13 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
         for (size_t j = 1; j < cp.cnode_off.size(); ++j) cnode_off[b.cnode + j] = cp.cnode_off[j] + (uint32_t)b.role;
         std::copy(cp.crole_contact.begin(), cp.crole_contact.end(), crole_contact.begin() + b.role);
         std::copy(cp.crole_slave.begin(), cp.crole_slave.end(), crole_slave.begin() + b.role);
-        std::copy(cp.crole_face.begin(), cp.crole_face.end(), crole_face.begin() + b.role);
-        std::copy(cp.crole_faces.begin(), cp.crole_faces.end(), crole_faces.begin() + b.rface);
-        for (size_t j = 1; j < cp.crole_faces_off.size(); ++j) crole_faces_off[b.role + j] = cp.crole_faces_off[j] + (uint32_t)b.rface;
+        auto cn_of = [&](uint32_t node) {  // the slot's contact nodes are in ascending node order, and include it
+            const auto it = std::lower_bound(cp.cnode.begin(), cp.cnode.end(), node);
+            if (it == cp.cnode.end() || *it != node) std::abort();
+            return (uint32_t)(b.cnode + (it - cp.cnode.begin())) | (cm.fixed[node] ? CN_FIXED : 0u);
+        };
+        for (size_t j = 0; j < cp.slaves.size(); ++j) slave_cn[b.slave + j] = cn_of(cp.slaves[j]);
+        for (size_t j = 0; j < cp.faces.size(); ++j) face_cn[4 * b.face + j] = cn_of(cp.faces[j]);
     });
     parts.clear();
     parts.shrink_to_fit();
@@ -1081,19 +1068,18 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     }
     TRY(c->alloc(&ca.ent_cursor, std::max(kc, 1)));
     TRY(c->alloc(&ca.gather_work, std::max<size_t>(cnode.size(), 1)));
-    TRY(c->alloc(&ca.gather_count, 1));
+    TRY(c->alloc(&ca.gather_cnt, std::max<size_t>(cnode.size(), 1)));
+    TRY(c->alloc(&ca.ev_pool_n, 2));
+    ca.gather_count = ca.ev_pool_n + 1;
     ca.n_buckets = tab_off.back();
     ca.exhaustive = 0;
     c->tab_off_h = tab_off;
-    {
-        int cap = 1;
-        for (int k = 0; k < c->n_contacts; ++k)
-            if (tab_off[k + 1] > tab_off[k]) cap = std::max(cap, face_off[k + 1] - face_off[k]);
-        ca.overflow_cap = cap;  // overflow lists exist only for contacts with a dynamic grid
-    }
-    TRY(c->alloc(&ca.overflow, (size_t)std::max(c->n_contacts, 1) * ca.overflow_cap));
-    TRY(c->alloc(&ca.n_overflow, std::max(c->n_contacts, 1)));
-    TRY(c->alloc(&ca.entry_overrun, std::max(c->n_contacts, 1)));
+    // Big faces: at most every face of the contacts with a dynamic grid.
+    ca.big_cap = std::max<long long>(ca.n_grid_faces, 1);
+    TRY(c->alloc(&ca.big_faces, (size_t)ca.big_cap));
+    TRY(c->alloc(&ca.big_box, 6 * (size_t)ca.big_cap));
+    TRY(c->alloc(&ca.big_count, 1));
+    TRY(c->alloc(&ca.big_best, (size_t)std::max<long long>(c->n_slaves, 1)));
     TRY(c->alloc(&ca.levels_used, std::max(c->n_contacts, 1)));
     TRY(c->alloc(&ca.search_stats, 3 * (size_t)std::max(c->n_contacts, 1)));
     TRY(c->alloc(&ca.pen_count, std::max(c->n_contacts, 1)));
@@ -1104,12 +1090,14 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->upload_const(&ca.cnode_off, cnode_off));
     TRY(c->upload_const(&ca.crole_contact, crole_contact));
     TRY(c->upload_const(&ca.crole_slave, crole_slave));
-    TRY(c->upload_const(&ca.crole_face, crole_face));
-    TRY(c->upload_const(&ca.crole_faces_off, crole_faces_off));
-    TRY(c->upload_const(&ca.crole_faces, crole_faces));
-    TRY(c->alloc(&ca.face_hits, std::max<long long>(c->n_faces, 1)));
-    ca.hit_cap = c->n_faces <= (1ll << 20) ? 32 : 8;
-    TRY(c->alloc(&ca.face_list, (size_t)std::max<long long>(c->n_faces, 1) * ca.hit_cap));
+    if (tot.cnode >= (long long)CN_FIXED || c->n_slaves >= (1ll << 31))
+        return crush::fail(CRUSH_ERR_UNSUPPORTED, "over 2^31 contact nodes or primary-node entries in one context");
+    TRY(c->upload_const(&ca.slave_cn, slave_cn));
+    TRY(c->upload_const(&ca.face_cn, face_cn));
+    TRY(c->alloc(&ca.ev_count, std::max<size_t>(cnode.size(), 1)));
+    TRY(c->alloc(&ca.ev_list, EV_CAP * std::max<size_t>(cnode.size(), 1)));
+    ca.ev_pool_cap = std::max<long long>(4096, c->n_slaves);
+    TRY(c->alloc(&ca.ev_pool, (size_t)ca.ev_pool_cap));
     TRY(c->upload_const(&ca.face_contact, face_contact));
     TRY(c->upload_const(&ca.slave_contact, slave_contact));
     TRY(c->upload_const(&ca.contact_slot, contact_slot));
@@ -1122,15 +1110,16 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     ca.n_dyn_faces = (long long)dyn_faces.size();
     TRY(c->upload_const(&ca.dyn_faces, dyn_faces));
     CK(cudaMemsetAsync(ca.counts, 0, sizeof(int) * std::max(tab_off.back(), 1), c->stream));
-    CK(cudaMemsetAsync(ca.n_overflow, 0, sizeof(int) * std::max(c->n_contacts, 1), c->stream));
-    CK(cudaMemsetAsync(ca.entry_overrun, 0, sizeof(int) * std::max(c->n_contacts, 1), c->stream));
+    CK(cudaMemsetAsync(ca.big_count, 0, sizeof(int), c->stream));
+    CK(cudaMemsetAsync(ca.big_best, 0x7F, sizeof(int) * std::max<long long>(c->n_slaves, 1), c->stream));  // BIG_NONE
     CK(cudaMemsetAsync(ca.levels_used, 0, sizeof(int) * std::max(c->n_contacts, 1), c->stream));
     CK(cudaMemsetAsync(ca.ent_cursor, 0, sizeof(int) * std::max(c->n_contacts, 1), c->stream));
     CK(cudaMemsetAsync(ca.blen, 0, sizeof(int) * std::max(tab_off.back(), 1), c->stream));
     CK(cudaMemsetAsync(ca.search_stats, 0, sizeof(unsigned long long) * 3 * std::max(c->n_contacts, 1), c->stream));
     CK(cudaMemsetAsync(ca.pen_count, 0, sizeof(unsigned long long) * std::max(c->n_contacts, 1), c->stream));
     CK(cudaMemsetAsync(ca.pen_max_bits, 0, sizeof(unsigned long long) * std::max(c->n_contacts, 1), c->stream));
-    CK(cudaMemsetAsync(ca.face_hits, 0, sizeof(int) * std::max<long long>(c->n_faces, 1), c->stream));
+    CK(cudaMemsetAsync(ca.ev_count, 0, sizeof(int) * std::max<size_t>(cnode.size(), 1), c->stream));
+    CK(cudaMemsetAsync(ca.ev_pool_n, 0, 2 * sizeof(int), c->stream));
     trace.mark("contacts");
 
     // ---- vehicles ----
@@ -1411,6 +1400,10 @@ int run_begin(crush_ctx* c) {
     CK(cudaMemsetAsync(c->v_half, 0, sizeof(double) * 3 * N, c->stream));
     CK(cudaMemsetAsync(c->f_ext, 0, sizeof(double) * 3 * N, c->stream));
     CK(cudaMemsetAsync(c->added, 0, sizeof(double) * N, c->stream));
+    if (c->n_contacts > 0) {
+        CK(cudaMemsetAsync(c->ca.big_count, 0, sizeof(int), c->stream));
+        CK(cudaMemsetAsync(c->ca.big_best, 0x7F, sizeof(int) * std::max<long long>(c->n_slaves, 1), c->stream));  // BIG_NONE
+    }
     CK(cudaMemsetAsync(c->eroded_all, 0, c->n_all, c->stream));
     launch_init_state(c->stream, c->n_hc, c->stride, c->state);
     launch_node_masses(c->stream, N, c->all_off, c->all_slot, c->lumped, c->mass, c->inv_mass);

@@ -841,10 +841,9 @@ __device__ __forceinline__ void face_geometry(const ContactArrays& ca, const Nod
     }
 }
 
-// The grid level and cell range of face f's key box (from its geometry):
-// returns the level, GRID_LEVELS for the overflow list, -1 for no insertion.
-__device__ __forceinline__ int face_cells(const ContactArrays& ca, const FaceGeo& g, int c, long long* r) {
-    double klo[3], khi[3];
+// The grid level and cell range of face f's key box (from its geometry, into klo/khi):
+// returns the level, GRID_LEVELS for a big face, -1 for no insertion.
+__device__ __forceinline__ int face_cells(const ContactArrays& ca, const FaceGeo& g, int c, long long* r, double* klo, double* khi) {
     face_key_box(g.x, g.n, g.c, ca.max_distance[c], klo, khi);
     if (klo[0] > khi[0] || klo[1] > khi[1] || klo[2] > khi[2]) return -1;  // no point can hit the face
     double cs = ca.cell[c];
@@ -869,9 +868,9 @@ __device__ __forceinline__ void contact_face_body(const ContactArrays& ca, const
 
 // Warp per face of a contact with a dynamic grid: every lane derives the
 // face's grid level and key-box cells from its geometry, and the lanes split
-// the cells. Pass 0 counts the cells' inserts per bucket (or puts the face on
-// the overflow list); pass 1, after k_grid_alloc, fills the buckets, which
-// returns every count to zero.
+// the cells. Pass 0 counts the cells' inserts per bucket (or lists the face as
+// a big face with its key box); pass 1, after k_grid_alloc, fills the
+// buckets, which returns every count to zero.
 __global__ void k_contact_insert(ContactArrays ca, Control* ctls, int c0, const uint32_t* __restrict__ face_list, long long n,
                                  int run_mode, int pass) {
     const long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // warp-uniform
@@ -883,14 +882,22 @@ __global__ void k_contact_insert(ContactArrays ca, Control* ctls, int c0, const 
     if (ca.tab_off[c + 1] == tab || (run_mode && ctls[ca.contact_slot[c]].done)) return;
     const FaceGeo g = ca.geo[f];
     long long r[6];
-    const int level = face_cells(ca, g, c, r);
+    double klo[3], khi[3];
+    const int level = face_cells(ca, g, c, r, klo, khi);
     if (level < 0) return;
     const int local = (int)(f - ca.face_off[c]);
     if (level == GRID_LEVELS) {
         if (pass == 0 && lane == 0) {
-            int slot = atomicAdd(&ca.n_overflow[c], 1);
-            if (slot < ca.overflow_cap) ca.overflow[(long long)c * ca.overflow_cap + slot] = local;
-            else ca.entry_overrun[c] = 1;
+            // A face is listed at most once per search and the list holds
+            // every face of the grid contacts, so it cannot overrun.
+            const int slot = atomicAdd(ca.big_count, 1);
+            if (slot < ca.big_cap) {
+                ca.big_faces[slot] = (uint32_t)f;
+                for (int d = 0; d < 3; ++d) {
+                    ca.big_box[6 * (long long)slot + d] = klo[d];
+                    ca.big_box[6 * (long long)slot + 3 + d] = khi[d];
+                }
+            }
             atomicAdd(&ca.search_stats[3 * c + 1], 1ull);
         }
         return;
@@ -910,8 +917,20 @@ __global__ void k_contact_insert(ContactArrays ca, Control* ctls, int c0, const 
     }
 }
 
-__global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, const uint32_t* __restrict__ face_list,
+// Thread per face: its geometry. Pass 0 (a search) first clears the grid
+// bookkeeping of contacts [c0, c1) and the big-face list, so every search
+// starts from nothing whatever ran before it; pass 2 is geometry alone.
+__global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, int c1, const uint32_t* __restrict__ face_list,
                                 long long n, int run_mode, int pass, Active act) {
+    if (pass == 0) {
+        const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        const long long nthreads = (long long)gridDim.x * blockDim.x;
+        if (t == 0) *ca.big_count = 0;
+        for (long long c = c0 + t; c < c1; c += nthreads) {
+            ca.levels_used[c] = 0;
+            ca.ent_cursor[c] = 0;
+        }
+    }
     FOR_ACTIVE(act, n, 1, g) {
         int lane;
         contact_face_body(ca, nd, ctls, c0, face_list, n, run_mode, pass, active_entity(act, g, 1, &lane));
@@ -982,19 +1001,60 @@ __device__ __forceinline__ bool face_hit(const FaceGeo& g, const double* p, doub
     return inside;
 }
 
-// First-hit search: LANES lanes per primary node (a power of two <= 32,
-// chosen per context by the launch autotuner) test the faces its broad phase
-// offers — the static grid's bucket, or the dynamic grid's bucket at every
-// level in use plus the contact's overflow faces — or every face of the
-// contact when it has no grid (small contacts), its overflow list overran, or
-// this is a drop-in call on a static contact; and keep the smallest face
-// index that hits: the face the reference's in-order scan with `break` finds
-// (src/contact.rs:115-157).
+// Block per big face (blocks stride over the search's list): every primary
+// node of the face's contact inside the face's key box gets the narrow test,
+// and a hit lowers the node's big_best to the face's local index, so
+// big_best ends as the smallest big face that hits, whatever the order.
+constexpr int BIG_TPB = 128;
+constexpr int BIG_BLOCKS = 148 * 4;
+__global__ void __launch_bounds__(BIG_TPB) k_contact_big(ContactArrays ca, NodeArrays nd) {
+    __shared__ FaceGeo sg;
+    __shared__ double sbox[6];
+    const int count = min(*ca.big_count, (int)ca.big_cap);
+    for (int k = blockIdx.x; k < count; k += gridDim.x) {  // block-uniform
+        const long long f = ca.big_faces[k];
+        __syncthreads();  // the previous face's readers are done
+        if (threadIdx.x < sizeof(FaceGeo) / sizeof(double))
+            reinterpret_cast<double*>(&sg)[threadIdx.x] = reinterpret_cast<const double*>(ca.geo + f)[threadIdx.x];
+        if (threadIdx.x < 6) sbox[threadIdx.x] = ca.big_box[6 * (long long)k + threadIdx.x];
+        __syncthreads();
+        const int c = ca.face_contact[f];
+        const int local = (int)(f - ca.face_off[c]);
+        const double md = ca.max_distance[c];
+        const long long s1 = ca.slave_off[c + 1];
+        for (long long s = ca.slave_off[c] + threadIdx.x; s < s1; s += BIG_TPB) {
+            const long long n = ca.slaves[s];
+            const double p[3] = {nd.pos[3 * n] + nd.u[3 * n], nd.pos[3 * n + 1] + nd.u[3 * n + 1], nd.pos[3 * n + 2] + nd.u[3 * n + 2]};
+            if (!(p[0] >= sbox[0] && p[0] <= sbox[3] && p[1] >= sbox[1] && p[1] <= sbox[4] && p[2] >= sbox[2] && p[2] <= sbox[5])) continue;
+            double sd;
+            if (face_hit(sg, p, md, &sd)) atomicMin(&ca.big_best[s], local);
+        }
+    }
+}
+
+// One reaction event of a hit: key 2s (the primary node's own +F) or 2s+1
+// (-F/4 on a node of the hit face) appended to the contact node's list, or
+// to the shared pool once the list holds EV_CAP; fixed nodes take none when
+// the pass skips them.
+__device__ __forceinline__ void emit_event(const ContactArrays& ca, uint32_t code, uint32_t key, int skip_fixed) {
+    if (skip_fixed && (code & CN_FIXED)) return;
+    const uint32_t cn = code & ~CN_FIXED;
+    const int slot = atomicAdd(&ca.ev_count[cn], 1);
+    if (slot < EV_CAP) {
+        ca.ev_list[(long long)cn * EV_CAP + slot] = key;
+    } else {
+        const int p = atomicAdd(ca.ev_pool_n, 1);
+        if (p < ca.ev_pool_cap) ca.ev_pool[p] = make_uint2(cn, key);
+    }
+}
+
 // The penalty force of primary-node entry s (node n of contact c) on its
 // first-hit face `best` (src/contact.rs:130-153: depth capped at 0.1 md,
-// stiffness limited to 0.1 m / dt^2, force capped at m * 1e5).
+// stiffness limited to 0.1 m / dt^2, force capped at m * 1e5), and its five
+// reaction events: +F on the node, -F/4 on each of the face's four corners
+// (a node on two corners takes two).
 __device__ __forceinline__ void record_hit(const ContactArrays& ca, long long s, int c, long long n, int best, double best_sd, double dt,
-                                           const double* __restrict__ masses, const FaceGeo& g) {
+                                           const double* __restrict__ masses, const FaceGeo& g, int skip_fixed) {
     const double md = ca.max_distance[c];
     const double m = masses[n];
     const double depth = fmin(-best_sd, 0.1 * md);
@@ -1005,19 +1065,33 @@ __device__ __forceinline__ void record_hit(const ContactArrays& ca, long long s,
     ca.hit_force[3 * s + 1] = mag * g.n[1];
     ca.hit_force[3 * s + 2] = mag * g.n[2];
     const long long F = ca.face_off[c] + best;
-    const int slot = atomicAdd(&ca.face_hits[F], 1);
-    if (slot < ca.hit_cap) ca.face_list[F * ca.hit_cap + slot] = (int)s;
+    const uint32_t key = 2u * (uint32_t)s;
+    emit_event(ca, ca.slave_cn[s], key, skip_fixed);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) emit_event(ca, ca.face_cn[4 * F + j], key + 1u, skip_fixed);
     atomicAdd(&ca.pen_count[c], 1ull);
     atomicMax(&ca.pen_max_bits[c], (unsigned long long)__double_as_longlong(-best_sd));
 }
 
+// First-hit search: LANES lanes per primary node (a power of two <= 32,
+// chosen per context by the launch autotuner) test the faces its broad phase
+// offers — the static grid's bucket, or the dynamic grid's bucket at every
+// level in use, starting from the smallest big face that hit — or every face
+// of the contact when it has no grid (small contacts), or this is a drop-in
+// call on a static contact; and keep the smallest face index that hits: the
+// face the reference's in-order scan with `break` finds
+// (src/contact.rs:115-157). Lane 0 sets the node's big_best back to
+// BIG_NONE for the next search, also when its crash has stopped.
 template <int LANES>
 __device__ __forceinline__ void contact_slave_body(const ContactArrays& ca, const NodeArrays& nd, const Control* ctls, int c0, int c1,
                                                    int run_mode, double dt_override, const double* __restrict__ masses, long long s,
                                                    bool live, int lane) {
     const Control* ctl = nullptr;
+    bool reset_big = false;
     if (live) {
-        ctl = ctls + ca.contact_slot[ca.slave_contact[s]];
+        const int c = ca.slave_contact[s];
+        reset_big = lane == 0 && ca.tab_off[c + 1] > ca.tab_off[c] && !ca.exhaustive;
+        ctl = ctls + ca.contact_slot[c];
         if (run_mode && ctl->done) live = false;
     }
     int best = INT_MAX;
@@ -1053,7 +1127,12 @@ __device__ __forceinline__ void contact_slave_body(const ContactArrays& ca, cons
                 const int f = ca.st_entries[k];
                 if (f < best && face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; }
             }
-        } else if (dyn_grid && !ca.exhaustive && !ca.entry_overrun[c]) {
+        } else if (dyn_grid && !ca.exhaustive) {
+            const int big = ca.big_best[s];
+            if (big != BIG_NONE && face_hit(geo[big], p, md, &sd)) {  // always hits: the big-face pass's own test
+                best = big;
+                best_sd = sd;
+            }
             const unsigned mask = (unsigned)(ca.tab_off[c + 1] - tab - 1);
             const int used = ca.levels_used[c];
             double cs = ca.cell[c];
@@ -1067,14 +1146,8 @@ __device__ __forceinline__ void contact_slave_body(const ContactArrays& ca, cons
                     if (f < best && face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; }
                 }
             }
-            const int no = min(ca.n_overflow[c], ca.overflow_cap);
-            for (int k = lane; k < no; k += LANES) {
-                const int f = ca.overflow[(long long)c * ca.overflow_cap + k];
-                if (f < best && face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; }
-            }
         } else {
             all = true;
-            if (dyn_grid && !ca.exhaustive && lane == 0) atomicAdd(&ca.search_stats[3 * c], 1ull);
         }
         if (all)
             for (int f = lane; f < nf; f += LANES)
@@ -1086,6 +1159,7 @@ __device__ __forceinline__ void contact_slave_body(const ContactArrays& ca, cons
         const double osd = __shfl_down_sync(0xffffffffu, best_sd, off, LANES);
         if (ob < best) { best = ob; best_sd = osd; }
     }
+    if (reset_big) ca.big_best[s] = BIG_NONE;
     if (!live || lane != 0) return;
     if (best == INT_MAX) {
         ca.hit[s] = -1;
@@ -1174,9 +1248,9 @@ __global__ void __launch_bounds__(BRUTE_TPB) k_contact_brute(ContactArrays ca, N
 // The penalty forces of the hits the search found (src/contact.rs:130-153),
 // thread per primary-node entry: run the search finished before (possibly
 // overlapping other work); this pass needs the step's dt and records the
-// per-face hit lists and the penetration counters.
+// reaction events and the penetration counters.
 __global__ void k_contact_force(ContactArrays ca, Control* ctls, int c0, int run_mode, double dt_override,
-                                const double* __restrict__ masses, long long n_slaves) {
+                                const double* __restrict__ masses, long long n_slaves, int skip_fixed) {
     const Active act = run_mode ? ca.act_allslave : Active{nullptr, nullptr};
     const long long s0 = ca.slave_off[c0];
     FOR_ACTIVE(act, n_slaves, 1, g) {
@@ -1190,72 +1264,111 @@ __global__ void k_contact_force(ContactArrays ca, Control* ctls, int c0, int run
         const Control* ctl = ctls + ca.contact_slot[c];
         if (run_mode && ctl->done) continue;
         record_hit(ca, s, c, ca.slaves[s], best, ca.hit_sd[s], dt_override > 0.0 ? dt_override : step_dt(ctl), masses,
-                   ca.geo[ca.face_off[c] + best]);
+                   ca.geo[ca.face_off[c] + best], skip_fixed);
     }
 }
 
-constexpr int MAX_NODE_EVENTS = 64;
 constexpr int GATHER_TPB = 128;
-constexpr int WALK_BLOCKS = 296;  // 2 x 148 SMs of 4 warps
+constexpr int HEAVY_TPB = 256;
+constexpr int HEAVY_KEYS = 2048;     // events a block sorts itself
+constexpr int WALK_PER_THREAD = 4;   // consecutive primary nodes per thread in a walk round
+constexpr int HEAVY_BLOCKS = 296;    // 2 x 148 SMs
+// keys of one walk round: up to 5 per entry (own + four corners)
+constexpr int HEAVY_BUF = HEAVY_TPB * WALK_PER_THREAD * 5 > HEAVY_KEYS ? HEAVY_TPB * WALK_PER_THREAD * 5 : HEAVY_KEYS;
 
-// Lane 0's part of one role of contact node n (contact c, own primary-node
-// entry `own` or -1): collect its own hit (+F) and the hits on the faces it
-// belongs to (-F/4), sort them by primary-node order (own before face for the
-// same primary node) and add them in that order to (sx, sy, sz) — the
-// sequence in which src/contact.rs:146-153 adds them to f_ext. Returns false,
-// adding nothing, when the per-face hit lists overflowed.
-__device__ __forceinline__ bool role_sum(const ContactArrays& ca, uint32_t r, int c, int own, double& sx, double& sy, double& sz) {
-    const long long sb = ca.slave_off[c];
-    unsigned long long ev[MAX_NODE_EVENTS];
-    int ne = 0;
-    if (own >= 0 && ca.hit[sb + own] >= 0) ev[ne++] = 2ull * (unsigned long long)(sb + own);
-    for (uint32_t q = ca.crole_faces_off[r]; q < ca.crole_faces_off[r + 1]; ++q) {
-        const long long f = ca.face_off[c] + ca.crole_faces[q];
-        const int cnt = ca.face_hits[f];
-        if (cnt > ca.hit_cap || ne + cnt > MAX_NODE_EVENTS) return false;
-        for (int k = 0; k < cnt; ++k) ev[ne++] = 2ull * (unsigned long long)ca.face_list[f * ca.hit_cap + k] + 1ull;
+// Adds one event to (sx, sy, sz) the way src/contact.rs:146-153 adds it to
+// f_ext: += F for the primary node itself, -= 0.25 F for a face corner.
+__device__ __forceinline__ void apply_event(bool face, double fx, double fy, double fz, double& sx, double& sy, double& sz) {
+    if (face) {
+        sx -= 0.25 * fx;
+        sy -= 0.25 * fy;
+        sz -= 0.25 * fz;
+    } else {
+        sx += fx;
+        sy += fy;
+        sz += fz;
     }
-    for (int a = 1; a < ne; ++a) {  // insertion sort, tiny lists
-        unsigned long long key = ev[a];
-        int b = a - 1;
-        while (b >= 0 && ev[b] > key) { ev[b + 1] = ev[b]; --b; }
-        ev[b + 1] = key;
-    }
-    for (int a = 0; a < ne; ++a) {
-        const long long s = (long long)(ev[a] >> 1);
-        const double fx = ca.hit_force[3 * s], fy = ca.hit_force[3 * s + 1], fz = ca.hit_force[3 * s + 2];
-        if (ev[a] & 1ull) { sx -= 0.25 * fx; sy -= 0.25 * fy; sz -= 0.25 * fz; }
-        else { sx += fx; sy += fy; sz += fz; }
-    }
-    return true;
 }
 
-// Ordered reaction gather, one thread per contact node, over its contacts in
-// order. A node whose per-face hit lists overflowed is handed to
-// k_contact_gather_walk instead (its output is written there). Then the grid
-// bookkeeping is cleared for the next build.
+// Ordered reaction gather, one thread per contact node. The node's events
+// carry keys 2s (own) and 2s+1 (face) of the global primary-node index s;
+// contacts are numbered in order and so are their entries, so ascending keys
+// are the order in which src/contact.rs:146-153 adds the reactions to f_ext,
+// contact after contact. Up to EV_CAP keys are sorted in registers (a
+// bitonic network) and their forces loaded together; a node with more goes
+// to k_contact_gather_heavy, which writes its output. The gather zeroes the
+// node's event count for the next pass.
 __device__ __forceinline__ void gather_body(const ContactArrays& ca, const NodeArrays& nd, const Control* ctls, int c0, int c1,
                                             int run_mode, double* __restrict__ f_out, int skip_fixed, long long i) {
-    if (i < ca.n_cnodes) {
-        const long long n = ca.cnode[i];
-        if (!(skip_fixed && nd.fixed[n]) && !(run_mode && ctls[nd.node_slot[n]].done)) {
-            double sx = 0.0, sy = 0.0, sz = 0.0;
-            bool touched = false, ok = true;
-            for (uint32_t r = ca.cnode_off[i]; r < ca.cnode_off[i + 1] && ok; ++r) {
-                const int c = ca.crole_contact[r];
-                if (c < c0 || c >= c1) continue;
-                touched = true;
-                ok = role_sum(ca, r, c, ca.crole_slave[r], sx, sy, sz);
-            }
-            if (!ok) {
-                ca.gather_work[atomicAdd(ca.gather_count, 1)] = (int)i;
-            } else if (touched) {
-                f_out[3 * n] = sx;
-                f_out[3 * n + 1] = sy;
-                f_out[3 * n + 2] = sz;
+    if (i >= ca.n_cnodes) return;
+    const long long n = ca.cnode[i];
+    if ((skip_fixed && nd.fixed[n]) || (run_mode && ctls[nd.node_slot[n]].done)) return;
+    if (!run_mode) {  // a drop-in call writes the nodes with a role in contacts [c0, c1)
+        bool touched = false;
+        for (uint32_t r = ca.cnode_off[i]; r < ca.cnode_off[i + 1]; ++r) {
+            const int c = ca.crole_contact[r];
+            touched |= c >= c0 && c < c1;
+        }
+        if (!touched) return;
+    }
+    const int cnt = ca.ev_count[i];
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    if (cnt > 0) {
+        ca.ev_count[i] = 0;
+        if (cnt > EV_CAP) {
+            const int w = atomicAdd(ca.gather_count, 1);
+            ca.gather_work[w] = (int)i;
+            ca.gather_cnt[w] = cnt;
+            return;
+        }
+        uint32_t k[EV_CAP];
+        const uint4* row = reinterpret_cast<const uint4*>(ca.ev_list + i * EV_CAP);
+#pragma unroll
+        for (int q = 0; q < EV_CAP / 4; ++q) {
+            const uint4 v = row[q];
+            k[4 * q] = v.x;
+            k[4 * q + 1] = v.y;
+            k[4 * q + 2] = v.z;
+            k[4 * q + 3] = v.w;
+        }
+#pragma unroll
+        for (int j = 0; j < EV_CAP; ++j)
+            if (j >= cnt) k[j] = 0xFFFFFFFFu;
+#pragma unroll
+        for (int size = 2; size <= EV_CAP; size <<= 1)
+#pragma unroll
+            for (int stride = size >> 1; stride > 0; stride >>= 1)
+#pragma unroll
+                for (int a = 0; a < EV_CAP; ++a) {
+                    const int b = a ^ stride;
+                    if (b > a) {
+                        const uint32_t lo = min(k[a], k[b]), hi = max(k[a], k[b]);
+                        const bool up = (a & size) == 0;
+                        k[a] = up ? lo : hi;
+                        k[b] = up ? hi : lo;
+                    }
+                }
+#pragma unroll
+        for (int g = 0; g < EV_CAP; g += 8) {
+            if (g < cnt) {
+                double fx[8], fy[8], fz[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const long long e = (long long)(k[g + j] >> 1);
+                    const bool ok = g + j < cnt;
+                    fx[j] = ok ? __ldg(ca.hit_force + 3 * e) : 0.0;
+                    fy[j] = ok ? __ldg(ca.hit_force + 3 * e + 1) : 0.0;
+                    fz[j] = ok ? __ldg(ca.hit_force + 3 * e + 2) : 0.0;
+                }
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    if (g + j < cnt) apply_event(k[g + j] & 1u, fx[j], fy[j], fz[j], sx, sy, sz);
             }
         }
     }
+    f_out[3 * n] = sx;
+    f_out[3 * n + 1] = sy;
+    f_out[3 * n + 2] = sz;
 }
 
 __global__ void __launch_bounds__(GATHER_TPB) k_contact_gather(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, int c1,
@@ -1265,78 +1378,154 @@ __global__ void __launch_bounds__(GATHER_TPB) k_contact_gather(ContactArrays ca,
         int lane;
         gather_body(ca, nd, ctls, c0, c1, run_mode, f_out, skip_fixed, active_entity(act, g, 1, &lane));
     }
-    // Clear the grid bookkeeping for the next build.
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long nthreads = (long long)gridDim.x * blockDim.x;
-    for (long long c = c0 + t; c < c1; c += nthreads) {
-        ca.n_overflow[c] = 0;
-        ca.entry_overrun[c] = 0;
-        ca.levels_used[c] = 0;
-        ca.ent_cursor[c] = 0;
+}
+
+// Thread 0 adds, in order, the events listed in keys[0, count) (ascending),
+// their forces fetched HEAVY_TPB at a time by the whole block.
+__device__ void heavy_sum(const ContactArrays& ca, const uint32_t* keys, int count, double (*sf)[3], double& sx, double& sy, double& sz) {
+    for (int b0 = 0; b0 < count; b0 += HEAVY_TPB) {  // block-uniform
+        const int t = b0 + threadIdx.x;
+        if (t < count) {
+            const long long e = (long long)(keys[t] >> 1);
+            sf[threadIdx.x][0] = ca.hit_force[3 * e];
+            sf[threadIdx.x][1] = ca.hit_force[3 * e + 1];
+            sf[threadIdx.x][2] = ca.hit_force[3 * e + 2];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int m = min(HEAVY_TPB, count - b0);
+            for (int j = 0; j < m; ++j) apply_event(keys[b0 + j] & 1u, sf[j][0], sf[j][1], sf[j][2], sx, sy, sz);
+        }
+        __syncthreads();
     }
 }
 
-// The contact nodes whose hit lists overflowed, one warp per node (warps
-// stride over the list): lane 0 sums the roles whose lists fit; for a role
-// whose lists overflowed the warp walks the contact's primary nodes in order,
-// 32 per round, and every lane applies the round's matches in lane order, so
-// all lanes hold lane 0's running sum.
-__global__ void __launch_bounds__(GATHER_TPB) k_contact_gather_walk(ContactArrays ca, int c0, int c1, double* __restrict__ f_out) {
-    const int lane = threadIdx.x & 31;
-    const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
-    const int count = *ca.gather_count;
-    for (long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < count; w += warps) {
-        const long long i = ca.gather_work[w];
-        const long long n = ca.cnode[i];
-        double sx = 0.0, sy = 0.0, sz = 0.0;  // lane 0's sum
-        for (uint32_t r = ca.cnode_off[i]; r < ca.cnode_off[i + 1]; ++r) {
-            const int c = ca.crole_contact[r];
-            if (c < c0 || c >= c1) continue;
-            const long long sb = ca.slave_off[c];
-            const int own = ca.crole_slave[r];
-            int ok = 1;
-            if (lane == 0) ok = role_sum(ca, r, c, own, sx, sy, sz) ? 1 : 0;
-            ok = __shfl_sync(0xffffffffu, ok, 0);
-            if (ok) continue;
-            double wx = __shfl_sync(0xffffffffu, sx, 0), wy = __shfl_sync(0xffffffffu, sy, 0), wz = __shfl_sync(0xffffffffu, sz, 0);
-            const long long se = ca.slave_off[c + 1];
-            const uint32_t* faces = ca.faces + 4 * ca.face_off[c];
-            for (long long s0 = sb; s0 < se; s0 += 32) {
-                const long long s = s0 + lane;
-                int kind = 0;  // bit 0: own hit, bit 1: hit on a face containing n
-                double fx = 0.0, fy = 0.0, fz = 0.0;
+// The events of contact node i (node n) rebuilt without its lists: the block
+// walks, contact after contact (its roles are grouped by contact, in order),
+// the contact's primary nodes in rounds of HEAVY_TPB x WALK_PER_THREAD
+// consecutive entries; per entry an own hit (one of the node's entries in
+// the contact) gives key 2s and each corner of the hit face that is n gives
+// 2s+1. A block scan places the round's keys in entry order (already
+// ascending) and heavy_sum adds them.
+__device__ void walk_node(const ContactArrays& ca, int c0, int c1, long long i, long long n, uint32_t* keys, double (*sf)[3],
+                          int* s_warp, double& sx, double& sy, double& sz) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t r_end = ca.cnode_off[i + 1];
+    for (uint32_t r = ca.cnode_off[i], r1; r < r_end; r = r1) {
+        const int c = ca.crole_contact[r];
+        r1 = r + 1;
+        while (r1 < r_end && ca.crole_contact[r1] == c) ++r1;
+        if (c < c0 || c >= c1) continue;
+        if (threadIdx.x == 0) atomicAdd(&ca.search_stats[3 * c + 2], 1ull);
+        const long long sb = ca.slave_off[c], se = ca.slave_off[c + 1];
+        const uint32_t* faces = ca.faces + 4 * ca.face_off[c];
+        for (long long base = sb; base < se; base += HEAVY_TPB * WALK_PER_THREAD) {  // block-uniform
+            int own_j[WALK_PER_THREAD], m_j[WALK_PER_THREAD];
+            int mine = 0;
+#pragma unroll
+            for (int j = 0; j < WALK_PER_THREAD; ++j) {
+                const long long s = base + threadIdx.x * WALK_PER_THREAD + j;
+                own_j[j] = 0;
+                m_j[j] = 0;
                 if (s < se) {
                     const int h = ca.hit[s];
                     if (h >= 0) {
                         const uint32_t* qn = faces + 4 * (long long)h;
-                        kind = (s - sb == own ? 1 : 0) | ((qn[0] == n || qn[1] == n || qn[2] == n || qn[3] == n) ? 2 : 0);
-                        if (kind) {
-                            fx = ca.hit_force[3 * s];
-                            fy = ca.hit_force[3 * s + 1];
-                            fz = ca.hit_force[3 * s + 2];
-                        }
+                        for (uint32_t q = r; q < r1; ++q) own_j[j] |= ca.crole_slave[q] == s - sb ? 1 : 0;
+                        m_j[j] = (qn[0] == n ? 1 : 0) + (qn[1] == n ? 1 : 0) + (qn[2] == n ? 1 : 0) + (qn[3] == n ? 1 : 0);
                     }
                 }
-                unsigned m = __ballot_sync(0xffffffffu, kind != 0);
-                while (m) {
-                    const int l = __ffs(m) - 1;
-                    m &= m - 1;
-                    const int k = __shfl_sync(0xffffffffu, kind, l);
-                    const double gx = __shfl_sync(0xffffffffu, fx, l), gy = __shfl_sync(0xffffffffu, fy, l),
-                                 gz = __shfl_sync(0xffffffffu, fz, l);
-                    if (k & 1) { wx += gx; wy += gy; wz += gz; }
-                    if (k & 2) { wx -= 0.25 * gx; wy -= 0.25 * gy; wz -= 0.25 * gz; }
+                mine += own_j[j] + m_j[j];
+            }
+            int incl = mine;  // block exclusive scan of the keys per thread
+            for (int off = 1; off < 32; off <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, off);
+                if (lane >= off) incl += y;
+            }
+            if (lane == 31) s_warp[warp] = incl;
+            __syncthreads();
+            int before = 0, total = 0;
+            for (int k = 0; k < HEAVY_TPB / 32; ++k) {
+                const int v = s_warp[k];
+                before += k < warp ? v : 0;
+                total += v;
+            }
+            int pos = before + incl - mine;
+#pragma unroll
+            for (int j = 0; j < WALK_PER_THREAD; ++j) {
+                const uint32_t key = 2u * (uint32_t)(base + threadIdx.x * WALK_PER_THREAD + j);
+                if (own_j[j]) keys[pos++] = key;
+                for (int a = 0; a < m_j[j]; ++a) keys[pos++] = key + 1u;
+            }
+            __syncthreads();
+            heavy_sum(ca, keys, total, sf, sx, sy, sz);  // ends with a barrier: keys and s_warp are free again
+        }
+    }
+}
+
+// Contact nodes with more than EV_CAP events, a block each (blocks stride
+// over the list): the node's list and its events in the shared pool are
+// collected (EV_CAP + pool = the count when nothing was dropped), sorted by a
+// bitonic sort in shared memory and added in order. A node whose events do
+// not fit HEAVY_KEYS, or lost some to a full pool, is rebuilt by walk_node.
+__global__ void __launch_bounds__(HEAVY_TPB) k_contact_gather_heavy(ContactArrays ca, int c0, int c1, double* __restrict__ f_out) {
+    __shared__ uint32_t keys[HEAVY_BUF];
+    __shared__ double sf[HEAVY_TPB][3];
+    __shared__ int s_warp[HEAVY_TPB / 32];
+    __shared__ int s_n;
+    const int count = *ca.gather_count;
+    for (int w = blockIdx.x; w < count; w += gridDim.x) {  // block-uniform
+        const long long i = ca.gather_work[w];
+        const int cnt = ca.gather_cnt[w];
+        const long long n = ca.cnode[i];
+        double sx = 0.0, sy = 0.0, sz = 0.0;  // thread 0's running sum
+        bool walk = cnt > HEAVY_KEYS;
+        if (!walk) {
+            if (threadIdx.x == 0) s_n = 0;
+            __syncthreads();
+            for (int t = threadIdx.x; t < EV_CAP; t += HEAVY_TPB) keys[t] = ca.ev_list[i * EV_CAP + t];
+            const int np = (int)min((long long)*ca.ev_pool_n, ca.ev_pool_cap);
+            for (int p = threadIdx.x; p < np; p += HEAVY_TPB) {
+                const uint2 e = ca.ev_pool[p];
+                if (e.x == (uint32_t)i) {
+                    const int q = EV_CAP + atomicAdd(&s_n, 1);
+                    if (q < HEAVY_KEYS) keys[q] = e.y;
                 }
             }
-            sx = wx;
-            sy = wy;
-            sz = wz;
+            __syncthreads();
+            walk = EV_CAP + s_n != cnt;  // block-uniform
         }
-        if (lane == 0) {
+        if (walk) {
+            __syncthreads();
+            walk_node(ca, c0, c1, i, n, keys, sf, s_warp, sx, sy, sz);
+        } else {
+            int P = EV_CAP;
+            while (P < cnt) P <<= 1;
+            for (int t = cnt + threadIdx.x; t < P; t += HEAVY_TPB) keys[t] = 0xFFFFFFFFu;
+            __syncthreads();
+            for (int size = 2; size <= P; size <<= 1)
+                for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                    for (int a = threadIdx.x; a < P; a += HEAVY_TPB) {
+                        const int b = a ^ stride;
+                        if (b > a) {
+                            const uint32_t x = keys[a], y = keys[b];
+                            const bool up = (a & size) == 0;
+                            if ((x > y) == up) {
+                                keys[a] = y;
+                                keys[b] = x;
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
+            heavy_sum(ca, keys, cnt, sf, sx, sy, sz);
+        }
+        if (threadIdx.x == 0) {
             f_out[3 * n] = sx;
             f_out[3 * n + 1] = sy;
             f_out[3 * n + 2] = sz;
         }
+        __syncthreads();
     }
 }
 
@@ -1498,7 +1687,7 @@ void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeAr
     const uint32_t* list = run_mode ? ca.dyn_faces : nullptr;
     const long long n_list = run_mode ? ca.n_dyn_faces : n_faces;
     if (n_list > 0)
-        k_contact_faces<<<active_grid(n_list, 1, TPB, GRID_CAP), TPB, 0, s>>>(ca, nd, ctls, c0, list, n_list, run_mode, 0,
+        k_contact_faces<<<active_grid(n_list, 1, TPB, GRID_CAP), TPB, 0, s>>>(ca, nd, ctls, c0, c1, list, n_list, run_mode, 0,
                                                                             run_mode ? ca.act_dynf : Active{nullptr, nullptr});
     if (bk1 > bk0 && !ca.exhaustive) {
         const uint32_t* glist = run_mode ? ca.grid_faces : nullptr;
@@ -1506,8 +1695,10 @@ void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeAr
         if (n_glist > 0)
             k_contact_insert<<<(unsigned)blocks_for(n_glist * 32, TPB), TPB, 0, s>>>(ca, ctls, c0, glist, n_glist, run_mode, 0);
         k_grid_alloc<<<(unsigned)blocks_for(bk1 - bk0, TPB), TPB, 0, s>>>(ca, c0, c1);
-        if (n_glist > 0)
+        if (n_glist > 0) {
             k_contact_insert<<<(unsigned)blocks_for(n_glist * 32, TPB), TPB, 0, s>>>(ca, ctls, c0, glist, n_glist, run_mode, 1);
+            k_contact_big<<<(unsigned)(n_glist < BIG_BLOCKS ? n_glist : BIG_BLOCKS), BIG_TPB, 0, s>>>(ca, nd);
+        }
     }
     // Exhaustive contacts: a block each (run: the listed ones; drop-in: the one contact if it is one).
     if (!ca.exhaustive) {
@@ -1538,15 +1729,16 @@ void launch_contact_finish(cudaStream_t s, const ContactArrays& ca, const NodeAr
                            int skip_fixed) {
     if (c1 <= c0) return;
     const int run_mode = dt_override > 0.0 ? 0 : 1;
-    if (n_faces > 0) cudaMemsetAsync(ca.face_hits + f0, 0, sizeof(int) * n_faces, s);
+    (void)f0;
+    (void)n_faces;
+    cudaMemsetAsync(ca.ev_pool_n, 0, 2 * sizeof(int), s);  // pool entries and heavy nodes (gather_count)
     if (n_slaves > 0)
-        k_contact_force<<<active_grid(n_slaves, 1, TPB, GRID_CAP), TPB, 0, s>>>(ca, ctls, c0, run_mode, dt_override, masses, n_slaves);
-    cudaMemsetAsync(ca.gather_count, 0, sizeof(int), s);
+        k_contact_force<<<active_grid(n_slaves, 1, TPB, GRID_CAP), TPB, 0, s>>>(ca, ctls, c0, run_mode, dt_override, masses, n_slaves,
+                                                                               skip_fixed);
     long long nodes = ca.n_cnodes > 0 ? ca.n_cnodes : 1;
     k_contact_gather<<<active_grid(nodes, 1, GATHER_TPB, GRID_CAP * 2), GATHER_TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, f_out,
                                                                                           skip_fixed);
-    const long long walk_blocks = blocks_for(nodes * 32, GATHER_TPB);
-    k_contact_gather_walk<<<(unsigned)(walk_blocks < WALK_BLOCKS ? walk_blocks : WALK_BLOCKS), GATHER_TPB, 0, s>>>(ca, c0, c1, f_out);
+    k_contact_gather_heavy<<<(unsigned)(nodes < HEAVY_BLOCKS ? nodes : HEAVY_BLOCKS), HEAVY_TPB, 0, s>>>(ca, c0, c1, f_out);
 }
 
 void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
@@ -1560,7 +1752,7 @@ int contact_search_launches(const ContactArrays& ca, bool run_mode, long long n_
                             int c0) {
     int k = 0;
     if ((run_mode ? ca.n_dyn_faces : n_faces) > 0) ++k;
-    if (bk1 > bk0 && !ca.exhaustive) k += (run_mode ? ca.n_grid_faces : n_faces) > 0 ? 3 : 1;
+    if (bk1 > bk0 && !ca.exhaustive) k += (run_mode ? ca.n_grid_faces : n_faces) > 0 ? 4 : 1;
     if (!ca.exhaustive) {
         if (run_mode) {
             k += ca.n_brute > 0 ? 1 : 0;
@@ -1585,7 +1777,7 @@ void launch_contact_geometry(cudaStream_t s, const ContactArrays& ca, const Node
                              long long n_faces) {
     (void)f0;
     if (c1 <= c0 || n_faces <= 0) return;
-    k_contact_faces<<<active_grid(n_faces, 1, TPB, GRID_CAP), TPB, 0, s>>>(ca, nd, nullptr, c0, nullptr, n_faces, 0, 2,
+    k_contact_faces<<<active_grid(n_faces, 1, TPB, GRID_CAP), TPB, 0, s>>>(ca, nd, nullptr, c0, c1, nullptr, n_faces, 0, 2,
                                                                          Active{nullptr, nullptr});
 }
 

@@ -63,17 +63,22 @@ struct FaceGeo {
     double hi[3];
 };
 
-// Per-face hit lists hold hit_cap primary nodes (32, or 8 for contexts with
-// over a million faces; fuller lists make the gather walk the contact's
-// primary nodes in order).
+// Reaction events per contact node: EV_CAP keys in the node's own list, the
+// rest in a shared pool; CN_FIXED marks a fixed node in slave_cn / face_cn.
+constexpr int EV_CAP = 16;
+constexpr uint32_t CN_FIXED = 0x80000000u;
 // Dynamic grids are hashed and hierarchical: level l has cells of size
 // cell * 4^l, and a face goes into the finest level where its key box covers
-// at most LEVEL_CELL_BUDGET cells (beyond the last level, or not finite: the
-// overflow list). Buckets are exact CSR ranges rebuilt every step (count,
-// allocate, fill), so a contact needs at most faces x LEVEL_CELL_BUDGET
-// entries and no bucket ever overflows.
-constexpr int GRID_LEVELS = 6;
+// at most LEVEL_CELL_BUDGET cells. Buckets are exact CSR ranges rebuilt every
+// step (count, allocate, fill), so a contact needs at most faces x
+// LEVEL_CELL_BUDGET entries and no bucket ever overflows. A face whose key
+// box fits no level (a stretched face: one of its nodes flew off with
+// eroded elements) is a big face: one pass per big face tests it against
+// every primary node of its contact, and the primary-node search starts
+// from the smallest big face that hit (big_best).
+constexpr int GRID_LEVELS = 2;
 constexpr int LEVEL_CELL_BUDGET = 64;
+constexpr int BIG_NONE = 0x7F7F7F7F;  // big_best of a primary node no big face hit (memset byte 0x7F)
 
 struct ContactArrays {
     int n_contacts;
@@ -96,28 +101,31 @@ struct ContactArrays {
     const long long* ent_off;   // n_contacts+1: entry capacity ranges (faces x LEVEL_CELL_BUDGET)
     int* ent_cursor;            // per contact: entries allocated this step
     int* entries;               // local face indices
-    int* overflow;              // per contact: faces whose key box spans too many cells
-    int* n_overflow;            // per contact
-    int* entry_overrun;         // per contact flag: overflow list full (search every face)
-    unsigned long long* search_stats;  // 3 per contact, accumulated: primary-node searches that tested
-                                       // every face of a contact with a grid (overflow list overrun),
-                                       // faces put on the overflow list, (unused: 0)
-    int overflow_cap;           // per contact capacity of overflow
+    uint32_t* big_faces;        // this search's big faces (global index), capacity big_cap
+    double* big_box;            // 6 per big face: its key box (lo xyz, hi xyz)
+    int* big_count;             // big faces listed this search (cleared by the gather)
+    long long big_cap;          // faces of the contacts with a dynamic grid
+    int* big_best;              // per primary node: smallest local big face that hit, or BIG_NONE
+    unsigned long long* search_stats;  // 3 per contact, accumulated: (unused: 0), big faces
+                                       // searched face by face, contact-node roles gathered by
+                                       // walking the primary nodes (per-face hit lists overflowed)
     unsigned long long* pen_count;  // per contact, per step
     unsigned long long* pen_max_bits;
     const int* counts_for_stop; // per contact: faces not all fixed
-    // contact-node gather: nodes with roles in contacts
+    // contact-node gather: nodes with roles in contacts, and the reaction
+    // events the force pass appends to per-node lists
     long long n_cnodes;
     const uint32_t* cnode;      // node id
-    const uint32_t* cnode_off;  // n_cnodes+1
+    const uint32_t* cnode_off;  // n_cnodes+1: range of the node's roles
     const int* crole_contact;   // per role: contact id
     const int* crole_slave;     // per role: position among the contact's primary nodes (-1 none)
-    const uint8_t* crole_face;  // per role: node belongs to a face of the contact
-    const uint32_t* crole_faces_off;  // per role + 1: range in crole_faces
-    const int* crole_faces;     // local indices of the contact's faces that contain the node
-    int* face_hits;             // per face: primary nodes hitting it this step
-    int* face_list;             // hit_cap primary nodes (global index) per face
-    int hit_cap;
+    const uint32_t* slave_cn;   // per primary-node entry: contact node of its node (| CN_FIXED if fixed)
+    const uint32_t* face_cn;    // 4 per face: contact node of each corner (| CN_FIXED if fixed)
+    int* ev_count;              // per contact node: events this pass (zeroed again by the gather)
+    uint32_t* ev_list;          // EV_CAP event keys per contact node
+    uint2* ev_pool;             // (contact node, key) of the events past a full list
+    int* ev_pool_n;             // [0] pool entries, [1] heavy contact nodes (= gather_count)
+    long long ev_pool_cap;
     const int* face_contact;    // contact of each face
     const int* slave_contact;   // contact of each primary node entry
     const int* contact_slot;    // crash slot of each contact
@@ -136,8 +144,9 @@ struct ContactArrays {
     long long n_grid_faces;
     long long n_buckets;        // total dynamic buckets (tab_off[n_contacts])
     int exhaustive;             // 1: every search tests every face of its contact (no broad phase)
-    int* gather_work;           // contact nodes whose hit lists overflowed this pass (n_cnodes capacity)
-    int* gather_count;          // their number
+    int* gather_work;           // contact nodes with over EV_CAP events this pass (n_cnodes capacity)
+    int* gather_cnt;            // their event counts
+    int* gather_count;          // their number (ev_pool_n + 1)
     Active act_slave, act_cnode, act_dynf;  // active chunks of grid-searched entries, contact nodes, moving faces
     Active act_allslave;        // active chunks of all primary-node entries (the force pass)
     // Contacts without a grid are searched by one block each; the entries of

@@ -176,7 +176,7 @@ class Context:
         check(self._lib.crush_set_contact_search(self.h, int(bool(exhaustive))))
 
     def contact_search_stats(self, contact_id, reset=False):
-        """(exhaustive fallback searches, overflow faces, reserved) of a contact."""
+        """(exhaustive fallback searches, overflow faces, walked gather roles) of a contact."""
         out = (C.c_uint64 * 3)()
         check(self._lib.crush_contact_search_stats(self.h, contact_id, out, int(reset)))
         return tuple(out)

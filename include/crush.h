@@ -248,8 +248,9 @@ int64_t crush_launch_count(const crush_ctx* ctx);
  * (or the last reset): out[0] primary-node searches of a contact with a grid
  * that tested every face (its overflow list overran), out[1] faces put on the
  * overflow list (key box not finite or beyond the coarsest grid level),
- * out[2] reserved (0). No counterpart in the reference (whose search is
- * exhaustive). reset != 0 zeroes them after reading. */
+ * out[2] contact-node roles whose reaction sum walked the contact's primary
+ * nodes (a per-face hit list overflowed). No counterpart in the reference
+ * (whose search is exhaustive). reset != 0 zeroes them after reading. */
 int crush_contact_search_stats(crush_ctx* ctx, int contact_id, uint64_t* out, int reset);
 /* exhaustive = 1 makes every contact search test every face of its contact,
  * as the reference does (src/contact.rs:115); 0 (default) uses the grids.
