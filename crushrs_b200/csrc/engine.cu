@@ -1066,7 +1066,11 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
         ca.is_brute_h = c->is_brute_h.data();
         c->grid_slaves_h = std::move(gslaves);
     }
-    TRY(c->alloc(&ca.ent_cursor, std::max(kc, 1)));
+    TRY(c->alloc(&ca.grid_state, 2 * (size_t)std::max(kc, 1) + 1));
+    ca.levels_used = ca.grid_state;
+    ca.ent_cursor = ca.grid_state + kc;
+    ca.big_count = ca.grid_state + 2 * kc;
+    TRY(c->alloc(&ca.cells, (size_t)std::max<long long>(c->n_faces, 1)));
     TRY(c->alloc(&ca.gather_work, std::max<size_t>(cnode.size(), 1)));
     TRY(c->alloc(&ca.gather_cnt, std::max<size_t>(cnode.size(), 1)));
     TRY(c->alloc(&ca.ev_pool_n, 2));
@@ -1078,9 +1082,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     ca.big_cap = std::max<long long>(ca.n_grid_faces, 1);
     TRY(c->alloc(&ca.big_faces, (size_t)ca.big_cap));
     TRY(c->alloc(&ca.big_box, 6 * (size_t)ca.big_cap));
-    TRY(c->alloc(&ca.big_count, 1));
     TRY(c->alloc(&ca.big_best, (size_t)std::max<long long>(c->n_slaves, 1)));
-    TRY(c->alloc(&ca.levels_used, std::max(c->n_contacts, 1)));
     TRY(c->alloc(&ca.search_stats, 3 * (size_t)std::max(c->n_contacts, 1)));
     TRY(c->alloc(&ca.pen_count, std::max(c->n_contacts, 1)));
     TRY(c->alloc(&ca.pen_max_bits, std::max(c->n_contacts, 1)));
@@ -1110,10 +1112,8 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     ca.n_dyn_faces = (long long)dyn_faces.size();
     TRY(c->upload_const(&ca.dyn_faces, dyn_faces));
     CK(cudaMemsetAsync(ca.counts, 0, sizeof(int) * std::max(tab_off.back(), 1), c->stream));
-    CK(cudaMemsetAsync(ca.big_count, 0, sizeof(int), c->stream));
     CK(cudaMemsetAsync(ca.big_best, 0x7F, sizeof(int) * std::max<long long>(c->n_slaves, 1), c->stream));  // BIG_NONE
-    CK(cudaMemsetAsync(ca.levels_used, 0, sizeof(int) * std::max(c->n_contacts, 1), c->stream));
-    CK(cudaMemsetAsync(ca.ent_cursor, 0, sizeof(int) * std::max(c->n_contacts, 1), c->stream));
+    CK(cudaMemsetAsync(ca.grid_state, 0, sizeof(int) * (2 * (size_t)std::max(kc, 1) + 1), c->stream));
     CK(cudaMemsetAsync(ca.blen, 0, sizeof(int) * std::max(tab_off.back(), 1), c->stream));
     CK(cudaMemsetAsync(ca.search_stats, 0, sizeof(unsigned long long) * 3 * std::max(c->n_contacts, 1), c->stream));
     CK(cudaMemsetAsync(ca.pen_count, 0, sizeof(unsigned long long) * std::max(c->n_contacts, 1), c->stream));
@@ -1401,7 +1401,6 @@ int run_begin(crush_ctx* c) {
     CK(cudaMemsetAsync(c->f_ext, 0, sizeof(double) * 3 * N, c->stream));
     CK(cudaMemsetAsync(c->added, 0, sizeof(double) * N, c->stream));
     if (c->n_contacts > 0) {
-        CK(cudaMemsetAsync(c->ca.big_count, 0, sizeof(int), c->stream));
         CK(cudaMemsetAsync(c->ca.big_best, 0x7F, sizeof(int) * std::max<long long>(c->n_slaves, 1), c->stream));  // BIG_NONE
     }
     CK(cudaMemsetAsync(c->eroded_all, 0, c->n_all, c->stream));

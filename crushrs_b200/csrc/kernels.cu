@@ -28,6 +28,7 @@ namespace crush {
 namespace {
 
 constexpr int TPB = 256;
+constexpr int FACE_TPB = 64;  // small blocks for the face pass: a few thousand latency-bound faces spread over more SMs
 
 __host__ __device__ inline long long blocks_for(long long n, int tpb) { return (n + tpb - 1) / tpb; }
 
@@ -855,85 +856,98 @@ __device__ __forceinline__ int face_cells(const ContactArrays& ca, const FaceGeo
 // Thread per face: the face's geometry at X + u. The faces are
 // face_list[0, n) when face_list is given (the run: moving faces only), else
 // face_off[c0] + [0, n).
+// Thread per face: its geometry at X + u, and — when the search builds the
+// dynamic grids (do_grid) and the face's contact has one — its key box's
+// grid level and cells, stored for the fill pass, with one count per cell
+// added to the cell's bucket; a face whose box fits no level is listed as a
+// big face with its key box. Every face of a grid contact that the pass
+// visits gets its cell record (level -1: no inserts), so the fill pass, over
+// the same faces, inserts exactly what was counted.
 __device__ __forceinline__ void contact_face_body(const ContactArrays& ca, const NodeArrays& nd, const Control* ctls, int c0,
-                                                  const uint32_t* __restrict__ face_list, long long n, int run_mode, int pass, long long t) {
-    if (t >= n) return;
-    const long long f = face_list ? (long long)face_list[t] : ca.face_off[c0] + t;
-    const int c = ca.face_contact[f];
-    if (run_mode && ctls[ca.contact_slot[c]].done) return;
-    FaceGeo g;
-    face_geometry(ca, nd, f, ca.max_distance[c], g);
-    ca.geo[f] = g;
-}
-
-// Warp per face of a contact with a dynamic grid: every lane derives the
-// face's grid level and key-box cells from its geometry, and the lanes split
-// the cells. Pass 0 counts the cells' inserts per bucket (or lists the face as
-// a big face with its key box); pass 1, after k_grid_alloc, fills the
-// buckets, which returns every count to zero.
-__global__ void k_contact_insert(ContactArrays ca, Control* ctls, int c0, const uint32_t* __restrict__ face_list, long long n,
-                                 int run_mode, int pass) {
-    const long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // warp-uniform
-    const int lane = threadIdx.x & 31;
+                                                  const uint32_t* __restrict__ face_list, long long n, int run_mode, int do_grid,
+                                                  long long t) {
     if (t >= n) return;
     const long long f = face_list ? (long long)face_list[t] : ca.face_off[c0] + t;
     const int c = ca.face_contact[f];
     const int tab = ca.tab_off[c];
-    if (ca.tab_off[c + 1] == tab || (run_mode && ctls[ca.contact_slot[c]].done)) return;
-    const FaceGeo g = ca.geo[f];
+    const bool grid = do_grid && ca.tab_off[c + 1] > tab;
+    if (run_mode && ctls[ca.contact_slot[c]].done) {
+        if (grid) ca.cells[f].level = -1;
+        return;
+    }
+    FaceGeo g;
+    face_geometry(ca, nd, f, ca.max_distance[c], g);
+    ca.geo[f] = g;
+    if (!grid) return;
     long long r[6];
     double klo[3], khi[3];
     const int level = face_cells(ca, g, c, r, klo, khi);
-    if (level < 0) return;
-    const int local = (int)(f - ca.face_off[c]);
+    FaceCells fc;
+    fc.level = level;
+    fc.lo[0] = r[0];
+    fc.lo[1] = r[2];
+    fc.lo[2] = r[4];
+    fc.span[0] = fc.span[1] = fc.span[2] = 0;
     if (level == GRID_LEVELS) {
-        if (pass == 0 && lane == 0) {
-            // A face is listed at most once per search and the list holds
-            // every face of the grid contacts, so it cannot overrun.
-            const int slot = atomicAdd(ca.big_count, 1);
-            if (slot < ca.big_cap) {
-                ca.big_faces[slot] = (uint32_t)f;
-                for (int d = 0; d < 3; ++d) {
-                    ca.big_box[6 * (long long)slot + d] = klo[d];
-                    ca.big_box[6 * (long long)slot + 3 + d] = khi[d];
-                }
+        // A face is listed at most once per search and the list holds every
+        // face of the grid contacts, so it cannot overrun.
+        const int slot = atomicAdd(ca.big_count, 1);
+        if (slot < ca.big_cap) {
+            ca.big_faces[slot] = (uint32_t)f;
+            for (int d = 0; d < 3; ++d) {
+                ca.big_box[6 * (long long)slot + d] = klo[d];
+                ca.big_box[6 * (long long)slot + 3 + d] = khi[d];
             }
-            atomicAdd(&ca.search_stats[3 * c + 1], 1ull);
         }
-        return;
+        atomicAdd(&ca.search_stats[3 * c + 1], 1ull);
+    } else if (level >= 0) {
+        if (!(ca.levels_used[c] & (1 << level))) atomicOr(&ca.levels_used[c], 1 << level);
+        const unsigned mask = (unsigned)(ca.tab_off[c + 1] - tab - 1);
+        const int ni = (int)(r[1] - r[0] + 1), nj = (int)(r[3] - r[2] + 1), nk = (int)(r[5] - r[4] + 1);
+        fc.span[0] = ni;
+        fc.span[1] = nj;
+        fc.span[2] = nk;
+        for (int kk = 0; kk < nk; ++kk)
+            for (int jj = 0; jj < nj; ++jj)
+                for (int ii = 0; ii < ni; ++ii)
+                    atomicAdd(&ca.counts[tab + (int)(cell_hash(r[0] + ii, r[2] + jj, r[4] + kk, level) & mask)], 1);
     }
-    if (pass == 0 && lane == 0 && !(ca.levels_used[c] & (1 << level))) atomicOr(&ca.levels_used[c], 1 << level);
-    const unsigned mask = (unsigned)(ca.tab_off[c + 1] - tab - 1);
-    const int ni = (int)(r[1] - r[0] + 1), nj = (int)(r[3] - r[2] + 1), nk = (int)(r[5] - r[4] + 1);
-    for (int q = lane; q < ni * nj * nk; q += 32) {
-        const long long i = r[0] + q % ni, j = r[2] + (q / ni) % nj, k = r[4] + q / (ni * nj);
-        const int b = tab + (int)(cell_hash(i, j, k, level) & mask);
-        if (pass == 0) {
-            atomicAdd(&ca.counts[b], 1);
-        } else {
+    ca.cells[f] = fc;
+}
+
+// Fill pass, warp per face over the faces the geometry pass visited (same
+// list, same active chunks): the lanes split the face's stored cells and
+// place the face in each cell's bucket range from k_grid_alloc, which
+// returns every count to zero.
+__global__ void k_contact_insert(ContactArrays ca, int c0, const uint32_t* __restrict__ face_list, long long n, Active act) {
+    FOR_ACTIVE(act, n, 32, g) {
+        int lane;
+        const long long t = active_entity(act, g, 32, &lane);  // warp-uniform
+        if (t >= n) continue;
+        const long long f = face_list ? (long long)face_list[t] : ca.face_off[c0] + t;
+        const int c = ca.face_contact[f];
+        const int tab = ca.tab_off[c];
+        if (ca.tab_off[c + 1] == tab) continue;
+        const FaceCells fc = ca.cells[f];
+        if (fc.level < 0 || fc.level >= GRID_LEVELS) continue;
+        const int local = (int)(f - ca.face_off[c]);
+        const unsigned mask = (unsigned)(ca.tab_off[c + 1] - tab - 1);
+        const int ni = fc.span[0], nj = fc.span[1], nk = fc.span[2];
+        for (int q = lane; q < ni * nj * nk; q += 32) {
+            const long long i = fc.lo[0] + q % ni, j = fc.lo[1] + (q / ni) % nj, k = fc.lo[2] + q / (ni * nj);
+            const int b = tab + (int)(cell_hash(i, j, k, fc.level) & mask);
             const int pos = atomicSub(&ca.counts[b], 1) - 1;
             ca.entries[ca.boff[b] + pos] = local;
         }
     }
 }
 
-// Thread per face: its geometry. Pass 0 (a search) first clears the grid
-// bookkeeping of contacts [c0, c1) and the big-face list, so every search
-// starts from nothing whatever ran before it; pass 2 is geometry alone.
-__global__ void k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, int c1, const uint32_t* __restrict__ face_list,
-                                long long n, int run_mode, int pass, Active act) {
-    if (pass == 0) {
-        const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-        const long long nthreads = (long long)gridDim.x * blockDim.x;
-        if (t == 0) *ca.big_count = 0;
-        for (long long c = c0 + t; c < c1; c += nthreads) {
-            ca.levels_used[c] = 0;
-            ca.ent_cursor[c] = 0;
-        }
-    }
+__global__ void __launch_bounds__(FACE_TPB) k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctls, int c0,
+                                                            const uint32_t* __restrict__ face_list, long long n, int run_mode, int do_grid,
+                                                            Active act) {
     FOR_ACTIVE(act, n, 1, g) {
         int lane;
-        contact_face_body(ca, nd, ctls, c0, face_list, n, run_mode, pass, active_entity(act, g, 1, &lane));
+        contact_face_body(ca, nd, ctls, c0, face_list, n, run_mode, do_grid, active_entity(act, g, 1, &lane));
     }
 }
 
@@ -1686,18 +1700,19 @@ void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeAr
     // run: only moving faces (static ones keep their geometry); drop-in: every face of the range
     const uint32_t* list = run_mode ? ca.dyn_faces : nullptr;
     const long long n_list = run_mode ? ca.n_dyn_faces : n_faces;
+    const Active act = run_mode ? ca.act_dynf : Active{nullptr, nullptr};
+    const int do_grid = bk1 > bk0 && !ca.exhaustive ? 1 : 0;
+    // Every search starts from clear grid bookkeeping (levels in use, entry
+    // cursors, big-face list), whatever ran before it.
+    cudaMemsetAsync(ca.grid_state, 0, sizeof(int) * (2 * (size_t)ca.n_contacts + 1), s);
     if (n_list > 0)
-        k_contact_faces<<<active_grid(n_list, 1, TPB, GRID_CAP), TPB, 0, s>>>(ca, nd, ctls, c0, c1, list, n_list, run_mode, 0,
-                                                                            run_mode ? ca.act_dynf : Active{nullptr, nullptr});
-    if (bk1 > bk0 && !ca.exhaustive) {
-        const uint32_t* glist = run_mode ? ca.grid_faces : nullptr;
-        const long long n_glist = run_mode ? ca.n_grid_faces : n_faces;
-        if (n_glist > 0)
-            k_contact_insert<<<(unsigned)blocks_for(n_glist * 32, TPB), TPB, 0, s>>>(ca, ctls, c0, glist, n_glist, run_mode, 0);
+        k_contact_faces<<<active_grid(n_list, 1, FACE_TPB, GRID_CAP), FACE_TPB, 0, s>>>(ca, nd, ctls, c0, list, n_list, run_mode, do_grid,
+                                                                                      act);
+    if (do_grid) {
         k_grid_alloc<<<(unsigned)blocks_for(bk1 - bk0, TPB), TPB, 0, s>>>(ca, c0, c1);
-        if (n_glist > 0) {
-            k_contact_insert<<<(unsigned)blocks_for(n_glist * 32, TPB), TPB, 0, s>>>(ca, ctls, c0, glist, n_glist, run_mode, 1);
-            k_contact_big<<<(unsigned)(n_glist < BIG_BLOCKS ? n_glist : BIG_BLOCKS), BIG_TPB, 0, s>>>(ca, nd);
+        if (n_list > 0) {
+            k_contact_insert<<<active_grid(n_list, 32, TPB, GRID_CAP), TPB, 0, s>>>(ca, c0, list, n_list, act);
+            k_contact_big<<<(unsigned)(n_list < BIG_BLOCKS ? n_list : BIG_BLOCKS), BIG_TPB, 0, s>>>(ca, nd);
         }
     }
     // Exhaustive contacts: a block each (run: the listed ones; drop-in: the one contact if it is one).
@@ -1751,8 +1766,9 @@ void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& n
 int contact_search_launches(const ContactArrays& ca, bool run_mode, long long n_faces, long long n_slaves, long long bk0, long long bk1,
                             int c0) {
     int k = 0;
-    if ((run_mode ? ca.n_dyn_faces : n_faces) > 0) ++k;
-    if (bk1 > bk0 && !ca.exhaustive) k += (run_mode ? ca.n_grid_faces : n_faces) > 0 ? 4 : 1;
+    const bool faces = (run_mode ? ca.n_dyn_faces : n_faces) > 0;
+    if (faces) ++k;
+    if (bk1 > bk0 && !ca.exhaustive) k += faces ? 3 : 1;
     if (!ca.exhaustive) {
         if (run_mode) {
             k += ca.n_brute > 0 ? 1 : 0;
@@ -1777,8 +1793,9 @@ void launch_contact_geometry(cudaStream_t s, const ContactArrays& ca, const Node
                              long long n_faces) {
     (void)f0;
     if (c1 <= c0 || n_faces <= 0) return;
-    k_contact_faces<<<active_grid(n_faces, 1, TPB, GRID_CAP), TPB, 0, s>>>(ca, nd, nullptr, c0, c1, nullptr, n_faces, 0, 2,
-                                                                         Active{nullptr, nullptr});
+    (void)c1;
+    k_contact_faces<<<active_grid(n_faces, 1, FACE_TPB, GRID_CAP), FACE_TPB, 0, s>>>(ca, nd, nullptr, c0, nullptr, n_faces, 0, 0,
+                                                                                   Active{nullptr, nullptr});
 }
 
 }  // namespace crush

@@ -54,6 +54,14 @@ struct NodeArrays {
     Active act_node;            // active chunks of nodes
 };
 
+// A face's key-box cells at its grid level (level -1: no inserts,
+// GRID_LEVELS: a big face), written by the face pass for the fill pass.
+struct FaceCells {
+    long long lo[3];
+    int span[3];
+    int level;
+};
+
 // Contact runtime arrays (all contacts concatenated).
 struct FaceGeo {
     double x[4][3];
@@ -100,10 +108,12 @@ struct ContactArrays {
     int* blen;                  // per bucket: length of its range
     const long long* ent_off;   // n_contacts+1: entry capacity ranges (faces x LEVEL_CELL_BUDGET)
     int* ent_cursor;            // per contact: entries allocated this step
+    int* grid_state;            // levels_used (n_contacts), ent_cursor (n_contacts), big_count (1): cleared per search
+    FaceCells* cells;           // per face: its cells this search (faces of contacts with a dynamic grid)
     int* entries;               // local face indices
     uint32_t* big_faces;        // this search's big faces (global index), capacity big_cap
     double* big_box;            // 6 per big face: its key box (lo xyz, hi xyz)
-    int* big_count;             // big faces listed this search (cleared by the gather)
+    int* big_count;             // big faces listed this search
     long long big_cap;          // faces of the contacts with a dynamic grid
     int* big_best;              // per primary node: smallest local big face that hit, or BIG_NONE
     unsigned long long* search_stats;  // 3 per contact, accumulated: (unused: 0), big faces
