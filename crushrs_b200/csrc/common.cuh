@@ -110,9 +110,58 @@ __host__ __device__ __forceinline__ unsigned cell_hash(long long i, long long j,
 // when the two planes are perpendicular). So the key box is the box of those
 // corners over the four triangles, extended by md along -n, grown by a
 // rounding margin and clipped to the face box +- md (which alone bounds it).
-// Degenerate triangles accept nothing and are skipped.
-__host__ __device__ inline void face_key_box(const double x[4][3], const double n[3], const double c[3], double md, double* klo,
-                                             double* khi) {
+// Degenerate triangles accept nothing and are skipped. The margin (1e-7
+// relative) and the 1.3001 scale dwarf the rounding of the reciprocals used
+// here, so the box stays a superset of the narrow test's region.
+constexpr int KEY_TRI_NONE = 0;   // degenerate triangle: accepts nothing
+constexpr int KEY_TRI_PERP = 1;   // plane nearly perpendicular to the face: keep the whole face box +- md
+constexpr int KEY_TRI_ADDED = 2;  // its corners were added to rlo/rhi
+
+// Triangle t's part of the key box: its three moved corners added to
+// (rlo, rhi), or one of the other outcomes above.
+__host__ __device__ inline int key_box_triangle(const double x[4][3], const double n[3], const double c[3], int t, double* rlo,
+                                                double* rhi) {
+    // corners of triangles 012, 023, 123, 130, picked by value (no indexing
+    // by t, which would put x in local memory on the device)
+    double a[3], b[3], e[3];
+    for (int d = 0; d < 3; ++d) {
+        a[d] = t < 2 ? x[0][d] : x[1][d];
+        b[d] = t == 0 ? x[1][d] : (t == 3 ? x[3][d] : x[2][d]);
+        e[d] = t == 0 ? x[2][d] : (t == 3 ? x[0][d] : x[3][d]);
+    }
+    double u[3], v[3];
+    for (int d = 0; d < 3; ++d) {
+        u[d] = b[d] - a[d];
+        v[d] = e[d] - a[d];
+    }
+    double m[3] = {u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]};
+    const double len = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+    if (!(len > 0.0)) return KEY_TRI_NONE;  // degenerate (or non-finite)
+    const double il = 1.0 / len;
+    for (int d = 0; d < 3; ++d) m[d] *= il;
+    const double dn = n[0] * m[0] + n[1] * m[1] + n[2] * m[2];
+    if (!(fabs(dn) > 1e-6)) return KEY_TRI_PERP;
+    const double idn = 1.0 / dn;
+    double cen[3];
+    for (int d = 0; d < 3; ++d) cen[d] = (a[d] + b[d] + e[d]) * (1.0 / 3.0);
+    for (int k = 0; k < 3; ++k) {
+        double w[3];
+        for (int d = 0; d < 3; ++d) w[d] = cen[d] + 1.3001 * ((k == 0 ? a[d] : (k == 1 ? b[d] : e[d])) - cen[d]);
+        const double tt = (n[0] * (c[0] - w[0]) + n[1] * (c[1] - w[1]) + n[2] * (c[2] - w[2])) * idn;
+        for (int d = 0; d < 3; ++d) {
+            const double q = w[d] + tt * m[d];
+            rlo[d] = fmin(rlo[d], q);
+            rhi[d] = fmax(rhi[d], q);
+        }
+    }
+    return KEY_TRI_ADDED;
+}
+
+// The key box from the triangles' parts: the face box +- md when a triangle
+// was perpendicular, empty (klo > khi) when none added corners, else their
+// box extended by md along -n, grown by the margin and clipped.
+__host__ __device__ inline void key_box_finish(const double x[4][3], const double n[3], double md, bool any_perp, const double* rlo,
+                                               const double* rhi, double* klo, double* khi) {
     double flo[3], fhi[3];
     for (int d = 0; d < 3; ++d) {
         double lo = x[0][d], hi = x[0][d];
@@ -125,37 +174,7 @@ __host__ __device__ inline void face_key_box(const double x[4][3], const double 
         klo[d] = lo + -md;  // the narrow test's face box
         khi[d] = hi + md;
     }
-    const int tri[4][3] = {{0, 1, 2}, {0, 2, 3}, {1, 2, 3}, {1, 3, 0}};
-    double rlo[3] = {1e300, 1e300, 1e300}, rhi[3] = {-1e300, -1e300, -1e300};
-    for (int t = 0; t < 4; ++t) {
-        const double* a = x[tri[t][0]];
-        const double* b = x[tri[t][1]];
-        const double* e = x[tri[t][2]];
-        double u[3], v[3];
-        for (int d = 0; d < 3; ++d) {
-            u[d] = b[d] - a[d];
-            v[d] = e[d] - a[d];
-        }
-        double m[3] = {u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]};
-        const double len = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
-        if (!(len > 0.0)) continue;  // degenerate (or non-finite): accepts nothing
-        for (int d = 0; d < 3; ++d) m[d] /= len;
-        const double dn = n[0] * m[0] + n[1] * m[1] + n[2] * m[2];
-        if (!(fabs(dn) > 1e-6)) return;  // nearly perpendicular planes: keep the face box +- md
-        double cen[3];
-        for (int d = 0; d < 3; ++d) cen[d] = (a[d] + b[d] + e[d]) / 3.0;
-        const double* corner[3] = {a, b, e};
-        for (int k = 0; k < 3; ++k) {
-            double w[3];
-            for (int d = 0; d < 3; ++d) w[d] = cen[d] + 1.3001 * (corner[k][d] - cen[d]);
-            const double tt = (n[0] * (c[0] - w[0]) + n[1] * (c[1] - w[1]) + n[2] * (c[2] - w[2])) / dn;
-            for (int d = 0; d < 3; ++d) {
-                const double q = w[d] + tt * m[d];
-                rlo[d] = fmin(rlo[d], q);
-                rhi[d] = fmax(rhi[d], q);
-            }
-        }
-    }
+    if (any_perp) return;
     if (!(rlo[0] <= rhi[0])) {  // every triangle degenerate: no point can hit
         for (int d = 0; d < 3; ++d) {
             klo[d] = 1.0;
@@ -169,6 +188,14 @@ __host__ __device__ inline void face_key_box(const double x[4][3], const double 
         klo[d] = fmax(klo[d], rlo[d] - md * fmax(n[d], 0.0) - margin);
         khi[d] = fmin(khi[d], rhi[d] + md * fmax(-n[d], 0.0) + margin);
     }
+}
+
+__host__ __device__ inline void face_key_box(const double x[4][3], const double n[3], const double c[3], double md, double* klo,
+                                             double* khi) {
+    double rlo[3] = {1e300, 1e300, 1e300}, rhi[3] = {-1e300, -1e300, -1e300};
+    bool perp = false;
+    for (int t = 0; t < 4 && !perp; ++t) perp = key_box_triangle(x, n, c, t, rlo, rhi) == KEY_TRI_PERP;
+    key_box_finish(x, n, md, perp, rlo, rhi, klo, khi);
 }
 
 }  // namespace crush

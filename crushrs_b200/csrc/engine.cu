@@ -235,7 +235,8 @@ struct crush_ctx {
     std::vector<uint8_t> is_static_h;
     std::vector<int> tab_off_h;
     std::vector<uint8_t> is_brute_h;      // per contact: searched by one block, exhaustively
-    std::vector<uint32_t> grid_slaves_h;  // entries of the other contacts
+    std::vector<uint32_t> grid_slaves_h;  // entries of the other contacts (dynamic grid or none)
+    std::vector<uint32_t> st_slaves_h;    // entries of the contacts with a static grid
     int slave_lanes = 32;  // lanes per primary-node contact search (autotuned)
     bool tuned = false;
     long long last_tune_step = 0;  // the open run's step of the last tuning
@@ -299,6 +300,7 @@ struct crush_ctx {
         x.act_cnode = active(4);
         x.act_dynf = active(5);
         x.act_allslave = active(6);
+        x.act_stslave = active(7);
         return x;
     }
     Active active(int space) const {
@@ -1046,25 +1048,29 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     {
         // exhaustive contacts (no grid) get a block each; the rest are listed by entry
         std::vector<int> brute;
-        std::vector<uint32_t> gslaves;
+        std::vector<uint32_t> gslaves, stslaves;
         c->is_brute_h.assign(std::max(kc, 1), 0);
         for (int k = 0; k < kc; ++k) {
-            const bool grid = tab_off[k + 1] > tab_off[k] || st_tab_off[k + 1] > st_tab_off[k];
+            const bool st_grid = st_tab_off[k + 1] > st_tab_off[k];
+            const bool grid = tab_off[k + 1] > tab_off[k] || st_grid;
             if (!grid && face_off[k + 1] - face_off[k] <= 255 && slave_off[k + 1] > slave_off[k]) {
                 brute.push_back(k);
                 c->is_brute_h[k] = 1;
             } else {
-                for (int q = slave_off[k]; q < slave_off[k + 1]; ++q) gslaves.push_back((uint32_t)q);
+                for (int q = slave_off[k]; q < slave_off[k + 1]; ++q) (st_grid ? stslaves : gslaves).push_back((uint32_t)q);
             }
         }
         ca.n_brute = (int)brute.size();
         ca.brute_max_faces = 1;
         for (int k : brute) ca.brute_max_faces = std::max(ca.brute_max_faces, face_off[k + 1] - face_off[k]);
         ca.n_grid_slaves = (long long)gslaves.size();
+        ca.n_st_slaves = (long long)stslaves.size();
         TRY(c->upload_const(&ca.brute_contacts, brute));
         TRY(c->upload_const(&ca.grid_slaves, gslaves));
+        TRY(c->upload_const(&ca.st_slaves, stslaves));
         ca.is_brute_h = c->is_brute_h.data();
         c->grid_slaves_h = std::move(gslaves);
+        c->st_slaves_h = std::move(stslaves);
     }
     TRY(c->alloc(&ca.grid_state, 2 * (size_t)std::max(kc, 1) + 1));
     ca.levels_used = ca.grid_state;
@@ -1169,7 +1175,8 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     // ---- active chunk tables: slot range of every 256-entity chunk ----
     {
         const long long sizes[ACTIVE_SPACES] = {c->n_hc, E, N, (long long)c->grid_slaves_h.size(), (long long)cnode.size(),
-                                                (long long)dyn_faces.size(), (long long)slaves.size()};
+                                                (long long)dyn_faces.size(), (long long)slaves.size(),
+                                                (long long)c->st_slaves_h.size()};
         c->space_off_h.assign(ACTIVE_SPACES + 1, 0);
         for (int sp = 0; sp < ACTIVE_SPACES; ++sp) c->space_off_h[sp + 1] = c->space_off_h[sp] + (sizes[sp] + CHUNK - 1) / CHUNK;
         const long long nch = c->space_off_h[ACTIVE_SPACES];
@@ -1182,7 +1189,8 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
                 case 3: return contact_slot[slave_contact[c->grid_slaves_h[i]]];
                 case 4: return (int)cm.node_slot[cnode[i]];
                 case 5: return contact_slot[face_contact[dyn_faces[i]]];
-                default: return contact_slot[slave_contact[i]];
+                case 6: return contact_slot[slave_contact[i]];
+                default: return contact_slot[slave_contact[c->st_slaves_h[i]]];
             }
         };
         parallel_for(nch, [&](long long q) {

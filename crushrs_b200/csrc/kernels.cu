@@ -842,10 +842,9 @@ __device__ __forceinline__ void face_geometry(const ContactArrays& ca, const Nod
     }
 }
 
-// The grid level and cell range of face f's key box (from its geometry, into klo/khi):
-// returns the level, GRID_LEVELS for a big face, -1 for no insertion.
-__device__ __forceinline__ int face_cells(const ContactArrays& ca, const FaceGeo& g, int c, long long* r, double* klo, double* khi) {
-    face_key_box(g.x, g.n, g.c, ca.max_distance[c], klo, khi);
+// The grid level and cell range of a face's key box (klo, khi) in contact
+// c: returns the level, GRID_LEVELS for a big face, -1 for no insertion.
+__device__ __forceinline__ int box_level(const ContactArrays& ca, int c, const double* klo, const double* khi, long long* r) {
     if (klo[0] > khi[0] || klo[1] > khi[1] || klo[2] > khi[2]) return -1;  // no point can hit the face
     double cs = ca.cell[c];
     for (int level = 0; level < GRID_LEVELS; ++level, cs *= 4.0)
@@ -856,32 +855,55 @@ __device__ __forceinline__ int face_cells(const ContactArrays& ca, const FaceGeo
 // Thread per face: the face's geometry at X + u. The faces are
 // face_list[0, n) when face_list is given (the run: moving faces only), else
 // face_off[c0] + [0, n).
-// Thread per face: its geometry at X + u, and — when the search builds the
-// dynamic grids (do_grid) and the face's contact has one — its key box's
-// grid level and cells, stored for the fill pass, with one count per cell
-// added to the cell's bucket; a face whose box fits no level is listed as a
-// big face with its key box. Every face of a grid contact that the pass
-// visits gets its cell record (level -1: no inserts), so the fill pass, over
-// the same faces, inserts exactly what was counted.
+// FACE_LANES lanes per face: its geometry at X + u, and — when the search
+// builds the dynamic grids (do_grid) and the face's contact has one — its key
+// box (lane t takes triangle t, the quad combines them), grid level and
+// cells, stored for the fill pass, with one count per cell added to the
+// cell's bucket (the lanes split the cells); a face whose box fits no level
+// is listed as a big face with its key box. Every face of a grid contact that
+// the pass visits gets its cell record (level -1: no inserts), so the fill
+// pass, over the same faces, inserts exactly what was counted.
+constexpr int FACE_LANES = 4;
 __device__ __forceinline__ void contact_face_body(const ContactArrays& ca, const NodeArrays& nd, const Control* ctls, int c0,
                                                   const uint32_t* __restrict__ face_list, long long n, int run_mode, int do_grid,
-                                                  long long t) {
-    if (t >= n) return;
+                                                  long long t, int lane) {
+    if (t >= n) return;  // uniform over the face's lanes, as is every branch before the shuffles
+    const unsigned qmask = 0xFu << (threadIdx.x & 28u);
     const long long f = face_list ? (long long)face_list[t] : ca.face_off[c0] + t;
     const int c = ca.face_contact[f];
     const int tab = ca.tab_off[c];
     const bool grid = do_grid && ca.tab_off[c + 1] > tab;
     if (run_mode && ctls[ca.contact_slot[c]].done) {
-        if (grid) ca.cells[f].level = -1;
+        if (grid && lane == 0) ca.cells[f].level = -1;
         return;
     }
+    const double md = ca.max_distance[c];
     FaceGeo g;
-    face_geometry(ca, nd, f, ca.max_distance[c], g);
-    ca.geo[f] = g;
+    face_geometry(ca, nd, f, md, g);
+    {
+        constexpr int per = (int)(sizeof(FaceGeo) / sizeof(double)) / FACE_LANES;
+        const double* src = reinterpret_cast<const double*>(&g);
+        double* dst = reinterpret_cast<double*>(ca.geo + f);
+#pragma unroll
+        for (int k = 0; k < (int)(sizeof(FaceGeo) / sizeof(double)); ++k)
+            if (k / per == lane) dst[k] = src[k];
+    }
     if (!grid) return;
-    long long r[6];
+    double rlo[3] = {1e300, 1e300, 1e300}, rhi[3] = {-1e300, -1e300, -1e300};
+    int perp = key_box_triangle(g.x, g.n, g.c, lane, rlo, rhi) == KEY_TRI_PERP ? 1 : 0;
+#pragma unroll
+    for (int off = 1; off < FACE_LANES; off <<= 1) {
+        perp |= __shfl_xor_sync(qmask, perp, off, FACE_LANES);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            rlo[d] = fmin(rlo[d], __shfl_xor_sync(qmask, rlo[d], off, FACE_LANES));
+            rhi[d] = fmax(rhi[d], __shfl_xor_sync(qmask, rhi[d], off, FACE_LANES));
+        }
+    }
     double klo[3], khi[3];
-    const int level = face_cells(ca, g, c, r, klo, khi);
+    key_box_finish(g.x, g.n, md, perp != 0, rlo, rhi, klo, khi);
+    long long r[6];
+    const int level = box_level(ca, c, klo, khi, r);
     FaceCells fc;
     fc.level = level;
     fc.lo[0] = r[0];
@@ -889,30 +911,32 @@ __device__ __forceinline__ void contact_face_body(const ContactArrays& ca, const
     fc.lo[2] = r[4];
     fc.span[0] = fc.span[1] = fc.span[2] = 0;
     if (level == GRID_LEVELS) {
-        // A face is listed at most once per search and the list holds every
-        // face of the grid contacts, so it cannot overrun.
-        const int slot = atomicAdd(ca.big_count, 1);
-        if (slot < ca.big_cap) {
-            ca.big_faces[slot] = (uint32_t)f;
-            for (int d = 0; d < 3; ++d) {
-                ca.big_box[6 * (long long)slot + d] = klo[d];
-                ca.big_box[6 * (long long)slot + 3 + d] = khi[d];
+        if (lane == 0) {
+            // A face is listed at most once per search and the list holds
+            // every face of the grid contacts, so it cannot overrun.
+            const int slot = atomicAdd(ca.big_count, 1);
+            if (slot < ca.big_cap) {
+                ca.big_faces[slot] = (uint32_t)f;
+                for (int d = 0; d < 3; ++d) {
+                    ca.big_box[6 * (long long)slot + d] = klo[d];
+                    ca.big_box[6 * (long long)slot + 3 + d] = khi[d];
+                }
             }
+            atomicAdd(&ca.search_stats[3 * c + 1], 1ull);
         }
-        atomicAdd(&ca.search_stats[3 * c + 1], 1ull);
     } else if (level >= 0) {
-        if (!(ca.levels_used[c] & (1 << level))) atomicOr(&ca.levels_used[c], 1 << level);
+        if (lane == 0 && !(ca.levels_used[c] & (1 << level))) atomicOr(&ca.levels_used[c], 1 << level);
         const unsigned mask = (unsigned)(ca.tab_off[c + 1] - tab - 1);
         const int ni = (int)(r[1] - r[0] + 1), nj = (int)(r[3] - r[2] + 1), nk = (int)(r[5] - r[4] + 1);
         fc.span[0] = ni;
         fc.span[1] = nj;
         fc.span[2] = nk;
-        for (int kk = 0; kk < nk; ++kk)
-            for (int jj = 0; jj < nj; ++jj)
-                for (int ii = 0; ii < ni; ++ii)
-                    atomicAdd(&ca.counts[tab + (int)(cell_hash(r[0] + ii, r[2] + jj, r[4] + kk, level) & mask)], 1);
+        for (int q = lane; q < ni * nj * nk; q += FACE_LANES) {
+            const long long i = r[0] + q % ni, j = r[2] + (q / ni) % nj, k = r[4] + q / (ni * nj);
+            atomicAdd(&ca.counts[tab + (int)(cell_hash(i, j, k, level) & mask)], 1);
+        }
     }
-    ca.cells[f] = fc;
+    if (lane == 0) ca.cells[f] = fc;
 }
 
 // Fill pass, warp per face over the faces the geometry pass visited (same
@@ -945,9 +969,10 @@ __global__ void k_contact_insert(ContactArrays ca, int c0, const uint32_t* __res
 __global__ void __launch_bounds__(FACE_TPB) k_contact_faces(ContactArrays ca, NodeArrays nd, Control* ctls, int c0,
                                                             const uint32_t* __restrict__ face_list, long long n, int run_mode, int do_grid,
                                                             Active act) {
-    FOR_ACTIVE(act, n, 1, g) {
+    FOR_ACTIVE(act, n, FACE_LANES, g) {
         int lane;
-        contact_face_body(ca, nd, ctls, c0, face_list, n, run_mode, do_grid, active_entity(act, g, 1, &lane));
+        const long long t = active_entity(act, g, FACE_LANES, &lane);
+        contact_face_body(ca, nd, ctls, c0, face_list, n, run_mode, do_grid, t, lane);
     }
 }
 
@@ -1066,9 +1091,16 @@ __device__ __forceinline__ void emit_event(const ContactArrays& ca, uint32_t cod
 // first-hit face `best` (src/contact.rs:130-153: depth capped at 0.1 md,
 // stiffness limited to 0.1 m / dt^2, force capped at m * 1e5), and its five
 // reaction events: +F on the node, -F/4 on each of the face's four corners
-// (a node on two corners takes two).
+// (a node on two corners takes two). FORCE_LANES lanes share an entry: lane
+// j emits corner j's event, lane 0 also the node's own and the force.
+constexpr int FORCE_LANES = 4;
 __device__ __forceinline__ void record_hit(const ContactArrays& ca, long long s, int c, long long n, int best, double best_sd, double dt,
-                                           const double* __restrict__ masses, const FaceGeo& g, int skip_fixed) {
+                                           const double* __restrict__ masses, const FaceGeo& g, int skip_fixed, int lane) {
+    const long long F = ca.face_off[c] + best;
+    const uint32_t key = 2u * (uint32_t)s;
+    emit_event(ca, ca.face_cn[4 * F + lane], key + 1u, skip_fixed);
+    if (lane != 0) return;
+    emit_event(ca, ca.slave_cn[s], key, skip_fixed);
     const double md = ca.max_distance[c];
     const double m = masses[n];
     const double depth = fmin(-best_sd, 0.1 * md);
@@ -1078,11 +1110,6 @@ __device__ __forceinline__ void record_hit(const ContactArrays& ca, long long s,
     ca.hit_force[3 * s] = mag * g.n[0];
     ca.hit_force[3 * s + 1] = mag * g.n[1];
     ca.hit_force[3 * s + 2] = mag * g.n[2];
-    const long long F = ca.face_off[c] + best;
-    const uint32_t key = 2u * (uint32_t)s;
-    emit_event(ca, ca.slave_cn[s], key, skip_fixed);
-#pragma unroll
-    for (int j = 0; j < 4; ++j) emit_event(ca, ca.face_cn[4 * F + j], key + 1u, skip_fixed);
     atomicAdd(&ca.pen_count[c], 1ull);
     atomicMax(&ca.pen_max_bits[c], (unsigned long long)__double_as_longlong(-best_sd));
 }
@@ -1183,22 +1210,22 @@ __device__ __forceinline__ void contact_slave_body(const ContactArrays& ca, cons
     ca.hit_sd[s] = best_sd;
 }
 
+// run: the entries of `list` (grid_slaves or st_slaves, over their active
+// chunks), else the entries of contacts [c0, c1).
 template <int LANES>
 __global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, int c1, int run_mode, double dt_override,
-                                 const double* __restrict__ masses, long long n_slaves) {
-    // run: the primary-node entries of contacts with a grid (a list), else
-    // the entries of contacts [c0, c1)
-    const bool listed = run_mode && !ca.exhaustive;
-    const Active act = listed ? ca.act_slave : Active{nullptr, nullptr};
+                                 const double* __restrict__ masses, long long n_slaves, const uint32_t* __restrict__ list, Active act) {
     const long long s_begin = ca.slave_off[c0];
     FOR_ACTIVE(act, n_slaves, LANES, g) {
         int lane;
         const long long e = active_entity(act, g, LANES, &lane);
         const bool live = e < n_slaves;
-        const long long s = !live ? 0 : (listed ? (long long)ca.grid_slaves[e] : s_begin + e);
+        const long long s = !live ? 0 : (list ? (long long)list[e] : s_begin + e);
         contact_slave_body<LANES>(ca, nd, ctls, c0, c1, run_mode, dt_override, masses, s, live, lane);
     }
 }
+
+constexpr int ST_LANES = 2;  // lanes per entry of a static-grid contact (a box test, then a short bucket)
 
 // Contacts searched exhaustively (fewer faces than the grid threshold), one
 // block per contact: the contact's face geometry is staged in shared memory
@@ -1267,9 +1294,9 @@ __global__ void k_contact_force(ContactArrays ca, Control* ctls, int c0, int run
                                 const double* __restrict__ masses, long long n_slaves, int skip_fixed) {
     const Active act = run_mode ? ca.act_allslave : Active{nullptr, nullptr};
     const long long s0 = ca.slave_off[c0];
-    FOR_ACTIVE(act, n_slaves, 1, g) {
+    FOR_ACTIVE(act, n_slaves, FORCE_LANES, g) {
         int lane;
-        const long long e = active_entity(act, g, 1, &lane);
+        const long long e = active_entity(act, g, FORCE_LANES, &lane);
         if (e >= n_slaves) continue;
         const long long s = s0 + e;
         const int best = ca.hit[s];
@@ -1278,7 +1305,7 @@ __global__ void k_contact_force(ContactArrays ca, Control* ctls, int c0, int run
         const Control* ctl = ctls + ca.contact_slot[c];
         if (run_mode && ctl->done) continue;
         record_hit(ca, s, c, ca.slaves[s], best, ca.hit_sd[s], dt_override > 0.0 ? dt_override : step_dt(ctl), masses,
-                   ca.geo[ca.face_off[c] + best], skip_fixed);
+                   ca.geo[ca.face_off[c] + best], skip_fixed, lane);
     }
 }
 
@@ -1394,9 +1421,11 @@ __global__ void __launch_bounds__(GATHER_TPB) k_contact_gather(ContactArrays ca,
     }
 }
 
-// Thread 0 adds, in order, the events listed in keys[0, count) (ascending),
-// their forces fetched HEAVY_TPB at a time by the whole block.
-__device__ void heavy_sum(const ContactArrays& ca, const uint32_t* keys, int count, double (*sf)[3], double& sx, double& sy, double& sz) {
+// Threads 0, 1 and 2 add, in order, component 0, 1 and 2 of the events
+// listed in keys[0, count) (ascending) to their running sum acc, the
+// forces fetched HEAVY_TPB at a time by the whole block. The components'
+// sums are independent, so each is the reference's sequence for its axis.
+__device__ void heavy_sum(const ContactArrays& ca, const uint32_t* keys, int count, double (*sf)[3], double& acc) {
     for (int b0 = 0; b0 < count; b0 += HEAVY_TPB) {  // block-uniform
         const int t = b0 + threadIdx.x;
         if (t < count) {
@@ -1406,9 +1435,17 @@ __device__ void heavy_sum(const ContactArrays& ca, const uint32_t* keys, int cou
             sf[threadIdx.x][2] = ca.hit_force[3 * e + 2];
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
+        if (threadIdx.x < 3) {
             const int m = min(HEAVY_TPB, count - b0);
-            for (int j = 0; j < m; ++j) apply_event(keys[b0 + j] & 1u, sf[j][0], sf[j][1], sf[j][2], sx, sy, sz);
+            const int d = threadIdx.x;
+            double a = acc;
+#pragma unroll 4
+            for (int j = 0; j < m; ++j) {
+                const double fd = sf[j][d];
+                if (keys[b0 + j] & 1u) a -= 0.25 * fd;
+                else a += fd;
+            }
+            acc = a;
         }
         __syncthreads();
     }
@@ -1422,7 +1459,7 @@ __device__ void heavy_sum(const ContactArrays& ca, const uint32_t* keys, int cou
 // 2s+1. A block scan places the round's keys in entry order (already
 // ascending) and heavy_sum adds them.
 __device__ void walk_node(const ContactArrays& ca, int c0, int c1, long long i, long long n, uint32_t* keys, double (*sf)[3],
-                          int* s_warp, double& sx, double& sy, double& sz) {
+                          int* s_warp, double& acc) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t r_end = ca.cnode_off[i + 1];
     for (uint32_t r = ca.cnode_off[i], r1; r < r_end; r = r1) {
@@ -1472,7 +1509,7 @@ __device__ void walk_node(const ContactArrays& ca, int c0, int c1, long long i, 
                 for (int a = 0; a < m_j[j]; ++a) keys[pos++] = key + 1u;
             }
             __syncthreads();
-            heavy_sum(ca, keys, total, sf, sx, sy, sz);  // ends with a barrier: keys and s_warp are free again
+            heavy_sum(ca, keys, total, sf, acc);  // ends with a barrier: keys and s_warp are free again
         }
     }
 }
@@ -1492,7 +1529,7 @@ __global__ void __launch_bounds__(HEAVY_TPB) k_contact_gather_heavy(ContactArray
         const long long i = ca.gather_work[w];
         const int cnt = ca.gather_cnt[w];
         const long long n = ca.cnode[i];
-        double sx = 0.0, sy = 0.0, sz = 0.0;  // thread 0's running sum
+        double acc = 0.0;  // thread d < 3: component d of the running sum
         bool walk = cnt > HEAVY_KEYS;
         if (!walk) {
             if (threadIdx.x == 0) s_n = 0;
@@ -1511,7 +1548,7 @@ __global__ void __launch_bounds__(HEAVY_TPB) k_contact_gather_heavy(ContactArray
         }
         if (walk) {
             __syncthreads();
-            walk_node(ca, c0, c1, i, n, keys, sf, s_warp, sx, sy, sz);
+            walk_node(ca, c0, c1, i, n, keys, sf, s_warp, acc);
         } else {
             int P = EV_CAP;
             while (P < cnt) P <<= 1;
@@ -1532,13 +1569,9 @@ __global__ void __launch_bounds__(HEAVY_TPB) k_contact_gather_heavy(ContactArray
                     }
                     __syncthreads();
                 }
-            heavy_sum(ca, keys, cnt, sf, sx, sy, sz);
+            heavy_sum(ca, keys, cnt, sf, acc);
         }
-        if (threadIdx.x == 0) {
-            f_out[3 * n] = sx;
-            f_out[3 * n + 1] = sy;
-            f_out[3 * n + 2] = sz;
-        }
+        if (threadIdx.x < 3) f_out[3 * n + threadIdx.x] = acc;
         __syncthreads();
     }
 }
@@ -1706,8 +1739,8 @@ void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeAr
     // cursors, big-face list), whatever ran before it.
     cudaMemsetAsync(ca.grid_state, 0, sizeof(int) * (2 * (size_t)ca.n_contacts + 1), s);
     if (n_list > 0)
-        k_contact_faces<<<active_grid(n_list, 1, FACE_TPB, GRID_CAP), FACE_TPB, 0, s>>>(ca, nd, ctls, c0, list, n_list, run_mode, do_grid,
-                                                                                      act);
+        k_contact_faces<<<active_grid(n_list, FACE_LANES, FACE_TPB, GRID_CAP), FACE_TPB, 0, s>>>(ca, nd, ctls, c0, list, n_list,
+                                                                                               run_mode, do_grid, act);
     if (do_grid) {
         k_grid_alloc<<<(unsigned)blocks_for(bk1 - bk0, TPB), TPB, 0, s>>>(ca, c0, c1);
         if (n_list > 0) {
@@ -1726,15 +1759,23 @@ void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeAr
         }
         if (run_mode) n_slaves = ca.n_grid_slaves;
     }
+    // run: the listed entries (the static-grid ones apart); drop-in and
+    // exhaustive: every entry of [c0, c1)
+    const bool listed = run_mode && !ca.exhaustive;
+    const uint32_t* slist = listed ? ca.grid_slaves : nullptr;
+    const Active sact = listed ? ca.act_slave : Active{nullptr, nullptr};
+    if (listed && ca.n_st_slaves > 0)
+        k_contact_slaves<ST_LANES><<<active_grid(ca.n_st_slaves, ST_LANES, TPB, GRID_CAP), TPB, 0, s>>>(
+            ca, nd, ctls, c0, c1, run_mode, 0.0, nullptr, ca.n_st_slaves, ca.st_slaves, ca.act_stslave);
     if (n_slaves > 0) {
         const unsigned g = active_grid(n_slaves, lanes, TPB, GRID_CAP);
         switch (lanes) {
-            case 1: k_contact_slaves<1><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, 0.0, nullptr, n_slaves); break;
-            case 2: k_contact_slaves<2><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, 0.0, nullptr, n_slaves); break;
-            case 4: k_contact_slaves<4><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, 0.0, nullptr, n_slaves); break;
-            case 8: k_contact_slaves<8><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, 0.0, nullptr, n_slaves); break;
-            case 16: k_contact_slaves<16><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, 0.0, nullptr, n_slaves); break;
-            default: k_contact_slaves<32><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, 0.0, nullptr, n_slaves); break;
+            case 1: k_contact_slaves<1><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, 0.0, nullptr, n_slaves, slist, sact); break;
+            case 2: k_contact_slaves<2><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, 0.0, nullptr, n_slaves, slist, sact); break;
+            case 4: k_contact_slaves<4><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, 0.0, nullptr, n_slaves, slist, sact); break;
+            case 8: k_contact_slaves<8><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, 0.0, nullptr, n_slaves, slist, sact); break;
+            case 16: k_contact_slaves<16><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, 0.0, nullptr, n_slaves, slist, sact); break;
+            default: k_contact_slaves<32><<<g, TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, 0.0, nullptr, n_slaves, slist, sact); break;
         }
     }
 }
@@ -1748,8 +1789,8 @@ void launch_contact_finish(cudaStream_t s, const ContactArrays& ca, const NodeAr
     (void)n_faces;
     cudaMemsetAsync(ca.ev_pool_n, 0, 2 * sizeof(int), s);  // pool entries and heavy nodes (gather_count)
     if (n_slaves > 0)
-        k_contact_force<<<active_grid(n_slaves, 1, TPB, GRID_CAP), TPB, 0, s>>>(ca, ctls, c0, run_mode, dt_override, masses, n_slaves,
-                                                                               skip_fixed);
+        k_contact_force<<<active_grid(n_slaves, FORCE_LANES, TPB, GRID_CAP), TPB, 0, s>>>(ca, ctls, c0, run_mode, dt_override, masses,
+                                                                                         n_slaves, skip_fixed);
     long long nodes = ca.n_cnodes > 0 ? ca.n_cnodes : 1;
     k_contact_gather<<<active_grid(nodes, 1, GATHER_TPB, GRID_CAP * 2), GATHER_TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, f_out,
                                                                                           skip_fixed);
@@ -1772,6 +1813,7 @@ int contact_search_launches(const ContactArrays& ca, bool run_mode, long long n_
     if (!ca.exhaustive) {
         if (run_mode) {
             k += ca.n_brute > 0 ? 1 : 0;
+            k += ca.n_st_slaves > 0 ? 1 : 0;
             n_slaves = ca.n_grid_slaves;
         } else if (ca.is_brute_h && ca.is_brute_h[c0]) {
             ++k;
@@ -1794,8 +1836,8 @@ void launch_contact_geometry(cudaStream_t s, const ContactArrays& ca, const Node
     (void)f0;
     if (c1 <= c0 || n_faces <= 0) return;
     (void)c1;
-    k_contact_faces<<<active_grid(n_faces, 1, FACE_TPB, GRID_CAP), FACE_TPB, 0, s>>>(ca, nd, nullptr, c0, nullptr, n_faces, 0, 0,
-                                                                                   Active{nullptr, nullptr});
+    k_contact_faces<<<active_grid(n_faces, FACE_LANES, FACE_TPB, GRID_CAP), FACE_TPB, 0, s>>>(ca, nd, nullptr, c0, nullptr, n_faces,
+                                                                                            0, 0, Active{nullptr, nullptr});
 }
 
 }  // namespace crush

@@ -159,14 +159,17 @@ struct ContactArrays {
     int* gather_count;          // their number (ev_pool_n + 1)
     Active act_slave, act_cnode, act_dynf;  // active chunks of grid-searched entries, contact nodes, moving faces
     Active act_allslave;        // active chunks of all primary-node entries (the force pass)
+    Active act_stslave;         // active chunks of st_slaves
     // Contacts without a grid are searched by one block each; the entries of
     // the others are listed for the lane-parallel search.
     const int* brute_contacts;
     int n_brute;
     int brute_max_faces;        // most faces of a listed contact (its shared-memory stage)
     const double* st_box;       // 6 per contact: union of a static contact's key boxes (lo xyz, hi xyz)
-    const uint32_t* grid_slaves;
+    const uint32_t* grid_slaves;  // entries searched with the tuned lane count (dynamic grids, no usable grid)
     long long n_grid_slaves;
+    const uint32_t* st_slaves;    // entries of contacts with a static grid (searched with ST_LANES lanes)
+    long long n_st_slaves;
     const uint8_t* is_brute_h;  // host copy, per contact (launchers only)
 };
 
@@ -180,8 +183,8 @@ struct ActiveBuild {
     int* lists;                  // same layout as the chunks
     int* counts;                 // ACTIVE_SPACES
 };
-constexpr int ACTIVE_SPACES = 7;  // honeycomb elements, all elements, nodes, grid-searched entries, contact nodes, moving faces,
-                                  // all primary-node entries
+constexpr int ACTIVE_SPACES = 8;  // honeycomb elements, all elements, nodes, searched entries (dynamic grids and the
+                                  // rest), contact nodes, moving faces, all primary-node entries, static-grid entries
 
 // Vehicles of all crash slots: node lists and the reduction layout.
 struct VehicleArrays {
