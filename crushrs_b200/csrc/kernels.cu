@@ -447,18 +447,32 @@ __device__ __forceinline__ void forces_body(const ElementArrays& el, const NodeA
     for (int k = 0; k < 6; ++k) out[k] = make_float4(fo[4 * k], fo[4 * k + 1], fo[4 * k + 2], fo[4 * k + 3]);
 }
 
-// Nodal internal force: ordered f64 sum of incident corner forces.
+// Nodal internal force, component d: ordered f64 sum of the incident corner
+// forces (element order). Up to 8 corners (every node of a structured hex
+// mesh) the loads are all issued before the sum.
+__device__ __forceinline__ double gather_component(const NodeArrays& nd, const float* __restrict__ corner, long long n, int d) {
+    const uint32_t b = __ldg(nd.hc_off + n), m = __ldg(nd.hc_off + n + 1) - b;
+    double f = 0.0;
+    if (m <= 8) {
+        uint32_t sl[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) sl[j] = (uint32_t)j < m ? __ldg(nd.hc_slot + b + j) : 0u;
+        float c[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) c[j] = (uint32_t)j < m ? __ldg(corner + 3ull * sl[j] + d) : 0.f;  // slot = 8 e + corner
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            if ((uint32_t)j < m) f += (double)c[j];
+    } else {
+        for (uint32_t k = 0; k < m; ++k) f += (double)__ldg(corner + 3ull * __ldg(nd.hc_slot + b + k) + d);
+    }
+    return f;
+}
 __device__ __forceinline__ void gather_node(const NodeArrays& nd, const float* __restrict__ corner, long long n,
                                             double& fx, double& fy, double& fz) {
-    fx = 0.0; fy = 0.0; fz = 0.0;
-    const uint32_t b = nd.hc_off[n], en = nd.hc_off[n + 1];
-    for (uint32_t k = b; k < en; ++k) {
-        const uint32_t s = __ldg(nd.hc_slot + k);
-        const float* c = corner + 3ull * s;  // slot = 8 e + corner -> 24 e + 3 corner
-        fx += (double)__ldg(c);
-        fy += (double)__ldg(c + 1);
-        fz += (double)__ldg(c + 2);
-    }
+    fx = gather_component(nd, corner, n, 0);
+    fy = gather_component(nd, corner, n, 1);
+    fz = gather_component(nd, corner, n, 2);
 }
 
 __global__ void __launch_bounds__(FORCES_TPB, FORCES_MINB) k_forces(ElementArrays el, NodeArrays nd, Control* ctls, int respect_done) {
@@ -479,59 +493,60 @@ __global__ void k_gather(ElementArrays el, NodeArrays nd, double* __restrict__ f
 }
 
 // Half step: v½ = v + ½dt (f_ext - f_int)/m ; u += dt v½ ; fixed -> 0 (src/solver.rs:314-323).
-__device__ __forceinline__ void half_body(const NodeArrays& nd, const Control* ctls, long long n) {
+// Thread per node component d: the loads are issued before the crash's
+// done flag is known (they are harmless), so one latency covers them all.
+__device__ __forceinline__ void half_body(const NodeArrays& nd, const Control* ctls, long long n, int d) {
     if (n >= nd.n) return;
-    const Control* ctl = ctls + nd.node_slot[n];
+    const long long k = 3 * n + d;
+    const int slot = nd.node_slot[n];
+    const double fe = nd.f_ext[k], fi = nd.f_int[k], v = nd.v[k], u0 = nd.u[k], im = nd.inv_mass[n];
+    const bool fixed = nd.fixed[n] != 0;
+    const Control* ctl = ctls + slot;
     if (ctl->done) return;
     const double dt = step_dt(ctl);
-    const double im = nd.inv_mass[n];
-    const bool fixed = nd.fixed[n] != 0;
-    for (int d = 0; d < 3; ++d) {
-        const long long k = 3 * n + d;
-        const double a = (nd.f_ext[k] - nd.f_int[k]) * im;
-        double vh = nd.v[k] + 0.5 * dt * a;
-        double u = nd.u[k] + dt * vh;
-        if (fixed) {
-            u = 0.0;
-            vh = 0.0;
-            nd.v[k] = 0.0;
-        }
-        nd.v_half[k] = vh;
-        nd.u[k] = u;
+    const double a = (fe - fi) * im;
+    double vh = v + 0.5 * dt * a;
+    double u = u0 + dt * vh;
+    if (fixed) {
+        u = 0.0;
+        vh = 0.0;
+        nd.v[k] = 0.0;
     }
+    nd.v_half[k] = vh;
+    nd.u[k] = u;
 }
 
 __global__ void k_half(NodeArrays nd, Control* ctls) {
-    FOR_ACTIVE(nd.act_node, nd.n, 1, g) {
-        int lane;
-        half_body(nd, ctls, active_entity(nd.act_node, g, 1, &lane));
+    FOR_ACTIVE(nd.act_node, nd.n, 3, g) {
+        int d;
+        const long long n = active_entity(nd.act_node, g, 3, &d);
+        half_body(nd, ctls, n, d);
     }
 }
 
 // Full step with the fused force gather: v = (v½ + ½dt a) damping (src/solver.rs:334-342).
-__device__ __forceinline__ void full_body(const ElementArrays& el, const NodeArrays& nd, const Control* ctls, long long n) {
+// Thread per node component d, loads issued before the done flag is known.
+__device__ __forceinline__ void full_body(const ElementArrays& el, const NodeArrays& nd, const Control* ctls, long long n, int d) {
     if (n >= nd.n) return;
-    const Control* ctl = ctls + nd.node_slot[n];
+    const long long k = 3 * n + d;
+    const int slot = nd.node_slot[n];
+    const double fe = nd.f_ext[k], vh = nd.v_half[k], im = nd.inv_mass[n];
+    const bool fixed = nd.fixed[n] != 0;
+    const double f = gather_component(nd, el.corner, n, d);
+    const Control* ctl = ctls + slot;
     if (ctl->done) return;
     const double dt = step_dt(ctl);
-    double f[3];
-    gather_node(nd, el.corner, n, f[0], f[1], f[2]);
-    const double im = nd.inv_mass[n];
-    const bool fixed = nd.fixed[n] != 0;
-    const double damping = ctl->damping;
-    for (int d = 0; d < 3; ++d) {
-        const long long k = 3 * n + d;
-        const double a = (nd.f_ext[k] - f[d]) * im;
-        double v = (nd.v_half[k] + 0.5 * dt * a) * damping;
-        nd.v[k] = fixed ? 0.0 : v;
-        nd.f_int[k] = f[d];
-    }
+    const double a = (fe - f) * im;
+    const double v = (vh + 0.5 * dt * a) * ctl->damping;
+    nd.v[k] = fixed ? 0.0 : v;
+    nd.f_int[k] = f;
 }
 
 __global__ void k_full(ElementArrays el, NodeArrays nd, Control* ctls) {
-    FOR_ACTIVE(nd.act_node, nd.n, 1, g) {
-        int lane;
-        full_body(el, nd, ctls, active_entity(nd.act_node, g, 1, &lane));
+    FOR_ACTIVE(nd.act_node, nd.n, 3, g) {
+        int d;
+        const long long n = active_entity(nd.act_node, g, 3, &d);
+        full_body(el, nd, ctls, n, d);
     }
 }
 
@@ -586,15 +601,21 @@ __device__ __forceinline__ void elem_dt_body(const ElementArrays& el, const Node
     uint32_t slot = 0xffffffffu;
     double dt = CUDART_INF, extra = 0.0;
     if (e < el.n_all) {
+        // Loads that do not depend on the crash's done flag go first.
         slot = el.elem_slot[e];
+        const bool eroded = el.eroded_all[e] != 0;
+        const uint4 q0 = __ldg(reinterpret_cast<const uint4*>(el.conn_all + 8 * e));
+        const uint4 q1 = __ldg(reinterpret_cast<const uint4*>(el.conn_all + 8 * e) + 1);
         Control* ctl = ctls + slot;
         if (respect_done && ctl->done) {
             slot = 0xffffffffu;
         } else {
-            if (!el.eroded_all[e]) {
+            if (!eroded) {
+                const uint32_t conn[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
                 double p[8][3];
+#pragma unroll
                 for (int i = 0; i < 8; ++i) {
-                    long long n = el.conn_all[8 * e + i];
+                    const long long n = conn[i];
                     for (int d = 0; d < 3; ++d) p[i][d] = nd.pos[3 * n + d] + u[3 * n + d];
                 }
                 double l, vol;
@@ -1686,10 +1707,10 @@ void launch_gather(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd
     k_gather<<<(unsigned)blocks_for(nd.n, TPB), TPB, 0, s>>>(el, nd, f_out);
 }
 void launch_half(cudaStream_t s, const NodeArrays& nd, Control* ctls) {
-    k_half<<<active_grid(nd.n, 1, TPB, GRID_CAP), TPB, 0, s>>>(nd, ctls);
+    k_half<<<active_grid(nd.n, 3, TPB, GRID_CAP), TPB, 0, s>>>(nd, ctls);
 }
 void launch_full(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls) {
-    k_full<<<active_grid(nd.n, 1, TPB, GRID_CAP), TPB, 0, s>>>(el, nd, ctls);
+    k_full<<<active_grid(nd.n, 3, TPB, GRID_CAP), TPB, 0, s>>>(el, nd, ctls);
 }
 void launch_elem_dt(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, const double* u, int respect_done) {
     if (el.n_all <= 0) return;
