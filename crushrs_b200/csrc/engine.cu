@@ -1080,6 +1080,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->alloc(&ca.gather_work, std::max<size_t>(cnode.size(), 1)));
     TRY(c->alloc(&ca.gather_cnt, std::max<size_t>(cnode.size(), 1)));
     TRY(c->alloc(&ca.ev_pool_n, 2));
+    TRY(c->alloc(&ca.u_next, 3 * (size_t)std::max<long long>(c->n_nodes, 1)));
     ca.gather_count = ca.ev_pool_n + 1;
     ca.n_buckets = tab_off.back();
     ca.exhaustive = 0;
@@ -1301,17 +1302,20 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
         n += contact_finish_launches(c->n_slaves);
     }
     mark(2);
-    launch_half(c->stream, nd, c->ctls);
-    // The next step's contact search needs only the new X + u: it runs on
-    // the side stream while this step's forces and update run.
+    // The next step's contact search needs only the new X + u of the contact
+    // nodes, which the gather wrote to u_next: it runs on the side stream
+    // while this step's half step, forces and update run.
     if (c->n_contacts > 0) {
+        NodeArrays nds = nd;
+        nds.u = c->ca.u_next;
         cudaEventRecord(c->ev_fork, c->stream);
         cudaStreamWaitEvent(c->side, c->ev_fork, 0);
-        launch_contact_search(c->side, cr, nd, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 1,
+        launch_contact_search(c->side, cr, nds, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 1,
                               c->slave_lanes);
         n += contact_search_launches(c->ca, true, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 0);
         cudaEventRecord(c->ev_join, c->side);
     }
+    launch_half(c->stream, nd, c->ctls);
     mark(3);
     launch_forces(c->stream, el, nd, c->ctls, 1);
     mark(4);
@@ -1410,6 +1414,7 @@ int run_begin(crush_ctx* c) {
     CK(cudaMemsetAsync(c->added, 0, sizeof(double) * N, c->stream));
     if (c->n_contacts > 0) {
         CK(cudaMemsetAsync(c->ca.big_best, 0x7F, sizeof(int) * std::max<long long>(c->n_slaves, 1), c->stream));  // BIG_NONE
+        CK(cudaMemsetAsync(c->ca.u_next, 0, sizeof(double) * 3 * N, c->stream));                                  // = u
     }
     CK(cudaMemsetAsync(c->eroded_all, 0, c->n_all, c->stream));
     launch_init_state(c->stream, c->n_hc, c->stride, c->state);

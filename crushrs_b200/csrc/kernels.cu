@@ -1352,6 +1352,16 @@ __device__ __forceinline__ void apply_event(bool face, double fx, double fy, dou
     }
 }
 
+// The half step's u of component d of node n given its new f_ext: the
+// arithmetic of half_body, so the value is the one the half step writes.
+__device__ __forceinline__ double half_u(const NodeArrays& nd, const Control* ctl, long long n, int d, double fe) {
+    const long long k = 3 * n + d;
+    const double dt = step_dt(ctl);
+    const double a = (fe - nd.f_int[k]) * nd.inv_mass[n];
+    const double vh = nd.v[k] + 0.5 * dt * a;
+    return nd.u[k] + dt * vh;
+}
+
 // Ordered reaction gather, one thread per contact node. The node's events
 // carry keys 2s (own) and 2s+1 (face) of the global primary-node index s;
 // contacts are numbered in order and so are their entries, so ascending keys
@@ -1359,7 +1369,9 @@ __device__ __forceinline__ void apply_event(bool face, double fx, double fy, dou
 // contact after contact. Up to EV_CAP keys are sorted in registers (a
 // bitonic network) and their forces loaded together; a node with more goes
 // to k_contact_gather_heavy, which writes its output. The gather zeroes the
-// node's event count for the next pass.
+// node's event count for the next pass. In a run it also writes the node's
+// half-step u to u_next (fixed nodes and stopped crashes keep theirs), so
+// the next step's search can start before the half step.
 __device__ __forceinline__ void gather_body(const ContactArrays& ca, const NodeArrays& nd, const Control* ctls, int c0, int c1,
                                             int run_mode, double* __restrict__ f_out, int skip_fixed, long long i) {
     if (i >= ca.n_cnodes) return;
@@ -1431,6 +1443,12 @@ __device__ __forceinline__ void gather_body(const ContactArrays& ca, const NodeA
     f_out[3 * n] = sx;
     f_out[3 * n + 1] = sy;
     f_out[3 * n + 2] = sz;
+    if (run_mode) {
+        const Control* ctl = ctls + nd.node_slot[n];
+        ca.u_next[3 * n] = half_u(nd, ctl, n, 0, sx);
+        ca.u_next[3 * n + 1] = half_u(nd, ctl, n, 1, sy);
+        ca.u_next[3 * n + 2] = half_u(nd, ctl, n, 2, sz);
+    }
 }
 
 __global__ void __launch_bounds__(GATHER_TPB) k_contact_gather(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, int c1,
@@ -1540,7 +1558,8 @@ __device__ void walk_node(const ContactArrays& ca, int c0, int c1, long long i, 
 // collected (EV_CAP + pool = the count when nothing was dropped), sorted by a
 // bitonic sort in shared memory and added in order. A node whose events do
 // not fit HEAVY_KEYS, or lost some to a full pool, is rebuilt by walk_node.
-__global__ void __launch_bounds__(HEAVY_TPB) k_contact_gather_heavy(ContactArrays ca, int c0, int c1, double* __restrict__ f_out) {
+__global__ void __launch_bounds__(HEAVY_TPB) k_contact_gather_heavy(ContactArrays ca, NodeArrays nd, const Control* ctls, int c0, int c1,
+                                                                    int run_mode, double* __restrict__ f_out) {
     __shared__ uint32_t keys[HEAVY_BUF];
     __shared__ double sf[HEAVY_TPB][3];
     __shared__ int s_warp[HEAVY_TPB / 32];
@@ -1592,7 +1611,10 @@ __global__ void __launch_bounds__(HEAVY_TPB) k_contact_gather_heavy(ContactArray
                 }
             heavy_sum(ca, keys, cnt, sf, acc);
         }
-        if (threadIdx.x < 3) f_out[3 * n + threadIdx.x] = acc;
+        if (threadIdx.x < 3) {
+            f_out[3 * n + threadIdx.x] = acc;
+            if (run_mode) ca.u_next[3 * n + threadIdx.x] = half_u(nd, ctls + nd.node_slot[n], n, threadIdx.x, acc);
+        }
         __syncthreads();
     }
 }
@@ -1701,7 +1723,9 @@ void launch_init_state(cudaStream_t s, long long n_hc, long long stride, float4*
 }
 void launch_forces(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, int respect_done) {
     if (el.n_hc <= 0) return;
-    k_forces<<<active_grid(el.n_hc, 1, FORCES_TPB, 148 * FORCES_MINB * 4), FORCES_TPB, 0, s>>>(el, nd, ctls, respect_done);
+    // Persistent: one wave of FORCES_MINB blocks per SM striding over the
+    // active chunks (measured faster than several waves: no tail).
+    k_forces<<<active_grid(el.n_hc, 1, FORCES_TPB, 148 * FORCES_MINB), FORCES_TPB, 0, s>>>(el, nd, ctls, respect_done);
 }
 void launch_gather(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, double* f_out) {
     k_gather<<<(unsigned)blocks_for(nd.n, TPB), TPB, 0, s>>>(el, nd, f_out);
@@ -1815,7 +1839,8 @@ void launch_contact_finish(cudaStream_t s, const ContactArrays& ca, const NodeAr
     long long nodes = ca.n_cnodes > 0 ? ca.n_cnodes : 1;
     k_contact_gather<<<active_grid(nodes, 1, GATHER_TPB, GRID_CAP * 2), GATHER_TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, f_out,
                                                                                           skip_fixed);
-    k_contact_gather_heavy<<<(unsigned)(nodes < HEAVY_BLOCKS ? nodes : HEAVY_BLOCKS), HEAVY_TPB, 0, s>>>(ca, c0, c1, f_out);
+    k_contact_gather_heavy<<<(unsigned)(nodes < HEAVY_BLOCKS ? nodes : HEAVY_BLOCKS), HEAVY_TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode,
+                                                                                                      f_out);
 }
 
 void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,

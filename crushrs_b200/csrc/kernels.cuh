@@ -154,6 +154,8 @@ struct ContactArrays {
     long long n_grid_faces;
     long long n_buckets;        // total dynamic buckets (tab_off[n_contacts])
     int exhaustive;             // 1: every search tests every face of its contact (no broad phase)
+    double* u_next;             // 3N: the half step's u of every contact node, written by the run's gather
+                                //     (the next search reads it while the half step runs)
     int* gather_work;           // contact nodes with over EV_CAP events this pass (n_cnodes capacity)
     int* gather_cnt;            // their event counts
     int* gather_count;          // their number (ev_pool_n + 1)
