@@ -192,7 +192,8 @@ struct crush_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;               // the contact search of the next step runs here, beside the forces
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaStream_t side2 = nullptr;              // its static-grid part, beside the dynamic grid build
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join2 = nullptr;
     std::vector<void*> allocs;
     int64_t launches = 0;
 
@@ -363,10 +364,13 @@ struct crush_ctx {
         for (cudaEvent_t e : prof_ev) cudaEventDestroy(e);
         if (stream) cudaStreamSynchronize(stream);
         if (side) cudaStreamSynchronize(side);
+        if (side2) cudaStreamSynchronize(side2);
         for (void* p : allocs) cudaFree(p);
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
+        if (ev_join2) cudaEventDestroy(ev_join2);
         if (side) cudaStreamDestroy(side);
+        if (side2) cudaStreamDestroy(side2);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -662,8 +666,8 @@ void build_contacts(const crush_model_desc* d, const Slot& sl, const Combined& c
             cp.st_off.push_back((uint32_t)cp.st_entries.size());
             for (int64_t f = 0; f < cd.n_faces; ++f) cp.dyn_faces.push_back((uint32_t)(face0 + f));
             if (cd.n_faces >= GRID_MIN_FACES) {
-                // Hierarchical table: four times the level-0 key-box cells of
-                // the faces at the reference positions, a power of two.
+                // Hierarchical table: twice the level-0 key-box cells of the
+                // faces at the reference positions, a power of two.
                 size_t inserts = 0;
                 for (int64_t f = 0; f < cd.n_faces; ++f) {
                     double x[4][3], nr[3], ctr[3], klo[3], khi[3];
@@ -673,7 +677,7 @@ void build_contacts(const crush_model_desc* d, const Slot& sl, const Combined& c
                     for (int dd = 0; dd < 3; ++dd) cells *= std::floor(khi[dd] / cs) - std::floor(klo[dd] / cs) + 1.0;
                     inserts += (size_t)std::min(std::isfinite(cells) && cells > 0.0 ? cells : 0.0, (double)LEVEL_CELL_BUDGET);
                 }
-                t = next_pow2(std::max<size_t>(1024, 4 * inserts));
+                t = next_pow2(std::max<size_t>(1024, 2 * inserts));
                 for (int64_t f = 0; f < cd.n_faces; ++f) cp.grid_faces.push_back((uint32_t)(face0 + f));
             }
         }
@@ -737,8 +741,10 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
         int lo = 0, hi = 0;
         CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
         CK(cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, hi));  // search blocks first when SMs free up
+        CK(cudaStreamCreateWithPriority(&c->side2, cudaStreamNonBlocking, hi));
         CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c->ev_join2, cudaEventDisableTiming));
     }
     c->n_slots = n_desc;
     c->slots.resize(n_desc);
@@ -1310,10 +1316,13 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
         nds.u = c->ca.u_next;
         cudaEventRecord(c->ev_fork, c->stream);
         cudaStreamWaitEvent(c->side, c->ev_fork, 0);
+        cudaStreamWaitEvent(c->side2, c->ev_fork, 0);
+        // static-grid entries on side2: they need no dynamic grid
         launch_contact_search(c->side, cr, nds, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 1,
-                              c->slave_lanes);
+                              c->slave_lanes, c->side2);
         n += contact_search_launches(c->ca, true, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 0);
         cudaEventRecord(c->ev_join, c->side);
+        cudaEventRecord(c->ev_join2, c->side2);
     }
     launch_half(c->stream, nd, c->ctls);
     mark(3);
@@ -1333,7 +1342,10 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
     }
     launch_step_end(c->stream, c->ctls, cr, c->va, sep ? 1 : 0, c->slot_done);
     ++n;
-    if (c->n_contacts > 0) cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+    if (c->n_contacts > 0) {
+        cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+        cudaStreamWaitEvent(c->stream, c->ev_join2, 0);
+    }
     mark(6);
     return check_launch(c, n);
 }

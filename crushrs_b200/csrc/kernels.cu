@@ -1197,15 +1197,29 @@ __device__ __forceinline__ void contact_slave_body(const ContactArrays& ca, cons
             }
             const unsigned mask = (unsigned)(ca.tab_off[c + 1] - tab - 1);
             const int used = ca.levels_used[c];
-            double cs = ca.cell[c];
-            for (int level = 0; level < GRID_LEVELS; ++level, cs *= 4.0) {
-                if (!(used & (1 << level))) continue;
+            static_assert(GRID_LEVELS == 2, "the lane split below assumes two grid levels");
+            if (LANES >= 2 && used == 3) {
+                // both levels in use: half the lanes scan each, concurrently
+                const int level = lane < LANES / 2 ? 0 : 1;
+                const double cs = level ? ca.cell[c] * 4.0 : ca.cell[c];
                 const int b = tab + (int)(point_cell_hash(p, cs, level) & mask);
                 const unsigned e0 = ca.boff[b];
                 const int cnt = ca.blen[b];
-                for (int k = lane; k < cnt; k += LANES) {
+                for (int k = lane % (LANES / 2); k < cnt; k += LANES / 2) {
                     const int f = ca.entries[e0 + k];
                     if (f < best && face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; }
+                }
+            } else {
+                double cs = ca.cell[c];
+                for (int level = 0; level < GRID_LEVELS; ++level, cs *= 4.0) {
+                    if (!(used & (1 << level))) continue;
+                    const int b = tab + (int)(point_cell_hash(p, cs, level) & mask);
+                    const unsigned e0 = ca.boff[b];
+                    const int cnt = ca.blen[b];
+                    for (int k = lane; k < cnt; k += LANES) {
+                        const int f = ca.entries[e0 + k];
+                        if (f < best && face_hit(geo[f], p, md, &sd)) { best = f; best_sd = sd; }
+                    }
                 }
             }
         } else {
@@ -1772,7 +1786,8 @@ void launch_vehicle_vx(cudaStream_t s, const VehicleArrays& va, const double* ma
 }
 
 void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
-                           long long n_faces, long long n_slaves, long long bk0, long long bk1, int run_mode, int lanes) {
+                           long long n_faces, long long n_slaves, long long bk0, long long bk1, int run_mode, int lanes,
+                           cudaStream_t s_static) {
     (void)f0;
     if (c1 <= c0) return;
     // run: only moving faces (static ones keep their geometry); drop-in: every face of the range
@@ -1810,7 +1825,7 @@ void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeAr
     const uint32_t* slist = listed ? ca.grid_slaves : nullptr;
     const Active sact = listed ? ca.act_slave : Active{nullptr, nullptr};
     if (listed && ca.n_st_slaves > 0)
-        k_contact_slaves<ST_LANES><<<active_grid(ca.n_st_slaves, ST_LANES, TPB, GRID_CAP), TPB, 0, s>>>(
+        k_contact_slaves<ST_LANES><<<active_grid(ca.n_st_slaves, ST_LANES, TPB, GRID_CAP), TPB, 0, s_static ? s_static : s>>>(
             ca, nd, ctls, c0, c1, run_mode, 0.0, nullptr, ca.n_st_slaves, ca.st_slaves, ca.act_stslave);
     if (n_slaves > 0) {
         const unsigned g = active_grid(n_slaves, lanes, TPB, GRID_CAP);

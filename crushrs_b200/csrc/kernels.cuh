@@ -233,8 +233,11 @@ int contact_launches(const ContactArrays& ca, bool run_mode, long long n_faces, 
 // hits) needs only X + u and may run while other work of the step runs; the
 // finish (forces of the hits with the step's dt, hit lists, counters, the
 // ordered gather into f_out) follows it.
+// s_static (optional): the stream for the static-grid entries' search,
+// which needs nothing else the search builds.
 void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
-                           long long n_faces, long long n_slaves, long long bk0, long long bk1, int run_mode, int lanes);
+                           long long n_faces, long long n_slaves, long long bk0, long long bk1, int run_mode, int lanes,
+                           cudaStream_t s_static = nullptr);
 void launch_contact_finish(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
                            long long n_faces, long long n_slaves, double dt_override, const double* masses, double* f_out,
                            int skip_fixed);
