@@ -192,8 +192,10 @@ struct crush_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;               // the contact search of the next step runs here, beside the forces
-    cudaStream_t side2 = nullptr;              // its static-grid part, beside the dynamic grid build
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join2 = nullptr;
+    cudaStream_t side2 = nullptr;              // its static-grid part, then the next step's element dt pass
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join2 = nullptr, ev_forces = nullptr;
+    cudaEvent_t ev_heavy = nullptr, ev_heavy_done = nullptr;  // the heavy-node gather beside the contact gather
+    int* mass_flag = nullptr;                  // device: some crash scales its masses this step
     std::vector<void*> allocs;
     int64_t launches = 0;
 
@@ -326,6 +328,7 @@ struct crush_ctx {
         a.all_off = all_off;
         a.all_slot = all_slot;
         a.node_slot = node_slot;
+        a.mass_flag = mass_flag;
         a.act_node = Active{nullptr, nullptr};
         return a;
     }
@@ -369,6 +372,9 @@ struct crush_ctx {
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
         if (ev_join2) cudaEventDestroy(ev_join2);
+        if (ev_forces) cudaEventDestroy(ev_forces);
+        if (ev_heavy) cudaEventDestroy(ev_heavy);
+        if (ev_heavy_done) cudaEventDestroy(ev_heavy_done);
         if (side) cudaStreamDestroy(side);
         if (side2) cudaStreamDestroy(side2);
         if (stream) cudaStreamDestroy(stream);
@@ -745,6 +751,9 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
         CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&c->ev_join2, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c->ev_forces, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c->ev_heavy, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c->ev_heavy_done, cudaEventDisableTiming));
     }
     c->n_slots = n_desc;
     c->slots.resize(n_desc);
@@ -890,6 +899,8 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->alloc(&c->ctls, c->n_slots));
     TRY(c->alloc(&c->ctls_aux, c->n_slots));
     TRY(c->alloc(&c->slot_done, c->n_slots));
+    TRY(c->alloc(&c->mass_flag, 1));
+    CK(cudaMemsetAsync(c->mass_flag, 0, sizeof(int), c->stream));
     CK(cudaMemsetAsync(c->planes, 0, sizeof(float4) * N_STATIC_PLANES * c->stride, c->stream));
     CK(cudaMemsetAsync(c->eroded_all, 0, E, c->stream));
     CK(cudaMemsetAsync(c->ctls, 0, sizeof(Control) * c->n_slots, c->stream));
@@ -1084,7 +1095,6 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     ca.big_count = ca.grid_state + 2 * kc;
     TRY(c->alloc(&ca.cells, (size_t)std::max<long long>(c->n_faces, 1)));
     TRY(c->alloc(&ca.gather_work, std::max<size_t>(cnode.size(), 1)));
-    TRY(c->alloc(&ca.gather_cnt, std::max<size_t>(cnode.size(), 1)));
     TRY(c->alloc(&ca.ev_pool_n, 2));
     TRY(c->alloc(&ca.u_next, 3 * (size_t)std::max<long long>(c->n_nodes, 1)));
     ca.gather_count = ca.ev_pool_n + 1;
@@ -1294,17 +1304,19 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
         launch_build_active(c->stream, c->ab, c->ctls);
         ++n;
     }
+    // Stable step check: the element pass ran at the end of the previous
+    // step (or at run begin) on this step's X + u.
     if (c->adaptive && step % c->check_steps == 0) {
-        launch_elem_dt(c->stream, el, nd, c->ctls, c->u, 1);
-        launch_dt_finalize(c->stream, c->ctls, c->n_slots);
+        launch_dt_finalize(c->stream, c->ctls, c->n_slots, c->mass_flag);
         launch_mass_scaling(c->stream, el, nd, c->ctls, 0);
-        n += 3;
+        n += 2;
     }
     mark(1);
     // Contact forces of this step from the search run beside the previous
     // step's forces (or at crush_run_begin for the first step).
     if (c->n_contacts > 0) {
-        launch_contact_finish(c->stream, cr, nd, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0.0, c->mass, c->f_ext, 1);
+        launch_contact_finish(c->stream, cr, nd, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0.0, c->mass, c->f_ext, 1,
+                              c->side2, c->ev_heavy, c->ev_heavy_done);
         n += contact_finish_launches(c->n_slaves);
     }
     mark(2);
@@ -1327,6 +1339,17 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
     launch_half(c->stream, nd, c->ctls);
     mark(3);
     launch_forces(c->stream, el, nd, c->ctls, 1);
+    // The next step's element dt pass needs its X + u (final after the half
+    // step) and this step's erosion (final after the forces): it runs on
+    // side2 beside the full update.
+    const bool dt_next = c->adaptive && (step + 1) % c->check_steps == 0;
+    if (dt_next) {
+        cudaEventRecord(c->ev_forces, c->stream);
+        cudaStreamWaitEvent(c->side2, c->ev_forces, 0);
+        launch_elem_dt(c->side2, el, nd, c->ctls, c->u, 1);
+        ++n;
+        if (c->n_contacts == 0) cudaEventRecord(c->ev_join2, c->side2);
+    }
     mark(4);
     launch_full(c->stream, el, nd, c->ctls);
     mark(5);
@@ -1340,10 +1363,13 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
         launch_vehicle_vx(c->stream, c->va, c->mass, c->v, c->ctls);
         ++n;
     }
-    launch_step_end(c->stream, c->ctls, cr, c->va, sep ? 1 : 0, c->slot_done);
+    launch_step_end(c->stream, c->ctls, cr, c->va, sep ? 1 : 0, c->slot_done, c->mass_flag);
     ++n;
     if (c->n_contacts > 0) {
+        if (dt_next) cudaEventRecord(c->ev_join2, c->side2);
         cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+        cudaStreamWaitEvent(c->stream, c->ev_join2, 0);
+    } else if (dt_next) {
         cudaStreamWaitEvent(c->stream, c->ev_join2, 0);
     }
     mark(6);
@@ -1465,6 +1491,13 @@ int run_begin(crush_ctx* c) {
     st = check_launch(c, c->n_faces > 0 ? 1 : 0);
     if (st != CRUSH_OK) return st;
     CK(cudaMemcpyAsync(c->ctls, h.data(), sizeof(Control) * h.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(c->mass_flag, 0, sizeof(int), c->stream));
+    if (c->adaptive) {
+        // Step 0's element dt pass (each step runs the next check's pass).
+        launch_elem_dt(c->stream, c->el(), c->nd(), c->ctls, c->u, 1);
+        st = check_launch(c);
+        if (st != CRUSH_OK) return st;
+    }
     c->done_h.resize(c->n_slots);
     for (int k = 0; k < c->n_slots; ++k) c->done_h[k] = h[k].done;
     CK(cudaMemcpyAsync(c->slot_done, c->done_h.data(), sizeof(int) * c->n_slots, cudaMemcpyHostToDevice, c->stream));

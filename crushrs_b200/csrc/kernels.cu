@@ -658,7 +658,7 @@ __global__ void __launch_bounds__(DT_TPB) k_elem_dt(ElementArrays el, NodeArrays
 }
 
 // The adaptive step decision of src/solver.rs:288-299, one thread per slot.
-__global__ void k_dt_finalize(Control* ctls, int n_slots) {
+__global__ void k_dt_finalize(Control* ctls, int n_slots, int* __restrict__ mass_flag) {
     const int sl = blockIdx.x * blockDim.x + threadIdx.x;
     if (sl >= n_slots) return;
     Control* ctl = ctls + sl;
@@ -671,6 +671,7 @@ __global__ void k_dt_finalize(Control* ctls, int n_slots) {
     double dt_use = dt_stable;
     if (ctl->dt_floor > 0.0 && dt_stable < ctl->dt_floor) {
         ctl->mass_scale_now = 1;
+        *mass_flag = 1;  // some crash scales its masses this step
         ctl->added_total = total;
         ctl->added_mass_max = fmax(ctl->added_mass_max, total);
         dt_use = ctl->dt_floor;
@@ -681,7 +682,7 @@ __global__ void k_dt_finalize(Control* ctls, int n_slots) {
 // Added nodal mass (element order, src/kernel.rs:246-255) and 1/(m + added).
 __device__ __forceinline__ void mass_scaling_body(const ElementArrays& el, const NodeArrays& nd, const Control* ctls, int force_apply,
                                                   long long n) {
-    if (n >= nd.n) return;
+    if (n >= nd.n || (!force_apply && !*nd.mass_flag)) return;
     const Control* ctl = ctls + nd.node_slot[n];
     if (!force_apply && (ctl->done || !ctl->mass_scale_now)) return;
     const double floor = ctl->dt_floor;
@@ -743,8 +744,10 @@ __device__ void step_end_slot(Control* ctl, int sl, const ContactArrays& ca, con
 
 // One thread per slot; also mirrors each slot's done flag into done_out (a
 // compact array the host polls).
-__global__ void k_step_end(Control* ctls, ContactArrays ca, VehicleArrays va, int check_separation, int* __restrict__ done_out) {
+__global__ void k_step_end(Control* ctls, ContactArrays ca, VehicleArrays va, int check_separation, int* __restrict__ done_out,
+                           int* __restrict__ mass_flag) {
     const int sl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sl == 0) *mass_flag = 0;  // the step's mass scaling is done
     if (sl >= ca.n_slots) return;
     Control* ctl = ctls + sl;
     if (!ctl->done) step_end_slot(ctl, sl, ca, va, check_separation);
@@ -1103,6 +1106,7 @@ __device__ __forceinline__ void emit_event(const ContactArrays& ca, uint32_t cod
     if (slot < EV_CAP) {
         ca.ev_list[(long long)cn * EV_CAP + slot] = key;
     } else {
+        if (slot == EV_CAP) ca.gather_work[atomicAdd(ca.gather_count, 1)] = (int)cn;  // the node turns heavy, once
         const int p = atomicAdd(ca.ev_pool_n, 1);
         if (p < ca.ev_pool_cap) ca.ev_pool[p] = make_uint2(cn, key);
     }
@@ -1382,8 +1386,9 @@ __device__ __forceinline__ double half_u(const NodeArrays& nd, const Control* ct
 // are the order in which src/contact.rs:146-153 adds the reactions to f_ext,
 // contact after contact. Up to EV_CAP keys are sorted in registers (a
 // bitonic network) and their forces loaded together; a node with more goes
-// to k_contact_gather_heavy, which writes its output. The gather zeroes the
-// node's event count for the next pass. In a run it also writes the node's
+// to k_contact_gather_heavy (the force pass listed it), which writes its
+// output and zeroes its count. The gather zeroes the other nodes' event
+// counts for the next pass. In a run it also writes the node's
 // half-step u to u_next (fixed nodes and stopped crashes keep theirs), so
 // the next step's search can start before the half step.
 __device__ __forceinline__ void gather_body(const ContactArrays& ca, const NodeArrays& nd, const Control* ctls, int c0, int c1,
@@ -1400,15 +1405,10 @@ __device__ __forceinline__ void gather_body(const ContactArrays& ca, const NodeA
         if (!touched) return;
     }
     const int cnt = ca.ev_count[i];
+    if (cnt > EV_CAP) return;  // k_contact_gather_heavy's node
     double sx = 0.0, sy = 0.0, sz = 0.0;
     if (cnt > 0) {
         ca.ev_count[i] = 0;
-        if (cnt > EV_CAP) {
-            const int w = atomicAdd(ca.gather_count, 1);
-            ca.gather_work[w] = (int)i;
-            ca.gather_cnt[w] = cnt;
-            return;
-        }
         uint32_t k[EV_CAP];
         const uint4* row = reinterpret_cast<const uint4*>(ca.ev_list + i * EV_CAP);
 #pragma unroll
@@ -1581,7 +1581,7 @@ __global__ void __launch_bounds__(HEAVY_TPB) k_contact_gather_heavy(ContactArray
     const int count = *ca.gather_count;
     for (int w = blockIdx.x; w < count; w += gridDim.x) {  // block-uniform
         const long long i = ca.gather_work[w];
-        const int cnt = ca.gather_cnt[w];
+        const int cnt = ca.ev_count[i];  // final: the force pass is done
         const long long n = ca.cnode[i];
         double acc = 0.0;  // thread d < 3: component d of the running sum
         bool walk = cnt > HEAVY_KEYS;
@@ -1629,7 +1629,8 @@ __global__ void __launch_bounds__(HEAVY_TPB) k_contact_gather_heavy(ContactArray
             f_out[3 * n + threadIdx.x] = acc;
             if (run_mode) ca.u_next[3 * n + threadIdx.x] = half_u(nd, ctls + nd.node_slot[n], n, threadIdx.x, acc);
         }
-        __syncthreads();
+        __syncthreads();  // every thread has read the count
+        if (threadIdx.x == 0) ca.ev_count[i] = 0;
     }
 }
 
@@ -1754,8 +1755,8 @@ void launch_elem_dt(cudaStream_t s, const ElementArrays& el, const NodeArrays& n
     if (el.n_all <= 0) return;
     k_elem_dt<<<active_grid(el.n_all, 1, DT_TPB, GRID_CAP), DT_TPB, 0, s>>>(el, nd, ctls, u, respect_done);
 }
-void launch_dt_finalize(cudaStream_t s, Control* ctls, int n_slots) {
-    k_dt_finalize<<<(unsigned)blocks_for(n_slots, 128), 128, 0, s>>>(ctls, n_slots);
+void launch_dt_finalize(cudaStream_t s, Control* ctls, int n_slots, int* mass_flag) {
+    k_dt_finalize<<<(unsigned)blocks_for(n_slots, 128), 128, 0, s>>>(ctls, n_slots, mass_flag);
 }
 void launch_mass_scaling(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, int force_apply) {
     k_mass_scaling<<<active_grid(nd.n, 1, TPB, GRID_CAP), TPB, 0, s>>>(el, nd, ctls, force_apply);
@@ -1769,8 +1770,8 @@ void launch_build_active(cudaStream_t s, const ActiveBuild& b, const Control* ct
     k_build_active<<<(unsigned)blocks_for(b.n_chunks, TPB), TPB, 0, s>>>(b, ctls);
 }
 void launch_step_end(cudaStream_t s, Control* ctls, const ContactArrays& ca, const VehicleArrays& va, int check_separation,
-                     int* done_out) {
-    k_step_end<<<(unsigned)blocks_for(ca.n_slots, 128), 128, 0, s>>>(ctls, ca, va, check_separation, done_out);
+                     int* done_out, int* mass_flag) {
+    k_step_end<<<(unsigned)blocks_for(ca.n_slots, 128), 128, 0, s>>>(ctls, ca, va, check_separation, done_out, mass_flag);
 }
 void launch_vehicle_sums(cudaStream_t s, const VehicleArrays& va, const double* mass, const double* v, const double* v0, double* out) {
     if (va.n_vehicles <= 0) return;
@@ -1842,7 +1843,7 @@ void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeAr
 
 void launch_contact_finish(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
                            long long n_faces, long long n_slaves, double dt_override, const double* masses, double* f_out,
-                           int skip_fixed) {
+                           int skip_fixed, cudaStream_t s_heavy, cudaEvent_t ev_a, cudaEvent_t ev_b) {
     if (c1 <= c0) return;
     const int run_mode = dt_override > 0.0 ? 0 : 1;
     (void)f0;
@@ -1852,10 +1853,21 @@ void launch_contact_finish(cudaStream_t s, const ContactArrays& ca, const NodeAr
         k_contact_force<<<active_grid(n_slaves, FORCE_LANES, TPB, GRID_CAP), TPB, 0, s>>>(ca, ctls, c0, run_mode, dt_override, masses,
                                                                                          n_slaves, skip_fixed);
     long long nodes = ca.n_cnodes > 0 ? ca.n_cnodes : 1;
+    // The heavy nodes (listed by the force pass) and the rest are disjoint:
+    // with a second stream the two gathers run side by side.
+    cudaStream_t sh = s_heavy ? s_heavy : s;
+    if (s_heavy) {
+        cudaEventRecord(ev_a, s);
+        cudaStreamWaitEvent(sh, ev_a, 0);
+    }
+    k_contact_gather_heavy<<<(unsigned)(nodes < HEAVY_BLOCKS ? nodes : HEAVY_BLOCKS), HEAVY_TPB, 0, sh>>>(ca, nd, ctls, c0, c1, run_mode,
+                                                                                                       f_out);
     k_contact_gather<<<active_grid(nodes, 1, GATHER_TPB, GRID_CAP * 2), GATHER_TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, f_out,
                                                                                           skip_fixed);
-    k_contact_gather_heavy<<<(unsigned)(nodes < HEAVY_BLOCKS ? nodes : HEAVY_BLOCKS), HEAVY_TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode,
-                                                                                                      f_out);
+    if (s_heavy) {
+        cudaEventRecord(ev_b, sh);
+        cudaStreamWaitEvent(s, ev_b, 0);
+    }
 }
 
 void launch_contact(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,

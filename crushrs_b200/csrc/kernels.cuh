@@ -51,6 +51,7 @@ struct NodeArrays {
     const uint32_t* all_off; // N+1 CSR over all model (element, corner) slots
     const uint32_t* all_slot;
     const uint32_t* node_slot;  // crash slot per node
+    const int* mass_flag;       // set when some crash scales its masses this step
     Active act_node;            // active chunks of nodes
 };
 
@@ -157,7 +158,6 @@ struct ContactArrays {
     double* u_next;             // 3N: the half step's u of every contact node, written by the run's gather
                                 //     (the next search reads it while the half step runs)
     int* gather_work;           // contact nodes with over EV_CAP events this pass (n_cnodes capacity)
-    int* gather_cnt;            // their event counts
     int* gather_count;          // their number (ev_pool_n + 1)
     Active act_slave, act_cnode, act_dynf;  // active chunks of grid-searched entries, contact nodes, moving faces
     Active act_allslave;        // active chunks of all primary-node entries (the force pass)
@@ -212,12 +212,14 @@ void launch_gather(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd
 void launch_half(cudaStream_t s, const NodeArrays& nd, Control* ctls);
 void launch_full(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls);
 void launch_elem_dt(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, const double* u, int respect_done);
-void launch_dt_finalize(cudaStream_t s, Control* ctls, int n_slots);
+// mass_flag: set when a crash scales its masses this step (k_mass_scaling
+// does nothing otherwise), cleared by the step's end.
+void launch_dt_finalize(cudaStream_t s, Control* ctls, int n_slots, int* mass_flag);
 void launch_mass_scaling(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, int force_apply);
 void launch_nonfinite(cudaStream_t s, const NodeArrays& nd, Control* ctls);
 void launch_build_active(cudaStream_t s, const ActiveBuild& b, const Control* ctls);
 void launch_step_end(cudaStream_t s, Control* ctls, const ContactArrays& ca, const VehicleArrays& va, int check_separation,
-                     int* done_out);
+                     int* done_out, int* mass_flag);
 // Contact pass over contacts [c0, c1) (faces [f0, f0 + n_faces), n_slaves
 // primary-node entries, dynamic grid buckets [bk0, bk1)); `lanes` lanes per
 // primary-node search (4, 8, 16 or 32). dt_override > 0 is a drop-in call: every face's
@@ -240,7 +242,8 @@ void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeAr
                            cudaStream_t s_static = nullptr);
 void launch_contact_finish(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
                            long long n_faces, long long n_slaves, double dt_override, const double* masses, double* f_out,
-                           int skip_fixed);
+                           int skip_fixed, cudaStream_t s_heavy = nullptr, cudaEvent_t ev_a = nullptr,
+                           cudaEvent_t ev_b = nullptr);
 int contact_search_launches(const ContactArrays& ca, bool run_mode, long long n_faces, long long n_slaves, long long bk0, long long bk1,
                             int c0);
 int contact_finish_launches(long long n_slaves);
