@@ -159,6 +159,19 @@ def dist_setup(backend=None):
     return world, rank, local
 
 
+def all_sum(x, world):
+    """Sum of x over the ranks."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def all_max(x, world):
     """Max of x over the ranks (the job's time is its slowest rank's)."""
     if world == 1:
@@ -249,17 +262,29 @@ def e2e_run(desc, device, n_hc, n_nodes):
             "delta_v": [r.vehicle[k].delta_v[0] for k in range(r.n_vehicles)]}
 
 
-def batched_section(n, plain_sample, oracle_sample, device):
+def batched_section(n, plain_sample, oracle_sample, device, world=1):
     """4096 seeded uneven head-on crashes in one batched context vs the plain
-    one-crash-per-launch path."""
+    one-crash-per-launch path. With several ranks the crashes are split by
+    estimated device bytes (serve.partition_by_footprint, the same on every
+    rank) and each rank runs its share as one batched context; the time is
+    the slowest rank's, with no collective on the data path."""
     from crushrs_b200 import scenarios as S
     from crushrs_b200.engine import Context
+    from crushrs_b200.serve import partition_by_footprint
 
-    models = [S.Model.build(S.batch_headon(i)) for i in range(n)]
+    all_models = [S.Model.build(S.batch_headon(i)) for i in range(n)]
+    if world > 1:
+        import torch.distributed as dist
+
+        mine = partition_by_footprint([m.desc for m in all_models], world)[dist.get_rank()]
+        models = [all_models[i] for i in mine]
+    else:
+        models = all_models
     elems = sum(m.n_hexes for m in models)
     w = Context(models[0].desc, device=device)  # CUDA and module warm-up
     w.run()
     w.close()
+    barrier(world)
     t0 = time.perf_counter()
     ctx = Context([m.desc for m in models], device=device)
     t1 = time.perf_counter()
@@ -270,6 +295,12 @@ def batched_section(n, plain_sample, oracle_sample, device):
     ctx.close()
     steps = [int(r.steps) for r in rs]
     eu = sum(m.n_hexes * st for m, st in zip(models, steps))
+    if world > 1:
+        wall = all_max(t2 - t0, world)
+        total_eu = all_sum(eu, world)
+        return {"crashes": n, "ranks": world, "crashes_this_rank": len(models), "crashes_per_s": n / wall, "wall_s": wall,
+                "elem_upd_per_s": total_eu / wall, "split": "by estimated device bytes, largest first to the least-loaded rank",
+                "scaling": "strong: the same crashes shared by the ranks"}
     # plain path: one context and one run per crash, a sample, after its own warm-up
     times = []
     same = True
@@ -383,8 +414,10 @@ def main():
 
     if "refined" not in sections:
         line = {"metric": METRIC, "sections": sorted(sections)}
-        if rank == 0 and world == 1 and args.batch > 0:
-            line["batched"] = batched_section(args.batch, args.plain_sample, args.oracle_sample, local)
+        if args.batch > 0:
+            b = batched_section(args.batch, args.plain_sample, args.oracle_sample, local, world)
+            if rank == 0:
+                line["batched"] = b
         if rank == 0 and world == 1 and args.serve_rates:
             line["serving"] = [serving_section(float(r), args.serve_seconds, local) for r in args.serve_rates.split(",") if r]
         if rank == 0:
@@ -441,8 +474,10 @@ def main():
         c3.close()
         line["e2e_dropin"] = {"value": e, "unit": "elem-upd/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                               "path": "crush_contact_apply x contacts + crush_compute_forces per step, host f64 state, pinned buffers"}
-    if rank == 0 and world == 1 and args.batch > 0:
-        line["batched"] = batched_section(args.batch, args.plain_sample, args.oracle_sample, local)
+    if args.batch > 0:
+        b = batched_section(args.batch, args.plain_sample, args.oracle_sample, local, world)
+        if rank == 0:
+            line["batched"] = b
     if rank == 0 and world == 1 and args.serve_rates:
         line["serving"] = [serving_section(float(r), args.serve_seconds, local) for r in args.serve_rates.split(",") if r]
     if rank == 0 and world == 1 and not args.no_cpu:

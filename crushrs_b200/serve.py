@@ -65,6 +65,21 @@ def footprint(desc):
     return lib().crush_model_footprint(C.byref(desc))
 
 
+def partition_by_footprint(descs, parts):
+    """Split crashes across `parts` GPUs by estimated device bytes: largest
+    first onto the least-loaded GPU (ties: the lower index), so every rank
+    computes the same split. Returns one list of crash indices per part,
+    each ascending."""
+    sizes = [footprint(d) for d in descs]
+    load = [0.0] * parts
+    out = [[] for _ in range(parts)]
+    for i in sorted(range(len(descs)), key=lambda k: (-sizes[k], k)):
+        g = min(range(parts), key=lambda q: (load[q], q))
+        out[g].append(i)
+        load[g] += sizes[i]
+    return [sorted(x) for x in out]
+
+
 def open_loop(server, models, rate, seed=1):
     """Submit `models` (objects with .desc) at Poisson arrival times of the
     given rate (req/s), open loop; returns (results by ticket, wall seconds,
