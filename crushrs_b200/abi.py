@@ -220,6 +220,11 @@ def declare_engine_api(lib):
     lib.crush_server_destroy.restype = None
     lib.crush_model_footprint.argtypes = [P(ModelDesc)]
     lib.crush_model_footprint.restype = C.c_double
+    lib.crush_history_config.argtypes = [vp, C.c_int, C.c_int, C.c_int64, C.c_int, P(Accelerometer)]
+    lib.crush_history_counts.argtypes = [vp, C.c_int, P(C.c_int64), P(C.c_int), P(C.c_int64)]
+    lib.crush_history_get.argtypes = [vp, C.c_int, dp, P(C.c_int64), P(PartState), P(NodeSample)]
+    lib.crush_cfc_filter.argtypes = [dp, C.c_int64, C.c_double, C.c_double, dp]
+    lib.crush_resample.argtypes = [dp, dp, C.c_int64, C.c_double, C.c_double, C.c_double, dp, dp, C.c_int64, P(C.c_int64)]
     lib.crush_contact_apply_static.argtypes = [C.c_int64, vp, vp, vp, C.c_int64, vp, vp, C.c_int64, vp,
                                                C.c_double, C.c_double, C.c_double, vp, vp, vp]
 
@@ -268,6 +273,42 @@ class Tuning(C.Structure):
         ("slave_lanes", C.c_int32),
         ("reserved", C.c_int32),
         ("contact_ms", C.c_double * 6),
+    ]
+
+
+class Accelerometer(C.Structure):
+    """crush_accelerometer (include/crush.h)."""
+    _fields_ = [
+        ("n_nodes", C.c_int64),
+        ("nodes", C.POINTER(C.c_uint32)),
+        ("has_frame", C.c_int32),
+        ("origin", C.c_uint32),
+        ("x_axis", C.c_uint32),
+        ("plane", C.c_uint32),
+    ]
+
+
+class PartState(C.Structure):
+    _fields_ = [
+        ("mass", C.c_double),
+        ("velocity", C.c_double * 3),
+        ("displacement", C.c_double * 3),
+        ("acceleration", C.c_double * 3),
+        ("kinetic_energy", C.c_double),
+    ]
+
+
+class NodeSample(C.Structure):
+    _fields_ = [
+        ("accelerometer", C.c_int32),
+        ("node", C.c_uint32),
+        ("position", C.c_double * 3),
+        ("displacement", C.c_double * 3),
+        ("velocity", C.c_double * 3),
+        ("acceleration", C.c_double * 3),
+        ("local_displacement", C.c_double * 3),
+        ("local_velocity", C.c_double * 3),
+        ("local_acceleration", C.c_double * 3),
     ]
 
 

@@ -104,7 +104,15 @@ struct Slot {
     crush_settings settings{};
     long long node0 = 0, n_nodes = 0, elem0 = 0, n_elems = 0;
     int contact0 = 0, n_contacts = 0, vehicle0 = 0, n_vehicles = 0;
+    int part0 = 0, n_parts = 0;  // the slot's parts in the concatenated part numbering
     double contact_dt = INF, stable = INF, dt_floor = 0.0, dt0 = 0.0;
+};
+
+// One slot's accelerometer (crush_accelerometer), node ids local to the slot.
+struct HistAccel {
+    std::vector<uint32_t> nodes;
+    int has_frame = 0;
+    uint32_t frame[3] = {0, 0, 0};
 };
 
 // Runs fn(i) for i in [0, n) on up to `hardware_concurrency` host threads
@@ -258,6 +266,15 @@ struct crush_ctx {
     bool run_open = false;
     long long host_step = 0;
     int period = 20;
+    int base_period = 20;            // the graph period without time histories
+    // time histories (crush_history_config)
+    std::vector<int> hist_steps;                 // per slot: history_steps, 0 = off
+    std::vector<long long> hist_max;             // per slot: records kept
+    std::vector<std::vector<HistAccel>> hist_acc;
+    HistoryArrays hist{};
+    bool hist_on = false;
+    bool hist_ran = false;                       // a run began since the configuration
+    std::vector<void*> hist_bufs;                // device buffers of `hist`
     cudaGraphExec_t graph = nullptr;
     int64_t graph_launches = 0;
     bool profiling = false;
@@ -774,6 +791,8 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
         sl.contact0 = K;
         sl.n_contacts = d->n_contacts;
         part0[k] = P;
+        sl.part0 = P;
+        sl.n_parts = d->n_parts;
         N += d->n_nodes;
         E += d->n_hexes;
         P += d->n_parts;
@@ -1276,6 +1295,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     trace.mark("initial stable step");
     c->period = std::lcm(c->check_steps, 20);
     if (c->period > 200) c->period = 0;  // no graph for odd periods
+    c->base_period = c->period;
     return CRUSH_OK;
 #undef TRY
 }
@@ -1365,6 +1385,12 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
     }
     launch_step_end(c->stream, c->ctls, cr, c->va, sep ? 1 : 0, c->slot_done, c->mass_flag);
     ++n;
+    // Time-history records of the slots whose step is a multiple of
+    // history_steps (src/solver.rs:349-351); u, v and the forces are final.
+    if (c->hist_on && (step + 1) % c->hist.steps == 0) {
+        launch_history(c->stream, c->hist, nd, c->ctls, c->f_ext, HIST_STEP);
+        n += (c->hist.n_pu > 0 ? 1 : 0) + 1;
+    }
     if (c->n_contacts > 0) {
         if (dt_next) cudaEventRecord(c->ev_join2, c->side2);
         cudaStreamWaitEvent(c->stream, c->ev_join, 0);
@@ -1439,6 +1465,108 @@ int autotune(crush_ctx* c) {
     return CRUSH_OK;
 }
 
+// Device structures of the time histories from the slots' configuration:
+// part units (each recording slot's parts and their element nodes, from the
+// device connectivity), accelerometer nodes and frames, record buffers.
+int rebuild_history(crush_ctx* c) {
+    for (void* p : c->hist_bufs) {
+        cudaFree(p);
+        c->allocs.erase(std::remove(c->allocs.begin(), c->allocs.end(), p), c->allocs.end());
+    }
+    c->hist_bufs.clear();
+    c->hist = HistoryArrays{};
+    c->hist_ran = false;
+    if (c->graph) {
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+    }
+    int steps = 0;
+    long long stride = 0;
+    for (int k = 0; k < c->n_slots; ++k)
+        if (c->hist_steps[k] > 0) {
+            steps = c->hist_steps[k];
+            stride = std::max(stride, c->hist_max[k]);
+        }
+    c->hist_on = steps > 0;
+    c->period = c->base_period;
+    if (!c->hist_on) return CRUSH_OK;
+    if (c->period > 0) {
+        c->period = std::lcm(c->period, steps);
+        if (c->period > 200) c->period = 0;  // no graph for odd periods
+    }
+    std::vector<int> on(c->n_slots), pu_slot_off(c->n_slots + 1, 0), an_off(c->n_slots + 1, 0), pu_slot, an_frame;
+    std::vector<long long> smax(c->n_slots, 0);
+    std::vector<uint32_t> pu_off(1, 0), pu_nodes, an_node, fr_nodes;
+    for (int k = 0; k < c->n_slots; ++k) {
+        const Slot& sl = c->slots[k];
+        on[k] = c->hist_steps[k] > 0;
+        smax[k] = on[k] ? c->hist_max[k] : 0;
+        if (on[k]) {
+            // part_nodes (src/mesh.rs:74-82): ascending nodes of each part's elements
+            std::vector<int32_t> part(sl.n_elems);
+            std::vector<uint32_t> conn(8 * sl.n_elems);
+            CK(cudaMemcpy(part.data(), c->part + sl.elem0, sizeof(int32_t) * sl.n_elems, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(conn.data(), c->conn_all + 8 * sl.elem0, sizeof(uint32_t) * 8 * sl.n_elems, cudaMemcpyDeviceToHost));
+            std::vector<std::vector<uint32_t>> nodes(sl.n_parts);
+            for (long long e = 0; e < sl.n_elems; ++e) {
+                const int p = part[e] - sl.part0;
+                if (p >= 0 && p < sl.n_parts) nodes[p].insert(nodes[p].end(), conn.begin() + 8 * e, conn.begin() + 8 * e + 8);
+            }
+            for (auto& v : nodes) {
+                std::sort(v.begin(), v.end());
+                v.erase(std::unique(v.begin(), v.end()), v.end());
+                pu_nodes.insert(pu_nodes.end(), v.begin(), v.end());
+                pu_off.push_back((uint32_t)pu_nodes.size());
+                pu_slot.push_back(k);
+            }
+            for (const HistAccel& a : c->hist_acc[k]) {
+                int f = -1;
+                if (a.has_frame) {
+                    f = (int)(fr_nodes.size() / 3);
+                    for (int j = 0; j < 3; ++j) fr_nodes.push_back((uint32_t)(sl.node0 + a.frame[j]));
+                }
+                for (uint32_t n : a.nodes) {
+                    an_node.push_back((uint32_t)(sl.node0 + n));
+                    an_frame.push_back(f);
+                }
+            }
+        }
+        pu_slot_off[k + 1] = (int)pu_slot.size();
+        an_off[k + 1] = (int)an_node.size();
+    }
+    HistoryArrays& h = c->hist;
+    h.n_slots = c->n_slots;
+    h.steps = steps;
+    h.max_rec = stride;
+    h.n_pu = (int)pu_slot.size();
+    h.n_an = (int)an_node.size();
+    const size_t mark = c->allocs.size();
+    auto up = [&](auto** dst, const auto& v) { return c->upload_const(dst, v); };
+    int st = CRUSH_OK;
+    if (st == CRUSH_OK) st = up(&h.slot_on, on);
+    if (st == CRUSH_OK) st = up(&h.slot_max, smax);
+    if (st == CRUSH_OK) st = up(&h.slot_pu_off, pu_slot_off);
+    if (st == CRUSH_OK) st = up(&h.slot_an_off, an_off);
+    if (st == CRUSH_OK) st = up(&h.pu_off, pu_off);
+    if (st == CRUSH_OK) st = up(&h.pu_nodes, pu_nodes);
+    if (st == CRUSH_OK) st = up(&h.pu_slot, pu_slot);
+    if (st == CRUSH_OK) st = up(&h.an_node, an_node);
+    if (st == CRUSH_OK) st = up(&h.an_frame, an_frame);
+    if (st == CRUSH_OK) st = up(&h.fr_nodes, fr_nodes);
+    if (st == CRUSH_OK) st = c->alloc(&h.partial, (size_t)std::max(h.n_pu, 1) * HIST_BLOCKS * HIST_PART_VALUES);
+    if (st == CRUSH_OK) st = c->alloc(&h.rec_count, c->n_slots);
+    if (st == CRUSH_OK) st = c->alloc(&h.last_step, c->n_slots);
+    if (st == CRUSH_OK) st = c->alloc(&h.rec_time, (size_t)c->n_slots * stride);
+    if (st == CRUSH_OK) st = c->alloc(&h.rec_step, (size_t)c->n_slots * stride);
+    if (st == CRUSH_OK) st = c->alloc(&h.part_rec, (size_t)std::max(h.n_pu, 1) * stride * HIST_PART_VALUES);
+    if (st == CRUSH_OK) st = c->alloc(&h.node_rec, (size_t)std::max(h.n_an, 1) * stride * HIST_NODE_VALUES);
+    c->hist_bufs.assign(c->allocs.begin() + (long)mark, c->allocs.end());
+    if (st != CRUSH_OK) return st;
+    CK(cudaMemsetAsync(h.rec_count, 0, sizeof(long long) * c->n_slots, c->stream));
+    CK(cudaMemsetAsync(h.last_step, 0xFF, sizeof(long long) * c->n_slots, c->stream));  // -1
+    return sync(c);
+}
+
 int run_begin(crush_ctx* c) {
     const long long N = c->n_nodes;
     if (c->graph) {
@@ -1510,6 +1638,27 @@ int run_begin(crush_ctx* c) {
     }
     st = search_now(c);
     if (st != CRUSH_OK) return st;
+    if (c->hist_on) {
+        // The run's first record (src/solver.rs:283-286): accelerations from
+        // the step-0 forces, contact included (the contact pass at u = 0 with
+        // the first dt, src/solver.rs:257-262), into scratch.
+        CK(cudaMemsetAsync(c->hist.rec_count, 0, sizeof(long long) * c->n_slots, c->stream));
+        CK(cudaMemsetAsync(c->hist.last_step, 0xFF, sizeof(long long) * c->n_slots, c->stream));
+        CK(cudaMemsetAsync(c->f_tmp, 0, sizeof(double) * 3 * N, c->stream));
+        if (c->n_contacts > 0) {
+            launch_contact_finish(c->stream, c->ca, c->nd(), c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves,
+                                  0.0, c->mass, c->f_tmp, 1);
+            st = check_launch(c, contact_finish_launches(c->n_slaves));
+            if (st != CRUSH_OK) return st;
+            // that pass counted penetrations; the run starts from none
+            CK(cudaMemsetAsync(c->ca.pen_count, 0, sizeof(unsigned long long) * c->n_contacts, c->stream));
+            CK(cudaMemsetAsync(c->ca.pen_max_bits, 0, sizeof(unsigned long long) * c->n_contacts, c->stream));
+        }
+        launch_history(c->stream, c->hist, c->nd(), c->ctls, c->f_tmp, HIST_INITIAL);
+        st = check_launch(c, (c->hist.n_pu > 0 ? 1 : 0) + 1);
+        if (st != CRUSH_OK) return st;
+        c->hist_ran = true;
+    }
     return sync(c);
 }
 
@@ -2003,6 +2152,142 @@ int crush_autotune(crush_ctx* c, crush_tuning* out) {
     int st = autotune(c);
     if (st != CRUSH_OK) return st;
     return crush_get_tuning(c, out);
+}
+
+int crush_history_config(crush_ctx* c, int slot, int history_steps, int64_t max_records, int n_acc, const crush_accelerometer* acc) {
+    if (!c) return crush::fail(CRUSH_ERR_INVALID, "null context");
+    if (slot < 0 || slot >= c->n_slots) return crush::fail(CRUSH_ERR_INVALID, "slot out of range");
+    if (c->run_open) return crush::fail(CRUSH_ERR_BUSY, "history configuration while a run is open");
+    if (history_steps < 0) return crush::fail(CRUSH_ERR_INVALID, "history_steps must be >= 0");
+    if (history_steps > 0 && (max_records < 1 || max_records > (1ll << 31)))
+        return crush::fail(CRUSH_ERR_INVALID, "max_records must be in [1, 2^31]");
+    if (n_acc < 0 || (n_acc > 0 && !acc)) return crush::fail(CRUSH_ERR_INVALID, "invalid accelerometer list");
+    const Slot& sl = c->slots[slot];
+    std::vector<HistAccel> list;
+    for (int k = 0; k < n_acc; ++k) {
+        const crush_accelerometer& a = acc[k];
+        if (a.n_nodes < 0 || (a.n_nodes > 0 && !a.nodes)) return crush::fail(CRUSH_ERR_INVALID, "invalid accelerometer nodes");
+        HistAccel h;
+        h.nodes.assign(a.nodes, a.nodes + a.n_nodes);
+        h.has_frame = a.has_frame ? 1 : 0;
+        h.frame[0] = a.origin;
+        h.frame[1] = a.x_axis;
+        h.frame[2] = a.plane;
+        // out-of-range nodes: the reference panics (src/solver.rs:245-248)
+        for (uint32_t n : h.nodes)
+            if (n >= (uint64_t)sl.n_nodes) return crush::fail(CRUSH_ERR_INVALID, "accelerometer node out of range");
+        if (h.has_frame)
+            for (uint32_t n : h.frame)
+                if (n >= (uint64_t)sl.n_nodes) return crush::fail(CRUSH_ERR_INVALID, "accelerometer frame node out of range");
+        list.push_back(std::move(h));
+    }
+    c->hist_steps.resize(c->n_slots, 0);
+    c->hist_max.resize(c->n_slots, 0);
+    c->hist_acc.resize(c->n_slots);
+    for (int k = 0; k < c->n_slots; ++k)
+        if (k != slot && history_steps > 0 && c->hist_steps[k] > 0 && c->hist_steps[k] != history_steps)
+            return crush::fail(CRUSH_ERR_UNSUPPORTED, "the recording slots of one context must share history_steps");
+    CK(cudaSetDevice(c->device));
+    c->hist_steps[slot] = history_steps;
+    c->hist_max[slot] = history_steps > 0 ? max_records : 0;
+    c->hist_acc[slot] = std::move(list);
+    return rebuild_history(c);
+}
+
+// The last-step record of finished crashes, when due (src/solver.rs:356-358).
+static int history_final(crush_ctx* c) {
+    launch_history(c->stream, c->hist, c->nd(), c->ctls, c->f_ext, HIST_FINAL);
+    return check_launch(c, (c->hist.n_pu > 0 ? 1 : 0) + 1);
+}
+
+int crush_history_counts(crush_ctx* c, int slot, int64_t* n_records, int* n_parts, int64_t* n_node_samples) {
+    if (!c) return crush::fail(CRUSH_ERR_INVALID, "null context");
+    if (slot < 0 || slot >= c->n_slots) return crush::fail(CRUSH_ERR_INVALID, "slot out of range");
+    CK(cudaSetDevice(c->device));
+    const bool on = c->hist_on && c->hist_ran && slot < (int)c->hist_steps.size() && c->hist_steps[slot] > 0;
+    long long count = 0;
+    if (on) {
+        int st = history_final(c);
+        if (st != CRUSH_OK) return st;
+        CK(cudaMemcpyAsync(&count, c->hist.rec_count + slot, sizeof(count), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    long long nodes = 0;
+    if (on)
+        for (const HistAccel& a : c->hist_acc[slot]) nodes += (long long)a.nodes.size();
+    if (n_records) *n_records = count;
+    if (n_parts) *n_parts = on ? c->slots[slot].n_parts : 0;
+    if (n_node_samples) *n_node_samples = nodes;
+    return CRUSH_OK;
+}
+
+int crush_history_get(crush_ctx* c, int slot, double* time, int64_t* step, crush_part_state* parts, crush_node_sample* samples) {
+    int64_t n_rec = 0, n_nodes = 0;
+    int n_parts = 0;
+    int st = crush_history_counts(c, slot, &n_rec, &n_parts, &n_nodes);
+    if (st != CRUSH_OK) return st;
+    if (n_rec == 0) return CRUSH_OK;
+    const HistoryArrays& h = c->hist;
+    const long long kept = std::min<long long>(n_rec, c->hist_max[slot]);
+    const long long stride = h.max_rec;
+    std::vector<long long> pu_off(c->n_slots + 1), an_off(c->n_slots + 1);
+    {
+        std::vector<int> a(c->n_slots + 1), b(c->n_slots + 1);
+        CK(cudaMemcpy(a.data(), h.slot_pu_off, sizeof(int) * a.size(), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(b.data(), h.slot_an_off, sizeof(int) * b.size(), cudaMemcpyDeviceToHost));
+        for (size_t k = 0; k < a.size(); ++k) {
+            pu_off[k] = a[k];
+            an_off[k] = b[k];
+        }
+    }
+    if (time) CK(cudaMemcpy(time, h.rec_time + slot * stride, sizeof(double) * kept, cudaMemcpyDeviceToHost));
+    if (step) {
+        std::vector<long long> s(kept);
+        CK(cudaMemcpy(s.data(), h.rec_step + slot * stride, sizeof(long long) * kept, cudaMemcpyDeviceToHost));
+        for (long long k = 0; k < kept; ++k) step[k] = s[k];
+    }
+    if (parts && n_parts > 0) {
+        std::vector<double> buf((size_t)n_parts * stride * HIST_PART_VALUES);
+        CK(cudaMemcpy(buf.data(), h.part_rec + pu_off[slot] * stride * HIST_PART_VALUES, sizeof(double) * buf.size(),
+                      cudaMemcpyDeviceToHost));
+        for (long long r = 0; r < kept; ++r)
+            for (int p = 0; p < n_parts; ++p) {
+                const double* v = &buf[((size_t)p * stride + r) * HIST_PART_VALUES];
+                crush_part_state& o = parts[r * n_parts + p];
+                o.mass = v[0];
+                for (int d = 0; d < 3; ++d) {
+                    o.velocity[d] = v[1 + d];
+                    o.displacement[d] = v[4 + d];
+                    o.acceleration[d] = v[7 + d];
+                }
+                o.kinetic_energy = v[10];
+            }
+    }
+    if (samples && n_nodes > 0) {
+        std::vector<double> buf((size_t)n_nodes * stride * HIST_NODE_VALUES);
+        CK(cudaMemcpy(buf.data(), h.node_rec + an_off[slot] * stride * HIST_NODE_VALUES, sizeof(double) * buf.size(),
+                      cudaMemcpyDeviceToHost));
+        std::vector<std::pair<int, uint32_t>> who;  // (accelerometer, node) of each sampled node
+        for (size_t k = 0; k < c->hist_acc[slot].size(); ++k)
+            for (uint32_t n : c->hist_acc[slot][k].nodes) who.push_back({(int)k, n});
+        for (long long r = 0; r < kept; ++r)
+            for (long long j = 0; j < n_nodes; ++j) {
+                const double* v = &buf[((size_t)j * stride + r) * HIST_NODE_VALUES];
+                crush_node_sample& o = samples[r * n_nodes + j];
+                o.accelerometer = who[j].first;
+                o.node = who[j].second;
+                for (int d = 0; d < 3; ++d) {
+                    o.position[d] = v[d];
+                    o.displacement[d] = v[3 + d];
+                    o.velocity[d] = v[6 + d];
+                    o.acceleration[d] = v[9 + d];
+                    o.local_displacement[d] = v[12 + d];
+                    o.local_velocity[d] = v[15 + d];
+                    o.local_acceleration[d] = v[18 + d];
+                }
+            }
+    }
+    return CRUSH_OK;
 }
 
 int crush_get_tuning(const crush_ctx* c, crush_tuning* out) {

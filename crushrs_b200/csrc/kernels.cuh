@@ -275,6 +275,45 @@ struct StaticContactScratch {
     int error;                         // 1: a node id was out of range (nothing is written)
 };
 
+// ---- Time histories (part states and accelerometer samples) ----
+// A part unit is one (crash slot, part) pair of a slot that records; its
+// nodes (the part's element nodes, ascending, src/mesh.rs:74-82) are reduced
+// by HIST_BLOCKS blocks into fixed-order partial sums, which the finishing
+// kernel adds in block order. Records are kept per slot in arrays of
+// max_rec entries.
+constexpr int HIST_BLOCKS = 32;
+constexpr int HIST_PART_VALUES = 11;  // mass, velocity 3, displacement 3, acceleration 3, kinetic energy
+constexpr int HIST_NODE_VALUES = 21;  // position, displacement, velocity, acceleration, local u, v, a (3 each)
+enum HistMode { HIST_INITIAL = 0, HIST_STEP = 1, HIST_FINAL = 2 };
+struct HistoryArrays {
+    int n_slots;
+    int steps;                  // history_steps shared by the recording slots
+    long long max_rec;          // record capacity per slot (the stride of the record arrays)
+    const int* slot_on;         // per slot: records
+    const long long* slot_max;  // per slot: records kept
+    const int* slot_pu_off;     // n_slots+1: the slot's part units
+    const int* slot_an_off;     // n_slots+1: the slot's accelerometer nodes
+    int n_pu;
+    const uint32_t* pu_off;     // n_pu+1 into pu_nodes
+    const uint32_t* pu_nodes;   // global node ids
+    const int* pu_slot;
+    double* partial;            // n_pu x HIST_BLOCKS x HIST_PART_VALUES
+    int n_an;
+    const uint32_t* an_node;    // global node id of each accelerometer node
+    const int* an_frame;        // frame of its accelerometer (-1: none)
+    const uint32_t* fr_nodes;   // 3 global node ids (origin, x axis, plane) per frame
+    long long* rec_count;       // per slot: records taken this run
+    long long* last_step;       // per slot: step of the last record (-1: none)
+    double* rec_time;           // n_slots x max_rec
+    long long* rec_step;        // n_slots x max_rec
+    double* part_rec;           // n_pu x max_rec x HIST_PART_VALUES
+    double* node_rec;           // n_an x max_rec x HIST_NODE_VALUES
+};
+// One record of every slot that is due (mode: the run's first record, a
+// step record every `steps` steps, or the last-step record of a finished
+// crash). f_ext is the external force the accelerations use.
+void launch_history(cudaStream_t s, const HistoryArrays& h, const NodeArrays& nd, const Control* ctls, const double* f_ext, int mode);
+
 // The call's kernels on `s`; every count is within the limits above.
 void launch_contact_static(cudaStream_t s, StaticContactScratch* sc, long long n_model_nodes, const double* pos, const double* u,
                            const double* masses, long long n_nodes, const uint32_t* nodes, const double* node_scale,

@@ -171,6 +171,48 @@ class Context:
         check(self._lib.crush_autotune(self.h, C.byref(t)))
         return t.slave_lanes, list(t.contact_ms)
 
+    def history_config(self, steps, max_records, accelerometers=(), slot=0):
+        """Record slot's part states and accelerometer nodes every `steps`
+        steps (include/crush.h crush_history_config). accelerometers: a list
+        of (nodes, frame) with frame None or (origin, x_axis, plane)."""
+        keep = []
+        arr = (abi.Accelerometer * max(len(accelerometers), 1))()
+        for k, (nodes, frame) in enumerate(accelerometers):
+            nodes = np.ascontiguousarray(nodes, dtype=np.uint32)
+            keep.append(nodes)
+            a = arr[k]
+            a.n_nodes = len(nodes)
+            a.nodes = nodes.ctypes.data_as(C.POINTER(C.c_uint32))
+            a.has_frame = 0 if frame is None else 1
+            if frame is not None:
+                a.origin, a.x_axis, a.plane = (int(x) for x in frame)
+        check(self._lib.crush_history_config(self.h, slot, steps, max_records, len(accelerometers), arr))
+        if not hasattr(self, "_hist_max"):
+            self._hist_max = {}
+        self._hist_max[slot] = max_records if steps > 0 else 0
+
+    def history(self, slot=0):
+        """The kept records: dict of numpy arrays time (R), step (R),
+        parts (R, P, 11: mass, velocity 3, displacement 3, acceleration 3,
+        kinetic energy) and nodes (R, J, 21: position, displacement,
+        velocity, acceleration, local displacement, velocity, acceleration),
+        plus the count of records taken."""
+        n_rec, n_parts, n_nodes = C.c_int64(), C.c_int(), C.c_int64()
+        check(self._lib.crush_history_counts(self.h, slot, C.byref(n_rec), C.byref(n_parts), C.byref(n_nodes)))
+        kept = min(n_rec.value, getattr(self, "_hist_max", {}).get(slot, 0))
+        t = np.zeros(max(kept, 1))
+        st = (C.c_int64 * max(kept, 1))()
+        ps = (abi.PartState * max(kept * n_parts.value, 1))()
+        ns = (abi.NodeSample * max(kept * n_nodes.value, 1))()
+        check(self._lib.crush_history_get(self.h, slot, _dp(t), st, ps, ns))
+        parts = np.ctypeslib.as_array(C.cast(ps, C.POINTER(C.c_double)), (max(kept * n_parts.value, 1) * 11,))
+        nodes = np.ctypeslib.as_array(C.cast(ns, C.POINTER(C.c_uint8)), (C.sizeof(abi.NodeSample) * max(kept * n_nodes.value, 1),))
+        node_vals = nodes.view(np.uint8).reshape(-1, C.sizeof(abi.NodeSample))[:, 8:].copy().view(np.float64)
+        return {"records": n_rec.value, "time": t[:kept].copy(), "step": np.array(st[:kept], dtype=np.int64),
+                "parts": parts[: kept * n_parts.value * 11].reshape(kept, n_parts.value, 11).copy(),
+                "nodes": node_vals[: kept * n_nodes.value].reshape(kept, n_nodes.value, 21),
+                "node_ids": np.array([ns[j].node for j in range(n_nodes.value)], dtype=np.uint32) if kept else np.zeros(0, np.uint32)}
+
     def set_contact_search(self, exhaustive):
         """True: every contact search tests every face (no broad phase)."""
         check(self._lib.crush_set_contact_search(self.h, int(bool(exhaustive))))

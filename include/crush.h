@@ -258,6 +258,66 @@ int crush_contact_search_stats(crush_ctx* ctx, int contact_id, uint64_t* out, in
  * narrow test. For checking that equality; takes effect at the next step. */
 int crush_set_contact_search(crush_ctx* ctx, int exhaustive);
 
+/* ---- Time histories: part states and accelerometer samples ----
+ * A sampled node set (Accelerometer, src/model.rs:64-73): `nodes` (model
+ * node ids) are recorded; with has_frame, also in the body-fixed frame of
+ * nodes origin / x_axis / plane (LocalFrame::axes, src/model.rs:45-61). */
+typedef struct crush_accelerometer {
+    int64_t n_nodes;
+    const uint32_t* nodes;
+    int32_t has_frame;
+    uint32_t origin, x_axis, plane;
+} crush_accelerometer;
+/* One part's state in one record (PartState, src/solver.rs:23-31): mass
+ * (lumped, no added mass) and the mass-weighted means of velocity,
+ * displacement and acceleration (net force / mass), and kinetic energy. */
+typedef struct crush_part_state {
+    double mass;
+    double velocity[3];
+    double displacement[3];
+    double acceleration[3];
+    double kinetic_energy;
+} crush_part_state;
+/* One accelerometer node in one record (a NodeHistory row,
+ * src/solver.rs:37-50); local_* repeat the global values without a frame. */
+typedef struct crush_node_sample {
+    int32_t accelerometer;
+    uint32_t node;
+    double position[3], displacement[3], velocity[3], acceleration[3];
+    double local_displacement[3], local_velocity[3], local_acceleration[3];
+} crush_node_sample;
+/* Records crash `slot` (0 for crush_create) every history_steps steps, on the
+ * device (Settings::history_steps and the record calls of
+ * src/solver.rs:283-286, :349-358): one record at step 0, one each step that
+ * is a multiple of history_steps, and one at the run's last step when that is
+ * not. A record holds time, step, every part's state (parts of the model, in
+ * order) and every accelerometer node's sample. Keeps up to max_records per
+ * run (later ones are counted, not kept). All configured slots of a context
+ * share history_steps; 0 turns a slot's recording off. Call between runs
+ * (not while a run is open); the accelerometer arrays are copied. Fixed
+ * nodes record zero acceleration (the reference's step-0 record keeps their
+ * contact reaction). */
+int crush_history_config(crush_ctx* ctx, int slot, int history_steps, int64_t max_records, int n_accelerometers,
+                         const crush_accelerometer* accelerometers);
+/* Sizes of slot's history of the last (or open) run: records taken
+ * (*n_records may exceed the kept ones, min(n_records, max_records)), parts
+ * per record and accelerometer nodes per record. Takes the last-step record
+ * of a finished crash first if it is due. */
+int crush_history_counts(crush_ctx* ctx, int slot, int64_t* n_records, int* n_parts, int64_t* n_node_samples);
+/* The kept records: time[k], step[k], parts[k * n_parts + p],
+ * samples[k * n_node_samples + j] (any pointer may be NULL). */
+int crush_history_get(crush_ctx* ctx, int slot, double* time, int64_t* step, crush_part_state* parts,
+                      crush_node_sample* samples);
+/* SAE J211 channel-frequency-class filter (cfc_filter, src/signal.rs:9-40):
+ * a 2-pole Butterworth run forward and backward with reflection padding;
+ * y may alias x. n < 4 copies x. */
+int crush_cfc_filter(const double* x, int64_t n, double dt, double cfc, double* y);
+/* Linear resampling of (t, y) (t ascending) onto t0 + k dt up to t_end
+ * (resample, src/signal.rs:42-66): writes min(cap, count) points and the
+ * count to *n_out. */
+int crush_resample(const double* t, const double* y, int64_t n, double t0, double dt, double t_end, double* tu, double* yu,
+                   int64_t cap, int64_t* n_out);
+
 /* Launch schedule of a context, chosen by the engine's autotuner (no
  * counterpart in the reference). The first crush_run_begin of a context times
  * the run's contact pass with 1, 2, 4, 8, 16 and 32 lanes per primary-node search

@@ -1,6 +1,7 @@
 // capi.cpp — TEST INFRASTRUCTURE ONLY (see oracle.hpp).
 // extern "C" entry points of the oracle, loaded by the tests and by the CPU
 // baseline leg of bench.py through ctypes.
+#include <algorithm>
 #include "oracle.hpp"
 #include <cstring>
 #include <memory>
@@ -252,6 +253,66 @@ int oracle_run(const crush_model_desc* d, int simd, int threads, crush_results* 
         seconds3[3] = r.loop_seconds;
     }
     return r.status;
+}
+
+// Whole run with time histories (solver.rs:114-187, :283-286, :349-358):
+// the records' times and steps (cap_records each), parts (cap x n_parts x 11)
+// and accelerometer node values (cap x n_acc_nodes x 21); *n_records = taken.
+int oracle_run_history(const crush_model_desc* d, int simd, int threads, int history_steps, int n_acc, const crush_accelerometer* acc,
+                       int64_t cap_records, double* time, int64_t* step, double* parts, double* nodes, int64_t* n_records,
+                       crush_results* out) {
+    Model m;
+    std::string e = model_from_desc(d, &m);
+    if (!e.empty()) return fail(e);
+    RunOptions opt;
+    opt.simd = simd != 0;
+    opt.threads = threads;
+    opt.history_steps = history_steps;
+    for (int k = 0; k < n_acc; ++k) {
+        HistoryAccel a;
+        a.nodes.assign(acc[k].nodes, acc[k].nodes + acc[k].n_nodes);
+        a.has_frame = acc[k].has_frame != 0;
+        a.origin = acc[k].origin;
+        a.x_axis = acc[k].x_axis;
+        a.plane = acc[k].plane;
+        opt.accelerometers.push_back(a);
+    }
+    RunResults r;
+    e = run(m, opt, &r);
+    if (!e.empty()) return fail(e);
+    const int64_t nr = (int64_t)r.hist_time.size();
+    *n_records = nr;
+    const size_t per_p = r.hist_parts.size() / std::max<int64_t>(nr, 1), per_n = r.hist_nodes.size() / std::max<int64_t>(nr, 1);
+    for (int64_t k = 0; k < nr && k < cap_records; ++k) {
+        time[k] = r.hist_time[k];
+        step[k] = r.hist_step[k];
+        std::memcpy(parts + k * per_p, r.hist_parts.data() + k * per_p, per_p * sizeof(double));
+        std::memcpy(nodes + k * per_n, r.hist_nodes.data() + k * per_n, per_n * sizeof(double));
+    }
+    if (out) {
+        std::memset(out, 0, sizeof(*out));
+        out->time = r.time;
+        out->steps = r.steps;
+        out->status = r.status;
+    }
+    return r.status;
+}
+
+// src/signal.rs:9-40 and :42-66.
+int oracle_cfc_filter(const double* x, int64_t n, double dt, double cfc, double* y) {
+    std::vector<double> in(x, x + n), outv = cfc_filter(in, dt, cfc);
+    std::memcpy(y, outv.data(), outv.size() * sizeof(double));
+    return 0;
+}
+int64_t oracle_resample(const double* t, const double* y, int64_t n, double t0, double dt, double t_end, double* tu, double* yu,
+                        int64_t cap) {
+    std::vector<double> tv(t, t + n), yv(y, y + n), a, b;
+    resample(tv, yv, t0, dt, t_end, &a, &b);
+    for (size_t k = 0; k < a.size() && (int64_t)k < cap; ++k) {
+        tu[k] = a[k];
+        yu[k] = b[k];
+    }
+    return (int64_t)a.size();
 }
 
 }  // extern "C"

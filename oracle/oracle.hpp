@@ -175,10 +175,17 @@ void contact_apply(ContactRuntime& c, const double* positions, const double* u, 
                    const double* masses, double dt, double* force);
 
 // ---------------- solver (src/solver.rs) ----------------
+struct HistoryAccel {  // Accelerometer, src/model.rs:64-73
+    std::vector<uint32_t> nodes;
+    bool has_frame = false;
+    uint32_t origin = 0, x_axis = 0, plane = 0;
+};
 struct RunOptions {
     bool simd = true;
     int threads = 1;
     bool log_steps = false;  // record dt per step
+    int history_steps = 0;   // Settings::history_steps
+    std::vector<HistoryAccel> accelerometers;
 };
 struct RunResults {
     double time = 0.0;
@@ -189,9 +196,19 @@ struct RunResults {
     int status = 0;
     std::vector<double> u, v, masses;
     std::vector<double> dt_log;
+    // history records (src/solver.rs:114-187): per record its time and step,
+    // n_parts x 11 part values (mass, v 3, u 3, a 3, ke) and per accelerometer
+    // node 21 values (x, u, v, a, local u, v, a)
+    std::vector<double> hist_time;
+    std::vector<int64_t> hist_step;
+    std::vector<double> hist_parts, hist_nodes;
     double force_seconds = 0.0, contact_seconds = 0.0, wall_seconds = 0.0, loop_seconds = 0.0;
 };
 std::string run(const Model& m, const RunOptions& opt, RunResults* r);
+// SAE J211 filter and resampling (src/signal.rs:9-66).
+std::vector<double> cfc_filter(const std::vector<double>& x, double dt, double cfc);
+void resample(const std::vector<double>& t, const std::vector<double>& y, double t0, double dt, double t_end, std::vector<double>* tu,
+              std::vector<double>* yu);
 // Delta-v / crush outputs (bin/crushrs.rs:237, :265).
 void vehicle_result(const Model& m, const RunResults& r, int vehicle, crush_vehicle_result* out);
 

@@ -1,5 +1,5 @@
 // solver.cpp — TEST INFRASTRUCTURE ONLY (see oracle.hpp).
-// Restates crushrs::run (src/solver.rs:190-381) without frames or history,
+// Restates crushrs::run (src/solver.rs:190-381) without frames,
 // plus the delta-v / crush outputs of src/bin/crushrs.rs:237-271 and the
 // separation stop rule of include/crush.h (CRUSH_STOP_SEPARATION), which the
 // reference does not have.
@@ -35,6 +35,35 @@ static double mean_vx(const std::vector<double>& masses, const double* v, const 
     double m = 0.0, p = 0.0;
     for (uint32_t n : nodes) { m += masses[n]; p += masses[n] * v[3 * n]; }
     return m > 0.0 ? p / m : 0.0;
+}
+
+// LocalFrame::axes, src/model.rs:45-61 (nalgebra's norm, normalize and
+// cross written out: sqrt of the ordered sum of squares, division by it).
+static void frame_axes(const double o[3], const double xa[3], const double pl[3], double ax[3][3]) {
+    auto norm = [](const double* a) { return std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]); };
+    auto cross = [](const double* a, const double* b, double* c) {
+        c[0] = a[1] * b[2] - a[2] * b[1];
+        c[1] = a[2] * b[0] - a[0] * b[2];
+        c[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    double e1[3], p[3], c[3], e2[3], e3[3];
+    for (int d = 0; d < 3; ++d) {
+        e1[d] = xa[d] - o[d];
+        p[d] = pl[d] - o[d];
+    }
+    if (norm(e1) < 1e-300) { e1[0] = 1.0; e1[1] = 0.0; e1[2] = 0.0; }
+    const double n1 = norm(e1);
+    for (double& x : e1) x /= n1;
+    cross(p, e1, c);
+    if (norm(c) < 1e-12 * std::fmax(norm(p), 1e-300)) {
+        const bool ux = std::fabs(e1[0]) < 0.9;
+        p[0] = ux ? 1.0 : 0.0; p[1] = ux ? 0.0 : 1.0; p[2] = 0.0;
+    }
+    cross(e1, p, e3);
+    const double n3 = norm(e3);
+    for (double& x : e3) x /= n3;
+    cross(e3, e1, e2);
+    for (int d = 0; d < 3; ++d) { ax[0][d] = e1[d]; ax[1][d] = e2[d]; ax[2][d] = e3[d]; }
 }
 
 std::string run(const Model& model, const RunOptions& opt, RunResults* res) {
@@ -85,6 +114,61 @@ std::string run(const Model& model, const RunOptions& opt, RunResults* res) {
     res->force_seconds = now_s() - tf;
     for (ContactRuntime& c : contacts) contact_apply(c, model.positions.data(), u.data(), v.data(), masses.data(), dt, f_ext.data());
     for (size_t k = 0; k < n; ++k) acc[k] = (f_ext[k] - f_int[k]) * inv_mass[k];
+
+    // Time histories: part_states and sample_accelerometers, src/solver.rs:114-187.
+    std::vector<std::vector<uint32_t>> part_nodes(model.materials.size());  // Mesh::part_nodes, src/mesh.rs:74-82
+    for (size_t p = 0; p < part_nodes.size(); ++p) {
+        std::set<uint32_t> set;
+        for (size_t e = 0; e < model.hexes.size(); ++e)
+            if (model.hex_part[e] == (int32_t)p) set.insert(model.hexes[e].begin(), model.hexes[e].end());
+        part_nodes[p].assign(set.begin(), set.end());
+    }
+    res->hist_time.clear();
+    res->hist_step.clear();
+    res->hist_parts.clear();
+    res->hist_nodes.clear();
+    auto record = [&](double tr, int64_t sr) {
+        res->hist_time.push_back(tr);
+        res->hist_step.push_back(sr);
+        for (const auto& nodes : part_nodes) {
+            double m = 0.0, mv[3] = {0, 0, 0}, mu[3] = {0, 0, 0}, ma[3] = {0, 0, 0}, ke = 0.0;
+            for (uint32_t nd : nodes) {
+                m += masses[nd];
+                for (int d = 0; d < 3; ++d) {
+                    mv[d] += masses[nd] * v[3 * nd + d];
+                    mu[d] += masses[nd] * u[3 * nd + d];
+                    ma[d] += masses[nd] * acc[3 * nd + d];
+                    ke += 0.5 * masses[nd] * v[3 * nd + d] * v[3 * nd + d];
+                }
+            }
+            const double inv = m > 0.0 ? 1.0 / m : 0.0;
+            res->hist_parts.push_back(m);
+            for (int d = 0; d < 3; ++d) res->hist_parts.push_back(mv[d] * inv);
+            for (int d = 0; d < 3; ++d) res->hist_parts.push_back(mu[d] * inv);
+            for (int d = 0; d < 3; ++d) res->hist_parts.push_back(ma[d] * inv);
+            res->hist_parts.push_back(ke);
+        }
+        auto x = [&](uint32_t nd, int d) { return model.positions[3 * nd + d] + u[3 * nd + d]; };
+        for (const HistoryAccel& a : opt.accelerometers) {
+            double ax[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+            if (a.has_frame) {
+                double o[3], xa[3], pl[3];
+                for (int d = 0; d < 3; ++d) { o[d] = x(a.origin, d); xa[d] = x(a.x_axis, d); pl[d] = x(a.plane, d); }
+                frame_axes(o, xa, pl, ax);
+            }
+            for (uint32_t nd : a.nodes) {
+                double un[3], vn[3], an[3];
+                for (int d = 0; d < 3; ++d) { un[d] = u[3 * nd + d]; vn[d] = v[3 * nd + d]; an[d] = acc[3 * nd + d]; }
+                for (int d = 0; d < 3; ++d) res->hist_nodes.push_back(x(nd, d));
+                for (const double* w : {un, vn, an})
+                    for (int d = 0; d < 3; ++d) res->hist_nodes.push_back(w[d]);
+                for (const double* w : {un, vn, an})
+                    for (int i = 0; i < 3; ++i)  // rotate, src/solver.rs:143-145
+                        res->hist_nodes.push_back(a.has_frame ? ax[i][0] * w[0] + ax[i][1] * w[1] + ax[i][2] * w[2] : w[i]);
+            }
+        }
+    };
+    if (opt.history_steps > 0) record(0.0, 0);
 
     // Separation rule bookkeeping: contacts whose faces are not all fixed.
     std::set<uint32_t> fixed_set(model.fixed_nodes.begin(), model.fixed_nodes.end());
@@ -150,6 +234,7 @@ std::string run(const Model& model, const RunOptions& opt, RunResults* res) {
         t += dt;
         dt_min = std::fmin(dt_min, dt);
         if (opt.log_steps) res->dt_log.push_back(dt);
+        if (opt.history_steps > 0 && step % opt.history_steps == 0) record(t, step);
         if (s.max_steps > 0 && step >= s.max_steps) break;
         if (s.stop_rule == CRUSH_STOP_SEPARATION && step % 10 == 0 && last_hit >= 0 && step - 1 - last_hit >= 100 &&
             model.vehicles.size() >= 2) {
@@ -158,6 +243,7 @@ std::string run(const Model& model, const RunOptions& opt, RunResults* res) {
             if (vb - va >= 0.0) break;
         }
     }
+    if (opt.history_steps > 0 && step % opt.history_steps != 0) record(t, step);
     res->time = t;
     res->steps = step;
     res->eroded = eroded_total;

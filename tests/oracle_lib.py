@@ -49,6 +49,11 @@ def load():
     lib.oracle_session_contact_apply.argtypes = [vp, C.c_int, dp, dp, dp, C.c_double, dp, P(C.c_int64), dp]
     lib.oracle_session_contact_nodes.argtypes = [vp, C.c_int, P(C.c_uint32), P(C.c_int64)]
     lib.oracle_run.argtypes = [P(abi.ModelDesc), C.c_int, C.c_int, P(abi.Results), dp, dp, dp, C.c_int64, dp]
+    lib.oracle_run_history.argtypes = [P(abi.ModelDesc), C.c_int, C.c_int, C.c_int, C.c_int, P(abi.Accelerometer), C.c_int64, dp,
+                                       P(C.c_int64), dp, dp, P(C.c_int64), P(abi.Results)]
+    lib.oracle_cfc_filter.argtypes = [dp, C.c_int64, C.c_double, C.c_double, dp]
+    lib.oracle_resample.argtypes = [dp, dp, C.c_int64, C.c_double, C.c_double, C.c_double, dp, dp, C.c_int64]
+    lib.oracle_resample.restype = C.c_int64
     _lib = lib
     return lib
 
@@ -185,3 +190,51 @@ def run(desc, simd=True, threads=1, want_state=False, want_dt=0):
     st = lib.oracle_run(C.byref(desc), int(simd), threads, C.byref(r), ptr(u), ptr(v), ptr(dt), want_dt, ptr(sec))
     assert st in (0, abi.CRUSH_ERR_NONFINITE), error()
     return r, u, v, dt, sec
+
+
+def run_history(desc, steps, accelerometers=(), cap=100000, simd=True, threads=1):
+    """Whole run with time histories: dict time (R), step (R), parts (R, P, 11),
+    nodes (R, J, 21), records, results. accelerometers: (nodes, frame|None)."""
+    lib = load()
+    arr = (abi.Accelerometer * max(len(accelerometers), 1))()
+    keep = []
+    n_nodes = 0
+    for k, (nodes, frame) in enumerate(accelerometers):
+        nodes = np.ascontiguousarray(nodes, dtype=np.uint32)
+        keep.append(nodes)
+        n_nodes += len(nodes)
+        arr[k].n_nodes = len(nodes)
+        arr[k].nodes = nodes.ctypes.data_as(C.POINTER(C.c_uint32))
+        arr[k].has_frame = 0 if frame is None else 1
+        if frame is not None:
+            arr[k].origin, arr[k].x_axis, arr[k].plane = (int(x) for x in frame)
+    n_parts = desc.n_parts
+    t = np.zeros(cap)
+    st = (C.c_int64 * cap)()
+    parts = np.zeros(cap * n_parts * 11)
+    nodes = np.zeros(max(cap * n_nodes * 21, 1))
+    nr = C.c_int64()
+    r = abi.Results()
+    status = lib.oracle_run_history(C.byref(desc), int(simd), threads, steps, len(accelerometers), arr, cap, ptr(t), st, ptr(parts),
+                                    ptr(nodes), C.byref(nr), C.byref(r))
+    assert status in (0, abi.CRUSH_ERR_NONFINITE), error()
+    k = min(nr.value, cap)
+    return {"records": nr.value, "time": t[:k], "step": np.array(st[:k], dtype=np.int64),
+            "parts": parts[: k * n_parts * 11].reshape(k, n_parts, 11), "nodes": nodes[: k * n_nodes * 21].reshape(k, n_nodes, 21),
+            "results": r}
+
+
+def cfc_filter(x, dt, cfc):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.empty_like(x)
+    load().oracle_cfc_filter(ptr(x), len(x), dt, cfc, ptr(y))
+    return y
+
+
+def resample(t, y, t0, dt, t_end):
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    n = load().oracle_resample(ptr(t), ptr(y), len(t), t0, dt, t_end, None, None, 0)
+    tu, yu = np.empty(n), np.empty(n)
+    load().oracle_resample(ptr(t), ptr(y), len(t), t0, dt, t_end, ptr(tu), ptr(yu), n)
+    return tu, yu
