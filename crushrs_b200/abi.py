@@ -223,6 +223,10 @@ def declare_engine_api(lib):
     lib.crush_history_config.argtypes = [vp, C.c_int, C.c_int, C.c_int64, C.c_int, P(Accelerometer)]
     lib.crush_history_counts.argtypes = [vp, C.c_int, P(C.c_int64), P(C.c_int), P(C.c_int64)]
     lib.crush_history_get.argtypes = [vp, C.c_int, dp, P(C.c_int64), P(PartState), P(NodeSample)]
+    lib.crush_frames_config.argtypes = [vp, C.c_int, C.c_int, C.c_int64]
+    lib.crush_frames_count.argtypes = [vp, C.c_int, P(C.c_int64)]
+    lib.crush_frame_get.argtypes = [vp, C.c_int, C.c_int64, dp, P(C.c_int64), P(C.c_float), P(C.c_float), P(C.c_float),
+                                    P(C.c_uint8)]
     lib.crush_cfc_filter.argtypes = [dp, C.c_int64, C.c_double, C.c_double, dp]
     lib.crush_resample.argtypes = [dp, dp, C.c_int64, C.c_double, C.c_double, C.c_double, dp, dp, C.c_int64, P(C.c_int64)]
     lib.crush_contact_apply_static.argtypes = [C.c_int64, vp, vp, vp, C.c_int64, vp, vp, C.c_int64, vp,

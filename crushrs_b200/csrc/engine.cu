@@ -275,6 +275,12 @@ struct crush_ctx {
     bool hist_on = false;
     bool hist_ran = false;                       // a run began since the configuration
     std::vector<void*> hist_bufs;                // device buffers of `hist`
+    // frames (crush_frames_config)
+    std::vector<int> frame_steps;                // per slot, 0 = off
+    std::vector<long long> frame_max;
+    FrameArrays frames{};
+    bool frames_on = false, frames_ran = false;
+    std::vector<void*> frame_bufs;
     cudaGraphExec_t graph = nullptr;
     int64_t graph_launches = 0;
     bool profiling = false;
@@ -1391,6 +1397,11 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
         launch_history(c->stream, c->hist, nd, c->ctls, c->f_ext, HIST_STEP);
         n += (c->hist.n_pu > 0 ? 1 : 0) + 1;
     }
+    // Frames at multiples of frame_steps (src/solver.rs:345-348).
+    if (c->frames_on && (step + 1) % c->frames.steps == 0) {
+        launch_frames(c->stream, c->frames, c->u, c->ctls, HIST_STEP);
+        n += 3;
+    }
     if (c->n_contacts > 0) {
         if (dt_next) cudaEventRecord(c->ev_join2, c->side2);
         cudaStreamWaitEvent(c->stream, c->ev_join, 0);
@@ -1465,15 +1476,107 @@ int autotune(crush_ctx* c) {
     return CRUSH_OK;
 }
 
+// The step graph's period: the dt-check and active-list cadences and the
+// recording cadences of histories and frames; no graph beyond 200 steps.
+void update_period(crush_ctx* c) {
+    long long p = c->base_period;
+    if (p > 0 && c->hist_on) p = std::lcm(p, (long long)c->hist.steps);
+    if (p > 0 && c->frames_on) p = std::lcm(p, (long long)c->frames.steps);
+    c->period = p > 200 ? 0 : (int)p;
+}
+
+static void free_bufs(crush_ctx* c, std::vector<void*>& bufs) {
+    for (void* p : bufs) {
+        cudaFree(p);
+        c->allocs.erase(std::remove(c->allocs.begin(), c->allocs.end(), p), c->allocs.end());
+    }
+    bufs.clear();
+}
+
+// Device structures of the frames from the slots' configuration.
+int rebuild_frames(crush_ctx* c) {
+    free_bufs(c, c->frame_bufs);
+    c->frames = FrameArrays{};
+    c->frames_ran = false;
+    if (c->graph) {
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+    }
+    int steps = 0;
+    long long stride = 0, max3n = 1, maxe = 1;
+    std::vector<int> on(c->n_slots);
+    std::vector<long long> smax(c->n_slots), node0(c->n_slots), nn(c->n_slots), elem0(c->n_slots), ne(c->n_slots),
+        dbase(c->n_slots), ebase(c->n_slots);
+    long long dtot = 0, etot = 0;
+    for (int k = 0; k < c->n_slots; ++k) {
+        const Slot& sl = c->slots[k];
+        on[k] = c->frame_steps[k] > 0;
+        smax[k] = on[k] ? c->frame_max[k] : 0;
+        if (on[k]) {
+            steps = c->frame_steps[k];
+            stride = std::max(stride, smax[k]);
+            max3n = std::max(max3n, 3 * sl.n_nodes);
+            maxe = std::max(maxe, sl.n_elems);
+        }
+        node0[k] = sl.node0;
+        nn[k] = sl.n_nodes;
+        elem0[k] = sl.elem0;
+        ne[k] = sl.n_elems;
+        dbase[k] = dtot;
+        ebase[k] = etot;
+        dtot += smax[k] * 3 * sl.n_nodes;
+        etot += smax[k] * sl.n_elems;
+    }
+    c->frames_on = steps > 0;
+    c->frames.steps = steps;
+    update_period(c);
+    if (!c->frames_on) return CRUSH_OK;
+    FrameArrays& f = c->frames;
+    f.n_slots = c->n_slots;
+    f.steps = steps;
+    f.stride = stride;
+    f.hc_index = c->hc_index_d;
+    f.eroded_all = c->eroded_all;
+    f.state = c->state;
+    f.state_stride = c->stride;
+    f.node_blocks = (int)std::min<long long>(1024, (max3n + 4095) / 4096);
+    f.elem_blocks = (int)std::min<long long>(1024, (maxe + 2047) / 2048);
+    const size_t mark = c->allocs.size();
+    int st = CRUSH_OK;
+    if (st == CRUSH_OK) st = c->upload_const(&f.slot_on, on);
+    if (st == CRUSH_OK) st = c->upload_const(&f.slot_max, smax);
+    if (st == CRUSH_OK) st = c->upload_const(&f.node0, node0);
+    if (st == CRUSH_OK) st = c->upload_const(&f.n_nodes, nn);
+    if (st == CRUSH_OK) st = c->upload_const(&f.elem0, elem0);
+    if (st == CRUSH_OK) st = c->upload_const(&f.n_elems, ne);
+    if (st == CRUSH_OK) st = c->upload_const(&f.disp_base, dbase);
+    if (st == CRUSH_OK) st = c->upload_const(&f.elem_base, ebase);
+    if (st == CRUSH_OK) st = c->alloc(&f.count, c->n_slots);
+    if (st == CRUSH_OK) st = c->alloc(&f.last_step, c->n_slots);
+    if (st == CRUSH_OK) st = c->alloc(&f.time, (size_t)c->n_slots * stride);
+    if (st == CRUSH_OK) st = c->alloc(&f.step, (size_t)c->n_slots * stride);
+    if (st == CRUSH_OK) st = c->alloc(&f.disp, (size_t)std::max<long long>(dtot, 1));
+    if (st == CRUSH_OK) st = c->alloc(&f.pstrain, (size_t)std::max<long long>(etot, 1));
+    if (st == CRUSH_OK) st = c->alloc(&f.stress, 6 * (size_t)std::max<long long>(etot, 1));
+    if (st == CRUSH_OK) st = c->alloc(&f.eroded, (size_t)std::max<long long>(etot, 1));
+    c->frame_bufs.assign(c->allocs.begin() + (long)mark, c->allocs.end());
+    if (st != CRUSH_OK) {
+        free_bufs(c, c->frame_bufs);
+        c->frames = FrameArrays{};
+        c->frames_on = false;
+        update_period(c);
+        return st;
+    }
+    CK(cudaMemsetAsync(f.count, 0, sizeof(long long) * c->n_slots, c->stream));
+    CK(cudaMemsetAsync(f.last_step, 0xFF, sizeof(long long) * c->n_slots, c->stream));  // -1
+    return sync(c);
+}
+
 // Device structures of the time histories from the slots' configuration:
 // part units (each recording slot's parts and their element nodes, from the
 // device connectivity), accelerometer nodes and frames, record buffers.
 int rebuild_history(crush_ctx* c) {
-    for (void* p : c->hist_bufs) {
-        cudaFree(p);
-        c->allocs.erase(std::remove(c->allocs.begin(), c->allocs.end(), p), c->allocs.end());
-    }
-    c->hist_bufs.clear();
+    free_bufs(c, c->hist_bufs);
     c->hist = HistoryArrays{};
     c->hist_ran = false;
     if (c->graph) {
@@ -1488,12 +1591,9 @@ int rebuild_history(crush_ctx* c) {
             stride = std::max(stride, c->hist_max[k]);
         }
     c->hist_on = steps > 0;
-    c->period = c->base_period;
+    c->hist.steps = steps;
+    update_period(c);
     if (!c->hist_on) return CRUSH_OK;
-    if (c->period > 0) {
-        c->period = std::lcm(c->period, steps);
-        if (c->period > 200) c->period = 0;  // no graph for odd periods
-    }
     std::vector<int> on(c->n_slots), pu_slot_off(c->n_slots + 1, 0), an_off(c->n_slots + 1, 0), pu_slot, an_frame;
     std::vector<long long> smax(c->n_slots, 0);
     std::vector<uint32_t> pu_off(1, 0), pu_nodes, an_node, fr_nodes;
@@ -1658,6 +1758,15 @@ int run_begin(crush_ctx* c) {
         st = check_launch(c, (c->hist.n_pu > 0 ? 1 : 0) + 1);
         if (st != CRUSH_OK) return st;
         c->hist_ran = true;
+    }
+    if (c->frames_on) {
+        // the run's first frame (src/solver.rs:265-276), after the step-0 forces
+        CK(cudaMemsetAsync(c->frames.count, 0, sizeof(long long) * c->n_slots, c->stream));
+        CK(cudaMemsetAsync(c->frames.last_step, 0xFF, sizeof(long long) * c->n_slots, c->stream));
+        launch_frames(c->stream, c->frames, c->u, c->ctls, HIST_INITIAL);
+        st = check_launch(c, 3);
+        if (st != CRUSH_OK) return st;
+        c->frames_ran = true;
     }
     return sync(c);
 }
@@ -2287,6 +2396,70 @@ int crush_history_get(crush_ctx* c, int slot, double* time, int64_t* step, crush
                 }
             }
     }
+    return CRUSH_OK;
+}
+
+int crush_frames_config(crush_ctx* c, int slot, int frame_steps, int64_t max_frames) {
+    if (!c) return crush::fail(CRUSH_ERR_INVALID, "null context");
+    if (slot < 0 || slot >= c->n_slots) return crush::fail(CRUSH_ERR_INVALID, "slot out of range");
+    if (c->run_open) return crush::fail(CRUSH_ERR_BUSY, "frame configuration while a run is open");
+    if (frame_steps < 0) return crush::fail(CRUSH_ERR_INVALID, "frame_steps must be >= 0");
+    if (frame_steps > 0 && (max_frames < 1 || max_frames > (1ll << 31)))
+        return crush::fail(CRUSH_ERR_INVALID, "max_frames must be in [1, 2^31]");
+    if (frame_steps > 0 && c->n_slots > 65535) return crush::fail(CRUSH_ERR_UNSUPPORTED, "frames need at most 65535 crashes per context");
+    c->frame_steps.resize(c->n_slots, 0);
+    c->frame_max.resize(c->n_slots, 0);
+    for (int k = 0; k < c->n_slots; ++k)
+        if (k != slot && frame_steps > 0 && c->frame_steps[k] > 0 && c->frame_steps[k] != frame_steps)
+            return crush::fail(CRUSH_ERR_UNSUPPORTED, "the capturing slots of one context must share frame_steps");
+    CK(cudaSetDevice(c->device));
+    c->frame_steps[slot] = frame_steps;
+    c->frame_max[slot] = frame_steps > 0 ? max_frames : 0;
+    return rebuild_frames(c);
+}
+
+int crush_frames_count(crush_ctx* c, int slot, int64_t* n_frames) {
+    if (!c || !n_frames) return crush::fail(CRUSH_ERR_INVALID, "null argument");
+    if (slot < 0 || slot >= c->n_slots) return crush::fail(CRUSH_ERR_INVALID, "slot out of range");
+    *n_frames = 0;
+    if (!c->frames_on || !c->frames_ran || slot >= (int)c->frame_steps.size() || c->frame_steps[slot] == 0) return CRUSH_OK;
+    CK(cudaSetDevice(c->device));
+    launch_frames(c->stream, c->frames, c->u, c->ctls, HIST_FINAL);  // the last step's frame (src/solver.rs:353-355)
+    int st = check_launch(c, 3);
+    if (st != CRUSH_OK) return st;
+    long long n = 0;
+    CK(cudaMemcpyAsync(&n, c->frames.count + slot, sizeof(n), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    *n_frames = n;
+    return CRUSH_OK;
+}
+
+int crush_frame_get(crush_ctx* c, int slot, int64_t frame, double* time, int64_t* step, float* displacement, float* plastic_strain,
+                    float* stress, uint8_t* eroded) {
+    int64_t n = 0;
+    int st = crush_frames_count(c, slot, &n);
+    if (st != CRUSH_OK) return st;
+    if (frame < 0 || frame >= std::min<int64_t>(n, c->frame_max.empty() ? 0 : c->frame_max[slot]))
+        return crush::fail(CRUSH_ERR_INVALID, "frame not kept");
+    const Slot& sl = c->slots[slot];
+    const FrameArrays& f = c->frames;
+    long long dbase = 0, ebase = 0;
+    for (int k = 0; k < slot; ++k) {
+        dbase += (c->frame_steps[k] > 0 ? c->frame_max[k] : 0) * 3 * c->slots[k].n_nodes;
+        ebase += (c->frame_steps[k] > 0 ? c->frame_max[k] : 0) * c->slots[k].n_elems;
+    }
+    const long long e_off = ebase + frame * sl.n_elems;
+    if (time) CK(cudaMemcpy(time, f.time + slot * f.stride + frame, sizeof(double), cudaMemcpyDeviceToHost));
+    if (step) {
+        long long s = 0;
+        CK(cudaMemcpy(&s, f.step + slot * f.stride + frame, sizeof(long long), cudaMemcpyDeviceToHost));
+        *step = s;
+    }
+    if (displacement)
+        CK(cudaMemcpy(displacement, f.disp + dbase + frame * 3 * sl.n_nodes, sizeof(float) * 3 * sl.n_nodes, cudaMemcpyDeviceToHost));
+    if (plastic_strain) CK(cudaMemcpy(plastic_strain, f.pstrain + e_off, sizeof(float) * sl.n_elems, cudaMemcpyDeviceToHost));
+    if (stress) CK(cudaMemcpy(stress, f.stress + 6 * e_off, sizeof(float) * 6 * sl.n_elems, cudaMemcpyDeviceToHost));
+    if (eroded) CK(cudaMemcpy(eroded, f.eroded + e_off, sl.n_elems, cudaMemcpyDeviceToHost));
     return CRUSH_OK;
 }
 

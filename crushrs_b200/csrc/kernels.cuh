@@ -314,6 +314,37 @@ struct HistoryArrays {
 // crash). f_ext is the external force the accelerations use.
 void launch_history(cudaStream_t s, const HistoryArrays& h, const NodeArrays& nd, const Control* ctls, const double* f_ext, int mode);
 
+// ---- Frames: nodal displacement and element plastic strain, Cauchy
+// stress and erosion every frame_steps steps (Frame, src/solver.rs) ----
+struct FrameArrays {
+    int n_slots;
+    int steps;                  // frame_steps shared by the capturing slots
+    long long stride;           // frame capacity per slot (stride of time / step)
+    const int* slot_on;
+    const long long* slot_max;  // frames kept per slot
+    const long long* node0;     // per slot: first node, node count
+    const long long* n_nodes;
+    const long long* elem0;     // per slot: first model element, element count
+    const long long* n_elems;
+    const long long* disp_base; // per slot: float offset of its frames' displacements (max x 3 n_nodes)
+    const long long* elem_base; // per slot: offset of its frames' element records (max x n_elems)
+    long long* count;           // per slot: frames taken this run
+    long long* last_step;       // per slot: step of the last frame (-1: none)
+    double* time;               // n_slots x stride
+    long long* step;
+    float* disp;                // displacement (f32 of u)
+    float* pstrain;             // plastic strain (compaction; 0 for elastic elements)
+    float* stress;              // Cauchy stress, Voigt xx yy zz xy yz xz (0 when eroded)
+    uint8_t* eroded;
+    const int64_t* hc_index;    // model element -> honeycomb index or -1
+    const uint8_t* eroded_all;  // per model element
+    const float4* state;        // honeycomb state planes
+    long long state_stride;
+    int node_blocks, elem_blocks;  // blocks per slot of the two copy kernels
+};
+// One frame of every slot that is due (modes as for the histories).
+void launch_frames(cudaStream_t s, const FrameArrays& f, const double* u, const Control* ctls, int mode);
+
 // The call's kernels on `s`; every count is within the limits above.
 void launch_contact_static(cudaStream_t s, StaticContactScratch* sc, long long n_model_nodes, const double* pos, const double* u,
                            const double* masses, long long n_nodes, const uint32_t* nodes, const double* node_scale,

@@ -213,6 +213,35 @@ class Context:
                 "nodes": node_vals[: kept * n_nodes.value].reshape(kept, n_nodes.value, 21),
                 "node_ids": np.array([ns[j].node for j in range(n_nodes.value)], dtype=np.uint32) if kept else np.zeros(0, np.uint32)}
 
+    def frames_config(self, steps, max_frames, slot=0):
+        """Capture slot's frames every `steps` steps (crush_frames_config)."""
+        check(self._lib.crush_frames_config(self.h, slot, steps, max_frames))
+        if not hasattr(self, "_frame_max"):
+            self._frame_max = {}
+        self._frame_max[slot] = max_frames if steps > 0 else 0
+
+    def frames_count(self, slot=0):
+        n = C.c_int64()
+        check(self._lib.crush_frames_count(self.h, slot, C.byref(n)))
+        return n.value
+
+    def frame(self, k, slot=0, n_nodes=None, n_hexes=None):
+        """Kept frame k: time, step, displacement (N, 3), plastic_strain (E),
+        stress (E, 6: xx yy zz xy yz xz), eroded (E); sizes default to the
+        context's (a single-model context)."""
+        nn = self.n_nodes if n_nodes is None else n_nodes
+        ne = self.n_hexes if n_hexes is None else n_hexes
+        t, st = C.c_double(), C.c_int64()
+        d = np.zeros(3 * nn, np.float32)
+        ps = np.zeros(ne, np.float32)
+        sg = np.zeros(6 * ne, np.float32)
+        er = np.zeros(ne, np.uint8)
+        fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+        check(self._lib.crush_frame_get(self.h, slot, k, C.byref(t), C.byref(st), fp(d), fp(ps), fp(sg),
+                                        er.ctypes.data_as(C.POINTER(C.c_uint8))))
+        return {"time": t.value, "step": st.value, "displacement": d.reshape(nn, 3), "plastic_strain": ps,
+                "stress": sg.reshape(ne, 6), "eroded": er}
+
     def set_contact_search(self, exhaustive):
         """True: every contact search tests every face (no broad phase)."""
         check(self._lib.crush_set_contact_search(self.h, int(bool(exhaustive))))

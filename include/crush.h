@@ -308,6 +308,24 @@ int crush_history_counts(crush_ctx* ctx, int slot, int64_t* n_records, int* n_pa
  * samples[k * n_node_samples + j] (any pointer may be NULL). */
 int crush_history_get(crush_ctx* ctx, int slot, double* time, int64_t* step, crush_part_state* parts,
                       crush_node_sample* samples);
+/* Frames of crash `slot` (Frame and its capture in crushrs::run,
+ * src/solver.rs:52-60, :265-281, :345-355; Settings::frame_steps): at step
+ * 0, every frame_steps steps and at the last step when that is not a
+ * multiple, the device copies the nodal displacement (f32, 3 per node) and
+ * per element the plastic strain (honeycomb compaction; 0 for elastic
+ * elements), the Cauchy stress R sigma_hat R^T (Voigt xx yy zz xy yz xz,
+ * f32; zero when eroded, src/kernel.rs:269-321) and the erosion flag into
+ * buffers of max_frames frames (later frames are counted, not kept).
+ * Capturing slots of a context share frame_steps; 0 turns a slot off. Call
+ * between runs. Node and element indices are the slot's model's. */
+int crush_frames_config(crush_ctx* ctx, int slot, int frame_steps, int64_t max_frames);
+/* Frames of the last (or open) run taken so far (kept: min with max_frames);
+ * takes the last-step frame of a finished crash first if it is due. */
+int crush_frames_count(crush_ctx* ctx, int slot, int64_t* n_frames);
+/* Kept frame `frame`: time, step, displacement (3 n_nodes), plastic_strain,
+ * stress (6 per element), eroded (n_hexes each); any pointer may be NULL. */
+int crush_frame_get(crush_ctx* ctx, int slot, int64_t frame, double* time, int64_t* step, float* displacement,
+                    float* plastic_strain, float* stress, uint8_t* eroded);
 /* SAE J211 channel-frequency-class filter (cfc_filter, src/signal.rs:9-40):
  * a 2-pole Butterworth run forward and backward with reflection padding;
  * y may alias x. n < 4 copies x. */

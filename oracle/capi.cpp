@@ -298,6 +298,35 @@ int oracle_run_history(const crush_model_desc* d, int simd, int threads, int his
     return r.status;
 }
 
+// Whole run with frames every frame_steps (src/solver.rs:265-281): frame k's
+// time, step, displacement (3N), plastic strain (E), stress (6E), eroded (E)
+// into cap-frame arrays; returns the frames taken in *n_frames.
+int oracle_run_frames(const crush_model_desc* d, int simd, int threads, int frame_steps, int64_t cap, double* time, int64_t* step,
+                      float* disp, float* pstrain, float* stress, uint8_t* eroded, int64_t* n_frames) {
+    Model m;
+    std::string e = model_from_desc(d, &m);
+    if (!e.empty()) return fail(e);
+    RunOptions opt;
+    opt.simd = simd != 0;
+    opt.threads = threads;
+    opt.frame_steps = frame_steps;
+    RunResults r;
+    e = run(m, opt, &r);
+    if (!e.empty()) return fail(e);
+    const int64_t nf = (int64_t)r.frame_time.size();
+    *n_frames = nf;
+    const size_t n3 = 3 * m.n_nodes(), ne = m.hexes.size();
+    for (int64_t k = 0; k < nf && k < cap; ++k) {
+        time[k] = r.frame_time[k];
+        step[k] = r.frame_step[k];
+        std::memcpy(disp + k * n3, r.frame_disp.data() + k * n3, n3 * sizeof(float));
+        std::memcpy(pstrain + k * ne, r.frame_pstrain.data() + k * ne, ne * sizeof(float));
+        std::memcpy(stress + 6 * k * ne, r.frame_stress.data() + 6 * k * ne, 6 * ne * sizeof(float));
+        std::memcpy(eroded + k * ne, r.frame_eroded.data() + k * ne, ne);
+    }
+    return r.status;
+}
+
 // src/signal.rs:9-40 and :42-66.
 int oracle_cfc_filter(const double* x, int64_t n, double dt, double cfc, double* y) {
     std::vector<double> in(x, x + n), outv = cfc_filter(in, dt, cfc);

@@ -186,6 +186,7 @@ struct RunOptions {
     bool log_steps = false;  // record dt per step
     int history_steps = 0;   // Settings::history_steps
     std::vector<HistoryAccel> accelerometers;
+    int frame_steps = 0;     // Settings::frame_steps
 };
 struct RunResults {
     double time = 0.0;
@@ -202,6 +203,12 @@ struct RunResults {
     std::vector<double> hist_time;
     std::vector<int64_t> hist_step;
     std::vector<double> hist_parts, hist_nodes;
+    // frames (src/solver.rs:265-281): per frame time, step, displacement (3N
+    // f32), plastic strain (E f32), Cauchy stress (6E f32), eroded (E)
+    std::vector<double> frame_time;
+    std::vector<int64_t> frame_step;
+    std::vector<float> frame_disp, frame_pstrain, frame_stress;
+    std::vector<uint8_t> frame_eroded;
     double force_seconds = 0.0, contact_seconds = 0.0, wall_seconds = 0.0, loop_seconds = 0.0;
 };
 std::string run(const Model& m, const RunOptions& opt, RunResults* r);

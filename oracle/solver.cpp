@@ -170,6 +170,40 @@ std::string run(const Model& model, const RunOptions& opt, RunResults* res) {
     };
     if (opt.history_steps > 0) record(0.0, 0);
 
+    // Frames: the capture closure of crushrs::run (src/solver.rs:265-275)
+    // with plastic_strain and cauchy_stress (src/kernel.rs:269-321). Elastic
+    // elements here are rigid slabs at F = I: zero stress and strain.
+    res->frame_time.clear();
+    res->frame_step.clear();
+    res->frame_disp.clear();
+    res->frame_pstrain.clear();
+    res->frame_stress.clear();
+    res->frame_eroded.clear();
+    auto capture = [&](double tr, int64_t sr) {
+        sync_states(elements);
+        res->frame_time.push_back(tr);
+        res->frame_step.push_back(sr);
+        for (double x : u) res->frame_disp.push_back((float)x);
+        for (size_t e = 0; e < model.hexes.size(); ++e) {
+            const bool honey = elements.honeycomb[e] != 0;
+            const RateState& st = elements.state[e];
+            res->frame_pstrain.push_back(honey ? (float)st.compaction : 0.0f);
+            res->frame_eroded.push_back(elements.eroded[e] ? 1 : 0);
+            double c6[6] = {0, 0, 0, 0, 0, 0};
+            if (honey && !elements.eroded[e]) {
+                const double* s6 = st.stress;
+                M3 sh;
+                sh(0, 0) = s6[0]; sh(0, 1) = s6[3]; sh(0, 2) = s6[5];
+                sh(1, 0) = s6[3]; sh(1, 1) = s6[1]; sh(1, 2) = s6[4];
+                sh(2, 0) = s6[5]; sh(2, 1) = s6[4]; sh(2, 2) = s6[2];
+                const M3 c = m3_mul(m3_mul(st.rotation, sh), m3_transpose(st.rotation));
+                c6[0] = c(0, 0); c6[1] = c(1, 1); c6[2] = c(2, 2); c6[3] = c(0, 1); c6[4] = c(1, 2); c6[5] = c(0, 2);
+            }
+            for (double x : c6) res->frame_stress.push_back((float)x);
+        }
+    };
+    if (opt.frame_steps > 0) capture(0.0, 0);
+
     // Separation rule bookkeeping: contacts whose faces are not all fixed.
     std::set<uint32_t> fixed_set(model.fixed_nodes.begin(), model.fixed_nodes.end());
     std::vector<char> counts(contacts.size(), 0);
@@ -234,6 +268,7 @@ std::string run(const Model& model, const RunOptions& opt, RunResults* res) {
         t += dt;
         dt_min = std::fmin(dt_min, dt);
         if (opt.log_steps) res->dt_log.push_back(dt);
+        if (opt.frame_steps > 0 && step % opt.frame_steps == 0) capture(t, step);
         if (opt.history_steps > 0 && step % opt.history_steps == 0) record(t, step);
         if (s.max_steps > 0 && step >= s.max_steps) break;
         if (s.stop_rule == CRUSH_STOP_SEPARATION && step % 10 == 0 && last_hit >= 0 && step - 1 - last_hit >= 100 &&
@@ -243,6 +278,7 @@ std::string run(const Model& model, const RunOptions& opt, RunResults* res) {
             if (vb - va >= 0.0) break;
         }
     }
+    if (opt.frame_steps > 0 && step % opt.frame_steps != 0) capture(t, step);
     if (opt.history_steps > 0 && step % opt.history_steps != 0) record(t, step);
     res->time = t;
     res->steps = step;

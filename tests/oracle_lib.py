@@ -51,6 +51,8 @@ def load():
     lib.oracle_run.argtypes = [P(abi.ModelDesc), C.c_int, C.c_int, P(abi.Results), dp, dp, dp, C.c_int64, dp]
     lib.oracle_run_history.argtypes = [P(abi.ModelDesc), C.c_int, C.c_int, C.c_int, C.c_int, P(abi.Accelerometer), C.c_int64, dp,
                                        P(C.c_int64), dp, dp, P(C.c_int64), P(abi.Results)]
+    lib.oracle_run_frames.argtypes = [P(abi.ModelDesc), C.c_int, C.c_int, C.c_int, C.c_int64, dp, P(C.c_int64), fp, fp, fp,
+                                      P(C.c_uint8), P(C.c_int64)]
     lib.oracle_cfc_filter.argtypes = [dp, C.c_int64, C.c_double, C.c_double, dp]
     lib.oracle_resample.argtypes = [dp, dp, C.c_int64, C.c_double, C.c_double, C.c_double, dp, dp, C.c_int64]
     lib.oracle_resample.restype = C.c_int64
@@ -238,3 +240,24 @@ def resample(t, y, t0, dt, t_end):
     tu, yu = np.empty(n), np.empty(n)
     load().oracle_resample(ptr(t), ptr(y), len(t), t0, dt, t_end, ptr(tu), ptr(yu), n)
     return tu, yu
+
+
+def run_frames(desc, steps, cap=64, simd=True, threads=1):
+    """Whole run with frames: dict time, step, displacement (F, N, 3),
+    plastic_strain (F, E), stress (F, E, 6), eroded (F, E), frames."""
+    lib = load()
+    n, e = desc.n_nodes, desc.n_hexes
+    t = np.zeros(cap)
+    st = (C.c_int64 * cap)()
+    d = np.zeros(cap * 3 * n, np.float32)
+    ps = np.zeros(cap * e, np.float32)
+    sg = np.zeros(cap * 6 * e, np.float32)
+    er = np.zeros(cap * e, np.uint8)
+    nf = C.c_int64()
+    fpp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+    status = lib.oracle_run_frames(C.byref(desc), int(simd), threads, steps, cap, ptr(t), st, fpp(d), fpp(ps), fpp(sg),
+                                   er.ctypes.data_as(C.POINTER(C.c_uint8)), C.byref(nf))
+    assert status in (0, abi.CRUSH_ERR_NONFINITE), error()
+    k = min(nf.value, cap)
+    return {"frames": nf.value, "time": t[:k], "step": np.array(st[:k], dtype=np.int64), "displacement": d[: k * 3 * n].reshape(k, n, 3),
+            "plastic_strain": ps[: k * e].reshape(k, e), "stress": sg[: k * 6 * e].reshape(k, e, 6), "eroded": er[: k * e].reshape(k, e)}

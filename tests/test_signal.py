@@ -3,7 +3,7 @@ the oracle's restatement of src/signal.rs and the reference's own tests
 (src/signal.rs:310-345), restated. CPU only."""
 import numpy as np
 
-from crushrs_b200 import abi, signal as G
+from crushrs_b200 import abi, pulse as G
 from crushrs_b200.native import lib
 
 from . import oracle_lib as O
