@@ -1021,6 +1021,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     }
     slot_contact_off[n_desc] = kc;
     cnode_off[0] = 0;
+    std::atomic<bool> cn_missing{false};
     parallel_for(n_desc, [&](long long k) {
         const ContactPart& cp = parts[k];
         const Base& b = base[k];
@@ -1043,12 +1044,16 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
         std::copy(cp.crole_slave.begin(), cp.crole_slave.end(), crole_slave.begin() + b.role);
         auto cn_of = [&](uint32_t node) {  // the slot's contact nodes are in ascending node order, and include it
             const auto it = std::lower_bound(cp.cnode.begin(), cp.cnode.end(), node);
-            if (it == cp.cnode.end() || *it != node) std::abort();
+            if (it == cp.cnode.end() || *it != node) {
+                cn_missing = true;  // cannot happen: every primary node and face corner has a role
+                return 0u;
+            }
             return (uint32_t)(b.cnode + (it - cp.cnode.begin())) | (cm.fixed[node] ? CN_FIXED : 0u);
         };
         for (size_t j = 0; j < cp.slaves.size(); ++j) slave_cn[b.slave + j] = cn_of(cp.slaves[j]);
         for (size_t j = 0; j < cp.faces.size(); ++j) face_cn[4 * b.face + j] = cn_of(cp.faces[j]);
     });
+    if (cn_missing) return crush::fail(CRUSH_ERR_INVALID, "internal: a contact node without a role");
     parts.clear();
     parts.shrink_to_fit();
     c->n_contacts = kc;
