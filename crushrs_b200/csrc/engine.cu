@@ -12,6 +12,9 @@
 // arithmetic it has alone.
 #include <algorithm>
 #include <memory>
+#include <mutex>
+#include <map>
+#include <unordered_map>
 #include <thread>
 #include <atomic>
 #include <chrono>
@@ -138,24 +141,102 @@ void parallel_for(long long n, F&& fn) {
 // Host-to-device copies through two pinned staging buffers (set-up only):
 // chunks are copied into pinned memory by several threads and sent by DMA
 // while the next chunk is filled. Small copies go directly.
+// The pinned staging buffers are kept for the process and reused by the
+// next set-up (page-locking tens of MB costs milliseconds); a set-up that
+// finds them in use by another thread pins its own.
+struct PinnedPool {
+    std::mutex m;
+    char* buf[2] = {nullptr, nullptr};
+    size_t cap = 0;
+    bool busy = false;
+};
+PinnedPool g_pinned;
+
+// Device buffers of destroyed contexts are kept for the process, per device,
+// and handed to the next context's allocations of a size they fit (at most
+// twice over): set-up and teardown without cudaMalloc / cudaFree, whose
+// mapping work costs tens of milliseconds per context. A cudaMalloc that
+// runs out of memory frees the kept buffers and retries.
+struct DeviceCache {
+    std::mutex m;
+    std::map<int, std::multimap<size_t, void*>> free;  // device -> (bytes, buffer)
+};
+DeviceCache g_device_cache;
+
+// A kept buffer of at least *bytes (its size written back), or null.
+void* device_take(int device, size_t* bytes) {
+    std::lock_guard<std::mutex> lock(g_device_cache.m);
+    auto& f = g_device_cache.free[device];
+    auto it = f.lower_bound(*bytes);
+    if (it == f.end() || it->first > 2 * *bytes + (1u << 20)) return nullptr;
+    void* p = it->second;
+    *bytes = it->first;
+    f.erase(it);
+    return p;
+}
+// Keeps a buffer whose work has finished on every stream.
+void device_give(int device, void* p, size_t bytes) {
+    std::lock_guard<std::mutex> lock(g_device_cache.m);
+    g_device_cache.free[device].emplace(bytes, p);
+}
+void device_release_all(int device) {
+    std::lock_guard<std::mutex> lock(g_device_cache.m);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(device);
+    for (auto& kv : g_device_cache.free[device]) cudaFree(kv.second);
+    g_device_cache.free[device].clear();
+    cudaSetDevice(cur);
+}
+
 struct Stager {
     cudaStream_t s = nullptr;
     char* buf[2] = {nullptr, nullptr};
     cudaEvent_t ev[2] = {nullptr, nullptr};
     size_t cap = 0;
     int cur = 0;
+    bool pooled = false;  // the buffers are g_pinned's
     static constexpr size_t DIRECT = 1 << 20;
     int init(cudaStream_t stream, size_t total) {
         s = stream;
         if (total < 8 * DIRECT) return CRUSH_OK;  // small contexts: direct copies
         cap = std::min<size_t>(total, 64u << 20);
-        for (int k = 0; k < 2; ++k) {
-            if (cudaMallocHost(&buf[k], cap) != cudaSuccess || cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming) != cudaSuccess) {
+        for (int k = 0; k < 2; ++k)
+            if (cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming) != cudaSuccess) {
                 cudaGetLastError();
                 release();
                 return CRUSH_OK;  // fall back to direct copies
             }
+        {
+            std::lock_guard<std::mutex> lock(g_pinned.m);
+            if (!g_pinned.busy) {
+                if (g_pinned.cap < cap) {
+                    for (char*& b : g_pinned.buf)
+                        if (b) {
+                            cudaFreeHost(b);
+                            b = nullptr;
+                        }
+                    g_pinned.cap = 0;
+                    if (cudaMallocHost(&g_pinned.buf[0], cap) == cudaSuccess && cudaMallocHost(&g_pinned.buf[1], cap) == cudaSuccess)
+                        g_pinned.cap = cap;
+                    else
+                        cudaGetLastError();
+                }
+                if (g_pinned.cap >= cap) {
+                    g_pinned.busy = true;
+                    pooled = true;
+                    buf[0] = g_pinned.buf[0];
+                    buf[1] = g_pinned.buf[1];
+                    return CRUSH_OK;
+                }
+            }
         }
+        for (int k = 0; k < 2; ++k)
+            if (cudaMallocHost(&buf[k], cap) != cudaSuccess) {
+                cudaGetLastError();
+                release();
+                return CRUSH_OK;  // fall back to direct copies
+            }
         return CRUSH_OK;
     }
     int copy(void* dst, const void* src, size_t bytes) {
@@ -183,10 +264,15 @@ struct Stager {
     void release() {
         if (s) cudaStreamSynchronize(s);
         for (int k = 0; k < 2; ++k) {
-            if (buf[k]) cudaFreeHost(buf[k]);
+            if (buf[k] && !pooled) cudaFreeHost(buf[k]);
             if (ev[k]) cudaEventDestroy(ev[k]);
             buf[k] = nullptr;
             ev[k] = nullptr;
+        }
+        if (pooled) {
+            std::lock_guard<std::mutex> lock(g_pinned.m);
+            g_pinned.busy = false;
+            pooled = false;
         }
     }
     ~Stager() { release(); }
@@ -205,6 +291,7 @@ struct crush_ctx {
     cudaEvent_t ev_heavy = nullptr, ev_heavy_done = nullptr;  // the heavy-node gather beside the contact gather
     int* mass_flag = nullptr;                  // device: some crash scales its masses this step
     std::vector<void*> allocs;
+    std::unordered_map<void*, size_t> alloc_bytes;  // size of every device allocation
     int64_t launches = 0;
 
     // sizes
@@ -360,13 +447,24 @@ struct crush_ctx {
     int alloc(T** p, size_t count) {
         *p = nullptr;
         if (count == 0) count = 1;
-        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T));
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            return crush::fail(e == cudaErrorMemoryAllocation ? CRUSH_ERR_OOM : CRUSH_ERR_CUDA,
-                               std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        size_t bytes = count * sizeof(T);
+        void* q = device_take(device, &bytes);
+        if (!q) {
+            cudaError_t e = cudaMalloc(&q, bytes);
+            if (e == cudaErrorMemoryAllocation) {  // memory held for reuse goes back first
+                cudaGetLastError();
+                device_release_all(device);
+                e = cudaMalloc(&q, bytes);
+            }
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                return crush::fail(e == cudaErrorMemoryAllocation ? CRUSH_ERR_OOM : CRUSH_ERR_CUDA,
+                                   std::string("cudaMalloc: ") + cudaGetErrorString(e));
+            }
         }
-        allocs.push_back(*p);
+        *p = static_cast<T*>(q);
+        allocs.push_back(q);
+        alloc_bytes[q] = bytes;
         return CRUSH_OK;
     }
     template <typename T>
@@ -391,7 +489,7 @@ struct crush_ctx {
         if (stream) cudaStreamSynchronize(stream);
         if (side) cudaStreamSynchronize(side);
         if (side2) cudaStreamSynchronize(side2);
-        for (void* p : allocs) cudaFree(p);
+        for (void* p : allocs) device_give(device, p, alloc_bytes[p]);
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
         if (ev_join2) cudaEventDestroy(ev_join2);
@@ -766,6 +864,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     c->device = device;
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+
     {
         int lo = 0, hi = 0;
         CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
@@ -899,6 +998,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     Stager stager;
     stager.init(c->stream, sizeof(double) * 6 * N + sizeof(uint32_t) * 27 * E);
     c->stager = &stager;
+    trace.mark("pinned staging buffers");
     TRY(c->upload(&c->pos, cm.positions.data(), 3 * N));
     TRY(c->upload(&c->conn_all, cm.hexes.data(), 8 * E));
     TRY(c->upload(&c->part, cm.hex_part.data(), E));
@@ -913,6 +1013,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->upload(&c->hc_off, hc_off.data(), N + 1));
     TRY(c->upload(&c->hc_slot, hc_slot.data(), hc_slot.size()));
     TRY(c->upload(&c->v0, cm.v0.data(), 3 * N));
+    trace.mark("model uploads");
     for (double** p : {&c->u, &c->v, &c->v_half, &c->f_int, &c->f_ext, &c->u_tmp, &c->f_tmp}) TRY(c->alloc(p, 3 * N));
     for (double** p : {&c->inv_mass, &c->mass, &c->added, &c->n_tmp, &c->n_tmp2}) TRY(c->alloc(p, N));
     for (double** p : {&c->volume, &c->dt_factor, &c->elem_mass, &c->elem_dt, &c->elem_extra, &c->e_tmp}) TRY(c->alloc(p, E));
@@ -1491,8 +1592,10 @@ void update_period(crush_ctx* c) {
 }
 
 static void free_bufs(crush_ctx* c, std::vector<void*>& bufs) {
+    if (!bufs.empty()) cudaStreamSynchronize(c->stream);
     for (void* p : bufs) {
-        cudaFree(p);
+        device_give(c->device, p, c->alloc_bytes[p]);
+        c->alloc_bytes.erase(p);
         c->allocs.erase(std::remove(c->allocs.begin(), c->allocs.end(), p), c->allocs.end());
     }
     bufs.clear();
