@@ -85,8 +85,10 @@ __device__ __forceinline__ double step_dt(const Control* c) {
     return d > 1e-15 ? d : 1e-15;
 }
 
+// Static planes are read once per step: streamed past L1 (evict-first), so
+// L1 keeps the node positions that neighbouring elements share.
 __device__ __forceinline__ float4 ld_plane(const float4* __restrict__ planes, long long stride, int p, long long e) {
-    return __ldg(planes + p * stride + e);
+    return __ldcs(planes + p * stride + e);
 }
 
 // ---------------- contact broad phase, shared by the kernels and the host ----------------

@@ -395,7 +395,7 @@ __device__ __forceinline__ void forces_body(const ElementArrays& el, const NodeA
     float st[28];
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-        float4 s4 = el.state[k * S + e];
+        float4 s4 = __ldcs(el.state + k * S + e);
         st[4 * k] = s4.x; st[4 * k + 1] = s4.y; st[4 * k + 2] = s4.z; st[4 * k + 3] = s4.w;
     }
     st[24] = st6.x; st[25] = st6.y; st[26] = st6.z; st[27] = st6.w;
@@ -403,7 +403,7 @@ __device__ __forceinline__ void forces_body(const ElementArrays& el, const NodeA
     M3f tau, f_inv;
     honeycomb_update(f, det, st, mat, tau, f_inv);
 #pragma unroll
-    for (int k = 0; k < 7; ++k) el.state[k * S + e] = make_float4(st[4 * k], st[4 * k + 1], st[4 * k + 2], st[4 * k + 3]);
+    for (int k = 0; k < 7; ++k) __stcs(el.state + k * S + e, make_float4(st[4 * k], st[4 * k + 1], st[4 * k + 2], st[4 * k + 3]));
     // f_i = τ F⁻ᵀ ∇N_i V₀
     M3f m;
     mat_mul_t(tau, f_inv, m);
