@@ -1348,6 +1348,22 @@ __global__ void k_contact_force(ContactArrays ca, Control* ctls, int c0, int run
     }
 }
 
+// Start of a force pass, one block: the previous pass's heavy nodes (those
+// listed in gather_work) get their event counts back to zero, then the pool
+// and the heavy list are emptied. The heavy gather cannot clear its own
+// nodes' counts: the other gather, beside it on a second stream or after it
+// on the same stream, reads them to skip those nodes.
+constexpr int RESET_TPB = 512;
+__global__ void __launch_bounds__(RESET_TPB) k_contact_reset(ContactArrays ca) {
+    const int count = *ca.gather_count;
+    for (int w = threadIdx.x; w < count; w += RESET_TPB) ca.ev_count[ca.gather_work[w]] = 0;
+    __syncthreads();  // every thread has read the count
+    if (threadIdx.x == 0) {
+        *ca.ev_pool_n = 0;
+        *ca.gather_count = 0;
+    }
+}
+
 constexpr int GATHER_TPB = 128;
 constexpr int HEAVY_TPB = 256;
 constexpr int HEAVY_KEYS = 2048;     // events a block sorts itself
@@ -1387,8 +1403,9 @@ __device__ __forceinline__ double half_u(const NodeArrays& nd, const Control* ct
 // contact after contact. Up to EV_CAP keys are sorted in registers (a
 // bitonic network) and their forces loaded together; a node with more goes
 // to k_contact_gather_heavy (the force pass listed it), which writes its
-// output and zeroes its count. The gather zeroes the other nodes' event
-// counts for the next pass. In a run it also writes the node's
+// output; its count stays until k_contact_reset at the next pass, so this
+// gather skips it whichever kernel runs first. The gather zeroes the other
+// nodes' event counts for the next pass. In a run it also writes the node's
 // half-step u to u_next (fixed nodes and stopped crashes keep theirs), so
 // the next step's search can start before the half step.
 __device__ __forceinline__ void gather_body(const ContactArrays& ca, const NodeArrays& nd, const Control* ctls, int c0, int c1,
@@ -1572,6 +1589,7 @@ __device__ void walk_node(const ContactArrays& ca, int c0, int c1, long long i, 
 // collected (EV_CAP + pool = the count when nothing was dropped), sorted by a
 // bitonic sort in shared memory and added in order. A node whose events do
 // not fit HEAVY_KEYS, or lost some to a full pool, is rebuilt by walk_node.
+// The nodes' event counts are left for k_contact_reset.
 __global__ void __launch_bounds__(HEAVY_TPB) k_contact_gather_heavy(ContactArrays ca, NodeArrays nd, const Control* ctls, int c0, int c1,
                                                                     int run_mode, double* __restrict__ f_out) {
     __shared__ uint32_t keys[HEAVY_BUF];
@@ -1629,8 +1647,7 @@ __global__ void __launch_bounds__(HEAVY_TPB) k_contact_gather_heavy(ContactArray
             f_out[3 * n + threadIdx.x] = acc;
             if (run_mode) ca.u_next[3 * n + threadIdx.x] = half_u(nd, ctls + nd.node_slot[n], n, threadIdx.x, acc);
         }
-        __syncthreads();  // every thread has read the count
-        if (threadIdx.x == 0) ca.ev_count[i] = 0;
+        __syncthreads();  // every thread is done with s_n and the shared buffers
     }
 }
 
@@ -1848,7 +1865,7 @@ void launch_contact_finish(cudaStream_t s, const ContactArrays& ca, const NodeAr
     const int run_mode = dt_override > 0.0 ? 0 : 1;
     (void)f0;
     (void)n_faces;
-    cudaMemsetAsync(ca.ev_pool_n, 0, 2 * sizeof(int), s);  // pool entries and heavy nodes (gather_count)
+    k_contact_reset<<<1, RESET_TPB, 0, s>>>(ca);  // the last pass's heavy counts, the pool and the heavy list
     if (n_slaves > 0)
         k_contact_force<<<active_grid(n_slaves, FORCE_LANES, TPB, GRID_CAP), TPB, 0, s>>>(ca, ctls, c0, run_mode, dt_override, masses,
                                                                                          n_slaves, skip_fixed);
@@ -1897,7 +1914,7 @@ int contact_search_launches(const ContactArrays& ca, bool run_mode, long long n_
     return k;
 }
 
-int contact_finish_launches(long long n_slaves) { return 2 + (n_slaves > 0 ? 1 : 0); }
+int contact_finish_launches(long long n_slaves) { return 3 + (n_slaves > 0 ? 1 : 0); }
 
 int contact_launches(const ContactArrays& ca, bool run_mode, long long n_faces, long long n_slaves, long long bk0, long long bk1,
                      int c0) {

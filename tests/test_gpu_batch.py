@@ -107,3 +107,20 @@ def test_batch_rejects_mixed_check_cadence(models):
     with pytest.raises(CrushError) as e:
         Context([models[0].desc, m.desc])
     assert e.value.status == abi.CRUSH_ERR_UNSUPPORTED
+
+
+def test_large_batch_equals_alone():
+    """1024 uneven crashes (about 3 M nodes) in one context: the contact
+    gathers of heavy nodes (more than 16 reaction events) run beside the
+    ordinary gather on a second stream and the step's kernels loop over
+    their grids, so this covers the ordering between them that a handful of
+    slots never stresses. Sampled slots must equal the same crash alone."""
+    ms = [S.Model.build(S.batch_headon(i)) for i in range(1024)]
+    ctx = Context([m.desc for m in ms])
+    rs = ctx.batch_run()
+    ctx.close()
+    for i in (0, 85, 266, 363, 402, 1023):
+        a = Context(ms[i].desc)
+        r = a.run()
+        a.close()
+        _same(rs[i], r)
