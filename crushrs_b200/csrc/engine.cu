@@ -300,6 +300,9 @@ struct crush_ctx {
     long long n_nodes = 0, n_all = 0, n_hc = 0, stride = 0;
     std::vector<int64_t> hc_index;   // model element -> honeycomb index or -1
     std::vector<uint32_t> hc_model;  // honeycomb index -> model element
+    long long n_sc = 0;              // elastic elements (the scalar f64 path)
+    long long n_sc_free = 0;         // those with a node that is not fixed: numbered first
+    std::vector<uint32_t> sc_model;  // scalar index -> model element
     int check_steps = 5;             // common adaptive_check_steps of the slots
     bool adaptive = true;
     bool any_separation = false;
@@ -315,6 +318,9 @@ struct crush_ctx {
     int32_t* part = nullptr;
     double* mat4 = nullptr;
     int64_t* hc_index_d = nullptr;
+    int64_t* sc_index_d = nullptr;
+    uint32_t *sc_model_d = nullptr, *sc_off = nullptr, *sc_slot = nullptr;
+    double *sc_geo = nullptr, *sc_mat = nullptr, *sc_corner = nullptr;
     float4 *planes = nullptr, *state = nullptr;
     float* corner = nullptr;
     MaterialF32* mats = nullptr;
@@ -393,6 +399,13 @@ struct crush_ctx {
         e.elem_extra = elem_extra;
         e.elem_slot = elem_slot;
         e.act_hc = e.act_all = Active{nullptr, nullptr};
+        e.n_sc = n_sc;
+        e.sc_stride = n_sc;
+        e.sc_model = sc_model_d;
+        e.sc_geo = sc_geo;
+        e.sc_mat = sc_mat;
+        e.sc_corner = sc_corner;
+        e.act_sc = Active{nullptr, nullptr};
         return e;
     }
     // The run's bundles: kernels visit only the active chunks.
@@ -400,6 +413,11 @@ struct crush_ctx {
         ElementArrays e = el();
         e.act_hc = active(0);
         e.act_all = active(1);
+        // A run skips the elastic elements whose nodes are all fixed (a
+        // rigid road): their forces land only on fixed nodes, whose motion
+        // and outputs do not depend on them. Drop-in calls compute them all.
+        e.n_sc = n_sc_free;
+        e.act_sc = active(8);
         return e;
     }
     NodeArrays nd_run() const {
@@ -437,6 +455,8 @@ struct crush_ctx {
         a.hc_slot = hc_slot;
         a.all_off = all_off;
         a.all_slot = all_slot;
+        a.sc_off = sc_off;
+        a.sc_slot = sc_slot;
         a.node_slot = node_slot;
         a.mass_flag = mass_flag;
         a.act_node = Active{nullptr, nullptr};
@@ -628,8 +648,6 @@ void fill_slot(const crush_model_desc* d, int slot, const Slot& sl, int p0, Comb
         for (int i = 0; i < 8; ++i) {
             const uint64_t n = d->hexes[8 * e + i];
             if (n >= (uint64_t)N) return err.set(CRUSH_ERR_INVALID, "hexahedron node out of range");
-            if (!honey && !cm.fixed[n0 + n])
-                return err.set(CRUSH_ERR_UNSUPPORTED, "elastic elements are supported only as rigid slabs (every node fixed)");
             cm.hexes[8 * (e0 + e) + i] = (uint32_t)(n0 + n);
         }
         cm.hex_part[e0 + e] = p0 + p;
@@ -941,56 +959,100 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     // slot in parallel: a slot's nodes are touched only by its own elements.
     std::vector<long long> hc0(n_desc + 1, 0);
     for (int k = 0; k < n_desc; ++k) hc0[k + 1] = hc0[k] + slot_hc[k];
+    // Elastic elements with a free node per slot (they are numbered first,
+    // slot after slot, then the all-fixed ones).
+    std::vector<long long> slot_free(n_desc, 0);
+    parallel_for(n_desc, [&](long long k) {
+        const Slot& sl = c->slots[k];
+        long long nf = 0;
+        for (long long e = sl.elem0; e < sl.elem0 + sl.n_elems; ++e) {
+            if (cm.materials[cm.hex_part[e]].model == CRUSH_MAT_HONEYCOMB) continue;
+            bool all_fixed = true;
+            for (int i = 0; i < 8; ++i) all_fixed = all_fixed && cm.fixed[cm.hexes[8 * e + i]] != 0;
+            nf += all_fixed ? 0 : 1;
+        }
+        slot_free[k] = nf;
+    });
+    std::vector<long long> free0(n_desc + 1, 0), fixed0(n_desc + 1, 0);
+    for (int k = 0; k < n_desc; ++k) {
+        free0[k + 1] = free0[k] + slot_free[k];
+        fixed0[k + 1] = fixed0[k] + (c->slots[k].n_elems - slot_hc[k] - slot_free[k]);
+    }
+    c->n_sc_free = free0[n_desc];
     c->n_hc = hc0[n_desc];
     c->stride = std::max<long long>(32, (c->n_hc + 31) / 32 * 32);
+    c->n_sc = E - c->n_hc;
     c->hc_index.resize(E);
     c->hc_model.resize(c->n_hc);
-    Buf<uint32_t> all_off, hc_off, all_slot, hc_slot;
+    c->sc_model.resize(c->n_sc);
+    std::vector<int64_t> sc_index(E);
+    Buf<uint32_t> all_off, hc_off, all_slot, hc_slot, sc_off, sc_slot;
     all_off.alloc(N + 1);
     hc_off.alloc(N + 1);
+    sc_off.alloc(N + 1);
     all_slot.alloc(8 * E);
     hc_slot.alloc(8 * c->n_hc);
+    sc_slot.alloc(8 * c->n_sc);
     parallel_for(n_desc, [&](long long k) {
         const Slot& sl = c->slots[k];
         const long long n0 = sl.node0, e0 = sl.elem0, nn = sl.n_nodes;
-        long long h = hc0[k];
+        long long h = hc0[k], qf = free0[k], qx = free0[n_desc] + fixed0[k];
+        const long long q0 = e0 - hc0[k];  // the slot's first scalar CSR entry / 8
         for (long long e = e0; e < e0 + sl.n_elems; ++e)
             if (cm.materials[cm.hex_part[e]].model == CRUSH_MAT_HONEYCOMB) {
                 c->hc_index[e] = h;
                 c->hc_model[h++] = (uint32_t)e;
+                sc_index[e] = -1;
             } else {
                 c->hc_index[e] = -1;
+                bool all_fixed = true;
+                for (int i = 0; i < 8; ++i) all_fixed = all_fixed && cm.fixed[cm.hexes[8 * e + i]] != 0;
+                const long long q = all_fixed ? qx++ : qf++;
+                sc_index[e] = q;
+                c->sc_model[q] = (uint32_t)e;
             }
         // per-node counts, then offsets from the slot's first entry (a slot
         // writes only off[n0, n0 + nn))
-        std::vector<uint32_t> cnt_a(nn, 0), cnt_b(nn, 0);
+        std::vector<uint32_t> cnt_a(nn, 0), cnt_b(nn, 0), cnt_c(nn, 0);
         for (long long e = e0; e < e0 + sl.n_elems; ++e) {
             const bool honey = c->hc_index[e] >= 0;
             for (int i = 0; i < 8; ++i) {
                 const uint32_t n = cm.hexes[8 * e + i];
                 cnt_a[n - n0]++;
                 if (honey) cnt_b[n - n0]++;
+                else cnt_c[n - n0]++;
             }
         }
-        uint32_t a = (uint32_t)(8 * e0), b = (uint32_t)(8 * hc0[k]);
+        uint32_t a = (uint32_t)(8 * e0), b = (uint32_t)(8 * hc0[k]), cc = (uint32_t)(8 * q0);
         for (long long n = n0; n < n0 + nn; ++n) {
             all_off[n] = a;
             hc_off[n] = b;
+            sc_off[n] = cc;
             a += cnt_a[n - n0];
             b += cnt_b[n - n0];
+            cc += cnt_c[n - n0];
         }
-        std::vector<uint32_t> cura(all_off.data() + n0, all_off.data() + n0 + nn), curb(hc_off.data() + n0, hc_off.data() + n0 + nn);
+        std::vector<uint32_t> cura(all_off.data() + n0, all_off.data() + n0 + nn), curb(hc_off.data() + n0, hc_off.data() + n0 + nn),
+            curc(sc_off.data() + n0, sc_off.data() + n0 + nn);
         for (long long e = e0; e < e0 + sl.n_elems; ++e) {
-            const long long he = c->hc_index[e];
+            const long long he = c->hc_index[e], se = sc_index[e];
             for (int i = 0; i < 8; ++i) {
                 const uint32_t n = cm.hexes[8 * e + i];
                 all_slot[cura[n - n0]++] = (uint32_t)(8 * e + i);
                 if (he >= 0) hc_slot[curb[n - n0]++] = (uint32_t)(8 * he + i);
+                else sc_slot[curc[n - n0]++] = (uint32_t)(8 * se + i);
             }
         }
     });
     all_off[N] = (uint32_t)(8 * E);
     hc_off[N] = (uint32_t)(8 * c->n_hc);
+    sc_off[N] = (uint32_t)(8 * c->n_sc);
+    std::vector<double> sc_mat(2 * (size_t)std::max<long long>(c->n_sc, 1), 0.0);
+    for (long long q = 0; q < c->n_sc; ++q) {
+        const crush_material& m = cm.materials[cm.hex_part[c->sc_model[q]]];
+        sc_mat[2 * q] = m.youngs_modulus;
+        sc_mat[2 * q + 1] = m.poisson_ratio;
+    }
     trace.mark("node incidence CSR");
 
     int st;
@@ -1012,6 +1074,15 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->upload(&c->all_slot, all_slot.data(), all_slot.size()));
     TRY(c->upload(&c->hc_off, hc_off.data(), N + 1));
     TRY(c->upload(&c->hc_slot, hc_slot.data(), hc_slot.size()));
+    if (c->n_sc > 0) {
+        TRY(c->upload(&c->sc_index_d, sc_index.data(), E));
+        TRY(c->upload(&c->sc_model_d, c->sc_model.data(), c->n_sc));
+        TRY(c->upload(&c->sc_off, sc_off.data(), N + 1));
+        TRY(c->upload(&c->sc_slot, sc_slot.data(), sc_slot.size()));
+        TRY(c->upload(&c->sc_mat, sc_mat.data(), sc_mat.size()));
+        TRY(c->alloc(&c->sc_geo, (size_t)SC_PLANES * c->n_sc));
+        TRY(c->alloc(&c->sc_corner, (size_t)24 * c->n_sc));
+    }
     TRY(c->upload(&c->v0, cm.v0.data(), 3 * N));
     trace.mark("model uploads");
     for (double** p : {&c->u, &c->v, &c->v_half, &c->f_int, &c->f_ext, &c->u_tmp, &c->f_tmp}) TRY(c->alloc(p, 3 * N));
@@ -1037,7 +1108,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->alloc(&bad, 1));
     CK(cudaMemsetAsync(bad, 0, sizeof(int), c->stream));
     launch_setup_geometry(c->stream, E, c->pos, c->conn_all, c->part, c->mat4, c->hc_index_d, c->elem_slot, c->stride, c->planes,
-                          c->volume, c->lumped, c->dt_factor, c->elem_mass, bad);
+                          c->volume, c->lumped, c->dt_factor, c->elem_mass, bad, c->sc_index_d, c->n_sc, c->sc_geo);
     TRY(check_launch(c));
     launch_node_masses(c->stream, N, c->all_off, c->all_slot, c->lumped, c->mass, c->inv_mass);
     TRY(check_launch(c));
@@ -1324,7 +1395,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     {
         const long long sizes[ACTIVE_SPACES] = {c->n_hc, E, N, (long long)c->grid_slaves_h.size(), (long long)cnode.size(),
                                                 (long long)dyn_faces.size(), (long long)slaves.size(),
-                                                (long long)c->st_slaves_h.size()};
+                                                (long long)c->st_slaves_h.size(), c->n_sc_free};
         c->space_off_h.assign(ACTIVE_SPACES + 1, 0);
         for (int sp = 0; sp < ACTIVE_SPACES; ++sp) c->space_off_h[sp + 1] = c->space_off_h[sp] + (sizes[sp] + CHUNK - 1) / CHUNK;
         const long long nch = c->space_off_h[ACTIVE_SPACES];
@@ -1338,7 +1409,8 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
                 case 4: return (int)cm.node_slot[cnode[i]];
                 case 5: return contact_slot[face_contact[dyn_faces[i]]];
                 case 6: return contact_slot[slave_contact[i]];
-                default: return contact_slot[slave_contact[c->st_slaves_h[i]]];
+                case 7: return contact_slot[slave_contact[c->st_slaves_h[i]]];
+                default: return (int)cm.elem_slot[c->sc_model[i]];
             }
         };
         parallel_for(nch, [&](long long q) {
@@ -1485,7 +1557,7 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
     mark(4);
     launch_full(c->stream, el, nd, c->ctls);
     mark(5);
-    n += 2 + (c->n_hc > 0 ? 1 : 0);
+    n += 2 + forces_launches(el);
     if ((step + 1) % 20 == 0) {
         launch_nonfinite(c->stream, nd, c->ctls);
         ++n;
@@ -1647,6 +1719,12 @@ int rebuild_frames(crush_ctx* c) {
     f.eroded_all = c->eroded_all;
     f.state = c->state;
     f.state_stride = c->stride;
+    f.sc_index = c->n_sc > 0 ? c->sc_index_d : nullptr;
+    f.n_sc = c->n_sc;
+    f.sc_geo = c->sc_geo;
+    f.sc_mat = c->sc_mat;
+    f.conn_all = c->conn_all;
+    f.pos = c->pos;
     f.node_blocks = (int)std::min<long long>(1024, (max3n + 4095) / 4096);
     f.elem_blocks = (int)std::min<long long>(1024, (maxe + 2047) / 2048);
     const size_t mark = c->allocs.size();
@@ -1820,7 +1898,7 @@ int run_begin(crush_ctx* c) {
     // elements it erodes is not added to the run's total (as there).
     launch_forces(c->stream, c->el(), c->nd(), c->ctls, 0);
     launch_gather(c->stream, c->el(), c->nd(), c->f_int);
-    st = check_launch(c, (c->n_hc > 0 ? 1 : 0) + 1);
+    st = check_launch(c, forces_launches(c->el()) + 1);
     if (st != CRUSH_OK) return st;
     // Geometry of every contact face at u = 0; static faces keep it.
     launch_contact_geometry(c->stream, c->ca, c->nd(), 0, c->n_contacts, 0, c->n_faces);
@@ -2122,7 +2200,7 @@ int crush_compute_forces_device(crush_ctx* c, const double* u_device, double* f_
     }
     launch_forces(c->stream, c->el(), nd, c->ctls_aux, 0);
     launch_gather(c->stream, c->el(), nd, f_device);
-    int st = check_launch(c, (c->n_hc > 0 ? 1 : 0) + 1);
+    int st = check_launch(c, forces_launches(c->el()) + 1);
     if (st != CRUSH_OK) return st;
     if (newly) {
         std::vector<Control> aux;
@@ -2308,6 +2386,8 @@ int crush_set_state(crush_ctx* c, const float* state, const uint8_t* eroded) {
     if (!c || !state || !eroded) return crush::fail(CRUSH_ERR_INVALID, "null argument");
     std::vector<float4> sp((size_t)N_STATE_PLANES * c->stride);
     std::vector<uint8_t> er_all(c->n_all, 0);
+    CK(cudaMemcpyAsync(er_all.data(), c->eroded_all, c->n_all, cudaMemcpyDeviceToHost, c->stream));  // elastic elements keep theirs
+    CK(cudaStreamSynchronize(c->stream));
     for (long long e = 0; e < c->n_hc; ++e) {
         float v[28] = {};
         for (int k = 0; k < 25; ++k) v[k] = state[25 * e + k];

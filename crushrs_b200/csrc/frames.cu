@@ -4,6 +4,7 @@
 // :345-348, :353-355; plastic_strain and cauchy_stress, src/kernel.rs:269-321),
 // copied into device buffers sized at configuration.
 #include "kernels.cuh"
+#include "hencky.cuh"
 
 namespace crush {
 
@@ -34,10 +35,11 @@ __global__ void __launch_bounds__(FRAME_TPB) k_frame_nodes(FrameArrays f, const 
 
 // blockIdx.y = slot: per element the erosion flag, the plastic strain
 // (compaction of a honeycomb element, 0 for an elastic one) and the Cauchy
-// stress R sigma_hat R^T from the committed f32 state in f64, as
-// src/kernel.rs:285-293 computes it, 0 when eroded or elastic (every elastic
-// element here is a rigid slab at F = I, whose stress is zero).
-__global__ void __launch_bounds__(FRAME_TPB) k_frame_elems(FrameArrays f, const Control* ctls, int mode) {
+// stress: R sigma_hat R^T from the committed f32 state in f64 for a
+// honeycomb element, as src/kernel.rs:285-293 computes it; tau / J of the
+// Hencky stress at the current F for an elastic one (:294-315); 0 when
+// eroded or inverted.
+__global__ void __launch_bounds__(FRAME_TPB) k_frame_elems(FrameArrays f, const double* __restrict__ u, const Control* ctls, int mode) {
     const int slot = blockIdx.y;
     if (!frame_due(f, ctls + slot, slot, mode)) return;
     const long long r = f.count[slot];
@@ -79,6 +81,29 @@ __global__ void __launch_bounds__(FRAME_TPB) k_frame_elems(FrameArrays f, const 
                 c6[4] = (float)c[1][2];
                 c6[5] = (float)c[0][2];
             }
+        } else if (f.sc_index && !er) {
+            const long long q = f.sc_index[e];
+            double fm[9];
+            for (int k = 0; k < 9; ++k) fm[k] = 0.0;
+            for (int k = 0; k < 8; ++k) {
+                const long long n = f.conn_all[8 * e + k];
+                for (int a = 0; a < 3; ++a) {
+                    const double xa = f.pos[3 * n + a] + u[3 * n + a];
+                    for (int b = 0; b < 3; ++b) fm[3 * a + b] += xa * f.sc_geo[(SC_GRAD + 3 * k + b) * f.n_sc + q];
+                }
+            }
+            const double j = fm[0] * (fm[4] * fm[8] - fm[7] * fm[5]) - fm[1] * (fm[3] * fm[8] - fm[6] * fm[5]) +
+                             fm[2] * (fm[3] * fm[7] - fm[6] * fm[4]);
+            if (j > 0.0) {
+                double tau[9];
+                hencky_elastic(f.sc_mat[2 * q], f.sc_mat[2 * q + 1], fm, tau);
+                c6[0] = (float)(tau[0] / j);
+                c6[1] = (float)(tau[4] / j);
+                c6[2] = (float)(tau[8] / j);
+                c6[3] = (float)(tau[1] / j);
+                c6[4] = (float)(tau[5] / j);
+                c6[5] = (float)(tau[2] / j);
+            }
         }
         f.eroded[base + i] = er ? 1 : 0;
         f.pstrain[base + i] = ps;
@@ -104,7 +129,7 @@ __global__ void k_frame_finish(FrameArrays f, const Control* ctls, int mode) {
 
 void launch_frames(cudaStream_t s, const FrameArrays& f, const double* u, const Control* ctls, int mode) {
     k_frame_nodes<<<dim3((unsigned)f.node_blocks, (unsigned)f.n_slots), FRAME_TPB, 0, s>>>(f, u, ctls, mode);
-    k_frame_elems<<<dim3((unsigned)f.elem_blocks, (unsigned)f.n_slots), FRAME_TPB, 0, s>>>(f, ctls, mode);
+    k_frame_elems<<<dim3((unsigned)f.elem_blocks, (unsigned)f.n_slots), FRAME_TPB, 0, s>>>(f, u, ctls, mode);
     k_frame_finish<<<(unsigned)((f.n_slots + 127) / 128), 128, 0, s>>>(f, ctls, mode);
 }
 

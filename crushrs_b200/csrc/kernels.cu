@@ -22,6 +22,7 @@
 
 #include "element.cuh"
 #include "kernels.cuh"
+#include "hencky.cuh"
 
 namespace crush {
 
@@ -132,7 +133,9 @@ __global__ void __launch_bounds__(128) k_setup_geometry(long long n_all, const d
                                                         long long stride,
                                                         float4* __restrict__ planes, double* __restrict__ volume_out,
                                                         double* __restrict__ lumped_out, double* __restrict__ dt_factor,
-                                                        double* __restrict__ elem_mass, int* __restrict__ bad) {
+                                                        double* __restrict__ elem_mass, int* __restrict__ bad,
+                                                        const int64_t* __restrict__ sc_index, long long n_sc,
+                                                        double* __restrict__ sc_geo) {
     long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n_all) return;
     double x[8][3];
@@ -242,7 +245,15 @@ __global__ void __launch_bounds__(128) k_setup_geometry(long long n_all, const d
         dt_factor[e] = (1.0 - 0.36 * nu) / sqrt(mm / rho);
     }
     const long long h = hc_index[e];
-    if (h < 0) return;
+    const long long sc = sc_index ? sc_index[e] : -1;
+    if (h < 0 && sc < 0) return;
+    if (sc >= 0) {  // an elastic element keeps its geometry in f64 (src/kernel.rs:53-91)
+        for (int i = 0; i < 8; ++i)
+            for (int d = 0; d < 3; ++d) sc_geo[(SC_GRAD + 3 * i + d) * n_sc + sc] = gc[i][d];
+        sc_geo[SC_VOL * n_sc + sc] = volume;
+        for (int i = 0; i < 8; ++i)
+            for (int aa = 0; aa < 4; ++aa) sc_geo[(SC_GAMMA + 4 * i + aa) * n_sc + sc] = gam[i][aa];
+    }
     // A = (ΓᵀΓ)⁻¹ (GGᵀ = A⁻¹ ⊗ I3), by Gauss-Jordan with partial pivoting on 4x4.
     double a[4][8];
     for (int r = 0; r < 4; ++r)
@@ -288,7 +299,9 @@ __global__ void __launch_bounds__(128) k_setup_geometry(long long n_all, const d
                     s += a[ar][4 + a1] * g * a[b1][4 + bc];
                 }
             hs[h_index(r, c)] = (float)s;
+            if (sc >= 0) sc_geo[(SC_H + h_index(r, c)) * n_sc + sc] = s;
         }
+    if (h < 0) return;
     float4* pl = planes;
     pl[(P_CONN + 0) * stride + h] = make_float4(__uint_as_float(nid[0]), __uint_as_float(nid[1]), __uint_as_float(nid[2]), __uint_as_float(nid[3]));
     pl[(P_CONN + 1) * stride + h] = make_float4(__uint_as_float(nid[4]), __uint_as_float(nid[5]), __uint_as_float(nid[6]), __uint_as_float(nid[7]));
@@ -482,11 +495,115 @@ __global__ void __launch_bounds__(FORCES_TPB, FORCES_MINB) k_forces(ElementArray
     }
 }
 
+// Elastic elements: the reference's scalar f64 element (src/kernel.rs:116-156)
+// with the Hencky stress, one element per thread: F = Σ x_i ⊗ ∇N_i at
+// x = X + u; det F <= 0 erodes the element; f_i = (τ F⁻ᵀ V) ∇N_i plus the
+// hourglass force R Γᵀ with R = H (U Γ). Corner forces in f64.
+constexpr int SC_TPB = 128;
+__device__ __forceinline__ void scalar_force_body(const ElementArrays& el, const NodeArrays& nd, Control* ctls, int respect_done,
+                                                  long long i) {
+    if (i >= el.n_sc) return;
+    const long long e = el.sc_model[i];
+    Control* ctl = ctls + el.elem_slot[e];
+    if (respect_done && ctl->done) return;
+    double* out = el.sc_corner + 24 * i;
+    if (el.eroded_all[e]) {
+        for (int k = 0; k < 24; ++k) out[k] = 0.0;
+        return;
+    }
+    const long long S = el.sc_stride;
+    const double* G = el.sc_geo;
+    double x[8][3], ul[24];
+    for (int k = 0; k < 8; ++k) {
+        const long long n = el.conn_all[8 * e + k];
+        for (int d = 0; d < 3; ++d) {
+            const double ud = nd.u[3 * n + d];
+            x[k][d] = nd.pos[3 * n + d] + ud;
+            ul[3 * k + d] = ud;
+        }
+    }
+    double grad[24];
+    for (int k = 0; k < 24; ++k) grad[k] = G[(SC_GRAD + k) * S + i];
+    double f[9];
+    for (int k = 0; k < 9; ++k) f[k] = 0.0;
+    for (int k = 0; k < 8; ++k)
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) f[3 * a + b] += x[k][a] * grad[3 * k + b];
+    if (det3d(f) <= 0.0) {
+        el.eroded_all[e] = 1;
+        atomicAdd(reinterpret_cast<unsigned long long*>(&ctl->eroded_step), 1ull);
+        for (int k = 0; k < 24; ++k) out[k] = 0.0;
+        return;
+    }
+    double tau[9], finv[9];
+    hencky_elastic(el.sc_mat[2 * i], el.sc_mat[2 * i + 1], f, tau);
+    inv3d(f, finv);
+    const double vol = G[SC_VOL * S + i];
+    double m[9];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            double t = tau[3 * a] * finv[3 * b];
+            t = t + tau[3 * a + 1] * finv[3 * b + 1];
+            t = t + tau[3 * a + 2] * finv[3 * b + 2];
+            m[3 * a + b] = t * vol;
+        }
+    double o[24];
+    for (int k = 0; k < 8; ++k)
+        for (int a = 0; a < 3; ++a) {
+            double t = m[3 * a] * grad[3 * k];
+            t = t + m[3 * a + 1] * grad[3 * k + 1];
+            t = t + m[3 * a + 2] * grad[3 * k + 2];
+            o[3 * k + a] = t;
+        }
+    double gam[32];
+    for (int k = 0; k < 32; ++k) gam[k] = G[(SC_GAMMA + k) * S + i];
+    double q[12];
+    for (int a = 0; a < 4; ++a)
+        for (int d = 0; d < 3; ++d) {
+            double t = ul[d] * gam[a];
+            for (int k = 1; k < 8; ++k) t = t + ul[3 * k + d] * gam[4 * k + a];
+            q[3 * a + d] = t;
+        }
+    double r[12];
+    for (int row = 0; row < 12; ++row) {
+        double t = G[(SC_H + h_index(0, row)) * S + i] * q[0];
+        for (int c = 1; c < 12; ++c) t = t + G[(SC_H + (row <= c ? h_index(row, c) : h_index(c, row))) * S + i] * q[c];
+        r[row] = t;
+    }
+    for (int k = 0; k < 8; ++k)
+        for (int d = 0; d < 3; ++d) {
+            double t = r[d] * gam[4 * k];
+            for (int a = 1; a < 4; ++a) t = t + r[3 * a + d] * gam[4 * k + a];
+            out[3 * k + d] = o[3 * k + d] + t;
+        }
+}
+
+__global__ void __launch_bounds__(SC_TPB) k_forces_scalar(ElementArrays el, NodeArrays nd, Control* ctls, int respect_done) {
+    FOR_ACTIVE(el.act_sc, el.n_sc, 1, g) {
+        int lane;
+        scalar_force_body(el, nd, ctls, respect_done, active_entity(el.act_sc, g, 1, &lane));
+    }
+}
+
+// The elastic elements' corner forces on node n, component d, added to f in
+// element order after the honeycomb ones (src/kernel.rs:192-201 adds the
+// scalar elements after the lane blocks' scatter).
+__device__ __forceinline__ double add_scalar_corners(const ElementArrays& el, const NodeArrays& nd, long long n, int d, double f) {
+    const uint32_t b = nd.sc_off[n], m = nd.sc_off[n + 1] - b;
+    for (uint32_t k = 0; k < m; ++k) f += el.sc_corner[3ull * nd.sc_slot[b + k] + d];
+    return f;
+}
+
 __global__ void k_gather(ElementArrays el, NodeArrays nd, double* __restrict__ f_out) {
     long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= nd.n) return;
     double fx, fy, fz;
     gather_node(nd, el.corner, n, fx, fy, fz);
+    if (el.n_sc > 0) {
+        fx = add_scalar_corners(el, nd, n, 0, fx);
+        fy = add_scalar_corners(el, nd, n, 1, fy);
+        fz = add_scalar_corners(el, nd, n, 2, fz);
+    }
     f_out[3 * n] = fx;
     f_out[3 * n + 1] = fy;
     f_out[3 * n + 2] = fz;
@@ -532,7 +649,8 @@ __device__ __forceinline__ void full_body(const ElementArrays& el, const NodeArr
     const int slot = nd.node_slot[n];
     const double fe = nd.f_ext[k], vh = nd.v_half[k], im = nd.inv_mass[n];
     const bool fixed = nd.fixed[n] != 0;
-    const double f = gather_component(nd, el.corner, n, d);
+    double f = gather_component(nd, el.corner, n, d);
+    if (el.n_sc > 0) f = add_scalar_corners(el, nd, n, d, f);
     const Control* ctl = ctls + slot;
     if (ctl->done) return;
     const double dt = step_dt(ctl);
@@ -1740,10 +1858,12 @@ __global__ void __launch_bounds__(VEH_TPB) k_vehicle_vx(VehicleArrays va, const 
 // ---------------------------------------------------------------------------
 void launch_setup_geometry(cudaStream_t s, long long n_all, const double* pos, const uint32_t* conn_all, const int32_t* part,
                            const double* mat, const int64_t* hc_index, const uint32_t* elem_slot, long long stride,
-                           float4* planes, double* volume, double* lumped, double* dt_factor, double* elem_mass, int* bad) {
+                           float4* planes, double* volume, double* lumped, double* dt_factor, double* elem_mass, int* bad,
+                           const int64_t* sc_index, long long n_sc, double* sc_geo) {
     if (n_all <= 0) return;
     k_setup_geometry<<<(unsigned)blocks_for(n_all, 128), 128, 0, s>>>(n_all, pos, conn_all, part, mat, hc_index, elem_slot,
-                                                                       stride, planes, volume, lumped, dt_factor, elem_mass, bad);
+                                                                       stride, planes, volume, lumped, dt_factor, elem_mass, bad,
+                                                                       sc_index, n_sc, sc_geo);
 }
 void launch_node_masses(cudaStream_t s, long long n, const uint32_t* off, const uint32_t* slot, const double* lumped,
                         double* mass, double* inv_mass) {
@@ -1754,11 +1874,14 @@ void launch_init_state(cudaStream_t s, long long n_hc, long long stride, float4*
     k_init_state<<<(unsigned)blocks_for(n_hc, TPB), TPB, 0, s>>>(n_hc, stride, state);
 }
 void launch_forces(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, int respect_done) {
-    if (el.n_hc <= 0) return;
     // Persistent: one wave of FORCES_MINB blocks per SM striding over the
     // active chunks (measured faster than several waves: no tail).
-    k_forces<<<active_grid(el.n_hc, 1, FORCES_TPB, 148 * FORCES_MINB), FORCES_TPB, 0, s>>>(el, nd, ctls, respect_done);
+    if (el.n_hc > 0)
+        k_forces<<<active_grid(el.n_hc, 1, FORCES_TPB, 148 * FORCES_MINB), FORCES_TPB, 0, s>>>(el, nd, ctls, respect_done);
+    if (el.n_sc > 0)
+        k_forces_scalar<<<active_grid(el.n_sc, 1, SC_TPB, GRID_CAP), SC_TPB, 0, s>>>(el, nd, ctls, respect_done);
 }
+int forces_launches(const ElementArrays& el) { return (el.n_hc > 0 ? 1 : 0) + (el.n_sc > 0 ? 1 : 0); }
 void launch_gather(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, double* f_out) {
     k_gather<<<(unsigned)blocks_for(nd.n, TPB), TPB, 0, s>>>(el, nd, f_out);
 }

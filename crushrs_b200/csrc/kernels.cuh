@@ -32,7 +32,17 @@ struct ElementArrays {
     double* elem_extra;      // per model element added mass (mass scaling)
     const uint32_t* elem_slot;  // crash slot per model element
     Active act_hc, act_all;     // active chunks of honeycomb / all elements
+    // Elastic (Hencky) elements: the reference's scalar f64 path
+    // (src/kernel.rs:116-156), element order.
+    long long n_sc;              // scalar elements visited (a run: those with a free node, numbered first)
+    long long sc_stride;         // all scalar elements (the plane stride of sc_geo)
+    const uint32_t* sc_model;    // scalar index -> model element
+    const double* sc_geo;        // SC_PLANES x sc_stride (SoA): grad 24, volume, gamma 32, H upper triangle 78
+    const double* sc_mat;        // 2 per scalar element: Young's modulus, Poisson ratio
+    double* sc_corner;           // 24 per scalar element: corner forces (f64)
+    Active act_sc;               // active chunks of scalar elements
 };
+constexpr int SC_GRAD = 0, SC_VOL = 24, SC_GAMMA = 25, SC_H = 57, SC_PLANES = 135;
 
 struct NodeArrays {
     long long n;
@@ -50,6 +60,8 @@ struct NodeArrays {
     const uint32_t* hc_slot;
     const uint32_t* all_off; // N+1 CSR over all model (element, corner) slots
     const uint32_t* all_slot;
+    const uint32_t* sc_off;  // N+1 CSR over scalar (element, corner) slots, element order
+    const uint32_t* sc_slot;
     const uint32_t* node_slot;  // crash slot per node
     const int* mass_flag;       // set when some crash scales its masses this step
     Active act_node;            // active chunks of nodes
@@ -185,8 +197,9 @@ struct ActiveBuild {
     int* lists;                  // same layout as the chunks
     int* counts;                 // ACTIVE_SPACES
 };
-constexpr int ACTIVE_SPACES = 8;  // honeycomb elements, all elements, nodes, searched entries (dynamic grids and the
-                                  // rest), contact nodes, moving faces, all primary-node entries, static-grid entries
+constexpr int ACTIVE_SPACES = 9;  // honeycomb elements, all elements, nodes, searched entries (dynamic grids and the
+                                  // rest), contact nodes, moving faces, all primary-node entries, static-grid entries,
+                                  // scalar elements
 
 // Vehicles of all crash slots: node lists and the reduction layout.
 struct VehicleArrays {
@@ -203,11 +216,15 @@ struct VehicleArrays {
 void launch_setup_geometry(cudaStream_t s, long long n_all, const double* pos, const uint32_t* conn_all,
                            const int32_t* part, const double* mat_e_nu_rho_hg, const int64_t* hc_index,
                            const uint32_t* elem_slot, long long stride, float4* planes, double* volume, double* lumped,
-                           double* dt_factor, double* elem_mass, int* bad);
+                           double* dt_factor, double* elem_mass, int* bad, const int64_t* sc_index, long long n_sc,
+                           double* sc_geo);
 void launch_node_masses(cudaStream_t s, long long n, const uint32_t* off, const uint32_t* slot, const double* lumped,
                         double* mass, double* inv_mass);
 void launch_init_state(cudaStream_t s, long long n_hc, long long stride, float4* state);
+// Element forces: the honeycomb lane kernel and, when the model has
+// elastic elements, the scalar f64 kernel (forces_launches of them).
 void launch_forces(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, int respect_done);
+int forces_launches(const ElementArrays& el);
 void launch_gather(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, double* f_out);
 void launch_half(cudaStream_t s, const NodeArrays& nd, Control* ctls);
 void launch_full(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls);
@@ -341,6 +358,13 @@ struct FrameArrays {
     const float4* state;        // honeycomb state planes
     long long state_stride;
     int node_blocks, elem_blocks;  // blocks per slot of the two copy kernels
+    // elastic elements: Hencky stress at the current u
+    const int64_t* sc_index;    // model element -> scalar index or -1 (null: none)
+    long long n_sc;
+    const double* sc_geo;
+    const double* sc_mat;
+    const uint32_t* conn_all;
+    const double* pos;
 };
 // One frame of every slot that is due (modes as for the histories).
 void launch_frames(cudaStream_t s, const FrameArrays& f, const double* u, const Control* ctls, int mode);

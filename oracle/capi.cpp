@@ -344,4 +344,22 @@ int64_t oracle_resample(const double* t, const double* y, int64_t n, double t0, 
     return (int64_t)a.size();
 }
 
+// symmetric_eigen3 (material.rs:570) on a row-major 3x3; eigenvectors as
+// the columns of the row-major evec.
+int oracle_symmetric_eigen3(const double* a, double* eval, double* evec) {
+    M3 m, v;
+    for (int k = 0; k < 9; ++k) m.m[k] = a[k];
+    symmetric_eigen3(m, eval, &v);
+    for (int k = 0; k < 9; ++k) evec[k] = v.m[k];
+    return 0;
+}
+// Hencky elastic Kirchhoff stress (material.rs:708-771), row-major F and tau.
+int oracle_hencky_elastic(double youngs, double poisson, const double* f, double* tau) {
+    M3 m, t;
+    for (int k = 0; k < 9; ++k) m.m[k] = f[k];
+    hencky_elastic(youngs, poisson, m, &t);
+    for (int k = 0; k < 9; ++k) tau[k] = t.m[k];
+    return 0;
+}
+
 }  // extern "C"

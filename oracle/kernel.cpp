@@ -119,7 +119,6 @@ std::string elements_build(const Model& m, bool simd, int threads, Elements* el)
     el->lumped.resize(8 * ne);
     el->simd_ids.clear();
     el->scalar_ids.clear();
-    std::set<uint32_t> fixed(m.fixed_nodes.begin(), m.fixed_nodes.end());
     for (const crush_material& mat : m.materials) {
         if (mat.model == CRUSH_MAT_HONEYCOMB) {
             HoneycombParams p;
@@ -154,10 +153,6 @@ std::string elements_build(const Model& m, bool simd, int threads, Elements* el)
     for (size_t e = 0; e < ne; ++e) {
         const crush_material& mat = m.materials[m.hex_part[e]];
         el->honeycomb[e] = mat.model == CRUSH_MAT_HONEYCOMB;
-        if (!el->honeycomb[e]) {
-            for (int i = 0; i < 8; ++i)
-                if (!fixed.count(m.hexes[e][i])) return "elastic elements must have every node fixed (rigid slab)";
-        }
         if (simd && el->honeycomb[e]) el->simd_ids.push_back(e);
         else el->scalar_ids.push_back(e);
     }
@@ -176,7 +171,7 @@ std::string elements_build(const Model& m, bool simd, int threads, Elements* el)
     return "";
 }
 
-// kernel.rs:116-156 (honeycomb; rigid elastic elements carry no force).
+// kernel.rs:116-156, the scalar f64 element (honeycomb rate form or Hencky elastic).
 static bool element_force(const Elements& el, size_t e, const double* u, double* out, RateState* st) {
     const double* pos = el.model->positions.data();
     double x[8][3], ul[24];
@@ -196,12 +191,19 @@ static bool element_force(const Elements& el, size_t e, const double* u, double*
         for (int k = 0; k < 24; ++k) out[k] = 0.0;
         return false;
     }
-    HoneycombParams p;
-    honeycomb_params(el.model->materials[el.part[e]], &p);
+    // Elements::stress_update (kernel.rs:100-114): the honeycomb rate form
+    // commits its state; an elastic material is Hencky with no state.
+    const crush_material& mat = el.model->materials[el.part[e]];
     M3 tau;
-    RateState ns;
-    honeycomb_rate_update(p, f, *st, &tau, &ns);
-    *st = ns;
+    if (el.honeycomb[e]) {
+        HoneycombParams p;
+        honeycomb_params(mat, &p);
+        RateState ns;
+        honeycomb_rate_update(p, f, *st, &tau, &ns);
+        *st = ns;
+    } else {
+        hencky_elastic(mat.youngs_modulus, mat.poisson_ratio, f, &tau);
+    }
     M3 finv;
     m3_inverse(f, &finv);
     M3 m = m3_mul(tau, m3_transpose(finv));
@@ -285,7 +287,7 @@ size_t compute_forces(Elements& el, const double* u, double* global) {
         parallel_for(el.threads, ns, 32, [&](long k) {
             size_t e = ids[k];
             outs[k].fill(0.0);
-            if (er[k] || !el.honeycomb[e]) return;
+            if (er[k]) return;
             if (!element_force(el, e, u, outs[k].data(), &states[k])) { er[k] = 1; newly_flag[k] = 1; }
         });
         for (long k = 0; k < ns; ++k) {

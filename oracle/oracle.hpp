@@ -63,6 +63,12 @@ std::string honeycomb_params(const crush_material& m, HoneycombParams* out);
 // Plasticity::yield_at (material.rs:83), the curve-based form.
 void plasticity_yield_at(const crush_material& m, double c, double* sy, double* h);
 double dilatational_wave_speed(const crush_material& m);  // material.rs:226
+// Closed-form eigen-decomposition of a symmetric 3x3 (material.rs:570):
+// eigenvalues ascending, unit eigenvectors as the columns of *evec.
+void symmetric_eigen3(const M3& a, double eval[3], M3* evec);
+// Kirchhoff stress of an elastic (Hencky) material at F: finite_strain_return
+// (material.rs:708-771) without plasticity.
+void hencky_elastic(double youngs, double poisson, const M3& f, M3* tau);
 
 struct RateState {  // material.rs:383
     M3 f_prev_inv, rotation;

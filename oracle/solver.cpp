@@ -172,7 +172,8 @@ std::string run(const Model& model, const RunOptions& opt, RunResults* res) {
 
     // Frames: the capture closure of crushrs::run (src/solver.rs:265-275)
     // with plastic_strain and cauchy_stress (src/kernel.rs:269-321). Elastic
-    // elements here are rigid slabs at F = I: zero stress and strain.
+    // elements have no plastic strain; their Cauchy stress is the Hencky
+    // tau / J at the current u (zero when inverted).
     res->frame_time.clear();
     res->frame_step.clear();
     res->frame_disp.clear();
@@ -198,6 +199,24 @@ std::string run(const Model& model, const RunOptions& opt, RunResults* res) {
                 sh(2, 0) = s6[5]; sh(2, 1) = s6[4]; sh(2, 2) = s6[2];
                 const M3 c = m3_mul(m3_mul(st.rotation, sh), m3_transpose(st.rotation));
                 c6[0] = c(0, 0); c6[1] = c(1, 1); c6[2] = c(2, 2); c6[3] = c(0, 1); c6[4] = c(1, 2); c6[5] = c(0, 2);
+            } else if (!honey && !elements.eroded[e]) {
+                const double* grad = elements.center_grad[e].data();
+                M3 f = m3_zero();
+                for (int i = 0; i < 8; ++i) {
+                    const size_t nd = elements.conn[e][i];
+                    for (int a = 0; a < 3; ++a) {
+                        const double xa = model.positions[3 * nd + a] + u[3 * nd + a];
+                        for (int b = 0; b < 3; ++b) f(a, b) += xa * grad[3 * i + b];
+                    }
+                }
+                const double j = m3_det(f);
+                if (j > 0.0) {
+                    const crush_material& mat = model.materials[model.hex_part[e]];
+                    M3 tau;
+                    hencky_elastic(mat.youngs_modulus, mat.poisson_ratio, f, &tau);
+                    c6[0] = tau(0, 0) / j; c6[1] = tau(1, 1) / j; c6[2] = tau(2, 2) / j;
+                    c6[3] = tau(0, 1) / j; c6[4] = tau(1, 2) / j; c6[5] = tau(0, 2) / j;
+                }
             }
             for (double x : c6) res->frame_stress.push_back((float)x);
         }

@@ -56,6 +56,8 @@ def load():
     lib.oracle_cfc_filter.argtypes = [dp, C.c_int64, C.c_double, C.c_double, dp]
     lib.oracle_resample.argtypes = [dp, dp, C.c_int64, C.c_double, C.c_double, C.c_double, dp, dp, C.c_int64]
     lib.oracle_resample.restype = C.c_int64
+    lib.oracle_symmetric_eigen3.argtypes = [dp, dp, dp]
+    lib.oracle_hencky_elastic.argtypes = [C.c_double, C.c_double, dp, dp]
     _lib = lib
     return lib
 
@@ -224,6 +226,20 @@ def run_history(desc, steps, accelerometers=(), cap=100000, simd=True, threads=1
     return {"records": nr.value, "time": t[:k], "step": np.array(st[:k], dtype=np.int64),
             "parts": parts[: k * n_parts * 11].reshape(k, n_parts, 11), "nodes": nodes[: k * n_nodes * 21].reshape(k, n_nodes, 21),
             "results": r}
+
+
+def symmetric_eigen3(a):
+    a = np.ascontiguousarray(a, dtype=np.float64).reshape(9)
+    ev, vec = np.zeros(3), np.zeros(9)
+    load().oracle_symmetric_eigen3(ptr(a), ptr(ev), ptr(vec))
+    return ev, vec.reshape(3, 3)
+
+
+def hencky_elastic(youngs, poisson, f):
+    f = np.ascontiguousarray(f, dtype=np.float64).reshape(9)
+    tau = np.zeros(9)
+    load().oracle_hencky_elastic(C.c_double(youngs), C.c_double(poisson), ptr(f), ptr(tau))
+    return tau.reshape(3, 3)
 
 
 def cfc_filter(x, dt, cfc):

@@ -8,7 +8,7 @@ import os
 import numpy as np
 import pytest
 
-from crushrs_b200 import scenarios as S
+from crushrs_b200 import abi, scenarios as S
 
 from . import oracle_lib as O
 from .golden.make_golden import block8_model, hex1_model
@@ -37,6 +37,16 @@ def test_oracle_reproduces_golden_run():
     assert np.array_equal(got, GOLDEN["run_f32"])
 
 
+def _elastic_dofs(d):
+    """Degrees of freedom of the nodes of elastic elements."""
+    hexes = np.ctypeslib.as_array(d.hexes, (d.n_hexes, 8))
+    part = np.ctypeslib.as_array(d.hex_part, (d.n_hexes,))
+    elastic = np.array([d.materials[p].model == abi.MAT_ELASTIC for p in part])
+    mask = np.zeros(d.n_nodes, bool)
+    mask[hexes[elastic].ravel()] = True
+    return np.repeat(mask, 3)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("case", ["hex1", "block8", "plain"])
 def test_device_forces_match_golden(case):
@@ -44,10 +54,14 @@ def test_device_forces_match_golden(case):
 
     m = _models()[case]
     ctx = Context(m.desc)
+    el = _elastic_dofs(m.desc)
     for u, f32, f64 in zip(GOLDEN[f"{case}_u"], GOLDEN[f"{case}_f32"], GOLDEN[f"{case}_f64"]):
         f = np.zeros_like(f32)
         ctx.compute_forces(u, f)
-        assert np.array_equal(f, f32), case
+        # bit-equal where only honeycomb elements act; the elastic road's
+        # f64 forces (round-off of F = I here) to 1e-9 of the largest force
+        assert np.array_equal(f[~el], f32[~el]), case
+        assert np.abs(f[el] - f32[el]).max(initial=0.0) <= 1e-9 * np.abs(f32).max(), case
         assert np.linalg.norm(f - f32) <= 1e-5 * np.linalg.norm(f32)
         assert np.linalg.norm(f - f64) <= 1e-4 * np.linalg.norm(f64)
 

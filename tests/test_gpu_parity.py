@@ -19,6 +19,7 @@ from crushrs_b200.engine import Context
 from crushrs_b200.model import single_hex
 
 from . import oracle_lib as O
+from .test_golden import _elastic_dofs
 
 pytestmark = pytest.mark.gpu
 
@@ -88,7 +89,11 @@ def test_forces_match_lane_kernel_on_identical_state(plain):
         assert rel <= 1e-5, (step, rel)
         per_node = np.abs(f_dev - f_ref).max() / np.abs(f_ref).max()
         assert per_node <= 1e-5
-        exact_steps += int(np.array_equal(f_dev, f_ref))
+        # bit-identical where only honeycomb elements act; the elastic road's
+        # f64 forces (round-off of F = I) to 1e-9 of the largest force
+        el = _elastic_dofs(plain.desc)
+        assert np.abs(f_dev[el] - f_ref[el]).max(initial=0.0) <= 1e-9 * np.abs(f_ref).max()
+        exact_steps += int(np.array_equal(f_dev[~el], f_ref[~el]))
     st_d, er_d = ctx.get_state()
     st_o, er_o = s.get_state()
     hc = np.array([plain.material(p).model == abi.MAT_HONEYCOMB for p in plain.hex_part()])
