@@ -24,6 +24,7 @@ STOP_END_TIME = 0
 STOP_SEPARATION = 1
 LAYOUT_HEADON = 0
 LAYOUT_TBONE = 1
+LAYOUT_BARRIER = 2
 
 STATUS_NAMES = {
     CRUSH_OK: "OK", CRUSH_NONE: "NONE", CRUSH_ERR_INVALID: "INVALID", CRUSH_ERR_NONFINITE: "NONFINITE",
@@ -136,6 +137,11 @@ class VehicleSpec(C.Structure):
         ("rail_box_width", C.c_double),
         ("rail_box_z", C.c_double * 2),
         ("rail_box_force_fraction", C.c_double),
+        ("crush_zone_length", C.c_double),
+        ("body_modulus", C.c_double),
+        ("crush_zone_mass", C.c_double),
+        ("bumper", C.c_double * 3),
+        ("crush_element_size", C.c_double),
     ]
 
 

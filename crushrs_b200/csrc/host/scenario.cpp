@@ -196,9 +196,28 @@ double frontal_area(const crush_vehicle_spec& v) { return v.size[1] * v.size[2];
 double contact_modulus(const crush_vehicle_spec& v) {
     return v.contact_modulus > 0.0 ? v.contact_modulus : v.material.youngs_modulus;
 }
-// Vehicle::contact_stiffness_per_node, src/vehicle.rs:384 (no crush zone: h_front = h).
+// Vehicle::has_crush_zone, src/vehicle.rs:323 (a length of 0 means the whole block).
+bool has_crush_zone(const crush_vehicle_spec& v) { return v.crush_zone_length > 0.0 && v.crush_zone_length < v.size[0] - 1e-9; }
+double bumper_thickness(const crush_vehicle_spec& v) { return has_crush_zone(v) && v.bumper[0] > 0.0 ? v.bumper[0] : 0.0; }
+double bumper_mass(const crush_vehicle_spec& v) { return bumper_thickness(v) > 0.0 ? v.bumper[1] : 0.0; }
+// Vehicle::honeycomb_length, src/vehicle.rs:374.
+double honeycomb_length(const crush_vehicle_spec& v) { return v.crush_zone_length - bumper_thickness(v); }
+double block_density(const crush_vehicle_spec& v) { return v.mass / (v.size[0] * v.size[1] * v.size[2]); }
+// Vehicle::crush_density / body_density, src/vehicle.rs:454-467.
+double crush_density(const crush_vehicle_spec& v) {
+    if (v.crush_zone_mass > 0.0 && has_crush_zone(v)) return (v.crush_zone_mass - bumper_mass(v)) / (honeycomb_length(v) * frontal_area(v));
+    return block_density(v);
+}
+double body_density(const crush_vehicle_spec& v) {
+    if (v.crush_zone_mass > 0.0 && has_crush_zone(v))
+        return (v.mass - v.crush_zone_mass) / ((v.size[0] - v.crush_zone_length) * frontal_area(v));
+    return block_density(v);
+}
+// Vehicle::contact_stiffness_per_node, src/vehicle.rs:384: the crush zone's
+// element length at the front when there is a crush zone.
 double contact_stiffness_per_node(const crush_vehicle_spec& v, size_t n_face, double h) {
-    return contact_modulus(v) * frontal_area(v) / ((double)n_face * h);
+    const double h_front = has_crush_zone(v) && v.crush_element_size > 0.0 ? v.crush_element_size : h;
+    return contact_modulus(v) * frontal_area(v) / ((double)n_face * h_front);
 }
 bool in_rail_box(const crush_vehicle_spec& v, double y, double z) {
     return v.has_rail_box && std::fabs(y) < 0.5 * v.rail_box_width && z > v.rail_box_z[0] && z < v.rail_box_z[1];
@@ -213,32 +232,148 @@ void rail_box_factors(const crush_vehicle_spec& v, double area_fraction, double*
 
 crush_material crush_material_of(const crush_vehicle_spec& v) {
     crush_material m = v.material;
-    if (!(m.density > 0.0)) m.density = v.mass / (v.size[0] * v.size[1] * v.size[2]);
+    if (!(m.density > 0.0)) m.density = crush_density(v);
     return m;
 }
 
-// add_vehicle, src/vehicle.rs:663 (uniform block); the rail box, when asked,
-// is carved out of the whole block (src/vehicle.rs:710-733 does it on the crush zone).
+// Move the elements of part `from` whose cross-section centroid lies in the
+// rail box to a new part `to` (src/vehicle.rs:713-731).
+void carve_rail_box(crush_model* m, const VehicleCtx& vc, int from, const std::string& to_name) {
+    size_t to = add_part(m, to_name);
+    for (size_t e = 0; e < m->hex_part.size(); ++e) {
+        if (m->hex_part[e] != from) continue;
+        double ys = 0.0, zs = 0.0;
+        for (int i = 0; i < 8; ++i) {
+            ys += m->positions[3 * m->hexes[8 * e + i] + 1];
+            zs += m->positions[3 * m->hexes[8 * e + i] + 2];
+        }
+        double yc = ys / 8.0 - vc.y_center, zc = zs / 8.0 - vc.z_bottom;
+        if (in_rail_box(*vc.spec, yc, zc)) m->hex_part[e] = (int32_t)to;
+    }
+}
+
+// Mesh::merge_coincident_nodes, src/mesh.rs:176-233: nodes within `tol` of
+// an earlier kept node (looked up in its rounded cell and the 26 around it)
+// merge into it; the kept nodes are renumbered in order and every element,
+// face and node set follows (node sets sorted, duplicates dropped).
+size_t merge_coincident_nodes(crush_model* m, double tol) {
+    const size_t n = m->positions.size() / 3;
+    auto key = [&](const double* p) {
+        return std::array<long long, 3>{(long long)std::round(p[0] / tol), (long long)std::round(p[1] / tol), (long long)std::round(p[2] / tol)};
+    };
+    std::map<std::array<long long, 3>, size_t> first;
+    std::vector<uint32_t> map(n, 0);
+    std::vector<double> kept;
+    kept.reserve(3 * n);
+    size_t merged = 0;
+    for (size_t i = 0; i < n; ++i) {
+        const double* p = &m->positions[3 * i];
+        const std::array<long long, 3> k = key(p);
+        long long found = -1;
+        for (int dx = -1; dx <= 1 && found < 0; ++dx)
+            for (int dy = -1; dy <= 1 && found < 0; ++dy)
+                for (int dz = -1; dz <= 1 && found < 0; ++dz) {
+                    auto it = first.find({k[0] + dx, k[1] + dy, k[2] + dz});
+                    if (it == first.end()) continue;
+                    const double* q = &kept[3 * it->second];
+                    if (std::fabs(q[0] - p[0]) <= tol && std::fabs(q[1] - p[1]) <= tol && std::fabs(q[2] - p[2]) <= tol)
+                        found = (long long)it->second;
+                }
+        if (found >= 0) {
+            map[i] = (uint32_t)found;
+            ++merged;
+        } else {
+            map[i] = (uint32_t)(kept.size() / 3);
+            first[k] = kept.size() / 3;
+            kept.insert(kept.end(), p, p + 3);
+        }
+    }
+    if (merged == 0) return 0;
+    m->positions = kept;
+    m->velocity.assign(kept.size(), 0.0);
+    for (uint32_t& x : m->hexes) x = map[x];
+    for (auto& f : m->faces)
+        for (uint32_t& x : f) x = map[x];
+    for (auto& kv : m->node_sets) {
+        std::vector<uint32_t> v;
+        for (uint32_t x : kv.second) v.push_back(map[x]);
+        std::sort(v.begin(), v.end());
+        v.erase(std::unique(v.begin(), v.end()), v.end());
+        kv.second = v;
+    }
+    for (uint32_t& x : m->fixed) x = map[x];
+    return merged;
+}
+
+// add_vehicle, src/vehicle.rs:663-748. A homogeneous block (the rail box,
+// when asked, is then carved out of the whole block), or the two-part
+// vehicle: body block (part <name>), crush-zone block (<name>_crush) and an
+// optional one-element bumper layer (<name>_bumper) with matching y/z grids,
+// rear to front along the heading, underbody faces merged into
+// <name>_bottom, the rail box carved out of the crush zone and the bumper,
+// coincident nodes merged, and node set <name> spanning all the parts.
 void add_vehicle(crush_model* m, VehicleCtx& vc, double front_x, bool plus_x, double h) {
     const crush_vehicle_spec& v = *vc.spec;
     double x0 = plus_x ? front_x - v.size[0] : front_x;
     int face = plus_x ? XMax : XMin;
     double origin[3] = {x0, vc.y_center - v.size[1] / 2.0, vc.z_bottom};
-    add_hex_block(m, vc.name, origin, v.size, h, {{face, vc.name + "_front"}, {ZMin, vc.name + "_bottom"}});
-    if (v.has_rail_box) {
-        int from = part_index(m, vc.name);
-        size_t to = add_part(m, vc.name + "_rails");
-        for (size_t e = 0; e < m->hex_part.size(); ++e) {
-            if (m->hex_part[e] != from) continue;
-            double ys = 0.0, zs = 0.0;
-            for (int i = 0; i < 8; ++i) {
-                ys += m->positions[3 * m->hexes[8 * e + i] + 1];
-                zs += m->positions[3 * m->hexes[8 * e + i] + 2];
-            }
-            double yc = ys / 8.0 - vc.y_center, zc = zs / 8.0 - vc.z_bottom;
-            if (in_rail_box(v, yc, zc)) m->hex_part[e] = (int32_t)to;
-        }
+    const std::string front = vc.name + "_front", bottom = vc.name + "_bottom";
+    if (!has_crush_zone(v)) {
+        add_hex_block(m, vc.name, origin, v.size, h, {{face, front}, {ZMin, bottom}});
+        if (v.has_rail_box) carve_rail_box(m, vc, part_index(m, vc.name), vc.name + "_rails");
+        return;
     }
+    const double t_b = bumper_thickness(v);
+    const double l_c = v.crush_zone_length - t_b;
+    const double l_b = v.size[0] - v.crush_zone_length;
+    auto count = [](double len, double step) { return (int32_t)std::max(std::round(len / step), 1.0); };
+    const int32_t ny = count(v.size[1], h), nz = count(v.size[2], h), nxb = count(l_b, h);
+    const int32_t nxc = count(l_c, v.crush_element_size > 0.0 ? v.crush_element_size : h);
+    const double body_x0 = plus_x ? x0 : x0 + l_c + t_b;
+    const double crush_x0 = plus_x ? x0 + l_b : x0 + t_b;
+    const double bumper_x0 = plus_x ? x0 + l_b + l_c : x0;
+    auto sub = [&](const char* part) { return bottom + "_" + part; };
+    {
+        const double o[3] = {body_x0, origin[1], origin[2]}, sz[3] = {l_b, v.size[1], v.size[2]};
+        const int32_t n[3] = {nxb, ny, nz};
+        add_hex_block_n(m, vc.name, o, sz, n, {{ZMin, sub("body")}});
+    }
+    const std::string crush_name = vc.name + "_crush", bumper_name = vc.name + "_bumper";
+    std::vector<std::string> names{crush_name}, bottoms{sub("body"), sub("crush")};
+    {
+        const double o[3] = {crush_x0, origin[1], origin[2]}, sz[3] = {l_c, v.size[1], v.size[2]};
+        const int32_t n[3] = {nxc, ny, nz};
+        if (t_b > 0.0) add_hex_block_n(m, crush_name, o, sz, n, {{ZMin, sub("crush")}});
+        else add_hex_block_n(m, crush_name, o, sz, n, {{face, front}, {ZMin, sub("crush")}});
+    }
+    if (t_b > 0.0) {
+        const double o[3] = {bumper_x0, origin[1], origin[2]}, sz[3] = {t_b, v.size[1], v.size[2]};
+        const int32_t n[3] = {1, ny, nz};
+        add_hex_block_n(m, bumper_name, o, sz, n, {{face, front}, {ZMin, sub("bumper")}});
+        names.push_back(bumper_name);
+        bottoms.push_back(sub("bumper"));
+    }
+    std::vector<size_t> bottom_faces;
+    for (const std::string& b : bottoms) {
+        auto it = m->face_set_index.find(b);
+        if (it == m->face_set_index.end()) continue;
+        const std::vector<size_t>& set = m->face_set_list[it->second];
+        bottom_faces.insert(bottom_faces.end(), set.begin(), set.end());
+        m->face_set_index.erase(it);
+    }
+    m->face_set_index[bottom] = m->face_set_list.size();
+    m->face_set_list.push_back(bottom_faces);
+    if (v.has_rail_box) {
+        const int crush_part = part_index(m, crush_name), bumper_part = part_index(m, bumper_name);
+        carve_rail_box(m, vc, crush_part, vc.name + "_rails");
+        if (bumper_part >= 0) carve_rail_box(m, vc, bumper_part, vc.name + "_bumper_rails");
+    }
+    merge_coincident_nodes(m, 1e-6 * h);
+    std::vector<uint32_t> all = m->node_sets[vc.name];
+    for (const std::string& nm : names) all.insert(all.end(), m->node_sets[nm].begin(), m->node_sets[nm].end());
+    std::sort(all.begin(), all.end());
+    all.erase(std::unique(all.begin(), all.end()), all.end());
+    m->node_sets[vc.name] = all;
 }
 
 void set_velocity(crush_model* m, const std::string& set, const double v[3]) {
@@ -246,24 +381,35 @@ void set_velocity(crush_model* m, const std::string& set, const double v[3]) {
         for (int d = 0; d < 3; ++d) m->velocity[3 * n + d] = v[d];
 }
 
-// assign_vehicle, src/vehicle.rs:750 (+ the rail-box split of :755-770).
+// assign_vehicle, src/vehicle.rs:750-790: materials (the rail box and the
+// skin of the crush zone scaled by rail_box_factors over their element
+// counts; a two-part vehicle's elastic body and bumper plate) and the
+// initial velocity of node set <name>.
 void assign_vehicle(crush_model* m, const VehicleCtx& vc, const double vel[3]) {
     const crush_vehicle_spec& v = *vc.spec;
     crush_material crush = crush_material_of(v);
-    int skin = part_index(m, vc.name);
+    const bool two_part = has_crush_zone(v) && part_index(m, vc.name + "_crush") >= 0;
+    if (two_part) m->materials[part_index(m, vc.name)] = elastic_material(v.body_modulus, 0.3, body_density(v));
+    int skin = part_index(m, two_part ? vc.name + "_crush" : vc.name);
     int rails = v.has_rail_box ? part_index(m, vc.name + "_rails") : -1;
+    double fr = 1.0, fs = 1.0;
     if (rails >= 0) {
         size_t n_rails = 0, n_skin = 0;
         for (int32_t p : m->hex_part) {
             n_rails += p == rails;
             n_skin += p == skin;
         }
-        double fr = 1.0, fs = 1.0;
         if (n_rails > 0 && n_skin > 0) rail_box_factors(v, (double)n_rails / (double)(n_rails + n_skin), &fr, &fs);
         m->materials[rails] = scaled(crush, fr);
         m->materials[skin] = scaled(crush, fs);
     } else {
-        m->materials[skin] = crush;
+        m->materials[skin] = two_part ? scaled(crush, fs) : crush;
+    }
+    if (two_part && bumper_thickness(v) > 0.0) {
+        const crush_material plate = elastic_material(v.bumper[2], 0.3, v.bumper[1] / (v.bumper[0] * frontal_area(v)));
+        const int bumper = part_index(m, vc.name + "_bumper"), bumper_rails = part_index(m, vc.name + "_bumper_rails");
+        if (bumper >= 0) m->materials[bumper] = scaled(plate, fs);
+        if (bumper_rails >= 0) m->materials[bumper_rails] = scaled(plate, fr);
     }
     set_velocity(m, vc.name, vel);
 }
@@ -394,6 +540,14 @@ int check_spec(const crush_vehicle_spec& v) {
         return crush::fail(CRUSH_ERR_INVALID, "a vehicle needs a positive mass and size");
     if (v.material.model != CRUSH_MAT_HONEYCOMB) return crush::fail(CRUSH_ERR_UNSUPPORTED, "vehicle crush material must be honeycomb");
     if (!(v.material.youngs_modulus > 0.0)) return crush::fail(CRUSH_ERR_INVALID, "vehicle modulus must be positive");
+    if (has_crush_zone(v)) {
+        if (!(v.body_modulus > 0.0)) return crush::fail(CRUSH_ERR_INVALID, "a crush zone needs a positive body modulus");
+        if (v.crush_zone_mass > 0.0 && !(v.crush_zone_mass < v.mass)) return crush::fail(CRUSH_ERR_INVALID, "crush zone mass must be below the vehicle mass");
+        if (v.bumper[0] > 0.0 && (!(v.bumper[0] < v.crush_zone_length) || !(v.bumper[1] > 0.0) || !(v.bumper[2] > 0.0)))
+            return crush::fail(CRUSH_ERR_INVALID, "a bumper needs thickness below the crush zone length, a positive mass and modulus");
+        if (v.crush_zone_mass > 0.0 && !(v.crush_zone_mass > bumper_mass(v)))
+            return crush::fail(CRUSH_ERR_INVALID, "crush zone mass must exceed the bumper mass");
+    }
     return CRUSH_OK;
 }
 
@@ -420,7 +574,7 @@ int crush_scenario_build(const crush_scenario* s, crush_model** out) {
     if (!s || !out) return crush::fail(CRUSH_ERR_INVALID, "null scenario");
     *out = nullptr;
     int st = check_spec(s->a);
-    if (st == CRUSH_OK) st = check_spec(s->b);
+    if (st == CRUSH_OK && s->layout != CRUSH_LAYOUT_BARRIER) st = check_spec(s->b);
     if (st != CRUSH_OK) return st;
     if (!(s->element_size > 0.0)) return crush::fail(CRUSH_ERR_INVALID, "element size must be positive");
     crush_model* m = new crush_model();
@@ -472,13 +626,40 @@ int crush_scenario_build(const crush_scenario* s, crush_model** out) {
         face_set_nodes(m, "b_front", &fb);
         double k = std::min(contact_stiffness_per_node(s->b, fb.size(), h), contact_stiffness_per_node(s->a, fb.size(), h));
         add_contact_pair_scaled(m, "a_front", "b_front", k, 0.3, {}, {});
+    } else if (s->layout == CRUSH_LAYOUT_BARRIER) {
+        // barrier_model, src/vehicle.rs:951-973: A into a fixed elastic wall
+        // (add_rigid_wall, :851: face set wall_face at x = 0 facing -x), the
+        // road under A, and A's front against the wall at A's per-node
+        // penalty stiffness.
+        const crush_vehicle_spec& v = s->a;
+        add_vehicle(m, a, -gap, true, h);
+        const double w = v.size[1], z = v.size[2], thickness = 0.2;
+        {
+            const double y0 = -w * 0.75, y1 = w * 0.75, z0 = -0.2 * z, z1 = 1.2 * z;
+            const double hw = std::max(std::min(y1 - y0, z1 - z0) / 4.0, thickness);
+            const double origin[3] = {0.0, y0, z0}, size[3] = {thickness, y1 - y0, z1 - z0};
+            add_hex_block(m, "wall", origin, size, hw, {{XMin, "wall_face"}});
+        }
+        if (road) {
+            double xr[2] = {-v.size[0] - 1.0, -0.3}, yr[2] = {-w, w};
+            add_ground(m, -s->clearance, xr, yr, 0.3);
+        }
+        double va[3] = {s->speed_a, 0.0, 0.0};
+        assign_vehicle(m, a, va);
+        const int wall = part_index(m, "wall");
+        m->materials[wall] = elastic_material(1e9, 0.3, 1000.0);
+        for (uint32_t n : m->node_sets["wall"]) m->fixed.push_back(n);
+        if (road) add_ground_contact(m, a, s->clearance, h, false);
+        std::vector<uint32_t> fa;
+        face_set_nodes(m, "a_front", &fa);
+        add_contact_pair_scaled(m, "a_front", "wall_face", contact_stiffness_per_node(v, fa.size(), h), 0.3, front_contact_scales(m, a, h), {});
     } else {
         delete m;
         return crush::fail(CRUSH_ERR_INVALID, "unknown layout");
     }
     m->settings = s->settings;
     add_vehicle_output(m, "a", "a_front");
-    add_vehicle_output(m, "b", "b_front");
+    if (s->layout != CRUSH_LAYOUT_BARRIER) add_vehicle_output(m, "b", "b_front");
     *out = m;
     return CRUSH_OK;
 }

@@ -59,8 +59,15 @@ def elastic(youngs, poisson, density):
     return m
 
 
-def vehicle(mass, size, material, contact_modulus=0.0, rail_box=None):
-    """A crushable block (crush_vehicle_spec). rail_box = (width, (z0, z1), force_fraction)."""
+def vehicle(mass, size, material, contact_modulus=0.0, rail_box=None, crush_zone_length=0.0, body_modulus=0.0,
+            crush_zone_mass=0.0, bumper=None, crush_element_size=0.0):
+    """A crushable vehicle (crush_vehicle_spec). rail_box = (width, (z0, z1),
+    force_fraction). With 0 < crush_zone_length < length it is the
+    reference's two-part vehicle (src/vehicle.rs:663-790): a honeycomb crush
+    zone of that length (with `crush_zone_mass` kg, elements of
+    `crush_element_size` along x) in front of an elastic body of modulus
+    `body_modulus`, and bumper = (thickness, mass, modulus) an elastic front
+    layer."""
     v = abi.VehicleSpec()
     v.mass = mass
     for i in range(3):
@@ -72,7 +79,60 @@ def vehicle(mass, size, material, contact_modulus=0.0, rail_box=None):
         v.rail_box_width = rail_box[0]
         v.rail_box_z[0], v.rail_box_z[1] = rail_box[1]
         v.rail_box_force_fraction = rail_box[2]
+    v.crush_zone_length = crush_zone_length
+    v.body_modulus = body_modulus
+    v.crush_zone_mass = crush_zone_mass
+    if bumper is not None:
+        for i in range(3):
+            v.bumper[i] = bumper[i]
+    v.crush_element_size = crush_element_size
     return v
+
+
+LOCK_COMPACTION = 1.4    # src/vehicle.rs:503
+LOCK_SLOPE_FACTOR = 1.0  # src/vehicle.rs:504
+
+
+def force_table_material(modulus, density, table, honeycomb_length, area, transverse=TRANSVERSE_FACTOR):
+    """Vehicle::crush_material_axial with a force-crush table
+    (src/vehicle.rs:478-488, yield_curve :509): compaction c = -ln(1 - x/L_c)
+    (x/L_c capped at 0.95), yield stress F/A, locking up at c = 1.4 with slope
+    1.0 E."""
+    curve = [(-math.log(1.0 - min(x / honeycomb_length, 0.95)), f / area) for x, f in table]
+    return honeycomb(modulus, density, curve=curve, densification=(LOCK_COMPACTION, LOCK_SLOPE_FACTOR * modulus), transverse=transverse)
+
+
+def _pulse_vehicle(mass, size, crush_zone, crush_zone_mass, bumper, rail_box, modulus, body_modulus, knots, force_kn,
+                   crush_element_size=0.1):
+    area = size[1] * size[2]
+    l_c = crush_zone - bumper[0]
+    density = (crush_zone_mass - bumper[1]) / (l_c * area)  # Vehicle::crush_density
+    mat = force_table_material(modulus, density, [(x, f * 1e3) for x, f in zip(knots, force_kn)], l_c, area)
+    return vehicle(mass, size, mat, contact_modulus=modulus, rail_box=rail_box, crush_zone_length=crush_zone,
+                   body_modulus=body_modulus, crush_zone_mass=crush_zone_mass, bumper=bumper,
+                   crush_element_size=crush_element_size)
+
+
+def neon_1996_pulse():
+    """Vehicle::dodge_neon_1996_pulse (src/vehicle.rs:541-566): the Neon
+    fitted to a rear-seat barrier pulse, a 1.5 m crush zone of 0.1 m
+    elements and 190 kg with a 0.1 m bumper, ahead of an elastic body, and a
+    rail box carrying 80 % of the force."""
+    return _pulse_vehicle(1354.0, (4.36, 1.71, 1.35), 1.5, 190.0, (0.1, 25.0, 3.0e8), (0.45, (0.06, 0.41), 0.8), 4e6, 2.7e8,
+                          [0.0, 0.1165, 0.2330, 0.3496, 0.4661, 0.5826, 0.6991], [13.0, 135.0, 135.0, 146.0, 361.0, 364.0, 364.0])
+
+
+def ford_expedition_1999(mass=2460.0, size=(5.2, 2.0, 1.9)):
+    """Vehicle::ford_expedition_1999 (src/vehicle.rs:568-593): a 1.7 m crush
+    zone with 320 kg and a bumper, the rail box carrying 75 % of the force."""
+    return _pulse_vehicle(mass, size, 1.7, 320.0, (0.1, 35.0, 3.0e8), (1.25, (0.15, 0.72), 0.75), 7.3e6, 3.93e8,
+                          [0.0, 0.1064, 0.2128, 0.3192, 0.4256, 0.5320, 0.6384], [29.0, 183.0, 259.0, 417.0, 457.0, 457.0, 457.0])
+
+
+def lincoln_navigator_1999():
+    """Vehicle::lincoln_navigator_1999 (src/vehicle.rs:595-603): the
+    Expedition structure with 2873 kg and 5.175 x 2.049 x 1.9 m."""
+    return ford_expedition_1999(2873.0, (5.175, 2.049, 1.9))
 
 
 def _preset(mass, size, yield_force, stiffness, modulus):
@@ -183,6 +243,18 @@ class Model:
         w = self.desc.vehicles[v]
         return (np.ctypeslib.as_array(w.nodes, (w.n_nodes,)), int(w.accel_node),
                 np.ctypeslib.as_array(w.front_nodes, (w.n_front,)))
+
+
+PULSE_END = 0.15  # src/vehicle.rs:1104
+PULSE_DT = 1e-4   # src/vehicle.rs:1102
+
+
+def barrier(v, speed, element_size=TUNED_ELEMENT_SIZE, end_time=PULSE_END, clearance=0.15, **settings_kw):
+    """barrier_model (src/vehicle.rs:951): vehicle v at `speed` into a fixed
+    rigid wall at x = 0, on the road."""
+    dummy = vehicle(1.0, (1.0, 1.0, 1.0), honeycomb(1.0, 1.0))
+    return scenario(v, dummy, speed, 0.0, clearance=clearance, element_size=element_size, layout=abi.LAYOUT_BARRIER,
+                    end_time=end_time, **settings_kw)
 
 
 def crash_30_30():

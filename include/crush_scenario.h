@@ -25,21 +25,32 @@
 extern "C" {
 #endif
 
-/* A homogeneous crushable vehicle block (the reference's Vehicle with the
- * crush zone spanning the whole block). */
+/* A crushable vehicle (the reference's Vehicle, src/vehicle.rs:107-196):
+ * a homogeneous honeycomb block, or with crush_zone_length in (0, length)
+ * the two-part vehicle of add_vehicle / assign_vehicle (src/vehicle.rs:663-790):
+ * an elastic body (part <name>), a honeycomb crush zone in front of it
+ * (<name>_crush), an optional elastic bumper layer at the very front
+ * (<name>_bumper), and an optional rail box carved out of the crush zone
+ * (<name>_rails) and the bumper (<name>_bumper_rails). */
 typedef struct crush_vehicle_spec {
     double mass;             /* kg */
     double size[3];          /* length (x), width (y), height (z), m */
-    crush_material material; /* crush material; density <= 0 means mass / volume */
+    crush_material material; /* crush material; density <= 0 means the crush zone's mass / volume */
     double contact_modulus;  /* modulus for the penalty stiffness (Pa); <= 0: material E */
-    int32_t has_rail_box;    /* carve a rail box (CRUSH: whole block is the crush zone) */
+    int32_t has_rail_box;    /* carve a rail box (a homogeneous block: out of the whole block) */
     double rail_box_width;   /* m, centred on the block */
     double rail_box_z[2];    /* m above the block bottom */
     double rail_box_force_fraction;
+    double crush_zone_length;  /* m, bumper included; <= 0 or >= length: the whole block is the crush zone */
+    double body_modulus;       /* Pa, the elastic body's modulus (Poisson ratio 0.3, Vehicle::body_material) */
+    double crush_zone_mass;    /* kg of the crush zone with its bumper; <= 0: uniform density */
+    double bumper[3];          /* thickness m, mass kg, modulus Pa of the bumper layer; thickness <= 0: none */
+    double crush_element_size; /* m along x inside the crush zone; <= 0: the block element size */
 } crush_vehicle_spec;
 
 #define CRUSH_LAYOUT_HEADON 0 /* A heads +x, B heads -x, noses 2*5 mm apart (rear-end: negative speed_b) */
 #define CRUSH_LAYOUT_TBONE 1  /* A heads +x into the -x side of B; B is given as its side profile */
+#define CRUSH_LAYOUT_BARRIER 2 /* A heads +x into a fixed rigid wall at x = 0 (barrier_model, src/vehicle.rs:951); B unused */
 
 typedef struct crush_scenario {
     int32_t layout;

@@ -118,3 +118,28 @@ def test_elastic_frames_match_oracle():
     last = ctx.frame(n - 1)["stress"].reshape(-1, 6)
     assert np.abs(last[elastic]).max() > 0.0  # the elastic bodies carry stress by step 60
     ctx.close()
+
+
+@pytest.mark.parametrize("case", ["barrier", "headon"])
+def test_two_part_vehicles_match_oracle(case):
+    """The reference's two-part vehicles (honeycomb crush zone with a rail
+    box, elastic bumper and body): the pulse-fitted Neon into the rigid
+    barrier at 35 mph (src/vehicle.rs:951, :541) and head-on into the
+    Navigator at 30.14 mph each (the car-to-car test the rail boxes were
+    fitted to, src/headon.rs:40-66). Delta-v within 0.5 % of both oracles."""
+    if case == "barrier":
+        scen = S.barrier(S.neon_1996_pulse(), 35 * S.MPH)
+    else:
+        scen = S.scenario(S.lincoln_navigator_1999(), S.neon_1996_pulse(), 30.14 * S.MPH, 30.14 * S.MPH, element_size=0.3,
+                          end_time=S.PULSE_END)
+    m = S.Model.build(scen)
+    ctx = Context(m.desc)
+    r = ctx.run()
+    ctx.close()
+    assert r.status == 0 and r.steps > 1000
+    for simd in (True, False):
+        o, _, _, _, _ = O.run(m.desc, simd=simd, threads=8)
+        assert abs(r.steps - o.steps) <= 2
+        for k in range(m.desc.n_vehicles):
+            dv, dvo = r.vehicle[k].delta_v[0], o.vehicle[k].delta_v[0]
+            assert abs(dv - dvo) <= 5e-3 * abs(dvo), (case, simd, k, dv, dvo)

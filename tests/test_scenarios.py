@@ -54,3 +54,47 @@ def test_seeded_workloads_are_deterministic():
     assert 250 <= min(sizes) and max(sizes) <= 7000
     kinds = [S.serve_query(i)[0] for i in range(60)]
     assert set(kinds) == set(S.SERVE_KINDS)
+
+
+def test_two_part_vehicle_parts_and_mass():
+    """The reference's two-part vehicle (add_vehicle / assign_vehicle,
+    src/vehicle.rs:663-790) for the pulse-fitted Neon in the barrier model
+    (src/vehicle.rs:951): body, crush zone, bumper, rail box and bumper rails
+    with the rail-box factors over the element counts; coincident interface
+    nodes merged; every part's mass adds up to the test mass."""
+    from . import oracle_lib as O
+
+    v = S.neon_1996_pulse()
+    m = S.Model.build(S.barrier(v, 35 * S.MPH))
+    part = m.hex_part()
+    counts = np.bincount(part, minlength=m.desc.n_parts)
+    # body 10x6x5, crush zone 14x6x5 (0.1 m along x) minus the rail box, bumper 1x6x5 minus its rails
+    assert list(counts[:5]) == [300, 364, 26, 56, 4]
+    assert m.desc.n_vehicles == 1 and m.desc.n_contacts == 3
+    # nodes: blocks 11x7x6 + 15x7x6 + 2x7x6 with two interfaces of 7x6 merged, wall 2x6x5, road 13x9x2
+    assert m.n_nodes == (462 + 630 + 84 - 2 * 42) + 60 + 234
+    mats = [m.material(p) for p in range(m.desc.n_parts)]
+    assert mats[0].model == abi.MAT_ELASTIC and mats[0].youngs_modulus == 2.7e8 and mats[0].poisson_ratio == 0.3
+    assert mats[1].model == abi.MAT_HONEYCOMB and mats[3].model == abi.MAT_HONEYCOMB
+    f_rails, f_skin = 0.8 / (56 / 420), 0.2 / (1 - 56 / 420)  # Vehicle::rail_box_factors
+    assert abs(mats[3].youngs_modulus / mats[1].youngs_modulus - f_rails / f_skin) < 1e-9 * f_rails / f_skin
+    assert abs(mats[4].youngs_modulus / mats[2].youngs_modulus - f_rails / f_skin) < 1e-9 * f_rails / f_skin
+    lumped, _ = O.Session(m.desc).masses()
+    nodes, _, front = m.vehicle(0)
+    assert abs(lumped[nodes].sum() - 1354.0) < 1e-9 * 1354.0
+    x = m.positions()
+    assert np.all(x[front, 0] == x[front, 0].max())  # the bumper's front face, heading +x
+    assert len(np.unique(x[nodes].round(9), axis=0)) == len(nodes)  # no coincident nodes left
+
+
+def test_two_part_headon_builds_both_headings():
+    a, b = S.neon_1996_pulse(), S.lincoln_navigator_1999()
+    m = S.Model.build(S.scenario(a, b, 13.4, 13.4, element_size=0.3))
+    x = m.positions()
+    for k, sign in ((0, 1.0), (1, -1.0)):
+        nodes, accel, front = m.vehicle(k)
+        # the front face is the vehicle's extreme along its heading, the accelerometer in its body
+        ext = x[nodes, 0].max() if sign > 0 else x[nodes, 0].min()
+        assert np.all(x[front, 0] == ext)
+        assert sign * (x[accel, 0] - x[front, 0].mean()) < -1.0
+    assert m.desc.n_contacts == 4
