@@ -170,6 +170,7 @@ def declare_scenario_api(lib):
     lib.crush_model_desc_get.argtypes = [C.c_void_p, P(ModelDesc)]
     lib.crush_model_settings.argtypes = [C.c_void_p]
     lib.crush_model_settings.restype = P(Settings)
+    lib.crush_model_vehicle_frame.argtypes = [C.c_void_p, C.c_int32, P(C.c_uint32)]
     lib.crush_model_new.argtypes = [P(C.c_void_p)]
     lib.crush_model_add_block.argtypes = [C.c_void_p, P(C.c_double), P(C.c_double), P(C.c_int32), C.c_int32, P(C.c_int32)]
     lib.crush_model_face_set.argtypes = [C.c_void_p, C.c_int32, P(C.c_int64), P(C.c_uint32)]

@@ -1,0 +1,295 @@
+"""Calibration drivers as clients of the batched engine.
+
+The reference fits vehicles to measured crash pulses by running many
+independent impacts (src/headon.rs:147-250 calibrate_rail_boxes: a
+differential evolution whose generations are independent runs). Here every
+generation's trials run as ONE batched context on the GPU, each trial a crash
+slot recording its two rear-seat accelerometers every step on the device;
+the pulses are then taken from the device histories (src/signal.rs:129-146
+Pulse::from_history: local-x acceleration resampled to 0.1 ms, CFC 60).
+
+Pieces restated from the reference: Pulse and its integrals
+(src/signal.rs:68-210), PulseComparison and pulse_objective
+(src/vehicle.rs:1047-1135), the rail-box unit-cube parameterisation and the
+xorshift64* generator (src/headon.rs:88-131), and the synchronous
+rand/1/bin differential evolution of calibrate_rail_boxes
+(src/headon.rs:147-250).
+"""
+import math
+
+import numpy as np
+
+from . import scenarios as S
+from .engine import Context
+from .pulse import cfc_filter, resample
+
+PULSE_DT = S.PULSE_DT
+PULSE_END = S.PULSE_END
+G = 9.81
+
+
+def integrate(t, y, y0):
+    """Cumulative trapezoidal integral from y0 (src/signal.rs:68-78)."""
+    out = np.empty(len(y))
+    acc = y0
+    out[0] = acc
+    for i in range(1, len(y)):
+        acc += 0.5 * (y[i] + y[i - 1]) * (t[i] - t[i - 1])
+        out[i] = acc
+    return out
+
+
+class Pulse:
+    """A uniformly sampled acceleration history (m/s^2), t = 0 at first contact."""
+
+    def __init__(self, time, accel):
+        self.time = np.asarray(time, dtype=np.float64)
+        self.accel = np.asarray(accel, dtype=np.float64)
+
+    def dt(self):
+        n = len(self.time)
+        return (self.time[-1] - self.time[0]) / (n - 1) if n > 1 else 0.0
+
+    @classmethod
+    def from_history(cls, time, local_ax, dt=PULSE_DT):
+        """Pulse::from_history: the accelerometer's local-x acceleration
+        resampled onto 0, dt, ... up to the last record."""
+        if len(time) < 4:
+            raise ValueError("accelerometer history is empty")
+        t, a = resample(time, local_ax, 0.0, dt, time[-1])
+        return cls(t, a)
+
+    def filtered(self, cfc=60.0):
+        return Pulse(self.time, cfc_filter(self.accel, self.dt(), cfc))
+
+    def resampled(self, dt):
+        t, a = resample(self.time, self.accel, self.time[0], dt, self.time[-1])
+        return Pulse(t, a)
+
+    def truncated(self, t_end):
+        n = int(np.count_nonzero(self.time <= t_end + 1e-12)) if len(self.time) else 0
+        # take_while semantics on an ascending grid
+        return Pulse(self.time[:n], self.accel[:n])
+
+    def negated(self):
+        return Pulse(self.time, -self.accel)
+
+    def velocity(self, v0):
+        return integrate(self.time, self.accel, v0)
+
+    def displacement(self, v0):
+        return integrate(self.time, self.velocity(v0), 0.0)
+
+
+class PulseComparison:
+    """Measured vs simulated pulse on the measured grid
+    (PulseComparison::new, src/vehicle.rs:1059-1078)."""
+
+    def __init__(self, meas, sim, mass, speed):
+        t_end = min(meas.time[-1], sim.time[-1])
+        m = meas.truncated(t_end)
+        s = sim.resampled(m.dt()).truncated(t_end) if abs(sim.dt() - m.dt()) > 1e-9 * m.dt() else sim.truncated(t_end)
+        n = min(len(m.time), len(s.time))
+        self.mass, self.speed = mass, speed
+        self.time = m.time[:n]
+        self.a_meas, self.a_sim = m.accel[:n], s.accel[:n]
+        self.v_meas, self.v_sim = m.velocity(speed)[:n], s.velocity(speed)[:n]
+        self.x_meas, self.x_sim = m.displacement(speed)[:n], s.displacement(speed)[:n]
+
+    def rms_accel_error(self):
+        return math.sqrt(float(np.sum((self.a_meas - self.a_sim) ** 2)) / len(self.a_meas))
+
+
+def pulse_objective(cmp):
+    """Velocity-history RMS error + 0.5 end-velocity error + 0.1 x CFC 60
+    acceleration RMS error in g (src/vehicle.rs:1120-1125)."""
+    n = len(cmp.time)
+    v_rms = math.sqrt(float(np.sum((cmp.v_meas - cmp.v_sim) ** 2)) / n)
+    v_end = abs(cmp.v_sim[-1] - cmp.v_meas[-1])
+    return v_rms + 0.5 * v_end + 0.1 * cmp.rms_accel_error() / G
+
+
+class Rng(S.XorShift64Star):
+    """The calibrations' xorshift64* (src/headon.rs:112-131), so they are
+    repeatable; below(n) draws an index in [0, n)."""
+
+    def __init__(self, seed=0x9E3779B97F4A7C15):
+        super().__init__(seed)
+
+    def below(self, n):
+        return int(self.uniform() * n) % n
+
+
+def rail_box_from_unit(size, u):
+    """src/headon.rs:88-97: [width / vehicle width, z-centre / height,
+    z-extent / height, force fraction] in the unit cube -> (width, (z0, z1),
+    force fraction): 25-95 % of the width, centred at 15-50 % of the height,
+    15-60 % of the height tall, 50-95 % of the force."""
+    w, hgt = size[1], size[2]
+    width = (0.25 + 0.7 * u[0]) * w
+    zc = (0.15 + 0.35 * u[1]) * hgt
+    dz = (0.15 + 0.45 * u[2]) * hgt
+    return (width, (max(zc - 0.5 * dz, 0.0), min(zc + 0.5 * dz, hgt)), 0.5 + 0.45 * u[3])
+
+
+def unit_from_rail_box(size, rb):
+    """src/headon.rs:99-104, the inverse, clamped to the unit cube."""
+    w, hgt = size[1], size[2]
+    width, (z0, z1), f = rb
+    zc = 0.5 * (z0 + z1) / hgt
+    dz = (z1 - z0) / hgt
+    clamp = lambda x: min(max(x, 0.0), 1.0)
+    return [clamp((width / w - 0.25) / 0.7), clamp((zc - 0.15) / 0.35), clamp((dz - 0.15) / 0.45), clamp((f - 0.5) / 0.45)]
+
+
+def _rail_box_of(spec):
+    if not spec.has_rail_box:
+        return None
+    return (spec.rail_box_width, (spec.rail_box_z[0], spec.rail_box_z[1]), spec.rail_box_force_fraction)
+
+
+def _with_rail_box(spec, rb):
+    v = type(spec).from_buffer_copy(spec)
+    v.has_rail_box = 1
+    v.rail_box_width = rb[0]
+    v.rail_box_z[0], v.rail_box_z[1] = rb[1]
+    v.rail_box_force_fraction = rb[2]
+    return v
+
+
+class HeadOn:
+    """HeadOn (src/headon.rs:17-86): A heads +x at speed_a, B heads -x at
+    speed_b (the struct's own speeds; B's pulse is negated so each vehicle's
+    forward direction is positive)."""
+
+    def __init__(self, speed_a, speed_b, offset=0.0, clearance=0.15, element_size=S.TUNED_ELEMENT_SIZE, end_time=PULSE_END,
+                 max_records=20000):
+        self.max_records = max_records  # history records kept per crash (every step up to end_time)
+        self.speed_a, self.speed_b = speed_a, speed_b
+        self.offset, self.clearance = offset, clearance
+        self.element_size, self.end_time = element_size, end_time
+
+    def build(self, a, b):
+        return S.Model.build(S.scenario(a, b, self.speed_a, self.speed_b, offset=self.offset, clearance=self.clearance,
+                                        element_size=self.element_size, end_time=self.end_time))
+
+    def run_batch(self, pairs, device=0):
+        """Run every (a, b) pair as one slot of one batched context,
+        recording both rear-seat accelerometers every step on the device;
+        returns per pair (pulse A, pulse B), CFC 60, forward positive."""
+        models = [self.build(a, b) for a, b in pairs]
+        ctx = Context([m.desc for m in models], device=device)
+        for k, m in enumerate(models):
+            ctx.history_config(1, self.max_records, [m.accelerometer(0), m.accelerometer(1)], slot=k)
+        ctx.batch_run()
+        out = []
+        for k in range(len(models)):
+            h = ctx.history(slot=k)
+            if h["records"] > self.max_records:
+                raise RuntimeError(f"slot {k}: {h['records']} history records, more than max_records {self.max_records}")
+            pa = Pulse.from_history(h["time"], h["nodes"][:, 0, 18]).filtered(60.0)
+            pb = Pulse.from_history(h["time"], h["nodes"][:, 1, 18]).negated().filtered(60.0)
+            out.append((pa, pb))
+        ctx.close()
+        return out
+
+
+def differential_evolution(seed, dims, population, generations, evaluate_all, rng=None, log=None):
+    """The synchronous rand/1/bin differential evolution of
+    calibrate_rail_boxes (src/headon.rs:196-243) in the unit cube:
+    population max(population, 4) seeded with `seed` and uniform draws of the
+    xorshift64* generator (seed 0x9E3779B97F4A7C15), F 0.7, CR 0.9, trial
+    coordinates reflected into [0, 1], a trial replacing its parent when its
+    score is not worse. evaluate_all(list of members) -> list of tuples whose
+    first item is the score; a generation's members are evaluated together.
+    Returns (population, scores, index of the best, per generation (best,
+    mean) score)."""
+    rng = rng or Rng(0x9E3779B97F4A7C15)
+    npop = max(population, 4)
+    pop = [list(seed)]
+    while len(pop) < npop:
+        pop.append([rng.uniform() for _ in range(dims)])
+    scored = evaluate_all(pop)
+    best_index = lambda sc: min(range(len(sc)), key=lambda i: sc[i][0])
+    best = best_index(scored)
+    history = [(scored[best][0], sum(x[0] for x in scored) / npop)]
+    if log:
+        log(f"initial population of {npop}: best J {scored[best][0]:.3f}")
+    f_weight, cr = 0.7, 0.9
+    for gen in range(generations):
+        trials = []
+        for i in range(npop):
+            while True:
+                r = [rng.below(npop), rng.below(npop), rng.below(npop)]
+                if r[0] != i and r[1] != i and r[2] != i and r[0] != r[1] and r[0] != r[2] and r[1] != r[2]:
+                    break
+            r1, r2, r3 = r
+            j_rand = rng.below(dims)
+            trial = []
+            for j in range(dims):
+                if j == j_rand or rng.uniform() < cr:
+                    v = pop[r1][j] + f_weight * (pop[r2][j] - pop[r3][j])
+                    v = -v if v < 0.0 else (2.0 - v if v > 1.0 else v)  # reflect into the unit cube
+                    trial.append(min(max(v, 0.0), 1.0))
+                else:
+                    trial.append(pop[i][j])
+            trials.append(trial)
+        results = evaluate_all(trials)
+        for i, (trial, sc) in enumerate(zip(trials, results)):
+            if sc[0] <= scored[i][0]:
+                pop[i] = trial
+                scored[i] = sc
+        best = best_index(scored)
+        history.append((scored[best][0], sum(x[0] for x in scored) / npop))
+        if log:
+            log(f"generation {gen}: best J {scored[best][0]:.3f}, mean {history[-1][1]:.3f}")
+    return pop, scored, best, history
+
+
+class RailBoxFit:
+    def __init__(self, a, b, objective, cmp_a, cmp_b, evaluations, history):
+        self.a, self.b, self.objective = a, b, objective
+        self.cmp_a, self.cmp_b = cmp_a, cmp_b
+        self.evaluations = evaluations
+        self.history = history  # per generation: (best J, mean J)
+
+
+def calibrate_rail_boxes(a, b, setup, measured_a, measured_b, population, generations, device=0, log=None):
+    """calibrate_rail_boxes (src/headon.rs:147-250): fit the rail boxes of
+    both vehicles (width, height band, force fraction each: 8 parameters in
+    the unit cube, seeded with the current boxes) so the two rear-seat
+    pulses of `setup` match the measured ones, by synchronous rand/1/bin
+    differential evolution (F 0.7, CR 0.9, reflection into the cube). Each
+    generation's trials run together as one batched GPU context."""
+    meas_a = measured_a.filtered(60.0).resampled(PULSE_DT).truncated(setup.end_time)
+    meas_b = measured_b.filtered(60.0).resampled(PULSE_DT).truncated(setup.end_time)
+
+    def base(v):
+        if _rail_box_of(v) is None:
+            return _with_rail_box(v, (0.5 * v.size[1], (0.2 * v.size[2], 0.6 * v.size[2]), 0.7))
+        return v
+
+    a0, b0 = base(a), base(b)
+    size_a, size_b = tuple(a0.size), tuple(b0.size)
+    dims = 8
+
+    def with_(u):
+        return _with_rail_box(a0, rail_box_from_unit(size_a, u[:4])), _with_rail_box(b0, rail_box_from_unit(size_b, u[4:]))
+
+    evaluations = [0]
+
+    def evaluate_all(us):
+        pulses = setup.run_batch([with_(u) for u in us], device=device)
+        res = []
+        for pa, pb in pulses:
+            ca = PulseComparison(meas_a, pa, a.mass, setup.speed_a)
+            cb = PulseComparison(meas_b, pb, b.mass, setup.speed_b)
+            res.append((pulse_objective(ca) + pulse_objective(cb), ca, cb))
+        evaluations[0] += len(us)
+        return res
+
+    seed = unit_from_rail_box(size_a, _rail_box_of(a0)) + unit_from_rail_box(size_b, _rail_box_of(b0))
+    pop, scored, best, history = differential_evolution(seed, dims, population, generations, evaluate_all, log=log)
+    va, vb = with_(pop[best])
+    objective, ca, cb = scored[best]
+    return RailBoxFit(va, vb, objective, ca, cb, evaluations[0], history)

@@ -31,6 +31,7 @@ struct VehicleDef {
     std::vector<uint32_t> nodes;
     uint32_t accel = 0;
     std::vector<uint32_t> front;
+    uint32_t frame[3] = {0, 0, 0};  // body-fixed frame of the accelerometer: origin, x axis, plane
 };
 
 }  // namespace
@@ -527,11 +528,76 @@ uint32_t accelerometer_node(const crush_model* m, const std::string& part, const
     return best;
 }
 
+// Mesh::min_edge_at, src/mesh.rs:236-249: the shortest hexahedron edge at `node`.
+double min_edge_at(const crush_model* m, uint32_t node) {
+    static const int EDGES[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6}, {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+    double best = 1.0 / 0.0;
+    for (size_t e = 0; e < m->hex_part.size(); ++e) {
+        const uint32_t* h = &m->hexes[8 * e];
+        if (std::find(h, h + 8, node) == h + 8) continue;
+        for (const auto& ed : EDGES) {
+            if (h[ed[0]] != node && h[ed[1]] != node) continue;
+            const double* p = &m->positions[3 * h[ed[0]]];
+            const double* q = &m->positions[3 * h[ed[1]]];
+            const double d = std::sqrt((p[0] - q[0]) * (p[0] - q[0]) + (p[1] - q[1]) * (p[1] - q[1]) + (p[2] - q[2]) * (p[2] - q[2]));
+            best = std::min(best, d);
+        }
+    }
+    return best;
+}
+
+// Mesh::best_aligned_neighbour, src/mesh.rs:265-288: among the part's nodes
+// within `radius` of `node` (not `node`, not excluded), the one whose
+// direction has the largest cosine with `dir` (first maximum).
+bool best_aligned_neighbour(const crush_model* m, uint32_t node, const double dir[3], double radius, const std::vector<uint32_t>& cand,
+                            long long exclude, uint32_t* out, double* cos_out) {
+    const double* o = &m->positions[3 * node];
+    const double dn = std::sqrt(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
+    bool found = false;
+    double best = 0.0;
+    for (uint32_t n : cand) {
+        if (n == node || (long long)n == exclude) continue;
+        const double r[3] = {m->positions[3 * n] - o[0], m->positions[3 * n + 1] - o[1], m->positions[3 * n + 2] - o[2]};
+        const double rn = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+        if (rn > radius || rn == 0.0) continue;
+        const double c = (r[0] * dir[0] + r[1] * dir[1] + r[2] * dir[2]) / (rn * dn);
+        if (!found || c > best) {
+            found = true;
+            best = c;
+            *out = n;
+        }
+    }
+    *cos_out = best;
+    return found;
+}
+
+// Model::add_accelerometer_at, src/model.rs:185-214: the body-fixed frame
+// of accelerometer node `rec` in part `part`: x axis towards the neighbour
+// best aligned with +X (else the origin moves to the -X neighbour), plane
+// node the origin's neighbour towards +Y (else -Y), within 1.75 x the
+// shortest edge at `rec`.
+void accelerometer_frame(const crush_model* m, const std::string& part, uint32_t rec, uint32_t frame[3]) {
+    const std::vector<uint32_t> cand = part_nodes(m, part_index(m, part));
+    const double radius = 1.75 * min_edge_at(m, rec);
+    uint32_t origin = rec, x_axis = rec, n = 0;
+    double c = 0.0;
+    const double px[3] = {1.0, 0.0, 0.0}, mx[3] = {-1.0, 0.0, 0.0}, py[3] = {0.0, 1.0, 0.0}, my[3] = {0.0, -1.0, 0.0};
+    if (best_aligned_neighbour(m, rec, px, radius, cand, -1, &n, &c) && c > 0.5) x_axis = n;
+    else if (best_aligned_neighbour(m, rec, mx, radius, cand, -1, &n, &c)) origin = n;
+    uint32_t plane = origin;
+    if (best_aligned_neighbour(m, origin, py, radius, cand, x_axis, &n, &c) && c > 0.5) plane = n;
+    else if (best_aligned_neighbour(m, origin, my, radius, cand, x_axis, &n, &c)) plane = n;
+    frame[0] = origin;
+    frame[1] = x_axis;
+    frame[2] = plane;
+}
+
 void add_vehicle_output(crush_model* m, const std::string& name, const std::string& front_face) {
     VehicleDef v;
     v.nodes = m->node_sets[name];
     v.accel = accelerometer_node(m, name, front_face);
     face_set_nodes(m, front_face, &v.front);
+    accelerometer_frame(m, name, v.accel, v.frame);
     m->vehicles.push_back(v);
 }
 
@@ -665,6 +731,12 @@ int crush_scenario_build(const crush_scenario* s, crush_model** out) {
 }
 
 void crush_model_free(crush_model* m) { delete m; }
+
+int crush_model_vehicle_frame(const crush_model* m, int32_t vehicle, uint32_t frame[3]) {
+    if (!m || !frame || vehicle < 0 || vehicle >= (int32_t)m->vehicles.size()) return crush::fail(CRUSH_ERR_INVALID, "no such vehicle");
+    for (int k = 0; k < 3; ++k) frame[k] = m->vehicles[vehicle].frame[k];
+    return CRUSH_OK;
+}
 
 crush_settings* crush_model_settings(crush_model* m) { return m ? &m->settings : nullptr; }
 

@@ -244,6 +244,18 @@ class Model:
         return (np.ctypeslib.as_array(w.nodes, (w.n_nodes,)), int(w.accel_node),
                 np.ctypeslib.as_array(w.front_nodes, (w.n_front,)))
 
+    def vehicle_frame(self, v):
+        """(origin, x axis, plane) nodes of vehicle v's accelerometer frame
+        (Model::add_accelerometer_at, src/model.rs:185-214)."""
+        f = (C.c_uint32 * 3)()
+        check(lib().crush_model_vehicle_frame(self._h, v, f))
+        return tuple(int(x) for x in f)
+
+    def accelerometer(self, v):
+        """Vehicle v's rear-seat accelerometer with its body frame, as
+        history_config takes it."""
+        return ([self.vehicle(v)[1]], self.vehicle_frame(v))
+
 
 PULSE_END = 0.15  # src/vehicle.rs:1104
 PULSE_DT = 1e-4   # src/vehicle.rs:1102

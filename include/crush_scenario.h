@@ -75,6 +75,10 @@ void crush_model_free(crush_model* m);
 int crush_model_desc_get(const crush_model* m, crush_model_desc* out);
 /* Mutable settings of a built model. */
 crush_settings* crush_model_settings(crush_model* m);
+/* The body-fixed frame of vehicle `vehicle`'s accelerometer (origin, x-axis
+ * and plane nodes, Model::add_accelerometer_at, src/model.rs:185-214), for
+ * crush_history_config: the rear-seat pulse of src/vehicle.rs:792-822. */
+int crush_model_vehicle_frame(const crush_model* m, int32_t vehicle, uint32_t frame[3]);
 
 /* Generic block builder (Mesh::add_hex_block_n, src/mesh.rs:117) on an empty
  * model, for tests: adds one block as part `part`; `surfaces` is a bit mask of
