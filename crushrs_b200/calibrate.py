@@ -81,6 +81,39 @@ class Pulse:
         return integrate(self.time, self.velocity(v0), 0.0)
 
 
+class PulseMetrics:
+    """Barrier-test summary of a pulse (PulseMetrics::new,
+    src/signal.rs:212-236): maximum dynamic crush and its time, end
+    velocity, restitution, peak deceleration, and the loading phase's
+    force-crush samples F = -m a."""
+
+    def __init__(self, p, mass, v0):
+        v = p.velocity(v0)
+        x = p.displacement(v0)
+        i_max, max_crush = 0, 0.0
+        for i, xi in enumerate(x):
+            if xi > max_crush:
+                i_max, max_crush = i, xi
+        self.t_max_crush = p.time[i_max]
+        self.max_crush = max_crush
+        self.v_end = v[-1]
+        self.restitution = max(-min(v.min(), np.inf) / v0, 0.0)
+        self.peak_accel = min(0.0, float(p.accel.min()))
+        self.force_crush = [(x[i], -mass * p.accel[i]) for i in range(i_max + 1)]
+
+    def mean_force(self, x0, x1):
+        """Mean force over the crush window [x0, x1] of the loading phase
+        (src/signal.rs:275-290), None when fewer than two samples span it."""
+        pts = [q for q in self.force_crush if x0 <= q[0] <= x1]
+        if len(pts) < 2:
+            return None
+        e = 0.0
+        for (c0, f0), (c1, f1) in zip(pts, pts[1:]):
+            e += 0.5 * (f0 + f1) * (c1 - c0)
+        span = pts[-1][0] - pts[0][0]
+        return e / span if span > 0.0 else None
+
+
 class PulseComparison:
     """Measured vs simulated pulse on the measured grid
     (PulseComparison::new, src/vehicle.rs:1059-1078)."""
@@ -293,3 +326,104 @@ def calibrate_rail_boxes(a, b, setup, measured_a, measured_b, population, genera
     va, vb = with_(pop[best])
     objective, ca, cb = scored[best]
     return RailBoxFit(va, vb, objective, ca, cb, evaluations[0], history)
+
+
+def run_barrier_pulses(vehicles, speed, element_size=S.TUNED_ELEMENT_SIZE, end_time=PULSE_END, max_records=20000, device=0):
+    """run_barrier_pulse (src/vehicle.rs:1106-1115) for every vehicle spec,
+    all as one batched context: the barrier at `speed`, the rear-seat
+    accelerometer recorded every step on the device; returns the CFC 60
+    pulses."""
+    models = [S.Model.build(S.barrier(v, speed, element_size=element_size, end_time=end_time)) for v in vehicles]
+    ctx = Context([m.desc for m in models], device=device)
+    for k, m in enumerate(models):
+        ctx.history_config(1, max_records, [m.accelerometer(0)], slot=k)
+    ctx.batch_run()
+    out = []
+    for k in range(len(models)):
+        h = ctx.history(slot=k)
+        if h["records"] > max_records:
+            raise RuntimeError(f"slot {k}: {h['records']} history records, more than max_records {max_records}")
+        out.append(Pulse.from_history(h["time"], h["nodes"][:, 0, 18]).filtered(60.0))
+    ctx.close()
+    return out
+
+
+N_KNOTS = 7  # MAX_KNOTS - 1: one knot is the densification
+
+
+def calibrate_pulse(v, measured, speed, element_size=S.TUNED_ELEMENT_SIZE, rounds=8, device=0, log=None):
+    """calibrate_pulse (src/vehicle.rs:1144-1256): fit a TableVehicle's
+    force-crush table (7 knots over the measured dynamic crush, initialised
+    from the measured force-crush curve when the vehicle's table has another
+    length), the crush zone's modulus and the body's modulus so its
+    rigid-barrier rear-seat pulse matches `measured`: a pattern search on the
+    logs of the 9 parameters, each round's up-and-down probes (the table kept
+    non-decreasing from its second knot) run as ONE batched context, the best
+    probe taken when it improves, the step halved when none does, stopping
+    below 0.04. Returns (vehicle, comparison, per-round best objective)."""
+    meas = measured.filtered(60.0).resampled(PULSE_DT).truncated(PULSE_END)
+    mm = PulseMetrics(meas, v.mass, speed)
+    x_max = mm.max_crush
+    spacing = x_max * 0.95 / (N_KNOTS - 1)
+    knots = [i * spacing for i in range(N_KNOTS)]
+    w = 0.5 * spacing
+    tuned = v.copy()
+    if len(tuned.table) != N_KNOTS:
+        targets = []
+        for x in knots:
+            f = mm.mean_force(max(x - w, 0.0), min(x + w, x_max))
+            targets.append(max(f if f is not None else 0.0, 1e3))
+        for i in range(2, len(targets)):
+            targets[i] = max(targets[i], targets[i - 1])
+        tuned.table = list(zip(knots, targets))
+
+    def evaluate_all(cands):
+        pulses = run_barrier_pulses([c.spec() for c in cands], speed, element_size, device=device)
+        return [PulseComparison(meas, p, v.mass, speed) for p in pulses]
+
+    def candidate(base, param, factor):
+        cand = base.copy()
+        if param < N_KNOTS:
+            t = [list(k) for k in cand.table]
+            t[param][1] *= factor
+            for i in range(2, len(t)):
+                t[i][1] = max(t[i][1], t[i - 1][1])
+            t = [tuple(k) for k in t]
+            if t == base.table:
+                return None
+            cand.table = t
+        elif param == N_KNOTS:
+            cand.modulus = min(max(cand.modulus * factor, 2e6), 500e6)
+        else:
+            cand.body_modulus = min(max(cand.body_modulus * factor, 2e7), 5e9)
+        return cand
+
+    best_cmp = evaluate_all([tuned])[0]
+    best_j = pulse_objective(best_cmp)
+    history = [best_j]
+    if log:
+        log(f"start: J {best_j:.3f}")
+    step = 0.3
+    for rnd in range(rounds):
+        probes = []
+        for param in range(N_KNOTS + 2):
+            for d in (1.0, -1.0):
+                c = candidate(tuned, param, math.exp(d * step))
+                if c is not None:
+                    probes.append((param, d, c))
+        cmps = evaluate_all([c for _, _, c in probes])
+        js = [pulse_objective(c) for c in cmps]
+        i = min(range(len(js)), key=lambda k: js[k])
+        if js[i] < best_j:
+            best_j, tuned, best_cmp = js[i], probes[i][2], cmps[i]
+            if log:
+                log(f"round {rnd} p{probes[i][0]}{'+' if probes[i][1] > 0 else '-'}: J {best_j:.3f}")
+        else:
+            step *= 0.5
+            if log:
+                log(f"round {rnd}: no improvement, step {step:.3f}")
+            if step < 0.04:
+                history.append(best_j)
+                break
+        history.append(best_j)
+    return tuned, best_cmp, history

@@ -102,37 +102,64 @@ def force_table_material(modulus, density, table, honeycomb_length, area, transv
     return honeycomb(modulus, density, curve=curve, densification=(LOCK_COMPACTION, LOCK_SLOPE_FACTOR * modulus), transverse=transverse)
 
 
-def _pulse_vehicle(mass, size, crush_zone, crush_zone_mass, bumper, rail_box, modulus, body_modulus, knots, force_kn,
-                   crush_element_size=0.1):
-    area = size[1] * size[2]
-    l_c = crush_zone - bumper[0]
-    density = (crush_zone_mass - bumper[1]) / (l_c * area)  # Vehicle::crush_density
-    mat = force_table_material(modulus, density, [(x, f * 1e3) for x, f in zip(knots, force_kn)], l_c, area)
-    return vehicle(mass, size, mat, contact_modulus=modulus, rail_box=rail_box, crush_zone_length=crush_zone,
-                   body_modulus=body_modulus, crush_zone_mass=crush_zone_mass, bumper=bumper,
-                   crush_element_size=crush_element_size)
+class TableVehicle:
+    """A two-part vehicle whose crush zone follows a tabulated force-crush
+    curve (the reference's Vehicle with `force_table`, src/vehicle.rs:137-147,
+    478-488): the parameters a pulse calibration moves (the table, the crush
+    zone's and the body's moduli) and the rest of the vehicle. spec() builds
+    the crush_vehicle_spec."""
+
+    def __init__(self, mass, size, crush_zone, crush_zone_mass, bumper, rail_box, modulus, body_modulus, table,
+                 crush_element_size=0.1, transverse=TRANSVERSE_FACTOR):
+        self.mass, self.size = mass, tuple(size)
+        self.crush_zone, self.crush_zone_mass = crush_zone, crush_zone_mass
+        self.bumper, self.rail_box = tuple(bumper), rail_box
+        self.modulus, self.body_modulus = modulus, body_modulus
+        self.table = [tuple(k) for k in table]  # (crush m, force N)
+        self.crush_element_size, self.transverse = crush_element_size, transverse
+
+    def copy(self):
+        return TableVehicle(self.mass, self.size, self.crush_zone, self.crush_zone_mass, self.bumper, self.rail_box, self.modulus,
+                            self.body_modulus, list(self.table), self.crush_element_size, self.transverse)
+
+    def spec(self):
+        area = self.size[1] * self.size[2]
+        l_c = self.crush_zone - self.bumper[0]
+        density = (self.crush_zone_mass - self.bumper[1]) / (l_c * area)  # Vehicle::crush_density
+        mat = force_table_material(self.modulus, density, self.table, l_c, area, self.transverse)
+        return vehicle(self.mass, self.size, mat, contact_modulus=self.modulus, rail_box=self.rail_box,
+                       crush_zone_length=self.crush_zone, body_modulus=self.body_modulus, crush_zone_mass=self.crush_zone_mass,
+                       bumper=self.bumper, crush_element_size=self.crush_element_size)
 
 
-def neon_1996_pulse():
+def _pulse_vehicle(mass, size, crush_zone, crush_zone_mass, bumper, rail_box, modulus, body_modulus, knots, force_kn, table=False):
+    tv = TableVehicle(mass, size, crush_zone, crush_zone_mass, bumper, rail_box, modulus, body_modulus,
+                      [(x, f * 1e3) for x, f in zip(knots, force_kn)])
+    return tv if table else tv.spec()
+
+
+def neon_1996_pulse(table=False):
     """Vehicle::dodge_neon_1996_pulse (src/vehicle.rs:541-566): the Neon
     fitted to a rear-seat barrier pulse, a 1.5 m crush zone of 0.1 m
     elements and 190 kg with a 0.1 m bumper, ahead of an elastic body, and a
-    rail box carrying 80 % of the force."""
+    rail box carrying 80 % of the force (table=True: as a TableVehicle)."""
     return _pulse_vehicle(1354.0, (4.36, 1.71, 1.35), 1.5, 190.0, (0.1, 25.0, 3.0e8), (0.45, (0.06, 0.41), 0.8), 4e6, 2.7e8,
-                          [0.0, 0.1165, 0.2330, 0.3496, 0.4661, 0.5826, 0.6991], [13.0, 135.0, 135.0, 146.0, 361.0, 364.0, 364.0])
+                          [0.0, 0.1165, 0.2330, 0.3496, 0.4661, 0.5826, 0.6991], [13.0, 135.0, 135.0, 146.0, 361.0, 364.0, 364.0],
+                          table)
 
 
-def ford_expedition_1999(mass=2460.0, size=(5.2, 2.0, 1.9)):
+def ford_expedition_1999(mass=2460.0, size=(5.2, 2.0, 1.9), table=False):
     """Vehicle::ford_expedition_1999 (src/vehicle.rs:568-593): a 1.7 m crush
     zone with 320 kg and a bumper, the rail box carrying 75 % of the force."""
     return _pulse_vehicle(mass, size, 1.7, 320.0, (0.1, 35.0, 3.0e8), (1.25, (0.15, 0.72), 0.75), 7.3e6, 3.93e8,
-                          [0.0, 0.1064, 0.2128, 0.3192, 0.4256, 0.5320, 0.6384], [29.0, 183.0, 259.0, 417.0, 457.0, 457.0, 457.0])
+                          [0.0, 0.1064, 0.2128, 0.3192, 0.4256, 0.5320, 0.6384], [29.0, 183.0, 259.0, 417.0, 457.0, 457.0, 457.0],
+                          table)
 
 
-def lincoln_navigator_1999():
+def lincoln_navigator_1999(table=False):
     """Vehicle::lincoln_navigator_1999 (src/vehicle.rs:595-603): the
     Expedition structure with 2873 kg and 5.175 x 2.049 x 1.9 m."""
-    return ford_expedition_1999(2873.0, (5.175, 2.049, 1.9))
+    return ford_expedition_1999(2873.0, (5.175, 2.049, 1.9), table)
 
 
 def _preset(mass, size, yield_force, stiffness, modulus):

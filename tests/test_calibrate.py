@@ -85,3 +85,30 @@ def test_differential_evolution_descends():
     assert all(0.0 <= c <= 1.0 for u in pop for c in u)
     again = K.differential_evolution([0.5] * 8, 8, 10, 25, evaluate_all)
     assert again[0] == pop  # repeatable: the same generator and seed
+
+
+def test_pulse_metrics_of_a_half_sine():
+    # 10 m/s into a wall, a 100 ms half-sine deceleration of 200 m/s^2 peak:
+    # v = 10 - (20/pi)(1 - cos(pi t / 0.1)), rebounding at 2.73 m/s
+    t = np.arange(0.0, 0.1 + 1e-12, 1e-4)
+    a = -200.0 * np.sin(np.pi * t / 0.1)
+    m = K.PulseMetrics(K.Pulse(t, a), 1000.0, 10.0)
+    v_end = 10.0 - 40.0 / np.pi
+    assert abs(m.v_end - v_end) < 1e-4
+    assert abs(m.restitution + v_end / 10.0) < 1e-5
+    assert abs(m.peak_accel + 200.0) < 1e-3
+    t_stop = 0.1 / np.pi * np.arccos(1.0 - np.pi / 2.0)
+    crush = 10.0 * t_stop - (20.0 / np.pi) * (t_stop - 0.1 / np.pi * np.sin(np.pi * t_stop / 0.1))
+    assert abs(m.t_max_crush - t_stop) <= 1e-4 and abs(m.max_crush - crush) < 1e-5
+    # mean force over the loading phase = the initial kinetic energy / max crush
+    e = 0.5 * 1000.0 * 10.0 ** 2
+    assert abs(m.mean_force(0.0, m.max_crush) - e / m.max_crush) < 2e-3 * e / m.max_crush
+    assert m.mean_force(5.0, 6.0) is None
+
+
+def test_table_vehicle_is_the_preset():
+    assert bytes(S.neon_1996_pulse()) == bytes(S.neon_1996_pulse(table=True).spec())
+    tv = S.neon_1996_pulse(table=True)
+    mat = tv.spec().material
+    assert mat.n_curve == 7 and mat.has_densification  # 7 table knots, the lock-up knot added by the material
+    assert abs(mat.curve[1][1] - 135e3 / (1.71 * 1.35)) < 1e-9 * mat.curve[1][1]

@@ -60,3 +60,24 @@ def test_rail_box_calibration_batches():
     j = K.pulse_objective(K.PulseComparison(meas_a, qa, a.mass, setup.speed_a)) + \
         K.pulse_objective(K.PulseComparison(meas_b, qb, b.mass, setup.speed_b))
     assert j == fit.objective
+
+
+def test_pulse_calibration_batches_each_round():
+    """calibrate_pulse (src/vehicle.rs:1144-1256) against the preset Neon's
+    own barrier pulse, starting from a softer, weaker vehicle: each round's
+    18 probes run as one batched context, the best objective never rises and
+    improves on the start, and the fitted vehicle run alone reproduces the
+    recorded objective exactly."""
+    speed = 35 * S.MPH
+    target = S.neon_1996_pulse(table=True)
+    (measured,) = K.run_barrier_pulses([target.spec()], speed)
+    start = target.copy()
+    start.modulus *= 1.3
+    start.table = [(x, f * 0.8) for x, f in start.table]
+    tuned, cmp, history = K.calibrate_pulse(start, measured, speed, rounds=2)
+    assert len(history) == 3
+    assert all(b <= a for a, b in zip(history, history[1:]))
+    assert history[-1] < history[0]
+    (again,) = K.run_barrier_pulses([tuned.spec()], speed)
+    meas = measured.filtered(60.0).resampled(K.PULSE_DT).truncated(K.PULSE_END)
+    assert K.pulse_objective(K.PulseComparison(meas, again, target.mass, speed)) == history[-1]
