@@ -427,3 +427,188 @@ def calibrate_pulse(v, measured, speed, element_size=S.TUNED_ELEMENT_SIZE, round
                 break
         history.append(best_j)
     return tuned, best_cmp, history
+
+
+# ---------------- rigid-barrier calibration (src/vehicle.rs:985-1041) ----------------
+
+def kw_window(yield_force, stiffness, window):
+    """CrushCurve::kw_window (src/vehicle.rs:61-64): energy-equivalent
+    stiffness of the bilinear curve F = F_y + k C over a crush window."""
+    w0, w1 = window
+    return stiffness + 2.0 * (w1 - w0) / (w1 * w1 - w0 * w0) * yield_force
+
+
+def crush_for_energy(yield_force, stiffness, energy):
+    """CrushCurve::crush_for_energy (src/vehicle.rs:67-72)."""
+    a, b = 0.5 * stiffness, yield_force
+    return (-b + math.sqrt(b * b + 4.0 * a * energy)) / (2.0 * a)
+
+
+class CurveVehicle:
+    """A homogeneous honeycomb block with the bilinear frontal curve
+    F = F_y + k C (Vehicle::crush_material with the whole block as crush
+    zone, src/vehicle.rs:478-490): what the barrier calibration moves."""
+
+    def __init__(self, mass, size, yield_force, stiffness, modulus, transverse=S.TRANSVERSE_FACTOR):
+        self.mass, self.size = mass, tuple(size)
+        self.yield_force, self.stiffness, self.modulus = yield_force, stiffness, modulus
+        self.transverse = transverse
+
+    def copy(self):
+        return CurveVehicle(self.mass, self.size, self.yield_force, self.stiffness, self.modulus, self.transverse)
+
+    def spec(self):
+        area = self.size[1] * self.size[2]
+        density = self.mass / (self.size[0] * self.size[1] * self.size[2])
+        mat = S.honeycomb(self.modulus, density, self.yield_force / area, self.stiffness * self.size[0] / area,
+                          transverse=self.transverse)
+        return S.vehicle(self.mass, self.size, mat, contact_modulus=self.modulus)
+
+
+class BarrierTargets:
+    """BarrierTargets (src/vehicle.rs:985-1004): KW over the window, the
+    crush that absorbs the impact energy on the curve, restitution."""
+
+    def __init__(self, kw400, max_crush, restitution, speed, window=(0.025, 0.4)):
+        self.kw400, self.max_crush, self.restitution, self.speed, self.window = kw400, max_crush, restitution, speed, window
+
+    @classmethod
+    def from_curve(cls, v, speed, window, restitution):
+        crush = crush_for_energy(v.yield_force, v.stiffness, 0.5 * v.mass * speed * speed)
+        return cls(kw_window(v.yield_force, v.stiffness, window), crush, restitution, speed, window)
+
+    @classmethod
+    def from_vehicle(cls, v, restitution):
+        return cls.from_curve(v, 35.0 * S.MPH, (0.025, 0.4), restitution)
+
+
+class BarrierMetrics:
+    """barrier_metrics_window (src/vehicle.rs:887-948) from a series of
+    (t, mass, mean velocity, mean displacement) along the impact axis of the
+    vehicle's parts: force -m dv/dt (central differences, smoothed 1-2-1),
+    contact at 2 % of the peak, crush from there, KW over the window from
+    the loading curve's energy, mean force, restitution and delta-v."""
+
+    def __init__(self, series, window=(0.025, 0.4)):
+        n = len(series)
+        if n <= 3:
+            raise ValueError("no history")
+        v0 = series[0][2]
+        sign = math.copysign(1.0, v0)
+        force = [0.0] * n
+        for i in range(1, n - 1):
+            t0, m, v_prev, _ = series[i - 1]
+            t2, _, v_next, _ = series[i + 1]
+            force[i] = -sign * m * (v_next - v_prev) / (t2 - t0)
+        force = [force[i] if i == 0 or i == n - 1 else (force[i - 1] + 2.0 * force[i] + force[i + 1]) / 4.0 for i in range(n)]
+        peak = max([0.0] + force)
+        contact = next((i for i, f in enumerate(force) if f > 0.02 * peak), 0)
+        x_contact = series[contact][3]
+        crush = [sign * (s[3] - x_contact) for s in series]
+        i_max = max(range(n), key=lambda i: (crush[i], i))  # the last maximum
+        self.max_crush = crush[i_max]
+        self.curve = [(crush[i], force[i]) for i in range(contact, i_max + 1)]
+
+        def energy_at(d):
+            e = 0.0
+            for (c0, f0), (c1, f1) in zip(self.curve, self.curve[1:]):
+                if c1 <= c0:
+                    continue
+                if c1 <= d:
+                    e += 0.5 * (f0 + f1) * (c1 - c0)
+                elif c0 < d:
+                    f_d = f0 + (f1 - f0) * (d - c0) / (c1 - c0)
+                    e += 0.5 * (f0 + f_d) * (d - c0)
+                    break
+                else:
+                    break
+            return e
+
+        w0, w1 = window
+        self.kw400 = 2.0 * (energy_at(w1) - energy_at(w0)) / (w1 * w1 - w0 * w0)
+        self.mean_force = energy_at(self.max_crush) / self.max_crush if self.max_crush > 0.0 else 0.0
+        self.peak_force = peak
+        v_end = series[-1][2]
+        self.restitution = -v_end / v0
+        self.delta_v = v_end - v0
+
+
+def part_series(time, parts, vehicle_parts, axis=0):
+    """(t, m, mean v, mean u) of the vehicle's parts from device part-state
+    records (values mass, v 3, u 3, ...; the parts of a two-part vehicle
+    combined, src/vehicle.rs:892-907)."""
+    out = []
+    for r, t in enumerate(time):
+        m = mv = mu = 0.0
+        for q in vehicle_parts:
+            s = parts[r, q]
+            m += s[0]
+            mv += s[0] * s[1 + axis]
+            mu += s[0] * s[4 + axis]
+        out.append((t, m, mv / m, mu / m))
+    return out
+
+
+def vehicle_parts(model, vehicle=0):
+    """Parts whose elements all lie on the vehicle's nodes."""
+    nodes, _, _ = model.vehicle(vehicle)
+    inside = np.zeros(model.n_nodes, bool)
+    inside[nodes] = True
+    part = model.hex_part()
+    mine = inside[model.hexes()].all(axis=1)
+    return sorted(int(p) for p in np.unique(part[mine]) if np.all(mine[part == p]))
+
+
+def run_barrier_metrics(vehicles, targets, element_size, end_time=0.14, history_steps=2, max_records=20000, device=0):
+    """The barrier run of every vehicle at its target speed as one batched
+    context, part states recorded every `history_steps` steps on the
+    device (barrier_model's history_steps 2); returns BarrierMetrics each."""
+    models = [S.Model.build(S.barrier(v.spec(), t.speed, element_size=element_size, end_time=end_time)) for v, t in zip(vehicles, targets)]
+    ctx = Context([m.desc for m in models], device=device)
+    for k in range(len(models)):
+        ctx.history_config(history_steps, max_records, [], slot=k)
+    ctx.batch_run()
+    out = []
+    for k, (m, t) in enumerate(zip(models, targets)):
+        h = ctx.history(slot=k)
+        if h["records"] > max_records:
+            raise RuntimeError(f"slot {k}: {h['records']} history records, more than max_records {max_records}")
+        out.append(BarrierMetrics(part_series(h["time"], h["parts"], vehicle_parts(m)), t.window))
+    ctx.close()
+    return out
+
+
+def calibrate(vehicles, targets, element_size=S.TUNED_ELEMENT_SIZE, iterations=8, device=0, log=None):
+    """calibrate (src/vehicle.rs:1013-1041) for several vehicles at once:
+    each iteration runs every vehicle still unconverged as one batched
+    context, then moves its curve by the damped log-space secant on the KW,
+    crush and restitution ratios (yield force and stiffness; the modulus once
+    KW and crush are within 15 %), until all three are within 2 %, 2 % and
+    10 %. Returns [(vehicle, metrics)]."""
+    tuned = [v.copy() for v in vehicles]
+    last = [None] * len(tuned)
+    active = list(range(len(tuned)))
+    for it in range(iterations):
+        if not active:
+            break
+        ms = run_barrier_metrics([tuned[i] for i in active], [targets[i] for i in active], element_size, device=device)
+        still = []
+        for i, m in zip(active, ms):
+            tg, v = targets[i], tuned[i]
+            if log:
+                log(f"vehicle {i} it {it}: KW {m.kw400 / 1e3:.0f}/{tg.kw400 / 1e3:.0f} N/mm, crush {m.max_crush * 1e3:.0f}/"
+                    f"{tg.max_crush * 1e3:.0f} mm, e {m.restitution:.3f}/{tg.restitution:.3f}")
+            r_c = tg.max_crush / m.max_crush
+            r_k = tg.kw400 / m.kw400 if m.max_crush >= tg.window[1] else 1.0 / max(r_c, 1.0)
+            r_e = tg.restitution / max(m.restitution, 1e-3)
+            last[i] = m
+            if abs(r_k - 1.0) < 0.02 and abs(r_c - 1.0) < 0.02 and abs(r_e - 1.0) < 0.1:
+                continue
+            damp = 0.7
+            v.stiffness *= r_k ** damp
+            v.yield_force *= (1.0 / r_c) ** damp * r_k ** (0.3 * damp)
+            if abs(r_k - 1.0) < 0.15 and abs(r_c - 1.0) < 0.15:
+                v.modulus *= min(max((1.0 / r_e) ** (2.0 * damp), 0.5), 2.0)
+            still.append(i)
+        active = still
+    return list(zip(tuned, last))

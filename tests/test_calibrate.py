@@ -112,3 +112,32 @@ def test_table_vehicle_is_the_preset():
     mat = tv.spec().material
     assert mat.n_curve == 7 and mat.has_densification  # 7 table knots, the lock-up knot added by the material
     assert abs(mat.curve[1][1] - 135e3 / (1.71 * 1.35)) < 1e-9 * mat.curve[1][1]
+
+
+TUNED = {  # src/vehicle.rs:614-644: tuned curves and what the reference reports for them at 35 mph, 0.3 m elements
+    "neon": (K.CurveVehicle(1354.0, (4.36, 1.71, 1.35), 16.73e3, 2.930e5, 23.1e6), 1269e3, 0.538, 0.112),
+    "silverado": (K.CurveVehicle(2622.0, (5.85, 2.03, 1.87), 51.21e3, 5.592e5, 27.8e6), 2563e3, 0.540, 0.119),
+}
+
+
+def test_oracle_barrier_metrics_known_answers():
+    """The oracle's rigid-barrier runs of the tuned Neon and Silverado
+    reproduce the reference's documented calibration results
+    (src/vehicle.rs:614-644: KW400 1269 and 2563 N/mm, maximum crush 538
+    and 540 mm, restitution 0.112 and 0.119) within 4 %, 1 % and 0.01."""
+    for name, (v, kw, crush, e) in TUNED.items():
+        m = S.Model.build(S.barrier(v.spec(), 35 * S.MPH, end_time=0.14))
+        h = O.run_history(m.desc, 2, [], cap=20000, threads=8)
+        met = K.BarrierMetrics(K.part_series(h["time"], h["parts"], K.vehicle_parts(m)))
+        assert abs(met.kw400 - kw) <= 0.04 * kw, (name, met.kw400)
+        assert abs(met.max_crush - crush) <= 0.01 * crush, (name, met.max_crush)
+        assert abs(met.restitution - e) <= 0.01, (name, met.restitution)
+
+
+def test_barrier_targets_from_the_curve():
+    v = TUNED["neon"][0]
+    t = K.BarrierTargets.from_vehicle(v, 0.12)
+    # KW400 = k + 2 (0.375) / (0.16 - 0.000625) F_y; 0.5 k C^2 + F_y C = 0.5 m v^2
+    assert abs(t.kw400 - (2.930e5 + 2 * 0.375 / (0.16 - 0.000625) * 16.73e3)) < 1e-6 * t.kw400
+    e = 0.5 * 1354.0 * (35 * S.MPH) ** 2
+    assert abs(0.5 * 2.930e5 * t.max_crush ** 2 + 16.73e3 * t.max_crush - e) < 1e-6 * e

@@ -81,3 +81,30 @@ def test_pulse_calibration_batches_each_round():
     (again,) = K.run_barrier_pulses([tuned.spec()], speed)
     meas = measured.filtered(60.0).resampled(K.PULSE_DT).truncated(K.PULSE_END)
     assert K.pulse_objective(K.PulseComparison(meas, again, target.mass, speed)) == history[-1]
+
+
+def test_barrier_metrics_and_calibration_batches():
+    """The barrier runs of the tuned Neon and Silverado as one batched
+    context: their metrics from device part histories against the oracle's
+    (KW 1 %, crush 0.5 %, restitution 0.005); then calibrate (src/vehicle.rs:1013)
+    both at once towards the NHTSA targets the reference tuned them to
+    (src/vehicle.rs:614-644): each iteration is one batch whose metrics are
+    exactly those of the same vehicles run as a batch by hand."""
+    from .test_calibrate import TUNED
+
+    vs = [TUNED["neon"][0], TUNED["silverado"][0]]
+    targets = [K.BarrierTargets(1251e3, 0.527, 0.112, 35 * S.MPH), K.BarrierTargets(2550e3, 0.513, 0.119, 35 * S.MPH)]
+    mets = K.run_barrier_metrics(vs, targets, S.TUNED_ELEMENT_SIZE)
+    for v, met in zip(vs, mets):
+        m = S.Model.build(S.barrier(v.spec(), 35 * S.MPH, end_time=0.14))
+        h = O.run_history(m.desc, 2, [], cap=20000, threads=8)
+        ref = K.BarrierMetrics(K.part_series(h["time"], h["parts"], K.vehicle_parts(m)))
+        assert abs(met.kw400 - ref.kw400) <= 0.01 * ref.kw400
+        assert abs(met.max_crush - ref.max_crush) <= 0.005 * ref.max_crush
+        assert abs(met.restitution - ref.restitution) <= 0.005
+    first = K.calibrate(vs, targets, iterations=1)  # the same batch as above, then one curve update
+    for (tuned, met), before, v in zip(first, mets, vs):
+        assert (met.kw400, met.max_crush, met.restitution) == (before.kw400, before.max_crush, before.restitution)
+        assert (tuned.yield_force, tuned.stiffness) != (v.yield_force, v.stiffness)
+    out = K.calibrate(vs, targets, iterations=2)
+    assert len(out) == 2 and all(m is not None and m.max_crush > 0.0 for _, m in out)
