@@ -289,6 +289,7 @@ struct crush_ctx {
     cudaStream_t side2 = nullptr;              // its static-grid part, then the next step's element dt pass
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join2 = nullptr, ev_forces = nullptr;
     cudaEvent_t ev_heavy = nullptr, ev_heavy_done = nullptr;  // the heavy-node gather beside the contact gather
+    cudaEvent_t ev_gathered = nullptr;                         // the contact gather done: side2 resets the event counts
     int* mass_flag = nullptr;                  // device: some crash scales its masses this step
     std::vector<void*> allocs;
     std::unordered_map<void*, size_t> alloc_bytes;  // size of every device allocation
@@ -516,6 +517,7 @@ struct crush_ctx {
         if (ev_forces) cudaEventDestroy(ev_forces);
         if (ev_heavy) cudaEventDestroy(ev_heavy);
         if (ev_heavy_done) cudaEventDestroy(ev_heavy_done);
+        if (ev_gathered) cudaEventDestroy(ev_gathered);
         if (side) cudaStreamDestroy(side);
         if (side2) cudaStreamDestroy(side2);
         if (stream) cudaStreamDestroy(stream);
@@ -894,6 +896,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
         CK(cudaEventCreateWithFlags(&c->ev_forces, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&c->ev_heavy, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&c->ev_heavy_done, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c->ev_gathered, cudaEventDisableTiming));
     }
     c->n_slots = n_desc;
     c->slots.resize(n_desc);
@@ -1520,7 +1523,7 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
     // step's forces (or at crush_run_begin for the first step).
     if (c->n_contacts > 0) {
         launch_contact_finish(c->stream, cr, nd, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0.0, c->mass, c->f_ext, 1,
-                              c->side2, c->ev_heavy, c->ev_heavy_done);
+                              c->side2, c->ev_heavy, c->ev_heavy_done, c->ev_gathered);
         n += contact_finish_launches(c->n_slaves);
     }
     mark(2);

@@ -1466,11 +1466,12 @@ __global__ void k_contact_force(ContactArrays ca, Control* ctls, int c0, int run
     }
 }
 
-// Start of a force pass, one block: the previous pass's heavy nodes (those
-// listed in gather_work) get their event counts back to zero, then the pool
-// and the heavy list are emptied. The heavy gather cannot clear its own
-// nodes' counts: the other gather, beside it on a second stream or after it
-// on the same stream, reads them to skip those nodes.
+// End of a force pass, one block, once both gathers are done: the pass's
+// heavy nodes (those listed in gather_work) get their event counts back to
+// zero, then the pool and the heavy list are emptied, so every pass starts
+// from zero counts. The heavy gather cannot clear its own nodes' counts: the
+// other gather, beside it on a second stream or after it on the same
+// stream, reads them to skip those nodes.
 constexpr int RESET_TPB = 512;
 __global__ void __launch_bounds__(RESET_TPB) k_contact_reset(ContactArrays ca) {
     const int count = *ca.gather_count;
@@ -1983,12 +1984,11 @@ void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeAr
 
 void launch_contact_finish(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
                            long long n_faces, long long n_slaves, double dt_override, const double* masses, double* f_out,
-                           int skip_fixed, cudaStream_t s_heavy, cudaEvent_t ev_a, cudaEvent_t ev_b) {
+                           int skip_fixed, cudaStream_t s_heavy, cudaEvent_t ev_a, cudaEvent_t ev_b, cudaEvent_t ev_c) {
     if (c1 <= c0) return;
     const int run_mode = dt_override > 0.0 ? 0 : 1;
     (void)f0;
     (void)n_faces;
-    k_contact_reset<<<1, RESET_TPB, 0, s>>>(ca);  // the last pass's heavy counts, the pool and the heavy list
     if (n_slaves > 0)
         k_contact_force<<<active_grid(n_slaves, FORCE_LANES, TPB, GRID_CAP), TPB, 0, s>>>(ca, ctls, c0, run_mode, dt_override, masses,
                                                                                          n_slaves, skip_fixed);
@@ -2002,11 +2002,19 @@ void launch_contact_finish(cudaStream_t s, const ContactArrays& ca, const NodeAr
     }
     k_contact_gather_heavy<<<(unsigned)(nodes < HEAVY_BLOCKS ? nodes : HEAVY_BLOCKS), HEAVY_TPB, 0, sh>>>(ca, nd, ctls, c0, c1, run_mode,
                                                                                                        f_out);
+    if (s_heavy) cudaEventRecord(ev_b, sh);
     k_contact_gather<<<active_grid(nodes, 1, GATHER_TPB, GRID_CAP * 2), GATHER_TPB, 0, s>>>(ca, nd, ctls, c0, c1, run_mode, f_out,
                                                                                           skip_fixed);
+    // The counts' reset follows both gathers: on the heavy stream it stays
+    // off the caller's path (the caller joins that stream before its next
+    // pass); the caller's stream waits only for the heavy sums.
     if (s_heavy) {
-        cudaEventRecord(ev_b, sh);
+        cudaEventRecord(ev_c, s);
+        cudaStreamWaitEvent(sh, ev_c, 0);
+        k_contact_reset<<<1, RESET_TPB, 0, sh>>>(ca);
         cudaStreamWaitEvent(s, ev_b, 0);
+    } else {
+        k_contact_reset<<<1, RESET_TPB, 0, s>>>(ca);
     }
 }
 

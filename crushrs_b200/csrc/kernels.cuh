@@ -260,7 +260,7 @@ void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeAr
 void launch_contact_finish(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
                            long long n_faces, long long n_slaves, double dt_override, const double* masses, double* f_out,
                            int skip_fixed, cudaStream_t s_heavy = nullptr, cudaEvent_t ev_a = nullptr,
-                           cudaEvent_t ev_b = nullptr);
+                           cudaEvent_t ev_b = nullptr, cudaEvent_t ev_c = nullptr);
 int contact_search_launches(const ContactArrays& ca, bool run_mode, long long n_faces, long long n_slaves, long long bk0, long long bk1,
                             int c0);
 int contact_finish_launches(long long n_slaves);
