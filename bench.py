@@ -335,6 +335,45 @@ def batched_section(n, plain_sample, oracle_sample, device, world=1):
     return out
 
 
+def two_part_section(n, device):
+    """Two-part vehicles (crush zone, rail box, bumper, elastic Hencky body):
+    the Navigator into the pulse-fitted Neon at 30.14 mph each to 150 ms,
+    alone and as a batch of n with seeded rail boxes (the calibration's
+    workload, src/headon.rs:147-250)."""
+    from crushrs_b200 import calibrate as K, scenarios as S
+    from crushrs_b200.engine import Context
+
+    setup = K.HeadOn(30.14 * S.MPH, 30.14 * S.MPH)
+    a, b = S.lincoln_navigator_1999(), S.neon_1996_pulse()
+    m = setup.build(a, b)
+    elastic = sum(1 for p in m.hex_part() if m.material(p).model == 1)
+    w = Context(m.desc, device=device)
+    w.run()
+    w.close()
+    t0 = time.perf_counter()
+    c = Context(m.desc, device=device)
+    r = c.run()
+    c.close()
+    single = time.perf_counter() - t0
+    rng = K.Rng(0x5EED)
+    pairs = []
+    for _ in range(n):
+        u = [rng.uniform() for _ in range(8)]
+        pairs.append((K.with_rail_box(a, K.rail_box_from_unit(tuple(a.size), u[:4])),
+                      K.with_rail_box(b, K.rail_box_from_unit(tuple(b.size), u[4:]))))
+    models = [setup.build(x, y) for x, y in pairs]
+    t0 = time.perf_counter()
+    ctx = Context([x.desc for x in models], device=device)
+    rs = ctx.batch_run()
+    ctx.close()
+    batch = time.perf_counter() - t0
+    eu = sum(x.n_hexes * int(q.steps) for x, q in zip(models, rs))
+    return {"elements": m.n_hexes, "elastic_elements": elastic, "steps": int(r.steps), "single_s": single,
+            "single_elem_upd_per_s": m.n_hexes * r.steps / single, "batch": n, "batch_s": batch,
+            "batch_crashes_per_s": n / batch, "batch_elem_upd_per_s": eu / batch,
+            "path": "crush_create + crush_run (single); crush_batch_create + crush_batch_run (batch), set-up included"}
+
+
 def serving_section(rate, seconds, device):
     """The crash server under an open-loop Poisson stream at `rate` req/s."""
     from crushrs_b200 import scenarios as S
@@ -420,6 +459,8 @@ def main():
                 line["batched"] = b
         if rank == 0 and world == 1 and args.serve_rates:
             line["serving"] = [serving_section(float(r), args.serve_seconds, local) for r in args.serve_rates.split(",") if r]
+        if rank == 0 and "twopart" in sections:
+            line["two_part"] = two_part_section(64, local)
         if rank == 0:
             print(json.dumps(line), flush=True)
         return

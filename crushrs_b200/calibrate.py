@@ -181,7 +181,7 @@ def _rail_box_of(spec):
     return (spec.rail_box_width, (spec.rail_box_z[0], spec.rail_box_z[1]), spec.rail_box_force_fraction)
 
 
-def _with_rail_box(spec, rb):
+def with_rail_box(spec, rb):
     v = type(spec).from_buffer_copy(spec)
     v.has_rail_box = 1
     v.rail_box_width = rb[0]
@@ -299,7 +299,7 @@ def calibrate_rail_boxes(a, b, setup, measured_a, measured_b, population, genera
 
     def base(v):
         if _rail_box_of(v) is None:
-            return _with_rail_box(v, (0.5 * v.size[1], (0.2 * v.size[2], 0.6 * v.size[2]), 0.7))
+            return with_rail_box(v, (0.5 * v.size[1], (0.2 * v.size[2], 0.6 * v.size[2]), 0.7))
         return v
 
     a0, b0 = base(a), base(b)
@@ -307,7 +307,7 @@ def calibrate_rail_boxes(a, b, setup, measured_a, measured_b, population, genera
     dims = 8
 
     def with_(u):
-        return _with_rail_box(a0, rail_box_from_unit(size_a, u[:4])), _with_rail_box(b0, rail_box_from_unit(size_b, u[4:]))
+        return with_rail_box(a0, rail_box_from_unit(size_a, u[:4])), with_rail_box(b0, rail_box_from_unit(size_b, u[4:]))
 
     evaluations = [0]
 

@@ -513,22 +513,25 @@ __device__ __forceinline__ void scalar_force_body(const ElementArrays& el, const
     }
     const long long S = el.sc_stride;
     const double* G = el.sc_geo;
-    double x[8][3], ul[24];
+    // One pass over the nodes accumulates F (x = X + u) and q = U Γ, in the
+    // order of the all-node loops; ∇N and Γ rows are read again below, so
+    // no per-node arrays stay live (the kernel's occupancy is register-bound).
+    double f[9], q[12];
+    for (int k = 0; k < 9; ++k) f[k] = 0.0;
     for (int k = 0; k < 8; ++k) {
         const long long n = el.conn_all[8 * e + k];
+        double xk[3], uk[3], gk[3], ak[4];
         for (int d = 0; d < 3; ++d) {
-            const double ud = nd.u[3 * n + d];
-            x[k][d] = nd.pos[3 * n + d] + ud;
-            ul[3 * k + d] = ud;
+            uk[d] = nd.u[3 * n + d];
+            xk[d] = nd.pos[3 * n + d] + uk[d];
+            gk[d] = G[(SC_GRAD + 3 * k + d) * S + i];
         }
-    }
-    double grad[24];
-    for (int k = 0; k < 24; ++k) grad[k] = G[(SC_GRAD + k) * S + i];
-    double f[9];
-    for (int k = 0; k < 9; ++k) f[k] = 0.0;
-    for (int k = 0; k < 8; ++k)
+        for (int a = 0; a < 4; ++a) ak[a] = G[(SC_GAMMA + 4 * k + a) * S + i];
         for (int a = 0; a < 3; ++a)
-            for (int b = 0; b < 3; ++b) f[3 * a + b] += x[k][a] * grad[3 * k + b];
+            for (int b = 0; b < 3; ++b) f[3 * a + b] += xk[a] * gk[b];
+        for (int a = 0; a < 4; ++a)
+            for (int d = 0; d < 3; ++d) q[3 * a + d] = k == 0 ? uk[d] * ak[a] : q[3 * a + d] + uk[d] * ak[a];
+    }
     if (det3d(f) <= 0.0) {
         el.eroded_all[e] = 1;
         atomicAdd(reinterpret_cast<unsigned long long*>(&ctl->eroded_step), 1ull);
@@ -547,35 +550,26 @@ __device__ __forceinline__ void scalar_force_body(const ElementArrays& el, const
             t = t + tau[3 * a + 2] * finv[3 * b + 2];
             m[3 * a + b] = t * vol;
         }
-    double o[24];
-    for (int k = 0; k < 8; ++k)
-        for (int a = 0; a < 3; ++a) {
-            double t = m[3 * a] * grad[3 * k];
-            t = t + m[3 * a + 1] * grad[3 * k + 1];
-            t = t + m[3 * a + 2] * grad[3 * k + 2];
-            o[3 * k + a] = t;
-        }
-    double gam[32];
-    for (int k = 0; k < 32; ++k) gam[k] = G[(SC_GAMMA + k) * S + i];
-    double q[12];
-    for (int a = 0; a < 4; ++a)
-        for (int d = 0; d < 3; ++d) {
-            double t = ul[d] * gam[a];
-            for (int k = 1; k < 8; ++k) t = t + ul[3 * k + d] * gam[4 * k + a];
-            q[3 * a + d] = t;
-        }
     double r[12];
     for (int row = 0; row < 12; ++row) {
         double t = G[(SC_H + h_index(0, row)) * S + i] * q[0];
         for (int c = 1; c < 12; ++c) t = t + G[(SC_H + (row <= c ? h_index(row, c) : h_index(c, row))) * S + i] * q[c];
         r[row] = t;
     }
-    for (int k = 0; k < 8; ++k)
+    // f_i = (τ F⁻ᵀ V) ∇N_i plus the hourglass force (R Γᵀ)_i
+    for (int k = 0; k < 8; ++k) {
+        double gk[3], ak[4];
+        for (int d = 0; d < 3; ++d) gk[d] = G[(SC_GRAD + 3 * k + d) * S + i];
+        for (int a = 0; a < 4; ++a) ak[a] = G[(SC_GAMMA + 4 * k + a) * S + i];
         for (int d = 0; d < 3; ++d) {
-            double t = r[d] * gam[4 * k];
-            for (int a = 1; a < 4; ++a) t = t + r[3 * a + d] * gam[4 * k + a];
-            out[3 * k + d] = o[3 * k + d] + t;
+            double o = m[3 * d] * gk[0];
+            o = o + m[3 * d + 1] * gk[1];
+            o = o + m[3 * d + 2] * gk[2];
+            double t = r[d] * ak[0];
+            for (int a = 1; a < 4; ++a) t = t + r[3 * a + d] * ak[a];
+            out[3 * k + d] = o + t;
         }
+    }
 }
 
 __global__ void __launch_bounds__(SC_TPB) k_forces_scalar(ElementArrays el, NodeArrays nd, Control* ctls, int respect_done) {
