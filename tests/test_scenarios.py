@@ -98,3 +98,27 @@ def test_two_part_headon_builds_both_headings():
         assert np.all(x[front, 0] == ext)
         assert sign * (x[accel, 0] - x[front, 0].mean()) < -1.0
     assert m.desc.n_contacts == 4
+
+
+def test_two_part_variants_and_errors():
+    """A crush zone without a bumper or rail box, a T-bone with a two-part
+    striking vehicle, and the spec checks of the two-part fields."""
+    from crushrs_b200.native import CrushError
+    import pytest
+
+    mat = S.honeycomb(5e6, 0.0, 0.3e6, 0.2e6)  # density from the crush zone's mass
+    plain_two = S.vehicle(1500.0, (4.2, 1.8, 1.4), mat, crush_zone_length=1.2, body_modulus=2e8, crush_zone_mass=300.0)
+    m = S.Model.build(S.barrier(plain_two, 15.0))
+    counts = np.bincount(m.hex_part(), minlength=m.desc.n_parts)
+    mats = [m.material(p) for p in range(m.desc.n_parts)]
+    assert mats[0].model == abi.MAT_ELASTIC and mats[1].model == abi.MAT_HONEYCOMB and m.desc.n_parts == 4  # body, crush, wall, road
+    assert counts[0] == 10 * 6 * 5 and counts[1] == 4 * 6 * 5  # 3.0 m and 1.2 m at 0.3 m
+    assert abs(mats[1].density - 300.0 / (1.2 * 1.8 * 1.4)) < 1e-9 * mats[1].density
+    assert abs(mats[0].density - 1200.0 / (3.0 * 1.8 * 1.4)) < 1e-9 * mats[0].density
+    tb = S.Model.build(S.scenario(plain_two, S.neon_1996_tuned(), 15.0, 0.0, layout=abi.LAYOUT_TBONE))
+    assert tb.desc.n_vehicles == 2 and tb.desc.n_contacts >= 2
+    for bad in (dict(body_modulus=0.0), dict(crush_zone_mass=1500.0), dict(bumper=(1.5, 10.0, 1e8))):
+        kw = dict(crush_zone_length=1.2, body_modulus=2e8, crush_zone_mass=300.0)
+        kw.update(bad)
+        with pytest.raises(CrushError):
+            S.Model.build(S.barrier(S.vehicle(1500.0, (4.2, 1.8, 1.4), mat, **kw), 15.0))
