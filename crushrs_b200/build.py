@@ -20,7 +20,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_SOURCES = ["kernels.cu", "engine.cu", "contact_static.cu", "history.cu", "frames.cu"]
 HOST_SOURCES = ["host/scenario.cpp", "host/errors.cpp", "host/server.cpp", "host/signal.cpp"]
-HEADERS = ["common.cuh", "element.cuh", "kernels.cuh", "host/errors.hpp"]
+HEADERS = ["common.cuh", "element.cuh", "kernels.cuh", "hencky.cuh", "host/errors.hpp"]
 INCLUDE = ["-I", os.path.join(ROOT, "include"), "-I", CSRC]
 
 
