@@ -315,6 +315,7 @@ struct crush_ctx {
     double *u_tmp = nullptr, *f_tmp = nullptr, *n_tmp = nullptr, *n_tmp2 = nullptr, *e_tmp = nullptr;
     uint8_t *fixed = nullptr, *eroded_all = nullptr;
     uint32_t *conn_all = nullptr, *hc_off = nullptr, *hc_slot = nullptr, *all_off = nullptr, *all_slot = nullptr;
+    const uint4* hc_ell = nullptr;  // N x 8 honeycomb slots, padded rows (NodeArrays::hc_ell)
     uint32_t *node_slot = nullptr, *elem_slot = nullptr;
     int32_t* part = nullptr;
     double* mat4 = nullptr;
@@ -453,6 +454,7 @@ struct crush_ctx {
         a.added = added;
         a.fixed = fixed;
         a.hc_off = hc_off;
+        a.hc_ell = hc_ell;
         a.hc_slot = hc_slot;
         a.all_off = all_off;
         a.all_slot = all_slot;
@@ -995,6 +997,8 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     sc_off.alloc(N + 1);
     all_slot.alloc(8 * E);
     hc_slot.alloc(8 * c->n_hc);
+    Buf<uint32_t> hc_ell;
+    hc_ell.alloc(8 * (size_t)N);
     sc_slot.alloc(8 * c->n_sc);
     parallel_for(n_desc, [&](long long k) {
         const Slot& sl = c->slots[k];
@@ -1046,6 +1050,13 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
                 else sc_slot[curc[n - n0]++] = (uint32_t)(8 * se + i);
             }
         }
+        // the same honeycomb slots as padded rows of 8 (HC_ELL_MORE: the CSR)
+        for (long long n = n0; n < n0 + nn; ++n) {
+            uint32_t* row = &hc_ell[8 * (size_t)n];
+            const uint32_t m = cnt_b[n - n0];
+            for (int j = 0; j < 8; ++j) row[j] = (uint32_t)j < m ? hc_slot[hc_off[n] + j] : HC_ELL_NONE;
+            if (m > 8) row[0] = HC_ELL_MORE;
+        }
     });
     all_off[N] = (uint32_t)(8 * E);
     hc_off[N] = (uint32_t)(8 * c->n_hc);
@@ -1077,6 +1088,11 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->upload(&c->all_slot, all_slot.data(), all_slot.size()));
     TRY(c->upload(&c->hc_off, hc_off.data(), N + 1));
     TRY(c->upload(&c->hc_slot, hc_slot.data(), hc_slot.size()));
+    {
+        uint32_t* ell = nullptr;
+        TRY(c->upload(&ell, hc_ell.data(), 8 * (size_t)N));
+        c->hc_ell = reinterpret_cast<const uint4*>(ell);
+    }
     if (c->n_sc > 0) {
         TRY(c->upload(&c->sc_index_d, sc_index.data(), E));
         TRY(c->upload(&c->sc_model_d, c->sc_model.data(), c->n_sc));

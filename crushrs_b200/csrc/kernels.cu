@@ -463,20 +463,21 @@ __device__ __forceinline__ void forces_body(const ElementArrays& el, const NodeA
 // Nodal internal force, component d: ordered f64 sum of the incident corner
 // forces (element order). Up to 8 corners (every node of a structured hex
 // mesh) the loads are all issued before the sum.
+// The node's slots come from its padded row of 8 (one round of loads
+// before the corner loads); a node with more than 8 uses the CSR.
 __device__ __forceinline__ double gather_component(const NodeArrays& nd, const float* __restrict__ corner, long long n, int d) {
-    const uint32_t b = __ldg(nd.hc_off + n), m = __ldg(nd.hc_off + n + 1) - b;
+    const uint4 r0 = __ldg(nd.hc_ell + 2 * n), r1 = __ldg(nd.hc_ell + 2 * n + 1);
     double f = 0.0;
-    if (m <= 8) {
-        uint32_t sl[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) sl[j] = (uint32_t)j < m ? __ldg(nd.hc_slot + b + j) : 0u;
+    if (r0.x != HC_ELL_MORE) {
+        const uint32_t sl[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
         float c[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) c[j] = (uint32_t)j < m ? __ldg(corner + 3ull * sl[j] + d) : 0.f;  // slot = 8 e + corner
+        for (int j = 0; j < 8; ++j) c[j] = sl[j] != HC_ELL_NONE ? __ldg(corner + 3ull * sl[j] + d) : 0.f;  // slot = 8 e + corner
 #pragma unroll
         for (int j = 0; j < 8; ++j)
-            if ((uint32_t)j < m) f += (double)c[j];
+            if (sl[j] != HC_ELL_NONE) f += (double)c[j];
     } else {
+        const uint32_t b = __ldg(nd.hc_off + n), m = __ldg(nd.hc_off + n + 1) - b;
         for (uint32_t k = 0; k < m; ++k) f += (double)__ldg(corner + 3ull * __ldg(nd.hc_slot + b + k) + d);
     }
     return f;

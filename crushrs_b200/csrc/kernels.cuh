@@ -43,6 +43,7 @@ struct ElementArrays {
     Active act_sc;               // active chunks of scalar elements
 };
 constexpr int SC_GRAD = 0, SC_VOL = 24, SC_GAMMA = 25, SC_H = 57, SC_PLANES = 135;
+constexpr uint32_t HC_ELL_NONE = 0xFFFFFFFFu, HC_ELL_MORE = 0xFFFFFFFEu;
 
 struct NodeArrays {
     long long n;
@@ -57,6 +58,8 @@ struct NodeArrays {
     double* added;           // N
     const uint8_t* fixed;    // N
     const uint32_t* hc_off;  // N+1 CSR over honeycomb (element, corner) slots, element order
+    const uint4* hc_ell;     // N x 2 uint4: the node's first 8 of those slots, HC_ELL_NONE padding,
+                             // HC_ELL_MORE first when it has more (then the CSR)
     const uint32_t* hc_slot;
     const uint32_t* all_off; // N+1 CSR over all model (element, corner) slots
     const uint32_t* all_slot;
