@@ -37,7 +37,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -82,57 +81,74 @@ def read_traffic(n_elem):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled from NVML every ~2 ms on a
+    thread started before the warm-up, so the few milliseconds of a short
+    timed region still get samples. mark_start()/mark_end() bracket the
+    timed region; summary() reports the samples inside it ("timed region")
+    and, when it holds none, the samples from warm-up to its end."""
 
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
 
-    def __init__(self, device):
+    def __init__(self, device, period_s=0.002):
         self.device = device
-        self.proc = None
-        self.lines = []
+        self.period_s = period_s
+        self.samples = []  # (host time, sm MHz, max sm MHz, reasons bitmask)
+        self.t_start = self.t_end = None
+        self._stop = threading.Event()
+        self.thread = None
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                                          "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            import pynvml
+
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+            self._max = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+            self._reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.thread = threading.Thread(target=self._run, daemon=True)
             self.thread.start()
         except Exception:
-            self.proc = None
+            self.thread = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _run(self):
+        nv, h = self._nv, self._h
+        while not self._stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                rs = self._reasons(h)
+                self.samples.append((time.perf_counter(), float(sm), float(self._max), int(rs)))
+            except Exception:
+                return
+            self._stop.wait(self.period_s)
+
+    def mark_start(self):
+        self.t_start = time.perf_counter()
+
+    def mark_end(self):
+        self.t_end = time.perf_counter()
 
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
+        self._stop.set()
+        if self.thread:
             self.thread.join(timeout=2)
+            try:
+                self._nv.nvmlShutdown()
+            except Exception:
+                pass
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
-                continue
-            for name, val in zip(names, parts[5:9]):
-                if val.lower().startswith("active"):
-                    reasons.add(name)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        inside = [x for x in self.samples if self.t_start is not None and self.t_end is not None and self.t_start <= x[0] <= self.t_end]
+        window = "timed region"
+        if not inside:
+            inside = [x for x in self.samples if self.t_end is None or x[0] <= self.t_end]
+            window = "warm-up through timed region"
+        if not inside:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "window": None, "source": "nvml"}
+        reasons = sorted(name for name, bit in self.REASONS.items() if any(x[3] & bit for x in inside))
+        return {"sm_mhz": statistics.median(x[1] for x in inside), "sm_max_mhz": inside[-1][2], "reasons": reasons,
+                "samples": len(inside), "window": window, "source": "nvml, every 2 ms"}
 
 
 def dist_setup(backend=None):
@@ -422,32 +438,48 @@ def main():
         ap.error("--warmup must be >= 3")
 
     world, rank, local = dist_setup()
+    config = {"workload": "refined head-on, 0.05 m hexahedra (36x30x138 + 36x24x150), run to separation (<= 5000 steps)",
+              "elements": None, "nodes": None, "timed_steps": None,
+              "l2": "per-step working set > L2 (126 MB), no flush",
+              "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+
+    if args.impl == "reference":
+        # The reference's step loop as the oracle restates it (f32 8-lane
+        # element kernel on all host threads, serial scatter, contact and
+        # update), on the same refined head-on built by the checker's numpy
+        # builder: this arm never loads the engine library. Exactly K steps
+        # after W warm-up steps are timed.
+        if rank != 0:
+            return
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import headon as H
+        from tests import oracle_lib as O
+
+        threads = os.cpu_count() or 1
+        model = H.refined_headon(max_steps=args.warmup + args.steps)
+        n_hc = int((model.hex_part < 2).sum())
+        config["elements"] = n_hc
+        config["nodes"] = int(model.n_nodes)
+        config["timed_steps"] = f"steps {args.warmup}..{args.warmup + args.steps}"
+        r, _, _, _, sec = O.run_window(model.desc, time_from_step=args.warmup, simd=True, threads=threads)
+        steps = int(r.steps) - args.warmup
+        value = n_hc * steps / sec[4]
+        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "elem-upd/s", "n_gpus": args.gpus, "steps": steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * sec[4] / steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32 element / f64 nodal", "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": value, "unit": "elem-upd/s", "cores": threads, "kind": "port",
+                                 "sample": f"steps {args.warmup}..{args.warmup + args.steps} of the refined head-on (whole step: contact, "
+                                           "forces, update, dt), oracle f32 8-lane AVX2 restatement, model from the numpy builder"},
+                "e2e": {"value": value, "unit": "elem-upd/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
     from crushrs_b200 import scenarios as S
 
     model = S.Model.build(S.refined_headon())
     desc = model.desc
     n_nodes = desc.n_nodes
-    config = {"workload": "refined head-on, 0.05 m hexahedra (36x30x138 + 36x24x150), run to separation (<= 5000 steps)",
-              "elements": None, "nodes": n_nodes, "timed_steps": f"steps {args.warmup}..{args.warmup + args.steps}",
-              "l2": "per-step working set > L2 (126 MB), no flush",
-              "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
-
-    if args.impl == "reference":
-        if rank != 0:
-            return
-        threads = os.cpu_count() or 1
-        n_hc = sum(1 for p in model.hex_part() if model.material(p).model == 0)
-        config["elements"] = n_hc
-        steps, loop, sec = cpu_reference(desc, args.cpu_steps, threads)
-        value = n_hc * steps / loop
-        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "elem-upd/s", "n_gpus": args.gpus, "steps": int(steps),
-                "warmup": args.warmup, "ms_per_step": 1e3 * loop / steps, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32 element / f64 nodal", "data": "synthetic", "config": config,
-                "cpu_baseline": {"value": value, "unit": "elem-upd/s", "cores": threads, "kind": "port",
-                                 "sample": f"{steps} steps of the refined head-on (whole step: contact, forces, update, dt), oracle f32 8-lane AVX2 restatement"},
-                "e2e": {"value": value, "unit": "elem-upd/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
-        return
+    config["nodes"] = n_nodes
 
     from crushrs_b200.engine import Context
 
@@ -468,23 +500,28 @@ def main():
     ctx = Context(desc, device=local)
     n_hc = ctx.n_active
     config["elements"] = n_hc
+    clocks = ClockSampler(local).__enter__()
     ctx.run_begin()
     # Inside the timed region the step graph records CUDA events around the
     # element-force kernel only (two per step); the per-phase breakdown comes
     # from a short profiled region after it.
     ctx.set_profiling(1)
     ctx.run_steps_timed(args.warmup, phases=True)
-    # Extra untimed steps so the timed region starts on a step-graph boundary
-    # (the engine replays one captured graph per 20 steps).
+    # Untimed steps up to a step-graph boundary (the engine replays one
+    # captured graph per 20 steps), then one whole graph period, so the
+    # graph's capture and instantiation fall before the timed region.
     align = (-args.warmup) % 20
-    if align:
-        ctx.run_steps_timed(align, phases=True)
+    ctx.run_steps_timed(align + 20, phases=True)
+    first = args.warmup + align + 20
+    config["timed_steps"] = f"steps {first}..{first + args.steps} (warm-up: {args.warmup} steps, then {align + 20} more to a replayed step graph)"
     barrier(world)
     launches0 = ctx.launches()
     # phase events of the last graph only; the force kernel's average comes
     # from a separate profiled window of the same length inside the run
-    with ClockSampler(local) as clocks:
-        done, ms, phases, psteps = ctx.run_steps_timed(args.steps, phases=True)
+    clocks.mark_start()
+    done, ms, phases, psteps = ctx.run_steps_timed(args.steps, phases=True)
+    clocks.mark_end()
+    clocks.__exit__(None, None, None)
     launches = ctx.launches() - launches0
     ms_max = all_max(ms, world)
     barrier(world)

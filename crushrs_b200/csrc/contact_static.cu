@@ -2,13 +2,18 @@
 // that allocates nothing.
 //
 // Its scratch is one fixed-size record in static device memory of this
-// library (one copy per device, created when the module loads on that
-// device). The host resolves the record's address once per device with
-// cudaGetSymbolAddress and caches it; after that a call is argument checks
-// and six kernel launches on the caller's stream: no device or host
+// library (one copy per CUDA context, created when the module loads in that
+// context). The host resolves the record's address with
+// cudaGetSymbolAddress on the first call in a context and caches it per
+// device together with the context's unique id; a call from another context
+// on that device (a driver-API context, or the primary context recreated
+// after cudaDeviceReset) resolves it again. After that a call is argument
+// checks and six kernel launches on the caller's stream: no device or host
 // allocation, no copy, no synchronisation.
-#include <atomic>
+#include <cuda.h>  // CUcontext and CUresult only: the driver calls go through cudaGetDriverEntryPoint
+
 #include <cmath>
+#include <mutex>
 
 #include "crush.h"
 #include "host/errors.hpp"
@@ -22,7 +27,67 @@ namespace {
 static __device__ __align__(256) unsigned char g_contact_scratch[sizeof(StaticContactScratch)];
 
 constexpr int MAX_DEVICES = 64;
-std::atomic<void*> g_scratch_addr[MAX_DEVICES];  // static storage: starts null
+
+// Per device: the id of the context whose record address is cached, and the
+// address (static storage: starts empty).
+struct ScratchCache {
+    std::mutex lock;
+    unsigned long long ctx_id[MAX_DEVICES];
+    void* addr[MAX_DEVICES];
+};
+ScratchCache g_cache;
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+
+// The unique id of the current CUDA context (ids are never reused within a
+// process, unlike context handles); false when no context is current or the
+// driver lacks the calls. The driver entry points are looked up once.
+bool current_context_id(unsigned long long* id) {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<CtxGetIdFn>(f);
+        cudaGetLastError();
+    });
+    if (!get_current || !get_id) return false;
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+    return get_id(ctx, id) == CUDA_SUCCESS;
+}
+
+// The scratch record's device address in the current context of device `dev`.
+bool scratch_address(int dev, void** out) {
+    unsigned long long id = 0;
+    bool have_id = current_context_id(&id);
+    std::lock_guard<std::mutex> g(g_cache.lock);
+    if (have_id && dev < MAX_DEVICES && g_cache.addr[dev] && g_cache.ctx_id[dev] == id) {
+        *out = g_cache.addr[dev];
+        return true;
+    }
+    // First call in this context: resolve the address (this can load the
+    // library's kernels into the context, and makes the device's primary
+    // context current when none was).
+    void* addr = nullptr;
+    if (cudaGetSymbolAddress(&addr, g_contact_scratch) != cudaSuccess || !addr) {
+        cudaGetLastError();
+        return false;
+    }
+    if (!have_id) have_id = current_context_id(&id);
+    if (have_id && dev < MAX_DEVICES) {
+        g_cache.ctx_id[dev] = id;
+        g_cache.addr[dev] = addr;
+    }
+    *out = addr;
+    return true;
+}
 
 }  // namespace
 
@@ -51,16 +116,9 @@ extern "C" int crush_contact_apply_static(int64_t n_model_nodes, const double* p
         cudaGetLastError();
         return fail_literal(CRUSH_ERR_CUDA, "crush_contact_apply_static: no current CUDA device");
     }
-    void* addr = dev < MAX_DEVICES ? g_scratch_addr[dev].load(std::memory_order_acquire) : nullptr;
-    if (!addr) {
-        // First call on this device: resolve the record's address (this can
-        // load the library's kernels onto the device).
-        if (cudaGetSymbolAddress(&addr, g_contact_scratch) != cudaSuccess || !addr) {
-            cudaGetLastError();
-            return fail_literal(CRUSH_ERR_CUDA, "crush_contact_apply_static: cannot resolve the scratch address on this device");
-        }
-        if (dev < MAX_DEVICES) g_scratch_addr[dev].store(addr, std::memory_order_release);
-    }
+    void* addr = nullptr;
+    if (!scratch_address(dev, &addr))
+        return fail_literal(CRUSH_ERR_CUDA, "crush_contact_apply_static: cannot resolve the scratch address on this device");
     launch_contact_static(static_cast<cudaStream_t>(stream), static_cast<StaticContactScratch*>(addr), n_model_nodes, positions_device,
                           u_device, masses_device, n_nodes, nodes_device, node_scale_device, n_faces, faces_device, stiffness,
                           max_distance, dt, f_accum_device, stats_device ? &stats_device->penetration_count : nullptr,

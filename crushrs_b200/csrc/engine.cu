@@ -985,6 +985,10 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     }
     c->n_sc_free = free0[n_desc];
     c->n_hc = hc0[n_desc];
+    // Incidence entries are 32-bit (8 e + corner); the padded rows reserve
+    // the two largest values as markers.
+    if (8 * (unsigned long long)E >= (unsigned long long)HC_ELL_MORE)
+        return crush::fail(CRUSH_ERR_INVALID, "too many hexahedra for 32-bit node incidence entries (8 x elements must stay below 2^32 - 2)");
     c->stride = std::max<long long>(32, (c->n_hc + 31) / 32 * 32);
     c->n_sc = E - c->n_hc;
     c->hc_index.resize(E);

@@ -1249,7 +1249,9 @@ __device__ __forceinline__ void record_hit(const ContactArrays& ca, long long s,
     ca.hit_force[3 * s + 1] = mag * g.n[1];
     ca.hit_force[3 * s + 2] = mag * g.n[2];
     atomicAdd(&ca.pen_count[c], 1ull);
-    atomicMax(&ca.pen_max_bits[c], (unsigned long long)__double_as_longlong(-best_sd));
+    // + 0.0 turns a zero depth's -0.0 (signed_d == +0.0 hits) into +0.0, whose
+    // bits order below every positive depth.
+    atomicMax(&ca.pen_max_bits[c], (unsigned long long)__double_as_longlong(-best_sd + 0.0));
 }
 
 // First-hit search: LANES lanes per primary node (a power of two <= 32,
@@ -2218,7 +2220,7 @@ __global__ void k_static_search(StaticContactScratch* sc, const double* __restri
     sc->hit_force[3 * s + 1] = mag * g.n[1];
     sc->hit_force[3 * s + 2] = mag * g.n[2];
     atomicAdd(&sc->pen_count, 1ull);
-    atomicMax(&sc->pen_max_bits, (unsigned long long)__double_as_longlong(-best_sd));
+    atomicMax(&sc->pen_max_bits, (unsigned long long)__double_as_longlong(-best_sd + 0.0));  // + 0.0: no -0.0 bits
 }
 
 // Single block: the entries that hit, compacted in entry order.

@@ -405,15 +405,22 @@ int crush_batch_done(crush_ctx* ctx, int* done_flags, int* all);
  * Limits: n_nodes <= CRUSH_STATIC_MAX_NODES and n_faces <=
  * CRUSH_STATIC_MAX_FACES; larger contacts are rejected with
  * CRUSH_ERR_INVALID and a message (use crush_contact_apply). The primary-node
- * search is exhaustive (cost n_nodes x n_faces).
+ * search is exhaustive (cost n_nodes x n_faces), and the reaction pass scans
+ * the hits once per node occurrence (cost (n_nodes + 4 n_faces) x hits): at
+ * the limits one call is of the order of a billion comparisons, so the call
+ * suits small and mid-size contacts.
  *
  * Memory: the call allocates nothing, host or device. Its scratch is one
  * fixed-size record (about 5.4 MB) in this library's static device memory,
  * one copy per device. The call clears what it uses at its start, so nothing
- * needs zeroing by the caller. The FIRST call on each device resolves the
- * record's address (cudaGetSymbolAddress, which may load the library's
- * kernels onto the device): make that first call with the device current and
- * before any stream capture. Every call on a device shares the one record, so
+ * needs zeroing by the caller. The FIRST call in each CUDA context resolves
+ * the record's address (cudaGetSymbolAddress, which may load the library's
+ * kernels into the context) and caches it per device with the context's
+ * unique id: make that first call with the device current and before any
+ * stream capture. A new context on the device (a driver-API context, or the
+ * primary context after cudaDeviceReset, which also discards the record)
+ * makes the next call resolve the address again, so it counts as a first
+ * call. Every call on a device shares the one record, so
  * calls that can overlap in time (other streams or threads without ordering
  * between them) race and corrupt each other's results: serialise them.
  *

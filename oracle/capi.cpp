@@ -255,6 +255,44 @@ int oracle_run(const crush_model_desc* d, int simd, int threads, crush_results* 
     return r.status;
 }
 
+// Whole run (src/solver.rs:190-381) with the loop time of the steps from
+// `time_from_step` to the end in seconds5[4] (seconds5: wall, forces,
+// contact, step loop, window) and the end state: u, v (3N each) and the
+// per-element erosion flags (E), each optional.
+int oracle_run_window(const crush_model_desc* d, int simd, int threads, int64_t time_from_step, crush_results* out, double* u_out,
+                      double* v_out, uint8_t* eroded_out, double* seconds5) {
+    Model m;
+    std::string e = model_from_desc(d, &m);
+    if (!e.empty()) return fail(e);
+    RunOptions opt;
+    opt.simd = simd != 0;
+    opt.threads = threads;
+    opt.time_from_step = time_from_step;
+    RunResults r;
+    e = run(m, opt, &r);
+    if (!e.empty()) return fail(e);
+    std::memset(out, 0, sizeof(*out));
+    out->time = r.time;
+    out->steps = r.steps;
+    out->eroded_elements = r.eroded;
+    out->dt_min = r.dt_min;
+    out->added_mass_max = r.added_mass_max;
+    out->status = r.status;
+    out->n_vehicles = (int)m.vehicles.size();
+    for (int vi = 0; vi < (int)m.vehicles.size() && vi < 4; ++vi) vehicle_result(m, r, vi, &out->vehicle[vi]);
+    if (u_out) std::memcpy(u_out, r.u.data(), r.u.size() * sizeof(double));
+    if (v_out) std::memcpy(v_out, r.v.data(), r.v.size() * sizeof(double));
+    if (eroded_out) std::memcpy(eroded_out, r.eroded_flags.data(), r.eroded_flags.size());
+    if (seconds5) {
+        seconds5[0] = r.wall_seconds;
+        seconds5[1] = r.force_seconds;
+        seconds5[2] = r.contact_seconds;
+        seconds5[3] = r.loop_seconds;
+        seconds5[4] = r.window_seconds;
+    }
+    return r.status;
+}
+
 // Whole run with time histories (solver.rs:114-187, :283-286, :349-358):
 // the records' times and steps (cap_records each), parts (cap x n_parts x 11)
 // and accelerometer node values (cap x n_acc_nodes x 21); *n_records = taken.

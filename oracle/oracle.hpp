@@ -193,6 +193,7 @@ struct RunOptions {
     int history_steps = 0;   // Settings::history_steps
     std::vector<HistoryAccel> accelerometers;
     int frame_steps = 0;     // Settings::frame_steps
+    int64_t time_from_step = -1;  // window_seconds covers the steps from this one to the end
 };
 struct RunResults {
     double time = 0.0;
@@ -215,7 +216,8 @@ struct RunResults {
     std::vector<int64_t> frame_step;
     std::vector<float> frame_disp, frame_pstrain, frame_stress;
     std::vector<uint8_t> frame_eroded;
-    double force_seconds = 0.0, contact_seconds = 0.0, wall_seconds = 0.0, loop_seconds = 0.0;
+    double force_seconds = 0.0, contact_seconds = 0.0, wall_seconds = 0.0, loop_seconds = 0.0, window_seconds = 0.0;
+    std::vector<uint8_t> eroded_flags;  // per element at the end of the run
 };
 std::string run(const Model& m, const RunOptions& opt, RunResults* r);
 // SAE J211 filter and resampling (src/signal.rs:9-66).

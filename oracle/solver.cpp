@@ -238,7 +238,9 @@ std::string run(const Model& model, const RunOptions& opt, RunResults* res) {
     double dt_cfl = dt, dt_min = INF;
     res->status = 0;
     res->dt_log.clear();
+    double win0 = -1.0;
     while (t < s.end_time) {
+        if (step == opt.time_from_step) win0 = now_s();
         if (adaptive && step % s.adaptive_check_steps == 0) {
             double dt_stable;
             if (stable_time_step(elements, u.data(), &dt_stable)) {
@@ -308,6 +310,8 @@ std::string run(const Model& model, const RunOptions& opt, RunResults* res) {
     res->v = v;
     res->masses = masses;
     res->loop_seconds = now_s() - loop0;
+    res->window_seconds = win0 >= 0.0 ? now_s() - win0 : 0.0;
+    res->eroded_flags.assign(elements.eroded.begin(), elements.eroded.end());
     res->wall_seconds = now_s() - wall0;
     return "";
 }

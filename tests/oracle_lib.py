@@ -49,6 +49,7 @@ def load():
     lib.oracle_session_contact_apply.argtypes = [vp, C.c_int, dp, dp, dp, C.c_double, dp, P(C.c_int64), dp]
     lib.oracle_session_contact_nodes.argtypes = [vp, C.c_int, P(C.c_uint32), P(C.c_int64)]
     lib.oracle_run.argtypes = [P(abi.ModelDesc), C.c_int, C.c_int, P(abi.Results), dp, dp, dp, C.c_int64, dp]
+    lib.oracle_run_window.argtypes = [P(abi.ModelDesc), C.c_int, C.c_int, C.c_int64, P(abi.Results), dp, dp, P(C.c_uint8), dp]
     lib.oracle_run_history.argtypes = [P(abi.ModelDesc), C.c_int, C.c_int, C.c_int, C.c_int, P(abi.Accelerometer), C.c_int64, dp,
                                        P(C.c_int64), dp, dp, P(C.c_int64), P(abi.Results)]
     lib.oracle_run_frames.argtypes = [P(abi.ModelDesc), C.c_int, C.c_int, C.c_int, C.c_int64, dp, P(C.c_int64), fp, fp, fp,
@@ -194,6 +195,23 @@ def run(desc, simd=True, threads=1, want_state=False, want_dt=0):
     st = lib.oracle_run(C.byref(desc), int(simd), threads, C.byref(r), ptr(u), ptr(v), ptr(dt), want_dt, ptr(sec))
     assert st in (0, abi.CRUSH_ERR_NONFINITE), error()
     return r, u, v, dt, sec
+
+
+def run_window(desc, time_from_step=0, simd=True, threads=1, want_state=False):
+    """Whole run with the loop time of the steps from `time_from_step` on.
+    Returns results, u, v, eroded flags (None unless want_state) and
+    seconds (wall, forces, contact, step loop, window)."""
+    lib = load()
+    r = abi.Results()
+    n, e = desc.n_nodes, desc.n_hexes
+    u = np.zeros(3 * n) if want_state else None
+    v = np.zeros(3 * n) if want_state else None
+    er = np.zeros(e, np.uint8) if want_state else None
+    sec = np.zeros(5)
+    st = lib.oracle_run_window(C.byref(desc), int(simd), threads, int(time_from_step), C.byref(r), ptr(u), ptr(v),
+                               None if er is None else er.ctypes.data_as(C.POINTER(C.c_uint8)), ptr(sec))
+    assert st in (0, abi.CRUSH_ERR_NONFINITE), error()
+    return r, u, v, er, sec
 
 
 def run_history(desc, steps, accelerometers=(), cap=100000, simd=True, threads=1):

@@ -1,0 +1,109 @@
+"""The refined head-on (278,640 honeycomb hexahedra of 0.05 m, the
+bandwidth-roofline workload) under the oracle.
+
+Bars (tolerances written in each test):
+  * element forces on identical state, bit-identical to the oracle's f32
+    lane kernel (src/kernel_simd.rs:300-491), on an early state and on a late
+    state with ~2,500 eroded elements taken from a device run;
+  * the whole run to its stop (5000-step cap: the run erodes elements and
+    flings freed nodes, so the separation rule never holds, in the oracle as
+    on the device): the same step count and eroded count as the oracle's f32
+    lane path, delta-v and crush within 0.5 % (they agree to ~1e-9);
+  * the first 200 steps against the oracle's f64 scalar path (before any
+    erosion): delta-v within 0.5 % and displacements to 1e-3 of their
+    largest value, the f32-vs-f64 element arithmetic spread.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from crushrs_b200 import abi, scenarios as S
+from crushrs_b200.engine import Context
+
+from . import oracle_lib as O
+from .test_golden import _elastic_dofs
+
+pytestmark = pytest.mark.gpu
+
+THREADS = os.cpu_count() or 1
+
+
+@pytest.fixture(scope="module")
+def refined():
+    return S.Model.build(S.refined_headon(max_steps=5000))
+
+
+def _hc_mask(model):
+    return np.array([model.material(p).model == abi.MAT_HONEYCOMB for p in model.hex_part()])
+
+
+def _forces_equal(model, ctx, sess, u):
+    fd, fo = np.zeros(3 * model.n_nodes), np.zeros(3 * model.n_nodes)
+    nd = ctx.compute_forces(u, fd)
+    _, no = sess.forces(u, fo)
+    assert nd == no
+    el = _elastic_dofs(model.desc)
+    assert np.array_equal(fd[~el], fo[~el])
+    assert np.abs(fd[el] - fo[el]).max(initial=0.0) <= 1e-9 * np.abs(fo).max()
+    assert np.linalg.norm(fo) > 0.0
+    return nd
+
+
+def test_refined_forces_bit_exact_early_and_eroded(refined):
+    hc = _hc_mask(refined)
+    # early: a seeded crush field on the undeformed mesh
+    ctx = Context(refined.desc)
+    sess = O.Session(refined.desc, simd=True, threads=THREADS)
+    g, v, gm, hh = ctx.element_data()
+    sess.set_lane_geometry(g, v, gm, hh)
+    rng = np.random.default_rng(11)
+    x = refined.positions()
+    u = 0.03 * np.exp(-np.abs(x[:, 0]) / 0.3)[:, None] * rng.normal(size=x.shape)
+    u[refined.fixed_nodes()] = 0.0
+    _forces_equal(refined, ctx, sess, u.reshape(-1))
+    ctx.close()
+    # late: the device run's own state after 3000 steps (elements eroded,
+    # freed nodes far away), handed to the oracle
+    run = Context(refined.desc)
+    run.run_begin()
+    run.run_steps(3000)
+    u_run, _ = run.state()
+    st, er = run.get_state()
+    assert er.sum() > 1000
+    so, eo = sess.get_state()
+    so[hc], eo[hc] = st, er
+    sess.set_state(so, eo)
+    _forces_equal(refined, run, sess, u_run)
+    st2, er2 = run.get_state()
+    so2, eo2 = sess.get_state()
+    assert np.array_equal(st2, so2[hc]) and np.array_equal(er2, eo2[hc])
+
+
+def test_refined_run_matches_f32_oracle(refined):
+    """The whole job against the reference's production (f32 lane) path."""
+    r_dev = Context(refined.desc).run()
+    r_o, u_o, v_o, er_o, _ = O.run_window(refined.desc, simd=True, threads=THREADS)
+    assert r_dev.status == 0 and r_o.status == 0
+    assert r_dev.steps == r_o.steps == 5000
+    assert r_dev.eroded_elements == r_o.eroded_elements
+    for k in range(2):
+        a, b = r_dev.vehicle[k].delta_v[0], r_o.vehicle[k].delta_v[0]
+        assert abs(a - b) <= 5e-3 * abs(b), (k, a, b)
+        a, b = r_dev.vehicle[k].crush, r_o.vehicle[k].crush
+        assert abs(a - b) <= 5e-3 * abs(b), (k, a, b)
+
+
+def test_refined_first_steps_match_f64_oracle():
+    """Before erosion sets in, the device tracks the f64 scalar oracle."""
+    m = S.Model.build(S.refined_headon(max_steps=200))
+    ctx = Context(m.desc)
+    r_dev = ctx.run()
+    u_d, _ = ctx.state()
+    r_o, u_o, _, _, _ = O.run_window(m.desc, simd=False, threads=THREADS, want_state=True)
+    assert r_dev.steps == r_o.steps == 200
+    assert r_dev.eroded_elements == r_o.eroded_elements == 0
+    for k in range(2):
+        a, b = r_dev.vehicle[k].delta_v[0], r_o.vehicle[k].delta_v[0]
+        assert abs(a - b) <= 5e-3 * abs(b), (k, a, b)
+    assert np.abs(u_d - u_o).max() <= 1e-3 * np.abs(u_o).max()

@@ -154,3 +154,33 @@ def test_static_contact_rejects_oversized_and_bad_ids(plain):
     st = abi.ContactStats.from_buffer_copy(static.stats.cpu().numpy().tobytes())
     assert st.status == abi.CRUSH_ERR_INVALID
     assert bool(torch.all(f == 1.5))
+
+
+def test_static_contact_leaves_device_memory_unchanged(plain):
+    """After the first call in this process's context, further calls change
+    neither the device's free memory nor torch's allocator: the call takes
+    all its scratch from the library's static record."""
+    ctx = Context(plain.desc)
+    lumped, _ = ctx.masses()
+    static = _Static(plain, lumped)
+    nodes, faces, _, stiffness, md = plain.contact(plain.desc.n_contacts - 1)
+    nd = _dev(nodes.view(np.int32), torch.int32)
+    fc = _dev(faces.reshape(-1).view(np.int32), torch.int32)
+    ud = _dev(_field(plain.desc, 9, 0.3), torch.float64)
+    f = torch.zeros(3 * plain.n_nodes, dtype=torch.float64, device="cuda")
+
+    def call():
+        contact_apply_static(plain.n_nodes, static.pos.data_ptr(), ud.data_ptr(), static.masses.data_ptr(),
+                             (nd.data_ptr(), len(nodes)), None, (fc.data_ptr(), len(faces)), stiffness, md, 1.0e-4,
+                             f.data_ptr(), static.stats.data_ptr(), 0)
+
+    call()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    alloc0 = torch.cuda.memory_allocated()
+    for _ in range(16):
+        call()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert torch.cuda.memory_allocated() == alloc0
