@@ -211,6 +211,7 @@ def declare_engine_api(lib):
     lib.crush_set_profiling.argtypes = [vp, C.c_int]
     lib.crush_contact_search_stats.argtypes = [vp, C.c_int, P(C.c_uint64), C.c_int]
     lib.crush_set_contact_search.argtypes = [vp, C.c_int]
+    lib.crush_set_step_fusion.argtypes = [vp, C.c_int]
     lib.crush_autotune.argtypes = [vp, P(Tuning)]
     lib.crush_get_tuning.argtypes = [vp, P(Tuning)]
     lib.crush_batch_create.argtypes = [P(P(ModelDesc)), C.c_int, C.c_int, P(vp)]

@@ -85,6 +85,23 @@ __device__ __forceinline__ double step_dt(const Control* c) {
     return d > 1e-15 ? d : 1e-15;
 }
 
+// The dt of the step after the current one when no stable-dt check falls
+// between them: step_dt once the step's end has added this step's dt to t
+// (the same arithmetic, so it is the value the next step will use).
+__device__ __forceinline__ double next_step_dt(const Control* c) {
+    const double t1 = c->t + step_dt(c);
+    double rem = c->end_time - t1;
+    double d = c->dt_cfl < rem ? c->dt_cfl : rem;
+    return d > 1e-15 ? d : 1e-15;
+}
+
+// Whether the current step is the crash's last by the step count or the end
+// time (the stop rules that need no reduction), as the step's end decides it.
+__device__ __forceinline__ bool last_step_by_count_or_time(const Control* c) {
+    const double t1 = c->t + step_dt(c);
+    return (c->max_steps > 0 && c->step + 1 >= c->max_steps) || !(t1 < c->end_time);
+}
+
 // Static planes are read once per step: streamed past L1 (evict-first), so
 // L1 keeps the node positions that neighbouring elements share.
 __device__ __forceinline__ float4 ld_plane(const float4* __restrict__ planes, long long stride, int p, long long e) {

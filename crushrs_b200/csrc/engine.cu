@@ -290,7 +290,9 @@ struct crush_ctx {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join2 = nullptr, ev_forces = nullptr;
     cudaEvent_t ev_heavy = nullptr, ev_heavy_done = nullptr;  // the heavy-node gather beside the contact gather
     cudaEvent_t ev_gathered = nullptr;                         // the contact gather done: side2 resets the event counts
+    cudaEvent_t ev_static = nullptr;                           // the static-grid entries' search done (side2)
     int* mass_flag = nullptr;                  // device: some crash scales its masses this step
+    unsigned* fused_counter = nullptr;         // device: blocks of the fused pass that finished (last one ends the step)
     std::vector<void*> allocs;
     std::unordered_map<void*, size_t> alloc_bytes;  // size of every device allocation
     int64_t launches = 0;
@@ -310,6 +312,8 @@ struct crush_ctx {
 
     // device arrays
     double *pos = nullptr, *u = nullptr, *v = nullptr, *v0 = nullptr, *v_half = nullptr, *f_int = nullptr, *f_ext = nullptr;
+    double* f_ext_odd = nullptr;     // contact forces of odd steps (f_ext: even steps), so a step's pass can run
+                                     // while the previous step's update still reads its own
     double *inv_mass = nullptr, *mass = nullptr, *added = nullptr, *lumped = nullptr, *volume = nullptr, *dt_factor = nullptr;
     double *elem_mass = nullptr, *elem_dt = nullptr, *elem_extra = nullptr;
     double *u_tmp = nullptr, *f_tmp = nullptr, *n_tmp = nullptr, *n_tmp2 = nullptr, *e_tmp = nullptr;
@@ -360,6 +364,9 @@ struct crush_ctx {
     // run
     bool run_open = false;
     long long host_step = 0;
+    bool step_fusion = true;     // fused full + next half step where no check or record falls between
+    bool prologue_done = false;  // the last issued step was fused: the next step's contact forces and half step ran
+    long long pen_stride = 1;    // penetration counters: two sets (even and odd steps) of this many
     int period = 20;
     int base_period = 20;            // the graph period without time histories
     // time histories (crush_history_config)
@@ -436,6 +443,21 @@ struct crush_ctx {
         x.act_stslave = active(7);
         return x;
     }
+    double* f_ext_of(long long step) const { return (step & 1) ? f_ext_odd : f_ext; }
+    // The run's node arrays for step `step`: its contact forces and the next step's.
+    NodeArrays nd_step(long long step) const {
+        NodeArrays a = nd_run();
+        a.f_ext = f_ext_of(step);
+        a.f_ext_next = f_ext_of(step + 1);
+        return a;
+    }
+    // The run's contact arrays for step `step`: its set of penetration counters.
+    ContactArrays ca_step(long long step) const {
+        ContactArrays x = ca_run();
+        x.pen_count = ca.pen_count + (step & 1) * pen_stride;
+        x.pen_max_bits = ca.pen_max_bits + (step & 1) * pen_stride;
+        return x;
+    }
     Active active(int space) const {
         if (!ab.lists) return Active{nullptr, nullptr};
         return Active{ab.lists + space_off_h[space], ab.counts + space};
@@ -449,6 +471,7 @@ struct crush_ctx {
         a.v_half = v_half;
         a.f_int = f_int;
         a.f_ext = f_ext;
+        a.f_ext_next = f_ext_odd;
         a.inv_mass = inv_mass;
         a.mass = mass;
         a.added = added;
@@ -520,6 +543,7 @@ struct crush_ctx {
         if (ev_heavy) cudaEventDestroy(ev_heavy);
         if (ev_heavy_done) cudaEventDestroy(ev_heavy_done);
         if (ev_gathered) cudaEventDestroy(ev_gathered);
+        if (ev_static) cudaEventDestroy(ev_static);
         if (side) cudaStreamDestroy(side);
         if (side2) cudaStreamDestroy(side2);
         if (stream) cudaStreamDestroy(stream);
@@ -899,6 +923,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
         CK(cudaEventCreateWithFlags(&c->ev_heavy, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&c->ev_heavy_done, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&c->ev_gathered, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c->ev_static, cudaEventDisableTiming));
     }
     c->n_slots = n_desc;
     c->slots.resize(n_desc);
@@ -1108,7 +1133,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     }
     TRY(c->upload(&c->v0, cm.v0.data(), 3 * N));
     trace.mark("model uploads");
-    for (double** p : {&c->u, &c->v, &c->v_half, &c->f_int, &c->f_ext, &c->u_tmp, &c->f_tmp}) TRY(c->alloc(p, 3 * N));
+    for (double** p : {&c->u, &c->v, &c->v_half, &c->f_int, &c->f_ext, &c->f_ext_odd, &c->u_tmp, &c->f_tmp}) TRY(c->alloc(p, 3 * N));
     for (double** p : {&c->inv_mass, &c->mass, &c->added, &c->n_tmp, &c->n_tmp2}) TRY(c->alloc(p, N));
     for (double** p : {&c->volume, &c->dt_factor, &c->elem_mass, &c->elem_dt, &c->elem_extra, &c->e_tmp}) TRY(c->alloc(p, E));
     TRY(c->alloc(&c->lumped, 8 * E));
@@ -1121,6 +1146,8 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->alloc(&c->slot_done, c->n_slots));
     TRY(c->alloc(&c->mass_flag, 1));
     CK(cudaMemsetAsync(c->mass_flag, 0, sizeof(int), c->stream));
+    TRY(c->alloc(&c->fused_counter, 1));
+    CK(cudaMemsetAsync(c->fused_counter, 0, sizeof(unsigned), c->stream));
     CK(cudaMemsetAsync(c->planes, 0, sizeof(float4) * N_STATIC_PLANES * c->stride, c->stream));
     CK(cudaMemsetAsync(c->eroded_all, 0, E, c->stream));
     CK(cudaMemsetAsync(c->ctls, 0, sizeof(Control) * c->n_slots, c->stream));
@@ -1321,7 +1348,6 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->alloc(&ca.cells, (size_t)std::max<long long>(c->n_faces, 1)));
     TRY(c->alloc(&ca.gather_work, std::max<size_t>(cnode.size(), 1)));
     TRY(c->alloc(&ca.ev_pool_n, 2));
-    TRY(c->alloc(&ca.u_next, 3 * (size_t)std::max<long long>(c->n_nodes, 1)));
     ca.gather_count = ca.ev_pool_n + 1;
     ca.n_buckets = tab_off.back();
     ca.exhaustive = 0;
@@ -1332,8 +1358,9 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     TRY(c->alloc(&ca.big_box, 6 * (size_t)ca.big_cap));
     TRY(c->alloc(&ca.big_best, (size_t)std::max<long long>(c->n_slaves, 1)));
     TRY(c->alloc(&ca.search_stats, 3 * (size_t)std::max(c->n_contacts, 1)));
-    TRY(c->alloc(&ca.pen_count, std::max(c->n_contacts, 1)));
-    TRY(c->alloc(&ca.pen_max_bits, std::max(c->n_contacts, 1)));
+    c->pen_stride = std::max(c->n_contacts, 1);
+    TRY(c->alloc(&ca.pen_count, 2 * (size_t)c->pen_stride));
+    TRY(c->alloc(&ca.pen_max_bits, 2 * (size_t)c->pen_stride));
     TRY(c->upload_const(&ca.counts_for_stop, counts_for_stop));
     ca.n_cnodes = (long long)cnode.size();
     TRY(c->upload_const(&ca.cnode, cnode));
@@ -1364,8 +1391,8 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     CK(cudaMemsetAsync(ca.grid_state, 0, sizeof(int) * (2 * (size_t)std::max(kc, 1) + 1), c->stream));
     CK(cudaMemsetAsync(ca.blen, 0, sizeof(int) * std::max(tab_off.back(), 1), c->stream));
     CK(cudaMemsetAsync(ca.search_stats, 0, sizeof(unsigned long long) * 3 * std::max(c->n_contacts, 1), c->stream));
-    CK(cudaMemsetAsync(ca.pen_count, 0, sizeof(unsigned long long) * std::max(c->n_contacts, 1), c->stream));
-    CK(cudaMemsetAsync(ca.pen_max_bits, 0, sizeof(unsigned long long) * std::max(c->n_contacts, 1), c->stream));
+    CK(cudaMemsetAsync(ca.pen_count, 0, sizeof(unsigned long long) * 2 * c->pen_stride, c->stream));
+    CK(cudaMemsetAsync(ca.pen_max_bits, 0, sizeof(unsigned long long) * 2 * c->pen_stride, c->stream));
     CK(cudaMemsetAsync(ca.ev_count, 0, sizeof(int) * std::max<size_t>(cnode.size(), 1), c->stream));
     CK(cudaMemsetAsync(ca.ev_pool_n, 0, 2 * sizeof(int), c->stream));
     trace.mark("contacts");
@@ -1507,15 +1534,49 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
 #undef TRY
 }
 
+// Whether step `step` ends with the fused pass (its full update and the next
+// step's half step in one pass over the nodes, the next step's contact forces
+// computed beside its element forces): nothing falls between the two updates
+// (no stable-dt check or mass scaling, active-list rebuild, non-finite or
+// separation check, time-history record or frame at the next step's start),
+// and the step is not the last one of this issue, so the state between calls
+// is always a whole step's.
+bool fuse_step(const crush_ctx* c, long long step, bool last) {
+    if (!c->step_fusion || last) return false;
+    const long long s1 = step + 1;
+    if (s1 % 20 == 0) return false;
+    if (c->adaptive && s1 % c->check_steps == 0) return false;
+    if (c->any_separation && c->va.n_vehicles > 0 && s1 % 10 == 0) return false;
+    if (c->hist_on && s1 % c->hist.steps == 0) return false;
+    if (c->frames_on && s1 % c->frames.steps == 0) return false;
+    return true;
+}
+
 // One explicit step of every slot on the stream (src/solver.rs:287-345).
 // Phase boundaries of one step recorded when profiling: start, after dt,
 // after contact, after half step, after element forces, after full step, end.
 constexpr int N_PHASE_EVENTS = 7;
 
-int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool capturing = false) {
+// Step `step`:
+//   prologue (unless the previous step was fused, which did it): the active
+//     lists, the stable-dt decision and mass scaling, the contact forces of
+//     this step (its search ran beside the previous step) and the half step;
+//   the next step's contact search on the side streams, reading this step's
+//     X + u, beside the element forces; for a fused step the next step's
+//     contact forces follow the search there, with the next step's dt;
+//   the element forces;
+//   fused: the fused pass (full update, the next step's half step, the
+//     step's end); otherwise the full update, checks, the step's end and
+//     records, with the next step's element dt pass beside the full update.
+// Contact forces of even steps go to f_ext, of odd steps to f_ext_odd, and
+// so do the penetration counters, so the next step's pass can run while
+// this step's update still reads its own.
+int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool capturing = false, bool last = false) {
     ElementArrays el = c->el_run();
-    NodeArrays nd = c->nd_run();
-    ContactArrays cr = c->ca_run();
+    NodeArrays nd = c->nd_step(step);
+    ContactArrays cr = c->ca_step(step);
+    const bool pre = c->prologue_done;
+    const bool fuse = fuse_step(c, step, last);
     int n = 0;
     // Inside a stream capture an event record must be an external event node
     // for its timestamp to be readable after the graph runs.
@@ -1526,46 +1587,58 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
         else cudaEventRecord(ev[i], c->stream);
     };
     mark(0);
-    // Every 20 steps: the chunks that still hold a running crash.
-    if (step % 20 == 0) {
-        launch_build_active(c->stream, c->ab, c->ctls);
-        ++n;
-    }
-    // Stable step check: the element pass ran at the end of the previous
-    // step (or at run begin) on this step's X + u.
-    if (c->adaptive && step % c->check_steps == 0) {
-        launch_dt_finalize(c->stream, c->ctls, c->n_slots, c->mass_flag);
-        launch_mass_scaling(c->stream, el, nd, c->ctls, 0);
-        n += 2;
+    if (!pre) {
+        // Every 20 steps: the chunks that still hold a running crash.
+        if (step % 20 == 0) {
+            launch_build_active(c->stream, c->ab, c->ctls);
+            ++n;
+        }
+        // Stable step check: the element pass ran at the end of the previous
+        // step (or at run begin) on this step's X + u.
+        if (c->adaptive && step % c->check_steps == 0) {
+            launch_dt_finalize(c->stream, c->ctls, c->n_slots, c->mass_flag);
+            launch_mass_scaling(c->stream, el, nd, c->ctls, 0);
+            n += 2;
+        }
     }
     mark(1);
     // Contact forces of this step from the search run beside the previous
     // step's forces (or at crush_run_begin for the first step).
-    if (c->n_contacts > 0) {
-        launch_contact_finish(c->stream, cr, nd, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0.0, c->mass, c->f_ext, 1,
+    if (!pre && c->n_contacts > 0) {
+        launch_contact_finish(c->stream, cr, nd, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0.0, c->mass, nd.f_ext, 1,
                               c->side2, c->ev_heavy, c->ev_heavy_done, c->ev_gathered);
         n += contact_finish_launches(c->n_slaves);
     }
     mark(2);
-    // The next step's contact search needs only the new X + u of the contact
-    // nodes, which the gather wrote to u_next: it runs on the side stream
-    // while this step's half step, forces and update run.
+    if (!pre) {
+        launch_half(c->stream, nd, c->ctls);
+        ++n;
+    }
+    mark(3);
+    // The next step's contact search needs only its X + u, final now: it
+    // runs on the side streams (static-grid entries on side2) beside the
+    // element forces; a fused step's next contact forces follow it there.
     if (c->n_contacts > 0) {
-        NodeArrays nds = nd;
-        nds.u = c->ca.u_next;
+        const ContactArrays cn = c->ca_step(step + 1);
+        const NodeArrays nn = c->nd_step(step + 1);
         cudaEventRecord(c->ev_fork, c->stream);
         cudaStreamWaitEvent(c->side, c->ev_fork, 0);
         cudaStreamWaitEvent(c->side2, c->ev_fork, 0);
-        // static-grid entries on side2: they need no dynamic grid
-        launch_contact_search(c->side, cr, nds, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 1,
+        launch_contact_search(c->side, cn, nn, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 1,
                               c->slave_lanes, c->side2);
         n += contact_search_launches(c->ca, true, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 0);
+        if (fuse) {
+            cudaEventRecord(c->ev_static, c->side2);
+            cudaStreamWaitEvent(c->side, c->ev_static, 0);
+            launch_contact_finish(c->side, cn, nn, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0.0, c->mass, nn.f_ext, 1,
+                                  c->side2, c->ev_heavy, c->ev_heavy_done, c->ev_gathered, 1);
+            n += contact_finish_launches(c->n_slaves);
+        }
         cudaEventRecord(c->ev_join, c->side);
         cudaEventRecord(c->ev_join2, c->side2);
     }
-    launch_half(c->stream, nd, c->ctls);
-    mark(3);
     launch_forces(c->stream, el, nd, c->ctls, 1);
+    n += forces_launches(el);
     // The next step's element dt pass needs its X + u (final after the half
     // step) and this step's erosion (final after the forces): it runs on
     // side2 beside the full update.
@@ -1575,12 +1648,24 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
         cudaStreamWaitEvent(c->side2, c->ev_forces, 0);
         launch_elem_dt(c->side2, el, nd, c->ctls, c->u, 1);
         ++n;
-        if (c->n_contacts == 0) cudaEventRecord(c->ev_join2, c->side2);
+        cudaEventRecord(c->ev_join2, c->side2);
     }
     mark(4);
+    if (fuse) {
+        if (c->n_contacts > 0) {
+            cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+            cudaStreamWaitEvent(c->stream, c->ev_join2, 0);
+        }
+        launch_fused(c->stream, el, nd, c->ctls, cr, c->va, c->slot_done, c->mass_flag, c->fused_counter);
+        ++n;
+        mark(5);
+        c->prologue_done = true;
+        mark(6);
+        return check_launch(c, n);
+    }
     launch_full(c->stream, el, nd, c->ctls);
+    ++n;
     mark(5);
-    n += 2 + forces_launches(el);
     if ((step + 1) % 20 == 0) {
         launch_nonfinite(c->stream, nd, c->ctls);
         ++n;
@@ -1595,7 +1680,7 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
     // Time-history records of the slots whose step is a multiple of
     // history_steps (src/solver.rs:349-351); u, v and the forces are final.
     if (c->hist_on && (step + 1) % c->hist.steps == 0) {
-        launch_history(c->stream, c->hist, nd, c->ctls, c->f_ext, HIST_STEP);
+        launch_history(c->stream, c->hist, nd, c->ctls, nd.f_ext, HIST_STEP);
         n += (c->hist.n_pu > 0 ? 1 : 0) + 1;
     }
     // Frames at multiples of frame_steps (src/solver.rs:345-348).
@@ -1604,12 +1689,12 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
         n += 3;
     }
     if (c->n_contacts > 0) {
-        if (dt_next) cudaEventRecord(c->ev_join2, c->side2);
         cudaStreamWaitEvent(c->stream, c->ev_join, 0);
         cudaStreamWaitEvent(c->stream, c->ev_join2, 0);
     } else if (dt_next) {
         cudaStreamWaitEvent(c->stream, c->ev_join2, 0);
     }
+    c->prologue_done = false;
     mark(6);
     return check_launch(c, n);
 }
@@ -1886,10 +1971,14 @@ int run_begin(crush_ctx* c) {
     CK(cudaMemcpyAsync(c->v, c->v0, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, c->stream));
     CK(cudaMemsetAsync(c->v_half, 0, sizeof(double) * 3 * N, c->stream));
     CK(cudaMemsetAsync(c->f_ext, 0, sizeof(double) * 3 * N, c->stream));
+    CK(cudaMemsetAsync(c->f_ext_odd, 0, sizeof(double) * 3 * N, c->stream));
     CK(cudaMemsetAsync(c->added, 0, sizeof(double) * N, c->stream));
+    CK(cudaMemsetAsync(c->fused_counter, 0, sizeof(unsigned), c->stream));
+    c->prologue_done = false;
     if (c->n_contacts > 0) {
         CK(cudaMemsetAsync(c->ca.big_best, 0x7F, sizeof(int) * std::max<long long>(c->n_slaves, 1), c->stream));  // BIG_NONE
-        CK(cudaMemsetAsync(c->ca.u_next, 0, sizeof(double) * 3 * N, c->stream));                                  // = u
+        CK(cudaMemsetAsync(c->ca.pen_count, 0, sizeof(unsigned long long) * 2 * c->pen_stride, c->stream));
+        CK(cudaMemsetAsync(c->ca.pen_max_bits, 0, sizeof(unsigned long long) * 2 * c->pen_stride, c->stream));
     }
     CK(cudaMemsetAsync(c->eroded_all, 0, c->n_all, c->stream));
     launch_init_state(c->stream, c->n_hc, c->stride, c->state);
@@ -2002,6 +2091,11 @@ int build_graph(crush_ctx* c) {
         st = enqueue_step(c, k, c->profiling ? &c->prof_ev[(size_t)k * N_PHASE_EVENTS] : nullptr, true);
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
     if (st != CRUSH_OK) return st;
+    if (c->prologue_done) {  // the period's last step is never fused (it rebuilds the active lists)
+        cudaGraphDestroy(g);
+        c->prologue_done = false;
+        return crush::fail(CRUSH_ERR_INVALID, "step graph period ends on a fused step");
+    }
     if (e != cudaSuccess) return crush::fail(CRUSH_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
     e = cudaGraphInstantiate(&c->graph, g, 0);
     cudaGraphDestroy(g);
@@ -2022,7 +2116,7 @@ int issue_steps(crush_ctx* c, long long n_steps) {
             if (st != CRUSH_OK) return st;
             c->last_tune_step = c->host_step;
         }
-        const bool use_graph = c->period > 0 && c->host_step % c->period == 0 && n_steps - issued >= c->period;
+        const bool use_graph = c->period > 0 && c->host_step % c->period == 0 && n_steps - issued >= c->period && !c->prologue_done;
         if (use_graph) {
             if (!c->graph) {
                 int64_t before = c->launches;
@@ -2041,7 +2135,7 @@ int issue_steps(crush_ctx* c, long long n_steps) {
                 st = ensure_prof_events(c);
                 if (st != CRUSH_OK) return st;
             }
-            st = enqueue_step(c, c->host_step, c->profiling ? &c->prof_ev[0] : nullptr);
+            st = enqueue_step(c, c->host_step, c->profiling ? &c->prof_ev[0] : nullptr, false, issued + 1 == n_steps);
             if (st != CRUSH_OK) return st;
             c->host_step += 1;
             issued += 1;
@@ -2516,7 +2610,7 @@ int crush_history_config(crush_ctx* c, int slot, int history_steps, int64_t max_
 
 // The last-step record of finished crashes, when due (src/solver.rs:356-358).
 static int history_final(crush_ctx* c) {
-    launch_history(c->stream, c->hist, c->nd(), c->ctls, c->f_ext, HIST_FINAL);
+    launch_history(c->stream, c->hist, c->nd(), c->ctls, c->f_ext, HIST_FINAL, c->f_ext_odd);
     return check_launch(c, (c->hist.n_pu > 0 ? 1 : 0) + 1);
 }
 
@@ -2686,6 +2780,18 @@ int crush_set_contact_search(crush_ctx* c, int exhaustive) {
     if (!c || (exhaustive != 0 && exhaustive != 1)) return crush::fail(CRUSH_ERR_INVALID, "exhaustive must be 0 or 1");
     if (c->ca.exhaustive != exhaustive) {
         c->ca.exhaustive = exhaustive;
+        if (c->graph) {
+            cudaGraphExecDestroy(c->graph);
+            c->graph = nullptr;
+        }
+    }
+    return CRUSH_OK;
+}
+
+int crush_set_step_fusion(crush_ctx* c, int fused) {
+    if (!c || (fused != 0 && fused != 1)) return crush::fail(CRUSH_ERR_INVALID, "fused must be 0 or 1");
+    if (c->step_fusion != (fused == 1)) {
+        c->step_fusion = fused == 1;
         if (c->graph) {
             cudaGraphExecDestroy(c->graph);
             c->graph = nullptr;

@@ -77,11 +77,12 @@ __device__ void frame_axes(const NodeArrays& nd, const uint32_t* fn, double ax[3
 // Block (part unit, chunk b): mass-weighted sums over the chunk's nodes,
 // reduced in a fixed order into partial[pu][b].
 __global__ void __launch_bounds__(HIST_TPB) k_hist_parts(HistoryArrays h, NodeArrays nd, const Control* ctls,
-                                                         const double* __restrict__ f_ext, int mode) {
+                                                         const double* __restrict__ f_ext, int mode, const double* __restrict__ f_ext_odd) {
     __shared__ double sh[HIST_PART_VALUES][HIST_TPB];
     const int pu = blockIdx.x / HIST_BLOCKS, b = blockIdx.x % HIST_BLOCKS;
     const int slot = h.pu_slot[pu];
     if (!hist_due(h, ctls + slot, slot, mode)) return;  // block-uniform
+    if (mode == HIST_FINAL && f_ext_odd && ((ctls[slot].step - 1) & 1)) f_ext = f_ext_odd;
     const long long lo = h.pu_off[pu], len = (long long)h.pu_off[pu + 1] - lo;
     const long long per = (len + HIST_BLOCKS - 1) / HIST_BLOCKS;
     const long long i0 = lo + b * per, i1 = min(lo + len, i0 + per);
@@ -117,10 +118,11 @@ __global__ void __launch_bounds__(HIST_TPB) k_hist_parts(HistoryArrays h, NodeAr
 // then divided by the mass as src/solver.rs:131-139 does) and accelerometer
 // samples, its time and step, and the slot's record count.
 __global__ void __launch_bounds__(HIST_TPB) k_hist_finish(HistoryArrays h, NodeArrays nd, const Control* ctls,
-                                                          const double* __restrict__ f_ext, int mode) {
+                                                          const double* __restrict__ f_ext, int mode, const double* __restrict__ f_ext_odd) {
     const int slot = blockIdx.x;
     const Control* ctl = ctls + slot;
     if (!hist_due(h, ctl, slot, mode)) return;  // block-uniform
+    if (mode == HIST_FINAL && f_ext_odd && ((ctl->step - 1) & 1)) f_ext = f_ext_odd;
     const long long r = h.rec_count[slot];
     const bool keep = r < h.slot_max[slot];
     if (keep) {
@@ -182,9 +184,10 @@ __global__ void __launch_bounds__(HIST_TPB) k_hist_finish(HistoryArrays h, NodeA
 
 }  // namespace
 
-void launch_history(cudaStream_t s, const HistoryArrays& h, const NodeArrays& nd, const Control* ctls, const double* f_ext, int mode) {
-    if (h.n_pu > 0) k_hist_parts<<<(unsigned)(h.n_pu * HIST_BLOCKS), HIST_TPB, 0, s>>>(h, nd, ctls, f_ext, mode);
-    k_hist_finish<<<(unsigned)h.n_slots, HIST_TPB, 0, s>>>(h, nd, ctls, f_ext, mode);
+void launch_history(cudaStream_t s, const HistoryArrays& h, const NodeArrays& nd, const Control* ctls, const double* f_ext, int mode,
+                    const double* f_ext_odd) {
+    if (h.n_pu > 0) k_hist_parts<<<(unsigned)(h.n_pu * HIST_BLOCKS), HIST_TPB, 0, s>>>(h, nd, ctls, f_ext, mode, f_ext_odd);
+    k_hist_finish<<<(unsigned)h.n_slots, HIST_TPB, 0, s>>>(h, nd, ctls, f_ext, mode, f_ext_odd);
 }
 
 }  // namespace crush

@@ -663,6 +663,74 @@ __global__ void k_full(ElementArrays el, NodeArrays nd, Control* ctls) {
     }
 }
 
+// One step's full update fused with the next step's half step
+// (src/solver.rs:334-342, then :314-323 of the next step), thread per node
+// component: the ordered corner gather gives f_int at the new positions,
+// v = (v½ + ½dt a) damping; then, unless this step is the crash's last by
+// its step count or end time, the next step's v½ = v + ½dt' (f_ext' - f_int)/m
+// and u += dt' v½ with the next step's dt' and contact forces f_ext'. The
+// arithmetic is that of full_body followed by half_body; fixed DOFs are zero
+// as there. A crash that stops here keeps u and v½ of this step.
+__device__ __forceinline__ void fused_body(const ElementArrays& el, const NodeArrays& nd, const Control* ctls, long long n, int d) {
+    if (n >= nd.n) return;
+    const long long k = 3 * n + d;
+    const int slot = nd.node_slot[n];
+    const double fe = nd.f_ext[k], fe1 = nd.f_ext_next[k], vh = nd.v_half[k], u0 = nd.u[k], im = nd.inv_mass[n];
+    const bool fixed = nd.fixed[n] != 0;
+    double f = gather_component(nd, el.corner, n, d);
+    if (el.n_sc > 0) f = add_scalar_corners(el, nd, n, d, f);
+    const Control* ctl = ctls + slot;
+    if (ctl->done) return;
+    const double dt = step_dt(ctl);
+    const double a = (fe - f) * im;
+    const double v = fixed ? 0.0 : (vh + 0.5 * dt * a) * ctl->damping;
+    nd.v[k] = v;
+    nd.f_int[k] = f;
+    if (last_step_by_count_or_time(ctl)) return;
+    const double dt1 = next_step_dt(ctl);
+    const double a1 = (fe1 - f) * im;
+    double vh1 = v + 0.5 * dt1 * a1;
+    double u1 = u0 + dt1 * vh1;
+    if (fixed) {
+        u1 = 0.0;
+        vh1 = 0.0;
+    }
+    nd.v_half[k] = vh1;
+    nd.u[k] = u1;
+}
+
+__device__ void step_end_slot(Control* ctl, int sl, const ContactArrays& ca, const VehicleArrays& va, int check_separation);
+
+// The fused pass, then the step's end (k_step_end without the reduction stop
+// rules, which no fused step has) run by the last block to finish: every
+// other block has read the control blocks by then.
+__global__ void k_fused(ElementArrays el, NodeArrays nd, Control* ctls, ContactArrays ca, VehicleArrays va, int* __restrict__ done_out,
+                        int* __restrict__ mass_flag, unsigned* __restrict__ counter) {
+    FOR_ACTIVE(nd.act_node, nd.n, 3, g) {
+        int d;
+        const long long n = active_entity(nd.act_node, g, 3, &d);
+        fused_body(el, nd, ctls, n, d);
+    }
+    __shared__ int s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(counter, 1u) == gridDim.x - 1 ? 1 : 0;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (threadIdx.x == 0) {
+        *mass_flag = 0;
+        *counter = 0;
+    }
+    for (int sl = threadIdx.x; sl < ca.n_slots; sl += blockDim.x) {
+        Control* ctl = ctls + sl;
+        if (!ctl->done) step_end_slot(ctl, sl, ca, va, 0);
+        done_out[sl] = ctl->done;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Stable time step (src/kernel.rs:207-237, src/element.rs:176-186) and the
 // per-element added mass of selective mass scaling (src/kernel.rs:243-258).
@@ -1445,7 +1513,7 @@ __global__ void __launch_bounds__(BRUTE_TPB) k_contact_brute(ContactArrays ca, N
 // overlapping other work); this pass needs the step's dt and records the
 // reaction events and the penetration counters.
 __global__ void k_contact_force(ContactArrays ca, Control* ctls, int c0, int run_mode, double dt_override,
-                                const double* __restrict__ masses, long long n_slaves, int skip_fixed) {
+                                const double* __restrict__ masses, long long n_slaves, int skip_fixed, int next_step) {
     const Active act = run_mode ? ca.act_allslave : Active{nullptr, nullptr};
     const long long s0 = ca.slave_off[c0];
     FOR_ACTIVE(act, n_slaves, FORCE_LANES, g) {
@@ -1458,7 +1526,8 @@ __global__ void k_contact_force(ContactArrays ca, Control* ctls, int c0, int run
         const int c = ca.slave_contact[s];
         const Control* ctl = ctls + ca.contact_slot[c];
         if (run_mode && ctl->done) continue;
-        record_hit(ca, s, c, ca.slaves[s], best, ca.hit_sd[s], dt_override > 0.0 ? dt_override : step_dt(ctl), masses,
+        const double dt = dt_override > 0.0 ? dt_override : (next_step ? next_step_dt(ctl) : step_dt(ctl));
+        record_hit(ca, s, c, ca.slaves[s], best, ca.hit_sd[s], dt, masses,
                    ca.geo[ca.face_off[c] + best], skip_fixed, lane);
     }
 }
@@ -1500,16 +1569,6 @@ __device__ __forceinline__ void apply_event(bool face, double fx, double fy, dou
         sy += fy;
         sz += fz;
     }
-}
-
-// The half step's u of component d of node n given its new f_ext: the
-// arithmetic of half_body, so the value is the one the half step writes.
-__device__ __forceinline__ double half_u(const NodeArrays& nd, const Control* ctl, long long n, int d, double fe) {
-    const long long k = 3 * n + d;
-    const double dt = step_dt(ctl);
-    const double a = (fe - nd.f_int[k]) * nd.inv_mass[n];
-    const double vh = nd.v[k] + 0.5 * dt * a;
-    return nd.u[k] + dt * vh;
 }
 
 // Ordered reaction gather, one thread per contact node. The node's events
@@ -1590,12 +1649,6 @@ __device__ __forceinline__ void gather_body(const ContactArrays& ca, const NodeA
     f_out[3 * n] = sx;
     f_out[3 * n + 1] = sy;
     f_out[3 * n + 2] = sz;
-    if (run_mode) {
-        const Control* ctl = ctls + nd.node_slot[n];
-        ca.u_next[3 * n] = half_u(nd, ctl, n, 0, sx);
-        ca.u_next[3 * n + 1] = half_u(nd, ctl, n, 1, sy);
-        ca.u_next[3 * n + 2] = half_u(nd, ctl, n, 2, sz);
-    }
 }
 
 __global__ void __launch_bounds__(GATHER_TPB) k_contact_gather(ContactArrays ca, NodeArrays nd, Control* ctls, int c0, int c1,
@@ -1761,7 +1814,6 @@ __global__ void __launch_bounds__(HEAVY_TPB) k_contact_gather_heavy(ContactArray
         }
         if (threadIdx.x < 3) {
             f_out[3 * n + threadIdx.x] = acc;
-            if (run_mode) ca.u_next[3 * n + threadIdx.x] = half_u(nd, ctls + nd.node_slot[n], n, threadIdx.x, acc);
         }
         __syncthreads();  // every thread is done with s_n and the shared buffers
     }
@@ -1911,6 +1963,10 @@ void launch_step_end(cudaStream_t s, Control* ctls, const ContactArrays& ca, con
                      int* done_out, int* mass_flag) {
     k_step_end<<<(unsigned)blocks_for(ca.n_slots, 128), 128, 0, s>>>(ctls, ca, va, check_separation, done_out, mass_flag);
 }
+void launch_fused(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, const ContactArrays& ca,
+                  const VehicleArrays& va, int* done_out, int* mass_flag, unsigned* block_counter) {
+    k_fused<<<active_grid(nd.n, 3, TPB, GRID_CAP), TPB, 0, s>>>(el, nd, ctls, ca, va, done_out, mass_flag, block_counter);
+}
 void launch_vehicle_sums(cudaStream_t s, const VehicleArrays& va, const double* mass, const double* v, const double* v0, double* out) {
     if (va.n_vehicles <= 0) return;
     k_vehicle_sums<<<va.n_vehicles, VEH_TPB, 0, s>>>(va, mass, v, v0, out);
@@ -1981,14 +2037,14 @@ void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeAr
 
 void launch_contact_finish(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
                            long long n_faces, long long n_slaves, double dt_override, const double* masses, double* f_out,
-                           int skip_fixed, cudaStream_t s_heavy, cudaEvent_t ev_a, cudaEvent_t ev_b, cudaEvent_t ev_c) {
+                           int skip_fixed, cudaStream_t s_heavy, cudaEvent_t ev_a, cudaEvent_t ev_b, cudaEvent_t ev_c, int next_step) {
     if (c1 <= c0) return;
     const int run_mode = dt_override > 0.0 ? 0 : 1;
     (void)f0;
     (void)n_faces;
     if (n_slaves > 0)
         k_contact_force<<<active_grid(n_slaves, FORCE_LANES, TPB, GRID_CAP), TPB, 0, s>>>(ca, ctls, c0, run_mode, dt_override, masses,
-                                                                                         n_slaves, skip_fixed);
+                                                                                         n_slaves, skip_fixed, next_step);
     long long nodes = ca.n_cnodes > 0 ? ca.n_cnodes : 1;
     // The heavy nodes (listed by the force pass) and the rest are disjoint:
     // with a second stream the two gathers run side by side.

@@ -52,7 +52,8 @@ struct NodeArrays {
     double* v;
     double* v_half;
     double* f_int;
-    double* f_ext;
+    double* f_ext;           // the step's external (contact) forces
+    double* f_ext_next;      // the next step's, when the step's full update also makes the next step's half step
     double* inv_mass;        // N
     const double* mass;      // N lumped
     double* added;           // N
@@ -170,8 +171,6 @@ struct ContactArrays {
     long long n_grid_faces;
     long long n_buckets;        // total dynamic buckets (tab_off[n_contacts])
     int exhaustive;             // 1: every search tests every face of its contact (no broad phase)
-    double* u_next;             // 3N: the half step's u of every contact node, written by the run's gather
-                                //     (the next search reads it while the half step runs)
     int* gather_work;           // contact nodes with over EV_CAP events this pass (n_cnodes capacity)
     int* gather_count;          // their number (ev_pool_n + 1)
     Active act_slave, act_cnode, act_dynf;  // active chunks of grid-searched entries, contact nodes, moving faces
@@ -240,6 +239,13 @@ void launch_nonfinite(cudaStream_t s, const NodeArrays& nd, Control* ctls);
 void launch_build_active(cudaStream_t s, const ActiveBuild& b, const Control* ctls);
 void launch_step_end(cudaStream_t s, Control* ctls, const ContactArrays& ca, const VehicleArrays& va, int check_separation,
                      int* done_out, int* mass_flag);
+// A step's full update fused with the next step's half step, for steps
+// after which no stable-dt check, record or reduction stop rule comes: one
+// pass over the nodes (the ordered corner-force gather, v, then v_half and u
+// of the next step from nd.f_ext_next), and the step's end for every slot
+// in the last block to finish (block_counter: one zeroed int, left zero).
+void launch_fused(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, const ContactArrays& ca,
+                  const VehicleArrays& va, int* done_out, int* mass_flag, unsigned* block_counter);
 // Contact pass over contacts [c0, c1) (faces [f0, f0 + n_faces), n_slaves
 // primary-node entries, dynamic grid buckets [bk0, bk1)); `lanes` lanes per
 // primary-node search (4, 8, 16 or 32). dt_override > 0 is a drop-in call: every face's
@@ -254,7 +260,9 @@ int contact_launches(const ContactArrays& ca, bool run_mode, long long n_faces, 
 // The two halves of a contact pass. The search (face geometry, grids, first
 // hits) needs only X + u and may run while other work of the step runs; the
 // finish (forces of the hits with the step's dt, hit lists, counters, the
-// ordered gather into f_out) follows it.
+// ordered gather into f_out) follows it. A run's finish with next_step = 1
+// is the next step's pass, run beside this step's element forces: it takes
+// the next step's dt (next_step_dt).
 // s_static (optional): the stream for the static-grid entries' search,
 // which needs nothing else the search builds.
 void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
@@ -263,7 +271,7 @@ void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeAr
 void launch_contact_finish(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
                            long long n_faces, long long n_slaves, double dt_override, const double* masses, double* f_out,
                            int skip_fixed, cudaStream_t s_heavy = nullptr, cudaEvent_t ev_a = nullptr,
-                           cudaEvent_t ev_b = nullptr, cudaEvent_t ev_c = nullptr);
+                           cudaEvent_t ev_b = nullptr, cudaEvent_t ev_c = nullptr, int next_step = 0);
 int contact_search_launches(const ContactArrays& ca, bool run_mode, long long n_faces, long long n_slaves, long long bk0, long long bk1,
                             int c0);
 int contact_finish_launches(long long n_slaves);
@@ -332,7 +340,10 @@ struct HistoryArrays {
 // One record of every slot that is due (mode: the run's first record, a
 // step record every `steps` steps, or the last-step record of a finished
 // crash). f_ext is the external force the accelerations use.
-void launch_history(cudaStream_t s, const HistoryArrays& h, const NodeArrays& nd, const Control* ctls, const double* f_ext, int mode);
+// HIST_FINAL records take each slot's last step's forces: f_ext when that
+// step (ctl->step - 1) is even, f_ext_odd when it is odd.
+void launch_history(cudaStream_t s, const HistoryArrays& h, const NodeArrays& nd, const Control* ctls, const double* f_ext, int mode,
+                    const double* f_ext_odd = nullptr);
 
 // ---- Frames: nodal displacement and element plastic strain, Cauchy
 // stress and erosion every frame_steps steps (Frame, src/solver.rs) ----

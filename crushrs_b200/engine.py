@@ -246,6 +246,11 @@ class Context:
         """True: every contact search tests every face (no broad phase)."""
         check(self._lib.crush_set_contact_search(self.h, int(bool(exhaustive))))
 
+    def set_step_fusion(self, fused):
+        """True (default): fuse a step's full update with the next step's half
+        step where nothing falls between them; False: separate passes."""
+        check(self._lib.crush_set_step_fusion(self.h, int(bool(fused))))
+
     def contact_search_stats(self, contact_id, reset=False):
         """(exhaustive fallback searches, overflow faces, walked gather roles) of a contact."""
         out = (C.c_uint64 * 3)()

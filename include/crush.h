@@ -257,6 +257,14 @@ int crush_contact_search_stats(crush_ctx* ctx, int contact_id, uint64_t* out, in
  * Both give the same hits: the grids only skip faces that cannot pass the
  * narrow test. For checking that equality; takes effect at the next step. */
 int crush_set_contact_search(crush_ctx* ctx, int exhaustive);
+/* fused = 1 (default) runs a step whose next step starts with no stable-dt
+ * check, record or reduction stop rule as one pass over the nodes (the
+ * step's full update and the next step's half step), with the next step's
+ * contact forces computed beside this step's element forces; 0 runs every
+ * step's half and full updates as separate passes. Both give bit-identical
+ * results (for checking that, and for timing the schedules); takes effect
+ * at the next step. No counterpart in the reference. */
+int crush_set_step_fusion(crush_ctx* ctx, int fused);
 
 /* ---- Time histories: part states and accelerometer samples ----
  * A sampled node set (Accelerometer, src/model.rs:64-73): `nodes` (model

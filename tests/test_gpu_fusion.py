@@ -1,0 +1,78 @@
+"""The fused step schedule (a step's full update and the next step's half
+step as one pass over the nodes, the next step's contact forces computed
+beside the element forces) against separate passes: bit-identical states and
+results, for a whole run, for runs issued in odd-sized pieces, for batches
+whose crashes stop at different steps, and with time histories recorded."""
+import numpy as np
+import pytest
+
+from crushrs_b200 import scenarios as S
+from crushrs_b200.engine import Context
+
+from .test_gpu_batch import _same
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(desc, fused, steps=None):
+    ctx = Context(desc)
+    ctx.set_step_fusion(fused)
+    if steps is None:
+        r = ctx.run()
+    else:
+        ctx.run_begin()
+        for n in steps:  # odd-sized issues: the state between calls is a whole step's
+            ctx.run_steps(n)
+        r = ctx.results()
+    u, v = ctx.state()
+    ctx.close()
+    return r, u, v
+
+
+def test_fused_run_equals_separate_passes():
+    m = S.Model.build(S.plain_headon())
+    a, ua, va = _run(m.desc, True)
+    b, ub, vb = _run(m.desc, False)
+    _same(a, b)
+    assert np.array_equal(ua, ub) and np.array_equal(va, vb)
+
+
+def test_fused_steps_in_odd_issues_equal_separate_passes():
+    m = S.Model.build(S.refined_headon(max_steps=400))
+    a, ua, va = _run(m.desc, True, steps=[3, 7, 1, 29, 60, 13])
+    b, ub, vb = _run(m.desc, False, steps=[113])
+    _same(a, b)
+    assert a.steps == 113
+    assert np.array_equal(ua, ub) and np.array_equal(va, vb)
+
+
+def test_fused_batch_equals_separate_passes():
+    models = [S.Model.build(S.batch_headon(i)) for i in range(6)]
+    models.append(S.Model.build(S.plain_headon(end_time=0.0301)))  # stops on a step that is not a multiple of 5
+    ref = None
+    for fused in (True, False):
+        ctx = Context([m.desc for m in models])
+        ctx.set_step_fusion(fused)
+        rs = ctx.batch_run()
+        ctx.close()
+        if ref is None:
+            ref = rs
+        else:
+            for x, y in zip(ref, rs):
+                _same(x, y)
+
+
+def test_fused_histories_equal_separate_passes():
+    m = S.Model.build(S.plain_headon(end_time=0.05))
+    recs = []
+    for fused in (True, False):
+        ctx = Context(m.desc)
+        ctx.set_step_fusion(fused)
+        ctx.history_config(7, 4096, [m.accelerometer(0), m.accelerometer(1)])
+        ctx.run()
+        recs.append(ctx.history())
+        ctx.close()
+    a, b = recs
+    assert a["records"] == b["records"] > 10
+    for k in ("time", "step", "parts", "nodes"):
+        assert np.array_equal(a[k], b[k]), k
