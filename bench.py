@@ -420,6 +420,7 @@ def main():
     ap.add_argument("--oracle-sample", type=int, default=4)
     ap.add_argument("--serve-rates", default="100,200", help="req/s of the serving section ('' : skip)")
     ap.add_argument("--serve-seconds", type=float, default=30.0)
+    ap.add_argument("--schedule-steps", type=int, default=200, help="steps timed under each step schedule after the main region")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--sections", default="refined,e2e,batched,serving,cpu",
@@ -528,6 +529,14 @@ def main():
     ctx.set_profiling(2)
     _, _, all_phases, all_psteps = ctx.run_steps_timed(20, phases=True)
     lanes, tune_ms = ctx.tuning()
+    # The same run continued under each step schedule (bit-identical
+    # results): separate half and full passes, then the fused one.
+    schedules = {}
+    for name, fused in (("separate", False), ("fused", True)):
+        ctx.set_step_fusion(fused)
+        ctx.run_steps_timed(20)
+        _, ms_s, _, _ = ctx.run_steps_timed(args.schedule_steps)
+        schedules[name] = {"ms_per_step": ms_s / args.schedule_steps, "steps": args.schedule_steps}
     value = world * n_hc * args.steps / (ms_max / 1e3)
     peak, peak_kind = measured_peak()
     forces_ms = phases[3] / psteps
@@ -543,7 +552,7 @@ def main():
                          "peak_kind": peak_kind, "traffic": traffic, "bytes_per_launch": bytes_launch, "avg_launch_ms": forces_ms},
             "step_roofline": {"bytes_per_step": step_bytes, "achieved": step_gbs, "frac": step_gbs / peak},
             "phase_ms_per_step": {k: v / all_psteps for k, v in zip(["dt", "contact", "half", "forces", "gather_full", "checks"], all_phases)},
-            "clocks": clocks.summary(), "run_done_early": done, "slave_lanes": lanes}
+            "clocks": clocks.summary(), "run_done_early": done, "slave_lanes": lanes, "schedules": schedules}
     ctx.close()
     if rank == 0 and world == 1 and not args.no_e2e:
         line["e2e"] = e2e_run(desc, local, n_hc, n_nodes)

@@ -9,9 +9,10 @@ Bars (tolerances written in each test):
     flings freed nodes, so the separation rule never holds, in the oracle as
     on the device): the same step count and eroded count as the oracle's f32
     lane path, delta-v and crush within 0.5 % (they agree to ~1e-9);
-  * the first 200 steps against the oracle's f64 scalar path (before any
-    erosion): delta-v within 0.5 % and displacements to 1e-3 of their
-    largest value, the f32-vs-f64 element arithmetic spread.
+  * the first 200 steps (before any erosion): the state equal to the f32
+    lane path's to 1e-9 in norm, and within the reference's own f32-vs-f64
+    spread of the f64 scalar path (2e-3 in the norm of u, 0.5 % in delta-v
+    and crush).
 """
 import os
 
@@ -94,16 +95,26 @@ def test_refined_run_matches_f32_oracle(refined):
         assert abs(a - b) <= 5e-3 * abs(b), (k, a, b)
 
 
-def test_refined_first_steps_match_f64_oracle():
-    """Before erosion sets in, the device tracks the f64 scalar oracle."""
+def test_refined_first_steps_match_oracles():
+    """Before erosion sets in, the device tracks the f32 lane path to
+    rounding and the f64 scalar path within the reference's own f32-vs-f64
+    spread: after 200 steps the two oracle paths differ by 5.7e-4 in the
+    norm of u (1.2 cm at one contact-interface node), 8e-5 in delta-v and
+    2e-4 in crush; the bars are 2e-3 in the norm and 0.5 % in delta-v and
+    crush."""
     m = S.Model.build(S.refined_headon(max_steps=200))
     ctx = Context(m.desc)
     r_dev = ctx.run()
-    u_d, _ = ctx.state()
-    r_o, u_o, _, _, _ = O.run_window(m.desc, simd=False, threads=THREADS, want_state=True)
-    assert r_dev.steps == r_o.steps == 200
-    assert r_dev.eroded_elements == r_o.eroded_elements == 0
+    u_d, v_d = ctx.state()
+    r32, u32, v32, _, _ = O.run_window(m.desc, simd=True, threads=THREADS, want_state=True)
+    r64, u64, _, _, _ = O.run_window(m.desc, simd=False, threads=THREADS, want_state=True)
+    assert r_dev.steps == r32.steps == r64.steps == 200
+    assert r_dev.eroded_elements == r32.eroded_elements == r64.eroded_elements == 0
+    assert np.linalg.norm(u_d - u32) <= 1e-9 * np.linalg.norm(u32)
+    assert np.linalg.norm(v_d - v32) <= 1e-9 * np.linalg.norm(v32)
+    assert np.linalg.norm(u_d - u64) <= 2e-3 * np.linalg.norm(u64)
     for k in range(2):
-        a, b = r_dev.vehicle[k].delta_v[0], r_o.vehicle[k].delta_v[0]
+        a, b = r_dev.vehicle[k].delta_v[0], r64.vehicle[k].delta_v[0]
         assert abs(a - b) <= 5e-3 * abs(b), (k, a, b)
-    assert np.abs(u_d - u_o).max() <= 1e-3 * np.abs(u_o).max()
+        a, b = r_dev.vehicle[k].crush, r64.vehicle[k].crush
+        assert abs(a - b) <= 5e-3 * abs(b), (k, a, b)
