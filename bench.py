@@ -531,9 +531,13 @@ def main():
     lanes, tune_ms = ctx.tuning()
     # The same run continued under each step schedule (bit-identical
     # results): separate half and full passes, then the fused one.
-    schedules = {}
-    for name, fused in (("separate", False), ("fused", True)):
+    # The element kernel's schedule the run chose (and the trial's timings).
+    chosen, trial_ms = ctx.schedule()
+    schedules = {"chosen_forces_schedule": chosen, "trial_ms_per_step": trial_ms}
+    for name, fused, fs in (("separate, persistent forces", False, 0), ("fused, persistent forces", True, 0),
+                            ("fused, block-per-chunk forces", True, 1)):
         ctx.set_step_fusion(fused)
+        ctx.set_tuning(lanes, fs)
         ctx.run_steps_timed(20)
         _, ms_s, _, _ = ctx.run_steps_timed(args.schedule_steps)
         schedules[name] = {"ms_per_step": ms_s / args.schedule_steps, "steps": args.schedule_steps}

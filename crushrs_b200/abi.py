@@ -214,6 +214,7 @@ def declare_engine_api(lib):
     lib.crush_set_step_fusion.argtypes = [vp, C.c_int]
     lib.crush_autotune.argtypes = [vp, P(Tuning)]
     lib.crush_get_tuning.argtypes = [vp, P(Tuning)]
+    lib.crush_set_tuning.argtypes = [vp, P(Tuning)]
     lib.crush_batch_create.argtypes = [P(P(ModelDesc)), C.c_int, C.c_int, P(vp)]
     lib.crush_batch_size.argtypes = [vp]
     lib.crush_batch_run.argtypes = [vp, P(Results)]
@@ -283,8 +284,9 @@ class Tuning(C.Structure):
     """crush_tuning: the launch schedule the autotuner chose."""
     _fields_ = [
         ("slave_lanes", C.c_int32),
-        ("reserved", C.c_int32),
+        ("forces_schedule", C.c_int32),
         ("contact_ms", C.c_double * 6),
+        ("step_ms", C.c_double * 2),
     ]
 
 

@@ -383,7 +383,13 @@ struct crush_ctx {
     FrameArrays frames{};
     bool frames_on = false, frames_ran = false;
     std::vector<void*> frame_bufs;
-    cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph = nullptr;      // step graph of the current element-kernel schedule
+    cudaGraphExec_t graph_alt = nullptr;  // of the other schedule, kept while both are tried
+    int n_sms = 148;
+    int forces_schedule = 0;              // launch_forces schedule (0 persistent wave, 1 block per chunk)
+    bool tuning_fixed = false;            // set by crush_set_tuning: no automatic re-tuning
+    bool sched_trial_pending = false;     // time both schedules at the next four graph launches
+    double sched_ms[2] = {0.0, 0.0};      // measured ms per step of the step graph under each schedule
     int64_t graph_launches = 0;
     bool profiling = false;
     int prof_level = 2;  // 1: events around the element-force kernel only; 2: every phase
@@ -531,6 +537,7 @@ struct crush_ctx {
     }
     ~crush_ctx() {
         if (graph) cudaGraphExecDestroy(graph);
+        if (graph_alt) cudaGraphExecDestroy(graph_alt);
         for (cudaEvent_t e : prof_ev) cudaEventDestroy(e);
         if (stream) cudaStreamSynchronize(stream);
         if (side) cudaStreamSynchronize(side);
@@ -557,6 +564,14 @@ int check_launch(crush_ctx* c, int n = 1) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return crush::fail(CRUSH_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
     return CRUSH_OK;
+}
+
+// The step graphs (both element-kernel schedules) no longer match the
+// context's launch sequence.
+void drop_graphs(crush_ctx* c) {
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    if (c->graph_alt) cudaGraphExecDestroy(c->graph_alt);
+    c->graph = c->graph_alt = nullptr;
 }
 
 int sync(crush_ctx* c) {
@@ -910,6 +925,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     c->device = device;
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CK(cudaDeviceGetAttribute(&c->n_sms, cudaDevAttrMultiProcessorCount, device));
 
     {
         int lo = 0, hi = 0;
@@ -1637,7 +1653,7 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
         cudaEventRecord(c->ev_join, c->side);
         cudaEventRecord(c->ev_join2, c->side2);
     }
-    launch_forces(c->stream, el, nd, c->ctls, 1);
+    launch_forces(c->stream, el, nd, c->ctls, 1, c->n_sms, c->forces_schedule);
     n += forces_launches(el);
     // The next step's element dt pass needs its X + u (final after the half
     // step) and this step's erosion (final after the forces): it runs on
@@ -1700,6 +1716,11 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
 }
 
 constexpr long long RETUNE_STEPS = 1000;
+// Contexts at least this large time both element-kernel schedules on their
+// own steps: which is faster depends on how much of the next step's contact
+// pass the element kernel's SMs hold back.
+constexpr long long SCHED_TRIAL_MIN_ELEMENTS = 65536;
+
 
 // The contact search at the open run's current X + u, on the main stream:
 // what the next step's contact forces read (run begin, and after anything
@@ -1754,10 +1775,7 @@ int autotune(crush_ctx* c) {
     CK(cudaMemsetAsync(c->ca.pen_max_bits, 0, sizeof(unsigned long long) * c->n_contacts, c->stream));
     if (best_lanes != c->slave_lanes) {
         c->slave_lanes = best_lanes;
-        if (c->graph) {
-            cudaGraphExecDestroy(c->graph);
-            c->graph = nullptr;
-        }
+        drop_graphs(c);
     }
     return CRUSH_OK;
 }
@@ -1786,10 +1804,7 @@ int rebuild_frames(crush_ctx* c) {
     free_bufs(c, c->frame_bufs);
     c->frames = FrameArrays{};
     c->frames_ran = false;
-    if (c->graph) {
-        cudaGraphExecDestroy(c->graph);
-        c->graph = nullptr;
-    }
+    drop_graphs(c);
     int steps = 0;
     long long stride = 0, max3n = 1, maxe = 1;
     std::vector<int> on(c->n_slots);
@@ -1873,10 +1888,7 @@ int rebuild_history(crush_ctx* c) {
     free_bufs(c, c->hist_bufs);
     c->hist = HistoryArrays{};
     c->hist_ran = false;
-    if (c->graph) {
-        cudaGraphExecDestroy(c->graph);
-        c->graph = nullptr;
-    }
+    drop_graphs(c);
     int steps = 0;
     long long stride = 0;
     for (int k = 0; k < c->n_slots; ++k)
@@ -1963,10 +1975,7 @@ int rebuild_history(crush_ctx* c) {
 
 int run_begin(crush_ctx* c) {
     const long long N = c->n_nodes;
-    if (c->graph) {
-        cudaGraphExecDestroy(c->graph);
-        c->graph = nullptr;
-    }
+    drop_graphs(c);
     CK(cudaMemsetAsync(c->u, 0, sizeof(double) * 3 * N, c->stream));
     CK(cudaMemcpyAsync(c->v, c->v0, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, c->stream));
     CK(cudaMemsetAsync(c->v_half, 0, sizeof(double) * 3 * N, c->stream));
@@ -2030,7 +2039,8 @@ int run_begin(crush_ctx* c) {
     c->host_step = 0;
     c->last_tune_step = 0;
     c->run_open = true;
-    if (!c->tuned) {
+    c->sched_trial_pending = !c->tuning_fixed && c->n_hc >= SCHED_TRIAL_MIN_ELEMENTS;
+    if (!c->tuned && !c->tuning_fixed) {
         st = autotune(c);
         if (st != CRUSH_OK) return st;
     }
@@ -2104,6 +2114,59 @@ int build_graph(crush_ctx* c) {
 }
 
 // Issue n_steps steps (graphs where the step index is on a period boundary).
+// The step graph of element-kernel schedule `schedule`, built if missing
+// (the other schedule's graph is kept for switching back).
+int select_schedule(crush_ctx* c, int schedule) {
+    if (c->forces_schedule != schedule) {
+        std::swap(c->graph, c->graph_alt);
+        c->forces_schedule = schedule;
+    }
+    if (!c->graph) {
+        int64_t before = c->launches;
+        int st = build_graph(c);
+        if (st != CRUSH_OK) return st;
+        c->graph_launches = c->launches - before;
+        c->launches = before;
+    }
+    return CRUSH_OK;
+}
+
+
+// Schedule trial: four graph periods of the run's own steps, alternating
+// the two element-kernel schedules (both compute the same bits), each timed
+// by events on the stream; the faster schedule is kept.
+int schedule_trial(crush_ctx* c) {
+    c->sched_trial_pending = false;
+    cudaEvent_t ev[5];
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    int st = CRUSH_OK;
+    for (int k = 0; k < 4 && st == CRUSH_OK; ++k) {
+        st = select_schedule(c, k & 1);
+        if (st != CRUSH_OK) break;
+        CK(cudaEventRecord(ev[k], c->stream));
+        CK(cudaGraphLaunch(c->graph, c->stream));
+        c->launches += c->graph_launches;
+        c->host_step += c->period;
+    }
+    if (st == CRUSH_OK) {
+        CK(cudaEventRecord(ev[4], c->stream));
+        CK(cudaEventSynchronize(ev[4]));
+        double ms[2] = {0.0, 0.0};
+        for (int k = 0; k < 4; ++k) {
+            float x = 0.f;
+            cudaEventElapsedTime(&x, ev[k], ev[k + 1]);
+            ms[k & 1] += x / (2.0 * c->period);
+        }
+        c->sched_ms[0] = ms[0];
+        c->sched_ms[1] = ms[1];
+        st = select_schedule(c, ms[1] < ms[0] ? 1 : 0);
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    c->last_was_graph = true;
+    return st;
+}
+
+// Issue n_steps steps (graphs where the step index is on a period boundary).
 int issue_steps(crush_ctx* c, long long n_steps) {
     if (!c->run_open) return crush::fail(CRUSH_ERR_INVALID, "no open run (call crush_run_begin)");
     long long issued = 0;
@@ -2111,20 +2174,20 @@ int issue_steps(crush_ctx* c, long long n_steps) {
     while (issued < n_steps) {
         // Crushed faces change the contact search as a run goes on: re-tune
         // every RETUNE_STEPS steps, on a graph boundary.
-        if (c->host_step - c->last_tune_step >= RETUNE_STEPS && (c->period == 0 || c->host_step % c->period == 0)) {
+        if (!c->tuning_fixed && c->host_step - c->last_tune_step >= RETUNE_STEPS && (c->period == 0 || c->host_step % c->period == 0)) {
             st = autotune(c);
             if (st != CRUSH_OK) return st;
             c->last_tune_step = c->host_step;
+            c->sched_trial_pending = c->n_hc >= SCHED_TRIAL_MIN_ELEMENTS;
         }
         const bool use_graph = c->period > 0 && c->host_step % c->period == 0 && n_steps - issued >= c->period && !c->prologue_done;
-        if (use_graph) {
-            if (!c->graph) {
-                int64_t before = c->launches;
-                st = build_graph(c);
-                if (st != CRUSH_OK) return st;
-                c->graph_launches = c->launches - before;
-                c->launches = before;
-            }
+        if (use_graph && c->sched_trial_pending && !c->tuning_fixed && n_steps - issued >= 4 * (long long)c->period) {
+            st = schedule_trial(c);
+            if (st != CRUSH_OK) return st;
+            issued += 4 * (long long)c->period;
+        } else if (use_graph) {
+            st = select_schedule(c, c->forces_schedule);
+            if (st != CRUSH_OK) return st;
             CK(cudaGraphLaunch(c->graph, c->stream));
             c->launches += c->graph_launches;
             c->host_step += c->period;
@@ -2772,7 +2835,24 @@ int crush_get_tuning(const crush_ctx* c, crush_tuning* out) {
     if (!c || !out) return crush::fail(CRUSH_ERR_INVALID, "null argument");
     std::memset(out, 0, sizeof(*out));
     out->slave_lanes = c->slave_lanes;
+    out->forces_schedule = c->forces_schedule;
     for (int k = 0; k < 6; ++k) out->contact_ms[k] = c->tune_ms[k];
+    for (int k = 0; k < 2; ++k) out->step_ms[k] = c->sched_ms[k];
+    return CRUSH_OK;
+}
+
+int crush_set_tuning(crush_ctx* c, const crush_tuning* t) {
+    if (!c || !t) return crush::fail(CRUSH_ERR_INVALID, "null argument");
+    const int lanes = t->slave_lanes;
+    if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
+        return crush::fail(CRUSH_ERR_INVALID, "slave_lanes must be 1, 2, 4, 8, 16 or 32");
+    if (t->forces_schedule != 0 && t->forces_schedule != 1) return crush::fail(CRUSH_ERR_INVALID, "forces_schedule must be 0 or 1");
+    if (lanes != c->slave_lanes || t->forces_schedule != c->forces_schedule) drop_graphs(c);
+    c->slave_lanes = lanes;
+    c->forces_schedule = t->forces_schedule;
+    c->tuning_fixed = true;
+    c->tuned = true;
+    c->sched_trial_pending = false;
     return CRUSH_OK;
 }
 
@@ -2780,10 +2860,7 @@ int crush_set_contact_search(crush_ctx* c, int exhaustive) {
     if (!c || (exhaustive != 0 && exhaustive != 1)) return crush::fail(CRUSH_ERR_INVALID, "exhaustive must be 0 or 1");
     if (c->ca.exhaustive != exhaustive) {
         c->ca.exhaustive = exhaustive;
-        if (c->graph) {
-            cudaGraphExecDestroy(c->graph);
-            c->graph = nullptr;
-        }
+        drop_graphs(c);
     }
     return CRUSH_OK;
 }
@@ -2792,10 +2869,7 @@ int crush_set_step_fusion(crush_ctx* c, int fused) {
     if (!c || (fused != 0 && fused != 1)) return crush::fail(CRUSH_ERR_INVALID, "fused must be 0 or 1");
     if (c->step_fusion != (fused == 1)) {
         c->step_fusion = fused == 1;
-        if (c->graph) {
-            cudaGraphExecDestroy(c->graph);
-            c->graph = nullptr;
-        }
+        drop_graphs(c);
     }
     return CRUSH_OK;
 }
@@ -2819,10 +2893,7 @@ int crush_set_profiling(crush_ctx* c, int level) {
     if (!c || level < 1 || level > 2) return crush::fail(CRUSH_ERR_INVALID, "profiling level must be 1 or 2");
     if (level != c->prof_level) {
         c->prof_level = level;
-        if (c->graph) {
-            cudaGraphExecDestroy(c->graph);
-            c->graph = nullptr;
-        }
+        drop_graphs(c);
     }
     return CRUSH_OK;
 }
@@ -2833,10 +2904,7 @@ int crush_run_steps_timed(crush_ctx* c, int64_t n_steps, int* done, double* ms, 
     const bool want_phases = phase_ms != nullptr;
     if (want_phases != c->profiling) {
         c->profiling = want_phases;
-        if (c->graph) {
-            cudaGraphExecDestroy(c->graph);
-            c->graph = nullptr;
-        }
+        drop_graphs(c);
     }
     cudaEvent_t t0, t1;
     CK(cudaEventCreate(&t0));

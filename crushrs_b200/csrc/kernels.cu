@@ -1923,11 +1923,15 @@ void launch_init_state(cudaStream_t s, long long n_hc, long long stride, float4*
     if (n_hc <= 0) return;
     k_init_state<<<(unsigned)blocks_for(n_hc, TPB), TPB, 0, s>>>(n_hc, stride, state);
 }
-void launch_forces(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, int respect_done) {
-    // Persistent: one wave of FORCES_MINB blocks per SM striding over the
-    // active chunks (measured faster than several waves: no tail).
+void launch_forces(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, int respect_done, int n_sms,
+                   int schedule) {
+    // Schedule 0, persistent: one wave of FORCES_MINB blocks per SM striding
+    // over the active chunks (no tail). Schedule 1: a block per chunk, so
+    // blocks retire all along and work on other streams (the next step's
+    // contact pass) gets SMs while the kernel runs.
+    const long long cap = schedule == 1 ? GRID_CAP * 4 : (long long)n_sms * FORCES_MINB;
     if (el.n_hc > 0)
-        k_forces<<<active_grid(el.n_hc, 1, FORCES_TPB, 148 * FORCES_MINB), FORCES_TPB, 0, s>>>(el, nd, ctls, respect_done);
+        k_forces<<<active_grid(el.n_hc, 1, FORCES_TPB, cap), FORCES_TPB, 0, s>>>(el, nd, ctls, respect_done);
     if (el.n_sc > 0)
         k_forces_scalar<<<active_grid(el.n_sc, 1, SC_TPB, GRID_CAP), SC_TPB, 0, s>>>(el, nd, ctls, respect_done);
 }

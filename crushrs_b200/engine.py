@@ -165,6 +165,19 @@ class Context:
         check(self._lib.crush_get_tuning(self.h, C.byref(t)))
         return t.slave_lanes, list(t.contact_ms)
 
+    def schedule(self):
+        """(element-kernel schedule, measured ms per step of each schedule)."""
+        t = abi.Tuning()
+        check(self._lib.crush_get_tuning(self.h, C.byref(t)))
+        return t.forces_schedule, list(t.step_ms)
+
+    def set_tuning(self, slave_lanes, forces_schedule):
+        """Fix the launch schedule (automatic tuning off)."""
+        t = abi.Tuning()
+        t.slave_lanes = slave_lanes
+        t.forces_schedule = forces_schedule
+        check(self._lib.crush_set_tuning(self.h, C.byref(t)))
+
     def autotune(self):
         """Re-tune at the open run's current state; returns tuning()."""
         t = abi.Tuning()

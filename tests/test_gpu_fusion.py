@@ -76,3 +76,25 @@ def test_fused_histories_equal_separate_passes():
     assert a["records"] == b["records"] > 10
     for k in ("time", "step", "parts", "nodes"):
         assert np.array_equal(a[k], b[k]), k
+
+
+def test_every_launch_schedule_gives_the_same_bits():
+    """Element-kernel schedules (persistent wave, block per chunk) and
+    contact lane counts, fixed by crush_set_tuning, all compute the same
+    run; the automatic schedule trial (a context of 65,536+ hexahedra times
+    both schedules on its first four step graphs) does too."""
+    m = S.Model.build(S.refined_headon(max_steps=200))
+    out = []
+    for tuning in ((32, 0), (8, 1), None):
+        ctx = Context(m.desc)
+        if tuning is not None:
+            ctx.set_tuning(*tuning)
+        ctx.run_begin()
+        ctx.run_steps(200)
+        out.append((ctx.results(), ctx.state(), ctx.schedule()))
+        ctx.close()
+    for r, (u, v), _ in out[1:]:
+        _same(out[0][0], r)
+        assert np.array_equal(out[0][1][0], u) and np.array_equal(out[0][1][1], v)
+    sched, step_ms = out[2][2]
+    assert sched in (0, 1) and step_ms[0] > 0.0 and step_ms[1] > 0.0
