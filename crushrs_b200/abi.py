@@ -285,8 +285,10 @@ class Tuning(C.Structure):
     _fields_ = [
         ("slave_lanes", C.c_int32),
         ("forces_schedule", C.c_int32),
+        ("fused_contact_side", C.c_int32),
+        ("reserved", C.c_int32),
         ("contact_ms", C.c_double * 6),
-        ("step_ms", C.c_double * 2),
+        ("step_ms", C.c_double * 3),
     ]
 
 

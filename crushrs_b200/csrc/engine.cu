@@ -47,6 +47,7 @@ namespace {
     } while (0)
 
 const double INF = std::numeric_limits<double>::infinity();
+constexpr int N_FORCES_SCHEDULES = 3;  // launch_forces schedules 0, 1, 2
 const unsigned long long INF_BITS = 0x7ff0000000000000ull;
 
 // HoneycombParams::from_material with Plasticity::check (src/material.rs:116-151, :430-449).
@@ -384,12 +385,14 @@ struct crush_ctx {
     bool frames_on = false, frames_ran = false;
     std::vector<void*> frame_bufs;
     cudaGraphExec_t graph = nullptr;      // step graph of the current element-kernel schedule
-    cudaGraphExec_t graph_alt = nullptr;  // of the other schedule, kept while both are tried
+    cudaGraphExec_t graphs[N_FORCES_SCHEDULES] = {};  // per schedule, kept while the schedules are tried
     int n_sms = 148;
-    int forces_schedule = 0;              // launch_forces schedule (0 persistent wave, 1 block per chunk)
+    int forces_schedule = 0;              // launch_forces schedule (0 persistent wave, 1 block per chunk, 2 wave on fewer SMs)
+    bool fused_contact_side = false;      // a fused step's next contact forces on the side stream (else main, after the forces)
+    unsigned* forces_queue = nullptr;     // device: chunk queue of the persistent element-kernel waves
     bool tuning_fixed = false;            // set by crush_set_tuning: no automatic re-tuning
-    bool sched_trial_pending = false;     // time both schedules at the next four graph launches
-    double sched_ms[2] = {0.0, 0.0};      // measured ms per step of the step graph under each schedule
+    bool sched_trial_pending = false;     // time the schedules at the next graph launches
+    double sched_ms[N_FORCES_SCHEDULES] = {};  // measured ms per step of the step graph under each schedule
     int64_t graph_launches = 0;
     bool profiling = false;
     int prof_level = 2;  // 1: events around the element-force kernel only; 2: every phase
@@ -536,8 +539,8 @@ struct crush_ctx {
         return st;
     }
     ~crush_ctx() {
-        if (graph) cudaGraphExecDestroy(graph);
-        if (graph_alt) cudaGraphExecDestroy(graph_alt);
+        for (cudaGraphExec_t g : graphs)
+            if (g) cudaGraphExecDestroy(g);
         for (cudaEvent_t e : prof_ev) cudaEventDestroy(e);
         if (stream) cudaStreamSynchronize(stream);
         if (side) cudaStreamSynchronize(side);
@@ -569,9 +572,11 @@ int check_launch(crush_ctx* c, int n = 1) {
 // The step graphs (both element-kernel schedules) no longer match the
 // context's launch sequence.
 void drop_graphs(crush_ctx* c) {
-    if (c->graph) cudaGraphExecDestroy(c->graph);
-    if (c->graph_alt) cudaGraphExecDestroy(c->graph_alt);
-    c->graph = c->graph_alt = nullptr;
+    for (cudaGraphExec_t& g : c->graphs) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+    c->graph = nullptr;
 }
 
 int sync(crush_ctx* c) {
@@ -1164,6 +1169,8 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
     CK(cudaMemsetAsync(c->mass_flag, 0, sizeof(int), c->stream));
     TRY(c->alloc(&c->fused_counter, 1));
     CK(cudaMemsetAsync(c->fused_counter, 0, sizeof(unsigned), c->stream));
+    TRY(c->alloc(&c->forces_queue, 2));
+    CK(cudaMemsetAsync(c->forces_queue, 0, 2 * sizeof(unsigned), c->stream));
     CK(cudaMemsetAsync(c->planes, 0, sizeof(float4) * N_STATIC_PLANES * c->stride, c->stream));
     CK(cudaMemsetAsync(c->eroded_all, 0, E, c->stream));
     CK(cudaMemsetAsync(c->ctls, 0, sizeof(Control) * c->n_slots, c->stream));
@@ -1643,7 +1650,7 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
         launch_contact_search(c->side, cn, nn, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 1,
                               c->slave_lanes, c->side2);
         n += contact_search_launches(c->ca, true, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 0);
-        if (fuse) {
+        if (fuse && c->fused_contact_side) {
             cudaEventRecord(c->ev_static, c->side2);
             cudaStreamWaitEvent(c->side, c->ev_static, 0);
             launch_contact_finish(c->side, cn, nn, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0.0, c->mass, nn.f_ext, 1,
@@ -1653,7 +1660,7 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
         cudaEventRecord(c->ev_join, c->side);
         cudaEventRecord(c->ev_join2, c->side2);
     }
-    launch_forces(c->stream, el, nd, c->ctls, 1, c->n_sms, c->forces_schedule);
+    launch_forces(c->stream, el, nd, c->ctls, 1, c->n_sms, c->forces_schedule, c->forces_queue);
     n += forces_launches(el);
     // The next step's element dt pass needs its X + u (final after the half
     // step) and this step's erosion (final after the forces): it runs on
@@ -1671,6 +1678,17 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
         if (c->n_contacts > 0) {
             cudaStreamWaitEvent(c->stream, c->ev_join, 0);
             cudaStreamWaitEvent(c->stream, c->ev_join2, 0);
+            if (!c->fused_contact_side) {
+                // the next step's contact forces on the main stream, after
+                // the element forces (the search ran beside them)
+                const ContactArrays cn = c->ca_step(step + 1);
+                const NodeArrays nn = c->nd_step(step + 1);
+                launch_contact_finish(c->stream, cn, nn, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0.0, c->mass, nn.f_ext,
+                                      1, c->side2, c->ev_heavy, c->ev_heavy_done, c->ev_gathered, 1);
+                n += contact_finish_launches(c->n_slaves);
+                cudaEventRecord(c->ev_join2, c->side2);
+                cudaStreamWaitEvent(c->stream, c->ev_join2, 0);
+            }
         }
         launch_fused(c->stream, el, nd, c->ctls, cr, c->va, c->slot_done, c->mass_flag, c->fused_counter);
         ++n;
@@ -1716,8 +1734,8 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
 }
 
 constexpr long long RETUNE_STEPS = 1000;
-// Contexts at least this large time both element-kernel schedules on their
-// own steps: which is faster depends on how much of the next step's contact
+// Contexts at least this large time the element-kernel schedules on their
+// own steps: which is fastest depends on how much of the next step's contact
 // pass the element kernel's SMs hold back.
 constexpr long long SCHED_TRIAL_MIN_ELEMENTS = 65536;
 
@@ -2113,35 +2131,37 @@ int build_graph(crush_ctx* c) {
     return CRUSH_OK;
 }
 
-// Issue n_steps steps (graphs where the step index is on a period boundary).
 // The step graph of element-kernel schedule `schedule`, built if missing
 // (the other schedule's graph is kept for switching back).
 int select_schedule(crush_ctx* c, int schedule) {
-    if (c->forces_schedule != schedule) {
-        std::swap(c->graph, c->graph_alt);
-        c->forces_schedule = schedule;
-    }
+    c->forces_schedule = schedule;
+    c->graph = c->graphs[schedule];
     if (!c->graph) {
         int64_t before = c->launches;
         int st = build_graph(c);
         if (st != CRUSH_OK) return st;
+        c->graphs[schedule] = c->graph;
         c->graph_launches = c->launches - before;
         c->launches = before;
     }
     return CRUSH_OK;
 }
 
-
-// Schedule trial: four graph periods of the run's own steps, alternating
-// the two element-kernel schedules (both compute the same bits), each timed
-// by events on the stream; the faster schedule is kept.
+// Schedule trial: 2 x N_FORCES_SCHEDULES graph periods of the run's own
+// steps, cycling through the element-kernel schedules (all compute the same
+// bits), each timed by events on the stream (every schedule's graph is built
+// first, so no host work falls between them); the fastest is kept.
 int schedule_trial(crush_ctx* c) {
     c->sched_trial_pending = false;
-    cudaEvent_t ev[5];
-    for (auto& e : ev) CK(cudaEventCreate(&e));
+    const int keep = c->forces_schedule;
     int st = CRUSH_OK;
-    for (int k = 0; k < 4 && st == CRUSH_OK; ++k) {
-        st = select_schedule(c, k & 1);
+    for (int k = 0; k < N_FORCES_SCHEDULES && st == CRUSH_OK; ++k) st = select_schedule(c, k);
+    if (st != CRUSH_OK) return st;
+    constexpr int RUNS = 2 * N_FORCES_SCHEDULES;
+    cudaEvent_t ev[RUNS + 1];
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    for (int k = 0; k < RUNS && st == CRUSH_OK; ++k) {
+        st = select_schedule(c, k % N_FORCES_SCHEDULES);
         if (st != CRUSH_OK) break;
         CK(cudaEventRecord(ev[k], c->stream));
         CK(cudaGraphLaunch(c->graph, c->stream));
@@ -2149,17 +2169,20 @@ int schedule_trial(crush_ctx* c) {
         c->host_step += c->period;
     }
     if (st == CRUSH_OK) {
-        CK(cudaEventRecord(ev[4], c->stream));
-        CK(cudaEventSynchronize(ev[4]));
-        double ms[2] = {0.0, 0.0};
-        for (int k = 0; k < 4; ++k) {
+        CK(cudaEventRecord(ev[RUNS], c->stream));
+        CK(cudaEventSynchronize(ev[RUNS]));
+        double ms[N_FORCES_SCHEDULES] = {};
+        for (int k = 0; k < RUNS; ++k) {
             float x = 0.f;
             cudaEventElapsedTime(&x, ev[k], ev[k + 1]);
-            ms[k & 1] += x / (2.0 * c->period);
+            ms[k % N_FORCES_SCHEDULES] += x / (2.0 * c->period);
         }
-        c->sched_ms[0] = ms[0];
-        c->sched_ms[1] = ms[1];
-        st = select_schedule(c, ms[1] < ms[0] ? 1 : 0);
+        int best = keep;
+        for (int k = 0; k < N_FORCES_SCHEDULES; ++k) {
+            c->sched_ms[k] = ms[k];
+            if (ms[k] < ms[best]) best = k;
+        }
+        st = select_schedule(c, best);
     }
     for (auto& e : ev) cudaEventDestroy(e);
     c->last_was_graph = true;
@@ -2181,10 +2204,10 @@ int issue_steps(crush_ctx* c, long long n_steps) {
             c->sched_trial_pending = c->n_hc >= SCHED_TRIAL_MIN_ELEMENTS;
         }
         const bool use_graph = c->period > 0 && c->host_step % c->period == 0 && n_steps - issued >= c->period && !c->prologue_done;
-        if (use_graph && c->sched_trial_pending && !c->tuning_fixed && n_steps - issued >= 4 * (long long)c->period) {
+        if (use_graph && c->sched_trial_pending && !c->tuning_fixed && n_steps - issued >= 2 * N_FORCES_SCHEDULES * (long long)c->period) {
             st = schedule_trial(c);
             if (st != CRUSH_OK) return st;
-            issued += 4 * (long long)c->period;
+            issued += 2 * N_FORCES_SCHEDULES * (long long)c->period;
         } else if (use_graph) {
             st = select_schedule(c, c->forces_schedule);
             if (st != CRUSH_OK) return st;
@@ -2836,8 +2859,9 @@ int crush_get_tuning(const crush_ctx* c, crush_tuning* out) {
     std::memset(out, 0, sizeof(*out));
     out->slave_lanes = c->slave_lanes;
     out->forces_schedule = c->forces_schedule;
+    out->fused_contact_side = c->fused_contact_side ? 1 : 0;
     for (int k = 0; k < 6; ++k) out->contact_ms[k] = c->tune_ms[k];
-    for (int k = 0; k < 2; ++k) out->step_ms[k] = c->sched_ms[k];
+    for (int k = 0; k < N_FORCES_SCHEDULES; ++k) out->step_ms[k] = c->sched_ms[k];
     return CRUSH_OK;
 }
 
@@ -2846,10 +2870,14 @@ int crush_set_tuning(crush_ctx* c, const crush_tuning* t) {
     const int lanes = t->slave_lanes;
     if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
         return crush::fail(CRUSH_ERR_INVALID, "slave_lanes must be 1, 2, 4, 8, 16 or 32");
-    if (t->forces_schedule != 0 && t->forces_schedule != 1) return crush::fail(CRUSH_ERR_INVALID, "forces_schedule must be 0 or 1");
-    if (lanes != c->slave_lanes || t->forces_schedule != c->forces_schedule) drop_graphs(c);
+    if (t->forces_schedule < 0 || t->forces_schedule >= N_FORCES_SCHEDULES)
+        return crush::fail(CRUSH_ERR_INVALID, "forces_schedule must be 0, 1 or 2");
+    if (t->fused_contact_side != 0 && t->fused_contact_side != 1) return crush::fail(CRUSH_ERR_INVALID, "fused_contact_side must be 0 or 1");
+    if (lanes != c->slave_lanes || t->forces_schedule != c->forces_schedule || (t->fused_contact_side == 1) != c->fused_contact_side)
+        drop_graphs(c);
     c->slave_lanes = lanes;
     c->forces_schedule = t->forces_schedule;
+    c->fused_contact_side = t->fused_contact_side == 1;
     c->tuning_fixed = true;
     c->tuned = true;
     c->sched_trial_pending = false;

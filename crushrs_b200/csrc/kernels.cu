@@ -489,10 +489,39 @@ __device__ __forceinline__ void gather_node(const NodeArrays& nd, const float* _
     fz = gather_component(nd, corner, n, 2);
 }
 
-__global__ void __launch_bounds__(FORCES_TPB, FORCES_MINB) k_forces(ElementArrays el, NodeArrays nd, Control* ctls, int respect_done) {
-    FOR_ACTIVE(el.act_hc, el.n_hc, 1, g) {
-        int lane;
-        forces_body(el, nd, ctls, respect_done, active_entity(el.act_hc, g, 1, &lane));
+// queue == nullptr: grid-stride over the active chunks. Otherwise a
+// persistent grid whose blocks take active chunks from queue[0] one at a
+// time, so a block that starts late (its SM busy with other streams' work)
+// takes fewer chunks instead of finishing late; the last block to finish
+// (queue[1] counts them) sets both counters back to zero.
+__global__ void __launch_bounds__(FORCES_TPB, FORCES_MINB) k_forces(ElementArrays el, NodeArrays nd, Control* ctls, int respect_done,
+                                                                    unsigned* queue) {
+    if (!queue) {
+        FOR_ACTIVE(el.act_hc, el.n_hc, 1, g) {
+            int lane;
+            forces_body(el, nd, ctls, respect_done, active_entity(el.act_hc, g, 1, &lane));
+        }
+        return;
+    }
+    const long long chunks = active_total(el.act_hc, el.n_hc, 1) / CHUNK;
+    __shared__ long long s_item;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = (long long)atomicAdd(queue, 1u);
+        __syncthreads();
+        const long long item = s_item;
+        __syncthreads();
+        if (item >= chunks) break;
+        for (int t = threadIdx.x; t < CHUNK; t += FORCES_TPB) {
+            int lane;
+            forces_body(el, nd, ctls, respect_done, active_entity(el.act_hc, item * CHUNK + t, 1, &lane));
+        }
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(queue + 1, 1u) == gridDim.x - 1) {
+            queue[0] = 0u;
+            queue[1] = 0u;
+        }
     }
 }
 
@@ -1924,14 +1953,20 @@ void launch_init_state(cudaStream_t s, long long n_hc, long long stride, float4*
     k_init_state<<<(unsigned)blocks_for(n_hc, TPB), TPB, 0, s>>>(n_hc, stride, state);
 }
 void launch_forces(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, int respect_done, int n_sms,
-                   int schedule) {
-    // Schedule 0, persistent: one wave of FORCES_MINB blocks per SM striding
-    // over the active chunks (no tail). Schedule 1: a block per chunk, so
+                   int schedule, unsigned* queue) {
+    // Schedule 0, persistent: one wave of FORCES_MINB blocks per SM taking
+    // chunks from the queue (no tail). Schedule 1: a block per chunk, so
     // blocks retire all along and work on other streams (the next step's
-    // contact pass) gets SMs while the kernel runs.
-    const long long cap = schedule == 1 ? GRID_CAP * 4 : (long long)n_sms * FORCES_MINB;
+    // contact pass) gets SMs while the kernel runs. Schedule 2: the
+    // persistent wave on all but FORCES_FREE_SMS SMs, which stay free for
+    // the side streams. Without a queue, schedules 0 and 2 stride instead.
+    constexpr int FORCES_FREE_SMS = 8;
+    long long cap = (long long)n_sms * FORCES_MINB;
+    if (schedule == 1) cap = GRID_CAP * 4;
+    if (schedule == 2) cap = (long long)(n_sms > 2 * FORCES_FREE_SMS ? n_sms - FORCES_FREE_SMS : n_sms) * FORCES_MINB;
+    unsigned* q = schedule == 1 ? nullptr : queue;
     if (el.n_hc > 0)
-        k_forces<<<active_grid(el.n_hc, 1, FORCES_TPB, cap), FORCES_TPB, 0, s>>>(el, nd, ctls, respect_done);
+        k_forces<<<active_grid(el.n_hc, 1, FORCES_TPB, cap), FORCES_TPB, 0, s>>>(el, nd, ctls, respect_done, q);
     if (el.n_sc > 0)
         k_forces_scalar<<<active_grid(el.n_sc, 1, SC_TPB, GRID_CAP), SC_TPB, 0, s>>>(el, nd, ctls, respect_done);
 }

@@ -171,11 +171,12 @@ class Context:
         check(self._lib.crush_get_tuning(self.h, C.byref(t)))
         return t.forces_schedule, list(t.step_ms)
 
-    def set_tuning(self, slave_lanes, forces_schedule):
+    def set_tuning(self, slave_lanes, forces_schedule, fused_contact_side=0):
         """Fix the launch schedule (automatic tuning off)."""
         t = abi.Tuning()
         t.slave_lanes = slave_lanes
         t.forces_schedule = forces_schedule
+        t.fused_contact_side = fused_contact_side
         check(self._lib.crush_set_tuning(self.h, C.byref(t)))
 
     def autotune(self):

@@ -350,20 +350,25 @@ int crush_resample(const double* t, const double* y, int64_t n, double t0, doubl
  * on the context's own models and keeps the fastest; all choices find the
  * same hits. */
 typedef struct crush_tuning {
-    int32_t slave_lanes;      /* lanes per primary-node search */
-    int32_t forces_schedule;  /* element kernel: 0 one persistent wave of blocks, 1 a block per 256 elements */
-    double contact_ms[6];     /* measured contact pass with 1, 2, 4, 8, 16, 32 lanes (0 = not measured) */
-    double step_ms[2];        /* measured ms per step of the step graph with each forces_schedule (0 = not measured) */
+    int32_t slave_lanes;         /* lanes per primary-node search */
+    int32_t forces_schedule;     /* element kernel: 0 one persistent wave of blocks taking chunks from a queue,
+                                    1 a block per 256 elements, 2 the persistent wave on all but 8 SMs */
+    int32_t fused_contact_side;  /* a fused step computes the next step's contact forces 1: on a side stream
+                                    beside its element forces, 0: on the main stream after them */
+    int32_t reserved;
+    double contact_ms[6];        /* measured contact pass with 1, 2, 4, 8, 16, 32 lanes (0 = not measured) */
+    double step_ms[3];           /* measured ms per step of the step graph with each forces_schedule (0 = not measured) */
 } crush_tuning;
 /* Re-tune now, at the open run's current state (e.g. late in a crash, when
  * crushed faces change the search); the next step uses the new schedule.
  * The element kernel's schedule is tuned on the run's own steps: a run of a
- * context of 65,536+ hexahedra times both schedules over its first four step
- * graphs (and again every 1000 steps, with the lanes) and keeps the faster. */
+ * context of 65,536+ hexahedra times the three schedules over its first six
+ * step graphs (and again every 1000 steps, with the lanes) and keeps the
+ * fastest. */
 int crush_autotune(crush_ctx* ctx, crush_tuning* out);
 int crush_get_tuning(const crush_ctx* ctx, crush_tuning* out);
-/* Fixes the schedule to t's slave_lanes and forces_schedule (measured
- * fields ignored) and turns automatic tuning off for this context. Every
+/* Fixes the schedule to t's slave_lanes, forces_schedule and
+ * fused_contact_side (measured fields ignored) and turns automatic tuning off for this context. Every
  * schedule gives the same results. */
 int crush_set_tuning(crush_ctx* ctx, const crush_tuning* t);
 
