@@ -216,6 +216,8 @@ def declare_engine_api(lib):
     lib.crush_get_tuning.argtypes = [vp, P(Tuning)]
     lib.crush_set_tuning.argtypes = [vp, P(Tuning)]
     lib.crush_batch_create.argtypes = [P(P(ModelDesc)), C.c_int, C.c_int, P(vp)]
+    lib.crush_batch_create_reserved.argtypes = [P(P(ModelDesc)), C.c_int, C.c_int, P(Capacity), P(vp)]
+    lib.crush_batch_append.argtypes = [vp, P(P(ModelDesc)), C.c_int, P(C.c_int)]
     lib.crush_batch_size.argtypes = [vp]
     lib.crush_batch_run.argtypes = [vp, P(Results)]
     lib.crush_batch_results.argtypes = [vp, C.c_int, P(Results)]
@@ -277,6 +279,18 @@ class ServerStats(C.Structure):
         ("bytes_in_use", C.c_double),
         ("peak_bytes_in_use", C.c_double),
         ("budget_bytes", C.c_double),
+    ]
+
+
+class Capacity(C.Structure):
+    """crush_capacity: the room of a context that takes more models later."""
+    _fields_ = [
+        ("slots", C.c_int32),
+        ("contacts", C.c_int32),
+        ("nodes", C.c_int64),
+        ("hexes", C.c_int64),
+        ("faces", C.c_int64),
+        ("primary_nodes", C.c_int64),
     ]
 
 

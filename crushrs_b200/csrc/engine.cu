@@ -104,11 +104,47 @@ size_t next_pow2(size_t x) {
 // primary node; larger ones get a hashed grid.
 constexpr int64_t GRID_MIN_FACES = 256;
 
+// Device array capacities of a context (entities of every space); the first
+// add_slots call allocates them, later calls fill them further.
+struct Capacity {
+    long long slots = 0, nodes = 0, elems = 0, scalars = 0, parts = 0, contacts = 0, faces = 0, slaves = 0, buckets = 0, entries = 0,
+              st_tabs = 0, st_ents = 0, cnodes = 0, roles = 0, vehicles = 0, vnodes = 0;
+};
+
+// The capacities a reservation asks for, or at least `need`.
+Capacity capacity_for(const crush_capacity* r, const Capacity& need) {
+    Capacity c = need;
+    if (!r) return c;
+    auto up = [](long long& x, long long y) { x = std::max(x, y); };
+    up(c.slots, r->slots);
+    up(c.nodes, r->nodes);
+    up(c.elems, r->hexes);
+    // elastic (f64) elements: a road slab or two per slot, or a tenth of the elements
+    up(c.scalars, std::max<long long>(256ll * r->slots, r->hexes / 10));
+    up(c.contacts, r->contacts);
+    up(c.faces, r->faces);
+    up(c.slaves, r->primary_nodes);
+    up(c.parts, 16ll * r->slots);
+    up(c.vehicles, 4ll * r->slots);
+    up(c.vnodes, 2ll * r->nodes);
+    // hashed grids: tables of twice the key-box cells (about 27 per face at
+    // the reference positions) rounded up to a power of two, at least 1024
+    // buckets per contact; entries faces x LEVEL_CELL_BUDGET
+    up(c.buckets, 128ll * r->faces + 2048ll * r->contacts);
+    up(c.entries, (long long)LEVEL_CELL_BUDGET * r->faces);
+    up(c.st_tabs, 128ll * r->faces + 32ll * r->contacts);
+    up(c.st_ents, 64ll * r->faces);
+    up(c.cnodes, r->primary_nodes + 4ll * r->faces);
+    up(c.roles, r->primary_nodes + 4ll * r->faces);
+    return c;
+}
+
 struct Slot {
     crush_settings settings{};
     long long node0 = 0, n_nodes = 0, elem0 = 0, n_elems = 0;
     int contact0 = 0, n_contacts = 0, vehicle0 = 0, n_vehicles = 0;
     int part0 = 0, n_parts = 0;  // the slot's parts in the concatenated part numbering
+    long long hc0 = 0, n_hc = 0, sc0 = 0, n_sc = 0, face0 = 0, n_faces = 0;  // honeycomb, scalar and face ranges
     double contact_dt = INF, stable = INF, dt_floor = 0.0, dt0 = 0.0;
 };
 
@@ -305,7 +341,12 @@ struct crush_ctx {
     std::vector<int64_t> hc_index;   // model element -> honeycomb index or -1
     std::vector<uint32_t> hc_model;  // honeycomb index -> model element
     long long n_sc = 0;              // elastic elements (the scalar f64 path)
-    long long n_sc_free = 0;         // those with a node that is not fixed: numbered first
+    long long n_sc_free = 0;         // those with a node that is not fixed (listed in sc_list_d)
+    long long sc_stride = 1;         // plane stride of the scalar geometry (its room)
+    int n_parts = 0;                 // parts of all slots
+    Capacity cap;                    // room of every entity space (device arrays)
+    long long n_st_ents = 0, n_st_offs = 0, n_st_tabs = 0, n_entries = 0, n_roles = 0, n_vnodes = 0, max_vnodes = 0;
+    std::vector<int> chunk_lo_h, chunk_hi_h;  // slot range of every active chunk (host copy)
     std::vector<uint32_t> sc_model;  // scalar index -> model element
     int check_steps = 5;             // common adaptive_check_steps of the slots
     bool adaptive = true;
@@ -326,7 +367,21 @@ struct crush_ctx {
     double* mat4 = nullptr;
     int64_t* hc_index_d = nullptr;
     int64_t* sc_index_d = nullptr;
-    uint32_t *sc_model_d = nullptr, *sc_off = nullptr, *sc_slot = nullptr;
+    uint32_t *sc_model_d = nullptr, *sc_off = nullptr, *sc_slot = nullptr, *sc_list_d = nullptr;
+    int* setup_bad = nullptr;
+    // contact, vehicle and active-table arrays at their room (ContactArrays,
+    // VehicleArrays and ActiveBuild point into them)
+    int *face_off_d = nullptr, *slave_off_d = nullptr, *tab_off_d = nullptr;
+    long long *st_tab_off_d = nullptr, *ent_off_d = nullptr;
+    uint32_t *faces_d = nullptr, *slaves_d = nullptr, *grid_faces_d = nullptr, *dyn_faces_d = nullptr, *gslaves_d = nullptr,
+             *stslaves_d = nullptr, *cnode_d = nullptr, *cnode_off_d = nullptr, *slave_cn_d = nullptr, *face_cn_d = nullptr,
+             *st_off_d = nullptr, *vnodes_d = nullptr;
+    double *scales_d = nullptr, *stiff_d = nullptr, *md_d = nullptr, *cell_d = nullptr, *st_box_d = nullptr;
+    int *brute_d = nullptr, *counts_for_stop_d = nullptr, *crole_contact_d = nullptr, *crole_slave_d = nullptr, *face_contact_d = nullptr,
+        *slave_contact_d = nullptr, *contact_slot_d = nullptr, *slot_contact_off_d = nullptr, *st_entries_d = nullptr, *vslot_d = nullptr,
+        *vlocal_d = nullptr, *chunk_lo_d = nullptr, *chunk_hi_d = nullptr;
+    uint8_t* is_static_d = nullptr;
+    long long* voff_d = nullptr;
     double *sc_geo = nullptr, *sc_mat = nullptr, *sc_corner = nullptr;
     float4 *planes = nullptr, *state = nullptr;
     float* corner = nullptr;
@@ -418,7 +473,9 @@ struct crush_ctx {
         e.elem_slot = elem_slot;
         e.act_hc = e.act_all = Active{nullptr, nullptr};
         e.n_sc = n_sc;
-        e.sc_stride = n_sc;
+        e.sc_count = n_sc;
+        e.sc_list = nullptr;
+        e.sc_stride = sc_stride;
         e.sc_model = sc_model_d;
         e.sc_geo = sc_geo;
         e.sc_mat = sc_mat;
@@ -435,6 +492,7 @@ struct crush_ctx {
         // rigid road): their forces land only on fixed nodes, whose motion
         // and outputs do not depend on them. Drop-in calls compute them all.
         e.n_sc = n_sc_free;
+        e.sc_list = sc_list_d;
         e.act_sc = active(8);
         return e;
     }
@@ -614,8 +672,12 @@ struct Buf {
     size_t size() const { return n; }
 };
 
-// Combined host arrays of all slots.
+// Combined host arrays of the slots being added: node, element and part
+// arrays start at the context's node_base, elem_base and part_base (global
+// indices minus the base index them); the values stored are global.
 struct Combined {
+    long long node_base = 0, elem_base = 0;
+    int part_base = 0;
     Buf<double> positions, v0;
     std::vector<double> mat4;
     Buf<uint32_t> hexes;
@@ -654,14 +716,16 @@ int check_desc(const crush_model_desc* d) {
 // Slot k's nodes, parts and elements into the combined arrays at its offsets.
 void fill_slot(const crush_model_desc* d, int slot, const Slot& sl, int p0, Combined& cm, long long* n_hc, SlotError& err) {
     const long long N = d->n_nodes, E = d->n_hexes, n0 = sl.node0, e0 = sl.elem0;
-    std::memcpy(&cm.positions[3 * n0], d->positions, sizeof(double) * 3 * N);
-    if (d->initial_velocity) std::memcpy(&cm.v0[3 * n0], d->initial_velocity, sizeof(double) * 3 * N);
-    else std::memset(&cm.v0[3 * n0], 0, sizeof(double) * 3 * N);
-    std::memset(&cm.fixed[n0], 0, N);
-    for (long long i = 0; i < N; ++i) cm.node_slot[n0 + i] = (uint32_t)slot;
+    const long long ln0 = n0 - cm.node_base, le0 = e0 - cm.elem_base;  // positions in the combined arrays
+    const int lp0 = p0 - cm.part_base;
+    std::memcpy(&cm.positions[3 * ln0], d->positions, sizeof(double) * 3 * N);
+    if (d->initial_velocity) std::memcpy(&cm.v0[3 * ln0], d->initial_velocity, sizeof(double) * 3 * N);
+    else std::memset(&cm.v0[3 * ln0], 0, sizeof(double) * 3 * N);
+    std::memset(&cm.fixed[ln0], 0, N);
+    for (long long i = 0; i < N; ++i) cm.node_slot[ln0 + i] = (uint32_t)slot;
     for (int64_t i = 0; i < d->n_fixed; ++i) {
         if (d->fixed_nodes[i] >= (uint64_t)N) return err.set(CRUSH_ERR_INVALID, "fixed node out of range");
-        cm.fixed[n0 + d->fixed_nodes[i]] = 1;
+        cm.fixed[ln0 + d->fixed_nodes[i]] = 1;
     }
     for (int p = 0; p < d->n_parts; ++p) {
         const crush_material& m = d->materials[p];
@@ -683,10 +747,10 @@ void fill_slot(const crush_model_desc* d, int slot, const Slot& sl, int p0, Comb
         } else if (m.model != CRUSH_MAT_ELASTIC) {
             return err.set(CRUSH_ERR_UNSUPPORTED, "unknown material model");
         }
-        cm.mats[p0 + p] = mf;
-        cm.materials[p0 + p] = m;
+        cm.mats[lp0 + p] = mf;
+        cm.materials[lp0 + p] = m;
         const double m4[4] = {m.youngs_modulus, m.poisson_ratio, m.density, d->settings.hourglass};
-        std::memcpy(&cm.mat4[4 * (size_t)(p0 + p)], m4, sizeof(m4));
+        std::memcpy(&cm.mat4[4 * (size_t)(lp0 + p)], m4, sizeof(m4));
     }
     long long hc = 0;
     for (long long e = 0; e < E; ++e) {
@@ -696,10 +760,10 @@ void fill_slot(const crush_model_desc* d, int slot, const Slot& sl, int p0, Comb
         for (int i = 0; i < 8; ++i) {
             const uint64_t n = d->hexes[8 * e + i];
             if (n >= (uint64_t)N) return err.set(CRUSH_ERR_INVALID, "hexahedron node out of range");
-            cm.hexes[8 * (e0 + e) + i] = (uint32_t)(n0 + n);
+            cm.hexes[8 * (le0 + e) + i] = (uint32_t)(n0 + n);
         }
-        cm.hex_part[e0 + e] = p0 + p;
-        cm.elem_slot[e0 + e] = (uint32_t)slot;
+        cm.hex_part[le0 + e] = p0 + p;
+        cm.elem_slot[le0 + e] = (uint32_t)slot;
         hc += honey ? 1 : 0;
     }
     *n_hc = hc;
@@ -721,10 +785,11 @@ struct ContactPart {
 };
 
 // The geometry the broad phase needs of one face at the reference positions.
-void face_frame(const double* pos, const uint32_t* q, double x[4][3], double nr[3], double ctr[3]) {
+// pos holds the nodes from node_base on; q are global node ids.
+void face_frame(const double* pos, long long node_base, const uint32_t* q, double x[4][3], double nr[3], double ctr[3]) {
     double e1[3], e2[3];
     for (int j = 0; j < 4; ++j)
-        for (int dd = 0; dd < 3; ++dd) x[j][dd] = pos[3 * (size_t)q[j] + dd];
+        for (int dd = 0; dd < 3; ++dd) x[j][dd] = pos[3 * (size_t)(q[j] - node_base) + dd];
     for (int dd = 0; dd < 3; ++dd) {
         e1[dd] = x[1][dd] - x[0][dd];
         e2[dd] = x[2][dd] - x[0][dd];
@@ -770,9 +835,9 @@ void build_contacts(const crush_model_desc* d, const Slot& sl, const Combined& c
                 if (nl >= (uint64_t)d->n_nodes) return err.set(CRUSH_ERR_INVALID, "contact face node out of range");
                 const uint32_t n = (uint32_t)(n0 + nl);
                 cp.faces.push_back(n);
-                if (!cm.fixed[n]) stop = true;
+                if (!cm.fixed[n - cm.node_base]) stop = true;
                 for (int dd = 0; dd < 3; ++dd) {
-                    const double p = cm.positions[3 * (size_t)n + dd];
+                    const double p = cm.positions[3 * (size_t)(n - cm.node_base) + dd];
                     lo[dd] = std::fmin(lo[dd], p);
                     hi[dd] = std::fmax(hi[dd], p);
                     flo[dd] = std::fmin(flo[dd], p);
@@ -792,7 +857,7 @@ void build_contacts(const crush_model_desc* d, const Slot& sl, const Combined& c
             const uint32_t n = (uint32_t)(n0 + nl);
             bool inside = true;
             for (int dd = 0; dd < 3; ++dd) {
-                const double p = cm.positions[3 * (size_t)n + dd];
+                const double p = cm.positions[3 * (size_t)(n - cm.node_base) + dd];
                 if (!(p >= lo[dd] && p <= hi[dd])) inside = false;
             }
             if (!inside) continue;
@@ -814,7 +879,7 @@ void build_contacts(const crush_model_desc* d, const Slot& sl, const Combined& c
             double box[6] = {INF, INF, INF, -INF, -INF, -INF};  // union of the key boxes
             for (int64_t f = 0; f < cd.n_faces && ok; ++f) {
                 double x[4][3], nr[3], ctr[3], klo[3], khi[3];
-                face_frame(cm.positions.data(), fq + 4 * f, x, nr, ctr);
+                face_frame(cm.positions.data(), cm.node_base, fq + 4 * f, x, nr, ctr);
                 face_key_box(x, nr, ctr, cd.max_distance, klo, khi);
                 long long r[6];
                 double cells = 1.0;
@@ -864,7 +929,7 @@ void build_contacts(const crush_model_desc* d, const Slot& sl, const Combined& c
                 size_t inserts = 0;
                 for (int64_t f = 0; f < cd.n_faces; ++f) {
                     double x[4][3], nr[3], ctr[3], klo[3], khi[3];
-                    face_frame(cm.positions.data(), fq + 4 * f, x, nr, ctr);
+                    face_frame(cm.positions.data(), cm.node_base, fq + 4 * f, x, nr, ctr);
                     face_key_box(x, nr, ctr, cd.max_distance, klo, khi);
                     double cells = 1.0;
                     for (int dd = 0; dd < 3; ++dd) cells *= std::floor(khi[dd] / cs) - std::floor(klo[dd] / cs) + 1.0;
@@ -924,9 +989,828 @@ void append(std::vector<T>& dst, const std::vector<T>& src) {
     dst.insert(dst.end(), src.begin(), src.end());
 }
 
-int create_impl(const crush_model_desc* const* descs, int n_desc, int device, crush_ctx* c) {
+int begin_slots(crush_ctx* c, int s0, int s1);
+
+// Adds n_desc models as slots [c->n_slots, c->n_slots + n_desc) at the
+// context's current offsets of every entity space. The first call (creating)
+// allocates every device array with room for `reserve` (or exactly the
+// models); a later call fails with CRUSH_ERR_BUSY, changing nothing, when
+// the models do not fit that room. A slot's arrays are exactly those a
+// context of the same models in the same order would hold, so its
+// arithmetic is the same. A call on an open run sets the new slots up as
+// run begin does (their own step 0 starts at the run's current step) and
+// searches their contacts for their first step.
+int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bool creating, const crush_capacity* reserve) {
     if (n_desc <= 0 || !descs) return crush::fail(CRUSH_ERR_INVALID, "no models");
     Trace trace;
+    int st;
+#define TRY(x) do { st = (x); if (st != CRUSH_OK) return st; } while (0)
+    const int S0 = c->n_slots;
+    const long long N0 = c->n_nodes, E0 = c->n_all, H0 = c->n_hc, Q0 = c->n_sc, QF0 = c->n_sc_free;
+    const int P0 = c->n_parts, K0 = c->n_contacts;
+    // ---- sizes and offsets of every new slot ----
+    std::vector<Slot> slots(n_desc);
+    long long N = 0, E = 0;
+    int P = 0, K = 0;
+    std::vector<int> part0(n_desc);
+    for (int k = 0; k < n_desc; ++k) {
+        const crush_model_desc* d = descs[k];
+        TRY(check_desc(d));
+        Slot& sl = slots[k];
+        sl.settings = d->settings;
+        sl.node0 = N0 + N;
+        sl.n_nodes = d->n_nodes;
+        sl.elem0 = E0 + E;
+        sl.n_elems = d->n_hexes;
+        sl.contact0 = K0 + K;
+        sl.n_contacts = d->n_contacts;
+        part0[k] = P0 + P;
+        sl.part0 = P0 + P;
+        sl.n_parts = d->n_parts;
+        N += d->n_nodes;
+        E += d->n_hexes;
+        P += d->n_parts;
+        K += d->n_contacts;
+        if (N0 + N >= (1ll << 31) || E0 + E >= (1ll << 28)) return crush::fail(CRUSH_ERR_INVALID, "models too large for one context");
+    }
+    // The step schedule is shared: every slot must re-check its stable step
+    // on the same cadence.
+    bool adaptive = c->adaptive, any_sep = c->any_separation;
+    int check_steps = c->check_steps;
+    for (int k = 0; k < n_desc; ++k) {
+        const crush_settings& s = descs[k]->settings;
+        const bool ad = !(s.time_step > 0.0) && s.adaptive_check_steps > 0;
+        const int cs = s.adaptive_check_steps > 0 ? s.adaptive_check_steps : 1;
+        if (creating && k == 0) {
+            adaptive = ad;
+            check_steps = cs;
+        } else if (ad != adaptive || (ad && cs != check_steps)) {
+            return crush::fail(CRUSH_ERR_UNSUPPORTED, "models of one context must share adaptive_check_steps and time-step mode");
+        }
+        if (s.stop_rule == CRUSH_STOP_SEPARATION) any_sep = true;
+    }
+    if (!creating && (c->hist_on || c->frames_on))
+        return crush::fail(CRUSH_ERR_UNSUPPORTED, "slots cannot be added to a context that records histories or frames");
+    if (!creating && c->run_open && c->period > 0 && c->host_step % c->period != 0)
+        return crush::fail(CRUSH_ERR_INVALID, "slots join an open run only on a step-graph boundary");
+    Combined cm;
+    cm.node_base = N0;
+    cm.elem_base = E0;
+    cm.part_base = P0;
+    cm.positions.alloc(3 * N);
+    cm.v0.alloc(3 * N);
+    cm.fixed.alloc(N);
+    cm.node_slot.alloc(N);
+    cm.hexes.alloc(8 * E);
+    cm.hex_part.alloc(E);
+    cm.elem_slot.alloc(E);
+    cm.mats.resize(P);
+    cm.materials.resize(P);
+    cm.mat4.resize(4 * (size_t)P);
+    std::vector<SlotError> errs(n_desc);
+    std::vector<long long> slot_hc(n_desc, 0);
+    parallel_for(n_desc, [&](long long k) { fill_slot(descs[k], S0 + (int)k, slots[k], part0[k], cm, &slot_hc[k], errs[k]); });
+    for (auto& e : errs)
+        if (e.code != CRUSH_OK) return crush::fail(e.code, e.msg);
+    trace.mark("validate + concatenate");
+    auto mat_of = [&](long long e) -> const crush_material& { return cm.materials[cm.hex_part[e - E0] - P0]; };
+    auto hex = [&](long long e, int i) { return cm.hexes[8 * (e - E0) + i]; };
+    auto fixed_at = [&](uint32_t n) { return cm.fixed[n - N0] != 0; };
+    // Honeycomb numbering (element order) and, per slot, the elastic
+    // elements with a free node first, then the all-fixed ones (a run
+    // lists only the first).
+    std::vector<long long> slot_free(n_desc, 0);
+    parallel_for(n_desc, [&](long long k) {
+        const Slot& sl = slots[k];
+        long long nf = 0;
+        for (long long e = sl.elem0; e < sl.elem0 + sl.n_elems; ++e) {
+            if (mat_of(e).model == CRUSH_MAT_HONEYCOMB) continue;
+            bool all_fixed = true;
+            for (int i = 0; i < 8; ++i) all_fixed = all_fixed && fixed_at(hex(e, i));
+            nf += all_fixed ? 0 : 1;
+        }
+        slot_free[k] = nf;
+    });
+    std::vector<long long> hc0(n_desc + 1, H0), sc0(n_desc + 1, Q0), scf0(n_desc + 1, QF0);
+    for (int k = 0; k < n_desc; ++k) {
+        hc0[k + 1] = hc0[k] + slot_hc[k];
+        sc0[k + 1] = sc0[k] + (slots[k].n_elems - slot_hc[k]);
+        scf0[k + 1] = scf0[k] + slot_free[k];
+    }
+    const long long H = hc0[n_desc] - H0, Q = sc0[n_desc] - Q0, QF = scf0[n_desc] - QF0;
+    for (int k = 0; k < n_desc; ++k) {
+        slots[k].hc0 = hc0[k];
+        slots[k].n_hc = hc0[k + 1] - hc0[k];
+        slots[k].sc0 = sc0[k];
+        slots[k].n_sc = sc0[k + 1] - sc0[k];
+    }
+    if (8 * (unsigned long long)(E0 + E) >= (unsigned long long)HC_ELL_MORE)
+        return crush::fail(CRUSH_ERR_INVALID, "too many hexahedra for 32-bit node incidence entries (8 x elements must stay below 2^32 - 2)");
+    std::vector<int64_t> hc_index(E), sc_index(E);
+    std::vector<uint32_t> hc_model(H), sc_model(Q), sc_list(QF);
+    Buf<uint32_t> all_off, hc_off, all_slot, hc_slot, sc_off, sc_slot, hc_ell;
+    all_off.alloc(N + 1);
+    hc_off.alloc(N + 1);
+    sc_off.alloc(N + 1);
+    all_slot.alloc(8 * E);
+    hc_slot.alloc(8 * H);
+    hc_ell.alloc(8 * (size_t)N);
+    sc_slot.alloc(8 * Q);
+    parallel_for(n_desc, [&](long long k) {
+        const Slot& sl = slots[k];
+        const long long n0 = sl.node0, e0 = sl.elem0, nn = sl.n_nodes;
+        long long h = hc0[k], qf = sc0[k], qx = sc0[k] + slot_free[k], lf = scf0[k];
+        for (long long e = e0; e < e0 + sl.n_elems; ++e)
+            if (mat_of(e).model == CRUSH_MAT_HONEYCOMB) {
+                hc_index[e - E0] = h;
+                hc_model[h++ - H0] = (uint32_t)e;
+                sc_index[e - E0] = -1;
+            } else {
+                hc_index[e - E0] = -1;
+                bool all_fixed = true;
+                for (int i = 0; i < 8; ++i) all_fixed = all_fixed && fixed_at(hex(e, i));
+                const long long q = all_fixed ? qx++ : qf++;
+                if (!all_fixed) sc_list[lf++ - QF0] = (uint32_t)q;
+                sc_index[e - E0] = q;
+                sc_model[q - Q0] = (uint32_t)e;
+            }
+        // per-node counts, then CSR offsets (global entry positions)
+        std::vector<uint32_t> cnt_a(nn, 0), cnt_b(nn, 0), cnt_c(nn, 0);
+        for (long long e = e0; e < e0 + sl.n_elems; ++e) {
+            const bool honey = hc_index[e - E0] >= 0;
+            for (int i = 0; i < 8; ++i) {
+                const uint32_t n = hex(e, i);
+                cnt_a[n - n0]++;
+                if (honey) cnt_b[n - n0]++;
+                else cnt_c[n - n0]++;
+            }
+        }
+        uint32_t a = (uint32_t)(8 * e0), b = (uint32_t)(8 * hc0[k]), cc = (uint32_t)(8 * sc0[k]);
+        for (long long n = n0; n < n0 + nn; ++n) {
+            all_off[n - N0] = a;
+            hc_off[n - N0] = b;
+            sc_off[n - N0] = cc;
+            a += cnt_a[n - n0];
+            b += cnt_b[n - n0];
+            cc += cnt_c[n - n0];
+        }
+        std::vector<uint32_t> cura(all_off.data() + (n0 - N0), all_off.data() + (n0 - N0) + nn),
+            curb(hc_off.data() + (n0 - N0), hc_off.data() + (n0 - N0) + nn), curc(sc_off.data() + (n0 - N0), sc_off.data() + (n0 - N0) + nn);
+        for (long long e = e0; e < e0 + sl.n_elems; ++e) {
+            const long long he = hc_index[e - E0], se = sc_index[e - E0];
+            for (int i = 0; i < 8; ++i) {
+                const uint32_t n = hex(e, i);
+                all_slot[cura[n - n0]++ - 8 * E0] = (uint32_t)(8 * e + i);
+                if (he >= 0) hc_slot[curb[n - n0]++ - 8 * H0] = (uint32_t)(8 * he + i);
+                else sc_slot[curc[n - n0]++ - 8 * Q0] = (uint32_t)(8 * se + i);
+            }
+        }
+        // the same honeycomb slots as padded rows of 8 (HC_ELL_MORE: the CSR)
+        for (long long n = n0; n < n0 + nn; ++n) {
+            uint32_t* row = &hc_ell[8 * (size_t)(n - N0)];
+            const uint32_t m = cnt_b[n - n0];
+            for (int j = 0; j < 8; ++j) row[j] = (uint32_t)j < m ? hc_slot[hc_off[n - N0] - 8 * H0 + j] : HC_ELL_NONE;
+            if (m > 8) row[0] = HC_ELL_MORE;
+        }
+    });
+    all_off[N] = (uint32_t)(8 * (E0 + E));
+    hc_off[N] = (uint32_t)(8 * (H0 + H));
+    sc_off[N] = (uint32_t)(8 * (Q0 + Q));
+    std::vector<double> sc_mat(2 * (size_t)std::max<long long>(Q, 1), 0.0);
+    for (long long q = 0; q < Q; ++q) {
+        const crush_material& m = mat_of(sc_model[q]);
+        sc_mat[2 * q] = m.youngs_modulus;
+        sc_mat[2 * q + 1] = m.poisson_ratio;
+    }
+    trace.mark("node incidence CSR");
+
+    // ---- contacts: per slot in parallel, then concatenated after the context's ----
+    std::vector<ContactPart> parts(n_desc);
+    parallel_for(n_desc, [&](long long k) { build_contacts(descs[k], slots[k], cm, parts[k], errs[k]); });
+    for (auto& e : errs)
+        if (e.code != CRUSH_OK) return crush::fail(e.code, e.msg);
+    struct Base {
+        long long face, slave, ste, stoff, dyn, grid, cnode, role;
+    };
+    std::vector<Base> base(n_desc + 1);
+    base[0] = Base{c->n_faces, c->n_slaves, c->n_st_ents, c->n_st_offs, c->ca.n_dyn_faces, c->ca.n_grid_faces, c->ca.n_cnodes, c->n_roles};
+    long long tabs = 0, st_tabs = 0, ents = 0;
+    for (int k = 0; k < n_desc; ++k) {
+        const ContactPart& cp = parts[k];
+        const Base& b0 = base[k];
+        base[k + 1] = Base{b0.face + (long long)cp.faces.size() / 4, b0.slave + (long long)cp.slaves.size(),
+                           b0.ste + (long long)cp.st_entries.size(), b0.stoff + (long long)cp.st_off.size(),
+                           b0.dyn + (long long)cp.dyn_faces.size(), b0.grid + (long long)cp.grid_faces.size(),
+                           b0.cnode + (long long)cp.cnode.size(), b0.role + (long long)cp.crole_contact.size()};
+        slots[k].face0 = b0.face;
+        slots[k].n_faces = (long long)cp.faces.size() / 4;
+        for (size_t j = 0; j < cp.nf.size(); ++j) {
+            tabs += cp.tab[j];
+            st_tabs += cp.st[j];
+            ents += cp.tab[j] > 0 ? (long long)cp.nf[j] * LEVEL_CELL_BUDGET : 0;
+        }
+    }
+    const Base& tot = base[n_desc];
+    if (tot.face >= (1ll << 31) || tot.slave >= (1ll << 31) || tot.ste >= (1ll << 32) || tot.role >= (1ll << 32) ||
+        tot.cnode >= (long long)CN_FIXED)
+        return crush::fail(CRUSH_ERR_INVALID, "contacts too large for one context");
+    long long n_veh = 0, n_vnodes = 0;
+    for (int k = 0; k < n_desc; ++k) {
+        const crush_model_desc* d = descs[k];
+        const int nv = std::min(d->n_vehicles, 4);
+        n_veh += nv;
+        for (int v = 0; v < nv; ++v) n_vnodes += std::max<int64_t>(d->vehicles[v].n_nodes, 0);
+    }
+    // ---- room: allocate it (creating) or check it ----
+    Capacity need;
+    need.slots = S0 + n_desc;
+    need.nodes = N0 + N;
+    need.elems = E0 + E;
+    need.scalars = Q0 + Q;
+    need.parts = P0 + P;
+    need.contacts = K0 + K;
+    need.faces = tot.face;
+    need.slaves = tot.slave;
+    need.buckets = c->ca.n_buckets + tabs;
+    need.entries = c->n_entries + ents;
+    need.st_tabs = c->n_st_tabs + st_tabs;
+    need.st_ents = tot.ste;
+    need.cnodes = tot.cnode;
+    need.roles = tot.role;
+    need.vehicles = c->va.n_vehicles + n_veh;
+    need.vnodes = c->n_vnodes + n_vnodes;
+    if (creating) {
+        c->cap = capacity_for(reserve, need);
+    } else {
+        const Capacity& cp = c->cap;
+        const bool fits = need.slots <= cp.slots && need.nodes <= cp.nodes && need.elems <= cp.elems && need.scalars <= cp.scalars &&
+                          need.parts <= cp.parts &&
+                          need.contacts <= cp.contacts && need.faces <= cp.faces && need.slaves <= cp.slaves &&
+                          need.buckets <= cp.buckets && need.entries <= cp.entries && need.st_tabs <= cp.st_tabs &&
+                          need.st_ents <= cp.st_ents && need.cnodes <= cp.cnodes && need.roles <= cp.roles &&
+                          need.vehicles <= cp.vehicles && need.vnodes <= cp.vnodes;
+        if (!fits) return crush::fail(CRUSH_ERR_BUSY, "the models do not fit the context's reserved room");
+    }
+    const Capacity& cap = c->cap;
+    // ---- contact arrays of the new slots (global values) ----
+    std::vector<int> face_off(K + 1), slave_off(K + 1), tab_off(K + 1), counts_for_stop(K), contact_slot(K), slot_contact_off(n_desc + 1);
+    std::vector<long long> st_tab_off(K + 1), ent_off(K + 1);
+    std::vector<int> face_contact(tot.face - base[0].face), slave_contact(tot.slave - base[0].slave);
+    std::vector<uint32_t> faces(4 * (tot.face - base[0].face)), slaves(tot.slave - base[0].slave), dyn_faces(tot.dyn - base[0].dyn),
+        grid_faces(tot.grid - base[0].grid);
+    std::vector<double> scales(slaves.size()), stiff(K), md(K), cell(K), st_box(6 * (size_t)std::max(K, 1));
+    std::vector<uint8_t> is_static(K);
+    std::vector<uint32_t> st_off(tot.stoff - base[0].stoff);
+    std::vector<int> st_entries(tot.ste - base[0].ste);
+    std::vector<uint32_t> cnode(tot.cnode - base[0].cnode), cnode_off(tot.cnode - base[0].cnode + 1);
+    std::vector<int> crole_contact(tot.role - base[0].role), crole_slave(tot.role - base[0].role);
+    std::vector<uint32_t> slave_cn(slaves.size()), face_cn(faces.size());
+    face_off[0] = (int)base[0].face;
+    slave_off[0] = (int)base[0].slave;
+    tab_off[0] = (int)c->ca.n_buckets;
+    st_tab_off[0] = c->n_st_tabs;
+    ent_off[0] = c->n_entries;
+    for (int k = 0, q = 0; k < n_desc; ++k) {
+        const ContactPart& cp = parts[k];
+        slot_contact_off[k] = K0 + q;
+        for (size_t j = 0; j < cp.nf.size(); ++j, ++q) {
+            face_off[q + 1] = face_off[q] + cp.nf[j];
+            slave_off[q + 1] = slave_off[q] + cp.ns[j];
+            tab_off[q + 1] = tab_off[q] + cp.tab[j];
+            st_tab_off[q + 1] = st_tab_off[q] + cp.st[j];
+            ent_off[q + 1] = ent_off[q] + (cp.tab[j] > 0 ? (long long)cp.nf[j] * LEVEL_CELL_BUDGET : 0);
+            is_static[q] = cp.stat[j];
+            counts_for_stop[q] = cp.stop[j];
+            contact_slot[q] = S0 + k;
+            stiff[q] = cp.stiff[j];
+            md[q] = cp.md[j];
+            cell[q] = cp.cell[j];
+        }
+        slots[k].contact_dt = INF;
+    }
+    slot_contact_off[n_desc] = K0 + K;
+    cnode_off[0] = (uint32_t)base[0].role;
+    std::atomic<bool> cn_missing{false};
+    parallel_for(n_desc, [&](long long k) {
+        const ContactPart& cp = parts[k];
+        const Base& b = base[k];
+        const int q0 = slots[k].contact0 - K0;  // local contact index
+        const long long f0 = base[0].face, s0 = base[0].slave;
+        for (size_t j = 0; j < cp.nf.size(); ++j) {
+            std::fill(face_contact.begin() + (face_off[q0 + j] - f0), face_contact.begin() + (face_off[q0 + j + 1] - f0), (int)(K0 + q0 + j));
+            std::fill(slave_contact.begin() + (slave_off[q0 + j] - s0), slave_contact.begin() + (slave_off[q0 + j + 1] - s0),
+                      (int)(K0 + q0 + j));
+        }
+        std::copy(cp.faces.begin(), cp.faces.end(), faces.begin() + 4 * (b.face - f0));
+        std::copy(cp.slaves.begin(), cp.slaves.end(), slaves.begin() + (b.slave - s0));
+        std::copy(cp.scales.begin(), cp.scales.end(), scales.begin() + (b.slave - s0));
+        std::copy(cp.box.begin(), cp.box.end(), st_box.begin() + 6 * (size_t)q0);
+        for (size_t j = 0; j < cp.st_off.size(); ++j) st_off[b.stoff - base[0].stoff + j] = cp.st_off[j] + (uint32_t)b.ste;
+        std::copy(cp.st_entries.begin(), cp.st_entries.end(), st_entries.begin() + (b.ste - base[0].ste));
+        for (size_t j = 0; j < cp.dyn_faces.size(); ++j) dyn_faces[b.dyn - base[0].dyn + j] = cp.dyn_faces[j] + (uint32_t)b.face;
+        for (size_t j = 0; j < cp.grid_faces.size(); ++j) grid_faces[b.grid - base[0].grid + j] = cp.grid_faces[j] + (uint32_t)b.face;
+        std::copy(cp.cnode.begin(), cp.cnode.end(), cnode.begin() + (b.cnode - base[0].cnode));
+        for (size_t j = 1; j < cp.cnode_off.size(); ++j) cnode_off[b.cnode - base[0].cnode + j] = cp.cnode_off[j] + (uint32_t)b.role;
+        std::copy(cp.crole_contact.begin(), cp.crole_contact.end(), crole_contact.begin() + (b.role - base[0].role));
+        std::copy(cp.crole_slave.begin(), cp.crole_slave.end(), crole_slave.begin() + (b.role - base[0].role));
+        auto cn_of = [&](uint32_t node) {  // the slot's contact nodes are in ascending node order, and include it
+            const auto it = std::lower_bound(cp.cnode.begin(), cp.cnode.end(), node);
+            if (it == cp.cnode.end() || *it != node) {
+                cn_missing = true;  // cannot happen: every primary node and face corner has a role
+                return 0u;
+            }
+            return (uint32_t)(b.cnode + (it - cp.cnode.begin())) | (fixed_at(node) ? CN_FIXED : 0u);
+        };
+        for (size_t j = 0; j < cp.slaves.size(); ++j) slave_cn[b.slave - s0 + j] = cn_of(cp.slaves[j]);
+        for (size_t j = 0; j < cp.faces.size(); ++j) face_cn[4 * (b.face - f0) + j] = cn_of(cp.faces[j]);
+    });
+    if (cn_missing) return crush::fail(CRUSH_ERR_INVALID, "internal: a contact node without a role");
+    // exhaustive contacts (no grid) get a block each; the rest are listed by entry
+    std::vector<int> brute;
+    std::vector<uint32_t> gslaves, stslaves;
+    std::vector<uint8_t> is_brute(std::max(K, 1), 0);
+    int brute_max = c->ca.brute_max_faces;
+    for (int q = 0; q < K; ++q) {
+        const bool st_grid = st_tab_off[q + 1] > st_tab_off[q];
+        const bool grid = tab_off[q + 1] > tab_off[q] || st_grid;
+        if (!grid && face_off[q + 1] - face_off[q] <= 255 && slave_off[q + 1] > slave_off[q]) {
+            brute.push_back(K0 + q);
+            is_brute[q] = 1;
+            brute_max = std::max(brute_max, face_off[q + 1] - face_off[q]);
+        } else {
+            for (int e = slave_off[q]; e < slave_off[q + 1]; ++e) (st_grid ? stslaves : gslaves).push_back((uint32_t)e);
+        }
+    }
+    // ---- vehicles ----
+    std::vector<long long> voff;
+    std::vector<uint32_t> vnodes;
+    std::vector<int> vslot, vlocal;
+    long long max_vnodes = c->max_vnodes;
+    std::vector<uint32_t> crush_nodes_new;
+    std::vector<size_t> crush_off_new;
+    for (int k = 0; k < n_desc; ++k) {
+        const crush_model_desc* d = descs[k];
+        const long long n0 = slots[k].node0;
+        slots[k].vehicle0 = c->va.n_vehicles + (int)vslot.size();
+        const int nv = std::min(d->n_vehicles, 4);
+        slots[k].n_vehicles = nv;
+        for (int v = 0; v < nv; ++v) {
+            const crush_vehicle& vd = d->vehicles[v];
+            if (vd.n_nodes < 0 || (vd.n_nodes > 0 && !vd.nodes) || vd.n_front < 0 || (vd.n_front > 0 && !vd.front_nodes))
+                return crush::fail(CRUSH_ERR_INVALID, "invalid vehicle");
+            for (int64_t i = 0; i < vd.n_nodes; ++i) {
+                if (vd.nodes[i] >= (uint64_t)d->n_nodes) return crush::fail(CRUSH_ERR_INVALID, "vehicle node out of range");
+                vnodes.push_back((uint32_t)(n0 + vd.nodes[i]));
+            }
+            max_vnodes = std::max<long long>(max_vnodes, vd.n_nodes);
+            voff.push_back(c->n_vnodes + (long long)vnodes.size());
+            if (vd.accel_node >= (uint64_t)d->n_nodes) return crush::fail(CRUSH_ERR_INVALID, "accelerometer node out of range");
+            for (int64_t i = 0; i < vd.n_front; ++i) {
+                if (vd.front_nodes[i] >= (uint64_t)d->n_nodes) return crush::fail(CRUSH_ERR_INVALID, "front node out of range");
+                crush_nodes_new.push_back((uint32_t)(n0 + vd.front_nodes[i]));
+            }
+            crush_nodes_new.push_back((uint32_t)(n0 + vd.accel_node));
+            crush_off_new.push_back(crush_nodes_new.size());
+            vslot.push_back(S0 + k);
+            vlocal.push_back(v);
+        }
+    }
+    trace.mark("contacts and vehicles built");
+
+    // ---- device arrays: allocated with the room (creating), then the new ranges uploaded ----
+    Stager stager;
+    stager.init(c->stream, sizeof(double) * 6 * N + sizeof(uint32_t) * 27 * E);
+    c->stager = &stager;
+    struct StagerRelease {
+        crush_ctx* c;
+        Stager* s;
+        ~StagerRelease() {
+            s->release();
+            c->stager = nullptr;
+        }
+    } release_stager{c, &stager};
+    ContactArrays& ca = c->ca;
+    VehicleArrays& va = c->va;
+    if (creating) {
+        const long long NC = cap.nodes, EC = cap.elems;
+        c->stride = std::max<long long>(32, (EC + 31) / 32 * 32);
+        const long long QC = std::max<long long>(1, cap.scalars);
+        c->sc_stride = QC;
+        TRY(c->alloc(&c->pos, 3 * NC));
+        TRY(c->alloc(&c->conn_all, 8 * EC));
+        TRY(c->alloc(&c->part, EC));
+        TRY(c->alloc(&c->mat4, 4 * cap.parts));
+        TRY(c->alloc(&c->mats, cap.parts));
+        TRY(c->alloc(&c->hc_index_d, EC));
+        TRY(c->alloc(&c->sc_index_d, EC));
+        TRY(c->alloc(&c->sc_model_d, QC));
+        TRY(c->alloc(&c->sc_list_d, QC));
+        TRY(c->alloc(&c->sc_mat, 2 * QC));
+        TRY(c->alloc(&c->fixed, NC));
+        TRY(c->alloc(&c->node_slot, NC));
+        TRY(c->alloc(&c->elem_slot, EC));
+        for (uint32_t** p : {&c->all_off, &c->hc_off, &c->sc_off}) TRY(c->alloc(p, NC + 1));
+        for (uint32_t** p : {&c->all_slot, &c->hc_slot}) TRY(c->alloc(p, 8 * EC));
+        TRY(c->alloc(&c->sc_slot, 8 * QC));
+        {
+            uint32_t* ell = nullptr;
+            TRY(c->alloc(&ell, 8 * (size_t)NC));
+            c->hc_ell = reinterpret_cast<const uint4*>(ell);
+        }
+        for (double** p : {&c->v0, &c->u, &c->v, &c->v_half, &c->f_int, &c->f_ext, &c->f_ext_odd, &c->u_tmp, &c->f_tmp})
+            TRY(c->alloc(p, 3 * NC));
+        for (double** p : {&c->inv_mass, &c->mass, &c->added, &c->n_tmp, &c->n_tmp2}) TRY(c->alloc(p, NC));
+        for (double** p : {&c->volume, &c->dt_factor, &c->elem_mass, &c->elem_dt, &c->elem_extra, &c->e_tmp}) TRY(c->alloc(p, EC));
+        TRY(c->alloc(&c->lumped, 8 * EC));
+        TRY(c->alloc(&c->eroded_all, EC));
+        TRY(c->alloc(&c->planes, (size_t)N_STATIC_PLANES * c->stride));
+        TRY(c->alloc(&c->state, (size_t)N_STATE_PLANES * c->stride));
+        TRY(c->alloc(&c->corner, (size_t)24 * EC));
+        TRY(c->alloc(&c->sc_geo, (size_t)SC_PLANES * c->sc_stride));
+        TRY(c->alloc(&c->sc_corner, (size_t)24 * QC));
+        TRY(c->alloc(&c->ctls, cap.slots));
+        TRY(c->alloc(&c->ctls_aux, cap.slots));
+        TRY(c->alloc(&c->slot_done, cap.slots));
+        TRY(c->alloc(&c->mass_flag, 1));
+        TRY(c->alloc(&c->fused_counter, 1));
+        TRY(c->alloc(&c->forces_queue, 2));
+        TRY(c->alloc(&c->setup_bad, 1));
+        CK(cudaMemsetAsync(c->mass_flag, 0, sizeof(int), c->stream));
+        CK(cudaMemsetAsync(c->fused_counter, 0, sizeof(unsigned), c->stream));
+        CK(cudaMemsetAsync(c->forces_queue, 0, 2 * sizeof(unsigned), c->stream));
+        CK(cudaMemsetAsync(c->planes, 0, sizeof(float4) * N_STATIC_PLANES * c->stride, c->stream));
+        CK(cudaMemsetAsync(c->eroded_all, 0, EC, c->stream));
+        CK(cudaMemsetAsync(c->ctls, 0, sizeof(Control) * cap.slots, c->stream));
+        CK(cudaMemsetAsync(c->slot_done, 0, sizeof(int) * cap.slots, c->stream));
+        // contacts
+        const long long KC = std::max<long long>(cap.contacts, 1), FC = std::max<long long>(cap.faces, 1),
+                        SC = std::max<long long>(cap.slaves, 1), CNC = std::max<long long>(cap.cnodes, 1);
+        TRY(c->alloc(&c->face_off_d, KC + 1));
+        TRY(c->alloc(&c->slave_off_d, KC + 1));
+        TRY(c->alloc(&c->tab_off_d, KC + 1));
+        TRY(c->alloc(&c->st_tab_off_d, KC + 1));
+        TRY(c->alloc(&c->ent_off_d, KC + 1));
+        TRY(c->alloc(&c->faces_d, 4 * FC));
+        TRY(c->alloc(&ca.geo, FC));
+        TRY(c->alloc(&c->slaves_d, SC));
+        TRY(c->alloc(&c->scales_d, SC));
+        TRY(c->alloc(&ca.hit, SC));
+        TRY(c->alloc(&ca.hit_force, 3 * SC));
+        TRY(c->alloc(&ca.hit_sd, SC));
+        for (double** p : {&c->stiff_d, &c->md_d, &c->cell_d}) TRY(c->alloc(p, KC));
+        TRY(c->alloc(&c->st_box_d, 6 * KC));
+        TRY(c->alloc(&ca.counts, std::max<long long>(cap.buckets, 1)));
+        TRY(c->alloc(&ca.boff, std::max<long long>(cap.buckets, 1)));
+        TRY(c->alloc(&ca.blen, std::max<long long>(cap.buckets, 1)));
+        TRY(c->alloc(&ca.entries, std::max<long long>(cap.entries, 1)));
+        TRY(c->alloc(&c->grid_faces_d, FC));
+        TRY(c->alloc(&c->dyn_faces_d, FC));
+        TRY(c->alloc(&c->brute_d, KC));
+        TRY(c->alloc(&c->gslaves_d, SC));
+        TRY(c->alloc(&c->stslaves_d, SC));
+        TRY(c->alloc(&ca.grid_state, 2 * KC + 1));
+        TRY(c->alloc(&ca.cells, FC));
+        TRY(c->alloc(&ca.gather_work, CNC));
+        TRY(c->alloc(&ca.ev_pool_n, 2));
+        ca.big_cap = FC;
+        TRY(c->alloc(&ca.big_faces, (size_t)ca.big_cap));
+        TRY(c->alloc(&ca.big_box, 6 * (size_t)ca.big_cap));
+        TRY(c->alloc(&ca.big_best, SC));
+        TRY(c->alloc(&ca.search_stats, 3 * KC));
+        c->pen_stride = KC;
+        TRY(c->alloc(&ca.pen_count, 2 * (size_t)c->pen_stride));
+        TRY(c->alloc(&ca.pen_max_bits, 2 * (size_t)c->pen_stride));
+        TRY(c->alloc(&c->counts_for_stop_d, KC));
+        TRY(c->alloc(&c->cnode_d, CNC));
+        TRY(c->alloc(&c->cnode_off_d, CNC + 1));
+        TRY(c->alloc(&c->crole_contact_d, std::max<long long>(cap.roles, 1)));
+        TRY(c->alloc(&c->crole_slave_d, std::max<long long>(cap.roles, 1)));
+        TRY(c->alloc(&c->slave_cn_d, SC));
+        TRY(c->alloc(&c->face_cn_d, 4 * FC));
+        TRY(c->alloc(&ca.ev_count, CNC));
+        TRY(c->alloc(&ca.ev_list, EV_CAP * CNC));
+        ca.ev_pool_cap = std::max<long long>(4096, SC);
+        TRY(c->alloc(&ca.ev_pool, (size_t)ca.ev_pool_cap));
+        TRY(c->alloc(&c->face_contact_d, FC));
+        TRY(c->alloc(&c->slave_contact_d, SC));
+        TRY(c->alloc(&c->contact_slot_d, KC));
+        TRY(c->alloc(&c->slot_contact_off_d, cap.slots + 1));
+        TRY(c->alloc(&c->is_static_d, KC));
+        TRY(c->alloc(&c->st_off_d, std::max<long long>(cap.st_tabs + cap.contacts, 1)));
+        TRY(c->alloc(&c->st_entries_d, std::max<long long>(cap.st_ents, 1)));
+        ca.face_off = c->face_off_d;
+        ca.slave_off = c->slave_off_d;
+        ca.tab_off = c->tab_off_d;
+        ca.st_tab_off = c->st_tab_off_d;
+        ca.ent_off = c->ent_off_d;
+        ca.faces = c->faces_d;
+        ca.slaves = c->slaves_d;
+        ca.slave_scale = c->scales_d;
+        ca.stiffness = c->stiff_d;
+        ca.max_distance = c->md_d;
+        ca.cell = c->cell_d;
+        ca.st_box = c->st_box_d;
+        ca.grid_faces = c->grid_faces_d;
+        ca.dyn_faces = c->dyn_faces_d;
+        ca.brute_contacts = c->brute_d;
+        ca.grid_slaves = c->gslaves_d;
+        ca.st_slaves = c->stslaves_d;
+        ca.counts_for_stop = c->counts_for_stop_d;
+        ca.cnode = c->cnode_d;
+        ca.cnode_off = c->cnode_off_d;
+        ca.crole_contact = c->crole_contact_d;
+        ca.crole_slave = c->crole_slave_d;
+        ca.slave_cn = c->slave_cn_d;
+        ca.face_cn = c->face_cn_d;
+        ca.face_contact = c->face_contact_d;
+        ca.slave_contact = c->slave_contact_d;
+        ca.contact_slot = c->contact_slot_d;
+        ca.slot_contact_off = c->slot_contact_off_d;
+        ca.is_static = c->is_static_d;
+        ca.st_off = c->st_off_d;
+        ca.st_entries = c->st_entries_d;
+        ca.levels_used = ca.grid_state;
+        ca.ent_cursor = ca.grid_state + KC;
+        ca.big_count = ca.grid_state + 2 * KC;
+        ca.gather_count = ca.ev_pool_n + 1;
+        ca.exhaustive = 0;
+        CK(cudaMemsetAsync(ca.counts, 0, sizeof(int) * std::max<long long>(cap.buckets, 1), c->stream));
+        CK(cudaMemsetAsync(ca.blen, 0, sizeof(int) * std::max<long long>(cap.buckets, 1), c->stream));
+        CK(cudaMemsetAsync(ca.big_best, 0x7F, sizeof(int) * SC, c->stream));  // BIG_NONE
+        CK(cudaMemsetAsync(ca.grid_state, 0, sizeof(int) * (2 * KC + 1), c->stream));
+        CK(cudaMemsetAsync(ca.search_stats, 0, sizeof(unsigned long long) * 3 * KC, c->stream));
+        CK(cudaMemsetAsync(ca.pen_count, 0, sizeof(unsigned long long) * 2 * c->pen_stride, c->stream));
+        CK(cudaMemsetAsync(ca.pen_max_bits, 0, sizeof(unsigned long long) * 2 * c->pen_stride, c->stream));
+        CK(cudaMemsetAsync(ca.ev_count, 0, sizeof(int) * CNC, c->stream));
+        CK(cudaMemsetAsync(ca.ev_pool_n, 0, 2 * sizeof(int), c->stream));
+        // vehicles
+        TRY(c->alloc(&c->voff_d, std::max<long long>(cap.vehicles, 1) + 1));
+        TRY(c->alloc(&c->vnodes_d, std::max<long long>(cap.vnodes, 1)));
+        TRY(c->alloc(&c->vslot_d, std::max<long long>(cap.vehicles, 1)));
+        TRY(c->alloc(&c->vlocal_d, std::max<long long>(cap.vehicles, 1)));
+        TRY(c->alloc(&c->veh_out, 7 * std::max<long long>(cap.vehicles, 1)));
+        va.off = c->voff_d;
+        va.nodes = c->vnodes_d;
+        va.slot = c->vslot_d;
+        va.local = c->vlocal_d;
+        const long long zero = 0;
+        CK(cudaMemcpyAsync(c->voff_d, &zero, sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));  // the zero above is a stack value
+        // active chunk tables: every space's chunks at its full room
+        const long long sizes[ACTIVE_SPACES] = {EC, EC, NC, SC, CNC, FC, SC, SC, QC};
+        c->space_off_h.assign(ACTIVE_SPACES + 1, 0);
+        for (int sp = 0; sp < ACTIVE_SPACES; ++sp) c->space_off_h[sp + 1] = c->space_off_h[sp] + (sizes[sp] + CHUNK - 1) / CHUNK;
+        const long long nch = c->space_off_h[ACTIVE_SPACES];
+        c->chunk_lo_h.assign(nch, INT32_MAX);
+        c->chunk_hi_h.assign(nch, -1);
+        TRY(c->alloc(&c->chunk_lo_d, std::max<long long>(nch, 1)));
+        TRY(c->alloc(&c->chunk_hi_d, std::max<long long>(nch, 1)));
+        const long long* off_d = nullptr;
+        TRY(c->upload_const(&off_d, c->space_off_h));
+        c->ab.n_chunks = nch;
+        c->ab.chunk_lo = c->chunk_lo_d;
+        c->ab.chunk_hi = c->chunk_hi_d;
+        c->ab.space_off = off_d;
+        TRY(c->alloc(&c->ab.lists, std::max<long long>(nch, 1)));
+        TRY(c->alloc(&c->ab.counts, ACTIVE_SPACES));
+        c->adaptive = adaptive;
+        c->check_steps = check_steps;
+        trace.mark("allocations");
+    }
+    c->any_separation = any_sep;
+    // uploads of the new ranges
+    auto put = [&](auto* dst, const auto* src, size_t count) -> int {
+        if (!count) return CRUSH_OK;
+        return stager_copy(&stager, dst, src, count * sizeof(*src));
+    };
+    TRY(put(c->pos + 3 * N0, cm.positions.data(), 3 * N));
+    TRY(put(c->v0 + 3 * N0, cm.v0.data(), 3 * N));
+    TRY(put(c->conn_all + 8 * E0, cm.hexes.data(), 8 * E));
+    TRY(put(c->part + E0, cm.hex_part.data(), E));
+    TRY(put(c->mat4 + 4 * P0, cm.mat4.data(), cm.mat4.size()));
+    TRY(put(c->mats + P0, cm.mats.data(), cm.mats.size()));
+    TRY(put(c->hc_index_d + E0, hc_index.data(), E));
+    TRY(put(c->sc_index_d + E0, sc_index.data(), E));
+    TRY(put(c->sc_model_d + Q0, sc_model.data(), Q));
+    TRY(put(c->sc_list_d + QF0, sc_list.data(), QF));
+    TRY(put(c->sc_mat + 2 * Q0, sc_mat.data(), 2 * Q));
+    TRY(put(c->fixed + N0, cm.fixed.data(), N));
+    TRY(put(c->node_slot + N0, cm.node_slot.data(), N));
+    TRY(put(c->elem_slot + E0, cm.elem_slot.data(), E));
+    TRY(put(c->all_off + N0, all_off.data(), N + 1));
+    TRY(put(c->hc_off + N0, hc_off.data(), N + 1));
+    TRY(put(c->sc_off + N0, sc_off.data(), N + 1));
+    TRY(put(c->all_slot + 8 * E0, all_slot.data(), 8 * E));
+    TRY(put(c->hc_slot + 8 * H0, hc_slot.data(), 8 * H));
+    TRY(put(c->sc_slot + 8 * Q0, sc_slot.data(), 8 * Q));
+    TRY(put(const_cast<uint32_t*>(reinterpret_cast<const uint32_t*>(c->hc_ell)) + 8 * N0, hc_ell.data(), 8 * (size_t)N));
+    CK(cudaMemsetAsync(c->eroded_all + E0, 0, E, c->stream));
+    trace.mark("model uploads");
+    const long long FB = base[0].face, SB = base[0].slave;
+    TRY(put(c->face_off_d + K0, face_off.data(), K + 1));
+    TRY(put(c->slave_off_d + K0, slave_off.data(), K + 1));
+    TRY(put(c->tab_off_d + K0, tab_off.data(), K + 1));
+    TRY(put(c->st_tab_off_d + K0, st_tab_off.data(), K + 1));
+    TRY(put(c->ent_off_d + K0, ent_off.data(), K + 1));
+    TRY(put(c->faces_d + 4 * FB, faces.data(), faces.size()));
+    TRY(put(c->slaves_d + SB, slaves.data(), slaves.size()));
+    TRY(put(c->scales_d + SB, scales.data(), scales.size()));
+    TRY(put(c->stiff_d + K0, stiff.data(), K));
+    TRY(put(c->md_d + K0, md.data(), K));
+    TRY(put(c->cell_d + K0, cell.data(), K));
+    TRY(put(c->st_box_d + 6 * K0, st_box.data(), 6 * (size_t)K));
+    TRY(put(c->grid_faces_d + base[0].grid, grid_faces.data(), grid_faces.size()));
+    TRY(put(c->dyn_faces_d + base[0].dyn, dyn_faces.data(), dyn_faces.size()));
+    TRY(put(c->brute_d + ca.n_brute, brute.data(), brute.size()));
+    TRY(put(c->gslaves_d + ca.n_grid_slaves, gslaves.data(), gslaves.size()));
+    TRY(put(c->stslaves_d + ca.n_st_slaves, stslaves.data(), stslaves.size()));
+    TRY(put(c->counts_for_stop_d + K0, counts_for_stop.data(), K));
+    TRY(put(c->cnode_d + base[0].cnode, cnode.data(), cnode.size()));
+    TRY(put(c->cnode_off_d + base[0].cnode, cnode_off.data(), cnode_off.size()));
+    TRY(put(c->crole_contact_d + base[0].role, crole_contact.data(), crole_contact.size()));
+    TRY(put(c->crole_slave_d + base[0].role, crole_slave.data(), crole_slave.size()));
+    TRY(put(c->slave_cn_d + SB, slave_cn.data(), slave_cn.size()));
+    TRY(put(c->face_cn_d + 4 * FB, face_cn.data(), face_cn.size()));
+    TRY(put(c->face_contact_d + FB, face_contact.data(), face_contact.size()));
+    TRY(put(c->slave_contact_d + SB, slave_contact.data(), slave_contact.size()));
+    TRY(put(c->contact_slot_d + K0, contact_slot.data(), K));
+    TRY(put(c->slot_contact_off_d + S0, slot_contact_off.data(), n_desc + 1));
+    TRY(put(c->is_static_d + K0, is_static.data(), K));
+    TRY(put(c->st_off_d + base[0].stoff, st_off.data(), st_off.size()));
+    TRY(put(c->st_entries_d + base[0].ste, st_entries.data(), st_entries.size()));
+    TRY(put(c->vnodes_d + c->n_vnodes, vnodes.data(), vnodes.size()));
+    TRY(put(c->voff_d + 1 + va.n_vehicles, voff.data(), voff.size()));
+    TRY(put(c->vslot_d + va.n_vehicles, vslot.data(), vslot.size()));
+    TRY(put(c->vlocal_d + va.n_vehicles, vlocal.data(), vlocal.size()));
+    trace.mark("contact uploads");
+
+    // ---- the context's counts and host copies take the new slots ----
+    c->slots.insert(c->slots.end(), slots.begin(), slots.end());
+    c->n_slots = S0 + n_desc;
+    c->n_nodes = N0 + N;
+    c->n_all = E0 + E;
+    c->n_hc = H0 + H;
+    c->n_sc = Q0 + Q;
+    c->n_sc_free = QF0 + QF;
+    c->n_parts = P0 + P;
+    c->hc_index.insert(c->hc_index.end(), hc_index.begin(), hc_index.end());
+    c->hc_model.insert(c->hc_model.end(), hc_model.begin(), hc_model.end());
+    c->sc_model.insert(c->sc_model.end(), sc_model.begin(), sc_model.end());
+    c->n_contacts = K0 + K;
+    c->n_faces = tot.face;
+    c->n_slaves = tot.slave;
+    c->n_st_ents = tot.ste;
+    c->n_st_offs = tot.stoff;
+    c->n_st_tabs = st_tab_off[K];
+    c->n_entries = ent_off[K];
+    c->n_roles = tot.role;
+    if (creating) {
+        c->face_off_h.assign(face_off.begin(), face_off.end());
+        c->slave_off_h.assign(slave_off.begin(), slave_off.end());
+        c->tab_off_h.assign(tab_off.begin(), tab_off.end());
+    } else {
+        c->face_off_h.insert(c->face_off_h.end(), face_off.begin() + 1, face_off.end());
+        c->slave_off_h.insert(c->slave_off_h.end(), slave_off.begin() + 1, slave_off.end());
+        c->tab_off_h.insert(c->tab_off_h.end(), tab_off.begin() + 1, tab_off.end());
+    }
+    c->is_static_h.insert(c->is_static_h.end(), is_static.begin(), is_static.begin() + K);
+    c->is_brute_h.resize(std::max(K0 + K, 1), 0);
+    for (int q = 0; q < K; ++q) c->is_brute_h[K0 + q] = is_brute[q];
+    c->grid_slaves_h.insert(c->grid_slaves_h.end(), gslaves.begin(), gslaves.end());
+    c->st_slaves_h.insert(c->st_slaves_h.end(), stslaves.begin(), stslaves.end());
+    ca.n_contacts = c->n_contacts;
+    ca.n_slots = c->n_slots;
+    ca.n_buckets = tab_off[K];
+    ca.n_grid_faces = tot.grid;
+    ca.n_dyn_faces = tot.dyn;
+    ca.n_cnodes = tot.cnode;
+    ca.n_brute += (int)brute.size();
+    ca.brute_max_faces = std::max(brute_max, 1);
+    ca.n_grid_slaves = (long long)c->grid_slaves_h.size();
+    ca.n_st_slaves = (long long)c->st_slaves_h.size();
+    ca.is_brute_h = c->is_brute_h.data();
+    va.n_vehicles += (int)vslot.size();
+    c->n_vnodes += (long long)vnodes.size();
+    c->max_vnodes = max_vnodes;
+    va.vx_blocks = (int)std::min<long long>(VX_BLOCKS, std::max<long long>(1, (max_vnodes + 2047) / 2048));
+    for (size_t i = 0; i < crush_off_new.size(); ++i) c->crush_off_h.push_back(c->crush_nodes_h.size() + crush_off_new[i]);
+    c->crush_nodes_h.insert(c->crush_nodes_h.end(), crush_nodes_new.begin(), crush_nodes_new.end());
+    // the crush-measure node list is small: a new copy of the whole list
+    TRY(c->upload(&c->crush_nodes, c->crush_nodes_h.data(), c->crush_nodes_h.size()));
+    TRY(c->alloc(&c->crush_ux, std::max<size_t>(c->crush_nodes_h.size(), 1)));
+    // ---- active chunk tables: the slot range of every chunk the new entities touch ----
+    {
+        const long long ends[ACTIVE_SPACES] = {c->n_hc, c->n_all, c->n_nodes, ca.n_grid_slaves, ca.n_cnodes, ca.n_dyn_faces,
+                                               c->n_slaves, ca.n_st_slaves, c->n_sc_free};
+        const long long begins[ACTIVE_SPACES] = {H0, E0, N0, ca.n_grid_slaves - (long long)gslaves.size(), base[0].cnode, base[0].dyn,
+                                                 SB, ca.n_st_slaves - (long long)stslaves.size(), QF0};
+        auto slot_of = [&](int sp, long long i) -> int {
+            switch (sp) {
+                case 0: return (int)cm.elem_slot[hc_model[i - H0] - E0];
+                case 1: return (int)cm.elem_slot[i - E0];
+                case 2: return (int)cm.node_slot[i - N0];
+                case 3: return contact_slot[slave_contact[gslaves[i - begins[3]] - SB] - K0];
+                case 4: return (int)cm.node_slot[cnode[i - base[0].cnode] - N0];
+                case 5: return contact_slot[face_contact[dyn_faces[i - base[0].dyn] - FB] - K0];
+                case 6: return contact_slot[slave_contact[i - SB] - K0];
+                case 7: return contact_slot[slave_contact[stslaves[i - begins[7]] - SB] - K0];
+                default: return (int)cm.elem_slot[sc_model[sc_list[i - QF0] - Q0] - E0];
+            }
+        };
+        for (int sp = 0; sp < ACTIVE_SPACES; ++sp) {
+            if (ends[sp] <= begins[sp]) continue;
+            const long long q0 = c->space_off_h[sp] + begins[sp] / CHUNK, q1 = c->space_off_h[sp] + (ends[sp] - 1) / CHUNK;
+            parallel_for(q1 - q0 + 1, [&](long long j) {
+                const long long q = q0 + j;
+                const long long i0 = std::max(begins[sp], (q - c->space_off_h[sp]) * CHUNK);
+                const long long i1 = std::min(ends[sp], (q - c->space_off_h[sp] + 1) * CHUNK);
+                int a = c->chunk_lo_h[q], b = c->chunk_hi_h[q];
+                for (long long i = i0; i < i1; ++i) {
+                    const int sl = slot_of(sp, i);
+                    a = std::min(a, sl);
+                    b = std::max(b, sl);
+                }
+                c->chunk_lo_h[q] = a;
+                c->chunk_hi_h[q] = b;
+            });
+            TRY(put(c->chunk_lo_d + q0, c->chunk_lo_h.data() + q0, q1 - q0 + 1));
+            TRY(put(c->chunk_hi_d + q0, c->chunk_hi_h.data() + q0, q1 - q0 + 1));
+        }
+    }
+    trace.mark("active chunk tables");
+
+    // ---- device set-up of the new elements and nodes ----
+    CK(cudaMemsetAsync(c->setup_bad, 0, sizeof(int), c->stream));
+    launch_setup_geometry(c->stream, E0, E0 + E, c->pos, c->conn_all, c->part, c->mat4, c->hc_index_d, c->elem_slot, c->stride, c->planes,
+                          c->volume, c->lumped, c->dt_factor, c->elem_mass, c->setup_bad, c->sc_index_d, c->sc_stride, c->sc_geo);
+    TRY(check_launch(c));
+    launch_node_masses(c->stream, N, c->all_off + N0, c->all_slot, c->lumped, c->mass + N0, c->inv_mass + N0);
+    TRY(check_launch(c));
+    launch_init_state(c->stream, H0, H0 + H, c->stride, c->state);
+    TRY(check_launch(c));
+    // contact_dt over every listed node of the slot's contacts (src/solver.rs:217-223)
+    std::vector<double> mass_h(N);
+    int bad_h = 0;
+    CK(cudaMemcpyAsync(&bad_h, c->setup_bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(mass_h.data(), c->mass + N0, N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    // the stable step of every new slot at u = 0, through the drop-in control blocks
+    CK(cudaMemsetAsync(c->u_tmp + 3 * N0, 0, sizeof(double) * 3 * N, c->stream));
+    std::vector<Control> aux(n_desc);
+    std::memset(aux.data(), 0, sizeof(Control) * aux.size());
+    for (Control& a : aux) a.dt_stable_bits = INF_BITS;
+    CK(cudaMemcpyAsync(c->ctls_aux + S0, aux.data(), sizeof(Control) * aux.size(), cudaMemcpyHostToDevice, c->stream));
+    launch_elem_dt(c->stream, c->el(), c->nd(), c->ctls_aux, c->u_tmp, 0, E0);
+    TRY(check_launch(c));
+    CK(cudaMemcpyAsync(aux.data(), c->ctls_aux + S0, sizeof(Control) * aux.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (bad_h == 1) return crush::fail(CRUSH_ERR_INVALID, "degenerate hexahedron (singular Jacobian)");
+    if (bad_h == 2) return crush::fail(CRUSH_ERR_INVALID, "hourglass modes not independent");
+    parallel_for(n_desc, [&](long long k) {
+        const crush_model_desc* d = descs[k];
+        Slot& sl = c->slots[S0 + k];
+        double cdt = INF;
+        for (int q = 0; q < d->n_contacts; ++q) {
+            const crush_contact& cd = d->contacts[q];
+            if (!(cd.stiffness > 0.0)) continue;
+            for (int64_t i = 0; i < cd.n_nodes; ++i) {
+                const double m = mass_h[sl.node0 - N0 + cd.nodes[i]];
+                if (m > 0.0) cdt = std::fmin(cdt, 2.0 * std::sqrt(m / cd.stiffness));
+            }
+        }
+        sl.contact_dt = cdt;
+        double stable;
+        std::memcpy(&stable, &aux[k].dt_stable_bits, sizeof(double));
+        if (!std::isfinite(stable)) {
+            static const int EDGES[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6}, {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+            double mn = INF, cmax = 0.0;
+            for (long long e = sl.elem0; e < sl.elem0 + sl.n_elems; ++e) {
+                cmax = std::fmax(cmax, wave_speed(mat_of(e)));
+                for (auto& ed : EDGES) {
+                    const double* p = &cm.positions[3 * (size_t)(hex(e, ed[0]) - N0)];
+                    const double* q = &cm.positions[3 * (size_t)(hex(e, ed[1]) - N0)];
+                    mn = std::fmin(mn, std::sqrt((p[0] - q[0]) * (p[0] - q[0]) + (p[1] - q[1]) * (p[1] - q[1]) + (p[2] - q[2]) * (p[2] - q[2])));
+                }
+            }
+            stable = mn / (std::sqrt(3.0) * cmax);
+        }
+        sl.stable = std::fmin(stable, sl.contact_dt);
+        sl.dt_floor = sl.settings.mass_scaling > 0.0 ? sl.settings.mass_scaling * sl.stable : 0.0;
+        sl.dt0 = sl.settings.time_step > 0.0 ? sl.settings.time_step : sl.stable * sl.settings.dt_scale;
+    });
+    trace.mark("initial stable step");
+    if (creating) {
+        c->period = std::lcm(c->check_steps, 20);
+        if (c->period > 200) c->period = 0;  // no graph for odd periods
+        c->base_period = c->period;
+    }
+    drop_graphs(c);
+    if (c->run_open) return begin_slots(c, S0, c->n_slots);
+    return CRUSH_OK;
+#undef TRY
+}
+
+int create_impl(const crush_model_desc* const* descs, int n_desc, int device, crush_ctx* c, const crush_capacity* room = nullptr) {
+    if (n_desc <= 0 || !descs) return crush::fail(CRUSH_ERR_INVALID, "no models");
     c->device = device;
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
@@ -946,615 +1830,7 @@ int create_impl(const crush_model_desc* const* descs, int n_desc, int device, cr
         CK(cudaEventCreateWithFlags(&c->ev_gathered, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&c->ev_static, cudaEventDisableTiming));
     }
-    c->n_slots = n_desc;
-    c->slots.resize(n_desc);
-    // ---- sizes and offsets of every slot ----
-    long long N = 0, E = 0;
-    int P = 0, K = 0;
-    std::vector<int> part0(n_desc);
-    for (int k = 0; k < n_desc; ++k) {
-        const crush_model_desc* d = descs[k];
-        int st0 = check_desc(d);
-        if (st0 != CRUSH_OK) return st0;
-        Slot& sl = c->slots[k];
-        sl.settings = d->settings;
-        sl.node0 = N;
-        sl.n_nodes = d->n_nodes;
-        sl.elem0 = E;
-        sl.n_elems = d->n_hexes;
-        sl.contact0 = K;
-        sl.n_contacts = d->n_contacts;
-        part0[k] = P;
-        sl.part0 = P;
-        sl.n_parts = d->n_parts;
-        N += d->n_nodes;
-        E += d->n_hexes;
-        P += d->n_parts;
-        K += d->n_contacts;
-        if (N >= (1ll << 31) || E >= (1ll << 28)) return crush::fail(CRUSH_ERR_INVALID, "models too large for one context");
-    }
-    // The step schedule is shared: every slot must re-check its stable step
-    // on the same cadence.
-    {
-        const crush_settings& s0 = descs[0]->settings;
-        c->adaptive = !(s0.time_step > 0.0) && s0.adaptive_check_steps > 0;
-        c->check_steps = s0.adaptive_check_steps > 0 ? s0.adaptive_check_steps : 1;
-        for (int k = 0; k < n_desc; ++k) {
-            const crush_settings& s = descs[k]->settings;
-            bool ad = !(s.time_step > 0.0) && s.adaptive_check_steps > 0;
-            if (ad != c->adaptive || (ad && s.adaptive_check_steps != c->check_steps))
-                return crush::fail(CRUSH_ERR_UNSUPPORTED, "models of one context must share adaptive_check_steps and time-step mode");
-            if (s.stop_rule == CRUSH_STOP_SEPARATION) c->any_separation = true;
-        }
-    }
-    Combined cm;
-    cm.positions.alloc(3 * N);
-    cm.v0.alloc(3 * N);
-    cm.fixed.alloc(N);
-    cm.node_slot.alloc(N);
-    cm.hexes.alloc(8 * E);
-    cm.hex_part.alloc(E);
-    cm.elem_slot.alloc(E);
-    cm.mats.resize(P);
-    cm.materials.resize(P);
-    cm.mat4.resize(4 * (size_t)P);
-    std::vector<SlotError> errs(n_desc);
-    std::vector<long long> slot_hc(n_desc, 0);
-    parallel_for(n_desc, [&](long long k) { fill_slot(descs[k], (int)k, c->slots[k], part0[k], cm, &slot_hc[k], errs[k]); });
-    for (auto& e : errs)
-        if (e.code != CRUSH_OK) return crush::fail(e.code, e.msg);
-    trace.mark("validate + concatenate");
-    c->n_nodes = N;
-    c->n_all = E;
-    // Honeycomb numbering (element order) and the node incidence CSRs, per
-    // slot in parallel: a slot's nodes are touched only by its own elements.
-    std::vector<long long> hc0(n_desc + 1, 0);
-    for (int k = 0; k < n_desc; ++k) hc0[k + 1] = hc0[k] + slot_hc[k];
-    // Elastic elements with a free node per slot (they are numbered first,
-    // slot after slot, then the all-fixed ones).
-    std::vector<long long> slot_free(n_desc, 0);
-    parallel_for(n_desc, [&](long long k) {
-        const Slot& sl = c->slots[k];
-        long long nf = 0;
-        for (long long e = sl.elem0; e < sl.elem0 + sl.n_elems; ++e) {
-            if (cm.materials[cm.hex_part[e]].model == CRUSH_MAT_HONEYCOMB) continue;
-            bool all_fixed = true;
-            for (int i = 0; i < 8; ++i) all_fixed = all_fixed && cm.fixed[cm.hexes[8 * e + i]] != 0;
-            nf += all_fixed ? 0 : 1;
-        }
-        slot_free[k] = nf;
-    });
-    std::vector<long long> free0(n_desc + 1, 0), fixed0(n_desc + 1, 0);
-    for (int k = 0; k < n_desc; ++k) {
-        free0[k + 1] = free0[k] + slot_free[k];
-        fixed0[k + 1] = fixed0[k] + (c->slots[k].n_elems - slot_hc[k] - slot_free[k]);
-    }
-    c->n_sc_free = free0[n_desc];
-    c->n_hc = hc0[n_desc];
-    // Incidence entries are 32-bit (8 e + corner); the padded rows reserve
-    // the two largest values as markers.
-    if (8 * (unsigned long long)E >= (unsigned long long)HC_ELL_MORE)
-        return crush::fail(CRUSH_ERR_INVALID, "too many hexahedra for 32-bit node incidence entries (8 x elements must stay below 2^32 - 2)");
-    c->stride = std::max<long long>(32, (c->n_hc + 31) / 32 * 32);
-    c->n_sc = E - c->n_hc;
-    c->hc_index.resize(E);
-    c->hc_model.resize(c->n_hc);
-    c->sc_model.resize(c->n_sc);
-    std::vector<int64_t> sc_index(E);
-    Buf<uint32_t> all_off, hc_off, all_slot, hc_slot, sc_off, sc_slot;
-    all_off.alloc(N + 1);
-    hc_off.alloc(N + 1);
-    sc_off.alloc(N + 1);
-    all_slot.alloc(8 * E);
-    hc_slot.alloc(8 * c->n_hc);
-    Buf<uint32_t> hc_ell;
-    hc_ell.alloc(8 * (size_t)N);
-    sc_slot.alloc(8 * c->n_sc);
-    parallel_for(n_desc, [&](long long k) {
-        const Slot& sl = c->slots[k];
-        const long long n0 = sl.node0, e0 = sl.elem0, nn = sl.n_nodes;
-        long long h = hc0[k], qf = free0[k], qx = free0[n_desc] + fixed0[k];
-        const long long q0 = e0 - hc0[k];  // the slot's first scalar CSR entry / 8
-        for (long long e = e0; e < e0 + sl.n_elems; ++e)
-            if (cm.materials[cm.hex_part[e]].model == CRUSH_MAT_HONEYCOMB) {
-                c->hc_index[e] = h;
-                c->hc_model[h++] = (uint32_t)e;
-                sc_index[e] = -1;
-            } else {
-                c->hc_index[e] = -1;
-                bool all_fixed = true;
-                for (int i = 0; i < 8; ++i) all_fixed = all_fixed && cm.fixed[cm.hexes[8 * e + i]] != 0;
-                const long long q = all_fixed ? qx++ : qf++;
-                sc_index[e] = q;
-                c->sc_model[q] = (uint32_t)e;
-            }
-        // per-node counts, then offsets from the slot's first entry (a slot
-        // writes only off[n0, n0 + nn))
-        std::vector<uint32_t> cnt_a(nn, 0), cnt_b(nn, 0), cnt_c(nn, 0);
-        for (long long e = e0; e < e0 + sl.n_elems; ++e) {
-            const bool honey = c->hc_index[e] >= 0;
-            for (int i = 0; i < 8; ++i) {
-                const uint32_t n = cm.hexes[8 * e + i];
-                cnt_a[n - n0]++;
-                if (honey) cnt_b[n - n0]++;
-                else cnt_c[n - n0]++;
-            }
-        }
-        uint32_t a = (uint32_t)(8 * e0), b = (uint32_t)(8 * hc0[k]), cc = (uint32_t)(8 * q0);
-        for (long long n = n0; n < n0 + nn; ++n) {
-            all_off[n] = a;
-            hc_off[n] = b;
-            sc_off[n] = cc;
-            a += cnt_a[n - n0];
-            b += cnt_b[n - n0];
-            cc += cnt_c[n - n0];
-        }
-        std::vector<uint32_t> cura(all_off.data() + n0, all_off.data() + n0 + nn), curb(hc_off.data() + n0, hc_off.data() + n0 + nn),
-            curc(sc_off.data() + n0, sc_off.data() + n0 + nn);
-        for (long long e = e0; e < e0 + sl.n_elems; ++e) {
-            const long long he = c->hc_index[e], se = sc_index[e];
-            for (int i = 0; i < 8; ++i) {
-                const uint32_t n = cm.hexes[8 * e + i];
-                all_slot[cura[n - n0]++] = (uint32_t)(8 * e + i);
-                if (he >= 0) hc_slot[curb[n - n0]++] = (uint32_t)(8 * he + i);
-                else sc_slot[curc[n - n0]++] = (uint32_t)(8 * se + i);
-            }
-        }
-        // the same honeycomb slots as padded rows of 8 (HC_ELL_MORE: the CSR)
-        for (long long n = n0; n < n0 + nn; ++n) {
-            uint32_t* row = &hc_ell[8 * (size_t)n];
-            const uint32_t m = cnt_b[n - n0];
-            for (int j = 0; j < 8; ++j) row[j] = (uint32_t)j < m ? hc_slot[hc_off[n] + j] : HC_ELL_NONE;
-            if (m > 8) row[0] = HC_ELL_MORE;
-        }
-    });
-    all_off[N] = (uint32_t)(8 * E);
-    hc_off[N] = (uint32_t)(8 * c->n_hc);
-    sc_off[N] = (uint32_t)(8 * c->n_sc);
-    std::vector<double> sc_mat(2 * (size_t)std::max<long long>(c->n_sc, 1), 0.0);
-    for (long long q = 0; q < c->n_sc; ++q) {
-        const crush_material& m = cm.materials[cm.hex_part[c->sc_model[q]]];
-        sc_mat[2 * q] = m.youngs_modulus;
-        sc_mat[2 * q + 1] = m.poisson_ratio;
-    }
-    trace.mark("node incidence CSR");
-
-    int st;
-#define TRY(x) do { st = (x); if (st != CRUSH_OK) return st; } while (0)
-    Stager stager;
-    stager.init(c->stream, sizeof(double) * 6 * N + sizeof(uint32_t) * 27 * E);
-    c->stager = &stager;
-    trace.mark("pinned staging buffers");
-    TRY(c->upload(&c->pos, cm.positions.data(), 3 * N));
-    TRY(c->upload(&c->conn_all, cm.hexes.data(), 8 * E));
-    TRY(c->upload(&c->part, cm.hex_part.data(), E));
-    TRY(c->upload(&c->mat4, cm.mat4.data(), cm.mat4.size()));
-    TRY(c->upload(&c->mats, cm.mats.data(), cm.mats.size()));
-    TRY(c->upload(&c->hc_index_d, c->hc_index.data(), E));
-    TRY(c->upload(&c->fixed, cm.fixed.data(), N));
-    TRY(c->upload(&c->node_slot, cm.node_slot.data(), N));
-    TRY(c->upload(&c->elem_slot, cm.elem_slot.data(), E));
-    TRY(c->upload(&c->all_off, all_off.data(), N + 1));
-    TRY(c->upload(&c->all_slot, all_slot.data(), all_slot.size()));
-    TRY(c->upload(&c->hc_off, hc_off.data(), N + 1));
-    TRY(c->upload(&c->hc_slot, hc_slot.data(), hc_slot.size()));
-    {
-        uint32_t* ell = nullptr;
-        TRY(c->upload(&ell, hc_ell.data(), 8 * (size_t)N));
-        c->hc_ell = reinterpret_cast<const uint4*>(ell);
-    }
-    if (c->n_sc > 0) {
-        TRY(c->upload(&c->sc_index_d, sc_index.data(), E));
-        TRY(c->upload(&c->sc_model_d, c->sc_model.data(), c->n_sc));
-        TRY(c->upload(&c->sc_off, sc_off.data(), N + 1));
-        TRY(c->upload(&c->sc_slot, sc_slot.data(), sc_slot.size()));
-        TRY(c->upload(&c->sc_mat, sc_mat.data(), sc_mat.size()));
-        TRY(c->alloc(&c->sc_geo, (size_t)SC_PLANES * c->n_sc));
-        TRY(c->alloc(&c->sc_corner, (size_t)24 * c->n_sc));
-    }
-    TRY(c->upload(&c->v0, cm.v0.data(), 3 * N));
-    trace.mark("model uploads");
-    for (double** p : {&c->u, &c->v, &c->v_half, &c->f_int, &c->f_ext, &c->f_ext_odd, &c->u_tmp, &c->f_tmp}) TRY(c->alloc(p, 3 * N));
-    for (double** p : {&c->inv_mass, &c->mass, &c->added, &c->n_tmp, &c->n_tmp2}) TRY(c->alloc(p, N));
-    for (double** p : {&c->volume, &c->dt_factor, &c->elem_mass, &c->elem_dt, &c->elem_extra, &c->e_tmp}) TRY(c->alloc(p, E));
-    TRY(c->alloc(&c->lumped, 8 * E));
-    TRY(c->alloc(&c->eroded_all, E));
-    TRY(c->alloc(&c->planes, (size_t)N_STATIC_PLANES * c->stride));
-    TRY(c->alloc(&c->state, (size_t)N_STATE_PLANES * c->stride));
-    TRY(c->alloc(&c->corner, (size_t)24 * std::max<long long>(c->n_hc, 1)));
-    TRY(c->alloc(&c->ctls, c->n_slots));
-    TRY(c->alloc(&c->ctls_aux, c->n_slots));
-    TRY(c->alloc(&c->slot_done, c->n_slots));
-    TRY(c->alloc(&c->mass_flag, 1));
-    CK(cudaMemsetAsync(c->mass_flag, 0, sizeof(int), c->stream));
-    TRY(c->alloc(&c->fused_counter, 1));
-    CK(cudaMemsetAsync(c->fused_counter, 0, sizeof(unsigned), c->stream));
-    TRY(c->alloc(&c->forces_queue, 2));
-    CK(cudaMemsetAsync(c->forces_queue, 0, 2 * sizeof(unsigned), c->stream));
-    CK(cudaMemsetAsync(c->planes, 0, sizeof(float4) * N_STATIC_PLANES * c->stride, c->stream));
-    CK(cudaMemsetAsync(c->eroded_all, 0, E, c->stream));
-    CK(cudaMemsetAsync(c->ctls, 0, sizeof(Control) * c->n_slots, c->stream));
-    trace.mark("uploads + allocations");
-
-    // Device set-up geometry (HexGeometry::new for every element).
-    int* bad = nullptr;
-    TRY(c->alloc(&bad, 1));
-    CK(cudaMemsetAsync(bad, 0, sizeof(int), c->stream));
-    launch_setup_geometry(c->stream, E, c->pos, c->conn_all, c->part, c->mat4, c->hc_index_d, c->elem_slot, c->stride, c->planes,
-                          c->volume, c->lumped, c->dt_factor, c->elem_mass, bad, c->sc_index_d, c->n_sc, c->sc_geo);
-    TRY(check_launch(c));
-    launch_node_masses(c->stream, N, c->all_off, c->all_slot, c->lumped, c->mass, c->inv_mass);
-    TRY(check_launch(c));
-    trace.mark("device geometry launched");
-
-    // ---- contacts: per slot in parallel (overlapping the device set-up), then concatenated ----
-    std::vector<ContactPart> parts(n_desc);
-    parallel_for(n_desc, [&](long long k) { build_contacts(descs[k], c->slots[k], cm, parts[k], errs[k]); });
-    for (auto& e : errs)
-        if (e.code != CRUSH_OK) return crush::fail(e.code, e.msg);
-    int bad_h = 0;
-    CK(cudaMemcpyAsync(&bad_h, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    std::vector<double> mass_h(N);
-    CK(cudaMemcpyAsync(mass_h.data(), c->mass, N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    if (bad_h == 1) return crush::fail(CRUSH_ERR_INVALID, "degenerate hexahedron (singular Jacobian)");
-    if (bad_h == 2) return crush::fail(CRUSH_ERR_INVALID, "hourglass modes not independent");
-    // contact_dt over every listed node of the slot's contacts (src/solver.rs:217-223)
-    parallel_for(n_desc, [&](long long k) {
-        const crush_model_desc* d = descs[k];
-        double cdt = INF;
-        for (int q = 0; q < d->n_contacts; ++q) {
-            const crush_contact& cd = d->contacts[q];
-            if (!(cd.stiffness > 0.0)) continue;
-            for (int64_t i = 0; i < cd.n_nodes; ++i) {
-                const double m = mass_h[c->slots[k].node0 + cd.nodes[i]];
-                if (m > 0.0) cdt = std::fmin(cdt, 2.0 * std::sqrt(m / cd.stiffness));
-            }
-        }
-        parts[k].contact_dt = cdt;
-    });
-    trace.mark("contacts built, masses");
-    // Concatenation: per-slot bases, then every slot copies its part in parallel.
-    struct Base {
-        long long face, slave, ste, stoff, dyn, grid, cnode, role;
-    };
-    std::vector<Base> base(n_desc + 1);
-    base[0] = Base{0, 0, 0, 0, 0, 0, 0, 0};
-    for (int k = 0; k < n_desc; ++k) {
-        const ContactPart& cp = parts[k];
-        const Base& b0 = base[k];
-        base[k + 1] = Base{b0.face + (long long)cp.faces.size() / 4, b0.slave + (long long)cp.slaves.size(),
-                           b0.ste + (long long)cp.st_entries.size(), b0.stoff + (long long)cp.st_off.size(),
-                           b0.dyn + (long long)cp.dyn_faces.size(), b0.grid + (long long)cp.grid_faces.size(),
-                           b0.cnode + (long long)cp.cnode.size(), b0.role + (long long)cp.crole_contact.size()};
-        c->slots[k].contact_dt = cp.contact_dt;
-    }
-    const Base& tot = base[n_desc];
-    const int kc = K;
-    if (tot.face >= (1ll << 31) || tot.slave >= (1ll << 31) || tot.ste >= (1ll << 32) || tot.role >= (1ll << 32))
-        return crush::fail(CRUSH_ERR_INVALID, "contacts too large for one context");
-    std::vector<int> face_off(kc + 1), slave_off(kc + 1), tab_off(kc + 1), counts_for_stop(kc), face_contact(tot.face),
-        slave_contact(tot.slave), contact_slot(kc), slot_contact_off(n_desc + 1);
-    std::vector<uint32_t> faces(4 * tot.face), slaves(tot.slave), dyn_faces(tot.dyn), grid_faces(tot.grid);
-    std::vector<double> scales(tot.slave), stiff(kc), md(kc), cell(kc), st_box(6 * (size_t)std::max(kc, 1));
-    std::vector<uint8_t> is_static(kc);
-    std::vector<long long> st_tab_off(kc + 1);
-    std::vector<uint32_t> st_off(tot.stoff);
-    std::vector<int> st_entries(tot.ste);
-    std::vector<uint32_t> cnode(tot.cnode), cnode_off(tot.cnode + 1);
-    std::vector<int> crole_contact(tot.role), crole_slave(tot.role);
-    // contact node of every primary-node entry and face corner (| CN_FIXED)
-    std::vector<uint32_t> slave_cn(tot.slave), face_cn(4 * tot.face);
-    // per-contact prefix sums (serial, one entry per contact)
-    face_off[0] = slave_off[0] = tab_off[0] = 0;
-    st_tab_off[0] = 0;
-    for (int k = 0, q = 0; k < n_desc; ++k) {
-        const ContactPart& cp = parts[k];
-        slot_contact_off[k] = q;
-        for (size_t j = 0; j < cp.nf.size(); ++j, ++q) {
-            face_off[q + 1] = face_off[q] + cp.nf[j];
-            slave_off[q + 1] = slave_off[q] + cp.ns[j];
-            tab_off[q + 1] = tab_off[q] + cp.tab[j];
-            st_tab_off[q + 1] = st_tab_off[q] + cp.st[j];
-            is_static[q] = cp.stat[j];
-            counts_for_stop[q] = cp.stop[j];
-            contact_slot[q] = k;
-            stiff[q] = cp.stiff[j];
-            md[q] = cp.md[j];
-            cell[q] = cp.cell[j];
-        }
-    }
-    slot_contact_off[n_desc] = kc;
-    cnode_off[0] = 0;
-    std::atomic<bool> cn_missing{false};
-    parallel_for(n_desc, [&](long long k) {
-        const ContactPart& cp = parts[k];
-        const Base& b = base[k];
-        const int q0 = c->slots[k].contact0;
-        for (size_t j = 0; j < cp.nf.size(); ++j) {
-            std::fill(face_contact.begin() + face_off[q0 + j], face_contact.begin() + face_off[q0 + j + 1], (int)(q0 + j));
-            std::fill(slave_contact.begin() + slave_off[q0 + j], slave_contact.begin() + slave_off[q0 + j + 1], (int)(q0 + j));
-        }
-        std::copy(cp.faces.begin(), cp.faces.end(), faces.begin() + 4 * b.face);
-        std::copy(cp.slaves.begin(), cp.slaves.end(), slaves.begin() + b.slave);
-        std::copy(cp.scales.begin(), cp.scales.end(), scales.begin() + b.slave);
-        std::copy(cp.box.begin(), cp.box.end(), st_box.begin() + 6 * (size_t)q0);
-        for (size_t j = 0; j < cp.st_off.size(); ++j) st_off[b.stoff + j] = cp.st_off[j] + (uint32_t)b.ste;
-        std::copy(cp.st_entries.begin(), cp.st_entries.end(), st_entries.begin() + b.ste);
-        for (size_t j = 0; j < cp.dyn_faces.size(); ++j) dyn_faces[b.dyn + j] = cp.dyn_faces[j] + (uint32_t)b.face;
-        for (size_t j = 0; j < cp.grid_faces.size(); ++j) grid_faces[b.grid + j] = cp.grid_faces[j] + (uint32_t)b.face;
-        std::copy(cp.cnode.begin(), cp.cnode.end(), cnode.begin() + b.cnode);
-        for (size_t j = 1; j < cp.cnode_off.size(); ++j) cnode_off[b.cnode + j] = cp.cnode_off[j] + (uint32_t)b.role;
-        std::copy(cp.crole_contact.begin(), cp.crole_contact.end(), crole_contact.begin() + b.role);
-        std::copy(cp.crole_slave.begin(), cp.crole_slave.end(), crole_slave.begin() + b.role);
-        auto cn_of = [&](uint32_t node) {  // the slot's contact nodes are in ascending node order, and include it
-            const auto it = std::lower_bound(cp.cnode.begin(), cp.cnode.end(), node);
-            if (it == cp.cnode.end() || *it != node) {
-                cn_missing = true;  // cannot happen: every primary node and face corner has a role
-                return 0u;
-            }
-            return (uint32_t)(b.cnode + (it - cp.cnode.begin())) | (cm.fixed[node] ? CN_FIXED : 0u);
-        };
-        for (size_t j = 0; j < cp.slaves.size(); ++j) slave_cn[b.slave + j] = cn_of(cp.slaves[j]);
-        for (size_t j = 0; j < cp.faces.size(); ++j) face_cn[4 * b.face + j] = cn_of(cp.faces[j]);
-    });
-    if (cn_missing) return crush::fail(CRUSH_ERR_INVALID, "internal: a contact node without a role");
-    parts.clear();
-    parts.shrink_to_fit();
-    c->n_contacts = kc;
-    c->n_faces = face_off.back();
-    c->n_slaves = slave_off.back();
-    c->face_off_h = face_off;
-    c->slave_off_h = slave_off;
-    c->is_static_h = is_static;
-    ContactArrays& ca = c->ca;
-    ca.n_contacts = c->n_contacts;
-    ca.n_slots = c->n_slots;
-    TRY(c->upload_const(&ca.face_off, face_off));
-    TRY(c->upload_const(&ca.faces, faces));
-    TRY(c->alloc(&ca.geo, std::max<long long>(c->n_faces, 1)));
-    TRY(c->upload_const(&ca.slave_off, slave_off));
-    TRY(c->upload_const(&ca.slaves, slaves));
-    TRY(c->upload_const(&ca.slave_scale, scales));
-    TRY(c->alloc(&ca.hit, std::max<long long>(c->n_slaves, 1)));
-    TRY(c->alloc(&ca.hit_force, 3 * std::max<long long>(c->n_slaves, 1)));
-    TRY(c->alloc(&ca.hit_sd, std::max<long long>(c->n_slaves, 1)));
-    TRY(c->upload_const(&ca.stiffness, stiff));
-    TRY(c->upload_const(&ca.max_distance, md));
-    TRY(c->upload_const(&ca.cell, cell));
-    TRY(c->upload_const(&ca.tab_off, tab_off));
-    TRY(c->alloc(&ca.counts, std::max(tab_off.back(), 1)));
-    TRY(c->alloc(&ca.boff, std::max(tab_off.back(), 1)));
-    TRY(c->alloc(&ca.blen, std::max(tab_off.back(), 1)));
-    {
-        std::vector<long long> ent_off(1, 0);
-        for (int k = 0; k < kc; ++k) {
-            const bool g = tab_off[k + 1] > tab_off[k];
-            ent_off.push_back(ent_off.back() + (g ? (long long)(face_off[k + 1] - face_off[k]) * LEVEL_CELL_BUDGET : 0));
-        }
-        TRY(c->upload_const(&ca.ent_off, ent_off));
-        TRY(c->alloc(&ca.entries, (size_t)std::max<long long>(ent_off.back(), 1)));
-        ca.n_grid_faces = (long long)grid_faces.size();
-        TRY(c->upload_const(&ca.grid_faces, grid_faces));
-    }
-    {
-        // exhaustive contacts (no grid) get a block each; the rest are listed by entry
-        std::vector<int> brute;
-        std::vector<uint32_t> gslaves, stslaves;
-        c->is_brute_h.assign(std::max(kc, 1), 0);
-        for (int k = 0; k < kc; ++k) {
-            const bool st_grid = st_tab_off[k + 1] > st_tab_off[k];
-            const bool grid = tab_off[k + 1] > tab_off[k] || st_grid;
-            if (!grid && face_off[k + 1] - face_off[k] <= 255 && slave_off[k + 1] > slave_off[k]) {
-                brute.push_back(k);
-                c->is_brute_h[k] = 1;
-            } else {
-                for (int q = slave_off[k]; q < slave_off[k + 1]; ++q) (st_grid ? stslaves : gslaves).push_back((uint32_t)q);
-            }
-        }
-        ca.n_brute = (int)brute.size();
-        ca.brute_max_faces = 1;
-        for (int k : brute) ca.brute_max_faces = std::max(ca.brute_max_faces, face_off[k + 1] - face_off[k]);
-        ca.n_grid_slaves = (long long)gslaves.size();
-        ca.n_st_slaves = (long long)stslaves.size();
-        TRY(c->upload_const(&ca.brute_contacts, brute));
-        TRY(c->upload_const(&ca.grid_slaves, gslaves));
-        TRY(c->upload_const(&ca.st_slaves, stslaves));
-        ca.is_brute_h = c->is_brute_h.data();
-        c->grid_slaves_h = std::move(gslaves);
-        c->st_slaves_h = std::move(stslaves);
-    }
-    TRY(c->alloc(&ca.grid_state, 2 * (size_t)std::max(kc, 1) + 1));
-    ca.levels_used = ca.grid_state;
-    ca.ent_cursor = ca.grid_state + kc;
-    ca.big_count = ca.grid_state + 2 * kc;
-    TRY(c->alloc(&ca.cells, (size_t)std::max<long long>(c->n_faces, 1)));
-    TRY(c->alloc(&ca.gather_work, std::max<size_t>(cnode.size(), 1)));
-    TRY(c->alloc(&ca.ev_pool_n, 2));
-    ca.gather_count = ca.ev_pool_n + 1;
-    ca.n_buckets = tab_off.back();
-    ca.exhaustive = 0;
-    c->tab_off_h = tab_off;
-    // Big faces: at most every face of the contacts with a dynamic grid.
-    ca.big_cap = std::max<long long>(ca.n_grid_faces, 1);
-    TRY(c->alloc(&ca.big_faces, (size_t)ca.big_cap));
-    TRY(c->alloc(&ca.big_box, 6 * (size_t)ca.big_cap));
-    TRY(c->alloc(&ca.big_best, (size_t)std::max<long long>(c->n_slaves, 1)));
-    TRY(c->alloc(&ca.search_stats, 3 * (size_t)std::max(c->n_contacts, 1)));
-    c->pen_stride = std::max(c->n_contacts, 1);
-    TRY(c->alloc(&ca.pen_count, 2 * (size_t)c->pen_stride));
-    TRY(c->alloc(&ca.pen_max_bits, 2 * (size_t)c->pen_stride));
-    TRY(c->upload_const(&ca.counts_for_stop, counts_for_stop));
-    ca.n_cnodes = (long long)cnode.size();
-    TRY(c->upload_const(&ca.cnode, cnode));
-    TRY(c->upload_const(&ca.cnode_off, cnode_off));
-    TRY(c->upload_const(&ca.crole_contact, crole_contact));
-    TRY(c->upload_const(&ca.crole_slave, crole_slave));
-    if (tot.cnode >= (long long)CN_FIXED || c->n_slaves >= (1ll << 31))
-        return crush::fail(CRUSH_ERR_UNSUPPORTED, "over 2^31 contact nodes or primary-node entries in one context");
-    TRY(c->upload_const(&ca.slave_cn, slave_cn));
-    TRY(c->upload_const(&ca.face_cn, face_cn));
-    TRY(c->alloc(&ca.ev_count, std::max<size_t>(cnode.size(), 1)));
-    TRY(c->alloc(&ca.ev_list, EV_CAP * std::max<size_t>(cnode.size(), 1)));
-    ca.ev_pool_cap = std::max<long long>(4096, c->n_slaves);
-    TRY(c->alloc(&ca.ev_pool, (size_t)ca.ev_pool_cap));
-    TRY(c->upload_const(&ca.face_contact, face_contact));
-    TRY(c->upload_const(&ca.slave_contact, slave_contact));
-    TRY(c->upload_const(&ca.contact_slot, contact_slot));
-    TRY(c->upload_const(&ca.slot_contact_off, slot_contact_off));
-    TRY(c->upload_const(&ca.is_static, is_static));
-    TRY(c->upload_const(&ca.st_tab_off, st_tab_off));
-    TRY(c->upload_const(&ca.st_off, st_off));
-    TRY(c->upload_const(&ca.st_entries, st_entries));
-    TRY(c->upload_const(&ca.st_box, st_box));
-    ca.n_dyn_faces = (long long)dyn_faces.size();
-    TRY(c->upload_const(&ca.dyn_faces, dyn_faces));
-    CK(cudaMemsetAsync(ca.counts, 0, sizeof(int) * std::max(tab_off.back(), 1), c->stream));
-    CK(cudaMemsetAsync(ca.big_best, 0x7F, sizeof(int) * std::max<long long>(c->n_slaves, 1), c->stream));  // BIG_NONE
-    CK(cudaMemsetAsync(ca.grid_state, 0, sizeof(int) * (2 * (size_t)std::max(kc, 1) + 1), c->stream));
-    CK(cudaMemsetAsync(ca.blen, 0, sizeof(int) * std::max(tab_off.back(), 1), c->stream));
-    CK(cudaMemsetAsync(ca.search_stats, 0, sizeof(unsigned long long) * 3 * std::max(c->n_contacts, 1), c->stream));
-    CK(cudaMemsetAsync(ca.pen_count, 0, sizeof(unsigned long long) * 2 * c->pen_stride, c->stream));
-    CK(cudaMemsetAsync(ca.pen_max_bits, 0, sizeof(unsigned long long) * 2 * c->pen_stride, c->stream));
-    CK(cudaMemsetAsync(ca.ev_count, 0, sizeof(int) * std::max<size_t>(cnode.size(), 1), c->stream));
-    CK(cudaMemsetAsync(ca.ev_pool_n, 0, 2 * sizeof(int), c->stream));
-    trace.mark("contacts");
-
-    // ---- vehicles ----
-    std::vector<long long> voff(1, 0);
-    std::vector<uint32_t> vnodes;
-    std::vector<int> vslot, vlocal;
-    long long max_vnodes = 0;
-    for (int sidx = 0; sidx < n_desc; ++sidx) {
-        const crush_model_desc* d = descs[sidx];
-        const long long n0 = c->slots[sidx].node0;
-        c->slots[sidx].vehicle0 = (int)vslot.size();
-        int nv = std::min(d->n_vehicles, 4);
-        c->slots[sidx].n_vehicles = nv;
-        for (int k = 0; k < nv; ++k) {
-            const crush_vehicle& vd = d->vehicles[k];
-            if (vd.n_nodes < 0 || (vd.n_nodes > 0 && !vd.nodes) || vd.n_front < 0 || (vd.n_front > 0 && !vd.front_nodes))
-                return crush::fail(CRUSH_ERR_INVALID, "invalid vehicle");
-            const size_t b = vnodes.size();
-            vnodes.resize(b + vd.n_nodes);
-            for (int64_t i = 0; i < vd.n_nodes; ++i) {
-                if (vd.nodes[i] >= (uint64_t)d->n_nodes) return crush::fail(CRUSH_ERR_INVALID, "vehicle node out of range");
-                vnodes[b + i] = (uint32_t)(n0 + vd.nodes[i]);
-            }
-            max_vnodes = std::max<long long>(max_vnodes, vd.n_nodes);
-            voff.push_back((long long)vnodes.size());
-            if (vd.accel_node >= (uint64_t)d->n_nodes) return crush::fail(CRUSH_ERR_INVALID, "accelerometer node out of range");
-            for (int64_t i = 0; i < vd.n_front; ++i) {
-                if (vd.front_nodes[i] >= (uint64_t)d->n_nodes) return crush::fail(CRUSH_ERR_INVALID, "front node out of range");
-                c->crush_nodes_h.push_back((uint32_t)(n0 + vd.front_nodes[i]));
-            }
-            c->crush_nodes_h.push_back((uint32_t)(n0 + vd.accel_node));
-            c->crush_off_h.push_back(c->crush_nodes_h.size());
-            vslot.push_back(sidx);
-            vlocal.push_back(k);
-        }
-    }
-    VehicleArrays& va = c->va;
-    va.n_vehicles = (int)vslot.size();
-    va.vx_blocks = (int)std::min<long long>(VX_BLOCKS, std::max<long long>(1, (max_vnodes + 2047) / 2048));
-    TRY(c->upload_const(&va.off, voff));
-    TRY(c->upload_const(&va.nodes, vnodes));
-    TRY(c->upload_const(&va.slot, vslot));
-    TRY(c->upload_const(&va.local, vlocal));
-    TRY(c->alloc(&c->veh_out, 7 * std::max(va.n_vehicles, 1)));
-    TRY(c->upload(&c->crush_nodes, c->crush_nodes_h.data(), c->crush_nodes_h.size()));
-    TRY(c->alloc(&c->crush_ux, std::max<size_t>(c->crush_nodes_h.size(), 1)));
-    // ---- active chunk tables: slot range of every 256-entity chunk ----
-    {
-        const long long sizes[ACTIVE_SPACES] = {c->n_hc, E, N, (long long)c->grid_slaves_h.size(), (long long)cnode.size(),
-                                                (long long)dyn_faces.size(), (long long)slaves.size(),
-                                                (long long)c->st_slaves_h.size(), c->n_sc_free};
-        c->space_off_h.assign(ACTIVE_SPACES + 1, 0);
-        for (int sp = 0; sp < ACTIVE_SPACES; ++sp) c->space_off_h[sp + 1] = c->space_off_h[sp] + (sizes[sp] + CHUNK - 1) / CHUNK;
-        const long long nch = c->space_off_h[ACTIVE_SPACES];
-        std::vector<int> lo(nch), hi(nch);
-        auto slot_of = [&](int sp, long long i) -> int {
-            switch (sp) {
-                case 0: return (int)cm.elem_slot[c->hc_model[i]];
-                case 1: return (int)cm.elem_slot[i];
-                case 2: return (int)cm.node_slot[i];
-                case 3: return contact_slot[slave_contact[c->grid_slaves_h[i]]];
-                case 4: return (int)cm.node_slot[cnode[i]];
-                case 5: return contact_slot[face_contact[dyn_faces[i]]];
-                case 6: return contact_slot[slave_contact[i]];
-                case 7: return contact_slot[slave_contact[c->st_slaves_h[i]]];
-                default: return (int)cm.elem_slot[c->sc_model[i]];
-            }
-        };
-        parallel_for(nch, [&](long long q) {
-            int sp = 0;
-            while (sp + 1 < ACTIVE_SPACES && q >= c->space_off_h[sp + 1]) ++sp;
-            const long long i0 = (q - c->space_off_h[sp]) * CHUNK, i1 = std::min(i0 + CHUNK, sizes[sp]);
-            int a = INT32_MAX, b = -1;
-            for (long long i = i0; i < i1; ++i) {
-                const int sl = slot_of(sp, i);
-                a = std::min(a, sl);
-                b = std::max(b, sl);
-            }
-            lo[q] = a;
-            hi[q] = b;
-        });
-        c->ab.n_chunks = nch;
-        const int* lo_d = nullptr;
-        const int* hi_d = nullptr;
-        const long long* off_d = nullptr;
-        TRY(c->upload_const(&lo_d, lo));
-        TRY(c->upload_const(&hi_d, hi));
-        TRY(c->upload_const(&off_d, c->space_off_h));
-        c->ab.chunk_lo = lo_d;
-        c->ab.chunk_hi = hi_d;
-        c->ab.space_off = off_d;
-        TRY(c->alloc(&c->ab.lists, std::max<long long>(nch, 1)));
-        TRY(c->alloc(&c->ab.counts, ACTIVE_SPACES));
-    }
-    stager.release();
-    c->stager = nullptr;
-    trace.mark("vehicles");
-
-    // ---- time step per slot (src/solver.rs:214-228; contact_dt above) ----
-    launch_init_state(c->stream, c->n_hc, c->stride, c->state);
-    TRY(check_launch(c));
-    CK(cudaMemsetAsync(c->u_tmp, 0, sizeof(double) * 3 * N, c->stream));
-    std::vector<Control> aux(c->n_slots);
-    std::memset(aux.data(), 0, sizeof(Control) * aux.size());
-    for (Control& a : aux) a.dt_stable_bits = INF_BITS;
-    CK(cudaMemcpyAsync(c->ctls_aux, aux.data(), sizeof(Control) * aux.size(), cudaMemcpyHostToDevice, c->stream));
-    launch_elem_dt(c->stream, c->el(), c->nd(), c->ctls_aux, c->u_tmp, 0);
-    TRY(check_launch(c));
-    CK(cudaMemcpyAsync(aux.data(), c->ctls_aux, sizeof(Control) * aux.size(), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    for (int sidx = 0; sidx < n_desc; ++sidx) {
-        Slot& sl = c->slots[sidx];
-        double stable;
-        std::memcpy(&stable, &aux[sidx].dt_stable_bits, sizeof(double));
-        if (!std::isfinite(stable)) {
-            static const int EDGES[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6}, {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
-            double mn = INF, cmax = 0.0;
-            for (long long e = sl.elem0; e < sl.elem0 + sl.n_elems; ++e) {
-                cmax = std::fmax(cmax, wave_speed(cm.materials[cm.hex_part[e]]));
-                for (auto& ed : EDGES) {
-                    const double* p = &cm.positions[3 * (size_t)cm.hexes[8 * e + ed[0]]];
-                    const double* q = &cm.positions[3 * (size_t)cm.hexes[8 * e + ed[1]]];
-                    mn = std::fmin(mn, std::sqrt((p[0] - q[0]) * (p[0] - q[0]) + (p[1] - q[1]) * (p[1] - q[1]) + (p[2] - q[2]) * (p[2] - q[2])));
-                }
-            }
-            stable = mn / (std::sqrt(3.0) * cmax);
-        }
-        sl.stable = std::fmin(stable, sl.contact_dt);
-        sl.dt_floor = sl.settings.mass_scaling > 0.0 ? sl.settings.mass_scaling * sl.stable : 0.0;
-        sl.dt0 = sl.settings.time_step > 0.0 ? sl.settings.time_step : sl.stable * sl.settings.dt_scale;
-    }
-    trace.mark("initial stable step");
-    c->period = std::lcm(c->check_steps, 20);
-    if (c->period > 200) c->period = 0;  // no graph for odd periods
-    c->base_period = c->period;
-    return CRUSH_OK;
-#undef TRY
+    return add_slots(c, descs, n_desc, true, room);
 }
 
 // Whether step `step` ends with the fused pass (its full update and the next
@@ -1861,7 +2137,7 @@ int rebuild_frames(crush_ctx* c) {
     f.state = c->state;
     f.state_stride = c->stride;
     f.sc_index = c->n_sc > 0 ? c->sc_index_d : nullptr;
-    f.n_sc = c->n_sc;
+    f.n_sc = c->sc_stride;  // the plane stride of the scalar geometry
     f.sc_geo = c->sc_geo;
     f.sc_mat = c->sc_mat;
     f.conn_all = c->conn_all;
@@ -1991,6 +2267,27 @@ int rebuild_history(crush_ctx* c) {
     return sync(c);
 }
 
+// A slot's control block at the start of its run (src/solver.rs:214-252).
+Control initial_control(const Slot& sl) {
+    Control x;
+    std::memset(&x, 0, sizeof(x));
+    x.t = 0.0;
+    x.end_time = sl.settings.end_time;
+    x.dt_cfl = sl.dt0;
+    x.dt_min = INF;
+    x.dt_floor = sl.dt_floor;
+    x.dt_scale = sl.settings.dt_scale;
+    x.contact_dt = sl.contact_dt;
+    x.damping = sl.settings.velocity_damping;
+    x.dt_stable_bits = INF_BITS;
+    x.step = 0;
+    x.last_hit = -1;
+    x.max_steps = sl.settings.max_steps;
+    x.done = (0.0 < sl.settings.end_time) ? 0 : 1;
+    x.stop_rule = sl.settings.stop_rule;
+    return x;
+}
+
 int run_begin(crush_ctx* c) {
     const long long N = c->n_nodes;
     drop_graphs(c);
@@ -2008,30 +2305,12 @@ int run_begin(crush_ctx* c) {
         CK(cudaMemsetAsync(c->ca.pen_max_bits, 0, sizeof(unsigned long long) * 2 * c->pen_stride, c->stream));
     }
     CK(cudaMemsetAsync(c->eroded_all, 0, c->n_all, c->stream));
-    launch_init_state(c->stream, c->n_hc, c->stride, c->state);
+    launch_init_state(c->stream, 0, c->n_hc, c->stride, c->state);
     launch_node_masses(c->stream, N, c->all_off, c->all_slot, c->lumped, c->mass, c->inv_mass);
     int st = check_launch(c, 2);
     if (st != CRUSH_OK) return st;
     std::vector<Control> h(c->n_slots);
-    std::memset(h.data(), 0, sizeof(Control) * h.size());
-    for (int k = 0; k < c->n_slots; ++k) {
-        const Slot& sl = c->slots[k];
-        Control& x = h[k];
-        x.t = 0.0;
-        x.end_time = sl.settings.end_time;
-        x.dt_cfl = sl.dt0;
-        x.dt_min = INF;
-        x.dt_floor = sl.dt_floor;
-        x.dt_scale = sl.settings.dt_scale;
-        x.contact_dt = sl.contact_dt;
-        x.damping = sl.settings.velocity_damping;
-        x.dt_stable_bits = INF_BITS;
-        x.step = 0;
-        x.last_hit = -1;
-        x.max_steps = sl.settings.max_steps;
-        x.done = (0.0 < sl.settings.end_time) ? 0 : 1;
-        x.stop_rule = sl.settings.stop_rule;
-    }
+    for (int k = 0; k < c->n_slots; ++k) h[k] = initial_control(c->slots[k]);
     CK(cudaMemcpyAsync(c->ctls, h.data(), sizeof(Control) * h.size(), cudaMemcpyHostToDevice, c->stream));
     // Initial internal forces at u = 0 (src/solver.rs:254); the count of
     // elements it erodes is not added to the run's total (as there).
@@ -2093,6 +2372,88 @@ int run_begin(crush_ctx* c) {
         st = check_launch(c, 3);
         if (st != CRUSH_OK) return st;
         c->frames_ran = true;
+    }
+    return sync(c);
+}
+
+// Slots [s0, s1) (the context's last ones, added while its run is open)
+// begin their run as crush_run_begin begins every slot's: zero
+// displacement, initial velocities, masses, state, the initial internal
+// forces at u = 0, the static faces' geometry, the element dt pass of their
+// step 0 and the contact search their first step's forces read. They join at
+// the run's current step, a step-graph boundary, so their own steps fall on
+// the same step-schedule positions as alone.
+int begin_slots(crush_ctx* c, int s0, int s1) {
+    if (s1 <= s0) return CRUSH_OK;
+    const Slot& a = c->slots[s0];
+    const Slot& z = c->slots[s1 - 1];
+    const long long n0 = a.node0, n1 = z.node0 + z.n_nodes, e0 = a.elem0;
+    const long long h0 = a.hc0, h1 = z.hc0 + z.n_hc, q0 = a.sc0, q1 = z.sc0 + z.n_sc;
+    const long long nn = n1 - n0;
+    CK(cudaMemsetAsync(c->u + 3 * n0, 0, sizeof(double) * 3 * nn, c->stream));
+    CK(cudaMemcpyAsync(c->v + 3 * n0, c->v0 + 3 * n0, sizeof(double) * 3 * nn, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemsetAsync(c->v_half + 3 * n0, 0, sizeof(double) * 3 * nn, c->stream));
+    CK(cudaMemsetAsync(c->f_ext + 3 * n0, 0, sizeof(double) * 3 * nn, c->stream));
+    CK(cudaMemsetAsync(c->f_ext_odd + 3 * n0, 0, sizeof(double) * 3 * nn, c->stream));
+    CK(cudaMemsetAsync(c->added + n0, 0, sizeof(double) * nn, c->stream));
+    CK(cudaMemsetAsync(c->eroded_all + e0, 0, c->n_all - e0, c->stream));
+    launch_init_state(c->stream, h0, h1, c->stride, c->state);
+    launch_node_masses(c->stream, nn, c->all_off + n0, c->all_slot, c->lumped, c->mass + n0, c->inv_mass + n0);
+    int st = check_launch(c, 2);
+    if (st != CRUSH_OK) return st;
+    std::vector<Control> h(s1 - s0);
+    std::vector<int> done(s1 - s0);
+    for (int k = s0; k < s1; ++k) {
+        h[k - s0] = initial_control(c->slots[k]);
+        done[k - s0] = h[k - s0].done;
+    }
+    CK(cudaMemcpyAsync(c->ctls + s0, h.data(), sizeof(Control) * h.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->slot_done + s0, done.data(), sizeof(int) * done.size(), cudaMemcpyHostToDevice, c->stream));
+    // Initial internal forces at u = 0 of the slots' elements (src/solver.rs:254)
+    // and their nodes' f_int: the element arrays and the node rows seen from
+    // the slots' first entries.
+    ElementArrays w = c->el();
+    w.planes += h0;
+    w.state += h0;
+    w.corner += 24 * h0;
+    w.n_hc = h1 - h0;
+    w.sc_model += q0;
+    w.sc_geo += q0;
+    w.sc_mat += 2 * q0;
+    w.sc_corner += 24 * q0;
+    w.n_sc = w.sc_count = q1 - q0;
+    launch_forces(c->stream, w, c->nd(), c->ctls, 0);
+    NodeArrays wn = c->nd();
+    wn.n = nn;
+    wn.hc_ell += 2 * n0;
+    wn.hc_off += n0;
+    wn.sc_off += n0;
+    launch_gather(c->stream, c->el(), wn, c->f_int + 3 * n0);
+    st = check_launch(c, forces_launches(w) + 1);
+    if (st != CRUSH_OK) return st;
+    const int c0 = a.contact0, c1 = z.contact0 + z.n_contacts;
+    if (c1 > c0) {
+        const long long f0 = a.face0, nf = z.face0 + z.n_faces - f0;
+        launch_contact_geometry(c->stream, c->ca, c->nd(), c0, c1, f0, nf);
+        st = check_launch(c, nf > 0 ? 1 : 0);
+        if (st != CRUSH_OK) return st;
+    }
+    // the element dt pass of the slots' step 0 (a step-graph boundary is a
+    // stable-dt check step), and the same data's control copy
+    CK(cudaMemcpyAsync(c->ctls + s0, h.data(), sizeof(Control) * h.size(), cudaMemcpyHostToDevice, c->stream));
+    if (c->adaptive) {
+        launch_elem_dt(c->stream, c->el(), c->nd(), c->ctls, c->u, 1, e0);
+        st = check_launch(c);
+        if (st != CRUSH_OK) return st;
+    }
+    // The first step's contact search of the new contacts at u = 0, contact
+    // by contact (the hits are those any search finds).
+    for (int k = c0; k < c1; ++k) {
+        const long long nf = c->face_off_h[k + 1] - c->face_off_h[k], ns = c->slave_off_h[k + 1] - c->slave_off_h[k];
+        const long long bk0 = c->tab_off_h[k], bk1 = c->tab_off_h[k + 1];
+        launch_contact_search(c->stream, c->ca, c->nd(), c->ctls, k, k + 1, c->face_off_h[k], nf, ns, bk0, bk1, 0, c->slave_lanes);
+        st = check_launch(c, contact_search_launches(c->ca, false, nf, ns, bk0, bk1, k));
+        if (st != CRUSH_OK) return st;
     }
     return sync(c);
 }
@@ -2370,6 +2731,32 @@ int crush_batch_create(const crush_model_desc* const* descs, int n, int device, 
         return st;
     }
     *out = c;
+    return CRUSH_OK;
+}
+
+int crush_batch_create_reserved(const crush_model_desc* const* descs, int n, int device, const crush_capacity* room, crush_ctx** out) {
+    if (!out || !room) return crush::fail(CRUSH_ERR_INVALID, "null argument");
+    if (room->slots < 0 || room->contacts < 0 || room->nodes < 0 || room->hexes < 0 || room->faces < 0 || room->primary_nodes < 0)
+        return crush::fail(CRUSH_ERR_INVALID, "negative room");
+    *out = nullptr;
+    crush_ctx* c = new crush_ctx();
+    int st = create_impl(descs, n, device, c, room);
+    if (st != CRUSH_OK) {
+        delete c;
+        return st;
+    }
+    *out = c;
+    return CRUSH_OK;
+}
+
+int crush_batch_append(crush_ctx* c, const crush_model_desc* const* descs, int n, int* first_slot) {
+    if (!c) return crush::fail(CRUSH_ERR_INVALID, "null context");
+    CK(cudaSetDevice(c->device));
+    if (c->prologue_done) return crush::fail(CRUSH_ERR_INVALID, "slots join an open run only between issues of steps");
+    const int first = c->n_slots;
+    int st = add_slots(c, descs, n, false, nullptr);
+    if (st != CRUSH_OK) return st;
+    if (first_slot) *first_slot = first;
     return CRUSH_OK;
 }
 

@@ -126,7 +126,7 @@ __device__ bool reference_gradients(const double x[8][3], const double dn[8][3],
     return true;
 }
 
-__global__ void __launch_bounds__(128) k_setup_geometry(long long n_all, const double* __restrict__ pos,
+__global__ void __launch_bounds__(128) k_setup_geometry(long long e_begin, long long n_all, const double* __restrict__ pos,
                                                         const uint32_t* __restrict__ conn, const int32_t* __restrict__ part,
                                                         const double* __restrict__ mat,
                                                         const int64_t* __restrict__ hc_index, const uint32_t* __restrict__ elem_slot,
@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(128) k_setup_geometry(long long n_all, const d
                                                         double* __restrict__ elem_mass, int* __restrict__ bad,
                                                         const int64_t* __restrict__ sc_index, long long n_sc,
                                                         double* __restrict__ sc_geo) {
-    long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long e = e_begin + (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n_all) return;
     double x[8][3];
     uint32_t nid[8];
@@ -329,8 +329,8 @@ __global__ void k_node_masses(long long n, const uint32_t* __restrict__ off, con
     inv_mass[i] = m > 0.0 ? 1.0 / m : 0.0;
 }
 
-__global__ void k_init_state(long long n_hc, long long stride, float4* __restrict__ st) {
-    long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_init_state(long long h_begin, long long n_hc, long long stride, float4* __restrict__ st) {
+    long long e = h_begin + (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n_hc) return;
     // identity F_prev⁻¹ (0-8), identity R (9-17), zero stress, compaction, not eroded.
     const float v[28] = {1, 0, 0, 0, 1, 0, 0, 0, 1, 1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -532,7 +532,7 @@ __global__ void __launch_bounds__(FORCES_TPB, FORCES_MINB) k_forces(ElementArray
 constexpr int SC_TPB = 128;
 __device__ __forceinline__ void scalar_force_body(const ElementArrays& el, const NodeArrays& nd, Control* ctls, int respect_done,
                                                   long long i) {
-    if (i >= el.n_sc) return;
+    if (i >= el.sc_count) return;
     const long long e = el.sc_model[i];
     Control* ctl = ctls + el.elem_slot[e];
     if (respect_done && ctl->done) return;
@@ -605,7 +605,9 @@ __device__ __forceinline__ void scalar_force_body(const ElementArrays& el, const
 __global__ void __launch_bounds__(SC_TPB) k_forces_scalar(ElementArrays el, NodeArrays nd, Control* ctls, int respect_done) {
     FOR_ACTIVE(el.act_sc, el.n_sc, 1, g) {
         int lane;
-        scalar_force_body(el, nd, ctls, respect_done, active_entity(el.act_sc, g, 1, &lane));
+        const long long t = active_entity(el.act_sc, g, 1, &lane);
+        // a run lists the elastic elements with a free node; drop-in calls take them all
+        scalar_force_body(el, nd, ctls, respect_done, el.sc_list ? (t < el.n_sc ? (long long)el.sc_list[t] : el.sc_count) : t);
     }
 }
 
@@ -860,10 +862,10 @@ __device__ __forceinline__ void elem_dt_body(const ElementArrays& el, const Node
 }
 
 __global__ void __launch_bounds__(DT_TPB) k_elem_dt(ElementArrays el, NodeArrays nd, Control* ctls, const double* __restrict__ u,
-                                                    int respect_done) {
-    FOR_ACTIVE(el.act_all, el.n_all, 1, g) {
+                                                    int respect_done, long long e_begin) {
+    FOR_ACTIVE(el.act_all, el.n_all - e_begin, 1, g) {
         int lane;
-        elem_dt_body(el, nd, ctls, u, respect_done, active_entity(el.act_all, g, 1, &lane));
+        elem_dt_body(el, nd, ctls, u, respect_done, e_begin + active_entity(el.act_all, g, 1, &lane));
     }
 }
 
@@ -1935,12 +1937,12 @@ __global__ void __launch_bounds__(VEH_TPB) k_vehicle_vx(VehicleArrays va, const 
 // ---------------------------------------------------------------------------
 // Launchers
 // ---------------------------------------------------------------------------
-void launch_setup_geometry(cudaStream_t s, long long n_all, const double* pos, const uint32_t* conn_all, const int32_t* part,
-                           const double* mat, const int64_t* hc_index, const uint32_t* elem_slot, long long stride,
+void launch_setup_geometry(cudaStream_t s, long long e_begin, long long n_all, const double* pos, const uint32_t* conn_all,
+                           const int32_t* part, const double* mat, const int64_t* hc_index, const uint32_t* elem_slot, long long stride,
                            float4* planes, double* volume, double* lumped, double* dt_factor, double* elem_mass, int* bad,
                            const int64_t* sc_index, long long n_sc, double* sc_geo) {
-    if (n_all <= 0) return;
-    k_setup_geometry<<<(unsigned)blocks_for(n_all, 128), 128, 0, s>>>(n_all, pos, conn_all, part, mat, hc_index, elem_slot,
+    if (n_all <= e_begin) return;
+    k_setup_geometry<<<(unsigned)blocks_for(n_all - e_begin, 128), 128, 0, s>>>(e_begin, n_all, pos, conn_all, part, mat, hc_index, elem_slot,
                                                                        stride, planes, volume, lumped, dt_factor, elem_mass, bad,
                                                                        sc_index, n_sc, sc_geo);
 }
@@ -1948,9 +1950,9 @@ void launch_node_masses(cudaStream_t s, long long n, const uint32_t* off, const 
                         double* mass, double* inv_mass) {
     k_node_masses<<<(unsigned)blocks_for(n, TPB), TPB, 0, s>>>(n, off, slot, lumped, mass, inv_mass);
 }
-void launch_init_state(cudaStream_t s, long long n_hc, long long stride, float4* state) {
-    if (n_hc <= 0) return;
-    k_init_state<<<(unsigned)blocks_for(n_hc, TPB), TPB, 0, s>>>(n_hc, stride, state);
+void launch_init_state(cudaStream_t s, long long h_begin, long long n_hc, long long stride, float4* state) {
+    if (n_hc <= h_begin) return;
+    k_init_state<<<(unsigned)blocks_for(n_hc - h_begin, TPB), TPB, 0, s>>>(h_begin, n_hc, stride, state);
 }
 void launch_forces(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, int respect_done, int n_sms,
                    int schedule, unsigned* queue) {
@@ -1980,9 +1982,10 @@ void launch_half(cudaStream_t s, const NodeArrays& nd, Control* ctls) {
 void launch_full(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls) {
     k_full<<<active_grid(nd.n, 3, TPB, GRID_CAP), TPB, 0, s>>>(el, nd, ctls);
 }
-void launch_elem_dt(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, const double* u, int respect_done) {
-    if (el.n_all <= 0) return;
-    k_elem_dt<<<active_grid(el.n_all, 1, DT_TPB, GRID_CAP), DT_TPB, 0, s>>>(el, nd, ctls, u, respect_done);
+void launch_elem_dt(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, const double* u, int respect_done,
+                    long long e_begin) {
+    if (el.n_all <= e_begin) return;
+    k_elem_dt<<<active_grid(el.n_all - e_begin, 1, DT_TPB, GRID_CAP), DT_TPB, 0, s>>>(el, nd, ctls, u, respect_done, e_begin);
 }
 void launch_dt_finalize(cudaStream_t s, Control* ctls, int n_slots, int* mass_flag) {
     k_dt_finalize<<<(unsigned)blocks_for(n_slots, 128), 128, 0, s>>>(ctls, n_slots, mass_flag);

@@ -37,6 +37,8 @@ struct ElementArrays {
     long long n_sc;              // scalar elements visited (a run: those with a free node, numbered first)
     long long sc_stride;         // all scalar elements (the plane stride of sc_geo)
     const uint32_t* sc_model;    // scalar index -> model element
+    long long sc_count;          // scalar elements (n_sc: those processed, the length of sc_list when given)
+    const uint32_t* sc_list;     // a run: the scalar indices of elastic elements with a free node (null: 0..n_sc)
     const double* sc_geo;        // SC_PLANES x sc_stride (SoA): grad 24, volume, gamma 32, H upper triangle 78
     const double* sc_mat;        // 2 per scalar element: Young's modulus, Poisson ratio
     double* sc_corner;           // 24 per scalar element: corner forces (f64)
@@ -215,14 +217,15 @@ struct VehicleArrays {
 
 // Every launcher takes the array of per-crash control blocks (`ctls`, one
 // per crash slot); entities find their slot through the *_slot arrays.
-void launch_setup_geometry(cudaStream_t s, long long n_all, const double* pos, const uint32_t* conn_all,
+// Elements [e_begin, n_all).
+void launch_setup_geometry(cudaStream_t s, long long e_begin, long long n_all, const double* pos, const uint32_t* conn_all,
                            const int32_t* part, const double* mat_e_nu_rho_hg, const int64_t* hc_index,
                            const uint32_t* elem_slot, long long stride, float4* planes, double* volume, double* lumped,
                            double* dt_factor, double* elem_mass, int* bad, const int64_t* sc_index, long long n_sc,
                            double* sc_geo);
 void launch_node_masses(cudaStream_t s, long long n, const uint32_t* off, const uint32_t* slot, const double* lumped,
                         double* mass, double* inv_mass);
-void launch_init_state(cudaStream_t s, long long n_hc, long long stride, float4* state);
+void launch_init_state(cudaStream_t s, long long h_begin, long long n_hc, long long stride, float4* state);
 // Element forces: the honeycomb lane kernel and, when the model has
 // elastic elements, the scalar f64 kernel (forces_launches of them).
 // schedule: 0 = one persistent wave of blocks on the n_sms SMs, 1 = a block
@@ -235,7 +238,9 @@ int forces_launches(const ElementArrays& el);
 void launch_gather(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, double* f_out);
 void launch_half(cudaStream_t s, const NodeArrays& nd, Control* ctls);
 void launch_full(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls);
-void launch_elem_dt(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, const double* u, int respect_done);
+// Elements [e_begin, el.n_all) (e_begin > 0: no active list).
+void launch_elem_dt(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, const double* u, int respect_done,
+                    long long e_begin = 0);
 // mass_flag: set when a crash scales its masses this step (k_mass_scaling
 // does nothing otherwise), cleared by the step's end.
 void launch_dt_finalize(cudaStream_t s, Control* ctls, int n_slots, int* mass_flag);

@@ -30,10 +30,18 @@ class Context:
     """One model, or a batch of models (a list of descriptors), resident on
     one GPU (crush_ctx)."""
 
-    def __init__(self, desc, device=0):
+    def __init__(self, desc, device=0, room=None):
+        """desc: one model or a list (a batch). room: a dict of the
+        crush_capacity fields (slots, contacts, nodes, hexes, faces,
+        primary_nodes) to keep room for models appended later."""
         self._lib = lib()
         h = C.c_void_p()
-        if isinstance(desc, (list, tuple)):
+        if room is not None:
+            descs = list(desc) if isinstance(desc, (list, tuple)) else [desc]
+            arr = (C.POINTER(abi.ModelDesc) * len(descs))(*[C.pointer(d) for d in descs])
+            cap = abi.Capacity(**room)
+            check(self._lib.crush_batch_create_reserved(arr, len(descs), device, C.byref(cap), C.byref(h)))
+        elif isinstance(desc, (list, tuple)):
             arr = (C.POINTER(abi.ModelDesc) * len(desc))(*[C.pointer(d) for d in desc])
             check(self._lib.crush_batch_create(arr, len(desc), device, C.byref(h)))
         else:
@@ -259,6 +267,26 @@ class Context:
     def set_contact_search(self, exhaustive):
         """True: every contact search tests every face (no broad phase)."""
         check(self._lib.crush_set_contact_search(self.h, int(bool(exhaustive))))
+
+    def append(self, descs):
+        """Add models as new slots (crush_batch_append); returns the first
+        new slot's index. With a run open, call on a multiple of 20 steps."""
+        descs = list(descs)
+        arr = (C.POINTER(abi.ModelDesc) * len(descs))(*[C.pointer(d) for d in descs])
+        first = C.c_int()
+        check(self._lib.crush_batch_append(self.h, arr, len(descs), C.byref(first)))
+        self.n_slots = self._lib.crush_batch_size(self.h)
+        nn, ne, na = C.c_int64(), C.c_int64(), C.c_int64()
+        check(self._lib.crush_sizes(self.h, C.byref(nn), C.byref(ne), C.byref(na)))
+        self.n_nodes, self.n_hexes, self.n_active = nn.value, ne.value, na.value
+        return first.value
+
+    def batch_done(self):
+        """(done flag per slot, all done) of the open run."""
+        flags = (C.c_int * self.n_slots)()
+        all_ = C.c_int()
+        check(self._lib.crush_batch_done(self.h, flags, C.byref(all_)))
+        return [bool(x) for x in flags], bool(all_.value)
 
     def set_step_fusion(self, fused):
         """True (default): fuse a step's full update with the next step's half

@@ -402,6 +402,37 @@ int crush_batch_results_range(crush_ctx* ctx, int first, int count, crush_result
  * step kernels keep; synchronises the context's stream. */
 int crush_batch_done(crush_ctx* ctx, int* done_flags, int* all);
 
+/* ---- continuous batching: slots added to a running context ----
+ * No counterpart in the reference. A context created with room to spare
+ * (crush_batch_create_reserved) takes more models later
+ * (crush_batch_append), also while its run is open: the new slots join the
+ * run at its current step and advance with the others from then on, each
+ * with its own step 0 (so a slot's results are bit-identical to the same
+ * model run alone). The room is fixed at creation: `room` gives the
+ * slots, contacts, nodes, hexahedra, contact faces and listed contact nodes
+ * (primary nodes) the context must hold in total (at least the initial
+ * models' needs; the grid tables, entries and contact-node lists get room in
+ * proportion to the faces). */
+typedef struct crush_capacity {
+    int32_t slots;
+    int32_t contacts;
+    int64_t nodes;
+    int64_t hexes;
+    int64_t faces;
+    int64_t primary_nodes;
+} crush_capacity;
+int crush_batch_create_reserved(const crush_model_desc* const* descs, int n, int device, const crush_capacity* room, crush_ctx** out);
+/* Adds n models as slots [*first_slot, *first_slot + n). With a run open,
+ * only on a step-graph boundary (a multiple of 20 steps: between
+ * crush_run_steps calls of multiples of 20 steps, the default issue of
+ * crush_run); the call sets the new slots up as crush_run_begin does and
+ * searches their contacts for their first step. CRUSH_ERR_BUSY, with
+ * nothing added, when the models do not fit the room; CRUSH_ERR_UNSUPPORTED
+ * for models with another stable-dt cadence or time-step mode than the
+ * context's, or a context recording histories or frames. Synchronises the
+ * context's stream. */
+int crush_batch_append(crush_ctx* ctx, const crush_model_desc* const* descs, int n, int* first_slot);
+
 /* ---- allocation-free contact call ----
  *
  * No counterpart in the reference (its ContactRuntime::new + ::apply,
