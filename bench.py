@@ -28,9 +28,12 @@ the element forces, the ordered force gather with the full step.
              the plain one-crash-per-launch path (crush_create + crush_run per
              crash) on a sample, and the FP64 delta-v error of a sample against
              the reference's f64 scalar restatement.
-  serving    the crash server under an open-loop Poisson stream of seeded
-             head-on / T-bone / rear-end queries (300-20000 elements):
-             crashes/s and p50/p99 submit-to-result latency.
+  serving    the crash server (continuous batching: requests join running
+             serving contexts between chunks of steps) under open-loop
+             Poisson streams of seeded head-on / T-bone / rear-end queries
+             (300-20000 elements) at 200, 500, 1000 and 2000 req/s:
+             crashes/s and p50/p99 submit-to-result latency, beside the
+             median time of one query run alone.
 --impl reference runs the CPU restatement of the reference as the reference arm.
 """
 import argparse
@@ -390,21 +393,54 @@ def two_part_section(n, device):
             "path": "crush_create + crush_run (single); crush_batch_create + crush_batch_run (batch), set-up included"}
 
 
-def serving_section(rate, seconds, device):
-    """The crash server under an open-loop Poisson stream at `rate` req/s."""
+def serving_pool(n):
+    """n distinct seeded serving queries (head-on, T-bone, rear-end; 300-20000
+    hexahedra), built once; the arrival stream cycles through them."""
     from crushrs_b200 import scenarios as S
+
+    return [S.Model.build(S.serve_query(i)[1]) for i in range(n)]
+
+
+def serving_section(rate, seconds, device, pool):
+    """The crash server under an open-loop Poisson stream at `rate` req/s
+    for `seconds` of arrivals (continuous batching: requests join running
+    serving contexts between chunks of steps)."""
     from crushrs_b200.serve import Server, open_loop
 
     n = max(1, int(rate * seconds))
-    models = [S.Model.build(S.serve_query(i)[1]) for i in range(n)]
-    with Server(device=device, max_waves=4) as srv:
+    models = [pool[i % len(pool)] for i in range(n)]
+    with Server(device=device) as srv:
         res, wall, _ = open_loop(srv, models, rate=rate)
         st = srv.stats()
     lat = sorted(r.finish_s - r.submit_s for r in res.values())
-    pick = lambda q: lat[min(len(lat) - 1, int(q * len(lat)))]
-    return {"rate_req_per_s": rate, "seconds": seconds, "crashes": len(res), "crashes_per_s": len(res) / wall,
-            "p50_ms": 1e3 * pick(0.5), "p99_ms": 1e3 * pick(0.99), "waves": int(st.waves), "peak_gb": st.peak_bytes_in_use / 1e9,
+    wait = sorted(r.start_s - r.submit_s for r in res.values())
+    pick = lambda xs, q: xs[min(len(xs) - 1, int(q * len(xs)))]
+    return {"rate_req_per_s": rate, "seconds": seconds, "crashes": len(res), "crashes_per_s": len(res) / wall, "wall_s": wall,
+            "p50_ms": 1e3 * pick(lat, 0.5), "p99_ms": 1e3 * pick(lat, 0.99), "admission_wait_p50_ms": 1e3 * pick(wait, 0.5),
+            "contexts": int(st.waves), "peak_gb": st.peak_bytes_in_use / 1e9,
             "elements_mean": sum(m.n_hexes for m in models) / n, "ok": all(r.status == 0 for r in res.values())}
+
+
+def serving_standalone(pool, device, sample=16):
+    """Median seconds of one query alone (crush_create + crush_run), the
+    reference point of the served latencies."""
+    from crushrs_b200.engine import Context
+
+    times = []
+    for m in pool[:sample]:
+        t = time.perf_counter()
+        c = Context(m.desc, device=device)
+        c.run()
+        c.close()
+        times.append(time.perf_counter() - t)
+    return statistics.median(times)
+
+
+def serving_all(args, device):
+    pool = serving_pool(args.serve_pool)
+    alone = serving_standalone(pool, device)
+    return {"standalone_median_ms": 1e3 * alone, "pool": len(pool),
+            "rates": [serving_section(float(r), args.serve_seconds, device, pool) for r in args.serve_rates.split(",") if r]}
 
 
 def main():
@@ -418,8 +454,9 @@ def main():
     ap.add_argument("--batch", type=int, default=4096, help="crashes of the batched section (0: skip)")
     ap.add_argument("--plain-sample", type=int, default=64)
     ap.add_argument("--oracle-sample", type=int, default=4)
-    ap.add_argument("--serve-rates", default="100,200", help="req/s of the serving section ('' : skip)")
-    ap.add_argument("--serve-seconds", type=float, default=30.0)
+    ap.add_argument("--serve-rates", default="200,500,1000,2000", help="req/s of the serving section ('' : skip)")
+    ap.add_argument("--serve-seconds", type=float, default=10.0, help="seconds of arrivals per rate")
+    ap.add_argument("--serve-pool", type=int, default=1024, help="distinct seeded queries the arrival stream cycles through")
     ap.add_argument("--schedule-steps", type=int, default=200, help="steps timed under each step schedule after the main region")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -491,7 +528,7 @@ def main():
             if rank == 0:
                 line["batched"] = b
         if rank == 0 and world == 1 and args.serve_rates:
-            line["serving"] = [serving_section(float(r), args.serve_seconds, local) for r in args.serve_rates.split(",") if r]
+            line["serving"] = serving_all(args, local)
         if rank == 0 and "twopart" in sections:
             line["two_part"] = two_part_section(64, local)
         if rank == 0:
@@ -570,7 +607,7 @@ def main():
         if rank == 0:
             line["batched"] = b
     if rank == 0 and world == 1 and args.serve_rates:
-        line["serving"] = [serving_section(float(r), args.serve_seconds, local) for r in args.serve_rates.split(",") if r]
+        line["serving"] = serving_all(args, local)
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         steps, loop, sec = cpu_reference(desc, args.cpu_steps, threads)

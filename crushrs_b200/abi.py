@@ -218,6 +218,7 @@ def declare_engine_api(lib):
     lib.crush_batch_create.argtypes = [P(P(ModelDesc)), C.c_int, C.c_int, P(vp)]
     lib.crush_batch_create_reserved.argtypes = [P(P(ModelDesc)), C.c_int, C.c_int, P(Capacity), P(vp)]
     lib.crush_batch_append.argtypes = [vp, P(P(ModelDesc)), C.c_int, P(C.c_int)]
+    lib.crush_run_issue.argtypes = [vp, C.c_int64]
     lib.crush_batch_size.argtypes = [vp]
     lib.crush_batch_run.argtypes = [vp, P(Results)]
     lib.crush_batch_results.argtypes = [vp, C.c_int, P(Results)]
@@ -254,6 +255,7 @@ class ServerConfig(C.Structure):
         ("max_wave_elements", C.c_int64),
         ("hbm_budget_bytes", C.c_double),
         ("gather_ms", C.c_double),
+        ("idle_ms", C.c_double),
     ]
 
 

@@ -127,13 +127,15 @@ Capacity capacity_for(const crush_capacity* r, const Capacity& need) {
     up(c.parts, 16ll * r->slots);
     up(c.vehicles, 4ll * r->slots);
     up(c.vnodes, 2ll * r->nodes);
-    // hashed grids: tables of twice the key-box cells (about 27 per face at
-    // the reference positions) rounded up to a power of two, at least 1024
-    // buckets per contact; entries faces x LEVEL_CELL_BUDGET
-    up(c.buckets, 128ll * r->faces + 2048ll * r->contacts);
+    // hashed grids: dynamic tables (contacts of 256+ faces: twice the
+    // key-box cells rounded up to a power of two, at least 1024 buckets) and
+    // their entries (faces x LEVEL_CELL_BUDGET); static tables of the fixed
+    // faces (a road's: about 8 cells per face). Models that need more than
+    // this room are refused with CRUSH_ERR_BUSY.
+    up(c.buckets, 16ll * r->faces + 1024ll * r->contacts);
     up(c.entries, (long long)LEVEL_CELL_BUDGET * r->faces);
-    up(c.st_tabs, 128ll * r->faces + 32ll * r->contacts);
-    up(c.st_ents, 64ll * r->faces);
+    up(c.st_tabs, 4ll * r->faces + 512ll * r->contacts);
+    up(c.st_ents, 16ll * r->faces + 256ll * r->contacts);
     up(c.cnodes, r->primary_nodes + 4ll * r->faces);
     up(c.roles, r->primary_nodes + 4ll * r->faces);
     return c;
@@ -1529,6 +1531,7 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
         ca.is_static = c->is_static_d;
         ca.st_off = c->st_off_d;
         ca.st_entries = c->st_entries_d;
+        ca.contact_room = KC;
         ca.levels_used = ca.grid_state;
         ca.ent_cursor = ca.grid_state + KC;
         ca.big_count = ca.grid_state + 2 * KC;
@@ -1733,8 +1736,17 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
                 c->chunk_lo_h[q] = a;
                 c->chunk_hi_h[q] = b;
             });
-            TRY(put(c->chunk_lo_d + q0, c->chunk_lo_h.data() + q0, q1 - q0 + 1));
-            TRY(put(c->chunk_hi_d + q0, c->chunk_hi_h.data() + q0, q1 - q0 + 1));
+            if (!creating) {
+                TRY(put(c->chunk_lo_d + q0, c->chunk_lo_h.data() + q0, q1 - q0 + 1));
+                TRY(put(c->chunk_hi_d + q0, c->chunk_hi_h.data() + q0, q1 - q0 + 1));
+            }
+        }
+        // A new context's tables in full: chunks no slot holds yet have the
+        // empty range (lo > hi), which the active-list pass never reads
+        // control blocks for.
+        if (creating) {
+            TRY(put(c->chunk_lo_d, c->chunk_lo_h.data(), c->chunk_lo_h.size()));
+            TRY(put(c->chunk_hi_d, c->chunk_hi_h.data(), c->chunk_hi_h.size()));
         }
     }
     trace.mark("active chunk tables");
@@ -2758,6 +2770,12 @@ int crush_batch_append(crush_ctx* c, const crush_model_desc* const* descs, int n
     if (st != CRUSH_OK) return st;
     if (first_slot) *first_slot = first;
     return CRUSH_OK;
+}
+
+int crush_run_issue(crush_ctx* c, int64_t n_steps) {
+    if (!c || n_steps < 0) return crush::fail(CRUSH_ERR_INVALID, "invalid argument");
+    CK(cudaSetDevice(c->device));
+    return issue_steps(c, n_steps);
 }
 
 int crush_create(const crush_model_desc* desc, int device, crush_ctx** out) {

@@ -13,6 +13,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -107,16 +108,21 @@ struct crush_server {
     std::deque<Request> queue;
     std::deque<crush_server_result> done;
     std::thread scheduler;
-    std::vector<std::pair<int, std::thread>> workers;  // (wave id, thread)
-    std::vector<int> finished;                         // waves whose thread is ending (to join)
+    std::vector<std::pair<int, std::thread>> workers;  // (context id, thread)
+    std::vector<int> finished;                         // contexts whose thread is ending (to join)
     double budget = 0.0, in_use = 0.0, peak = 0.0;
-    int active = 0;
+    int active = 0;                   // running contexts
+    std::map<int, int> accepting;     // schedule class -> running contexts of it that still take requests
     bool stop = false;
     uint64_t next_ticket = 1;
-    int64_t submitted = 0, completed = 0, waves = 0;
+    int64_t submitted = 0, completed = 0, contexts = 0;
 
-    void run_wave(std::vector<Request> wave, int wave_id, double bytes);
+    void run_context(std::vector<Request> first, int id, double bytes, crush_capacity room);
     void schedule();
+    // Requests from the head of the queue with schedule class `key` whose
+    // elements fit `elements` (at least one when `at_least_one`), removed
+    // from the queue; called with mu held.
+    std::vector<Request> take(int key, int64_t elements, int max_slots, bool at_least_one);
 };
 
 extern "C" double crush_model_footprint(const crush_model_desc* d) {
@@ -131,21 +137,85 @@ extern "C" double crush_model_footprint(const crush_model_desc* d) {
     return 1100.0 * (double)d->n_hexes + 300.0 * (double)d->n_nodes + 330.0 * faces + 120.0 * slaves + 8192.0;
 }
 
-void crush_server::run_wave(std::vector<Request> wave, int wave_id, double bytes) {
-    const double start = now_s(t0);
-    std::vector<const crush_model_desc*> descs(wave.size());
-    for (size_t k = 0; k < wave.size(); ++k) descs[k] = &wave[k].model->desc;
-    crush_ctx* ctx = nullptr;
-    const int n = (int)wave.size();
+namespace {
+
+// The room of a serving context: `elements` hexahedra and `slots` crashes
+// of the serving mix (per hexahedron about 1.3 nodes, 0.11 contact faces and
+// 0.17 listed contact nodes, plus per crash a few hundred of each for its
+// road and small blocks; 4 contacts per crash), with margin.
+crush_capacity serving_room(int64_t elements, int slots) {
+    crush_capacity r;
+    r.slots = slots;
+    r.contacts = 6 * slots;
+    r.hexes = elements;
+    r.nodes = 2 * elements + 1000ll * slots;
+    r.faces = elements / 4 + 1200ll * slots;
+    r.primary_nodes = elements / 3 + 600ll * slots;
+    return r;
+}
+
+// Device bytes of a context with that room (the admission measure of the
+// HBM budget): per hexahedron its planes, state, corner forces, incidence
+// and f64 arrays; per node the f64 node arrays; per contact face its
+// geometry, cells and grid room; per contact its table room; per listed
+// contact node its hit, events and roles; per slot its control blocks.
+double room_bytes(const crush_capacity& r) {
+    return 1100.0 * (double)r.hexes + 300.0 * (double)r.nodes + 800.0 * (double)r.faces + 15500.0 * (double)r.contacts +
+           270.0 * (double)r.primary_nodes + 10000.0 * (double)r.slots;
+}
+
+// The room of a new context: the configured one, or a smaller one of the
+// same mix that fits `left` bytes (never below the first request).
+crush_capacity room_within(int64_t elements, int slots, double left, int64_t first_elements) {
+    crush_capacity r = serving_room(elements, slots);
+    while (room_bytes(r) > left && elements > first_elements) {
+        elements = std::max<int64_t>(first_elements, elements / 2);
+        slots = std::max(1, slots / 2);
+        r = serving_room(elements, slots);
+    }
+    return r;
+}
+
+}  // namespace
+
+std::vector<Request> crush_server::take(int key, int64_t elements, int max_slots, bool at_least_one) {
+    std::vector<Request> out;
+    int64_t e = 0;
+    for (auto it = queue.begin(); it != queue.end() && (int)out.size() < max_slots;) {
+        if (it->check_key != key) {
+            ++it;
+            continue;
+        }
+        if (e + it->elements > elements && !(at_least_one && out.empty())) break;  // keep arrival order within a class
+        e += it->elements;
+        out.push_back(std::move(*it));
+        it = queue.erase(it);
+    }
+    return out;
+}
+
+// One serving context: a batched context with room for more crashes,
+// created from the first requests, driven in chunks of steps on its own
+// stream by this thread. Between chunks (step-graph boundaries) it admits
+// waiting requests of its schedule class into the open run
+// (crush_batch_append, whose host set-up overlaps the chunk just issued),
+// reports every crash the moment it stops, and ends once its room is spent
+// (or no request came for a while) and its crashes have all stopped.
+void crush_server::run_context(std::vector<Request> first, int id, double bytes, crush_capacity room) {
+    const int key = first.front().check_key;
+    std::vector<Request> slots;  // the context's requests, by slot
+    std::vector<double> start;   // when each slot began
+    std::vector<int> reported;
     std::vector<crush_server_result> out;
+    crush_ctx* ctx = nullptr;
     auto report = [&](int slot, int status, const crush_results* r) {
         crush_server_result x;
         std::memset(&x, 0, sizeof(x));
-        x.ticket = wave[slot].ticket;
+        x.ticket = slots[slot].ticket;
         x.status = status;
-        x.wave = wave_id;
-        x.submit_s = wave[slot].submit_s;
-        x.start_s = start;
+        x.wave = id;
+        x.submit_s = slots[slot].submit_s;
+        x.start_s = start[slot];
         x.finish_s = now_s(t0);
         if (r) x.results = *r;
         out.push_back(x);
@@ -158,53 +228,110 @@ void crush_server::run_wave(std::vector<Request> wave, int wave_id, double bytes
         out.clear();
         cv_done.notify_all();
     };
-    int st = crush_batch_create(descs.data(), n, cfg.device, &ctx);
+    int64_t used = 0;  // hexahedra admitted
+    auto add = [&](std::vector<Request>& batch) {
+        for (auto& r : batch) {
+            used += r.elements;
+            slots.push_back(std::move(r));
+            start.push_back(now_s(t0));
+            reported.push_back(0);
+        }
+        batch.clear();
+    };
+    std::vector<const crush_model_desc*> descs;
+    for (auto& r : first) descs.push_back(&r.model->desc);
+    int st = crush_batch_create_reserved(descs.data(), (int)descs.size(), cfg.device, &room, &ctx);
+    add(first);
     if (st == CRUSH_OK) st = crush_run_begin(ctx);
-    if (st == CRUSH_OK) {
-        std::vector<int> flags(n, 0), reported(n, 0);
-        std::vector<crush_results> rs;
-        int remaining = n, all = 0;
-        while (remaining > 0 && st == CRUSH_OK) {
-            st = crush_run_steps(ctx, cfg.chunk_steps, &all);
-            if (st != CRUSH_OK) break;
-            st = crush_batch_done(ctx, flags.data(), &all);
-            if (st != CRUSH_OK) break;
-            int lo = n, hi = -1;
-            for (int k = 0; k < n; ++k)
-                if (flags[k] && !reported[k]) {
-                    lo = std::min(lo, k);
-                    hi = std::max(hi, k);
+    bool open = true;  // still takes requests
+    const int chunk = std::max(20, cfg.chunk_steps / 20 * 20);
+    std::vector<int> flags;
+    std::vector<crush_results> rs;
+    while (st == CRUSH_OK) {
+        int running = 0;
+        for (size_t k = 0; k < slots.size(); ++k) running += reported[k] ? 0 : 1;
+        std::vector<Request> batch;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            if (running == 0) {
+                // Nothing on the device: wait for requests of this class, or end.
+                if (!open || stop) break;
+                const bool got = cv_work.wait_for(lk, std::chrono::duration<double, std::milli>(cfg.idle_ms), [&] {
+                    if (stop) return true;
+                    for (auto& q : queue)
+                        if (q.check_key == key) return true;
+                    return false;
+                });
+                if (!got || stop) break;
+            }
+            if (open) batch = take(key, room.hexes - used, room.slots - (int)slots.size(), false);
+        }
+        // Requests are waiting: short chunks, so the next admission comes soon.
+        const bool waiting = !batch.empty();
+        if (running > 0) st = crush_run_issue(ctx, waiting ? 20 : chunk);
+        if (st != CRUSH_OK) break;
+        if (!batch.empty()) {
+            descs.clear();
+            for (auto& r : batch) descs.push_back(&r.model->desc);
+            const int a = crush_batch_append(ctx, descs.data(), (int)descs.size(), nullptr);
+            if (a == CRUSH_OK) {
+                add(batch);
+            } else {
+                // No room (or not admissible here): back to the queue's head
+                // for another context; this one takes no more.
+                std::lock_guard<std::mutex> lk(mu);
+                for (auto it = batch.rbegin(); it != batch.rend(); ++it) queue.push_front(std::move(*it));
+                if (open) --accepting[key];
+                open = false;
+                cv_work.notify_all();
+                if (a != CRUSH_ERR_BUSY && a != CRUSH_ERR_UNSUPPORTED) {
+                    st = a;
+                    break;
                 }
-            if (hi < lo) continue;
+            }
+        }
+        flags.assign(slots.size(), 0);
+        int all = 0;
+        st = crush_batch_done(ctx, flags.data(), &all);
+        if (st != CRUSH_OK) break;
+        int lo = (int)slots.size(), hi = -1;
+        for (int k = 0; k < (int)slots.size(); ++k)
+            if (flags[k] && !reported[k]) {
+                lo = std::min(lo, k);
+                hi = std::max(hi, k);
+            }
+        if (hi >= lo) {
             rs.resize(hi - lo + 1);
             st = crush_batch_results_range(ctx, lo, hi - lo + 1, rs.data());
             if (st != CRUSH_OK) break;
             for (int k = lo; k <= hi; ++k)
                 if (flags[k] && !reported[k]) {
                     reported[k] = 1;
-                    --remaining;
                     report(k, rs[k - lo].status, &rs[k - lo]);
                 }
             flush();
         }
-        if (st != CRUSH_OK)
-            for (int k = 0; k < n; ++k)
-                if (!reported[k]) report(k, st, nullptr);
-    } else {
-        for (int k = 0; k < n; ++k) report(k, st, nullptr);
-    }
+        if (open && ((int)slots.size() >= room.slots || used >= room.hexes)) {
+            std::lock_guard<std::mutex> lk(mu);
+            --accepting[key];
+            open = false;
+            cv_work.notify_all();
+        }
+        }
+    for (size_t k = 0; k < slots.size(); ++k)
+        if (!reported[k]) report((int)k, st == CRUSH_OK ? CRUSH_ERR_INVALID : st, nullptr);
     if (ctx) crush_destroy(ctx);
-    wave.clear();
     flush();
     std::lock_guard<std::mutex> lk(mu);
+    if (open) --accepting[key];
     in_use -= bytes;
     --active;
-    finished.push_back(wave_id);
+    finished.push_back(id);
     cv_work.notify_all();
     cv_done.notify_all();
 }
 
-// Joins the threads of finished waves (called with mu held; those threads
+// Joins the threads of finished contexts (called with mu held; those threads
 // only return after releasing it).
 void join_finished(crush_server* s) {
     for (int id : s->finished)
@@ -217,52 +344,37 @@ void join_finished(crush_server* s) {
     s->finished.clear();
 }
 
-void join_finished(crush_server* s);
-
+// Opens a context when requests wait that no open context takes: none is
+// accepting (room spent) or none of their schedule class runs, within the
+// context and HBM limits.
 void crush_server::schedule() {
     std::unique_lock<std::mutex> lk(mu);
     for (;;) {
-        cv_work.wait(lk, [&] { return stop || !finished.empty() || (!queue.empty() && active < cfg.max_waves); });
+        cv_work.wait_for(lk, std::chrono::milliseconds(5));
         join_finished(this);
-        if (queue.empty()) {
-            if (stop) break;
-            continue;
+        if (stop && queue.empty()) break;
+        if (queue.empty() || active >= cfg.max_waves) continue;
+        // Classes that an accepting context serves take their requests
+        // themselves; a request of another class (or with every context
+        // full) opens a context.
+        const Request& head = queue.front();
+        if (accepting[head.check_key] > 0) continue;
+        // While other contexts run, give arrivals a moment to join this one.
+        if (active > 0 && cfg.gather_ms > 0.0) {
+            cv_work.wait_for(lk, std::chrono::duration<double, std::milli>(cfg.gather_ms));
+            if (queue.empty() || accepting[queue.front().check_key] > 0) continue;
         }
-        if (active >= cfg.max_waves) continue;
-        // While the GPU is busy, give arrivals a moment to join this wave.
-        if (active > 0 && cfg.gather_ms > 0.0 && !stop) {
-            cv_work.wait_for(lk, std::chrono::duration<double, std::milli>(cfg.gather_ms), [&] { return stop; });
-            if (queue.empty()) continue;
-        }
-        // Form a wave from the head of the queue: same step schedule, within
-        // the slot, element and memory limits.
-        const int key = queue.front().check_key;
-        std::vector<Request> wave;
-        double bytes = 0.0;
-        int64_t elements = 0;
-        for (auto it = queue.begin(); it != queue.end() && (int)wave.size() < cfg.max_wave_slots;) {
-            const bool fits = in_use + bytes + it->bytes <= budget && elements + it->elements <= cfg.max_wave_elements;
-            if (it->check_key == key && (fits || (wave.empty() && active == 0))) {
-                bytes += it->bytes;
-                elements += it->elements;
-                wave.push_back(std::move(*it));
-                it = queue.erase(it);
-            } else if (!fits && it->check_key == key) {
-                break;  // keep arrival order within a schedule class
-            } else {
-                ++it;
-            }
-        }
-        if (wave.empty()) {
-            // The head does not fit while other waves hold memory: wait for one to finish.
-            cv_work.wait(lk, [&] { return stop || active == 0 || in_use + queue.front().bytes <= budget; });
-            continue;
-        }
+        const crush_capacity room = room_within(cfg.max_wave_elements, cfg.max_wave_slots, budget - in_use, queue.front().elements);
+        const double bytes = room_bytes(room);
+        if (in_use + bytes > budget && active > 0) continue;  // wait for a context to finish
+        std::vector<Request> first = take(queue.front().check_key, room.hexes, room.slots, true);
+        if (first.empty()) continue;
         in_use += bytes;
         peak = std::max(peak, in_use);
         ++active;
-        const int id = (int)waves++;
-        workers.emplace_back(id, std::thread(&crush_server::run_wave, this, std::move(wave), id, bytes));
+        ++accepting[first.front().check_key];
+        const int id = (int)contexts++;
+        workers.emplace_back(id, std::thread(&crush_server::run_context, this, std::move(first), id, bytes, room));
     }
 }
 
@@ -275,11 +387,12 @@ int crush_server_create(const crush_server_config* config, crush_server** out) {
     crush_server_config c{};
     c.device = 0;
     c.max_waves = 4;
-    c.max_wave_slots = 2048;
+    c.max_wave_slots = 1024;
     c.chunk_steps = 100;
-    c.max_wave_elements = 8000000;
+    c.max_wave_elements = 2000000;
     c.hbm_budget_bytes = 0.0;
     c.gather_ms = 2.0;
+    c.idle_ms = 200.0;
     if (config) {
         c.device = config->device;
         if (config->max_waves > 0) c.max_waves = config->max_waves;
@@ -288,6 +401,7 @@ int crush_server_create(const crush_server_config* config, crush_server** out) {
         if (config->max_wave_elements > 0) c.max_wave_elements = config->max_wave_elements;
         if (config->hbm_budget_bytes > 0.0) c.hbm_budget_bytes = config->hbm_budget_bytes;
         if (config->gather_ms >= 0.0) c.gather_ms = config->gather_ms;
+        if (config->idle_ms > 0.0) c.idle_ms = config->idle_ms;
     }
     s->cfg = c;
     if (c.hbm_budget_bytes > 0.0) {
@@ -346,7 +460,7 @@ int crush_server_stats_get(crush_server* s, crush_server_stats* out) {
     std::lock_guard<std::mutex> lk(s->mu);
     out->submitted = s->submitted;
     out->completed = s->completed;
-    out->waves = s->waves;
+    out->waves = s->contexts;
     out->queued = (int64_t)s->queue.size();
     out->running = s->active;
     out->bytes_in_use = s->in_use;

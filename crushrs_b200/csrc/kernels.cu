@@ -2034,7 +2034,7 @@ void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeAr
     const int do_grid = bk1 > bk0 && !ca.exhaustive ? 1 : 0;
     // Every search starts from clear grid bookkeeping (levels in use, entry
     // cursors, big-face list), whatever ran before it.
-    cudaMemsetAsync(ca.grid_state, 0, sizeof(int) * (2 * (size_t)ca.n_contacts + 1), s);
+    cudaMemsetAsync(ca.grid_state, 0, sizeof(int) * (2 * (size_t)ca.contact_room + 1), s);
     if (n_list > 0)
         k_contact_faces<<<active_grid(n_list, FACE_LANES, FACE_TPB, GRID_CAP), FACE_TPB, 0, s>>>(ca, nd, ctls, c0, list, n_list,
                                                                                                run_mode, do_grid, act);

@@ -127,7 +127,8 @@ struct ContactArrays {
     int* blen;                  // per bucket: length of its range
     const long long* ent_off;   // n_contacts+1: entry capacity ranges (faces x LEVEL_CELL_BUDGET)
     int* ent_cursor;            // per contact: entries allocated this step
-    int* grid_state;            // levels_used (n_contacts), ent_cursor (n_contacts), big_count (1): cleared per search
+    int* grid_state;            // levels_used (contact_room), ent_cursor (contact_room), big_count (1): cleared per search
+    long long contact_room;     // contacts the per-contact arrays have room for (>= n_contacts)
     FaceCells* cells;           // per face: its cells this search (faces of contacts with a dynamic grid)
     int* entries;               // local face indices
     uint32_t* big_faces;        // this search's big faces (global index), capacity big_cap

@@ -18,10 +18,10 @@ from .native import check, lib
 class Server:
     """crush_server: waves of batched contexts on one GPU."""
 
-    def __init__(self, device=0, max_waves=4, max_wave_slots=2048, chunk_steps=100, max_wave_elements=8_000_000,
-                 hbm_budget_bytes=0.0, gather_ms=2.0):
+    def __init__(self, device=0, max_waves=4, max_wave_slots=1024, chunk_steps=100, max_wave_elements=2_000_000,
+                 hbm_budget_bytes=0.0, gather_ms=2.0, idle_ms=200.0):
         self._lib = lib()
-        cfg = abi.ServerConfig(device, max_waves, max_wave_slots, chunk_steps, max_wave_elements, hbm_budget_bytes, gather_ms)
+        cfg = abi.ServerConfig(device, max_waves, max_wave_slots, chunk_steps, max_wave_elements, hbm_budget_bytes, gather_ms, idle_ms)
         h = C.c_void_p()
         check(self._lib.crush_server_create(C.byref(cfg), C.byref(h)))
         self.h = h
@@ -78,6 +78,49 @@ def partition_by_footprint(descs, parts):
         out[g].append(i)
         load[g] += sizes[i]
     return [sorted(x) for x in out]
+
+
+def route_online(sizes, parts):
+    """Placement of a stream of crashes across `parts` GPUs as they arrive:
+    each goes to the GPU with the fewest estimated device bytes placed so far
+    (ties: the lower index). Every rank computes the same placement from the
+    same seeded stream, so each serves its share with no exchange of
+    requests. Returns the GPU of every crash, in arrival order."""
+    load = [0.0] * parts
+    out = []
+    for x in sizes:
+        g = min(range(parts), key=lambda q: (load[q], q))
+        out.append(g)
+        load[g] += x
+    return out
+
+
+def serve_share(server, models, rate, rank, parts, seed=1):
+    """This rank's share of an open-loop stream served across `parts` GPUs:
+    the full stream's arrival times are drawn on every rank (same seed), and
+    the rank submits the crashes route_online places on it at their arrival
+    times. Returns (results by stream index, wall seconds)."""
+    sizes = [footprint(m.desc) for m in models]
+    mine = [i for i, g in enumerate(route_online(sizes, parts)) if g == rank]
+    rng = _Rng(seed)
+    times, t = [], 0.0
+    for _ in models:
+        times.append(t)
+        t += -math.log(1.0 - rng.uniform()) / rate
+    t0 = time.perf_counter()
+    tickets, results, i = {}, {}, 0
+    while i < len(mine) or len(results) < len(mine):
+        now = time.perf_counter() - t0
+        while i < len(mine) and times[mine[i]] <= now:
+            tickets[server.submit(models[mine[i]].desc)] = mine[i]
+            i += 1
+        for r in server.poll(wait_ms=0 if i < len(mine) else 20):
+            results[tickets[r.ticket]] = r
+        if i < len(mine):
+            sleep = times[mine[i]] - (time.perf_counter() - t0)
+            if sleep > 0:
+                time.sleep(min(sleep, 0.002))
+    return results, time.perf_counter() - t0
 
 
 def open_loop(server, models, rate, seed=1):

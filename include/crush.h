@@ -432,6 +432,11 @@ int crush_batch_create_reserved(const crush_model_desc* const* descs, int n, int
  * context's, or a context recording histories or frames. Synchronises the
  * context's stream. */
 int crush_batch_append(crush_ctx* ctx, const crush_model_desc* const* descs, int n, int* first_slot);
+/* Issues n_steps steps of the open run on the context's stream and returns
+ * without waiting for them (crush_run_steps is this plus the wait and the
+ * done flags). Host work done after it, a crush_batch_append's set-up of new
+ * slots included, overlaps the steps on the device. */
+int crush_run_issue(crush_ctx* ctx, int64_t n_steps);
 
 /* ---- allocation-free contact call ----
  *

@@ -3,13 +3,18 @@
  *
  * No counterpart in the reference, which runs one crash per process
  * (src/bin/crushrs.rs:30). Requests (whole crash models) are submitted from
- * any thread and answered asynchronously. A scheduler thread groups waiting
- * requests into waves and starts each wave as a batched context
- * (crush_batch_create) on its own CUDA stream and host thread as soon as the
- * wave fits the HBM budget and a wave slot is free, so waves that start while
- * others run overlap on the device. Every crash is reported the moment its
- * own stop rule ends it (the wave's other crashes run on), and its results
- * are bit-identical to crush_create + crush_run of the same model alone.
+ * any thread and answered asynchronously. Each serving context is a batched
+ * context with room for more crashes (crush_batch_create_reserved), driven
+ * in chunks of steps on its own CUDA stream and host thread; between chunks
+ * it admits the requests waiting for it into its running batch
+ * (crush_batch_append, the new crashes' set-up overlapping the chunk just
+ * issued), so a request starts within one chunk of its arrival while the
+ * others keep running. A scheduler thread opens a context when requests wait
+ * that no open context takes (every context's room spent, or another
+ * schedule class) and the HBM budget has room; contexts run side by side on
+ * the device. Every crash is reported the moment its own stop rule ends it,
+ * and its results are bit-identical to crush_create + crush_run of the same
+ * model alone.
  */
 #ifndef CRUSH_SERVER_H
 #define CRUSH_SERVER_H
@@ -26,26 +31,28 @@ typedef struct crush_server crush_server;
 
 typedef struct crush_server_config {
     int32_t device;
-    int32_t max_waves;          /* waves running at once (default 4) */
-    int32_t max_wave_slots;     /* crashes per wave (default 2048) */
-    int32_t chunk_steps;        /* steps between completion checks of a wave (default 100) */
-    int64_t max_wave_elements;  /* elements per wave (default 8,000,000) */
-    double hbm_budget_bytes;    /* device memory the waves may hold together (0 = 80% of free memory) */
-    double gather_ms;           /* while a wave runs, wait this long for more arrivals before starting the next (default 2) */
+    int32_t max_waves;          /* serving contexts running at once (default 4) */
+    int32_t max_wave_slots;     /* crashes a context takes over its life (its slot room, default 1024) */
+    int32_t chunk_steps;        /* steps between admissions and completion checks (a multiple of 20, default 100;
+                                   20 while requests wait) */
+    int64_t max_wave_elements;  /* hexahedra a context takes over its life (its element room, default 2,000,000) */
+    double hbm_budget_bytes;    /* device memory the contexts may hold together (0 = 80% of free memory) */
+    double gather_ms;           /* while contexts run, a new context waits this long for more arrivals (default 2) */
+    double idle_ms;             /* a context with no crash running waits this long for requests before it ends (default 200) */
 } crush_server_config;
 
 typedef struct crush_server_result {
     uint64_t ticket;
     int32_t status;             /* CRUSH_OK, CRUSH_ERR_NONFINITE, or the error that stopped the wave */
-    int32_t wave;               /* index of the wave that ran it */
+    int32_t wave;               /* index of the serving context that ran it */
     double submit_s;            /* server clock (s since creation) at submit */
-    double start_s;             /* wave start (its context creation began) */
+    double start_s;             /* admitted into its context's run */
     double finish_s;            /* result available */
     crush_results results;
 } crush_server_result;
 
 typedef struct crush_server_stats {
-    int64_t submitted, completed, waves, queued, running;
+    int64_t submitted, completed, waves, queued, running;  /* waves: serving contexts opened; running: contexts running */
     double bytes_in_use, peak_bytes_in_use, budget_bytes;
 } crush_server_stats;
 

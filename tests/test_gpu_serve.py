@@ -1,7 +1,8 @@
-"""The crash server on the GPU: crashes submitted at random times are run in
-waves that overlap on the device, and each result equals the same model run
-alone (bit-identical f64 results; added_mass_max to 1e-12 relative, as in
-test_gpu_batch.py)."""
+"""The crash server on the GPU: crashes submitted at random times are
+admitted into running serving contexts (continuous batching) and into
+contexts that overlap on the device, and each result equals the same model
+run alone (bit-identical f64 results; added_mass_max to 1e-12 relative, as
+in test_gpu_batch.py)."""
 import pytest
 
 from crushrs_b200 import scenarios as S
@@ -40,9 +41,11 @@ def test_served_results_equal_alone(queries, alone):
     waves = {}
     for r in results.values():
         waves.setdefault(r.wave, []).append(r)
-    # waves overlapped in time
+    # contexts overlapped in time
     spans = sorted((min(x.start_s for x in v), max(x.finish_s for x in v)) for v in waves.values())
     assert any(spans[i + 1][0] < spans[i][1] for i in range(len(spans) - 1))
+    # crashes joined a context while others of it were running
+    assert any(b.start_s > a.start_s and b.start_s < a.finish_s for v in waves.values() for a in v for b in v)
 
 
 def test_admission_respects_the_memory_budget(queries, alone):

@@ -66,3 +66,82 @@ def test_footprint_split_is_balanced_and_complete():
         loads = [sum(sizes[i] for i in p) for p in split]
         assert max(loads) - min(loads) <= max(sizes)  # largest first onto the least loaded
         assert split == partition_by_footprint(descs, parts)
+
+
+class _FakeServer:
+    """Stands in for a crush_server on CPU: every submitted crash finishes at
+    once with its ticket as the result."""
+
+    def __init__(self):
+        self.pending = []
+        self.next = 1
+
+    def submit(self, desc):
+        t = self.next
+        self.next += 1
+        self.pending.append(t)
+        return t
+
+    def poll(self, wait_ms=0):
+        class R:
+            pass
+
+        out = []
+        for t in self.pending:
+            r = R()
+            r.ticket = t
+            r.submit_s = r.start_s = r.finish_s = 0.0
+            out.append(r)
+        self.pending = []
+        return out
+
+
+def _serve_rank(rank, world, port, out):
+    os.environ.update({"RANK": str(rank), "LOCAL_RANK": str(rank), "WORLD_SIZE": str(world), "MASTER_ADDR": "127.0.0.1",
+                       "MASTER_PORT": str(port)})
+    import bench
+    import torch
+    import torch.distributed as dist
+
+    w, r, _ = bench.dist_setup(backend="gloo")
+    from crushrs_b200 import scenarios as S
+    from crushrs_b200.serve import serve_share
+
+    models = [S.Model.build(S.serve_query(i, e_range=(300, 2000))[1]) for i in range(40)]
+    res, _ = serve_share(_FakeServer(), models, rate=4000.0, rank=r, parts=w, seed=5)
+    # the only exchange: which stream indices each rank served, gathered on the host
+    mine = torch.zeros(len(models), dtype=torch.int64)
+    for i in res:
+        mine[i] = r + 1
+    dist.all_reduce(mine)
+    out[r] = (sorted(res), mine.tolist())
+    dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_serve_disjoint_shares_of_one_stream():
+    """Multi-GPU serving: two ranks draw the same seeded stream, each serves
+    the crashes the online router places on it, and together they serve
+    every crash exactly once."""
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_serve_rank, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    a, b = out[0], out[1]
+    assert a[1] == b[1]  # both ranks see the same ownership after the gather
+    assert set(a[0]).isdisjoint(b[0]) and sorted(a[0] + b[0]) == list(range(40))
+    assert all(x in (1, 2) for x in a[1])
+    assert abs(len(a[0]) - len(b[0])) <= 8  # balanced by estimated bytes
+
+
+def test_online_router_is_least_loaded_and_deterministic():
+    from crushrs_b200.serve import route_online
+
+    sizes = [5.0, 1.0, 1.0, 3.0, 2.0, 2.0]
+    assert route_online(sizes, 2) == [0, 1, 1, 1, 0, 1]
+    assert route_online(sizes, 2) == route_online(list(sizes), 2)
+    assert route_online(sizes, 1) == [0] * 6
