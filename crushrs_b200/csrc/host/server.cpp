@@ -264,8 +264,21 @@ void crush_server::run_context(std::vector<Request> first, int id, double bytes,
                 });
                 if (!got || stop) break;
             }
-            if (open) batch = take(key, room.hexes - used, room.slots - (int)slots.size(), false);
+            if (open) {
+                batch = take(key, room.hexes - used, room.slots - (int)slots.size(), false);
+                // A request of this class waits that does not fit the room
+                // left: this context takes no more, so the scheduler opens
+                // another for it.
+                bool waits = false;
+                for (auto& q : queue) waits = waits || q.check_key == key;
+                if (batch.empty() && waits) {
+                    --accepting[key];
+                    open = false;
+                    cv_work.notify_all();
+                }
+            }
         }
+        if (running == 0 && batch.empty()) continue;  // nothing on the device, nothing admitted
         // Requests are waiting: short chunks, so the next admission comes soon.
         const bool waiting = !batch.empty();
         if (running > 0) st = crush_run_issue(ctx, waiting ? 20 : chunk);
