@@ -302,9 +302,9 @@ class Tuning(C.Structure):
         ("slave_lanes", C.c_int32),
         ("forces_schedule", C.c_int32),
         ("fused_contact_side", C.c_int32),
-        ("reserved", C.c_int32),
+        ("step_fusion", C.c_int32),
         ("contact_ms", C.c_double * 6),
-        ("step_ms", C.c_double * 3),
+        ("step_ms", C.c_double * 5),
     ]
 
 

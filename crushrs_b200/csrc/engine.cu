@@ -47,7 +47,15 @@ namespace {
     } while (0)
 
 const double INF = std::numeric_limits<double>::infinity();
-constexpr int N_FORCES_SCHEDULES = 3;  // launch_forces schedules 0, 1, 2
+constexpr int N_FORCES_SCHEDULES = 4;  // launch_forces schedules 0-3
+// Step schedules the trial chooses from: (fused steps, element-kernel schedule).
+struct SchedCand {
+    bool fused;
+    int forces;
+};
+constexpr int N_CANDS = 5;
+constexpr SchedCand CANDS[N_CANDS] = {{false, 0}, {false, 2}, {false, 3}, {true, 2}, {true, 0}};
+constexpr int DEFAULT_CAND = 3;  // without a trial (small contexts): fused steps, 8 SMs left to the side streams
 const unsigned long long INF_BITS = 0x7ff0000000000000ull;
 
 // HoneycombParams::from_material with Plasticity::check (src/material.rs:116-151, :430-449).
@@ -422,7 +430,7 @@ struct crush_ctx {
     // run
     bool run_open = false;
     long long host_step = 0;
-    bool step_fusion = true;     // fused full + next half step where no check or record falls between
+    bool step_fusion = CANDS[DEFAULT_CAND].fused;  // fused full + next half step where no check or record falls between
     bool prologue_done = false;  // the last issued step was fused: the next step's contact forces and half step ran
     long long pen_stride = 1;    // penetration counters: two sets (even and odd steps) of this many
     int period = 20;
@@ -442,14 +450,15 @@ struct crush_ctx {
     bool frames_on = false, frames_ran = false;
     std::vector<void*> frame_bufs;
     cudaGraphExec_t graph = nullptr;      // step graph of the current element-kernel schedule
-    cudaGraphExec_t graphs[N_FORCES_SCHEDULES] = {};  // per schedule, kept while the schedules are tried
+    cudaGraphExec_t graphs[N_CANDS + 1] = {};  // per trial candidate (the last: schedules set by the caller)
+    int cand = DEFAULT_CAND;              // the trial's choice
     int n_sms = 148;
-    int forces_schedule = 0;              // launch_forces schedule (0 persistent wave, 1 block per chunk, 2 wave on fewer SMs)
+    int forces_schedule = CANDS[DEFAULT_CAND].forces;  // launch_forces schedule (0 persistent wave, 1 block per chunk, 2/3 wave on fewer SMs)
     bool fused_contact_side = false;      // a fused step's next contact forces on the side stream (else main, after the forces)
     unsigned* forces_queue = nullptr;     // device: chunk queue of the persistent element-kernel waves
-    bool tuning_fixed = false;            // set by crush_set_tuning: no automatic re-tuning
+    bool tuning_fixed = false;            // set by crush_set_tuning / crush_set_step_fusion: no automatic re-tuning
     bool sched_trial_pending = false;     // time the schedules at the next graph launches
-    double sched_ms[N_FORCES_SCHEDULES] = {};  // measured ms per step of the step graph under each schedule
+    double sched_ms[N_CANDS] = {};        // measured ms per step of the step graph under each candidate
     int64_t graph_launches = 0;
     bool profiling = false;
     int prof_level = 2;  // 1: events around the element-force kernel only; 2: every phase
@@ -2506,35 +2515,42 @@ int build_graph(crush_ctx* c) {
 
 // The step graph of element-kernel schedule `schedule`, built if missing
 // (the other schedule's graph is kept for switching back).
-int select_schedule(crush_ctx* c, int schedule) {
-    c->forces_schedule = schedule;
-    c->graph = c->graphs[schedule];
+int select_schedule(crush_ctx* c, int cand) {
+    int slot = N_CANDS;  // schedules the caller set
+    if (!c->tuning_fixed) {
+        c->cand = cand;
+        c->step_fusion = CANDS[cand].fused;
+        c->forces_schedule = CANDS[cand].forces;
+        c->fused_contact_side = false;
+        slot = cand;
+    }
+    c->graph = c->graphs[slot];
     if (!c->graph) {
         int64_t before = c->launches;
         int st = build_graph(c);
         if (st != CRUSH_OK) return st;
-        c->graphs[schedule] = c->graph;
+        c->graphs[slot] = c->graph;
         c->graph_launches = c->launches - before;
         c->launches = before;
     }
     return CRUSH_OK;
 }
 
-// Schedule trial: 2 x N_FORCES_SCHEDULES graph periods of the run's own
-// steps, cycling through the element-kernel schedules (all compute the same
-// bits), each timed by events on the stream (every schedule's graph is built
-// first, so no host work falls between them); the fastest is kept.
+// Schedule trial: 2 x N_CANDS graph periods of the run's own steps, cycling
+// through the candidate step schedules (all compute the same bits), each
+// timed by events on the stream (every candidate's graph is built first, so
+// no host work falls between them); the fastest is kept.
 int schedule_trial(crush_ctx* c) {
     c->sched_trial_pending = false;
-    const int keep = c->forces_schedule;
+    const int keep = c->cand;
     int st = CRUSH_OK;
-    for (int k = 0; k < N_FORCES_SCHEDULES && st == CRUSH_OK; ++k) st = select_schedule(c, k);
+    for (int k = 0; k < N_CANDS && st == CRUSH_OK; ++k) st = select_schedule(c, k);
     if (st != CRUSH_OK) return st;
-    constexpr int RUNS = 2 * N_FORCES_SCHEDULES;
+    constexpr int RUNS = 2 * N_CANDS;
     cudaEvent_t ev[RUNS + 1];
     for (auto& e : ev) CK(cudaEventCreate(&e));
     for (int k = 0; k < RUNS && st == CRUSH_OK; ++k) {
-        st = select_schedule(c, k % N_FORCES_SCHEDULES);
+        st = select_schedule(c, k % N_CANDS);
         if (st != CRUSH_OK) break;
         CK(cudaEventRecord(ev[k], c->stream));
         CK(cudaGraphLaunch(c->graph, c->stream));
@@ -2544,14 +2560,14 @@ int schedule_trial(crush_ctx* c) {
     if (st == CRUSH_OK) {
         CK(cudaEventRecord(ev[RUNS], c->stream));
         CK(cudaEventSynchronize(ev[RUNS]));
-        double ms[N_FORCES_SCHEDULES] = {};
+        double ms[N_CANDS] = {};
         for (int k = 0; k < RUNS; ++k) {
             float x = 0.f;
             cudaEventElapsedTime(&x, ev[k], ev[k + 1]);
-            ms[k % N_FORCES_SCHEDULES] += x / (2.0 * c->period);
+            ms[k % N_CANDS] += x / (2.0 * c->period);
         }
         int best = keep;
-        for (int k = 0; k < N_FORCES_SCHEDULES; ++k) {
+        for (int k = 0; k < N_CANDS; ++k) {
             c->sched_ms[k] = ms[k];
             if (ms[k] < ms[best]) best = k;
         }
@@ -2577,12 +2593,12 @@ int issue_steps(crush_ctx* c, long long n_steps) {
             c->sched_trial_pending = c->n_hc >= SCHED_TRIAL_MIN_ELEMENTS;
         }
         const bool use_graph = c->period > 0 && c->host_step % c->period == 0 && n_steps - issued >= c->period && !c->prologue_done;
-        if (use_graph && c->sched_trial_pending && !c->tuning_fixed && n_steps - issued >= 2 * N_FORCES_SCHEDULES * (long long)c->period) {
+        if (use_graph && c->sched_trial_pending && !c->tuning_fixed && n_steps - issued >= 2 * N_CANDS * (long long)c->period) {
             st = schedule_trial(c);
             if (st != CRUSH_OK) return st;
-            issued += 2 * N_FORCES_SCHEDULES * (long long)c->period;
+            issued += 2 * N_CANDS * (long long)c->period;
         } else if (use_graph) {
-            st = select_schedule(c, c->forces_schedule);
+            st = select_schedule(c, c->cand);
             if (st != CRUSH_OK) return st;
             CK(cudaGraphLaunch(c->graph, c->stream));
             c->launches += c->graph_launches;
@@ -3266,7 +3282,8 @@ int crush_get_tuning(const crush_ctx* c, crush_tuning* out) {
     out->forces_schedule = c->forces_schedule;
     out->fused_contact_side = c->fused_contact_side ? 1 : 0;
     for (int k = 0; k < 6; ++k) out->contact_ms[k] = c->tune_ms[k];
-    for (int k = 0; k < N_FORCES_SCHEDULES; ++k) out->step_ms[k] = c->sched_ms[k];
+    out->step_fusion = c->step_fusion ? 1 : 0;
+    for (int k = 0; k < N_CANDS; ++k) out->step_ms[k] = c->sched_ms[k];
     return CRUSH_OK;
 }
 
@@ -3276,7 +3293,7 @@ int crush_set_tuning(crush_ctx* c, const crush_tuning* t) {
     if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
         return crush::fail(CRUSH_ERR_INVALID, "slave_lanes must be 1, 2, 4, 8, 16 or 32");
     if (t->forces_schedule < 0 || t->forces_schedule >= N_FORCES_SCHEDULES)
-        return crush::fail(CRUSH_ERR_INVALID, "forces_schedule must be 0, 1 or 2");
+        return crush::fail(CRUSH_ERR_INVALID, "forces_schedule must be 0, 1, 2 or 3");
     if (t->fused_contact_side != 0 && t->fused_contact_side != 1) return crush::fail(CRUSH_ERR_INVALID, "fused_contact_side must be 0 or 1");
     if (lanes != c->slave_lanes || t->forces_schedule != c->forces_schedule || (t->fused_contact_side == 1) != c->fused_contact_side)
         drop_graphs(c);
@@ -3300,6 +3317,9 @@ int crush_set_contact_search(crush_ctx* c, int exhaustive) {
 
 int crush_set_step_fusion(crush_ctx* c, int fused) {
     if (!c || (fused != 0 && fused != 1)) return crush::fail(CRUSH_ERR_INVALID, "fused must be 0 or 1");
+    c->tuning_fixed = true;
+    c->tuned = true;
+    c->sched_trial_pending = false;
     if (c->step_fusion != (fused == 1)) {
         c->step_fusion = fused == 1;
         drop_graphs(c);

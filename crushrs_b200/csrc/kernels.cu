@@ -701,7 +701,10 @@ __global__ void k_full(ElementArrays el, NodeArrays nd, Control* ctls) {
 // its step count or end time, the next step's v½ = v + ½dt' (f_ext' - f_int)/m
 // and u += dt' v½ with the next step's dt' and contact forces f_ext'. The
 // arithmetic is that of full_body followed by half_body; fixed DOFs are zero
-// as there. A crash that stops here keeps u and v½ of this step.
+// as there. A crash that stops here keeps u and v½ of this step. Neither v
+// nor f_int is read before the next full update rewrites them (the next
+// half step is done here; a step followed by a check or record is never
+// fused), so they are stored only for a crash that stops here.
 __device__ __forceinline__ void fused_body(const ElementArrays& el, const NodeArrays& nd, const Control* ctls, long long n, int d) {
     if (n >= nd.n) return;
     const long long k = 3 * n + d;
@@ -715,9 +718,11 @@ __device__ __forceinline__ void fused_body(const ElementArrays& el, const NodeAr
     const double dt = step_dt(ctl);
     const double a = (fe - f) * im;
     const double v = fixed ? 0.0 : (vh + 0.5 * dt * a) * ctl->damping;
-    nd.v[k] = v;
-    nd.f_int[k] = f;
-    if (last_step_by_count_or_time(ctl)) return;
+    if (last_step_by_count_or_time(ctl)) {
+        nd.v[k] = v;
+        nd.f_int[k] = f;
+        return;
+    }
     const double dt1 = next_step_dt(ctl);
     const double a1 = (fe1 - f) * im;
     double vh1 = v + 0.5 * dt1 * a1;
@@ -1959,13 +1964,12 @@ void launch_forces(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd
     // Schedule 0, persistent: one wave of FORCES_MINB blocks per SM taking
     // chunks from the queue (no tail). Schedule 1: a block per chunk, so
     // blocks retire all along and work on other streams (the next step's
-    // contact pass) gets SMs while the kernel runs. Schedule 2: the
-    // persistent wave on all but FORCES_FREE_SMS SMs, which stay free for
-    // the side streams. Without a queue, schedules 0 and 2 stride instead.
-    constexpr int FORCES_FREE_SMS = 8;
-    long long cap = (long long)n_sms * FORCES_MINB;
+    // contact pass) gets SMs while the kernel runs. Schedule 2 (3): the
+    // persistent wave on all but 8 (16) SMs, which stay free for the side
+    // streams' search. Without a queue, the persistent waves stride instead.
+    const int free_sms = schedule == 2 ? 8 : schedule == 3 ? 16 : 0;
+    long long cap = (long long)(n_sms > 2 * free_sms ? n_sms - free_sms : n_sms) * FORCES_MINB;
     if (schedule == 1) cap = GRID_CAP * 4;
-    if (schedule == 2) cap = (long long)(n_sms > 2 * FORCES_FREE_SMS ? n_sms - FORCES_FREE_SMS : n_sms) * FORCES_MINB;
     unsigned* q = schedule == 1 ? nullptr : queue;
     if (el.n_hc > 0)
         k_forces<<<active_grid(el.n_hc, 1, FORCES_TPB, cap), FORCES_TPB, 0, s>>>(el, nd, ctls, respect_done, q);

@@ -230,8 +230,8 @@ void launch_init_state(cudaStream_t s, long long h_begin, long long n_hc, long l
 // Element forces: the honeycomb lane kernel and, when the model has
 // elastic elements, the scalar f64 kernel (forces_launches of them).
 // schedule: 0 = one persistent wave of blocks on the n_sms SMs, 1 = a block
-// per chunk of 256 elements, 2 = the persistent wave on all but 8 SMs; all
-// compute the same bits. queue (two zeroed unsigned, left zero): the
+// per chunk of 256 elements, 2 (3) = the persistent wave on all but 8 (16)
+// SMs; all compute the same bits. queue (two zeroed unsigned, left zero): the
 // persistent waves take chunks from it (null: they stride).
 void launch_forces(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, int respect_done, int n_sms = 148,
                    int schedule = 0, unsigned* queue = nullptr);

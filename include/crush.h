@@ -257,13 +257,14 @@ int crush_contact_search_stats(crush_ctx* ctx, int contact_id, uint64_t* out, in
  * Both give the same hits: the grids only skip faces that cannot pass the
  * narrow test. For checking that equality; takes effect at the next step. */
 int crush_set_contact_search(crush_ctx* ctx, int exhaustive);
-/* fused = 1 (default) runs a step whose next step starts with no stable-dt
+/* fused = 1 runs a step whose next step starts with no stable-dt
  * check, record or reduction stop rule as one pass over the nodes (the
  * step's full update and the next step's half step), with the next step's
  * contact forces computed beside this step's element forces; 0 runs every
  * step's half and full updates as separate passes. Both give bit-identical
  * results (for checking that, and for timing the schedules); takes effect
- * at the next step. No counterpart in the reference. */
+ * at the next step and turns the automatic schedule choice off (see
+ * crush_autotune). No counterpart in the reference. */
 int crush_set_step_fusion(crush_ctx* ctx, int fused);
 
 /* ---- Time histories: part states and accelerometer samples ----
@@ -352,19 +353,21 @@ int crush_resample(const double* t, const double* y, int64_t n, double t0, doubl
 typedef struct crush_tuning {
     int32_t slave_lanes;         /* lanes per primary-node search */
     int32_t forces_schedule;     /* element kernel: 0 one persistent wave of blocks taking chunks from a queue,
-                                    1 a block per 256 elements, 2 the persistent wave on all but 8 SMs */
+                                    1 a block per 256 elements, 2 (3) the persistent wave on all but 8 (16) SMs */
     int32_t fused_contact_side;  /* a fused step computes the next step's contact forces 1: on a side stream
                                     beside its element forces, 0: on the main stream after them */
-    int32_t reserved;
+    int32_t step_fusion;         /* fused steps (read only; crush_set_step_fusion sets it) */
     double contact_ms[6];        /* measured contact pass with 1, 2, 4, 8, 16, 32 lanes (0 = not measured) */
-    double step_ms[3];           /* measured ms per step of the step graph with each forces_schedule (0 = not measured) */
+    double step_ms[5];           /* measured ms per step of the step graph under the trial's candidates (separate
+                                    passes, forces_schedule 0 / 2 / 3; fused steps, 2 / 0); 0 = not measured */
 } crush_tuning;
 /* Re-tune now, at the open run's current state (e.g. late in a crash, when
  * crushed faces change the search); the next step uses the new schedule.
- * The element kernel's schedule is tuned on the run's own steps: a run of a
- * context of 65,536+ hexahedra times the three schedules over its first six
- * step graphs (and again every 1000 steps, with the lanes) and keeps the
- * fastest. */
+ * The step schedule is tuned on the run's own steps: a run of a context of
+ * 65,536+ hexahedra times five candidates (separate or fused steps, and how
+ * many SMs the element kernel leaves to the side streams) over its first ten
+ * step graphs, again every 1000 steps with the lanes, and keeps the fastest;
+ * smaller contexts take fused steps with 8 SMs left free. */
 int crush_autotune(crush_ctx* ctx, crush_tuning* out);
 int crush_get_tuning(const crush_ctx* ctx, crush_tuning* out);
 /* Fixes the schedule to t's slave_lanes, forces_schedule and
