@@ -55,7 +55,10 @@ struct SchedCand {
 };
 constexpr int N_CANDS = 5;
 constexpr SchedCand CANDS[N_CANDS] = {{false, 0}, {false, 2}, {false, 3}, {true, 2}, {true, 0}};
-constexpr int DEFAULT_CAND = 3;  // without a trial (small contexts): fused steps, 8 SMs left to the side streams
+// Without a trial (small contexts, short issues): separate passes with 8 SMs
+// left to the side streams, the fastest measured on one small crash and on
+// the 278k-element head-on (fused steps win only on large batches).
+constexpr int DEFAULT_CAND = 1;
 const unsigned long long INF_BITS = 0x7ff0000000000000ull;
 
 // HoneycombParams::from_material with Plasticity::check (src/material.rs:116-151, :430-449).

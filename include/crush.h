@@ -367,7 +367,7 @@ typedef struct crush_tuning {
  * 65,536+ hexahedra times five candidates (separate or fused steps, and how
  * many SMs the element kernel leaves to the side streams) over its first ten
  * step graphs, again every 1000 steps with the lanes, and keeps the fastest;
- * smaller contexts take fused steps with 8 SMs left free. */
+ * smaller contexts take separate steps with 8 SMs left free. */
 int crush_autotune(crush_ctx* ctx, crush_tuning* out);
 int crush_get_tuning(const crush_ctx* ctx, crush_tuning* out);
 /* Fixes the schedule to t's slave_lanes, forces_schedule and
