@@ -303,6 +303,7 @@ class Tuning(C.Structure):
         ("forces_schedule", C.c_int32),
         ("fused_contact_side", C.c_int32),
         ("step_fusion", C.c_int32),
+        ("early_contact", C.c_int32),
         ("contact_ms", C.c_double * 6),
         ("step_ms", C.c_double * 5),
     ]

@@ -52,13 +52,14 @@ constexpr int N_FORCES_SCHEDULES = 4;  // launch_forces schedules 0-3
 struct SchedCand {
     bool fused;
     int forces;
+    bool early;  // separate steps: the next step's contact forces beside this step's element forces
 };
 constexpr int N_CANDS = 5;
-constexpr SchedCand CANDS[N_CANDS] = {{false, 0}, {false, 2}, {false, 3}, {true, 2}, {true, 0}};
+constexpr SchedCand CANDS[N_CANDS] = {{false, 2, false}, {false, 3, false}, {false, 2, true}, {false, 3, true}, {true, 2, false}};
 // Without a trial (small contexts, short issues): separate passes with 8 SMs
 // left to the side streams, the fastest measured on one small crash and on
 // the 278k-element head-on (fused steps win only on large batches).
-constexpr int DEFAULT_CAND = 1;
+constexpr int DEFAULT_CAND = 0;
 const unsigned long long INF_BITS = 0x7ff0000000000000ull;
 
 // HoneycombParams::from_material with Plasticity::check (src/material.rs:116-151, :430-449).
@@ -435,6 +436,8 @@ struct crush_ctx {
     long long host_step = 0;
     bool step_fusion = CANDS[DEFAULT_CAND].fused;  // fused full + next half step where no check or record falls between
     bool prologue_done = false;  // the last issued step was fused: the next step's contact forces and half step ran
+    bool early_contact = CANDS[DEFAULT_CAND].early;  // separate steps compute the next step's contact forces beside the forces
+    bool contact_done = false;   // the next step's contact forces ran beside the last issued step's element forces
     long long pen_stride = 1;    // penetration counters: two sets (even and odd steps) of this many
     int period = 20;
     int base_period = 20;            // the graph period without time histories
@@ -1927,11 +1930,16 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
     mark(1);
     // Contact forces of this step from the search run beside the previous
     // step's forces (or at crush_run_begin for the first step).
-    if (!pre && c->n_contacts > 0) {
+    if (!pre && c->n_contacts > 0 && !c->contact_done) {
         launch_contact_finish(c->stream, cr, nd, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0.0, c->mass, nd.f_ext, 1,
                               c->side2, c->ev_heavy, c->ev_heavy_done, c->ev_gathered);
         n += contact_finish_launches(c->n_slaves);
     }
+    c->contact_done = false;
+    // A separate step computes the next step's contact forces beside its
+    // element forces when the next step has no stable-dt check (its dt is
+    // then next_step_dt) and is issued with this one.
+    const bool early = !fuse && c->early_contact && c->n_contacts > 0 && !last && !(c->adaptive && (step + 1) % c->check_steps == 0);
     mark(2);
     if (!pre) {
         launch_half(c->stream, nd, c->ctls);
@@ -1950,7 +1958,7 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
         launch_contact_search(c->side, cn, nn, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 1,
                               c->slave_lanes, c->side2);
         n += contact_search_launches(c->ca, true, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 0);
-        if (fuse && c->fused_contact_side) {
+        if ((fuse && c->fused_contact_side) || early) {
             cudaEventRecord(c->ev_static, c->side2);
             cudaStreamWaitEvent(c->side, c->ev_static, 0);
             launch_contact_finish(c->side, cn, nn, c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0.0, c->mass, nn.f_ext, 1,
@@ -2009,6 +2017,12 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
         launch_vehicle_vx(c->stream, c->va, c->mass, c->v, c->ctls);
         ++n;
     }
+    if (early) {
+        // the side streams' contact pass read this step's time: it ends
+        // before the step's end moves it on
+        cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+        cudaStreamWaitEvent(c->stream, c->ev_join2, 0);
+    }
     launch_step_end(c->stream, c->ctls, cr, c->va, sep ? 1 : 0, c->slot_done, c->mass_flag);
     ++n;
     // Time-history records of the slots whose step is a multiple of
@@ -2029,6 +2043,7 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
         cudaStreamWaitEvent(c->stream, c->ev_join2, 0);
     }
     c->prologue_done = false;
+    c->contact_done = early;
     mark(6);
     return check_launch(c, n);
 }
@@ -2323,6 +2338,7 @@ int run_begin(crush_ctx* c) {
     CK(cudaMemsetAsync(c->added, 0, sizeof(double) * N, c->stream));
     CK(cudaMemsetAsync(c->fused_counter, 0, sizeof(unsigned), c->stream));
     c->prologue_done = false;
+    c->contact_done = false;
     if (c->n_contacts > 0) {
         CK(cudaMemsetAsync(c->ca.big_best, 0x7F, sizeof(int) * std::max<long long>(c->n_slaves, 1), c->stream));  // BIG_NONE
         CK(cudaMemsetAsync(c->ca.pen_count, 0, sizeof(unsigned long long) * 2 * c->pen_stride, c->stream));
@@ -2504,9 +2520,10 @@ int build_graph(crush_ctx* c) {
         st = enqueue_step(c, k, c->profiling ? &c->prof_ev[(size_t)k * N_PHASE_EVENTS] : nullptr, true);
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
     if (st != CRUSH_OK) return st;
-    if (c->prologue_done) {  // the period's last step is never fused (it rebuilds the active lists)
+    if (c->prologue_done || c->contact_done) {  // the period's last step has a stable-dt check next: never fused nor early
         cudaGraphDestroy(g);
         c->prologue_done = false;
+        c->contact_done = false;
         return crush::fail(CRUSH_ERR_INVALID, "step graph period ends on a fused step");
     }
     if (e != cudaSuccess) return crush::fail(CRUSH_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
@@ -2524,6 +2541,7 @@ int select_schedule(crush_ctx* c, int cand) {
         c->cand = cand;
         c->step_fusion = CANDS[cand].fused;
         c->forces_schedule = CANDS[cand].forces;
+        c->early_contact = CANDS[cand].early;
         c->fused_contact_side = false;
         slot = cand;
     }
@@ -2595,7 +2613,8 @@ int issue_steps(crush_ctx* c, long long n_steps) {
             c->last_tune_step = c->host_step;
             c->sched_trial_pending = c->n_hc >= SCHED_TRIAL_MIN_ELEMENTS;
         }
-        const bool use_graph = c->period > 0 && c->host_step % c->period == 0 && n_steps - issued >= c->period && !c->prologue_done;
+        const bool use_graph = c->period > 0 && c->host_step % c->period == 0 && n_steps - issued >= c->period && !c->prologue_done &&
+                               !c->contact_done;
         if (use_graph && c->sched_trial_pending && !c->tuning_fixed && n_steps - issued >= 2 * N_CANDS * (long long)c->period) {
             st = schedule_trial(c);
             if (st != CRUSH_OK) return st;
@@ -2783,7 +2802,7 @@ int crush_batch_create_reserved(const crush_model_desc* const* descs, int n, int
 int crush_batch_append(crush_ctx* c, const crush_model_desc* const* descs, int n, int* first_slot) {
     if (!c) return crush::fail(CRUSH_ERR_INVALID, "null context");
     CK(cudaSetDevice(c->device));
-    if (c->prologue_done) return crush::fail(CRUSH_ERR_INVALID, "slots join an open run only between issues of steps");
+    if (c->prologue_done || c->contact_done) return crush::fail(CRUSH_ERR_INVALID, "slots join an open run only between issues of steps");
     const int first = c->n_slots;
     int st = add_slots(c, descs, n, false, nullptr);
     if (st != CRUSH_OK) return st;
@@ -3286,6 +3305,7 @@ int crush_get_tuning(const crush_ctx* c, crush_tuning* out) {
     out->fused_contact_side = c->fused_contact_side ? 1 : 0;
     for (int k = 0; k < 6; ++k) out->contact_ms[k] = c->tune_ms[k];
     out->step_fusion = c->step_fusion ? 1 : 0;
+    out->early_contact = c->early_contact ? 1 : 0;
     for (int k = 0; k < N_CANDS; ++k) out->step_ms[k] = c->sched_ms[k];
     return CRUSH_OK;
 }
@@ -3298,8 +3318,11 @@ int crush_set_tuning(crush_ctx* c, const crush_tuning* t) {
     if (t->forces_schedule < 0 || t->forces_schedule >= N_FORCES_SCHEDULES)
         return crush::fail(CRUSH_ERR_INVALID, "forces_schedule must be 0, 1, 2 or 3");
     if (t->fused_contact_side != 0 && t->fused_contact_side != 1) return crush::fail(CRUSH_ERR_INVALID, "fused_contact_side must be 0 or 1");
-    if (lanes != c->slave_lanes || t->forces_schedule != c->forces_schedule || (t->fused_contact_side == 1) != c->fused_contact_side)
+    if (t->early_contact != 0 && t->early_contact != 1) return crush::fail(CRUSH_ERR_INVALID, "early_contact must be 0 or 1");
+    if (lanes != c->slave_lanes || t->forces_schedule != c->forces_schedule || (t->fused_contact_side == 1) != c->fused_contact_side ||
+        (t->early_contact == 1) != c->early_contact)
         drop_graphs(c);
+    c->early_contact = t->early_contact == 1;
     c->slave_lanes = lanes;
     c->forces_schedule = t->forces_schedule;
     c->fused_contact_side = t->fused_contact_side == 1;

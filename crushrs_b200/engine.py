@@ -179,12 +179,13 @@ class Context:
         check(self._lib.crush_get_tuning(self.h, C.byref(t)))
         return t.forces_schedule, list(t.step_ms)
 
-    def set_tuning(self, slave_lanes, forces_schedule, fused_contact_side=0):
+    def set_tuning(self, slave_lanes, forces_schedule, fused_contact_side=0, early_contact=0):
         """Fix the launch schedule (automatic tuning off)."""
         t = abi.Tuning()
         t.slave_lanes = slave_lanes
         t.forces_schedule = forces_schedule
         t.fused_contact_side = fused_contact_side
+        t.early_contact = early_contact
         check(self._lib.crush_set_tuning(self.h, C.byref(t)))
 
     def autotune(self):

@@ -357,21 +357,25 @@ typedef struct crush_tuning {
     int32_t fused_contact_side;  /* a fused step computes the next step's contact forces 1: on a side stream
                                     beside its element forces, 0: on the main stream after them */
     int32_t step_fusion;         /* fused steps (read only; crush_set_step_fusion sets it) */
+    int32_t early_contact;       /* separate steps compute the next step's contact forces beside their element
+                                    forces when the next step has no stable-dt check */
     double contact_ms[6];        /* measured contact pass with 1, 2, 4, 8, 16, 32 lanes (0 = not measured) */
-    double step_ms[5];           /* measured ms per step of the step graph under the trial's candidates (separate
-                                    passes, forces_schedule 0 / 2 / 3; fused steps, 2 / 0); 0 = not measured */
+    double step_ms[5];           /* measured ms per step of the step graph under the trial's candidates: separate
+                                    steps with forces_schedule 2 / 3, the same with early contact forces, fused
+                                    steps with 2; 0 = not measured */
 } crush_tuning;
 /* Re-tune now, at the open run's current state (e.g. late in a crash, when
  * crushed faces change the search); the next step uses the new schedule.
  * The step schedule is tuned on the run's own steps: a run of a context of
- * 65,536+ hexahedra times five candidates (separate or fused steps, and how
- * many SMs the element kernel leaves to the side streams) over its first ten
+ * 65,536+ hexahedra times five candidates (separate steps leaving 8 or 16
+ * SMs of the element kernel's wave to the side streams, with or without the
+ * next step's contact forces computed there; fused steps) over its first ten
  * step graphs, again every 1000 steps with the lanes, and keeps the fastest;
  * smaller contexts take separate steps with 8 SMs left free. */
 int crush_autotune(crush_ctx* ctx, crush_tuning* out);
 int crush_get_tuning(const crush_ctx* ctx, crush_tuning* out);
-/* Fixes the schedule to t's slave_lanes, forces_schedule and
- * fused_contact_side (measured fields ignored) and turns automatic tuning off for this context. Every
+/* Fixes the schedule to t's slave_lanes, forces_schedule,
+ * fused_contact_side and early_contact (measured fields ignored) and turns automatic tuning off for this context. Every
  * schedule gives the same results. */
 int crush_set_tuning(crush_ctx* ctx, const crush_tuning* t);
 

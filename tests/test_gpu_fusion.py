@@ -86,7 +86,7 @@ def test_every_launch_schedule_gives_the_same_bits():
     schedules on its first step graphs) does too."""
     m = S.Model.build(S.refined_headon(max_steps=200))
     out = []
-    for tuning in ((32, 0, 0), (8, 1, 1), (4, 2, 0), None):
+    for tuning in ((32, 0, 0, 0), (8, 1, 1, 1), (4, 2, 0, 1), (16, 3, 0, 0), None):
         ctx = Context(m.desc)
         if tuning is not None:
             ctx.set_tuning(*tuning)
