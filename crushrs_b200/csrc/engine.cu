@@ -28,6 +28,9 @@
 #include <numeric>
 #include <string>
 #include <vector>
+#include <new>
+#include <type_traits>
+#include <sys/mman.h>
 
 #include "crush.h"
 #include "host/errors.hpp"
@@ -673,20 +676,46 @@ struct Trace {
 };
 
 // A host array left uninitialised on allocation (large set-up arrays are
-// written in full by the per-slot passes, so zeroing them first is waste).
+// written in full by the per-slot passes, so zeroing them first is waste,
+// and their pages are first touched by those passes' threads, not by one).
+// Arrays of 2 MB and more sit on 2 MB boundaries with transparent huge
+// pages requested: a batched set-up writes gigabytes of them, and 4 KB page
+// faults cost it more than the writes.
 template <typename T>
 struct Buf {
-    std::unique_ptr<T[]> p;
+    static_assert(std::is_trivially_copyable<T>::value, "plain data only");
+    static constexpr size_t HUGE_PAGE = size_t(2) << 20;
+    T* p = nullptr;
     size_t n = 0;
+    Buf() = default;
+    explicit Buf(size_t m) { alloc(m); }
+    Buf(const Buf&) = delete;
+    Buf& operator=(const Buf&) = delete;
+    ~Buf() { std::free(p); }
     void alloc(size_t m) {
-        p.reset(new T[m ? m : 1]);
+        std::free(p);
+        p = nullptr;
+        size_t bytes = sizeof(T) * (m ? m : 1);
+        if (bytes >= HUGE_PAGE) {
+            bytes = (bytes + HUGE_PAGE - 1) / HUGE_PAGE * HUGE_PAGE;
+            p = static_cast<T*>(std::aligned_alloc(HUGE_PAGE, bytes));
+            if (p) madvise(p, bytes, MADV_HUGEPAGE);
+        } else {
+            p = static_cast<T*>(std::malloc(bytes));
+        }
+        if (!p) throw std::bad_alloc();
         n = m;
     }
-    T* data() { return p.get(); }
-    const T* data() const { return p.get(); }
+    T* data() { return p; }
+    const T* data() const { return p; }
     T& operator[](size_t i) { return p[i]; }
     const T& operator[](size_t i) const { return p[i]; }
     size_t size() const { return n; }
+    bool empty() const { return n == 0; }
+    T* begin() { return p; }
+    T* end() { return p + n; }
+    const T* begin() const { return p; }
+    const T* end() const { return p + n; }
 };
 
 // Combined host arrays of the slots being added: node, element and part
@@ -834,6 +863,17 @@ void build_contacts(const crush_model_desc* d, const Slot& sl, const Combined& c
         int face;   // >= 0: local face index
     };
     std::vector<RoleItem> items;
+    {
+        size_t nf = 0, nn = 0;
+        for (int k = 0; k < d->n_contacts; ++k) {
+            nf += (size_t)std::max<int64_t>(d->contacts[k].n_faces, 0);
+            nn += (size_t)std::max<int64_t>(d->contacts[k].n_nodes, 0);
+        }
+        cp.faces.reserve(4 * nf);
+        cp.slaves.reserve(nn);
+        cp.scales.reserve(nn);
+        items.reserve(nn + 4 * nf);
+    }
     int seq = 0;
     for (int k = 0; k < d->n_contacts; ++k) {
         const crush_contact& cd = d->contacts[k];
@@ -926,13 +966,16 @@ void build_contacts(const crush_model_desc* d, const Slot& sl, const Combined& c
             if (ok) cp.box.insert(cp.box.end(), box, box + 6);
             if (ok) {
                 st = next_pow2(std::max<size_t>(16, 2 * ins.size()));
-                std::vector<uint32_t> cnt(st + 1, 0);
-                for (auto& e : ins) cnt[(e.first & (st - 1)) + 1]++;
-                for (size_t b2 = 0; b2 < st; ++b2) cnt[b2 + 1] += cnt[b2];
+                const size_t o0 = cp.st_off.size();
+                cp.st_off.resize(o0 + st + 1, 0);
+                uint32_t* off = cp.st_off.data() + o0;  // counts, then bucket starts, then the entry cursors
+                for (auto& e : ins) off[(e.first & (st - 1)) + 1]++;
+                for (size_t b2 = 0; b2 < st; ++b2) off[b2 + 1] += off[b2];
                 cp.st_entries.resize(base + ins.size());
-                std::vector<uint32_t> cur(cnt.begin(), cnt.end() - 1);
-                for (auto& e : ins) cp.st_entries[base + cur[e.first & (st - 1)]++] = e.second;  // faces ascending in a bucket
-                for (size_t b2 = 0; b2 <= st; ++b2) cp.st_off.push_back(base + cnt[b2]);
+                for (auto& e : ins) cp.st_entries[base + off[e.first & (st - 1)]++] = e.second;  // faces ascending in a bucket
+                // the cursors end at the next bucket's start: shift back, and offset by base
+                for (size_t b2 = st; b2 > 0; --b2) off[b2] = base + off[b2 - 1];
+                off[0] = base;
             } else {
                 st = 0;
                 cp.st_off.push_back(base);
@@ -970,9 +1013,20 @@ void build_contacts(const crush_model_desc* d, const Slot& sl, const Combined& c
         cp.md.push_back(cd.max_distance);
         cp.cell.push_back(cs);
     }
-    std::sort(items.begin(), items.end(), [](const RoleItem& x, const RoleItem& y) {
-        return x.node != y.node ? x.node < y.node : (x.contact != y.contact ? x.contact < y.contact : x.seq < y.seq);
-    });
+    // Items were made in (contact, seq) order: a stable counting sort by node
+    // gives the (node, contact, seq) order.
+    {
+        std::vector<uint32_t> cnt((size_t)d->n_nodes + 1, 0);
+        for (const RoleItem& it : items) cnt[it.node - n0 + 1]++;
+        for (size_t i = 0; i < (size_t)d->n_nodes; ++i) cnt[i + 1] += cnt[i];
+        std::vector<RoleItem> sorted(items.size());
+        for (const RoleItem& it : items) sorted[cnt[it.node - n0]++] = it;
+        items.swap(sorted);
+    }
+    cp.cnode.reserve(items.size());
+    cp.cnode_off.reserve(items.size() + 1);
+    cp.crole_contact.reserve(items.size());
+    cp.crole_slave.reserve(items.size());
     for (size_t i0 = 0; i0 < items.size();) {
         size_t i1 = i0;
         while (i1 < items.size() && items[i1].node == items[i0].node) ++i1;
@@ -1123,8 +1177,8 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
     }
     if (8 * (unsigned long long)(E0 + E) >= (unsigned long long)HC_ELL_MORE)
         return crush::fail(CRUSH_ERR_INVALID, "too many hexahedra for 32-bit node incidence entries (8 x elements must stay below 2^32 - 2)");
-    std::vector<int64_t> hc_index(E), sc_index(E);
-    std::vector<uint32_t> hc_model(H), sc_model(Q), sc_list(QF);
+    Buf<int64_t> hc_index(E), sc_index(E);
+    Buf<uint32_t> hc_model(H), sc_model(Q), sc_list(QF);
     Buf<uint32_t> all_off, hc_off, all_slot, hc_slot, sc_off, sc_slot, hc_ell;
     all_off.alloc(N + 1);
     hc_off.alloc(N + 1);
@@ -1206,6 +1260,7 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
     parallel_for(n_desc, [&](long long k) { build_contacts(descs[k], slots[k], cm, parts[k], errs[k]); });
     for (auto& e : errs)
         if (e.code != CRUSH_OK) return crush::fail(e.code, e.msg);
+    trace.mark("contact runtimes per slot");
     struct Base {
         long long face, slave, ste, stoff, dyn, grid, cnode, role;
     };
@@ -1228,6 +1283,10 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
         }
     }
     const Base& tot = base[n_desc];
+    if (trace.on)
+        std::fprintf(stderr, "[crush] new contact tables: faces %lld, entries %lld, static-grid entries %lld, offsets %lld, contact nodes %lld, roles %lld\n",
+                     tot.face - base[0].face, tot.slave - base[0].slave, tot.ste - base[0].ste, tot.stoff - base[0].stoff,
+                     tot.cnode - base[0].cnode, tot.role - base[0].role);
     if (tot.face >= (1ll << 31) || tot.slave >= (1ll << 31) || tot.ste >= (1ll << 32) || tot.role >= (1ll << 32) ||
         tot.cnode >= (long long)CN_FIXED)
         return crush::fail(CRUSH_ERR_INVALID, "contacts too large for one context");
@@ -1272,16 +1331,18 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
     // ---- contact arrays of the new slots (global values) ----
     std::vector<int> face_off(K + 1), slave_off(K + 1), tab_off(K + 1), counts_for_stop(K), contact_slot(K), slot_contact_off(n_desc + 1);
     std::vector<long long> st_tab_off(K + 1), ent_off(K + 1);
-    std::vector<int> face_contact(tot.face - base[0].face), slave_contact(tot.slave - base[0].slave);
-    std::vector<uint32_t> faces(4 * (tot.face - base[0].face)), slaves(tot.slave - base[0].slave), dyn_faces(tot.dyn - base[0].dyn),
+    // written in full by the per-slot pass below
+    Buf<int> face_contact(tot.face - base[0].face), slave_contact(tot.slave - base[0].slave);
+    Buf<uint32_t> faces(4 * (tot.face - base[0].face)), slaves(tot.slave - base[0].slave), dyn_faces(tot.dyn - base[0].dyn),
         grid_faces(tot.grid - base[0].grid);
-    std::vector<double> scales(slaves.size()), stiff(K), md(K), cell(K), st_box(6 * (size_t)std::max(K, 1));
+    Buf<double> scales(slaves.size());
+    std::vector<double> stiff(K), md(K), cell(K), st_box(6 * (size_t)std::max(K, 1));
     std::vector<uint8_t> is_static(K);
-    std::vector<uint32_t> st_off(tot.stoff - base[0].stoff);
-    std::vector<int> st_entries(tot.ste - base[0].ste);
-    std::vector<uint32_t> cnode(tot.cnode - base[0].cnode), cnode_off(tot.cnode - base[0].cnode + 1);
-    std::vector<int> crole_contact(tot.role - base[0].role), crole_slave(tot.role - base[0].role);
-    std::vector<uint32_t> slave_cn(slaves.size()), face_cn(faces.size());
+    Buf<uint32_t> st_off(tot.stoff - base[0].stoff);
+    Buf<int> st_entries(tot.ste - base[0].ste);
+    Buf<uint32_t> cnode(tot.cnode - base[0].cnode), cnode_off(tot.cnode - base[0].cnode + 1);
+    Buf<int> crole_contact(tot.role - base[0].role), crole_slave(tot.role - base[0].role);
+    Buf<uint32_t> slave_cn(slaves.size()), face_cn(faces.size());
     face_off[0] = (int)base[0].face;
     slave_off[0] = (int)base[0].slave;
     tab_off[0] = (int)c->ca.n_buckets;
@@ -1330,18 +1391,23 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
         for (size_t j = 1; j < cp.cnode_off.size(); ++j) cnode_off[b.cnode - base[0].cnode + j] = cp.cnode_off[j] + (uint32_t)b.role;
         std::copy(cp.crole_contact.begin(), cp.crole_contact.end(), crole_contact.begin() + (b.role - base[0].role));
         std::copy(cp.crole_slave.begin(), cp.crole_slave.end(), crole_slave.begin() + (b.role - base[0].role));
-        auto cn_of = [&](uint32_t node) {  // the slot's contact nodes are in ascending node order, and include it
-            const auto it = std::lower_bound(cp.cnode.begin(), cp.cnode.end(), node);
-            if (it == cp.cnode.end() || *it != node) {
+        // the slot's contact nodes (ascending node order): node -> their index
+        const long long n0 = slots[k].node0;
+        std::vector<uint32_t> at((size_t)descs[k]->n_nodes, UINT32_MAX);
+        for (size_t j = 0; j < cp.cnode.size(); ++j) at[cp.cnode[j] - n0] = (uint32_t)j;
+        auto cn_of = [&](uint32_t node) {
+            const uint32_t j = at[node - n0];
+            if (j == UINT32_MAX) {
                 cn_missing = true;  // cannot happen: every primary node and face corner has a role
                 return 0u;
             }
-            return (uint32_t)(b.cnode + (it - cp.cnode.begin())) | (fixed_at(node) ? CN_FIXED : 0u);
+            return (uint32_t)(b.cnode + j) | (fixed_at(node) ? CN_FIXED : 0u);
         };
         for (size_t j = 0; j < cp.slaves.size(); ++j) slave_cn[b.slave - s0 + j] = cn_of(cp.slaves[j]);
         for (size_t j = 0; j < cp.faces.size(); ++j) face_cn[4 * (b.face - f0) + j] = cn_of(cp.faces[j]);
     });
     if (cn_missing) return crush::fail(CRUSH_ERR_INVALID, "internal: a contact node without a role");
+    trace.mark("contact tables concatenated");
     // exhaustive contacts (no grid) get a block each; the rest are listed by entry
     std::vector<int> brute;
     std::vector<uint32_t> gslaves, stslaves;
@@ -1358,40 +1424,59 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
             for (int e = slave_off[q]; e < slave_off[q + 1]; ++e) (st_grid ? stslaves : gslaves).push_back((uint32_t)e);
         }
     }
-    // ---- vehicles ----
-    std::vector<long long> voff;
-    std::vector<uint32_t> vnodes;
-    std::vector<int> vslot, vlocal;
+    trace.mark("contact entry lists");
+    // ---- vehicles: per slot its ranges, then the node lists filled in parallel ----
+    std::vector<long long> vh_off(n_desc + 1, 0), vn_off(n_desc + 1, 0), cn_off(n_desc + 1, 0);
     long long max_vnodes = c->max_vnodes;
-    std::vector<uint32_t> crush_nodes_new;
-    std::vector<size_t> crush_off_new;
     for (int k = 0; k < n_desc; ++k) {
         const crush_model_desc* d = descs[k];
-        const long long n0 = slots[k].node0;
-        slots[k].vehicle0 = c->va.n_vehicles + (int)vslot.size();
         const int nv = std::min(d->n_vehicles, 4);
+        slots[k].vehicle0 = c->va.n_vehicles + (int)vh_off[k];
         slots[k].n_vehicles = nv;
+        long long vn = 0, cn = 0;
         for (int v = 0; v < nv; ++v) {
             const crush_vehicle& vd = d->vehicles[v];
             if (vd.n_nodes < 0 || (vd.n_nodes > 0 && !vd.nodes) || vd.n_front < 0 || (vd.n_front > 0 && !vd.front_nodes))
                 return crush::fail(CRUSH_ERR_INVALID, "invalid vehicle");
-            for (int64_t i = 0; i < vd.n_nodes; ++i) {
-                if (vd.nodes[i] >= (uint64_t)d->n_nodes) return crush::fail(CRUSH_ERR_INVALID, "vehicle node out of range");
-                vnodes.push_back((uint32_t)(n0 + vd.nodes[i]));
-            }
-            max_vnodes = std::max<long long>(max_vnodes, vd.n_nodes);
-            voff.push_back(c->n_vnodes + (long long)vnodes.size());
             if (vd.accel_node >= (uint64_t)d->n_nodes) return crush::fail(CRUSH_ERR_INVALID, "accelerometer node out of range");
-            for (int64_t i = 0; i < vd.n_front; ++i) {
-                if (vd.front_nodes[i] >= (uint64_t)d->n_nodes) return crush::fail(CRUSH_ERR_INVALID, "front node out of range");
-                crush_nodes_new.push_back((uint32_t)(n0 + vd.front_nodes[i]));
-            }
-            crush_nodes_new.push_back((uint32_t)(n0 + vd.accel_node));
-            crush_off_new.push_back(crush_nodes_new.size());
-            vslot.push_back(S0 + k);
-            vlocal.push_back(v);
+            vn += vd.n_nodes;
+            cn += vd.n_front + 1;
+            max_vnodes = std::max<long long>(max_vnodes, vd.n_nodes);
         }
+        vh_off[k + 1] = vh_off[k] + nv;
+        vn_off[k + 1] = vn_off[k] + vn;
+        cn_off[k + 1] = cn_off[k] + cn;
     }
+    // voff: each vehicle's end in the context's vehicle-node list; crush_off_new:
+    // its end in the new crush-measure node list (front nodes, then the accelerometer)
+    std::vector<long long> voff(vh_off[n_desc]);
+    std::vector<size_t> crush_off_new(vh_off[n_desc]);
+    std::vector<int> vslot(vh_off[n_desc]), vlocal(vh_off[n_desc]);
+    Buf<uint32_t> vnodes(vn_off[n_desc]), crush_nodes_new(cn_off[n_desc]);
+    parallel_for(n_desc, [&](long long k) {
+        const crush_model_desc* d = descs[k];
+        const long long n0 = slots[k].node0;
+        long long a = vn_off[k], b = cn_off[k];
+        for (int v = 0; v < slots[k].n_vehicles; ++v) {
+            const crush_vehicle& vd = d->vehicles[v];
+            for (int64_t i = 0; i < vd.n_nodes; ++i) {
+                if (vd.nodes[i] >= (uint64_t)d->n_nodes) return errs[k].set(CRUSH_ERR_INVALID, "vehicle node out of range");
+                vnodes[a++] = (uint32_t)(n0 + vd.nodes[i]);
+            }
+            for (int64_t i = 0; i < vd.n_front; ++i) {
+                if (vd.front_nodes[i] >= (uint64_t)d->n_nodes) return errs[k].set(CRUSH_ERR_INVALID, "front node out of range");
+                crush_nodes_new[b++] = (uint32_t)(n0 + vd.front_nodes[i]);
+            }
+            crush_nodes_new[b++] = (uint32_t)(n0 + vd.accel_node);
+            const long long q = vh_off[k] + v;
+            voff[q] = c->n_vnodes + a;
+            crush_off_new[q] = (size_t)b;
+            vslot[q] = S0 + (int)k;
+            vlocal[q] = v;
+        }
+    });
+    for (auto& e : errs)
+        if (e.code != CRUSH_OK) return crush::fail(e.code, e.msg);
     trace.mark("contacts and vehicles built");
 
     // ---- device arrays: allocated with the room (creating), then the new ranges uploaded ----
