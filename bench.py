@@ -282,13 +282,17 @@ def e2e_run(desc, device, n_hc, n_nodes):
 
 
 def batched_section(n, plain_sample, oracle_sample, device, world=1):
-    """4096 seeded uneven head-on crashes in one batched context vs the plain
-    one-crash-per-launch path. With several ranks the crashes are split by
-    estimated device bytes (serve.partition_by_footprint, the same on every
-    rank) and each rank runs its share as one batched context; the time is
-    the slowest rank's, with no collective on the data path."""
+    """4096 seeded uneven head-on crashes as one batch vs the plain
+    one-crash-per-launch path. The batch runs through crush_batch_solve (the
+    set-up pipelined with the run: later groups of crashes join the open
+    run) and, beside it, as one context created from all crashes before its
+    run (crush_batch_create + crush_batch_run, "one_shot"). With several
+    ranks the crashes are split by estimated device bytes
+    (serve.partition_by_footprint, the same on every rank) and each rank
+    solves its share; the time is the slowest rank's, with no collective on
+    the data path."""
     from crushrs_b200 import scenarios as S
-    from crushrs_b200.engine import Context
+    from crushrs_b200.engine import Context, solve_batch
     from crushrs_b200.serve import partition_by_footprint
 
     all_models = [S.Model.build(S.batch_headon(i)) for i in range(n)]
@@ -305,21 +309,28 @@ def batched_section(n, plain_sample, oracle_sample, device, world=1):
     w.close()
     barrier(world)
     t0 = time.perf_counter()
-    ctx = Context([m.desc for m in models], device=device)
+    rs = solve_batch([m.desc for m in models], device=device)
     t1 = time.perf_counter()
-    rs = ctx.batch_run()
-    t2 = time.perf_counter()
-    lanes, _ = ctx.tuning()
-    launches = ctx.launches()
-    ctx.close()
     steps = [int(r.steps) for r in rs]
     eu = sum(m.n_hexes * st for m, st in zip(models, steps))
     if world > 1:
-        wall = all_max(t2 - t0, world)
+        wall = all_max(t1 - t0, world)
         total_eu = all_sum(eu, world)
         return {"crashes": n, "ranks": world, "crashes_this_rank": len(models), "crashes_per_s": n / wall, "wall_s": wall,
                 "elem_upd_per_s": total_eu / wall, "split": "by estimated device bytes, largest first to the least-loaded rank",
-                "scaling": "strong: the same crashes shared by the ranks"}
+                "scaling": "strong: the same crashes shared by the ranks", "path": "crush_batch_solve per rank"}
+    # the same crashes as one context created from all of them, then run
+    t2 = time.perf_counter()
+    ctx = Context([m.desc for m in models], device=device)
+    t3 = time.perf_counter()
+    rs1 = ctx.batch_run()
+    t4 = time.perf_counter()
+    lanes, _ = ctx.tuning()
+    launches = ctx.launches()
+    ctx.close()
+    fields = lambda r: (r.status, r.steps, r.time, r.dt_min, r.eroded_elements,
+                        [tuple(r.vehicle[k].delta_v) + (r.vehicle[k].crush,) for k in range(r.n_vehicles)])
+    solve_equals_one_shot = all(fields(a) == fields(b) for a, b in zip(rs, rs1))
     # plain path: one context and one run per crash, a sample, after its own warm-up
     times = []
     same = True
@@ -330,15 +341,20 @@ def batched_section(n, plain_sample, oracle_sample, device, world=1):
         c.close()
         times.append(time.perf_counter() - t)
         same &= r.steps == rs[i].steps and list(r.vehicle[0].delta_v) == list(rs[i].vehicle[0].delta_v)
-    batched_cps = n / (t2 - t0)
-    out = {"crashes": n, "elements": elems, "create_s": t1 - t0, "run_s": t2 - t1, "crashes_per_s": batched_cps,
-           "elem_upd_per_s": eu / (t2 - t0), "steps_mean": statistics.mean(steps), "steps_max": max(steps),
-           "gpu_launches": int(launches), "slave_lanes": lanes}
+    batched_cps = n / (t1 - t0)
+    out = {"crashes": n, "elements": elems, "wall_s": t1 - t0, "crashes_per_s": batched_cps,
+           "elem_upd_per_s": eu / (t1 - t0), "steps_mean": statistics.mean(steps), "steps_max": max(steps),
+           "path": "crush_batch_solve: a context from the first sixteenth of the elements starts the run, the rest join it "
+                   "group by group at step-graph boundaries (set-up overlapping the run)",
+           "one_shot": {"create_s": t3 - t2, "run_s": t4 - t3, "crashes_per_s": n / (t4 - t2), "gpu_launches": int(launches),
+                        "slave_lanes": lanes, "path": "crush_batch_create of all crashes, then crush_batch_run"},
+           "solve_equals_one_shot": bool(solve_equals_one_shot)}
     if times:
         plain_s = statistics.median(times)
         out["plain"] = {"crashes_per_s": 1.0 / plain_s, "median_s_per_crash": plain_s, "sample": plain_sample,
                         "path": "crush_create + crush_run per crash (CUDA graphs of 20 steps)"}
         out["speedup_vs_plain"] = batched_cps * plain_s
+        out["one_shot"]["speedup_vs_plain"] = n / (t4 - t2) * plain_s
         out["batched_equals_plain"] = bool(same)
     if oracle_sample:
         from tests import oracle_lib as O
@@ -546,12 +562,13 @@ def main():
     ctx.set_profiling(1)
     ctx.run_steps_timed(args.warmup, phases=True)
     # Untimed steps up to a step-graph boundary (the engine replays one
-    # captured graph per 20 steps), then one whole graph period, so the
-    # graph's capture and instantiation fall before the timed region.
+    # captured graph per 20 steps), then two whole graph periods (an issue
+    # of two periods builds the graph), so the graph's capture and
+    # instantiation fall before the timed region.
     align = (-args.warmup) % 20
-    ctx.run_steps_timed(align + 20, phases=True)
-    first = args.warmup + align + 20
-    config["timed_steps"] = f"steps {first}..{first + args.steps} (warm-up: {args.warmup} steps, then {align + 20} more to a replayed step graph)"
+    ctx.run_steps_timed(align + 40, phases=True)
+    first = args.warmup + align + 40
+    config["timed_steps"] = f"steps {first}..{first + args.steps} (warm-up: {args.warmup} steps, then {align + 40} more to a replayed step graph)"
     barrier(world)
     launches0 = ctx.launches()
     # phase events of the last graph only; the force kernel's average comes
@@ -564,7 +581,7 @@ def main():
     ms_max = all_max(ms, world)
     barrier(world)
     ctx.set_profiling(2)
-    _, _, all_phases, all_psteps = ctx.run_steps_timed(20, phases=True)
+    _, _, all_phases, all_psteps = ctx.run_steps_timed(40, phases=True)
     lanes, tune_ms = ctx.tuning()
     # The same run continued under each step schedule (bit-identical
     # results): separate half and full passes, then the fused one.
@@ -575,7 +592,7 @@ def main():
                             ("fused, block-per-chunk forces", True, 1)):
         ctx.set_step_fusion(fused)
         ctx.set_tuning(lanes, fs)
-        ctx.run_steps_timed(20)
+        ctx.run_steps_timed(40)
         _, ms_s, _, _ = ctx.run_steps_timed(args.schedule_steps)
         schedules[name] = {"ms_per_step": ms_s / args.schedule_steps, "steps": args.schedule_steps}
     value = world * n_hc * args.steps / (ms_max / 1e3)

@@ -217,6 +217,7 @@ def declare_engine_api(lib):
     lib.crush_set_tuning.argtypes = [vp, P(Tuning)]
     lib.crush_batch_create.argtypes = [P(P(ModelDesc)), C.c_int, C.c_int, P(vp)]
     lib.crush_batch_create_reserved.argtypes = [P(P(ModelDesc)), C.c_int, C.c_int, P(Capacity), P(vp)]
+    lib.crush_batch_solve.argtypes = [P(P(ModelDesc)), C.c_int, C.c_int, P(Results)]
     lib.crush_batch_append.argtypes = [vp, P(P(ModelDesc)), C.c_int, P(C.c_int)]
     lib.crush_run_issue.argtypes = [vp, C.c_int64]
     lib.crush_batch_size.argtypes = [vp]

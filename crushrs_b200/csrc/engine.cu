@@ -145,11 +145,12 @@ Capacity capacity_for(const crush_capacity* r, const Capacity& need) {
     // hashed grids: dynamic tables (contacts of 256+ faces: twice the
     // key-box cells rounded up to a power of two, at least 1024 buckets) and
     // their entries (faces x LEVEL_CELL_BUDGET); static tables of the fixed
-    // faces (a road's: about 8 cells per face). Models that need more than
-    // this room are refused with CRUSH_ERR_BUSY.
+    // faces (a road's: about 8 cells per face, a table of twice the cells
+    // rounded up to a power of two). Models that need more than this room are
+    // refused with CRUSH_ERR_BUSY.
     up(c.buckets, 16ll * r->faces + 1024ll * r->contacts);
     up(c.entries, (long long)LEVEL_CELL_BUDGET * r->faces);
-    up(c.st_tabs, 4ll * r->faces + 512ll * r->contacts);
+    up(c.st_tabs, 8ll * r->faces + 1024ll * r->contacts);
     up(c.st_ents, 16ll * r->faces + 256ll * r->contacts);
     up(c.cnodes, r->primary_nodes + 4ll * r->faces);
     up(c.roles, r->primary_nodes + 4ll * r->faces);
@@ -316,7 +317,7 @@ struct Stager {
         return CRUSH_OK;
     }
     void release() {
-        if (s) cudaStreamSynchronize(s);
+        if (s && buf[0]) cudaStreamSynchronize(s);  // the staging buffers' DMA (direct copies are staged on return)
         for (int k = 0; k < 2; ++k) {
             if (buf[k] && !pooled) cudaFreeHost(buf[k]);
             if (ev[k]) cudaEventDestroy(ev[k]);
@@ -465,6 +466,16 @@ struct crush_ctx {
     int forces_schedule = CANDS[DEFAULT_CAND].forces;  // launch_forces schedule (0 persistent wave, 1 block per chunk, 2/3 wave on fewer SMs)
     bool fused_contact_side = false;      // a fused step's next contact forces on the side stream (else main, after the forces)
     unsigned* forces_queue = nullptr;     // device: chunk queue of the persistent element-kernel waves
+    // Slots added to an open run are set up on `setup`, beside the steps
+    // issued last (the set-up writes only the new slots' ranges); the main
+    // stream waits for ev_setup before its next step, and takes the
+    // active-chunk table updates from pinned memory (tab_pinned, free again
+    // once ev_tab has passed).
+    cudaStream_t setup = nullptr;
+    cudaEvent_t ev_setup = nullptr, ev_tab = nullptr;
+    int* tab_pinned = nullptr;
+    size_t tab_pinned_cap = 0;
+    int eager_periods = 0;                // graph periods launched step by step since the graphs were dropped
     bool tuning_fixed = false;            // set by crush_set_tuning / crush_set_step_fusion: no automatic re-tuning
     bool sched_trial_pending = false;     // time the schedules at the next graph launches
     double sched_ms[N_CANDS] = {};        // measured ms per step of the step graph under each candidate
@@ -632,6 +643,11 @@ struct crush_ctx {
         if (ev_heavy_done) cudaEventDestroy(ev_heavy_done);
         if (ev_gathered) cudaEventDestroy(ev_gathered);
         if (ev_static) cudaEventDestroy(ev_static);
+        if (setup) cudaStreamSynchronize(setup);
+        if (ev_setup) cudaEventDestroy(ev_setup);
+        if (ev_tab) cudaEventDestroy(ev_tab);
+        if (tab_pinned) cudaFreeHost(tab_pinned);
+        if (setup) cudaStreamDestroy(setup);
         if (side) cudaStreamDestroy(side);
         if (side2) cudaStreamDestroy(side2);
         if (stream) cudaStreamDestroy(stream);
@@ -650,6 +666,7 @@ int check_launch(crush_ctx* c, int n = 1) {
 // The step graphs (both element-kernel schedules) no longer match the
 // context's launch sequence.
 void drop_graphs(crush_ctx* c) {
+    c->eager_periods = 0;
     for (cudaGraphExec_t& g : c->graphs) {
         if (g) cudaGraphExecDestroy(g);
         g = nullptr;
@@ -1060,7 +1077,9 @@ void append(std::vector<T>& dst, const std::vector<T>& src) {
     dst.insert(dst.end(), src.begin(), src.end());
 }
 
-int begin_slots(crush_ctx* c, int s0, int s1);
+int begin_slots(crush_ctx* c, int s0, int s1, bool search);
+int search_new_contacts(crush_ctx* c, int s0, int s1);
+static void free_bufs(crush_ctx* c, std::vector<void*>& bufs);
 
 // Adds n_desc models as slots [c->n_slots, c->n_slots + n_desc) at the
 // context's current offsets of every entity space. The first call (creating)
@@ -1179,17 +1198,11 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
         return crush::fail(CRUSH_ERR_INVALID, "too many hexahedra for 32-bit node incidence entries (8 x elements must stay below 2^32 - 2)");
     Buf<int64_t> hc_index(E), sc_index(E);
     Buf<uint32_t> hc_model(H), sc_model(Q), sc_list(QF);
-    Buf<uint32_t> all_off, hc_off, all_slot, hc_slot, sc_off, sc_slot, hc_ell;
-    all_off.alloc(N + 1);
-    hc_off.alloc(N + 1);
-    sc_off.alloc(N + 1);
-    all_slot.alloc(8 * E);
-    hc_slot.alloc(8 * H);
-    hc_ell.alloc(8 * (size_t)N);
-    sc_slot.alloc(8 * Q);
+    // Honeycomb and elastic numbering per slot (the node incidence lists are
+    // built on the device from these and the connectivity).
     parallel_for(n_desc, [&](long long k) {
         const Slot& sl = slots[k];
-        const long long n0 = sl.node0, e0 = sl.elem0, nn = sl.n_nodes;
+        const long long e0 = sl.elem0;
         long long h = hc0[k], qf = sc0[k], qx = sc0[k] + slot_free[k], lf = scf0[k];
         for (long long e = e0; e < e0 + sl.n_elems; ++e)
             if (mat_of(e).model == CRUSH_MAT_HONEYCOMB) {
@@ -1205,55 +1218,14 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
                 sc_index[e - E0] = q;
                 sc_model[q - Q0] = (uint32_t)e;
             }
-        // per-node counts, then CSR offsets (global entry positions)
-        std::vector<uint32_t> cnt_a(nn, 0), cnt_b(nn, 0), cnt_c(nn, 0);
-        for (long long e = e0; e < e0 + sl.n_elems; ++e) {
-            const bool honey = hc_index[e - E0] >= 0;
-            for (int i = 0; i < 8; ++i) {
-                const uint32_t n = hex(e, i);
-                cnt_a[n - n0]++;
-                if (honey) cnt_b[n - n0]++;
-                else cnt_c[n - n0]++;
-            }
-        }
-        uint32_t a = (uint32_t)(8 * e0), b = (uint32_t)(8 * hc0[k]), cc = (uint32_t)(8 * sc0[k]);
-        for (long long n = n0; n < n0 + nn; ++n) {
-            all_off[n - N0] = a;
-            hc_off[n - N0] = b;
-            sc_off[n - N0] = cc;
-            a += cnt_a[n - n0];
-            b += cnt_b[n - n0];
-            cc += cnt_c[n - n0];
-        }
-        std::vector<uint32_t> cura(all_off.data() + (n0 - N0), all_off.data() + (n0 - N0) + nn),
-            curb(hc_off.data() + (n0 - N0), hc_off.data() + (n0 - N0) + nn), curc(sc_off.data() + (n0 - N0), sc_off.data() + (n0 - N0) + nn);
-        for (long long e = e0; e < e0 + sl.n_elems; ++e) {
-            const long long he = hc_index[e - E0], se = sc_index[e - E0];
-            for (int i = 0; i < 8; ++i) {
-                const uint32_t n = hex(e, i);
-                all_slot[cura[n - n0]++ - 8 * E0] = (uint32_t)(8 * e + i);
-                if (he >= 0) hc_slot[curb[n - n0]++ - 8 * H0] = (uint32_t)(8 * he + i);
-                else sc_slot[curc[n - n0]++ - 8 * Q0] = (uint32_t)(8 * se + i);
-            }
-        }
-        // the same honeycomb slots as padded rows of 8 (HC_ELL_MORE: the CSR)
-        for (long long n = n0; n < n0 + nn; ++n) {
-            uint32_t* row = &hc_ell[8 * (size_t)(n - N0)];
-            const uint32_t m = cnt_b[n - n0];
-            for (int j = 0; j < 8; ++j) row[j] = (uint32_t)j < m ? hc_slot[hc_off[n - N0] - 8 * H0 + j] : HC_ELL_NONE;
-            if (m > 8) row[0] = HC_ELL_MORE;
-        }
     });
-    all_off[N] = (uint32_t)(8 * (E0 + E));
-    hc_off[N] = (uint32_t)(8 * (H0 + H));
-    sc_off[N] = (uint32_t)(8 * (Q0 + Q));
     std::vector<double> sc_mat(2 * (size_t)std::max<long long>(Q, 1), 0.0);
     for (long long q = 0; q < Q; ++q) {
         const crush_material& m = mat_of(sc_model[q]);
         sc_mat[2 * q] = m.youngs_modulus;
         sc_mat[2 * q + 1] = m.poisson_ratio;
     }
-    trace.mark("node incidence CSR");
+    trace.mark("element numbering");
 
     // ---- contacts: per slot in parallel, then concatenated after the context's ----
     std::vector<ContactPart> parts(n_desc);
@@ -1480,6 +1452,26 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
     trace.mark("contacts and vehicles built");
 
     // ---- device arrays: allocated with the room (creating), then the new ranges uploaded ----
+    // Slots added to an open run are set up on the set-up stream (c->stream
+    // names it until this function returns), beside the steps already
+    // issued on the main stream: their set-up writes only their own ranges.
+    const bool appending = !creating && c->run_open;
+    cudaStream_t main_stream = c->stream;
+    if (appending && !c->setup) {
+        CK(cudaStreamCreateWithFlags(&c->setup, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&c->ev_setup, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c->ev_tab, cudaEventDisableTiming));
+    }
+    struct StreamRestore {
+        crush_ctx* c;
+        cudaStream_t s;
+        bool on;
+        ~StreamRestore() {
+            if (on) c->stream = s;
+        }
+    } restore{c, main_stream, appending};
+    if (appending) c->stream = c->setup;
+    std::vector<std::pair<long long, long long>> tab_ranges;  // appending: chunk-table entries the main stream updates
     Stager stager;
     stager.init(c->stream, sizeof(double) * 6 * N + sizeof(uint32_t) * 27 * E);
     c->stager = &stager;
@@ -1700,13 +1692,6 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
     TRY(put(c->fixed + N0, cm.fixed.data(), N));
     TRY(put(c->node_slot + N0, cm.node_slot.data(), N));
     TRY(put(c->elem_slot + E0, cm.elem_slot.data(), E));
-    TRY(put(c->all_off + N0, all_off.data(), N + 1));
-    TRY(put(c->hc_off + N0, hc_off.data(), N + 1));
-    TRY(put(c->sc_off + N0, sc_off.data(), N + 1));
-    TRY(put(c->all_slot + 8 * E0, all_slot.data(), 8 * E));
-    TRY(put(c->hc_slot + 8 * H0, hc_slot.data(), 8 * H));
-    TRY(put(c->sc_slot + 8 * Q0, sc_slot.data(), 8 * Q));
-    TRY(put(const_cast<uint32_t*>(reinterpret_cast<const uint32_t*>(c->hc_ell)) + 8 * N0, hc_ell.data(), 8 * (size_t)N));
     CK(cudaMemsetAsync(c->eroded_all + E0, 0, E, c->stream));
     trace.mark("model uploads");
     const long long FB = base[0].face, SB = base[0].slave;
@@ -1798,9 +1783,11 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
     va.vx_blocks = (int)std::min<long long>(VX_BLOCKS, std::max<long long>(1, (max_vnodes + 2047) / 2048));
     for (size_t i = 0; i < crush_off_new.size(); ++i) c->crush_off_h.push_back(c->crush_nodes_h.size() + crush_off_new[i]);
     c->crush_nodes_h.insert(c->crush_nodes_h.end(), crush_nodes_new.begin(), crush_nodes_new.end());
+    trace.mark("host copies");
     // the crush-measure node list is small: a new copy of the whole list
     TRY(c->upload(&c->crush_nodes, c->crush_nodes_h.data(), c->crush_nodes_h.size()));
     TRY(c->alloc(&c->crush_ux, std::max<size_t>(c->crush_nodes_h.size(), 1)));
+    trace.mark("crush-measure nodes");
     // ---- active chunk tables: the slot range of every chunk the new entities touch ----
     {
         const long long ends[ACTIVE_SPACES] = {c->n_hc, c->n_all, c->n_nodes, ca.n_grid_slaves, ca.n_cnodes, ca.n_dyn_faces,
@@ -1836,7 +1823,12 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
                 c->chunk_lo_h[q] = a;
                 c->chunk_hi_h[q] = b;
             });
-            if (!creating) {
+            // A chunk the new entities share with running slots is read by
+            // the steps in flight: an append updates the tables in the main
+            // stream's order.
+            if (appending) {
+                tab_ranges.emplace_back(q0, q1);
+            } else if (!creating) {
                 TRY(put(c->chunk_lo_d + q0, c->chunk_lo_h.data() + q0, q1 - q0 + 1));
                 TRY(put(c->chunk_hi_d + q0, c->chunk_hi_h.data() + q0, q1 - q0 + 1));
             }
@@ -1852,6 +1844,22 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
     trace.mark("active chunk tables");
 
     // ---- device set-up of the new elements and nodes ----
+    // node incidence (CSR and padded rows), in scratch returned after the set-up's sync below
+    std::vector<void*> scratch_bufs;
+    {
+        const size_t bytes = incidence_scratch_bytes(E, N);
+        char* scratch = nullptr;
+        const size_t mark = c->allocs.size();
+        TRY(c->alloc(&scratch, bytes));
+        scratch_bufs.assign(c->allocs.begin() + (long)mark, c->allocs.end());
+        uint32_t* ell = const_cast<uint32_t*>(reinterpret_cast<const uint32_t*>(c->hc_ell)) + 8 * N0;
+        if (launch_incidence(c->stream, E0, E, N0, N, c->conn_all, c->hc_index_d, c->sc_index_d, (uint32_t)(8 * E0), (uint32_t)(8 * H0),
+                             (uint32_t)(8 * Q0), c->all_off + N0, c->all_slot, c->hc_off + N0, c->hc_slot, c->sc_off + N0, c->sc_slot,
+                             ell, scratch) != 0)
+            return crush::fail(CRUSH_ERR_CUDA, std::string("node incidence: ") + cudaGetErrorString(cudaGetLastError()));
+        c->launches += 2;
+    }
+    trace.mark("node incidence queued");
     CK(cudaMemsetAsync(c->setup_bad, 0, sizeof(int), c->stream));
     launch_setup_geometry(c->stream, E0, E0 + E, c->pos, c->conn_all, c->part, c->mat4, c->hc_index_d, c->elem_slot, c->stride, c->planes,
                           c->volume, c->lumped, c->dt_factor, c->elem_mass, c->setup_bad, c->sc_index_d, c->sc_stride, c->sc_geo);
@@ -1875,6 +1883,8 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
     TRY(check_launch(c));
     CK(cudaMemcpyAsync(aux.data(), c->ctls_aux + S0, sizeof(Control) * aux.size(), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    trace.mark("device set-up (sync)");
+    free_bufs(c, scratch_bufs);
     if (bad_h == 1) return crush::fail(CRUSH_ERR_INVALID, "degenerate hexahedron (singular Jacobian)");
     if (bad_h == 2) return crush::fail(CRUSH_ERR_INVALID, "hourglass modes not independent");
     parallel_for(n_desc, [&](long long k) {
@@ -1916,8 +1926,39 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
         c->base_period = c->period;
     }
     drop_graphs(c);
-    if (c->run_open) return begin_slots(c, S0, c->n_slots);
-    return CRUSH_OK;
+    if (!c->run_open) return CRUSH_OK;
+    if (!appending) return begin_slots(c, S0, c->n_slots, true);
+    TRY(begin_slots(c, S0, c->n_slots, false));
+    // The main stream: the set-up done, the chunk tables, then the new
+    // contacts' first search (its scratch is shared with the steps').
+    CK(cudaEventRecord(c->ev_setup, c->setup));
+    c->stream = main_stream;
+    restore.on = false;
+    CK(cudaStreamWaitEvent(main_stream, c->ev_setup, 0));
+    size_t n_tab = 0;
+    for (auto& r : tab_ranges) n_tab += (size_t)(r.second - r.first + 1);
+    if (n_tab > 0) {
+        CK(cudaEventSynchronize(c->ev_tab));  // the previous append's copies are done
+        if (2 * n_tab > c->tab_pinned_cap) {
+            if (c->tab_pinned) CK(cudaFreeHost(c->tab_pinned));
+            c->tab_pinned = nullptr;
+            c->tab_pinned_cap = 0;
+            const size_t want = std::max<size_t>(2 * n_tab, 1 << 16);
+            CK(cudaMallocHost(&c->tab_pinned, sizeof(int) * want));
+            c->tab_pinned_cap = want;
+        }
+        int* hp = c->tab_pinned;
+        for (auto& r : tab_ranges) {
+            const size_t n = (size_t)(r.second - r.first + 1);
+            std::memcpy(hp, c->chunk_lo_h.data() + r.first, sizeof(int) * n);
+            std::memcpy(hp + n, c->chunk_hi_h.data() + r.first, sizeof(int) * n);
+            CK(cudaMemcpyAsync(c->chunk_lo_d + r.first, hp, sizeof(int) * n, cudaMemcpyHostToDevice, main_stream));
+            CK(cudaMemcpyAsync(c->chunk_hi_d + r.first, hp + n, sizeof(int) * n, cudaMemcpyHostToDevice, main_stream));
+            hp += 2 * n;
+        }
+        CK(cudaEventRecord(c->ev_tab, main_stream));
+    }
+    return search_new_contacts(c, S0, c->n_slots);
 #undef TRY
 }
 
@@ -2507,8 +2548,10 @@ int run_begin(crush_ctx* c) {
 // forces at u = 0, the static faces' geometry, the element dt pass of their
 // step 0 and the contact search their first step's forces read. They join at
 // the run's current step, a step-graph boundary, so their own steps fall on
-// the same step-schedule positions as alone.
-int begin_slots(crush_ctx* c, int s0, int s1) {
+// the same step-schedule positions as alone. search = false leaves the
+// contact search to search_new_contacts (an append issues it on the main
+// stream) and does not wait for the stream.
+int begin_slots(crush_ctx* c, int s0, int s1, bool search) {
     if (s1 <= s0) return CRUSH_OK;
     const Slot& a = c->slots[s0];
     const Slot& z = c->slots[s1 - 1];
@@ -2571,16 +2614,25 @@ int begin_slots(crush_ctx* c, int s0, int s1) {
         st = check_launch(c);
         if (st != CRUSH_OK) return st;
     }
-    // The first step's contact search of the new contacts at u = 0, contact
-    // by contact (the hits are those any search finds).
+    if (!search) return CRUSH_OK;
+    st = search_new_contacts(c, s0, s1);
+    if (st != CRUSH_OK) return st;
+    return sync(c);
+}
+
+// The first step's contact search of the contacts of slots [s0, s1) at
+// u = 0, contact by contact (the hits are those any search finds).
+int search_new_contacts(crush_ctx* c, int s0, int s1) {
+    if (s1 <= s0) return CRUSH_OK;
+    const int c0 = c->slots[s0].contact0, c1 = c->slots[s1 - 1].contact0 + c->slots[s1 - 1].n_contacts;
     for (int k = c0; k < c1; ++k) {
         const long long nf = c->face_off_h[k + 1] - c->face_off_h[k], ns = c->slave_off_h[k + 1] - c->slave_off_h[k];
         const long long bk0 = c->tab_off_h[k], bk1 = c->tab_off_h[k + 1];
         launch_contact_search(c->stream, c->ca, c->nd(), c->ctls, k, k + 1, c->face_off_h[k], nf, ns, bk0, bk1, 0, c->slave_lanes);
-        st = check_launch(c, contact_search_launches(c->ca, false, nf, ns, bk0, bk1, k));
+        const int st = check_launch(c, contact_search_launches(c->ca, false, nf, ns, bk0, bk1, k));
         if (st != CRUSH_OK) return st;
     }
-    return sync(c);
+    return CRUSH_OK;
 }
 
 int ensure_prof_events(crush_ctx* c) {
@@ -2620,6 +2672,9 @@ int build_graph(crush_ctx* c) {
 
 // The step graph of element-kernel schedule `schedule`, built if missing
 // (the other schedule's graph is kept for switching back).
+// Whether the step graph of the schedule the next issue uses is built.
+bool graph_ready(const crush_ctx* c) { return c->graphs[c->tuning_fixed ? N_CANDS : c->cand] != nullptr; }
+
 int select_schedule(crush_ctx* c, int cand) {
     int slot = N_CANDS;  // schedules the caller set
     if (!c->tuning_fixed) {
@@ -2698,8 +2753,15 @@ int issue_steps(crush_ctx* c, long long n_steps) {
             c->last_tune_step = c->host_step;
             c->sched_trial_pending = c->n_hc >= SCHED_TRIAL_MIN_ELEMENTS;
         }
-        const bool use_graph = c->period > 0 && c->host_step % c->period == 0 && n_steps - issued >= c->period && !c->prologue_done &&
-                               !c->contact_done;
+        // A graph that is not built yet is built for an issue of two periods
+        // or more, or at the second period since the graphs were dropped:
+        // the first single period after slots joined is launched step by
+        // step, which costs the host less than capturing and instantiating a
+        // graph that the next join drops.
+        const bool boundary = c->period > 0 && c->host_step % c->period == 0 && n_steps - issued >= c->period && !c->prologue_done &&
+                              !c->contact_done;
+        const bool use_graph = boundary && (graph_ready(c) || c->eager_periods > 0 || n_steps - issued >= 2 * (long long)c->period);
+        if (boundary && !use_graph) ++c->eager_periods;
         if (use_graph && c->sched_trial_pending && !c->tuning_fixed && n_steps - issued >= 2 * N_CANDS * (long long)c->period) {
             st = schedule_trial(c);
             if (st != CRUSH_OK) return st;
@@ -2755,14 +2817,24 @@ int results_range(crush_ctx* c, int s0, int s1, crush_results* r) {
     if (s0 < 0 || s1 > c->n_slots || s0 >= s1) return crush::fail(CRUSH_ERR_INVALID, "slot out of range");
     std::vector<Control> h(s1 - s0);
     CK(cudaMemcpyAsync(h.data(), c->ctls + s0, sizeof(Control) * h.size(), cudaMemcpyDeviceToHost, c->stream));
-    std::vector<double> sums(7 * std::max(c->va.n_vehicles, 1)), ux(std::max<size_t>(c->crush_nodes_h.size(), 1));
-    if (c->va.n_vehicles > 0) {
-        launch_vehicle_sums(c->stream, c->va, c->mass, c->v, c->v0, c->veh_out);
-        launch_gather_ux(c->stream, (long long)c->crush_nodes_h.size(), c->crush_nodes, c->u, c->crush_ux);
+    // only the vehicles of slots [s0, s1) (consecutive, in slot order) and their crush-measure nodes
+    const int v0 = c->slots[s0].vehicle0, v1 = c->slots[s1 - 1].vehicle0 + c->slots[s1 - 1].n_vehicles;
+    const size_t q0 = c->crush_off_h[v0], q1 = c->crush_off_h[v1];
+    std::vector<double> sums(7 * (size_t)std::max(c->va.n_vehicles, 1)), ux(std::max<size_t>(c->crush_nodes_h.size(), 1));
+    if (v1 > v0) {
+        VehicleArrays vr = c->va;
+        vr.n_vehicles = v1 - v0;
+        vr.off += v0;
+        vr.slot += v0;
+        vr.local += v0;
+        launch_vehicle_sums(c->stream, vr, c->mass, c->v, c->v0, c->veh_out + 7 * (size_t)v0);
+        launch_gather_ux(c->stream, (long long)(q1 - q0), c->crush_nodes + q0, c->u, c->crush_ux + q0);
         int st = check_launch(c, 2);
         if (st != CRUSH_OK) return st;
-        CK(cudaMemcpyAsync(sums.data(), c->veh_out, sizeof(double) * 7 * c->va.n_vehicles, cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaMemcpyAsync(ux.data(), c->crush_ux, sizeof(double) * c->crush_nodes_h.size(), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(sums.data() + 7 * (size_t)v0, c->veh_out + 7 * (size_t)v0, sizeof(double) * 7 * (v1 - v0), cudaMemcpyDeviceToHost,
+                           c->stream));
+        if (q1 > q0)
+            CK(cudaMemcpyAsync(ux.data() + q0, c->crush_ux + q0, sizeof(double) * (q1 - q0), cudaMemcpyDeviceToHost, c->stream));
     }
     CK(cudaStreamSynchronize(c->stream));
     for (int slot = s0; slot < s1; ++slot) {
@@ -2835,6 +2907,70 @@ int run_to_end(crush_ctx* c) {
         total += chunk;
     }
     if (!done) return crush::fail(CRUSH_ERR_TIMEOUT, "run did not finish within " + std::to_string(cap) + " steps");
+    return CRUSH_OK;
+}
+
+// Set-up of a batch pipelined with its run (crush_batch_solve): a context
+// with room for every model is created from the first sixteenth of the
+// elements and begins its run; each later group joins the open run at the
+// next step-graph boundary (crush_batch_append's path: its host set-up runs
+// while the steps issued before it run, its device set-up on the set-up
+// stream), one group per 20-step chunk, so the set-up of all but the first
+// group is hidden behind the run. Every model's results equal its own run
+// (a slot's steps do not depend on when it joined). Models that the room
+// estimate cannot take run in a further context after this one.
+int solve_models(const crush_model_desc* const* descs, int n, int device, crush_results* out) {
+    long long total = 0;
+    crush_capacity room{};
+    room.slots = n;
+    for (int k = 0; k < n; ++k) {
+        const crush_model_desc* d = descs[k];
+        room.nodes += std::max<int64_t>(d->n_nodes, 0);
+        room.hexes += std::max<int64_t>(d->n_hexes, 0);
+        room.contacts += std::max(d->n_contacts, 0);
+        for (int q = 0; q < d->n_contacts && d->contacts; ++q) {
+            room.faces += std::max<int64_t>(d->contacts[q].n_faces, 0);
+            room.primary_nodes += std::max<int64_t>(d->contacts[q].n_nodes, 0);
+        }
+        total += std::max<int64_t>(d->n_hexes, 1);
+    }
+    constexpr int GROUPS = 16;
+    // group ends: model k closes group g when the running element count reaches g / GROUPS of the total
+    std::vector<int> ends;
+    long long acc = 0;
+    for (int k = 0; k < n; ++k) {
+        acc += std::max<int64_t>(descs[k]->n_hexes, 1);
+        if (k == n - 1 || acc * GROUPS >= total * (long long)(ends.size() + 1)) ends.push_back(k + 1);
+    }
+    std::unique_ptr<crush_ctx> c(new crush_ctx());
+    int st = create_impl(descs, ends[0], device, c.get(), &room);
+    if (st != CRUSH_OK) return st;
+    st = run_begin(c.get());
+    if (st != CRUSH_OK) return st;
+    int placed = ends[0];
+    const long long per = c->period > 0 ? c->period : 20;
+    for (size_t g = 1; g < ends.size(); ++g) {
+        st = issue_steps(c.get(), per);
+        if (st != CRUSH_OK) return st;
+        st = add_slots(c.get(), descs + placed, ends[g] - placed, false, nullptr);
+        if (st == CRUSH_ERR_BUSY) break;  // beyond the room estimate: the rest run afterwards
+        if (st != CRUSH_OK) return st;
+        placed = ends[g];
+    }
+    // to the end: every slot, the last joined included
+    long long cap = 0;
+    for (const Slot& sl : c->slots) cap = std::max<long long>(cap, sl.settings.max_steps > 0 ? sl.settings.max_steps : 2000000ll);
+    cap += c->host_step + 10 * per;
+    int done = 0;
+    while (!done && c->host_step < cap) {
+        st = run_steps(c.get(), 10 * per, &done);
+        if (st != CRUSH_OK) return st;
+    }
+    if (!done) return crush::fail(CRUSH_ERR_TIMEOUT, "batch did not finish within " + std::to_string(cap) + " steps");
+    st = results_range(c.get(), 0, c->n_slots, out);
+    if (st != CRUSH_OK) return st;
+    c.reset();
+    if (placed < n) return solve_models(descs + placed, n - placed, device, out + placed);
     return CRUSH_OK;
 }
 
@@ -3521,6 +3657,14 @@ int crush_batch_run(crush_ctx* c, crush_results* r) {
     int st = run_to_end(c);
     if (st != CRUSH_OK) return st;
     return results_range(c, 0, c->n_slots, r);
+}
+
+int crush_batch_solve(const crush_model_desc* const* descs, int n, int device, crush_results* out) {
+    if (!descs || n <= 0 || !out) return crush::fail(CRUSH_ERR_INVALID, "invalid argument");
+    for (int k = 0; k < n; ++k)
+        if (!descs[k]) return crush::fail(CRUSH_ERR_INVALID, "null model description");
+    CK(cudaSetDevice(device));
+    return solve_models(descs, n, device, out);
 }
 
 }  // extern "C"

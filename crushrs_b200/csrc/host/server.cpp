@@ -11,6 +11,8 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -92,6 +94,29 @@ struct Request {
 double now_s(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
+
+// CRUSH_TRACE=1: each serving context prints where its host thread spent
+// its time when it ends (diagnostics only).
+struct ContextTrace {
+    bool on = std::getenv("CRUSH_TRACE") && std::getenv("CRUSH_TRACE")[0] == '1';
+    std::chrono::steady_clock::time_point born = std::chrono::steady_clock::now(), t = born;
+    double ms[6] = {};  // create + begin, issue, append, wait for the chunk, results, other
+    long long chunks = 0, appends = 0, appended = 0;
+    void lap(int what) {
+        if (!on) return;
+        auto now = std::chrono::steady_clock::now();
+        ms[what] += std::chrono::duration<double, std::milli>(now - t).count();
+        t = now;
+    }
+    void print(int id, size_t slots) const {
+        if (!on) return;
+        const double life = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - born).count();
+        std::fprintf(stderr,
+                     "[crush-serve] context %d: %zu crashes, %lld chunks, %lld appends (%lld crashes); ms: create %.1f issue %.1f "
+                     "append %.1f chunk wait %.1f results %.1f other %.1f life %.1f\n",
+                     id, slots, chunks, appends, appended, ms[0], ms[1], ms[2], ms[3], ms[4], ms[5], life);
+    }
+};
 
 int schedule_key(const crush_settings& s) {
     const bool adaptive = !(s.time_step > 0.0) && s.adaptive_check_steps > 0;
@@ -240,9 +265,11 @@ void crush_server::run_context(std::vector<Request> first, int id, double bytes,
     };
     std::vector<const crush_model_desc*> descs;
     for (auto& r : first) descs.push_back(&r.model->desc);
+    ContextTrace tr;
     int st = crush_batch_create_reserved(descs.data(), (int)descs.size(), cfg.device, &room, &ctx);
     add(first);
     if (st == CRUSH_OK) st = crush_run_begin(ctx);
+    tr.lap(0);
     bool open = true;  // still takes requests
     const int chunk = std::max(20, cfg.chunk_steps / 20 * 20);
     std::vector<int> flags;
@@ -278,16 +305,24 @@ void crush_server::run_context(std::vector<Request> first, int id, double bytes,
                 }
             }
         }
+        tr.lap(5);
         if (running == 0 && batch.empty()) continue;  // nothing on the device, nothing admitted
         // Requests are waiting: short chunks, so the next admission comes soon.
         const bool waiting = !batch.empty();
-        if (running > 0) st = crush_run_issue(ctx, waiting ? 20 : chunk);
+        if (running > 0) {
+            st = crush_run_issue(ctx, waiting ? 20 : chunk);
+            ++tr.chunks;
+        }
+        tr.lap(1);
         if (st != CRUSH_OK) break;
         if (!batch.empty()) {
             descs.clear();
             for (auto& r : batch) descs.push_back(&r.model->desc);
             const int a = crush_batch_append(ctx, descs.data(), (int)descs.size(), nullptr);
+            tr.lap(2);
             if (a == CRUSH_OK) {
+                ++tr.appends;
+                tr.appended += (long long)batch.size();
                 add(batch);
             } else {
                 // No room (or not admissible here): back to the queue's head
@@ -306,6 +341,7 @@ void crush_server::run_context(std::vector<Request> first, int id, double bytes,
         flags.assign(slots.size(), 0);
         int all = 0;
         st = crush_batch_done(ctx, flags.data(), &all);
+        tr.lap(3);
         if (st != CRUSH_OK) break;
         int lo = (int)slots.size(), hi = -1;
         for (int k = 0; k < (int)slots.size(); ++k)
@@ -323,6 +359,7 @@ void crush_server::run_context(std::vector<Request> first, int id, double bytes,
                     report(k, rs[k - lo].status, &rs[k - lo]);
                 }
             flush();
+            tr.lap(4);
         }
         if (open && ((int)slots.size() >= room.slots || used >= room.hexes)) {
             std::lock_guard<std::mutex> lk(mu);
@@ -335,6 +372,8 @@ void crush_server::run_context(std::vector<Request> first, int id, double bytes,
         if (!reported[k]) report((int)k, st == CRUSH_OK ? CRUSH_ERR_INVALID : st, nullptr);
     if (ctx) crush_destroy(ctx);
     flush();
+    tr.lap(5);
+    tr.print(id, slots.size());
     std::lock_guard<std::mutex> lk(mu);
     if (open) --accepting[key];
     in_use -= bytes;

@@ -20,6 +20,8 @@
 #include <climits>
 #include <math_constants.h>
 
+#include <cub/cub.cuh>
+
 #include "element.cuh"
 #include "kernels.cuh"
 #include "hencky.cuh"
@@ -335,6 +337,66 @@ __global__ void k_init_state(long long h_begin, long long n_hc, long long stride
     // identity F_prev⁻¹ (0-8), identity R (9-17), zero stress, compaction, not eroded.
     const float v[28] = {1, 0, 0, 0, 1, 0, 0, 0, 1, 1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int k = 0; k < N_STATE_PLANES; ++k) st[k * stride + e] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+}
+
+// Node incidence of new elements [e0, e0 + ne) over their nodes [n0, n0 + nn)
+// (set-up): per node its (element, corner) slots 8 e + i in increasing
+// element order, the order of the reference's serial force scatter
+// (src/kernel_simd.rs:573-586). Count pass: the sort keys (node) and values
+// (slot) in element order, and per node its entries in all, honeycomb and
+// elastic elements.
+__global__ void k_incidence_count(long long e0, long long ne, long long n0, const uint32_t* __restrict__ conn,
+                                  const int64_t* __restrict__ hc_index, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                                  uint32_t* __restrict__ cnt_all, uint32_t* __restrict__ cnt_hc, uint32_t* __restrict__ cnt_sc) {
+    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ne) return;
+    const long long e = e0 + j;
+    const bool honey = hc_index[e] >= 0;
+    for (int i = 0; i < 8; ++i) {
+        const uint32_t key = (uint32_t)(conn[8 * e + i] - n0);
+        keys[8 * j + i] = key;
+        vals[8 * j + i] = (uint32_t)(8 * e + i);
+        atomicAdd(cnt_all + key, 1u);
+        atomicAdd(honey ? cnt_hc + key : cnt_sc + key, 1u);
+    }
+}
+
+// Split pass, a thread per node: its slots in element order (the stable
+// sort's output at the node's offset) go to the honeycomb list (8 h + i) or
+// the elastic list (8 q + i); the offsets get their global bases; the padded
+// row holds the first 8 honeycomb slots (HC_ELL_MORE in front past 8).
+__global__ void k_incidence_split(long long nn, const uint32_t* __restrict__ rel_all, const uint32_t* __restrict__ rel_hc,
+                                  const uint32_t* __restrict__ rel_sc, uint32_t base_all, uint32_t base_hc, uint32_t base_sc,
+                                  const int64_t* __restrict__ hc_index, const int64_t* __restrict__ sc_index,
+                                  const uint32_t* __restrict__ all_slot, uint32_t* __restrict__ all_off, uint32_t* __restrict__ hc_off,
+                                  uint32_t* __restrict__ hc_slot, uint32_t* __restrict__ sc_off, uint32_t* __restrict__ sc_slot,
+                                  uint32_t* __restrict__ hc_ell) {
+    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j > nn) return;
+    all_off[j] = base_all + rel_all[j];
+    hc_off[j] = base_hc + rel_hc[j];
+    sc_off[j] = base_sc + rel_sc[j];
+    if (j == nn) return;
+    uint32_t ph = base_hc + rel_hc[j], ps = base_sc + rel_sc[j];
+    uint32_t row[8];
+    int m = 0;
+    for (uint32_t k = base_all + rel_all[j]; k < base_all + rel_all[j + 1]; ++k) {
+        const uint32_t v = all_slot[k];
+        const long long e = v >> 3;
+        const uint32_t i = v & 7u;
+        const long long h = hc_index[e];
+        if (h >= 0) {
+            const uint32_t x = (uint32_t)(8 * h + i);
+            hc_slot[ph++] = x;
+            if (m < 8) row[m] = x;
+            ++m;
+        } else {
+            sc_slot[ps++] = (uint32_t)(8 * sc_index[e] + i);
+        }
+    }
+    for (int q = m; q < 8; ++q) row[q] = HC_ELL_NONE;
+    if (m > 8) row[0] = HC_ELL_MORE;
+    for (int q = 0; q < 8; ++q) hc_ell[8 * j + q] = row[q];
 }
 
 // ---------------------------------------------------------------------------
@@ -1954,6 +2016,72 @@ void launch_setup_geometry(cudaStream_t s, long long e_begin, long long n_all, c
 void launch_node_masses(cudaStream_t s, long long n, const uint32_t* off, const uint32_t* slot, const double* lumped,
                         double* mass, double* inv_mass) {
     k_node_masses<<<(unsigned)blocks_for(n, TPB), TPB, 0, s>>>(n, off, slot, lumped, mass, inv_mass);
+}
+// Scratch of launch_incidence: sort keys and values, their second buffers,
+// three count arrays, three offset arrays and CUB's temporary storage.
+struct IncidenceScratch {
+    size_t keys, keys2, vals, vals2, cnt, rel, temp, total;
+};
+IncidenceScratch incidence_layout(long long ne, long long nn) {
+    const size_t m = 8 * (size_t)std::max<long long>(ne, 1), c = (size_t)nn + 1;
+    size_t sort_bytes = 0, scan_bytes = 0;
+    cub::DoubleBuffer<uint32_t> k(nullptr, nullptr), v(nullptr, nullptr);
+    cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, k, v, (int)m, 0, 32);
+    cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (uint32_t*)nullptr, (uint32_t*)nullptr, (int)c);
+    auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+    IncidenceScratch l;
+    l.keys = 0;
+    l.keys2 = l.keys + up(4 * m);
+    l.vals = l.keys2 + up(4 * m);
+    l.vals2 = l.vals + up(4 * m);
+    l.cnt = l.vals2 + up(4 * m);
+    l.rel = l.cnt + 3 * up(4 * c);
+    l.temp = l.rel + 3 * up(4 * c);
+    l.total = l.temp + up(std::max(sort_bytes, scan_bytes));
+    return l;
+}
+size_t incidence_scratch_bytes(long long ne, long long nn) { return incidence_layout(ne, nn).total; }
+
+int launch_incidence(cudaStream_t s, long long e0, long long ne, long long n0, long long nn, const uint32_t* conn_all,
+                     const int64_t* hc_index, const int64_t* sc_index, uint32_t base_all, uint32_t base_hc, uint32_t base_sc,
+                     uint32_t* all_off, uint32_t* all_slot, uint32_t* hc_off, uint32_t* hc_slot, uint32_t* sc_off, uint32_t* sc_slot,
+                     uint32_t* hc_ell, void* scratch) {
+    if (nn <= 0) return 0;
+    const IncidenceScratch l = incidence_layout(ne, nn);
+    char* b = static_cast<char*>(scratch);
+    const size_t m = 8 * (size_t)ne, c = (size_t)nn + 1;
+    auto up = [](size_t x) { return (x + 255) / 256 * 256; };
+    uint32_t* keys = reinterpret_cast<uint32_t*>(b + l.keys);
+    uint32_t* keys2 = reinterpret_cast<uint32_t*>(b + l.keys2);
+    uint32_t* vals = reinterpret_cast<uint32_t*>(b + l.vals);
+    uint32_t* vals2 = reinterpret_cast<uint32_t*>(b + l.vals2);
+    uint32_t* cnt[3];
+    uint32_t* rel[3];
+    for (int k = 0; k < 3; ++k) {
+        cnt[k] = reinterpret_cast<uint32_t*>(b + l.cnt + k * up(4 * c));
+        rel[k] = reinterpret_cast<uint32_t*>(b + l.rel + k * up(4 * c));
+    }
+    void* temp = b + l.temp;
+    const size_t temp_bytes = l.total - l.temp;
+    for (int k = 0; k < 3; ++k)
+        if (cudaMemsetAsync(cnt[k], 0, 4 * c, s) != cudaSuccess) return -1;
+    if (ne > 0)
+        k_incidence_count<<<(unsigned)blocks_for(ne, TPB), TPB, 0, s>>>(e0, ne, n0, conn_all, hc_index, keys, vals, cnt[0], cnt[1], cnt[2]);
+    for (int k = 0; k < 3; ++k) {
+        size_t tb = temp_bytes;
+        if (cub::DeviceScan::ExclusiveSum(temp, tb, cnt[k], rel[k], (int)c, s) != cudaSuccess) return -1;
+    }
+    if (m > 0) {
+        int bits = 1;
+        while (bits < 32 && ((uint64_t)1 << bits) < (uint64_t)nn) ++bits;
+        cub::DoubleBuffer<uint32_t> dk(keys, keys2), dv(vals, vals2);
+        size_t tb = temp_bytes;
+        if (cub::DeviceRadixSort::SortPairs(temp, tb, dk, dv, (int)m, 0, bits, s) != cudaSuccess) return -1;
+        if (cudaMemcpyAsync(all_slot + base_all, dv.Current(), 4 * m, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return -1;
+    }
+    k_incidence_split<<<(unsigned)blocks_for(nn + 1, TPB), TPB, 0, s>>>(nn, rel[0], rel[1], rel[2], base_all, base_hc, base_sc, hc_index,
+                                                                     sc_index, all_slot, all_off, hc_off, hc_slot, sc_off, sc_slot, hc_ell);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 void launch_init_state(cudaStream_t s, long long h_begin, long long n_hc, long long stride, float4* state) {
     if (n_hc <= h_begin) return;

@@ -227,6 +227,19 @@ void launch_setup_geometry(cudaStream_t s, long long e_begin, long long n_all, c
 void launch_node_masses(cudaStream_t s, long long n, const uint32_t* off, const uint32_t* slot, const double* lumped,
                         double* mass, double* inv_mass);
 void launch_init_state(cudaStream_t s, long long h_begin, long long n_hc, long long stride, float4* state);
+// Node incidence of new elements [e0, e0 + ne) over their nodes [n0, n0 + nn)
+// on the device: per node its (element, corner) slots in element order (a
+// stable radix sort by node), in all elements (all_off / all_slot), split
+// into honeycomb and elastic lists, and the padded honeycomb rows. The
+// offset arrays and hc_ell point at the new nodes' first entries, the slot
+// arrays at their context-wide start (base_* = the new entries' first global
+// position). scratch holds incidence_scratch_bytes(ne, nn). Returns 0, or -1
+// on a CUDA error.
+size_t incidence_scratch_bytes(long long ne, long long nn);
+int launch_incidence(cudaStream_t s, long long e0, long long ne, long long n0, long long nn, const uint32_t* conn_all,
+                     const int64_t* hc_index, const int64_t* sc_index, uint32_t base_all, uint32_t base_hc, uint32_t base_sc,
+                     uint32_t* all_off, uint32_t* all_slot, uint32_t* hc_off, uint32_t* hc_slot, uint32_t* sc_off, uint32_t* sc_slot,
+                     uint32_t* hc_ell, void* scratch);
 // Element forces: the honeycomb lane kernel and, when the model has
 // elastic elements, the scalar f64 kernel (forces_launches of them).
 // schedule: 0 = one persistent wave of blocks on the n_sms SMs, 1 = a block

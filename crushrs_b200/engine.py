@@ -322,3 +322,14 @@ def run(desc, device=0):
         return ctx.run()
     finally:
         ctx.close()
+
+
+def solve_batch(descs, device=0):
+    """crush_batch_solve: every model of `descs` run as one batch, set-up
+    pipelined with the run (later groups of models join the open run);
+    per-model Results, each equal to the model run alone."""
+    descs = list(descs)
+    arr = (C.POINTER(abi.ModelDesc) * len(descs))(*[C.pointer(d) for d in descs])
+    rs = (abi.Results * len(descs))()
+    check(lib().crush_batch_solve(arr, len(descs), device, rs))
+    return list(rs)

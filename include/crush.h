@@ -429,6 +429,13 @@ typedef struct crush_capacity {
     int64_t primary_nodes;
 } crush_capacity;
 int crush_batch_create_reserved(const crush_model_desc* const* descs, int n, int device, const crush_capacity* room, crush_ctx** out);
+/* Runs n models as one batch and writes each one's results to out[k]: the
+ * one-call form of crush_batch_create + crush_batch_run, with the set-up
+ * pipelined with the run (the first sixteenth of the elements starts the
+ * run; the other models join it group by group at step-graph boundaries,
+ * their set-up overlapping the steps in flight). Results are those of each
+ * model run alone. The descriptions must stay valid for the call. */
+int crush_batch_solve(const crush_model_desc* const* descs, int n, int device, crush_results* out);
 /* Adds n models as slots [*first_slot, *first_slot + n). With a run open,
  * only on a step-graph boundary (a multiple of 20 steps: between
  * crush_run_steps calls of multiples of 20 steps, the default issue of

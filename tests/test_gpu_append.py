@@ -70,6 +70,25 @@ def test_append_into_a_running_context_equals_alone(models, alone):
         _same(ctx.results(slot), alone[k])
 
 
+def test_append_every_period_equals_alone(models, alone):
+    """The serving pattern: one graph period issued at a time with slots
+    joining at most boundaries (each set up beside the period in flight,
+    the period after a join launched step by step), then periods without
+    joins (graphs again); every slot gives its alone results."""
+    ctx = Context([models[0].desc], room=ROOM)
+    ctx.run_begin()
+    order = [0]
+    for k in range(1, len(models)):
+        ctx.run_steps(20)
+        ctx.append([models[k].desc])
+        order.append(k)
+        if k % 3 == 0:
+            ctx.run_steps(40)
+    _run_to_end(ctx, chunk=20)
+    for slot, k in enumerate(order):
+        _same(ctx.results(slot), alone[k])
+
+
 def test_append_refuses_beyond_room_and_runs_on(models, alone):
     small = dict(slots=3, contacts=12, nodes=10_000, hexes=8_000, faces=3_000, primary_nodes=4_000)
     ctx = Context([models[0].desc], room=small)

@@ -124,3 +124,21 @@ def test_large_batch_equals_alone():
         r = a.run()
         a.close()
         _same(rs[i], r)
+
+
+def test_solve_equals_alone(models, alone):
+    """crush_batch_solve (set-up pipelined with the run: later groups join
+    the open run) gives every model its alone results; 40 models so that
+    several groups join, in an order that mixes long and short crashes."""
+    from crushrs_b200.engine import solve_batch
+
+    extra = [S.Model.build(S.batch_headon(i)) for i in range(4, 40)]
+    order = list(models) + extra
+    rs = solve_batch([m.desc for m in order])
+    assert len(rs) == len(order)
+    for r, a in zip(rs, alone):
+        _same(r, a)
+    for m, r in zip(extra[::7], rs[len(models)::7]):
+        ctx = Context(m.desc)
+        _same(r, ctx.run())
+        ctx.close()
