@@ -174,11 +174,13 @@ struct HistAccel {
 };
 
 // Runs fn(i) for i in [0, n) on up to `hardware_concurrency` host threads
-// (dynamic scheduling); serial for n == 1.
+// (dynamic scheduling), each taking at least `grain` items' worth of the
+// range; serial when that leaves one thread (a thread costs tens of
+// microseconds to start, more than a few small items take).
 template <class F>
-void parallel_for(long long n, F&& fn) {
+void parallel_for(long long n, F&& fn, long long grain = 1) {
     unsigned hw = std::thread::hardware_concurrency();
-    const long long T = std::min<long long>(n, std::min<unsigned>(hw ? hw : 1, 64));
+    const long long T = std::min<long long>(n / std::max<long long>(grain, 1), std::min<unsigned>(hw ? hw : 1, 64));
     if (T <= 1) {
         for (long long i = 0; i < n; ++i) fn(i);
         return;
@@ -251,6 +253,12 @@ struct Stager {
     size_t cap = 0;
     int cur = 0;
     bool pooled = false;  // the buffers are g_pinned's
+    // arena mode (slots joining an open run): every copy's source is packed
+    // into a pinned arena the caller keeps, so the copies do not wait for the
+    // stream; arena_done is recorded after them on release
+    char* arena = nullptr;
+    size_t arena_cap = 0, arena_used = 0;
+    cudaEvent_t arena_done = nullptr;
     static constexpr size_t DIRECT = 1 << 20;
     int init(cudaStream_t stream, size_t total) {
         s = stream;
@@ -294,8 +302,21 @@ struct Stager {
             }
         return CRUSH_OK;
     }
+    void use_arena(char* base, size_t cap, cudaEvent_t done) {
+        arena = base;
+        arena_cap = cap;
+        arena_used = 0;
+        arena_done = done;
+    }
     int copy(void* dst, const void* src, size_t bytes) {
         if (!bytes) return CRUSH_OK;
+        if (arena && arena_used + bytes <= arena_cap) {
+            char* b = arena + arena_used;
+            std::memcpy(b, src, bytes);
+            arena_used += (bytes + 255) / 256 * 256;
+            CK(cudaMemcpyAsync(dst, b, bytes, cudaMemcpyHostToDevice, s));
+            return CRUSH_OK;
+        }
         if (!buf[0] || bytes < DIRECT) {
             CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
             return CRUSH_OK;
@@ -317,6 +338,8 @@ struct Stager {
         return CRUSH_OK;
     }
     void release() {
+        if (arena && arena_used > 0 && arena_done) cudaEventRecord(arena_done, s);
+        arena = nullptr;
         if (s && buf[0]) cudaStreamSynchronize(s);  // the staging buffers' DMA (direct copies are staged on return)
         for (int k = 0; k < 2; ++k) {
             if (buf[k] && !pooled) cudaFreeHost(buf[k]);
@@ -434,6 +457,7 @@ struct crush_ctx {
     std::vector<size_t> crush_off_h{0};
     uint32_t* crush_nodes = nullptr;
     double* crush_ux = nullptr;
+    size_t crush_cap = 0;  // room of crush_nodes / crush_ux
 
     // run
     bool run_open = false;
@@ -473,6 +497,9 @@ struct crush_ctx {
     // once ev_tab has passed).
     cudaStream_t setup = nullptr;
     cudaEvent_t ev_setup = nullptr, ev_tab = nullptr;
+    char* arena = nullptr;  // pinned upload arena of those set-ups (ev_arena: its last copies done)
+    size_t arena_cap = 0;
+    cudaEvent_t ev_arena = nullptr;
     int* tab_pinned = nullptr;
     size_t tab_pinned_cap = 0;
     int eager_periods = 0;                // graph periods launched step by step since the graphs were dropped
@@ -647,6 +674,8 @@ struct crush_ctx {
         if (ev_setup) cudaEventDestroy(ev_setup);
         if (ev_tab) cudaEventDestroy(ev_tab);
         if (tab_pinned) cudaFreeHost(tab_pinned);
+        if (arena) cudaFreeHost(arena);
+        if (ev_arena) cudaEventDestroy(ev_arena);
         if (setup) cudaStreamDestroy(setup);
         if (side) cudaStreamDestroy(side);
         if (side2) cudaStreamDestroy(side2);
@@ -1077,8 +1106,8 @@ void append(std::vector<T>& dst, const std::vector<T>& src) {
     dst.insert(dst.end(), src.begin(), src.end());
 }
 
-int begin_slots(crush_ctx* c, int s0, int s1, bool search);
-int search_new_contacts(crush_ctx* c, int s0, int s1);
+int begin_slots(crush_ctx* c, int s0, int s1);
+int search_now(crush_ctx* c);
 static void free_bufs(crush_ctx* c, std::vector<void*>& bufs);
 
 // Adds n_desc models as slots [c->n_slots, c->n_slots + n_desc) at the
@@ -1159,7 +1188,10 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
     cm.mat4.resize(4 * (size_t)P);
     std::vector<SlotError> errs(n_desc);
     std::vector<long long> slot_hc(n_desc, 0);
-    parallel_for(n_desc, [&](long long k) { fill_slot(descs[k], S0 + (int)k, slots[k], part0[k], cm, &slot_hc[k], errs[k]); });
+    // per-slot passes: a thread per ~16k elements at least (a few small
+    // models, as one request adds, are set up on the calling thread)
+    const long long G = std::max<long long>(1, (long long)n_desc * 16384 / std::max<long long>(E, 1));
+    parallel_for(n_desc, [&](long long k) { fill_slot(descs[k], S0 + (int)k, slots[k], part0[k], cm, &slot_hc[k], errs[k]); }, G);
     for (auto& e : errs)
         if (e.code != CRUSH_OK) return crush::fail(e.code, e.msg);
     trace.mark("validate + concatenate");
@@ -1180,7 +1212,7 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
             nf += all_fixed ? 0 : 1;
         }
         slot_free[k] = nf;
-    });
+    }, G);
     std::vector<long long> hc0(n_desc + 1, H0), sc0(n_desc + 1, Q0), scf0(n_desc + 1, QF0);
     for (int k = 0; k < n_desc; ++k) {
         hc0[k + 1] = hc0[k] + slot_hc[k];
@@ -1218,7 +1250,7 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
                 sc_index[e - E0] = q;
                 sc_model[q - Q0] = (uint32_t)e;
             }
-    });
+    }, G);
     std::vector<double> sc_mat(2 * (size_t)std::max<long long>(Q, 1), 0.0);
     for (long long q = 0; q < Q; ++q) {
         const crush_material& m = mat_of(sc_model[q]);
@@ -1229,7 +1261,7 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
 
     // ---- contacts: per slot in parallel, then concatenated after the context's ----
     std::vector<ContactPart> parts(n_desc);
-    parallel_for(n_desc, [&](long long k) { build_contacts(descs[k], slots[k], cm, parts[k], errs[k]); });
+    parallel_for(n_desc, [&](long long k) { build_contacts(descs[k], slots[k], cm, parts[k], errs[k]); }, G);
     for (auto& e : errs)
         if (e.code != CRUSH_OK) return crush::fail(e.code, e.msg);
     trace.mark("contact runtimes per slot");
@@ -1377,7 +1409,7 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
         };
         for (size_t j = 0; j < cp.slaves.size(); ++j) slave_cn[b.slave - s0 + j] = cn_of(cp.slaves[j]);
         for (size_t j = 0; j < cp.faces.size(); ++j) face_cn[4 * (b.face - f0) + j] = cn_of(cp.faces[j]);
-    });
+    }, G);
     if (cn_missing) return crush::fail(CRUSH_ERR_INVALID, "internal: a contact node without a role");
     trace.mark("contact tables concatenated");
     // exhaustive contacts (no grid) get a block each; the rest are listed by entry
@@ -1446,7 +1478,7 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
             vslot[q] = S0 + (int)k;
             vlocal[q] = v;
         }
-    });
+    }, G);
     for (auto& e : errs)
         if (e.code != CRUSH_OK) return crush::fail(e.code, e.msg);
     trace.mark("contacts and vehicles built");
@@ -1458,9 +1490,13 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
     const bool appending = !creating && c->run_open;
     cudaStream_t main_stream = c->stream;
     if (appending && !c->setup) {
-        CK(cudaStreamCreateWithFlags(&c->setup, cudaStreamNonBlocking));
+        // high priority: its blocks go first as the steps' blocks retire
+        int lo = 0, hi = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        CK(cudaStreamCreateWithPriority(&c->setup, cudaStreamNonBlocking, hi));
         CK(cudaEventCreateWithFlags(&c->ev_setup, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&c->ev_tab, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c->ev_arena, cudaEventDisableTiming));
     }
     struct StreamRestore {
         crush_ctx* c;
@@ -1474,6 +1510,22 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
     std::vector<std::pair<long long, long long>> tab_ranges;  // appending: chunk-table entries the main stream updates
     Stager stager;
     stager.init(c->stream, sizeof(double) * 6 * N + sizeof(uint32_t) * 27 * E);
+    if (appending) {
+        // model, incidence-numbering, contact and vehicle arrays of the new
+        // slots, generously: copies beyond the arena go direct (and wait)
+        const size_t want = 2 * (96 * (size_t)N + 64 * (size_t)E + 64 * (size_t)(tot.face - base[0].face) + 64 * (size_t)(tot.ste - base[0].ste) +
+                                 8 * (size_t)(tot.stoff - base[0].stoff)) + (1u << 20);
+        CK(cudaEventSynchronize(c->ev_arena));  // the previous set-up's copies are done
+        if (want > c->arena_cap) {
+            if (c->arena) CK(cudaFreeHost(c->arena));
+            c->arena = nullptr;
+            c->arena_cap = 0;
+            const size_t cap = std::max<size_t>(want, 32u << 20);
+            CK(cudaMallocHost(&c->arena, cap));
+            c->arena_cap = cap;
+        }
+        stager.use_arena(c->arena, c->arena_cap, c->ev_arena);
+    }
     c->stager = &stager;
     struct StagerRelease {
         crush_ctx* c;
@@ -1782,11 +1834,23 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
     c->max_vnodes = max_vnodes;
     va.vx_blocks = (int)std::min<long long>(VX_BLOCKS, std::max<long long>(1, (max_vnodes + 2047) / 2048));
     for (size_t i = 0; i < crush_off_new.size(); ++i) c->crush_off_h.push_back(c->crush_nodes_h.size() + crush_off_new[i]);
+    const size_t crush_before = c->crush_nodes_h.size();
     c->crush_nodes_h.insert(c->crush_nodes_h.end(), crush_nodes_new.begin(), crush_nodes_new.end());
     trace.mark("host copies");
-    // the crush-measure node list is small: a new copy of the whole list
-    TRY(c->upload(&c->crush_nodes, c->crush_nodes_h.data(), c->crush_nodes_h.size()));
-    TRY(c->alloc(&c->crush_ux, std::max<size_t>(c->crush_nodes_h.size(), 1)));
+    // the crush-measure node list: room for the context's vehicle nodes and
+    // an accelerometer per vehicle; a list beyond it moves to a new buffer
+    {
+        const size_t ncn = c->crush_nodes_h.size();
+        if (ncn > c->crush_cap) {
+            const size_t room = std::max<size_t>(std::max<size_t>(ncn, 1), (size_t)(c->cap.vnodes + c->cap.vehicles));
+            TRY(c->alloc(&c->crush_nodes, room));
+            TRY(c->alloc(&c->crush_ux, room));
+            c->crush_cap = room;
+            TRY(put(c->crush_nodes, c->crush_nodes_h.data(), ncn));
+        } else {
+            TRY(put(c->crush_nodes + crush_before, c->crush_nodes_h.data() + crush_before, ncn - crush_before));
+        }
+    }
     trace.mark("crush-measure nodes");
     // ---- active chunk tables: the slot range of every chunk the new entities touch ----
     {
@@ -1822,7 +1886,7 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
                 }
                 c->chunk_lo_h[q] = a;
                 c->chunk_hi_h[q] = b;
-            });
+            }, 64);
             // A chunk the new entities share with running slots is read by
             // the steps in flight: an append updates the tables in the main
             // stream's order.
@@ -1918,7 +1982,7 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
         sl.stable = std::fmin(stable, sl.contact_dt);
         sl.dt_floor = sl.settings.mass_scaling > 0.0 ? sl.settings.mass_scaling * sl.stable : 0.0;
         sl.dt0 = sl.settings.time_step > 0.0 ? sl.settings.time_step : sl.stable * sl.settings.dt_scale;
-    });
+    }, G);
     trace.mark("initial stable step");
     if (creating) {
         c->period = std::lcm(c->check_steps, 20);
@@ -1927,8 +1991,7 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
     }
     drop_graphs(c);
     if (!c->run_open) return CRUSH_OK;
-    if (!appending) return begin_slots(c, S0, c->n_slots, true);
-    TRY(begin_slots(c, S0, c->n_slots, false));
+    TRY(begin_slots(c, S0, c->n_slots));
     // The main stream: the set-up done, the chunk tables, then the new
     // contacts' first search (its scratch is shared with the steps').
     CK(cudaEventRecord(c->ev_setup, c->setup));
@@ -1958,7 +2021,9 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
         }
         CK(cudaEventRecord(c->ev_tab, main_stream));
     }
-    return search_new_contacts(c, S0, c->n_slots);
+    // the first step's contact search of every contact at the run's current
+    // X + u (the running slots' hits are found again, the same ones)
+    return search_now(c);
 #undef TRY
 }
 
@@ -2545,13 +2610,12 @@ int run_begin(crush_ctx* c) {
 // Slots [s0, s1) (the context's last ones, added while its run is open)
 // begin their run as crush_run_begin begins every slot's: zero
 // displacement, initial velocities, masses, state, the initial internal
-// forces at u = 0, the static faces' geometry, the element dt pass of their
-// step 0 and the contact search their first step's forces read. They join at
+// forces at u = 0, the static faces' geometry and the element dt pass of
+// their step 0 (the caller then runs the contact search their first step's
+// forces read, on the main stream: its scratch is the steps'). They join at
 // the run's current step, a step-graph boundary, so their own steps fall on
-// the same step-schedule positions as alone. search = false leaves the
-// contact search to search_new_contacts (an append issues it on the main
-// stream) and does not wait for the stream.
-int begin_slots(crush_ctx* c, int s0, int s1, bool search) {
+// the same step-schedule positions as alone.
+int begin_slots(crush_ctx* c, int s0, int s1) {
     if (s1 <= s0) return CRUSH_OK;
     const Slot& a = c->slots[s0];
     const Slot& z = c->slots[s1 - 1];
@@ -2612,24 +2676,6 @@ int begin_slots(crush_ctx* c, int s0, int s1, bool search) {
     if (c->adaptive) {
         launch_elem_dt(c->stream, c->el(), c->nd(), c->ctls, c->u, 1, e0);
         st = check_launch(c);
-        if (st != CRUSH_OK) return st;
-    }
-    if (!search) return CRUSH_OK;
-    st = search_new_contacts(c, s0, s1);
-    if (st != CRUSH_OK) return st;
-    return sync(c);
-}
-
-// The first step's contact search of the contacts of slots [s0, s1) at
-// u = 0, contact by contact (the hits are those any search finds).
-int search_new_contacts(crush_ctx* c, int s0, int s1) {
-    if (s1 <= s0) return CRUSH_OK;
-    const int c0 = c->slots[s0].contact0, c1 = c->slots[s1 - 1].contact0 + c->slots[s1 - 1].n_contacts;
-    for (int k = c0; k < c1; ++k) {
-        const long long nf = c->face_off_h[k + 1] - c->face_off_h[k], ns = c->slave_off_h[k + 1] - c->slave_off_h[k];
-        const long long bk0 = c->tab_off_h[k], bk1 = c->tab_off_h[k + 1];
-        launch_contact_search(c->stream, c->ca, c->nd(), c->ctls, k, k + 1, c->face_off_h[k], nf, ns, bk0, bk1, 0, c->slave_lanes);
-        const int st = check_launch(c, contact_search_launches(c->ca, false, nf, ns, bk0, bk1, k));
         if (st != CRUSH_OK) return st;
     }
     return CRUSH_OK;
