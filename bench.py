@@ -344,7 +344,7 @@ def batched_section(n, plain_sample, oracle_sample, device, world=1):
     batched_cps = n / (t1 - t0)
     out = {"crashes": n, "elements": elems, "wall_s": t1 - t0, "crashes_per_s": batched_cps,
            "elem_upd_per_s": eu / (t1 - t0), "steps_mean": statistics.mean(steps), "steps_max": max(steps),
-           "path": "crush_batch_solve: a context from the first sixteenth of the elements starts the run, the rest join it "
+           "path": "crush_batch_solve: a context from the first eighth of the elements starts the run, the rest join it "
                    "group by group at step-graph boundaries (set-up overlapping the run)",
            "one_shot": {"create_s": t3 - t2, "run_s": t4 - t3, "crashes_per_s": n / (t4 - t2), "gpu_launches": int(launches),
                         "slave_lanes": lanes, "path": "crush_batch_create of all crashes, then crush_batch_run"},

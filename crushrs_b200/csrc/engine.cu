@@ -1510,19 +1510,19 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
     std::vector<std::pair<long long, long long>> tab_ranges;  // appending: chunk-table entries the main stream updates
     Stager stager;
     stager.init(c->stream, sizeof(double) * 6 * N + sizeof(uint32_t) * 27 * E);
-    if (appending) {
-        // model, incidence-numbering, contact and vehicle arrays of the new
-        // slots, generously: copies beyond the arena go direct (and wait)
-        const size_t want = 2 * (96 * (size_t)N + 64 * (size_t)E + 64 * (size_t)(tot.face - base[0].face) + 64 * (size_t)(tot.ste - base[0].ste) +
-                                 8 * (size_t)(tot.stoff - base[0].stoff)) + (1u << 20);
+    // A small addition (one or a few requests) packs its uploads into the
+    // context's pinned arena, allocated once at ARENA_BYTES; a larger one
+    // goes through the staging buffers (several threads fill them). Pinned
+    // memory is never freed or grown while a run is open: freeing it waits
+    // for the whole device.
+    constexpr size_t ARENA_BYTES = size_t(64) << 20;
+    const size_t want = 96 * (size_t)N + 64 * (size_t)E + 64 * (size_t)(tot.face - base[0].face) + 16 * (size_t)(tot.ste - base[0].ste) +
+                        8 * (size_t)(tot.stoff - base[0].stoff) + 64 * (size_t)(tot.slave - base[0].slave) + (1u << 20);
+    if (appending && want <= ARENA_BYTES) {
         CK(cudaEventSynchronize(c->ev_arena));  // the previous set-up's copies are done
-        if (want > c->arena_cap) {
-            if (c->arena) CK(cudaFreeHost(c->arena));
-            c->arena = nullptr;
-            c->arena_cap = 0;
-            const size_t cap = std::max<size_t>(want, 32u << 20);
-            CK(cudaMallocHost(&c->arena, cap));
-            c->arena_cap = cap;
+        if (!c->arena) {
+            CK(cudaMallocHost(&c->arena, ARENA_BYTES));
+            c->arena_cap = ARENA_BYTES;
         }
         stager.use_arena(c->arena, c->arena_cap, c->ev_arena);
     }
@@ -2957,12 +2957,12 @@ int run_to_end(crush_ctx* c) {
 }
 
 // Set-up of a batch pipelined with its run (crush_batch_solve): a context
-// with room for every model is created from the first sixteenth of the
-// elements and begins its run; each later group joins the open run at the
-// next step-graph boundary (crush_batch_append's path: its host set-up runs
+// with room for every model is created from the first eighth of the
+// elements and begins its run; each later eighth joins the open run at a
+// step-graph boundary (crush_batch_append's path: its host set-up runs
 // while the steps issued before it run, its device set-up on the set-up
-// stream), one group per 20-step chunk, so the set-up of all but the first
-// group is hidden behind the run. Every model's results equal its own run
+// stream), so the set-up of all but the first group is hidden behind the
+// run. Every model's results equal its own run
 // (a slot's steps do not depend on when it joined). Models that the room
 // estimate cannot take run in a further context after this one.
 int solve_models(const crush_model_desc* const* descs, int n, int device, crush_results* out) {
@@ -2980,7 +2980,7 @@ int solve_models(const crush_model_desc* const* descs, int n, int device, crush_
         }
         total += std::max<int64_t>(d->n_hexes, 1);
     }
-    constexpr int GROUPS = 16;
+    constexpr int GROUPS = 8;
     // group ends: model k closes group g when the running element count reaches g / GROUPS of the total
     std::vector<int> ends;
     long long acc = 0;
@@ -2995,13 +2995,24 @@ int solve_models(const crush_model_desc* const* descs, int n, int device, crush_
     if (st != CRUSH_OK) return st;
     int placed = ends[0];
     const long long per = c->period > 0 ? c->period : 20;
+    // Periods issued before each group joins: doubled (up to 8) whenever the
+    // device finished them before the group's set-up did.
+    long long periods = 1;
+    cudaEvent_t issued = nullptr;
+    CK(cudaEventCreateWithFlags(&issued, cudaEventDisableTiming));
+    struct EventGuard {
+        cudaEvent_t e;
+        ~EventGuard() { cudaEventDestroy(e); }
+    } issued_guard{issued};
     for (size_t g = 1; g < ends.size(); ++g) {
-        st = issue_steps(c.get(), per);
+        st = issue_steps(c.get(), periods * per);
         if (st != CRUSH_OK) return st;
+        CK(cudaEventRecord(issued, c->stream));
         st = add_slots(c.get(), descs + placed, ends[g] - placed, false, nullptr);
         if (st == CRUSH_ERR_BUSY) break;  // beyond the room estimate: the rest run afterwards
         if (st != CRUSH_OK) return st;
         placed = ends[g];
+        if (cudaEventQuery(issued) == cudaSuccess) periods = std::min<long long>(2 * periods, 8);
     }
     // to the end: every slot, the last joined included
     long long cap = 0;

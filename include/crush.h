@@ -431,7 +431,7 @@ typedef struct crush_capacity {
 int crush_batch_create_reserved(const crush_model_desc* const* descs, int n, int device, const crush_capacity* room, crush_ctx** out);
 /* Runs n models as one batch and writes each one's results to out[k]: the
  * one-call form of crush_batch_create + crush_batch_run, with the set-up
- * pipelined with the run (the first sixteenth of the elements starts the
+ * pipelined with the run (the first eighth of the elements starts the
  * run; the other models join it group by group at step-graph boundaries,
  * their set-up overlapping the steps in flight). Results are those of each
  * model run alone. The descriptions must stay valid for the call. */
