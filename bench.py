@@ -417,6 +417,9 @@ def serving_pool(n):
     return [S.Model.build(S.serve_query(i)[1]) for i in range(n)]
 
 
+SERVE_QUEUE = 1024
+
+
 def serving_section(rate, seconds, device, pool):
     """The crash server under an open-loop Poisson stream at `rate` req/s
     for `seconds` of arrivals (continuous batching: requests join running
@@ -425,13 +428,17 @@ def serving_section(rate, seconds, device, pool):
 
     n = max(1, int(rate * seconds))
     models = [pool[i % len(pool)] for i in range(n)]
-    with Server(device=device) as srv:
-        res, wall, _ = open_loop(srv, models, rate=rate)
+    # admission control: at most SERVE_QUEUE requests wait; arrivals beyond
+    # are refused (counted), as a service under overload sheds load
+    with Server(device=device, max_queue=SERVE_QUEUE) as srv:
+        res, wall, tickets = open_loop(srv, models, rate=rate)
         st = srv.stats()
+    refused = sum(1 for t in tickets if t < 0)
     lat = sorted(r.finish_s - r.submit_s for r in res.values())
     wait = sorted(r.start_s - r.submit_s for r in res.values())
     pick = lambda xs, q: xs[min(len(xs) - 1, int(q * len(xs)))]
-    return {"rate_req_per_s": rate, "seconds": seconds, "crashes": len(res), "crashes_per_s": len(res) / wall, "wall_s": wall,
+    return {"rate_req_per_s": rate, "seconds": seconds, "arrivals": n, "refused": refused, "queue_limit": SERVE_QUEUE,
+            "crashes": len(res), "crashes_per_s": len(res) / wall, "wall_s": wall,
             "p50_ms": 1e3 * pick(lat, 0.5), "p99_ms": 1e3 * pick(lat, 0.99), "admission_wait_p50_ms": 1e3 * pick(wait, 0.5),
             "contexts": int(st.waves), "peak_gb": st.peak_bytes_in_use / 1e9,
             "elements_mean": sum(m.n_hexes for m in models) / n, "ok": all(r.status == 0 for r in res.values())}

@@ -257,6 +257,7 @@ class ServerConfig(C.Structure):
         ("hbm_budget_bytes", C.c_double),
         ("gather_ms", C.c_double),
         ("idle_ms", C.c_double),
+        ("max_queue", C.c_int32),
     ]
 
 

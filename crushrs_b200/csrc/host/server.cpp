@@ -454,6 +454,7 @@ int crush_server_create(const crush_server_config* config, crush_server** out) {
         if (config->hbm_budget_bytes > 0.0) c.hbm_budget_bytes = config->hbm_budget_bytes;
         if (config->gather_ms >= 0.0) c.gather_ms = config->gather_ms;
         if (config->idle_ms > 0.0) c.idle_ms = config->idle_ms;
+        if (config->max_queue > 0) c.max_queue = config->max_queue;
     }
     s->cfg = c;
     if (c.hbm_budget_bytes > 0.0) {
@@ -478,6 +479,11 @@ int crush_server_submit(crush_server* s, const crush_model_desc* desc, uint64_t*
         desc->n_parts <= 0 || !desc->materials || (desc->n_contacts > 0 && !desc->contacts) || (desc->n_vehicles > 0 && !desc->vehicles) ||
         (desc->n_fixed > 0 && !desc->fixed_nodes))
         return crush::fail(CRUSH_ERR_INVALID, "invalid model description");
+    auto full = [&]() { return s->cfg.max_queue > 0 && (int64_t)s->queue.size() >= (int64_t)s->cfg.max_queue; };
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (full()) return crush::fail(CRUSH_ERR_BUSY, "request queue full");
+    }
     Request r;
     r.model.reset(new OwnedModel(*desc));
     r.bytes = crush_model_footprint(desc);
@@ -485,6 +491,7 @@ int crush_server_submit(crush_server* s, const crush_model_desc* desc, uint64_t*
     r.check_key = schedule_key(desc->settings);
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stop) return crush::fail(CRUSH_ERR_BUSY, "server is shutting down");
+    if (full()) return crush::fail(CRUSH_ERR_BUSY, "request queue full");
     r.ticket = s->next_ticket++;
     r.submit_s = now_s(s->t0);
     if (ticket) *ticket = r.ticket;

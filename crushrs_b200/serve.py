@@ -19,17 +19,20 @@ class Server:
     """crush_server: waves of batched contexts on one GPU."""
 
     def __init__(self, device=0, max_waves=4, max_wave_slots=1024, chunk_steps=100, max_wave_elements=2_000_000,
-                 hbm_budget_bytes=0.0, gather_ms=2.0, idle_ms=200.0):
+                 hbm_budget_bytes=0.0, gather_ms=2.0, idle_ms=200.0, max_queue=0):
         self._lib = lib()
-        cfg = abi.ServerConfig(device, max_waves, max_wave_slots, chunk_steps, max_wave_elements, hbm_budget_bytes, gather_ms, idle_ms)
+        cfg = abi.ServerConfig(device, max_waves, max_wave_slots, chunk_steps, max_wave_elements, hbm_budget_bytes, gather_ms, idle_ms,
+                               max_queue)
         h = C.c_void_p()
         check(self._lib.crush_server_create(C.byref(cfg), C.byref(h)))
         self.h = h
 
     def submit(self, desc):
+        """Queue a model; its ticket, or None when the server's max_queue
+        requests already wait (the request is refused)."""
         t = C.c_uint64()
-        check(self._lib.crush_server_submit(self.h, C.byref(desc), C.byref(t)))
-        return t.value
+        st = check(self._lib.crush_server_submit(self.h, C.byref(desc), C.byref(t)), allow=(abi.CRUSH_OK, abi.CRUSH_ERR_BUSY))
+        return t.value if st == abi.CRUSH_OK else None
 
     def poll(self, max_results=256, wait_ms=0):
         out = (abi.ServerResult * max_results)()
@@ -126,17 +129,24 @@ def serve_share(server, models, rate, rank, parts, seed=1):
 def open_loop(server, models, rate, seed=1):
     """Submit `models` (objects with .desc) at Poisson arrival times of the
     given rate (req/s), open loop; returns (results by ticket, wall seconds,
-    ticket -> model index)."""
+    ticket -> model index). Requests the server refuses (its queue full) are
+    counted in the returned map under negative keys, without results."""
     rng = _Rng(seed)
     t0 = time.perf_counter()
     t_next = 0.0
     tickets = {}
     results = {}
+    refused = 0
     i = 0
-    while i < len(models) or len(results) < len(models):
+    while i < len(models) or len(results) < len(models) - refused:
         now = time.perf_counter() - t0
         while i < len(models) and t_next <= now:
-            tickets[server.submit(models[i].desc)] = i
+            t = server.submit(models[i].desc)
+            if t is None:
+                refused += 1
+                tickets[-refused] = i
+            else:
+                tickets[t] = i
             i += 1
             t_next += -math.log(1.0 - rng.uniform()) / rate
         wait = 0 if i < len(models) else 20

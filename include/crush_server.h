@@ -39,6 +39,8 @@ typedef struct crush_server_config {
     double hbm_budget_bytes;    /* device memory the contexts may hold together (0 = 80% of free memory) */
     double gather_ms;           /* while contexts run, a new context waits this long for more arrivals (default 2) */
     double idle_ms;             /* a context with no crash running waits this long for requests before it ends (default 200) */
+    int32_t max_queue;          /* admission control: a submit that finds this many requests waiting is refused with
+                                   CRUSH_ERR_BUSY, nothing copied (0 = no limit) */
 } crush_server_config;
 
 typedef struct crush_server_result {
@@ -58,7 +60,8 @@ typedef struct crush_server_stats {
 
 /* config may be NULL (defaults). */
 int crush_server_create(const crush_server_config* config, crush_server** out);
-/* Copies the model (the caller may free it on return) and queues it. */
+/* Copies the model (the caller may free it on return) and queues it;
+ * CRUSH_ERR_BUSY when max_queue requests already wait. */
 int crush_server_submit(crush_server* srv, const crush_model_desc* desc, uint64_t* ticket);
 /* Up to max finished results into out, waiting up to wait_ms for the first. */
 int crush_server_poll(crush_server* srv, crush_server_result* out, int max, int* n, int wait_ms);

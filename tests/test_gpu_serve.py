@@ -60,3 +60,32 @@ def test_admission_respects_the_memory_budget(queries, alone):
     assert st.peak_bytes_in_use <= budget
     for t, r in got.items():
         _same(r.results, alone[tickets[t]])
+
+
+def test_queue_limit_refuses_and_serves_the_rest(queries, alone):
+    """Admission control: with max_queue requests waiting, a submit is
+    refused (None) and copies nothing; every accepted request is answered
+    once, with its alone results, and refusals stop once the queue drains."""
+    with Server(max_waves=2, max_wave_slots=4, gather_ms=0.0, max_queue=2) as srv:
+        tickets = {}
+        refused = 0
+        for i, m in enumerate(queries):
+            t = srv.submit(m.desc)
+            if t is None:
+                refused += 1
+            else:
+                tickets[t] = i
+        got = {}
+        while len(got) < len(tickets):
+            for r in srv.poll(wait_ms=50):
+                assert r.ticket not in got
+                got[r.ticket] = r
+        late = srv.submit(queries[0].desc)  # the queue has drained
+        assert late is not None
+        while late not in got:
+            for r in srv.poll(wait_ms=50):
+                got[r.ticket] = r
+    assert refused + len(tickets) == len(queries) and len(tickets) >= 2
+    for t, i in tickets.items():
+        _same(got[t].results, alone[i])
+    _same(got[late].results, alone[0])
