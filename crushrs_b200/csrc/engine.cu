@@ -1108,6 +1108,7 @@ void append(std::vector<T>& dst, const std::vector<T>& src) {
 
 int begin_slots(crush_ctx* c, int s0, int s1);
 int search_now(crush_ctx* c);
+int search_added(crush_ctx* c, int k0, long long dyn0, long long gs0, long long st0, int brute0);
 static void free_bufs(crush_ctx* c, std::vector<void*>& bufs);
 
 // Adds n_desc models as slots [c->n_slots, c->n_slots + n_desc) at the
@@ -1127,6 +1128,9 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
     const int S0 = c->n_slots;
     const long long N0 = c->n_nodes, E0 = c->n_all, H0 = c->n_hc, Q0 = c->n_sc, QF0 = c->n_sc_free;
     const int P0 = c->n_parts, K0 = c->n_contacts;
+    // the contact lists' lengths before these slots (their entries follow)
+    const long long dyn0 = c->ca.n_dyn_faces, gs0 = c->ca.n_grid_slaves, st0 = c->ca.n_st_slaves;
+    const int brute0 = c->ca.n_brute;
     // ---- sizes and offsets of every new slot ----
     std::vector<Slot> slots(n_desc);
     long long N = 0, E = 0;
@@ -2021,9 +2025,7 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
         }
         CK(cudaEventRecord(c->ev_tab, main_stream));
     }
-    // the first step's contact search of every contact at the run's current
-    // X + u (the running slots' hits are found again, the same ones)
-    return search_now(c);
+    return search_added(c, K0, dyn0, gs0, st0, brute0);
 #undef TRY
 }
 
@@ -2254,6 +2256,29 @@ int search_now(crush_ctx* c) {
     launch_contact_search(c->stream, c->ca, c->nd(), c->ctls, 0, c->n_contacts, 0, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 1,
                           c->slave_lanes);
     return check_launch(c, contact_search_launches(c->ca, true, c->n_faces, c->n_slaves, 0, c->ca.n_buckets, 0));
+}
+
+// The first step's contact search of contacts [k0, n_contacts) (added to the
+// open run): the run's search over the tails of its lists — moving faces
+// from dyn0, dynamic-grid and static-grid entries from gs0 and st0,
+// exhaustive contacts from brute0 — and the new contacts' bucket range. The
+// running slots' hits (found beside the last step) stay as they are; the
+// search's shared bookkeeping is cleared as every search clears it.
+int search_added(crush_ctx* c, int k0, long long dyn0, long long gs0, long long st0, int brute0) {
+    if (c->n_contacts <= k0) return CRUSH_OK;
+    if (c->ca.exhaustive) return search_now(c);
+    ContactArrays v = c->ca;
+    v.dyn_faces += dyn0;
+    v.n_dyn_faces -= dyn0;
+    v.grid_slaves += gs0;
+    v.n_grid_slaves -= gs0;
+    v.st_slaves += st0;
+    v.n_st_slaves -= st0;
+    v.brute_contacts += brute0;
+    v.n_brute -= brute0;
+    const long long bk0 = c->tab_off_h[k0], bk1 = c->tab_off_h[c->n_contacts];
+    launch_contact_search(c->stream, v, c->nd(), c->ctls, k0, c->n_contacts, 0, c->n_faces, c->n_slaves, bk0, bk1, 1, c->slave_lanes);
+    return check_launch(c, contact_search_launches(v, true, c->n_faces, c->n_slaves, bk0, bk1, 0));
 }
 
 // Launch autotuner: times the run's contact pass (at the open run's state,
