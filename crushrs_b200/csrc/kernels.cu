@@ -128,18 +128,33 @@ __device__ bool reference_gradients(const double x[8][3], const double dn[8][3],
     return true;
 }
 
-__global__ void __launch_bounds__(128) k_setup_geometry(long long e_begin, long long n_all, const double* __restrict__ pos,
-                                                        const uint32_t* __restrict__ conn, const int32_t* __restrict__ part,
-                                                        const double* __restrict__ mat,
-                                                        const int64_t* __restrict__ hc_index, const uint32_t* __restrict__ elem_slot,
-                                                        long long stride,
-                                                        float4* __restrict__ planes, double* __restrict__ volume_out,
-                                                        double* __restrict__ lumped_out, double* __restrict__ dt_factor,
-                                                        double* __restrict__ elem_mass, int* __restrict__ bad,
-                                                        const int64_t* __restrict__ sc_index, long long n_sc,
-                                                        double* __restrict__ sc_geo) {
-    long long e = e_begin + (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= n_all) return;
+// Element set-up (HexGeometry::new, src/element.rs:141-162): centre
+// gradients, hourglass base vectors Γ, volume, consistent-mass row sums and
+// the hourglass stiffness H = A G K Gᵀ A (A = (ΓᵀΓ)⁻¹), with G K Gᵀ
+// accumulated per Gauss point as Mᵀ C M (M = (B_gp - B_c) Gᵀ, 6 x 12).
+// Eight lanes per element, one per Gauss point: each lane evaluates its
+// point's terms (the Mᵀ C M entries times det J, the consistent-mass
+// entries, det J) and every sum over the points is taken in point order by
+// shuffles, as a serial loop over the points adds them; the Gauss-Jordan
+// inverse is repeated by every lane, and the H entries and the stores are
+// split over the lanes. (One thread per element would keep the 12x12 and
+// 8x8 sums in local memory.)
+constexpr int GEO_LANES = 8, GEO_TPB = 128, GEO_PER_BLOCK = GEO_TPB / GEO_LANES;
+__global__ void __launch_bounds__(GEO_TPB) k_setup_geometry8(long long e_begin, long long n_all, const double* __restrict__ pos,
+                                                             const uint32_t* __restrict__ conn, const int32_t* __restrict__ part,
+                                                             const double* __restrict__ mat, const int64_t* __restrict__ hc_index,
+                                                             const uint32_t* __restrict__ elem_slot, long long stride,
+                                                             float4* __restrict__ planes, double* __restrict__ volume_out,
+                                                             double* __restrict__ lumped_out, double* __restrict__ dt_factor,
+                                                             double* __restrict__ elem_mass, int* __restrict__ bad,
+                                                             const int64_t* __restrict__ sc_index, long long n_sc,
+                                                             double* __restrict__ sc_geo) {
+    __shared__ double s_gkg[GEO_PER_BLOCK][78];
+    __shared__ double s_h[GEO_PER_BLOCK][80];
+    const int q = threadIdx.x % GEO_LANES, grp = threadIdx.x / GEO_LANES;
+    const long long e_raw = e_begin + (long long)blockIdx.x * GEO_PER_BLOCK + grp;
+    const bool live = e_raw < n_all;
+    const long long e = live ? e_raw : n_all - 1;  // lanes past the end take part in the shuffles only
     double x[8][3];
     uint32_t nid[8];
     for (int i = 0; i < 8; ++i) {
@@ -150,11 +165,7 @@ __global__ void __launch_bounds__(128) k_setup_geometry(long long e_begin, long 
     const double youngs = mat[4 * p], nu = mat[4 * p + 1], rho = mat[4 * p + 2], hourglass = mat[4 * p + 3];
     double dnc[8][3], gc[8][3], detc;
     shape_derivatives(0.0, 0.0, 0.0, dnc);
-    if (!reference_gradients(x, dnc, gc, &detc)) {
-        atomicExch(bad, 1);
-        return;
-    }
-    // Hourglass base vectors (src/element.rs:93-102).
+    bool ok = reference_gradients(x, dnc, gc, &detc);
     double gam[8][4];
     for (int a = 0; a < 4; ++a) {
         double hx[3] = {0.0, 0.0, 0.0};
@@ -165,98 +176,109 @@ __global__ void __launch_bounds__(128) k_setup_geometry(long long e_begin, long 
             gam[i][a] = c_modes[a][i] - dot;
         }
     }
-    // Isotropic stabilisation matrix with E_hg = hourglass * E (material.rs:662).
     const double ehg = hourglass * youngs;
     const double lam = ehg * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
     const double mu = ehg / (2.0 * (1.0 + nu));
-    // G K Gᵀ accumulated per Gauss point as Mᵀ C M with M = (B_gp - B_c) Gᵀ (6 x 12).
-    double gkg[12][12];
-    for (int r = 0; r < 12; ++r)
-        for (int c = 0; c < 12; ++c) gkg[r][c] = 0.0;
-    double mass[8][8];
-    for (int i = 0; i < 8; ++i)
-        for (int j = 0; j < 8; ++j) mass[i][j] = 0.0;
-    double volume = 0.0;
+    // this lane's Gauss point
     const double GAUSS = 0.5773502691896258;
-    for (int q = 0; q < 8; ++q) {
-        double xi = c_xi[q][0] * GAUSS, eta = c_xi[q][1] * GAUSS, zeta = c_xi[q][2] * GAUSS;
-        double dn[8][3], gq[8][3], detj;
+    const double xi = c_xi[q][0] * GAUSS, eta = c_xi[q][1] * GAUSS, zeta = c_xi[q][2] * GAUSS;
+    double detj;
+    double pm[4][3];
+    {
+        double dn[8][3], gq[8][3];
         shape_derivatives(xi, eta, zeta, dn);
-        if (!reference_gradients(x, dn, gq, &detj)) {
-            atomicExch(bad, 1);
-            return;
-        }
-        // P[b][d] = Σ_j γ_jb (g_q - g_c)_jd
-        double pm[4][3];
+        ok = reference_gradients(x, dn, gq, &detj) && ok;
         for (int b = 0; b < 4; ++b)
             for (int d = 0; d < 3; ++d) {
                 double s = 0.0;
                 for (int j = 0; j < 8; ++j) s += gam[j][b] * (gq[j][d] - gc[j][d]);
                 pm[b][d] = s;
             }
-        // M rows (Voigt xx, yy, zz, xy, yz, xz; engineering shear) over columns 3b + e.
-        double m[6][12];
-        for (int s = 0; s < 6; ++s)
-            for (int c = 0; c < 12; ++c) m[s][c] = 0.0;
-        for (int b = 0; b < 4; ++b) {
-            m[0][3 * b + 0] = pm[b][0];
-            m[1][3 * b + 1] = pm[b][1];
-            m[2][3 * b + 2] = pm[b][2];
-            m[3][3 * b + 0] = pm[b][1];
-            m[3][3 * b + 1] = pm[b][0];
-            m[4][3 * b + 1] = pm[b][2];
-            m[4][3 * b + 2] = pm[b][1];
-            m[5][3 * b + 0] = pm[b][2];
-            m[5][3 * b + 2] = pm[b][0];
-        }
-        // C M (normal block lam/lam+2mu, shear block mu).
-        double cm[6][12];
-        for (int c = 0; c < 12; ++c) {
-            double t0 = m[0][c], t1 = m[1][c], t2 = m[2][c];
-            cm[0][c] = (lam + 2.0 * mu) * t0 + lam * t1 + lam * t2;
-            cm[1][c] = lam * t0 + (lam + 2.0 * mu) * t1 + lam * t2;
-            cm[2][c] = lam * t0 + lam * t1 + (lam + 2.0 * mu) * t2;
-            cm[3][c] = mu * m[3][c];
-            cm[4][c] = mu * m[4][c];
-            cm[5][c] = mu * m[5][c];
-        }
-        for (int r = 0; r < 12; ++r)
-            for (int c = r; c < 12; ++c) {
-                double s = 0.0;
-                for (int t = 0; t < 6; ++t) s += m[t][r] * cm[t][c];
-                gkg[r][c] += s * detj;
-            }
-        volume += detj;
-        // Consistent mass rows, as src/element.rs:156-157 accumulates them.
-        double nq[8];
-        for (int i = 0; i < 8; ++i)
-            nq[i] = 0.125 * (1.0 + c_xi[i][0] * xi) * (1.0 + c_xi[i][1] * eta) * (1.0 + c_xi[i][2] * zeta);
-        for (int i = 0; i < 8; ++i)
-            for (int j = 0; j < 8; ++j) mass[i][j] += rho * nq[i] * nq[j] * detj;
     }
-    volume_out[e] = volume;
-    elem_mass[e] = volume * rho;
-    for (int i = 0; i < 8; ++i) {
-        double s = 0.0;
-        for (int j = 0; j < 8; ++j) s += mass[i][j];
-        lumped_out[8 * e + i] = s;
-    }
+    // Column col = 3 b + e' of M (rows xx, yy, zz, xy, yz, xz; the assignments
+    // of the per-element form, zeros where it leaves them).
+    auto mcol = [&](int col, double t[6]) {
+        const int b = col / 3, ee = col % 3;
+        for (int k = 0; k < 6; ++k) t[k] = 0.0;
+        if (ee == 0) {
+            t[0] = pm[b][0];
+            t[3] = pm[b][1];
+            t[5] = pm[b][2];
+        } else if (ee == 1) {
+            t[1] = pm[b][1];
+            t[3] = pm[b][0];
+            t[4] = pm[b][2];
+        } else {
+            t[2] = pm[b][2];
+            t[4] = pm[b][1];
+            t[5] = pm[b][0];
+        }
+    };
+    // G K G^T (upper triangle): each entry the point-ordered sum of the lanes' terms
     {
-        // Material::dilatational_wave_speed, src/material.rs:226; kernel.rs:73.
-        double mm = youngs * (1.0 - nu) / ((1.0 + nu) * (1.0 - 2.0 * nu));
-        dt_factor[e] = (1.0 - 0.36 * nu) / sqrt(mm / rho);
+        int k = 0;
+        for (int r = 0; r < 12; ++r) {
+            double mr[6];
+            mcol(r, mr);
+            for (int cc = r; cc < 12; ++cc, ++k) {
+                double mc[6], cm[6];
+                mcol(cc, mc);
+                cm[0] = (lam + 2.0 * mu) * mc[0] + lam * mc[1] + lam * mc[2];
+                cm[1] = lam * mc[0] + (lam + 2.0 * mu) * mc[1] + lam * mc[2];
+                cm[2] = lam * mc[0] + lam * mc[1] + (lam + 2.0 * mu) * mc[2];
+                cm[3] = mu * mc[3];
+                cm[4] = mu * mc[4];
+                cm[5] = mu * mc[5];
+                double s = 0.0;
+                for (int t = 0; t < 6; ++t) s += mr[t] * cm[t];
+                const double term = s * detj;
+                double acc = 0.0;
+                for (int g = 0; g < GEO_LANES; ++g) acc += __shfl_sync(0xffffffffu, term, g, GEO_LANES);
+                if (q == (k & (GEO_LANES - 1))) s_gkg[grp][h_index(r, cc)] = acc;
+            }
+        }
     }
+    // consistent mass rows and the volume, each summed over the points in order
+    double nq[8];
+    for (int i = 0; i < 8; ++i)
+        nq[i] = 0.125 * (1.0 + c_xi[i][0] * xi) * (1.0 + c_xi[i][1] * eta) * (1.0 + c_xi[i][2] * zeta);
+    double volume = 0.0;
+    for (int g = 0; g < GEO_LANES; ++g) volume += __shfl_sync(0xffffffffu, detj, g, GEO_LANES);
+    double lumped_i = 0.0;  // lane i < 8 keeps row i's sum
+    for (int i = 0; i < 8; ++i) {
+        double row = 0.0;
+        for (int j = 0; j < 8; ++j) {
+            const double term = rho * nq[i] * nq[j] * detj;
+            double mij = 0.0;
+            for (int g = 0; g < GEO_LANES; ++g) mij += __shfl_sync(0xffffffffu, term, g, GEO_LANES);
+            row += mij;
+        }
+        if (q == i) lumped_i = row;
+    }
+    // every lane of the element: did any point fail?
+    bool elem_ok = ok;
+    for (int g = 0; g < GEO_LANES; ++g) elem_ok = __shfl_sync(0xffffffffu, (int)ok, g, GEO_LANES) != 0 && elem_ok;
+    if (live && !elem_ok && q == 0) atomicExch(bad, 1);
     const long long h = hc_index[e];
     const long long sc = sc_index ? sc_index[e] : -1;
-    if (h < 0 && sc < 0) return;
-    if (sc >= 0) {  // an elastic element keeps its geometry in f64 (src/kernel.rs:53-91)
-        for (int i = 0; i < 8; ++i)
+    const bool store = live && elem_ok;
+    if (store) {
+        lumped_out[8 * e + q] = lumped_i;
+        if (q == 0) {
+            volume_out[e] = volume;
+            elem_mass[e] = volume * rho;
+            // Material::dilatational_wave_speed, src/material.rs:226; kernel.rs:73.
+            double mm = youngs * (1.0 - nu) / ((1.0 + nu) * (1.0 - 2.0 * nu));
+            dt_factor[e] = (1.0 - 0.36 * nu) / sqrt(mm / rho);
+        }
+        if (sc >= 0) {  // an elastic element keeps its geometry in f64 (src/kernel.rs:53-91)
+            const int i = q;
             for (int d = 0; d < 3; ++d) sc_geo[(SC_GRAD + 3 * i + d) * n_sc + sc] = gc[i][d];
-        sc_geo[SC_VOL * n_sc + sc] = volume;
-        for (int i = 0; i < 8; ++i)
+            if (q == 0) sc_geo[SC_VOL * n_sc + sc] = volume;
             for (int aa = 0; aa < 4; ++aa) sc_geo[(SC_GAMMA + 4 * i + aa) * n_sc + sc] = gam[i][aa];
+        }
     }
-    // A = (ΓᵀΓ)⁻¹ (GGᵀ = A⁻¹ ⊗ I3), by Gauss-Jordan with partial pivoting on 4x4.
+    // A = (ΓᵀΓ)⁻¹ by Gauss-Jordan with partial pivoting on 4x4 (every lane)
     double a[4][8];
     for (int r = 0; r < 4; ++r)
         for (int c = 0; c < 4; ++c) {
@@ -265,13 +287,14 @@ __global__ void __launch_bounds__(128) k_setup_geometry(long long e_begin, long 
             a[r][c] = s;
             a[r][4 + c] = (r == c) ? 1.0 : 0.0;
         }
-    for (int k = 0; k < 4; ++k) {
+    bool inv_ok = true;
+    for (int k = 0; k < 4 && inv_ok; ++k) {
         int pv = k;
         for (int r = k + 1; r < 4; ++r)
             if (fabs(a[r][k]) > fabs(a[pv][k])) pv = r;
         if (a[pv][k] == 0.0) {
-            atomicExch(bad, 2);
-            return;
+            inv_ok = false;
+            break;
         }
         if (pv != k)
             for (int c = 0; c < 8; ++c) {
@@ -287,36 +310,49 @@ __global__ void __launch_bounds__(128) k_setup_geometry(long long e_begin, long 
                 for (int c = 0; c < 8; ++c) a[r][c] -= f * a[k][c];
             }
     }
-    // H[(a,d),(b,e)] = Σ A[a][a'] GKG[(a',d),(b',e)] A[b'][b] (upper triangle).
-    float hs[80];
-    for (int k = 78; k < 80; ++k) hs[k] = 0.0f;
-    for (int r = 0; r < 12; ++r)
-        for (int c = r; c < 12; ++c) {
+    if (store && (h >= 0 || sc >= 0) && !inv_ok && q == 0) atomicExch(bad, 2);
+    __syncwarp();
+    // H entries (upper triangle), split over the lanes
+    for (int r = 0, k = 0; r < 12; ++r)
+        for (int c = r; c < 12; ++c, ++k) {
+            if ((k & (GEO_LANES - 1)) != q) continue;
             const int ar = r / 3, dr = r % 3, bc = c / 3, ec = c % 3;
             double s = 0.0;
             for (int a1 = 0; a1 < 4; ++a1)
                 for (int b1 = 0; b1 < 4; ++b1) {
-                    int rr = 3 * a1 + dr, cc = 3 * b1 + ec;
-                    double g = rr <= cc ? gkg[rr][cc] : gkg[cc][rr];
-                    s += a[ar][4 + a1] * g * a[b1][4 + bc];
+                    const int rr = 3 * a1 + dr, cc2 = 3 * b1 + ec;
+                    s += a[ar][4 + a1] * s_gkg[grp][h_index(rr, cc2)] * a[b1][4 + bc];
                 }
-            hs[h_index(r, c)] = (float)s;
-            if (sc >= 0) sc_geo[(SC_H + h_index(r, c)) * n_sc + sc] = s;
+            s_h[grp][h_index(r, c)] = s;
         }
+    __syncwarp();
+    if (!store || !inv_ok || (h < 0 && sc < 0)) return;
+    if (sc >= 0)
+        for (int k = q; k < 78; k += GEO_LANES) sc_geo[(SC_H + k) * n_sc + sc] = s_h[grp][k];
     if (h < 0) return;
-    float4* pl = planes;
-    pl[(P_CONN + 0) * stride + h] = make_float4(__uint_as_float(nid[0]), __uint_as_float(nid[1]), __uint_as_float(nid[2]), __uint_as_float(nid[3]));
-    pl[(P_CONN + 1) * stride + h] = make_float4(__uint_as_float(nid[4]), __uint_as_float(nid[5]), __uint_as_float(nid[6]), __uint_as_float(nid[7]));
-    float gf[24];
-    for (int i = 0; i < 8; ++i)
-        for (int d = 0; d < 3; ++d) gf[3 * i + d] = (float)gc[i][d];
-    for (int k = 0; k < 6; ++k) pl[(P_GRAD + k) * stride + h] = make_float4(gf[4 * k], gf[4 * k + 1], gf[4 * k + 2], gf[4 * k + 3]);
-    float gm[32];
-    for (int i = 0; i < 8; ++i)
-        for (int aa = 0; aa < 4; ++aa) gm[4 * i + aa] = (float)gam[i][aa];
-    for (int k = 0; k < 8; ++k) pl[(P_GAMMA + k) * stride + h] = make_float4(gm[4 * k], gm[4 * k + 1], gm[4 * k + 2], gm[4 * k + 3]);
-    for (int k = 0; k < 20; ++k) pl[(P_H + k) * stride + h] = make_float4(hs[4 * k], hs[4 * k + 1], hs[4 * k + 2], hs[4 * k + 3]);
-    pl[P_META * stride + h] = make_float4((float)volume, __uint_as_float((uint32_t)p), __uint_as_float((uint32_t)e), __uint_as_float(elem_slot[e]));
+    // the element's 37 planes, split over the lanes
+    for (int k = q; k < N_STATIC_PLANES; k += GEO_LANES) {
+        float4 v;
+        if (k < P_GRAD) {
+            const int o = 4 * (k - P_CONN);
+            v = make_float4(__uint_as_float(nid[o]), __uint_as_float(nid[o + 1]), __uint_as_float(nid[o + 2]), __uint_as_float(nid[o + 3]));
+        } else if (k < P_GAMMA) {
+            const int o = 4 * (k - P_GRAD);
+            v = make_float4((float)gc[(o) / 3][(o) % 3], (float)gc[(o + 1) / 3][(o + 1) % 3], (float)gc[(o + 2) / 3][(o + 2) % 3],
+                            (float)gc[(o + 3) / 3][(o + 3) % 3]);
+        } else if (k < P_H) {
+            const int i = k - P_GAMMA;  // gamma[4 i + a] = gam[i][a]
+            v = make_float4((float)gam[i][0], (float)gam[i][1], (float)gam[i][2], (float)gam[i][3]);
+        } else if (k < P_META) {
+            const int o = 4 * (k - P_H);
+            float f[4];
+            for (int t = 0; t < 4; ++t) f[t] = o + t < 78 ? (float)s_h[grp][o + t] : 0.0f;
+            v = make_float4(f[0], f[1], f[2], f[3]);
+        } else {
+            v = make_float4((float)volume, __uint_as_float((uint32_t)p), __uint_as_float((uint32_t)e), __uint_as_float(elem_slot[e]));
+        }
+        planes[k * stride + h] = v;
+    }
 }
 
 // Lumped nodal masses: Σ over incident (element, corner) in element order
@@ -2009,9 +2045,9 @@ void launch_setup_geometry(cudaStream_t s, long long e_begin, long long n_all, c
                            float4* planes, double* volume, double* lumped, double* dt_factor, double* elem_mass, int* bad,
                            const int64_t* sc_index, long long n_sc, double* sc_geo) {
     if (n_all <= e_begin) return;
-    k_setup_geometry<<<(unsigned)blocks_for(n_all - e_begin, 128), 128, 0, s>>>(e_begin, n_all, pos, conn_all, part, mat, hc_index, elem_slot,
-                                                                       stride, planes, volume, lumped, dt_factor, elem_mass, bad,
-                                                                       sc_index, n_sc, sc_geo);
+    k_setup_geometry8<<<(unsigned)blocks_for(n_all - e_begin, GEO_PER_BLOCK), GEO_TPB, 0, s>>>(
+        e_begin, n_all, pos, conn_all, part, mat, hc_index, elem_slot, stride, planes, volume, lumped, dt_factor, elem_mass, bad, sc_index,
+        n_sc, sc_geo);
 }
 void launch_node_masses(cudaStream_t s, long long n, const uint32_t* off, const uint32_t* slot, const double* lumped,
                         double* mass, double* inv_mass) {
