@@ -2198,17 +2198,14 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
         mark(6);
         return check_launch(c, n);
     }
-    const bool sep = c->any_separation && (step + 1) % 10 == 0 && c->va.n_vehicles > 0;
-    // no check between the full update and the step's end: one launch for both
-    const bool end_in_full = (step + 1) % 20 != 0 && !sep && !early;
-    if (end_in_full) launch_full_end(c->stream, el, nd, c->ctls, cr, c->va, c->slot_done, c->mass_flag, c->fused_counter);
-    else launch_full(c->stream, el, nd, c->ctls);
+    launch_full(c->stream, el, nd, c->ctls);
     ++n;
     mark(5);
     if ((step + 1) % 20 == 0) {
         launch_nonfinite(c->stream, nd, c->ctls);
         ++n;
     }
+    const bool sep = c->any_separation && (step + 1) % 10 == 0 && c->va.n_vehicles > 0;
     if (sep) {
         launch_vehicle_vx(c->stream, c->va, c->mass, c->v, c->ctls);
         ++n;
@@ -2219,10 +2216,8 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
         cudaStreamWaitEvent(c->stream, c->ev_join, 0);
         cudaStreamWaitEvent(c->stream, c->ev_join2, 0);
     }
-    if (!end_in_full) {
-        launch_step_end(c->stream, c->ctls, cr, c->va, sep ? 1 : 0, c->slot_done, c->mass_flag);
-        ++n;
-    }
+    launch_step_end(c->stream, c->ctls, cr, c->va, sep ? 1 : 0, c->slot_done, c->mass_flag);
+    ++n;
     // Time-history records of the slots whose step is a multiple of
     // history_steps (src/solver.rs:349-351); u, v and the forces are final.
     if (c->hist_on && (step + 1) % c->hist.steps == 0) {

@@ -865,36 +865,6 @@ __global__ void k_fused(ElementArrays el, NodeArrays nd, Control* ctls, ContactA
     }
 }
 
-// The full update with the step's end in the block that finishes last (as
-// k_fused ends it): for a step with no check between the two (no non-finite
-// or separation check, no early contact pass), one launch instead of two.
-__global__ void k_full_end(ElementArrays el, NodeArrays nd, Control* ctls, ContactArrays ca, VehicleArrays va, int* __restrict__ done_out,
-                           int* __restrict__ mass_flag, unsigned* __restrict__ counter) {
-    FOR_ACTIVE(nd.act_node, nd.n, 3, g) {
-        int d;
-        const long long n = active_entity(nd.act_node, g, 3, &d);
-        full_body(el, nd, ctls, n, d);
-    }
-    __shared__ int s_last;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        s_last = atomicAdd(counter, 1u) == gridDim.x - 1 ? 1 : 0;
-    }
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    if (threadIdx.x == 0) {
-        *mass_flag = 0;
-        *counter = 0;
-    }
-    for (int sl = threadIdx.x; sl < ca.n_slots; sl += blockDim.x) {
-        Control* ctl = ctls + sl;
-        if (!ctl->done) step_end_slot(ctl, sl, ca, va, 0);
-        done_out[sl] = ctl->done;
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Stable time step (src/kernel.rs:207-237, src/element.rs:176-186) and the
 // per-element added mass of selective mass scaling (src/kernel.rs:243-258).
@@ -2202,10 +2172,6 @@ void launch_build_active(cudaStream_t s, const ActiveBuild& b, const Control* ct
 void launch_step_end(cudaStream_t s, Control* ctls, const ContactArrays& ca, const VehicleArrays& va, int check_separation,
                      int* done_out, int* mass_flag) {
     k_step_end<<<(unsigned)blocks_for(ca.n_slots, 128), 128, 0, s>>>(ctls, ca, va, check_separation, done_out, mass_flag);
-}
-void launch_full_end(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, const ContactArrays& ca,
-                     const VehicleArrays& va, int* done_out, int* mass_flag, unsigned* block_counter) {
-    k_full_end<<<active_grid(nd.n, 3, TPB, GRID_CAP), TPB, 0, s>>>(el, nd, ctls, ca, va, done_out, mass_flag, block_counter);
 }
 void launch_fused(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, const ContactArrays& ca,
                   const VehicleArrays& va, int* done_out, int* mass_flag, unsigned* block_counter) {

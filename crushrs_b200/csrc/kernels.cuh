@@ -268,10 +268,6 @@ void launch_step_end(cudaStream_t s, Control* ctls, const ContactArrays& ca, con
 // pass over the nodes (the ordered corner-force gather, v, then v_half and u
 // of the next step from nd.f_ext_next), and the step's end for every slot
 // in the last block to finish (block_counter: one zeroed int, left zero).
-// The full update and the step's end (launch_step_end without the
-// separation check) in one launch; block_counter as launch_fused's.
-void launch_full_end(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, const ContactArrays& ca,
-                     const VehicleArrays& va, int* done_out, int* mass_flag, unsigned* block_counter);
 void launch_fused(cudaStream_t s, const ElementArrays& el, const NodeArrays& nd, Control* ctls, const ContactArrays& ca,
                   const VehicleArrays& va, int* done_out, int* mass_flag, unsigned* block_counter);
 // Contact pass over contacts [c0, c1) (faces [f0, f0 + n_faces), n_slaves
