@@ -1583,8 +1583,9 @@ __global__ void k_contact_slaves(ContactArrays ca, NodeArrays nd, Control* ctls,
 
 constexpr int ST_LANES = 2;  // lanes per entry of a static-grid contact (a box test, then a short bucket)
 
-// Contacts searched exhaustively (fewer faces than the grid threshold), one
-// block per contact: the contact's face geometry is staged in shared memory
+// Contacts searched exhaustively (fewer faces than the grid threshold), a
+// few blocks per contact (gridDim.y, brute_split) sharing its primary-node
+// entries: each block stages the contact's face geometry in shared memory
 // and each thread scans the faces in order for one primary node and stops at
 // the first hit, as src/contact.rs:115-157 does.
 constexpr int BRUTE_TPB = 128;
@@ -1607,7 +1608,9 @@ __global__ void __launch_bounds__(BRUTE_TPB) k_contact_brute(ContactArrays ca, N
     // face in order up to its first hit; the smallest hit index wins.
     const int lane = threadIdx.x % BRUTE_LANES;
     const long long s_end = ca.slave_off[c + 1];
-    for (long long base = ca.slave_off[c]; base < s_end; base += blockDim.x / BRUTE_LANES) {  // block-uniform
+    // the contact's entries are shared by gridDim.y blocks, in turns of a block's worth
+    const long long per_block = blockDim.x / BRUTE_LANES;
+    for (long long base = ca.slave_off[c] + blockIdx.y * per_block; base < s_end; base += gridDim.y * per_block) {  // block-uniform
         const long long s = base + threadIdx.x / BRUTE_LANES;
         const bool live = s < s_end;
         long long n = 0;
@@ -2190,6 +2193,13 @@ void launch_vehicle_vx(cudaStream_t s, const VehicleArrays& va, const double* ma
     k_vehicle_vx<<<(unsigned)(va.n_vehicles * va.vx_blocks), VEH_TPB, 0, s>>>(va, mass, v, ctls);
 }
 
+// Blocks per exhaustively searched contact: enough for about four blocks per
+// SM over all such contacts (each block stages the contact's faces), at most 8.
+unsigned brute_split(long long n_brute) {
+    const long long target = 4 * 148;
+    return (unsigned)std::min<long long>(8, std::max<long long>(1, (target + n_brute - 1) / std::max<long long>(n_brute, 1)));
+}
+
 void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
                            long long n_faces, long long n_slaves, long long bk0, long long bk1, int run_mode, int lanes,
                            cudaStream_t s_static) {
@@ -2216,10 +2226,12 @@ void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeAr
     // Exhaustive contacts: a block each (run: the listed ones; drop-in: the one contact if it is one).
     if (!ca.exhaustive) {
         if (run_mode && ca.n_brute > 0)
-            k_contact_brute<<<(unsigned)ca.n_brute, BRUTE_TPB, sizeof(FaceGeo) * ca.brute_max_faces, s>>>(ca, nd, ctls, ca.brute_contacts,
+            k_contact_brute<<<dim3((unsigned)ca.n_brute, brute_split(ca.n_brute)), BRUTE_TPB, sizeof(FaceGeo) * ca.brute_max_faces, s>>>(
+                ca, nd, ctls, ca.brute_contacts,
                                                                                                           0, 1, 0.0, nullptr);
         if (!run_mode && c1 == c0 + 1 && ca.is_brute_h && ca.is_brute_h[c0]) {
-            k_contact_brute<<<1, BRUTE_TPB, sizeof(FaceGeo) * BRUTE_MAX_FACES, s>>>(ca, nd, ctls, nullptr, c0, 0, 0.0, nullptr);
+            k_contact_brute<<<dim3(1, brute_split(1)), BRUTE_TPB, sizeof(FaceGeo) * BRUTE_MAX_FACES, s>>>(ca, nd, ctls, nullptr, c0, 0, 0.0,
+                                                                                                   nullptr);
             n_slaves = 0;
         }
         if (run_mode) n_slaves = ca.n_grid_slaves;
