@@ -477,7 +477,7 @@ def main():
     ap.add_argument("--batch", type=int, default=4096, help="crashes of the batched section (0: skip)")
     ap.add_argument("--plain-sample", type=int, default=64)
     ap.add_argument("--oracle-sample", type=int, default=4)
-    ap.add_argument("--serve-rates", default="200,500,1000,2000", help="req/s of the serving section ('' : skip)")
+    ap.add_argument("--serve-rates", default="100,200,500,1000,2000", help="req/s of the serving section ('' : skip)")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="seconds of arrivals per rate")
     ap.add_argument("--serve-pool", type=int, default=1024, help="distinct seeded queries the arrival stream cycles through")
     ap.add_argument("--schedule-steps", type=int, default=200, help="steps timed under each step schedule after the main region")
