@@ -307,7 +307,7 @@ class Tuning(C.Structure):
         ("step_fusion", C.c_int32),
         ("early_contact", C.c_int32),
         ("contact_ms", C.c_double * 6),
-        ("step_ms", C.c_double * 5),
+        ("step_ms", C.c_double * 6),
     ]
 
 

@@ -57,8 +57,9 @@ struct SchedCand {
     int forces;
     bool early;  // separate steps: the next step's contact forces beside this step's element forces
 };
-constexpr int N_CANDS = 5;
-constexpr SchedCand CANDS[N_CANDS] = {{false, 2, false}, {false, 3, false}, {false, 2, true}, {false, 3, true}, {true, 2, false}};
+constexpr int N_CANDS = 6;
+constexpr SchedCand CANDS[N_CANDS] = {{false, 2, false}, {false, 3, false}, {false, 2, true},
+                                     {false, 3, true},  {true, 2, false},  {true, 1, false}};
 // Without a trial (small contexts, short issues): separate passes with 8 SMs
 // left to the side streams, the fastest measured on one small crash and on
 // the 278k-element head-on (fused steps win only on large batches).

@@ -360,17 +360,18 @@ typedef struct crush_tuning {
     int32_t early_contact;       /* separate steps compute the next step's contact forces beside their element
                                     forces when the next step has no stable-dt check */
     double contact_ms[6];        /* measured contact pass with 1, 2, 4, 8, 16, 32 lanes (0 = not measured) */
-    double step_ms[5];           /* measured ms per step of the step graph under the trial's candidates: separate
+    double step_ms[6];           /* measured ms per step of the step graph under the trial's candidates: separate
                                     steps with forces_schedule 2 / 3, the same with early contact forces, fused
-                                    steps with 2; 0 = not measured */
+                                    steps with 2 / 1; 0 = not measured */
 } crush_tuning;
 /* Re-tune now, at the open run's current state (e.g. late in a crash, when
  * crushed faces change the search); the next step uses the new schedule.
  * The step schedule is tuned on the run's own steps: a run of a context of
- * 65,536+ hexahedra times five candidates (separate steps leaving 8 or 16
+ * 65,536+ hexahedra times six candidates (separate steps leaving 8 or 16
  * SMs of the element kernel's wave to the side streams, with or without the
- * next step's contact forces computed there; fused steps) over its first ten
- * step graphs, again every 1000 steps with the lanes, and keeps the fastest;
+ * next step's contact forces computed there; fused steps with the wave or a
+ * block per 256 elements) over its first twelve step graphs, again every
+ * 1000 steps with the lanes, and keeps the fastest;
  * smaller contexts take separate steps with 8 SMs left free. */
 int crush_autotune(crush_ctx* ctx, crush_tuning* out);
 int crush_get_tuning(const crush_ctx* ctx, crush_tuning* out);

@@ -98,4 +98,4 @@ def test_every_launch_schedule_gives_the_same_bits():
         _same(out[0][0], r)
         assert np.array_equal(out[0][1][0], u) and np.array_equal(out[0][1][1], v)
     sched, step_ms = out[-1][2]
-    assert sched in (0, 1, 2, 3) and len(step_ms) == 5 and all(x > 0.0 for x in step_ms)
+    assert sched in (0, 1, 2, 3) and len(step_ms) == 6 and all(x > 0.0 for x in step_ms)
