@@ -84,14 +84,14 @@ def test_every_launch_schedule_gives_the_same_bits():
     lane counts, fixed by crush_set_tuning, all compute the same run; the
     automatic schedule trial (a context of 65,536+ hexahedra times the
     schedules on its first step graphs) does too."""
-    m = S.Model.build(S.refined_headon(max_steps=200))
+    m = S.Model.build(S.refined_headon(max_steps=240))
     out = []
     for tuning in ((32, 0, 0, 0), (8, 1, 1, 1), (4, 2, 0, 1), (16, 3, 0, 0), None):
         ctx = Context(m.desc)
         if tuning is not None:
             ctx.set_tuning(*tuning)
         ctx.run_begin()
-        ctx.run_steps(200)
+        ctx.run_steps(240)  # the trial: 2 rounds x 6 candidates x 20 steps
         out.append((ctx.results(), ctx.state(), ctx.schedule()))
         ctx.close()
     for r, (u, v), _ in out[1:]:
