@@ -418,6 +418,7 @@ def serving_pool(n):
 
 
 SERVE_QUEUE = 1024
+TRIAL_STEPS = 240  # the engine's schedule trial: 2 rounds x 6 candidate schedules x a 20-step graph
 
 
 def serving_section(rate, seconds, device, pool):
@@ -568,14 +569,18 @@ def main():
     # from a short profiled region after it.
     ctx.set_profiling(1)
     ctx.run_steps_timed(args.warmup, phases=True)
-    # Untimed steps up to a step-graph boundary (the engine replays one
-    # captured graph per 20 steps), then two whole graph periods (an issue
-    # of two periods builds the graph), so the graph's capture and
-    # instantiation fall before the timed region.
+    # Untimed: steps up to a step-graph boundary (the engine replays one
+    # captured graph per 20 steps), the schedule trial (two rounds of its six
+    # candidate schedules, a graph period each), then the chosen schedule is
+    # kept for the rest of the run (no re-tuning, so no graph is captured
+    # inside the timed region) and its graph built over two periods.
     align = (-args.warmup) % 20
-    ctx.run_steps_timed(align + 40, phases=True)
-    first = args.warmup + align + 40
-    config["timed_steps"] = f"steps {first}..{first + args.steps} (warm-up: {args.warmup} steps, then {align + 40} more to a replayed step graph)"
+    ctx.run_steps_timed(align + TRIAL_STEPS, phases=True)
+    ctx.fix_schedule()
+    ctx.run_steps_timed(40, phases=True)
+    first = args.warmup + align + TRIAL_STEPS + 40
+    config["timed_steps"] = (f"steps {first}..{first + args.steps} (warm-up: {args.warmup} steps, {align} to a step-graph boundary, "
+                             f"the {TRIAL_STEPS}-step schedule trial, 40 on the kept schedule's graph)")
     barrier(world)
     launches0 = ctx.launches()
     # phase events of the last graph only; the force kernel's average comes

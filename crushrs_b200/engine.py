@@ -188,6 +188,15 @@ class Context:
         t.early_contact = early_contact
         check(self._lib.crush_set_tuning(self.h, C.byref(t)))
 
+    def fix_schedule(self):
+        """Keep the schedule the trial chose (lanes, element-kernel schedule,
+        fused or separate steps, early contact) for the rest of the run:
+        automatic re-tuning off."""
+        t = abi.Tuning()
+        check(self._lib.crush_get_tuning(self.h, C.byref(t)))
+        self.set_step_fusion(bool(t.step_fusion))
+        self.set_tuning(t.slave_lanes, t.forces_schedule, t.fused_contact_side, t.early_contact)
+
     def autotune(self):
         """Re-tune at the open run's current state; returns tuning()."""
         t = abi.Tuning()
