@@ -2967,7 +2967,8 @@ int run_to_end(crush_ctx* c) {
     int st = run_begin(c);
     if (st != CRUSH_OK) return st;
     int done = 0;
-    const long long chunk = c->period > 0 ? 10 * (long long)c->period : 200;
+    // chunks long enough for the schedule trial (2 rounds of the candidates, a period each)
+    const long long chunk = c->period > 0 ? 2 * N_CANDS * (long long)c->period : 200;
     long long total = 0;
     long long cap = 0;
     for (const Slot& sl : c->slots) cap = std::max<long long>(cap, sl.settings.max_steps > 0 ? sl.settings.max_steps : 2000000ll);
@@ -3043,10 +3044,10 @@ int solve_models(const crush_model_desc* const* descs, int n, int device, crush_
     // to the end: every slot, the last joined included
     long long cap = 0;
     for (const Slot& sl : c->slots) cap = std::max<long long>(cap, sl.settings.max_steps > 0 ? sl.settings.max_steps : 2000000ll);
-    cap += c->host_step + 10 * per;
+    cap += c->host_step + 2 * N_CANDS * per;
     int done = 0;
     while (!done && c->host_step < cap) {
-        st = run_steps(c.get(), 10 * per, &done);
+        st = run_steps(c.get(), 2 * N_CANDS * per, &done);
         if (st != CRUSH_OK) return st;
     }
     if (!done) return crush::fail(CRUSH_ERR_TIMEOUT, "batch did not finish within " + std::to_string(cap) + " steps");
