@@ -221,6 +221,41 @@ struct DeviceCache {
 };
 DeviceCache g_device_cache;
 
+// Pinned host buffers no longer in use, kept for the process and handed to
+// the next user of a size they fit (at most twice over): cudaFreeHost waits
+// for the whole device, which would stall every other context's steps (a
+// serving context ends every few seconds).
+struct PinnedCache {
+    std::mutex m;
+    std::multimap<size_t, void*> free;  // (bytes, buffer)
+};
+PinnedCache g_pinned_cache;
+// A kept pinned buffer of at least *bytes (its size written back), else a new one; null if pinning fails.
+void* pinned_take(size_t* bytes) {
+    {
+        std::lock_guard<std::mutex> lock(g_pinned_cache.m);
+        auto it = g_pinned_cache.free.lower_bound(*bytes);
+        if (it != g_pinned_cache.free.end() && it->first <= 2 * *bytes + (1u << 20)) {
+            void* p = it->second;
+            *bytes = it->first;
+            g_pinned_cache.free.erase(it);
+            return p;
+        }
+    }
+    void* p = nullptr;
+    if (cudaMallocHost(&p, *bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+// Keeps a pinned buffer whose copies have all finished.
+void pinned_give(void* p, size_t bytes) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(g_pinned_cache.m);
+    g_pinned_cache.free.emplace(bytes, p);
+}
+
 // A kept buffer of at least *bytes (its size written back), or null.
 void* device_take(int device, size_t* bytes) {
     std::lock_guard<std::mutex> lock(g_device_cache.m);
@@ -275,16 +310,22 @@ struct Stager {
             std::lock_guard<std::mutex> lock(g_pinned.m);
             if (!g_pinned.busy) {
                 if (g_pinned.cap < cap) {
-                    for (char*& b : g_pinned.buf)
-                        if (b) {
-                            cudaFreeHost(b);
+                    for (char*& b : g_pinned.buf) {
+                        pinned_give(b, g_pinned.cap);  // not in use (the pool is not busy)
+                        b = nullptr;
+                    }
+                    g_pinned.cap = 0;
+                    size_t got0 = cap, got1 = cap;
+                    g_pinned.buf[0] = static_cast<char*>(pinned_take(&got0));
+                    g_pinned.buf[1] = static_cast<char*>(pinned_take(&got1));
+                    if (g_pinned.buf[0] && g_pinned.buf[1]) {
+                        g_pinned.cap = std::min(got0, got1);
+                    } else {
+                        for (char*& b : g_pinned.buf) {
+                            pinned_give(b, b == g_pinned.buf[0] ? got0 : got1);
                             b = nullptr;
                         }
-                    g_pinned.cap = 0;
-                    if (cudaMallocHost(&g_pinned.buf[0], cap) == cudaSuccess && cudaMallocHost(&g_pinned.buf[1], cap) == cudaSuccess)
-                        g_pinned.cap = cap;
-                    else
-                        cudaGetLastError();
+                    }
                 }
                 if (g_pinned.cap >= cap) {
                     g_pinned.busy = true;
@@ -295,12 +336,14 @@ struct Stager {
                 }
             }
         }
-        for (int k = 0; k < 2; ++k)
-            if (cudaMallocHost(&buf[k], cap) != cudaSuccess) {
-                cudaGetLastError();
+        for (int k = 0; k < 2; ++k) {
+            size_t got = cap;
+            buf[k] = static_cast<char*>(pinned_take(&got));
+            if (!buf[k]) {
                 release();
                 return CRUSH_OK;  // fall back to direct copies
             }
+        }
         return CRUSH_OK;
     }
     void use_arena(char* base, size_t cap, cudaEvent_t done) {
@@ -343,7 +386,7 @@ struct Stager {
         arena = nullptr;
         if (s && buf[0]) cudaStreamSynchronize(s);  // the staging buffers' DMA (direct copies are staged on return)
         for (int k = 0; k < 2; ++k) {
-            if (buf[k] && !pooled) cudaFreeHost(buf[k]);
+            if (buf[k] && !pooled) pinned_give(buf[k], cap);
             if (ev[k]) cudaEventDestroy(ev[k]);
             buf[k] = nullptr;
             ev[k] = nullptr;
@@ -674,8 +717,8 @@ struct crush_ctx {
         if (setup) cudaStreamSynchronize(setup);
         if (ev_setup) cudaEventDestroy(ev_setup);
         if (ev_tab) cudaEventDestroy(ev_tab);
-        if (tab_pinned) cudaFreeHost(tab_pinned);
-        if (arena) cudaFreeHost(arena);
+        pinned_give(tab_pinned, sizeof(int) * tab_pinned_cap);
+        pinned_give(arena, arena_cap);
         if (ev_arena) cudaEventDestroy(ev_arena);
         if (setup) cudaStreamDestroy(setup);
         if (side) cudaStreamDestroy(side);
@@ -1526,8 +1569,10 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
     if (appending && want <= ARENA_BYTES) {
         CK(cudaEventSynchronize(c->ev_arena));  // the previous set-up's copies are done
         if (!c->arena) {
-            CK(cudaMallocHost(&c->arena, ARENA_BYTES));
-            c->arena_cap = ARENA_BYTES;
+            size_t got = ARENA_BYTES;
+            c->arena = static_cast<char*>(pinned_take(&got));
+            if (!c->arena) return crush::fail(CRUSH_ERR_OOM, "cannot pin the upload arena");
+            c->arena_cap = got;
         }
         stager.use_arena(c->arena, c->arena_cap, c->ev_arena);
     }
@@ -2008,12 +2053,13 @@ int add_slots(crush_ctx* c, const crush_model_desc* const* descs, int n_desc, bo
     if (n_tab > 0) {
         CK(cudaEventSynchronize(c->ev_tab));  // the previous append's copies are done
         if (2 * n_tab > c->tab_pinned_cap) {
-            if (c->tab_pinned) CK(cudaFreeHost(c->tab_pinned));
+            pinned_give(c->tab_pinned, sizeof(int) * c->tab_pinned_cap);  // its copies are done (ev_tab above)
             c->tab_pinned = nullptr;
             c->tab_pinned_cap = 0;
-            const size_t want = std::max<size_t>(2 * n_tab, 1 << 16);
-            CK(cudaMallocHost(&c->tab_pinned, sizeof(int) * want));
-            c->tab_pinned_cap = want;
+            size_t got = sizeof(int) * std::max<size_t>(2 * n_tab, 1 << 16);
+            c->tab_pinned = static_cast<int*>(pinned_take(&got));
+            if (!c->tab_pinned) return crush::fail(CRUSH_ERR_OOM, "cannot pin the chunk-table buffer");
+            c->tab_pinned_cap = got / sizeof(int);
         }
         int* hp = c->tab_pinned;
         for (auto& r : tab_ranges) {
