@@ -1589,8 +1589,8 @@ constexpr int ST_LANES = 2;  // lanes per entry of a static-grid contact (a box 
 // and each thread scans the faces in order for one primary node and stops at
 // the first hit, as src/contact.rs:115-157 does.
 constexpr int BRUTE_TPB = 128;
-constexpr int BRUTE_LANES = 4;
 constexpr int BRUTE_MAX_FACES = 255;  // 255 x 192 B fits the default 48 KB of shared memory
+template <int BRUTE_LANES>
 __global__ void __launch_bounds__(BRUTE_TPB) k_contact_brute(ContactArrays ca, NodeArrays nd, Control* ctls, const int* __restrict__ list,
                                                             int single, int run_mode, double dt_override, const double* __restrict__ masses) {
     extern __shared__ double sbuf[];
@@ -2199,6 +2199,24 @@ unsigned brute_split(long long n_brute) {
     const long long target = 4 * 148;
     return (unsigned)std::min<long long>(8, std::max<long long>(1, (target + n_brute - 1) / std::max<long long>(n_brute, 1)));
 }
+// Few such contacts (a serving-size context): 16 lanes per primary node,
+// each scanning every 16th face, and up to 16 blocks per contact, so that a
+// node's scan is a quarter as long; many (a large batch): 4 lanes. Every
+// choice finds the same first hit.
+template <int LANES>
+void launch_brute(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, const int* list, int single, unsigned n,
+                  unsigned split, size_t smem) {
+    k_contact_brute<LANES><<<dim3(n, split), BRUTE_TPB, smem, s>>>(ca, nd, ctls, list, single, list ? 1 : 0, 0.0, nullptr);
+}
+void launch_brute_any(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, const int* list, int single,
+                      long long n_brute, size_t smem) {
+    if (n_brute * 8 <= 4 * 148) {
+        const unsigned split = (unsigned)std::min<long long>(16, std::max<long long>(1, (16 * 148 + n_brute - 1) / std::max<long long>(n_brute, 1)));
+        launch_brute<16>(s, ca, nd, ctls, list, single, (unsigned)std::max<long long>(n_brute, 1), split, smem);
+    } else {
+        launch_brute<4>(s, ca, nd, ctls, list, single, (unsigned)n_brute, brute_split(n_brute), smem);
+    }
+}
 
 void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeArrays& nd, Control* ctls, int c0, int c1, long long f0,
                            long long n_faces, long long n_slaves, long long bk0, long long bk1, int run_mode, int lanes,
@@ -2226,12 +2244,9 @@ void launch_contact_search(cudaStream_t s, const ContactArrays& ca, const NodeAr
     // Exhaustive contacts: a block each (run: the listed ones; drop-in: the one contact if it is one).
     if (!ca.exhaustive) {
         if (run_mode && ca.n_brute > 0)
-            k_contact_brute<<<dim3((unsigned)ca.n_brute, brute_split(ca.n_brute)), BRUTE_TPB, sizeof(FaceGeo) * ca.brute_max_faces, s>>>(
-                ca, nd, ctls, ca.brute_contacts,
-                                                                                                          0, 1, 0.0, nullptr);
+            launch_brute_any(s, ca, nd, ctls, ca.brute_contacts, 0, ca.n_brute, sizeof(FaceGeo) * ca.brute_max_faces);
         if (!run_mode && c1 == c0 + 1 && ca.is_brute_h && ca.is_brute_h[c0]) {
-            k_contact_brute<<<dim3(1, brute_split(1)), BRUTE_TPB, sizeof(FaceGeo) * BRUTE_MAX_FACES, s>>>(ca, nd, ctls, nullptr, c0, 0, 0.0,
-                                                                                                   nullptr);
+            launch_brute_any(s, ca, nd, ctls, nullptr, c0, 1, sizeof(FaceGeo) * BRUTE_MAX_FACES);
             n_slaves = 0;
         }
         if (run_mode) n_slaves = ca.n_grid_slaves;
