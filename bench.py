@@ -570,17 +570,19 @@ def main():
     ctx.set_profiling(1)
     ctx.run_steps_timed(args.warmup, phases=True)
     # Untimed: steps up to a step-graph boundary (the engine replays one
-    # captured graph per 20 steps), the schedule trial (two rounds of its six
-    # candidate schedules, a graph period each), then the chosen schedule is
-    # kept for the rest of the run (no re-tuning, so no graph is captured
-    # inside the timed region) and its graph built over two periods.
+    # captured graph per 20 steps), TRIAL_STEPS more (where a context large
+    # enough holds the schedule trial: two rounds of its six candidate
+    # schedules, a graph period each), then the schedule is kept for the rest
+    # of the run (no re-tuning, so no graph is captured inside the timed
+    # region) and its graph built over two periods.
     align = (-args.warmup) % 20
     ctx.run_steps_timed(align + TRIAL_STEPS, phases=True)
     ctx.fix_schedule()
     ctx.run_steps_timed(40, phases=True)
     first = args.warmup + align + TRIAL_STEPS + 40
     config["timed_steps"] = (f"steps {first}..{first + args.steps} (warm-up: {args.warmup} steps, {align} to a step-graph boundary, "
-                             f"the {TRIAL_STEPS}-step schedule trial, 40 on the kept schedule's graph)")
+                             f"{TRIAL_STEPS} more (a context of 2M+ elements holds its schedule trial there), 40 on the kept "
+                             f"schedule's graph)")
     barrier(world)
     launches0 = ctx.launches()
     # phase events of the last graph only; the force kernel's average comes

@@ -2290,9 +2290,12 @@ int enqueue_step(crush_ctx* c, long long step, cudaEvent_t* ev = nullptr, bool c
 
 constexpr long long RETUNE_STEPS = 1000;
 // Contexts at least this large time the element-kernel schedules on their
-// own steps: which is fastest depends on how much of the next step's contact
-// pass the element kernel's SMs hold back.
-constexpr long long SCHED_TRIAL_MIN_ELEMENTS = 65536;
+// own steps, once, at the run's start: which is fastest depends on how much
+// of the next step's contact pass the element kernel's SMs hold back. The
+// trial builds a graph per candidate (milliseconds each), which a run of a
+// few hundred thousand elements does not win back (its candidates differ by
+// a few percent of a 0.13 ms step); a large batch does.
+constexpr long long SCHED_TRIAL_MIN_ELEMENTS = 2000000;
 
 
 // The contact search at the open run's current X + u, on the main stream:
@@ -2869,7 +2872,6 @@ int issue_steps(crush_ctx* c, long long n_steps) {
             st = autotune(c);
             if (st != CRUSH_OK) return st;
             c->last_tune_step = c->host_step;
-            c->sched_trial_pending = c->n_hc >= SCHED_TRIAL_MIN_ELEMENTS;
         }
         // A graph that is not built yet is built for an issue of two periods
         // or more, or at the second period since the graphs were dropped:

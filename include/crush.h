@@ -367,12 +367,12 @@ typedef struct crush_tuning {
 /* Re-tune now, at the open run's current state (e.g. late in a crash, when
  * crushed faces change the search); the next step uses the new schedule.
  * The step schedule is tuned on the run's own steps: a run of a context of
- * 65,536+ hexahedra times six candidates (separate steps leaving 8 or 16
+ * 2,000,000+ hexahedra times six candidates (separate steps leaving 8 or 16
  * SMs of the element kernel's wave to the side streams, with or without the
  * next step's contact forces computed there; fused steps with the wave or a
- * block per 256 elements) over its first twelve step graphs, again every
- * 1000 steps with the lanes, and keeps the fastest;
- * smaller contexts take separate steps with 8 SMs left free. */
+ * block per 256 elements) over its first twelve step graphs, once, and keeps
+ * the fastest; smaller contexts take separate steps with 8 SMs left free.
+ * The contact lanes are re-tuned every 1000 steps. */
 int crush_autotune(crush_ctx* ctx, crush_tuning* out);
 int crush_get_tuning(const crush_ctx* ctx, crush_tuning* out);
 /* Fixes the schedule to t's slave_lanes, forces_schedule,
