@@ -72,3 +72,22 @@ def test_ctypes_structs_match_the_headers():
         assert got[(cname, "__sizeof__")] == C.sizeof(py), cname
         for f in py._fields_:
             assert got[(cname, f[0])] == getattr(py, f[0]).offset, (cname, f[0])
+
+
+def test_batch_solve_rejects_bad_arguments_before_touching_a_device():
+    """crush_batch_solve checks its arguments first: no models, a null
+    model or a null output array is CRUSH_ERR_INVALID with a message."""
+    import ctypes as C
+
+    from crushrs_b200 import scenarios as S
+    from crushrs_b200.native import lib
+
+    L = lib()
+    m = S.Model.build(S.batch_headon(0))
+    arr = (C.POINTER(abi.ModelDesc) * 1)(C.pointer(m.desc))
+    out = (abi.Results * 1)()
+    assert L.crush_batch_solve(arr, 0, 0, out) == abi.CRUSH_ERR_INVALID
+    assert L.crush_batch_solve(arr, 1, 0, None) == abi.CRUSH_ERR_INVALID
+    nulls = (C.POINTER(abi.ModelDesc) * 1)()
+    assert L.crush_batch_solve(nulls, 1, 0, out) == abi.CRUSH_ERR_INVALID
+    assert L.crush_last_error().decode()
