@@ -258,6 +258,7 @@ class ServerConfig(C.Structure):
         ("gather_ms", C.c_double),
         ("idle_ms", C.c_double),
         ("max_queue", C.c_int32),
+        ("max_running", C.c_int32),
     ]
 
 

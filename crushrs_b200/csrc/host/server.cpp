@@ -138,6 +138,7 @@ struct crush_server {
     double budget = 0.0, in_use = 0.0, peak = 0.0;
     int active = 0;                   // running contexts
     std::map<int, int> accepting;     // schedule class -> running contexts of it that still take requests
+    std::map<int, std::pair<int, int>> load;  // accepting context id -> (schedule class, crashes running)
     bool stop = false;
     uint64_t next_ticket = 1;
     int64_t submitted = 0, completed = 0, contexts = 0;
@@ -292,14 +293,21 @@ void crush_server::run_context(std::vector<Request> first, int id, double bytes,
                 if (!got || stop) break;
             }
             if (open) {
-                batch = take(key, room.hexes - used, room.slots - (int)slots.size(), false);
+                load[id] = {key, running};
+                // With max_running crashes running here and room for another
+                // context, new requests are left to it (a crash's latency is
+                // its steps times its context's step, which grows with the
+                // crashes beside it).
+                const bool held = cfg.max_running > 0 && running >= cfg.max_running && active < cfg.max_waves;
+                if (!held) batch = take(key, room.hexes - used, room.slots - (int)slots.size(), false);
                 // A request of this class waits that does not fit the room
                 // left: this context takes no more, so the scheduler opens
                 // another for it.
                 bool waits = false;
                 for (auto& q : queue) waits = waits || q.check_key == key;
-                if (batch.empty() && waits) {
+                if (!held && batch.empty() && waits) {
                     --accepting[key];
+                    load.erase(id);
                     open = false;
                     cv_work.notify_all();
                 }
@@ -329,7 +337,10 @@ void crush_server::run_context(std::vector<Request> first, int id, double bytes,
                 // for another context; this one takes no more.
                 std::lock_guard<std::mutex> lk(mu);
                 for (auto it = batch.rbegin(); it != batch.rend(); ++it) queue.push_front(std::move(*it));
-                if (open) --accepting[key];
+                if (open) {
+                    --accepting[key];
+                    load.erase(id);
+                }
                 open = false;
                 cv_work.notify_all();
                 if (a != CRUSH_ERR_BUSY && a != CRUSH_ERR_UNSUPPORTED) {
@@ -364,6 +375,7 @@ void crush_server::run_context(std::vector<Request> first, int id, double bytes,
         if (open && ((int)slots.size() >= room.slots || used >= room.hexes)) {
             std::lock_guard<std::mutex> lk(mu);
             --accepting[key];
+            load.erase(id);
             open = false;
             cv_work.notify_all();
         }
@@ -376,6 +388,7 @@ void crush_server::run_context(std::vector<Request> first, int id, double bytes,
     tr.print(id, slots.size());
     std::lock_guard<std::mutex> lk(mu);
     if (open) --accepting[key];
+    load.erase(id);
     in_use -= bytes;
     --active;
     finished.push_back(id);
@@ -409,12 +422,21 @@ void crush_server::schedule() {
         // Classes that an accepting context serves take their requests
         // themselves; a request of another class (or with every context
         // full) opens a context.
+        // (With max_running, also when every accepting context of the class
+        // has that many crashes running.)
+        auto served = [&](int key) {
+            if (accepting[key] <= 0) return false;
+            if (cfg.max_running <= 0) return true;
+            for (auto& kv : load)
+                if (kv.second.first == key && kv.second.second < cfg.max_running) return true;
+            return false;
+        };
         const Request& head = queue.front();
-        if (accepting[head.check_key] > 0) continue;
+        if (served(head.check_key)) continue;
         // While other contexts run, give arrivals a moment to join this one.
         if (active > 0 && cfg.gather_ms > 0.0) {
             cv_work.wait_for(lk, std::chrono::duration<double, std::milli>(cfg.gather_ms));
-            if (queue.empty() || accepting[queue.front().check_key] > 0) continue;
+            if (queue.empty() || served(queue.front().check_key)) continue;
         }
         const crush_capacity room = room_within(cfg.max_wave_elements, cfg.max_wave_slots, budget - in_use, queue.front().elements);
         const double bytes = room_bytes(room);
@@ -426,6 +448,7 @@ void crush_server::schedule() {
         ++active;
         ++accepting[first.front().check_key];
         const int id = (int)contexts++;
+        load[id] = {first.front().check_key, (int)first.size()};
         workers.emplace_back(id, std::thread(&crush_server::run_context, this, std::move(first), id, bytes, room));
     }
 }
@@ -455,6 +478,7 @@ int crush_server_create(const crush_server_config* config, crush_server** out) {
         if (config->gather_ms >= 0.0) c.gather_ms = config->gather_ms;
         if (config->idle_ms > 0.0) c.idle_ms = config->idle_ms;
         if (config->max_queue > 0) c.max_queue = config->max_queue;
+        if (config->max_running > 0) c.max_running = config->max_running;
     }
     s->cfg = c;
     if (c.hbm_budget_bytes > 0.0) {

@@ -19,10 +19,10 @@ class Server:
     """crush_server: waves of batched contexts on one GPU."""
 
     def __init__(self, device=0, max_waves=4, max_wave_slots=1024, chunk_steps=100, max_wave_elements=2_000_000,
-                 hbm_budget_bytes=0.0, gather_ms=2.0, idle_ms=200.0, max_queue=0):
+                 hbm_budget_bytes=0.0, gather_ms=2.0, idle_ms=200.0, max_queue=0, max_running=0):
         self._lib = lib()
         cfg = abi.ServerConfig(device, max_waves, max_wave_slots, chunk_steps, max_wave_elements, hbm_budget_bytes, gather_ms, idle_ms,
-                               max_queue)
+                               max_queue, max_running)
         h = C.c_void_p()
         check(self._lib.crush_server_create(C.byref(cfg), C.byref(h)))
         self.h = h

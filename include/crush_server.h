@@ -41,6 +41,8 @@ typedef struct crush_server_config {
     double idle_ms;             /* a context with no crash running waits this long for requests before it ends (default 200) */
     int32_t max_queue;          /* admission control: a submit that finds this many requests waiting is refused with
                                    CRUSH_ERR_BUSY, nothing copied (0 = no limit) */
+    int32_t max_running;        /* a context with this many crashes running takes no new requests while another
+                                   context can be opened (within max_waves); 0 = no limit */
 } crush_server_config;
 
 typedef struct crush_server_result {
